@@ -1,0 +1,314 @@
+/*
+ * yr.h - C ABI of the B200 ray-casting hot path for YafRay 0.0.9.
+ *
+ * A YafRay host (scene, XML loader, light/shader plugin API) keeps building
+ * its scene as today and calls these entry points instead of the per-ray C++
+ * virtuals.  Plain C types only: no CUDA or torch types cross this boundary
+ * (streams are passed as `void*` = cudaStream_t).
+ *
+ * Every entry returns a yr_status; nothing calls exit() or throws across the
+ * ABI (the reference exits on internal inconsistencies, kdtree.cc:300).
+ * Device-side problems (iteration caps, stack overflow, corrupt trees) are
+ * written to a device status word and returned by the call that launched
+ * the kernel.
+ *
+ * Threading: calls are reentrant per (yr_scene, stream); one yr_scene may be
+ * used from one host thread at a time.  (The reference calls shoot() and
+ * illuminate() from N pthreads with a per-thread renderState_t,
+ * scene.h:51-73.)
+ */
+#ifndef YR_H
+#define YR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define YR_API __attribute__((visibility("default")))
+#else
+#define YR_API
+#endif
+
+typedef enum yr_status {
+    YR_OK = 0,
+    YR_ERR_INVALID_ARG = 1,     /* NULL pointer, bad index, bad size          */
+    YR_ERR_CUDA = 2,            /* a CUDA runtime call failed                  */
+    YR_ERR_OUT_OF_MEMORY = 3,   /* device or host allocation failed           */
+    YR_ERR_ITERATION_CAP = 4,   /* a device loop hit its iteration cap        */
+    YR_ERR_STACK_OVERFLOW = 5,  /* kd / object-tree stack deeper than the cap */
+    YR_ERR_BAD_TREE = 6,        /* node or primitive index out of range       */
+    YR_ERR_CANCELLED = 7,       /* the output sink asked to stop              */
+    YR_ERR_UNSUPPORTED = 8,     /* feature not on this path                   */
+    YR_ERR_EMPTY_SCENE = 9,     /* no objects / no triangles                  */
+    YR_ERR_NO_DEVICE = 10,      /* no CUDA device or kernel image missing     */
+    YR_ERR_TOO_LARGE = 11       /* request above a documented maximum size    */
+} yr_status;
+
+YR_API const char *yr_status_string(yr_status s);
+YR_API const char *yr_version(void);
+
+/* ------------------------------------------------------------------------
+ * Flattened kd-tree (the device format).
+ *
+ * Replaces kdTreeNode (kdtree.h:23-61): 8 bytes instead of 16 on 64-bit,
+ * because the leaf stores a 32-bit index instead of a pointer.
+ *   interior: word = bit pattern of the float split position,
+ *             flags = axis (0..2) | right_child << 2   (left child = this+1)
+ *   leaf:     flags = 3 | nprims << 2,
+ *             word  = triangle index when nprims == 1 (kdTreeNode::onePrimitive),
+ *                     else offset into `prims` (kdTreeNode::primitives)
+ * Triangle indices are local to the object (0..ntris-1); right_child is
+ * local to the object's node array.  `bound` is kdTree_t::treeBound
+ * (the triangle bound grown by 1e-4 of its diagonal, kdtree.cc:83-89).
+ * ------------------------------------------------------------------------ */
+typedef struct yr_kd_node {
+    uint32_t word;
+    uint32_t flags;
+} yr_kd_node;
+
+typedef struct yr_kdtree {
+    yr_kd_node *nodes;
+    uint32_t nnodes;
+    uint32_t *prims;
+    uint32_t nprims;
+    float bound[6];          /* min xyz, max xyz                               */
+    int32_t max_depth;       /* kdTree_t::maxDepth after the ctor's defaults  */
+    int32_t max_leaf_size;   /* kdTree_t::maxLeafSize                          */
+    float cost_ratio;        /* kdTree_t::costRatio (incl. the large-N penalty) */
+    float empty_bonus;
+} yr_kdtree;
+
+/* Build the SAH kd-tree of one mesh on the host, with the parameters that
+ * meshObject_t uses (mesh.cc:162,487: depth -1, leaf size -1, cost 1.2,
+ * empty bonus 0.40).  Replaces kdTree_t::kdTree_t (kdtree.cc:57-138).
+ * verts: 3*nverts floats; tris: 3*ntris vertex indices. */
+YR_API yr_status yr_kdtree_build(const float *verts, uint32_t nverts,
+                                 const uint32_t *tris, uint32_t ntris,
+                                 yr_kdtree **out);
+YR_API void yr_kdtree_free(yr_kdtree *tree);
+
+/* ------------------------------------------------------------------------
+ * Scene description.  The records below are also the on-disk layout of the
+ * "YRS1" scene files the tests and the benchmark exchange (little endian).
+ * ------------------------------------------------------------------------ */
+
+/* camera_t ctor arguments (camera.cc:27-87), pinhole (CM_PERSPECTIVE). */
+typedef struct yr_camera_desc {
+    float pos[3];
+    float look[3];
+    float up[3];             /* a POINT, as in the reference (vup = up - pos) */
+    int32_t resx, resy;
+    float aspect;            /* usually 1                                      */
+    float focal;             /* "focal": width-1 image plane at this distance  */
+} yr_camera_desc;
+
+enum { YR_TEX_NONE = 0, YR_TEX_MUSGRAVE_FBM = 1, YR_TEX_CLOUDS = 2 };
+enum { YR_NOISE_NEWPERLIN = 0 };
+
+/* genericShader_t (basicshaders.h:37-152) with at most one modulator
+ * (texture.cc:499-534, mode "mix", texco global/orco of an untransformed
+ * mesh, i.e. the hit position) driving a musgrave fBm texture
+ * (basictex.cc:656-709).  64 bytes of colour params + texture block. */
+typedef struct yr_shader_desc {
+    float color[3];          /* "color": diffuse albedo (scolor)               */
+    float specular[3];       /* "specular": Phong colour (ks)                  */
+    float hard;              /* "hard": Phong exponent                         */
+    uint32_t tex_type;       /* YR_TEX_*                                       */
+    float tex_color1[3];     /* musgrave "color1"                              */
+    float tex_color2[3];     /* musgrave "color2"                              */
+    float tex_H;             /* "H"                                            */
+    float tex_lacunarity;    /* "lacunarity"                                   */
+    float tex_octaves;       /* "octaves"                                      */
+    float tex_size;          /* texture "size" (p*size inside getFloat)        */
+    float tex_intensity;     /* "intensity" (iscale)                           */
+    float mod_color;         /* modulator "color": mix weight into C           */
+    float mod_size[3];       /* modulator sizex/y/z                            */
+    float mod_ofs[3];        /* modulator ofsx/y/z                             */
+    uint32_t tex_noise;      /* YR_NOISE_*                                     */
+    int32_t tex_depth;       /* clouds: turbulence octaves                     */
+    uint32_t tex_hard;       /* clouds: hard noise                             */
+    uint32_t reserved[1];
+} yr_shader_desc;
+
+enum { YR_LIGHT_POINT = 0, YR_LIGHT_AREA = 1, YR_LIGHT_HEMI = 2, YR_LIGHT_PATH = 3 };
+
+/* One record for every light plugin on the path:
+ *   point: pointlight.cc:70-90   (p[0] = "from")
+ *   area:  arealight.cc:235-254  (p[0..3] = "a","b","c","d", samples)
+ *   hemi:  hemilight.cc:117+     (samples, maxdist, use_QMC always)
+ *   path:  pathlight.cc:753-807  (samples, depth; use_QMC, cache off,
+ *          no photon maps, adaptive repetitions off) */
+typedef struct yr_light_desc {
+    uint32_t type;
+    float color[3];
+    float power;
+    float p[4][3];
+    int32_t samples;
+    int32_t depth;
+    float maxdist;
+    uint32_t cast_shadows;   /* point light "cast_shadows" (default 1)        */
+    uint32_t reserved[3];
+} yr_light_desc;
+
+/* Render parameters.  The pixel loop follows scene_t::render(renderArea_t&)
+ * (scene.cc:724-823) with every pixel resampled: sample 0 at the pixel
+ * centre, samples 1..spp-1 at the AA positions of one pass with
+ * AA_minsamples = spp-1.  QMC indices are explicit (see yr_render). */
+typedef struct yr_render_params {
+    float self_bias;         /* render "bias" (scene_t::self_bias, default 0.1) */
+    int32_t raydepth;        /* render "raydepth" (maxraylevel, default 3)     */
+    uint32_t spp;            /* camera samples per pixel (>= 1)               */
+    float aa_pixelwidth;     /* AA_pixelwidth (default 1)                      */
+    uint32_t seed;           /* Cranley-Patterson rotation seed               */
+    float background[3];     /* constant background colour (black = none)     */
+    uint32_t flags;          /* reserved, 0                                    */
+} yr_render_params;
+
+typedef struct yr_object_desc {
+    const float *verts;      /* 3*nverts                                       */
+    uint32_t nverts;
+    const uint32_t *tris;    /* 3*ntris                                        */
+    uint32_t ntris;
+    uint32_t shader;         /* index into the shader table; YR_PER_TRIANGLE =
+                                use tri_shaders (triangle_t::setShader)       */
+    uint32_t cast_shadows;   /* object3d_t::castShadows                        */
+    const uint32_t *tri_shaders; /* ntris shader indices when shader ==
+                                YR_PER_TRIANGLE, else ignored                 */
+    const yr_kdtree *tree;   /* optional prebuilt tree (e.g. flattened from
+                                YafRay's own kdTree_t); NULL = build here     */
+} yr_object_desc;
+
+#define YR_PER_TRIANGLE 0xffffffffu
+
+typedef struct yr_scene_desc {
+    const yr_object_desc *objects;
+    uint32_t nobjects;
+    const yr_shader_desc *shaders;
+    uint32_t nshaders;
+    const yr_light_desc *lights;
+    uint32_t nlights;
+    yr_camera_desc camera;
+    yr_render_params render;
+} yr_scene_desc;
+
+typedef struct yr_scene yr_scene;
+
+/* Upload the scene to `device`: builds missing kd-trees and the object tree
+ * (buildObjectTree, object3d.cc:30-53) on the host, flattens them, copies
+ * triangles as {a,Nx},{b,Ny},{c,Nz} float4 triples.  The library owns the
+ * device copies; yr_scene_destroy frees them. */
+YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene **out);
+YR_API yr_status yr_scene_destroy(yr_scene *scene);
+/* Host-side statistics of the uploaded scene. */
+typedef struct yr_scene_info {
+    uint32_t nobjects, ntriangles, nnodes, nprims, nlights;
+    uint64_t device_bytes;
+    double build_seconds;    /* host kd-tree + object-tree build time         */
+} yr_scene_info;
+YR_API yr_status yr_scene_info_get(const yr_scene *scene, yr_scene_info *info);
+/* Replace the colour parameters of the shaders / lights without a rebuild
+ * (used by the inverse-rendering loop). */
+YR_API yr_status yr_scene_set_params(yr_scene *scene, const yr_shader_desc *shaders,
+                                     const yr_light_desc *lights);
+
+/* ------------------------------------------------------------------------
+ * Ray queries (device pointers, asynchronous on `stream`).
+ * ------------------------------------------------------------------------ */
+typedef struct yr_ray {
+    float org[3];
+    float tmax;              /* "dis": <0 means infinity (mesh.cc:529)        */
+    float dir[3];            /* unit direction                                 */
+    uint32_t flags;          /* reserved, 0                                    */
+} yr_ray;
+
+typedef struct yr_hit {
+    float t;                 /* surfacePoint_t::Z()                            */
+    uint32_t object;         /* 0xffffffff = miss                              */
+    uint32_t triangle;       /* object-local triangle index                   */
+    uint32_t nodes_visited;  /* kd nodes + object-tree nodes touched          */
+} yr_hit;
+
+/* Closest hit over all objects: scene_t::firstHit (scene.cc:688-721):
+ * origin moved by dir*MIN_RAYDIST, objects front to back through the object
+ * tree, each object's kdTree_t::Intersect (kdtree.cc:591-727), Z > 0.
+ * `shadow_only` = 1 skips objects that do not cast shadows (firstHit's
+ * shadow argument). */
+YR_API yr_status yr_trace_closest(yr_scene *scene, const yr_ray *rays, uint32_t n,
+                                  yr_hit *hits, int shadow_only, void *stream);
+
+typedef struct yr_shadow_ray {
+    float p[3];              /* shading point sp.P()                           */
+    uint32_t object;         /* sp.getObject() (for the self_bias rule)        */
+    float l[3];              /* light point, or direction if flags&1          */
+    uint32_t flags;          /* bit0: l is a direction (isShadowed(dir))       */
+} yr_shadow_ray;
+
+/* scene_t::isShadowed (scene.cc:107-185): origin p+dir*self_bias for the
+ * point's own object, p+dir*MIN_RAYDIST for the others, any hit with
+ * 0 < t < |l-p| via kdTree_t::IntersectS (kdtree.cc:730-866). */
+YR_API yr_status yr_trace_shadow(yr_scene *scene, const yr_shadow_ray *rays, uint32_t n,
+                                 uint8_t *occluded, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Rendering.
+ * ------------------------------------------------------------------------ */
+typedef struct yr_render_stats {
+    uint64_t rays_primary;
+    uint64_t rays_shadow;
+    uint64_t rays_bounce;
+    double ms;               /* device time of the render (CUDA events)      */
+} yr_render_stats;
+
+/* Render the whole image: RGBA float, resy rows of resx pixels, row 0 at the
+ * top (colorOutput_t::putPixel(x, y) order).  `rgba` is a device pointer
+ * unless `rgba_on_host` != 0, in which case the library stages it.
+ * QMC: path, hemi and area-light samples use explicit Halton indices with a
+ * per-pixel Cranley-Patterson rotation (documented in DESIGN.md). */
+YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
+                           yr_render_stats *stats, void *stream);
+
+/* Render `count` independent scenes in one persistent launch with per-scene
+ * ray queues.  outs[i] are device pointers (RGBA float, scene i's size). */
+typedef struct yr_batch_params {
+    int32_t block_size;      /* 0 = autotuned                                  */
+    int32_t queue_tile;      /* pixels per work item, 0 = autotuned            */
+    int32_t use_graph;       /* capture the launch in a CUDA graph             */
+    int32_t reserved;
+} yr_batch_params;
+
+YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t count, float *const *outs,
+                                 const yr_batch_params *params, yr_render_stats *stats,
+                                 void *stream);
+
+/* ------------------------------------------------------------------------
+ * Adjoint.  Gradient of  L = sum_pixels w * |img - target|^2  ... see
+ * yr_backward_desc.  Parameter vector layout, per scene:
+ *   for each shader s: color[3], specular weight (the scalar that scales
+ *   "specular"), tex amplitude (tex_intensity), tex base colour (tex_color1[3])
+ *   for each light l: power
+ * ------------------------------------------------------------------------ */
+typedef struct yr_backward_desc {
+    const float *target;     /* device RGBA target image                      */
+    const float *image;      /* device RGBA forward image (from yr_render)    */
+    float loss_scale;        /* L = loss_scale * sum (img-target)^2 over RGB  */
+    uint32_t reserved;
+} yr_backward_desc;
+
+/* Number of floats in the parameter vector of `scene`. */
+YR_API uint32_t yr_param_count(const yr_scene *scene);
+/* Gather the current parameters into `params` (host pointer). */
+YR_API yr_status yr_params_get(const yr_scene *scene, float *params);
+/* Scatter `params` (host pointer) into the scene's shaders and lights. */
+YR_API yr_status yr_params_set(yr_scene *scene, const float *params);
+/* dparams: device pointer, yr_param_count floats, overwritten. */
+YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, float *dparams,
+                             float *loss_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* YR_H */

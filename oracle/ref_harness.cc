@@ -1,0 +1,536 @@
+// Test harness around the UNMODIFIED YafRay 0.0.9 reference (linked from
+// objects built from /root/reference by oracle/Makefile).  Test
+// infrastructure only: it generates golden vectors for tests/golden/ and is
+// the reference arm of bench.py; the product never links or runs it.
+//
+// Written in C++98 because the reference objects are built with -std=gnu++98.
+//
+//   yr_ref_harness tree    SCENE OUT           kd-trees + object tree
+//   yr_ref_harness rays    SCENE RAYS OUT      kd / scene ray queries
+//   yr_ref_harness camera  SCENE OUT           primary ray directions
+//   yr_ref_harness render  SCENE OUT THREADS [x0 x1 y0 y1]
+//                                              stock scene_t::render, float sink
+//   yr_ref_harness explicit SCENE OUT [x0 x1 y0 y1]
+//                                              index-explicit GI estimator
+//   yr_ref_harness noise   POINTS OUT          newPerlin / fBm / turbulence
+//   yr_ref_harness halton  OUT                 Halton setStart+getNext values
+//   yr_ref_harness shade   SCENE OUT           getSurface / fromLight probes
+//
+// Private members (kdTree_t::nodes, meshObject_t::triangles, scene_t::BTree)
+// are read by compiling the reference headers with private/protected
+// mapped to public; no reference source is changed.
+#define private public
+#define protected public
+#include "scene.h"
+#include "threadedscene.h"
+#include "mesh.h"
+#include "kdtree.h"
+#include "camera.h"
+#include "noise.h"
+#include "mcqmc.h"
+#include "texture.h"
+#include "geometree.h"
+#include "pointlight.h"
+#include "arealight.h"
+#include "hemilight.h"
+#include "pathlight.h"
+#include "basicshaders.h"
+#include "basictex.h"
+#undef private
+#undef protected
+
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/time.h>
+#include <map>
+#include <string>
+#include <vector>
+
+extern "C" {
+#include "../include/yr.h"
+}
+
+using namespace yafray;
+
+namespace yafray {
+// basictex.cc references the JPEG loader (jpeg.cc needs jpeglib.h, absent);
+// image textures are not on the path.
+cBuffer_t *load_jpeg(const char *name) { return NULL; }
+geomeTree_t<object3d_t> *buildObjectTree(std::list<object3d_t *> &obj_list);
+}
+
+static double now_s() {
+    struct timeval tv;
+    gettimeofday(&tv, NULL);
+    return tv.tv_sec + tv.tv_usec * 1e-6;
+}
+
+static void die(const char *msg) {
+    fprintf(stderr, "yr_ref_harness: %s\n", msg);
+    exit(2);
+}
+
+// ---------------------------------------------------------------- scene file
+struct SceneFile {
+    yr_camera_desc cam;
+    yr_render_params rp;
+    std::vector<yr_shader_desc> shaders;
+    std::vector<yr_light_desc> lights;
+    struct Obj {
+        uint32_t nv, nt, shader, cast;
+        std::vector<float> v;
+        std::vector<uint32_t> t;
+        std::vector<uint32_t> tri_shader;  // when shader == YR_PER_TRIANGLE
+    };
+    std::vector<Obj> objs;
+};
+
+static void rd(FILE *f, void *p, size_t n) {
+    if (n && fread(p, 1, n, f) != n) die("short read");
+}
+
+static void load_scene(const char *path, SceneFile &s) {
+    FILE *f = fopen(path, "rb");
+    if (!f) die("cannot open scene");
+    char magic[4];
+    rd(f, magic, 4);
+    if (memcmp(magic, "YRS1", 4)) die("bad scene magic");
+    uint32_t hdr[4];
+    rd(f, hdr, 16);
+    rd(f, &s.cam, sizeof(s.cam));
+    rd(f, &s.rp, sizeof(s.rp));
+    s.shaders.resize(hdr[1]);
+    if (hdr[1]) rd(f, &s.shaders[0], sizeof(yr_shader_desc) * hdr[1]);
+    s.lights.resize(hdr[2]);
+    if (hdr[2]) rd(f, &s.lights[0], sizeof(yr_light_desc) * hdr[2]);
+    s.objs.resize(hdr[0]);
+    for (uint32_t i = 0; i < hdr[0]; i++) {
+        uint32_t oh[4];
+        rd(f, oh, 16);
+        SceneFile::Obj &o = s.objs[i];
+        o.nv = oh[0];
+        o.nt = oh[1];
+        o.shader = oh[2];
+        o.cast = oh[3];
+        o.v.resize(3 * o.nv);
+        o.t.resize(3 * o.nt);
+        rd(f, &o.v[0], 4 * o.v.size());
+        rd(f, &o.t[0], 4 * o.t.size());
+        if (o.shader == YR_PER_TRIANGLE) {
+            o.tri_shader.resize(o.nt);
+            rd(f, &o.tri_shader[0], 4 * o.nt);
+        }
+    }
+    fclose(f);
+}
+
+// ------------------------------------------------------- reference objects
+struct RefScene {
+    scene_t *scene;
+    camera_t *camera;
+    std::vector<meshObject_t *> meshes;
+    std::vector<shader_t *> shaders;
+    std::vector<texture_t *> textures;
+    std::vector<light_t *> lights;
+    std::map<const object3d_t *, int> objindex;
+};
+
+static point3d_t P3(const float *p) { return point3d_t(p[0], p[1], p[2]); }
+static color_t C3(const float *p) { return color_t(p[0], p[1], p[2]); }
+
+static shader_t *make_shader(const yr_shader_desc &d, std::vector<texture_t *> &textures) {
+    // genericShader_t::factory defaults (basicshaders.cc:217-262)
+    genericShader_t *sh = new genericShader_t(C3(d.color), d.hard, (CFLOAT)1.0, color_t(0.0), color_t(0.0),
+                                              C3(d.specular), color_t(0.0), color_t(0.0), NULL, 0.0, (CFLOAT)1.0,
+                                              1.0, false, false, 0, 0, false, color_t(0.0));
+    if (d.tex_type != YR_TEX_NONE) {
+        texture_t *tex;
+        if (d.tex_type == YR_TEX_MUSGRAVE_FBM)
+            tex = new textureMusgrave_t(C3(d.tex_color1), C3(d.tex_color2), d.tex_H, d.tex_lacunarity,
+                                        d.tex_octaves, 1.0, 1.0, d.tex_size, d.tex_intensity, "newperlin", "fBm");
+        else
+            tex = new textureClouds_t(d.tex_depth, d.tex_size, d.tex_hard != 0, C3(d.tex_color1),
+                                      C3(d.tex_color2), "newperlin", "");
+        textures.push_back(tex);
+        modulator_t modu(tex);
+        modu.sizeX(d.mod_size[0]);
+        modu.sizeY(d.mod_size[1]);
+        modu.sizeZ(d.mod_size[2]);
+        modu.ofsX(d.mod_ofs[0]);
+        modu.ofsY(d.mod_ofs[1]);
+        modu.ofsZ(d.mod_ofs[2]);
+        modu.string2modetype("mix");
+        modu.color(d.mod_color);
+        modu.specular(0);
+        modu.hard(0);
+        modu.transmision(0);
+        modu.reflection(0);
+        modu.displace(0);
+        modu.string2maptype("flat");
+        modu.string2texcotype("global");
+        modu.string2cliptype("extend");
+        modu.string2texprojection("x", "y", "z");
+        sh->addModulator(modu);
+    }
+    return sh;
+}
+
+static light_t *make_light(const yr_light_desc &d) {
+    switch (d.type) {
+    case YR_LIGHT_POINT:
+        return new pointLight_t(P3(d.p[0]), C3(d.color), d.power, d.cast_shadows != 0);
+    case YR_LIGHT_AREA:
+        return new areaLight_t(P3(d.p[0]), P3(d.p[1]), P3(d.p[2]), P3(d.p[3]), d.samples, C3(d.color), d.power, 0,
+                               false);
+    case YR_LIGHT_HEMI:
+        return new hemiLight_t(d.samples, C3(d.color), d.power, d.maxdist, false, true);
+    case YR_LIGHT_PATH:
+        // use_QMC, no cache, adaptive repetitions off (threshold 1e9)
+        return new pathLight_t(d.samples, d.power, d.depth, 0, true, false, 1.0, 1e9f);
+    }
+    die("bad light type");
+    return NULL;
+}
+
+static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true) {
+    r.scene = scene_t::factory();
+    for (size_t i = 0; i < s.shaders.size(); i++) r.shaders.push_back(make_shader(s.shaders[i], r.textures));
+    for (size_t i = 0; i < s.objs.size(); i++) {
+        const SceneFile::Obj &o = s.objs[i];
+        std::vector<point3d_t> ver(o.nv);
+        for (uint32_t k = 0; k < o.nv; k++) ver[k] = P3(&o.v[3 * k]);
+        std::vector<triangle_t> ts(o.nt);
+        for (uint32_t k = 0; k < o.nt; k++)
+            ts[k] = triangle_t(&ver[o.t[3 * k]], &ver[o.t[3 * k + 1]], &ver[o.t[3 * k + 2]]);
+        if (o.shader == YR_PER_TRIANGLE)  // triangle_t::setShader, used by getSurface
+            for (uint32_t k = 0; k < o.nt; k++) ts[k].setShader(r.shaders.at(o.tri_shader[k]));
+        std::vector<vector3d_t> nor;
+        std::vector<GFLOAT> fuv;
+        std::vector<CFLOAT> fvcol;
+        meshObject_t *m = meshObject_t::factory(ver, nor, ts, fuv, fvcol);
+        m->setShader(r.shaders.at(o.shader == YR_PER_TRIANGLE ? o.tri_shader[0] : o.shader));
+        m->castShadows(o.cast != 0);
+        r.meshes.push_back(m);
+        r.objindex[m] = (int)i;
+        r.scene->addObject(m);
+    }
+    const yr_camera_desc &c = s.cam;
+    r.camera = new camera_t(P3(c.pos), P3(c.look), P3(c.up), c.resx, c.resy, c.aspect, c.focal, 0, 0, false,
+                            camera_t::CM_PERSPECTIVE, camera_t::BK_DISK1, camera_t::BB_NONE, 0);
+    r.scene->setCamera(r.camera);
+    r.scene->setBias(s.rp.self_bias);
+    r.scene->setMaxRayDepth(s.rp.raydepth);
+    r.scene->tonemap(false);
+    r.scene->clampRGB(false);
+    r.scene->alphaPremultiply(false);
+    r.scene->alphaMaskBackground(false);
+    r.scene->setFog(0, color_t(0.0));
+    if (with_lights)
+        for (size_t i = 0; i < s.lights.size(); i++) {
+            light_t *l = make_light(s.lights[i]);
+            r.lights.push_back(l);
+            r.scene->addLight(l);
+        }
+}
+
+static void wr(FILE *f, const void *p, size_t n) {
+    if (n && fwrite(p, 1, n, f) != n) die("short write");
+}
+
+// ------------------------------------------------------------------- tree
+static void cmd_tree(const SceneFile &s, const char *out) {
+    RefScene r;
+    build_ref(s, r, false);
+    FILE *f = fopen(out, "wb");
+    if (!f) die("cannot open output");
+    uint32_t n = (uint32_t)r.meshes.size();
+    wr(f, &n, 4);
+    for (size_t i = 0; i < r.meshes.size(); i++) {
+        meshObject_t *m = r.meshes[i];
+        kdTree_t *t = m->n_tree;
+        const triangle_t *base = &m->triangles[0];
+        std::vector<uint32_t> nodes, prims;
+        for (uint32_t k = 0; k < t->nextFreeNode; k++) {
+            const kdTreeNode &nd = t->nodes[k];
+            uint32_t word = 0;
+            if (nd.IsLeaf()) {
+                int np = nd.nPrimitives();
+                if (np == 1) word = (uint32_t)(nd.onePrimitive - base);
+                else if (np > 1) {
+                    word = (uint32_t)prims.size();
+                    for (int q = 0; q < np; q++) prims.push_back((uint32_t)(nd.primitives[q] - base));
+                }
+            } else {
+                float sp = nd.division;
+                memcpy(&word, &sp, 4);
+            }
+            nodes.push_back(word);
+            nodes.push_back(nd.flags);
+        }
+        uint32_t hdr[2] = {t->nextFreeNode, (uint32_t)prims.size()};
+        wr(f, hdr, 8);
+        float tb[6] = {t->treeBound.a.x, t->treeBound.a.y, t->treeBound.a.z,
+                       t->treeBound.g.x, t->treeBound.g.y, t->treeBound.g.z};
+        wr(f, tb, 24);
+        int32_t ip[2] = {t->maxDepth, t->maxLeafSize};
+        wr(f, ip, 8);
+        float fp[2] = {t->costRatio, t->eBonus};
+        wr(f, fp, 8);
+        bound_t ob = m->getBound();
+        float obf[6] = {ob.a.x, ob.a.y, ob.a.z, ob.g.x, ob.g.y, ob.g.z};
+        wr(f, obf, 24);
+        wr(f, &nodes[0], 4 * nodes.size());
+        if (!prims.empty()) wr(f, &prims[0], 4 * prims.size());
+    }
+    // object tree, depth-first preorder, left before right
+    geomeTree_t<object3d_t> *root = buildObjectTree(r.scene->obj_list);
+    std::vector<const geomeTree_t<object3d_t> *> stack, order;
+    stack.push_back(root);
+    while (!stack.empty()) {
+        const geomeTree_t<object3d_t> *nd = stack.back();
+        stack.pop_back();
+        order.push_back(nd);
+        if (!nd->isLeaf()) {
+            stack.push_back(nd->goRight());
+            stack.push_back(nd->goLeft());
+        }
+    }
+    std::map<const geomeTree_t<object3d_t> *, int> idx;
+    for (size_t i = 0; i < order.size(); i++) idx[order[i]] = (int)i;
+    uint32_t nn = (uint32_t)order.size();
+    wr(f, &nn, 4);
+    for (size_t i = 0; i < order.size(); i++) {
+        const geomeTree_t<object3d_t> *nd = order[i];
+        const bound_t &b = nd->getBound();
+        float bb[6] = {b.a.x, b.a.y, b.a.z, b.g.x, b.g.y, b.g.z};
+        int32_t lr[2];
+        if (nd->isLeaf()) {
+            lr[0] = -1;
+            lr[1] = r.objindex[nd->getElement()];
+        } else {
+            lr[0] = idx[nd->goLeft()];
+            lr[1] = idx[nd->goRight()];
+        }
+        wr(f, bb, 24);
+        wr(f, lr, 8);
+    }
+    fclose(f);
+}
+
+// ------------------------------------------------------------------- rays
+// Ray record: u32 mode, u32 object, f32 from[3], f32 dir[3], f32 dist, f32 l[3]
+//   mode 0: kdTree_t::Intersect on `object`  -> u32 hit, u32 tri, f32 Z
+//   mode 1: kdTree_t::IntersectS on `object` -> u32 hit, u32 tri, f32 0
+//   mode 2: scene_t::firstHit(from, dir, shadow=false) -> u32 hit, u32 obj, u32 tri, f32 Z
+//   mode 3: scene_t::isShadowed(sp{P=from, object}, l) -> u32 occluded
+//   mode 4: scene_t::firstHit(from, dir, shadow=true)  (as mode 2)
+struct RayRec {
+    uint32_t mode, object;
+    float from[3], dir[3], dist, l[3];
+};
+
+static void cmd_rays(const SceneFile &s, const char *rays_path, const char *out) {
+    RefScene r;
+    build_ref(s, r, false);
+    r.scene->BTree = buildObjectTree(r.scene->obj_list);
+    FILE *fi = fopen(rays_path, "rb");
+    if (!fi) die("cannot open rays");
+    uint32_t n;
+    rd(fi, &n, 4);
+    std::vector<RayRec> rays(n);
+    if (n) rd(fi, &rays[0], sizeof(RayRec) * n);
+    fclose(fi);
+    FILE *f = fopen(out, "wb");
+    if (!f) die("cannot open output");
+    renderState_t state;
+    for (uint32_t i = 0; i < n; i++) {
+        const RayRec &q = rays[i];
+        point3d_t from = P3(q.from);
+        vector3d_t dir(q.dir[0], q.dir[1], q.dir[2]);
+        uint32_t o[4] = {0, 0xffffffffu, 0xffffffffu, 0};
+        if (q.mode == 0 || q.mode == 1) {
+            meshObject_t *m = r.meshes.at(q.object);
+            const triangle_t *base = &m->triangles[0];
+            triangle_t *hitt = NULL;
+            PFLOAT dis = q.dist;
+            if (dis < 0) dis = std::numeric_limits<PFLOAT>::infinity();
+            PFLOAT Z = dis;
+            bool h = q.mode == 0 ? m->n_tree->Intersect(from, dir, dis, &hitt, Z)
+                                 : m->n_tree->IntersectS(from, dir, dis, &hitt);
+            o[0] = h;
+            if (h && hitt) o[2] = (uint32_t)(hitt - base);
+            float zf = q.mode == 0 && h ? Z : 0.f;
+            memcpy(&o[3], &zf, 4);
+            o[1] = q.object;
+        } else if (q.mode == 2 || q.mode == 4) {
+            surfacePoint_t sp;
+            bool h = r.scene->firstHit(state, sp, from, dir, q.mode == 4);
+            o[0] = h;
+            if (h) {
+                o[1] = r.objindex[sp.getObject()];
+                meshObject_t *m = r.meshes.at(o[1]);
+                o[2] = (uint32_t)((const triangle_t *)sp.getOrigin() - &m->triangles[0]);
+                float zf = sp.Z();
+                memcpy(&o[3], &zf, 4);
+            }
+        } else if (q.mode == 3) {
+            surfacePoint_t sp(r.meshes.at(q.object), from, from, vector3d_t(0, 0, 1), vector3d_t(0, 0, 1), 0, 0,
+                              color_t(0.0), 0);
+            o[0] = r.scene->isShadowed(state, sp, P3(q.l));
+        }
+        wr(f, o, 16);
+    }
+    fclose(f);
+}
+
+// ----------------------------------------------------------------- camera
+static void cmd_camera(const SceneFile &s, const char *out) {
+    RefScene r;
+    build_ref(s, r, false);
+    FILE *f = fopen(out, "wb");
+    for (int i = 0; i < s.cam.resy; i++)
+        for (int j = 0; j < s.cam.resx; j++) {
+            PFLOAT wt;
+            vector3d_t d = r.camera->shootRay((PFLOAT)j + 0.5f, (PFLOAT)i + 0.5f, wt);
+            float v[3] = {d.x, d.y, d.z};
+            wr(f, v, 12);
+        }
+    fclose(f);
+}
+
+// ----------------------------------------------------------------- render
+class floatSink_t : public colorOutput_t {
+  public:
+    floatSink_t(int w, int h) : W(w), H(h), img(4 * (size_t)w * h, 0.f) {}
+    virtual bool putPixel(int x, int y, const color_t &c, CFLOAT alpha, PFLOAT depth) {
+        float *p = &img[4 * ((size_t)y * W + x)];
+        p[0] = c.getR();
+        p[1] = c.getG();
+        p[2] = c.getB();
+        p[3] = alpha;
+        return true;
+    }
+    virtual void flush() {}
+    int W, H;
+    std::vector<float> img;
+};
+
+static void cmd_render(const SceneFile &s, const char *out, int threads, const int *crop) {
+    RefScene r;
+    build_ref(s, r, true);
+    scene_t *sc = r.scene;
+    threadedscene_t *tsc = NULL;
+    if (threads > 1) {
+        // threadedscene_t holds its own copy of the scene state; rebuild through it
+        tsc = (threadedscene_t *)threadedscene_t::factory();
+        tsc->setCPUs(threads);
+        for (size_t i = 0; i < r.meshes.size(); i++) tsc->addObject(r.meshes[i]);
+        for (size_t i = 0; i < r.lights.size(); i++) tsc->addLight(r.lights[i]);
+        tsc->setCamera(r.camera);
+        tsc->setBias(s.rp.self_bias);
+        tsc->setMaxRayDepth(s.rp.raydepth);
+        tsc->tonemap(false);
+        tsc->clampRGB(false);
+        tsc->alphaPremultiply(false);
+        tsc->alphaMaskBackground(false);
+        tsc->setFog(0, color_t(0.0));
+        sc = tsc;
+    }
+    const uint32_t spp = s.rp.spp ? s.rp.spp : 1;
+    // every pixel resampled: AA_threshold 0 (renderblock.cc:22-66 uses >=)
+    sc->setAASamples(spp > 1 ? 1 : 0, spp > 1 ? (int)spp - 1 : 1, s.rp.aa_pixelwidth, 0.0, false);
+    if (crop) {
+        // screen-space region in [-1,1] (scene.cc:745-747), from pixel bounds
+        PFLOAT rx = (PFLOAT)s.cam.resx, ry = (PFLOAT)s.cam.resy;
+        sc->setRegion(2.0 * crop[0] / rx - 1.0, 2.0 * crop[1] / rx - 1.0, 1.0 - 2.0 * crop[3] / ry,
+                      1.0 - 2.0 * crop[2] / ry);
+    }
+    floatSink_t sink(s.cam.resx, s.cam.resy);
+    double t0 = now_s();
+    sc->render(sink);
+    double t1 = now_s();
+    FILE *f = fopen(out, "wb");
+    wr(f, &sink.img[0], 4 * sink.img.size());
+    fclose(f);
+    printf("{\"render_s\": %.6f, \"threads\": %d}\n", t1 - t0, threads);
+}
+
+// ------------------------------------------------------------------- noise
+static void cmd_noise(const char *pts_path, const char *out) {
+    FILE *fi = fopen(pts_path, "rb");
+    if (!fi) die("cannot open points");
+    uint32_t n;
+    rd(fi, &n, 4);
+    std::vector<float> pts(3 * n);
+    rd(fi, &pts[0], 12 * n);
+    fclose(fi);
+    newPerlin_t perlin;
+    fBm_t fbm6(1.0, 2.0, 6.0, &perlin);
+    fBm_t fbm25(0.8, 2.5, 3.5, &perlin);
+    FILE *f = fopen(out, "wb");
+    for (uint32_t i = 0; i < n; i++) {
+        point3d_t p(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+        float v[5] = {perlin(p), fbm6(p), fbm25(p), turbulence(&perlin, p, 2, 1.0, false),
+                      turbulence(&perlin, p, 3, 2.5, true)};
+        wr(f, v, 20);
+    }
+    fclose(f);
+}
+
+// ------------------------------------------------------------------ halton
+static void cmd_halton(const char *out) {
+    FILE *f = fopen(out, "wb");
+    int base = 2;
+    for (int b = 0; b < 12; b++) {
+        for (unsigned int i = 0; i < 4096; i++) {
+            Halton h(base);
+            h.setStart(i);
+            float v = h.getNext();
+            wr(f, &v, 4);
+        }
+        base = nextPrime(base);
+    }
+    // RI_vdC / RI_S / RI_LP
+    for (unsigned int i = 0; i < 4096; i++) {
+        float v[3] = {RI_vdC(i * 2654435761u), RI_S(i * 40503u), RI_LP(i * 7919u)};
+        wr(f, v, 12);
+    }
+    fclose(f);
+}
+
+int main(int argc, char **argv) {
+    if (argc < 3) die("usage: yr_ref_harness CMD ARGS...");
+    std::string cmd = argv[1];
+    std::cout.setstate(std::ios::failbit);  // silence the reference's progress output
+    if (cmd == "noise") {
+        if (argc < 4) die("noise POINTS OUT");
+        cmd_noise(argv[2], argv[3]);
+        return 0;
+    }
+    if (cmd == "halton") {
+        cmd_halton(argv[2]);
+        return 0;
+    }
+    SceneFile s;
+    load_scene(argv[2], s);
+    if (cmd == "tree") {
+        cmd_tree(s, argv[3]);
+    } else if (cmd == "rays") {
+        if (argc < 5) die("rays SCENE RAYS OUT");
+        cmd_rays(s, argv[3], argv[4]);
+    } else if (cmd == "camera") {
+        cmd_camera(s, argv[3]);
+    } else if (cmd == "render") {
+        if (argc < 5) die("render SCENE OUT THREADS [x0 x1 y0 y1]");
+        int crop[4];
+        bool has_crop = argc >= 9;
+        if (has_crop)
+            for (int k = 0; k < 4; k++) crop[k] = atoi(argv[5 + k]);
+        cmd_render(s, argv[3], atoi(argv[4]), has_crop ? crop : NULL);
+    } else {
+        die("unknown command");
+    }
+    return 0;
+}

@@ -1,0 +1,71 @@
+// Host-only entry points of the C ABI (no CUDA calls).
+#include <cstring>
+#include <new>
+
+#include "host_build.h"
+
+extern "C" {
+
+YR_API const char *yr_status_string(yr_status s) {
+    switch (s) {
+    case YR_OK: return "ok";
+    case YR_ERR_INVALID_ARG: return "invalid argument";
+    case YR_ERR_CUDA: return "CUDA runtime error";
+    case YR_ERR_OUT_OF_MEMORY: return "out of memory";
+    case YR_ERR_ITERATION_CAP: return "device loop hit its iteration cap";
+    case YR_ERR_STACK_OVERFLOW: return "traversal stack overflow";
+    case YR_ERR_BAD_TREE: return "corrupt tree (index out of range)";
+    case YR_ERR_CANCELLED: return "cancelled";
+    case YR_ERR_UNSUPPORTED: return "unsupported";
+    case YR_ERR_EMPTY_SCENE: return "empty scene";
+    case YR_ERR_NO_DEVICE: return "no CUDA device";
+    case YR_ERR_TOO_LARGE: return "size above the documented maximum";
+    }
+    return "unknown status";
+}
+
+YR_API const char *yr_version(void) { return "yafray_b200 0.1 (YafRay 0.0.9 hot path, sm_100a)"; }
+
+YR_API yr_status yr_kdtree_build(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris,
+                                 yr_kdtree **out) {
+    if (!out) return YR_ERR_INVALID_ARG;
+    *out = nullptr;
+    yr::KdTree t;
+    yr_status st;
+    try {
+        st = yr::build_kdtree(verts, nverts, tris, ntris, t);
+    } catch (const std::bad_alloc &) {
+        return YR_ERR_OUT_OF_MEMORY;
+    }
+    if (st != YR_OK) return st;
+    yr_kdtree *r = new (std::nothrow) yr_kdtree;
+    if (!r) return YR_ERR_OUT_OF_MEMORY;
+    std::memset(r, 0, sizeof(*r));
+    r->nnodes = (uint32_t)t.nodes.size();
+    r->nprims = (uint32_t)t.prims.size();
+    r->nodes = new (std::nothrow) yr_kd_node[r->nnodes ? r->nnodes : 1];
+    r->prims = new (std::nothrow) uint32_t[r->nprims ? r->nprims : 1];
+    if (!r->nodes || !r->prims) {
+        yr_kdtree_free(r);
+        return YR_ERR_OUT_OF_MEMORY;
+    }
+    if (r->nnodes) std::memcpy(r->nodes, t.nodes.data(), sizeof(yr_kd_node) * r->nnodes);
+    if (r->nprims) std::memcpy(r->prims, t.prims.data(), 4 * (size_t)r->nprims);
+    std::memcpy(r->bound, t.bound.a, 12);
+    std::memcpy(r->bound + 3, t.bound.g, 12);
+    r->max_depth = t.max_depth;
+    r->max_leaf_size = t.max_leaf_size;
+    r->cost_ratio = t.cost_ratio;
+    r->empty_bonus = t.empty_bonus;
+    *out = r;
+    return YR_OK;
+}
+
+YR_API void yr_kdtree_free(yr_kdtree *tree) {
+    if (!tree) return;
+    delete[] tree->nodes;
+    delete[] tree->prims;
+    delete tree;
+}
+
+}  // extern "C"

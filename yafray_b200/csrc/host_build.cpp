@@ -1,0 +1,705 @@
+// Host-side SAH kd-tree build and object tree, producing the device format.
+//
+// The kd-tree must come out node-for-node identical to YafRay's kdTree_t
+// (kdtree.cc:57-582, triclip.cc:50-240): leaf order decides which of two
+// equally distant triangles a ray reports (Intersect keeps the first one it
+// tests, kdtree.cc:684-714), and identical trees make the per-ray node and
+// triangle counts comparable with the reference traversal.  So the split
+// search, the classification order, the clipping arithmetic and the float /
+// double types of every intermediate follow the reference; the code
+// structure (vectors per node instead of the shared scratch arrays, an
+// explicit node list instead of a growing pointer array) is our own.
+//
+// The reference ships built with -O3 -ffast-math (linux-settings.py:21-26),
+// and g++ rewrites four expressions of the split search under that flag.
+// The tree of the shipped build is the one to match, so these four are
+// written here in the rewritten form (each place is marked "fast-math"):
+//   1/(dx*dy + dx*dz + dy*dz)       -> 1/((dy + dz)*dx + dy*dz)
+//   l / d[axis] in the binned search -> l * (1/d[axis])
+//   raw - (0.1 + l/d)*eb*raw         -> raw * (1 - (l/d + 0.1)*eb)
+//   lo - 0.021*h - 1e-5*s            -> lo - (0.021*h + 1e-5*s)   (and hi + ...)
+#include "host_build.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <list>
+
+namespace yr {
+namespace {
+
+constexpr int kBins = 1024;          // KD_BINS (kdtree.cc:17)
+constexpr uint32_t kClipThresh = 32;  // TRI_CLIP_THRESH (kdtree.cc:16)
+constexpr uint32_t kPigeonThresh = 128;
+
+// 3-way min / max with the reference's comparison order (kdtree.cc:19-20).
+inline float min3(float a, float b, float c) { return (a > b) ? ((b > c) ? c : b) : ((a > c) ? c : a); }
+inline float max3(float a, float b, float c) { return (a < b) ? ((b > c) ? b : c) : ((a > c) ? a : c); }
+
+struct Bin {
+    int n = 0, c_left = 0, c_right = 0, c_bleft = 0, c_both = 0;
+    float t = 0.f;
+    bool empty() const { return n == 0; }
+};
+
+enum EdgeEnd { kLower = 0, kBoth = 1, kUpper = 2 };  // kdtree.cc:10-12
+
+struct Edge {
+    float pos;
+    int prim;
+    int end;
+    bool operator<(const Edge &e) const {  // boundEdge::operator< (kdtree.h:71-75)
+        if (pos == e.pos) return end < e.end;
+        return pos < e.pos;
+    }
+};
+
+struct Split {
+    int axis = -1;
+    int offset = -1;
+    float best_cost = 0.f;
+    float old_cost = 0.f;
+    float t = 0.f;
+    uint32_t n_below = 0, n_above = 0;
+    int n_edge = 0;
+};
+
+// Sutherland-Hodgman clip of a triangle against an axis-aligned box, in
+// double (triClip.cc:50-240).  Returns 0 = clipped bound in `box`,
+// 1 = nothing left, 2 = polygon overflow (caller keeps the full bound).
+int clip_triangle(const double bmin[3], const double bmax[3], const double v[3][3], Box &box) {
+    double buf1[11][3], buf2[11][3];
+    double(*poly)[3] = buf1;
+    double(*cpoly)[3] = buf2;
+    for (int q = 0; q < 3; q++) {
+        poly[q][0] = v[q][0];
+        poly[q][1] = v[q][1];
+        poly[q][2] = v[q][2];
+        poly[3][q] = v[0][q];
+    }
+    int n = 3;
+    for (int axis = 0; axis < 3; axis++) {
+        const int na = (axis + 1) % 3, pa = (axis + 2) % 3;
+        for (int side = 0; side < 2; side++) {
+            // side 0 clips against the lower plane, side 1 against the upper one
+            const double plane = side == 0 ? bmin[axis] : bmax[axis];
+            auto inside = [&](double x) { return side == 0 ? (x >= plane) : (x <= plane); };
+            auto strictly_in = [&](double x) { return side == 0 ? (x > plane) : (x < plane); };
+            int nc = 0;
+            bool p1_in = inside(poly[0][axis]);
+            for (int i = 0; i < n; i++) {
+                const double *p1 = poly[i], *p2 = poly[i + 1];
+                if (p1_in) {
+                    if (inside(p2[axis])) {
+                        std::memcpy(cpoly[nc], p2, sizeof(double) * 3);
+                        nc++;
+                        p1_in = true;
+                    } else {
+                        double t = (plane - p1[axis]) / (p2[axis] - p1[axis]);
+                        cpoly[nc][axis] = plane;
+                        cpoly[nc][na] = p1[na] + t * (p2[na] - p1[na]);
+                        cpoly[nc][pa] = p1[pa] + t * (p2[pa] - p1[pa]);
+                        nc++;
+                        p1_in = false;
+                    }
+                } else {
+                    if (strictly_in(p2[axis])) {
+                        double t = (plane - p2[axis]) / (p1[axis] - p2[axis]);
+                        cpoly[nc][axis] = plane;
+                        cpoly[nc][na] = p2[na] + t * (p1[na] - p2[na]);
+                        cpoly[nc][pa] = p2[pa] + t * (p1[pa] - p2[pa]);
+                        nc++;
+                        std::memcpy(cpoly[nc], p2, sizeof(double) * 3);
+                        nc++;
+                        p1_in = true;
+                    } else if (p2[axis] == plane) {
+                        std::memcpy(cpoly[nc], p2, sizeof(double) * 3);
+                        nc++;
+                        p1_in = true;
+                    } else {
+                        p1_in = false;
+                    }
+                }
+            }
+            if (nc > 9) return 2;
+            std::memcpy(cpoly[nc], cpoly[0], sizeof(double) * 3);
+            n = nc;
+            std::swap(poly, cpoly);
+        }
+    }
+    if (n < 2) return 1;
+    double a[3], g[3];
+    for (int k = 0; k < 3; k++) a[k] = g[k] = poly[0][k];
+    for (int i = 1; i < n; i++)
+        for (int k = 0; k < 3; k++) {
+            a[k] = std::min(a[k], poly[i][k]);
+            g[k] = std::max(g[k], poly[i][k]);
+        }
+    for (int k = 0; k < 3; k++) {
+        box.a[k] = (float)a[k];
+        box.g[k] = (float)g[k];
+    }
+    return 0;
+}
+
+class Builder {
+  public:
+    Builder(const float *verts, const uint32_t *tris, uint32_t ntris, KdTree &out)
+        : verts_(verts), tris_(tris), n_(ntris), out_(out) {}
+
+    yr_status run() {
+        // kdTree_t ctor parameter defaults (kdtree.cc:57-80)
+        cost_ratio_ = 1.2f;
+        ebonus_ = 0.40f;
+        max_depth_ = int(6.0f + 1.66f * std::log(float(n_)));
+        const double log_leaves = 1.442695f * std::log(double(n_));
+        max_leaf_ = int(log_leaves - 16.0);
+        if (max_leaf_ <= 0) max_leaf_ = 1;
+        if (max_depth_ > 64) max_depth_ = 64;
+        if (log_leaves > 16.0) cost_ratio_ = (float)(cost_ratio_ + 0.25 * (log_leaves - 16.0));
+
+        bounds_.resize(n_);
+        for (uint32_t i = 0; i < n_; i++) {
+            const float *A = vtx(i, 0), *B = vtx(i, 1), *C = vtx(i, 2);
+            Box &b = bounds_[i];
+            for (int k = 0; k < 3; k++) {
+                b.a[k] = min3(A[k], B[k], C[k]);
+                b.g[k] = max3(A[k], B[k], C[k]);
+            }
+            if (i == 0) {
+                tree_ = b;
+            } else {
+                // bound_t(const bound_t&, const bound_t&) with MIN/MAX (bound.cc:32-52)
+                for (int k = 0; k < 3; k++) {
+                    tree_.a[k] = (tree_.a[k] < b.a[k]) ? tree_.a[k] : b.a[k];
+                    tree_.g[k] = (tree_.g[k] > b.g[k]) ? tree_.g[k] : b.g[k];
+                }
+            }
+        }
+        // grow by 1e-4 of the diagonal (kdtree.cc:83-89)
+        float dx = tree_.g[0] - tree_.a[0], dy = tree_.g[1] - tree_.a[1], dz = tree_.g[2] - tree_.a[2];
+        float diag = (float)(std::sqrt(dx * dx + dy * dy + dz * dz) * 0.0001);
+        for (int k = 0; k < 3; k++) {
+            tree_.a[k] -= diag;
+            tree_.g[k] += diag;
+        }
+        std::vector<uint32_t> all(n_);
+        for (uint32_t i = 0; i < n_; i++) all[i] = i;
+        out_.nodes.clear();
+        out_.prims.clear();
+        out_.nodes.reserve(2 * (size_t)n_ + 16);
+        Box root = tree_;
+        yr_status st = build(all, root, 0, 0);
+        out_.bound = tree_;
+        out_.max_depth = max_depth_;
+        out_.max_leaf_size = max_leaf_;
+        out_.cost_ratio = cost_ratio_;
+        out_.empty_bonus = ebonus_;
+        return st;
+    }
+
+  private:
+    const float *vtx(uint32_t tri, int k) const { return verts_ + 3 * (size_t)tris_[3 * (size_t)tri + k]; }
+
+    void make_leaf(const std::vector<uint32_t> &prims) {
+        yr_kd_node nd;
+        const uint32_t np = (uint32_t)prims.size();
+        nd.flags = (np << 2) | 3u;
+        if (np == 1) {
+            nd.word = prims[0];
+        } else if (np > 1) {
+            nd.word = (uint32_t)out_.prims.size();
+            out_.prims.insert(out_.prims.end(), prims.begin(), prims.end());
+        } else {
+            nd.word = 0;
+        }
+        out_.nodes.push_back(nd);
+    }
+
+    // Binned SAH for > 128 primitives (kdTree_t::pigeonMinCost, kdtree.cc:167-304).
+    yr_status pigeon(const std::vector<uint32_t> &prims, const Box &nb, float ebonus, Split &sp) {
+        const uint32_t np = (uint32_t)prims.size();
+        float d[3] = {nb.g[0] - nb.a[0], nb.g[1] - nb.a[1], nb.g[2] - nb.a[2]};
+        sp.old_cost = float(np);
+        sp.best_cost = std::numeric_limits<float>::infinity();
+        const float inv_sa = 1.0f / ((d[1] + d[2]) * d[0] + d[1] * d[2]);  // fast-math
+        std::vector<Bin> bin(kBins + 1);
+        for (int axis = 0; axis < 3; axis++) {
+            const float s = kBins / d[axis];
+            const float lo = nb.a[axis];
+            for (uint32_t i = 0; i < np; i++) {
+                const Box &bb = bounds_[prims[i]];
+                const float tl = bb.a[axis], tu = bb.g[axis];
+                int bl = (int)((tl - lo) * s), br = (int)((tu - lo) * s);
+                bl = bl < 0 ? 0 : (bl > kBins ? kBins : bl);
+                br = br < 0 ? 0 : (br > kBins ? kBins : br);
+                Bin &L = bin[bl];
+                if (tl == tu) {
+                    if (L.empty() || tl >= L.t) {
+                        L.t = tl;
+                        L.c_both++;
+                    } else {
+                        L.c_left++;
+                        L.c_right++;
+                    }
+                    L.n += 2;
+                } else {
+                    if (L.empty() || tl > L.t) {
+                        L.t = tl;
+                        L.c_left += L.c_both + L.c_bleft;
+                        L.c_right += L.c_both;
+                        L.c_both = L.c_bleft = 0;
+                        L.c_bleft++;
+                    } else if (tl == L.t) {
+                        L.c_bleft++;
+                    } else {
+                        L.c_left++;
+                    }
+                    L.n++;
+                    Bin &R = bin[br];
+                    R.c_right++;
+                    if (R.empty() || tu > R.t) {
+                        R.t = tu;
+                        R.c_left += R.c_both + R.c_bleft;
+                        R.c_right += R.c_both;
+                        R.c_both = R.c_bleft = 0;
+                    }
+                    R.n++;
+                }
+            }
+            const float cap_area = d[(axis + 1) % 3] * d[(axis + 2) % 3];
+            const float cap_perim = d[(axis + 1) % 3] + d[(axis + 2) % 3];
+            const float rd = 1.0f / d[axis];  // fast-math: reciprocal hoisted out of the loop
+            uint32_t below = 0, above = np;
+            for (int i = 0; i <= kBins; i++) {
+                const Bin &b = bin[i];
+                if (b.empty()) continue;
+                below += b.c_left;
+                above -= b.c_right;
+                const float et = b.t;
+                if (et > nb.a[axis] && et < nb.g[axis]) {
+                    const float l1 = et - nb.a[axis], l2 = nb.g[axis] - et;
+                    const float below_sa = cap_area + l1 * cap_perim;
+                    const float above_sa = cap_area + l2 * cap_perim;
+                    const float raw = below_sa * below + above_sa * above;
+                    // fast-math: raw - (0.1 + l*rd)*eb*raw folded to raw*(1 - (l*rd + 0.1)*eb)
+                    float net;
+                    if (above == 0) net = raw * (1.0f - (l2 * rd + 0.1f) * ebonus);
+                    else if (below == 0) net = raw * (1.0f - (l1 * rd + 0.1f) * ebonus);
+                    else net = raw;
+                    const float cost = cost_ratio_ + inv_sa * net;
+                    if (cost < sp.best_cost) {
+                        sp.t = et;
+                        sp.best_cost = cost;
+                        sp.axis = axis;
+                        sp.offset = i;
+                        sp.n_below = below;
+                        sp.n_above = above;
+                    }
+                }
+                below += b.c_both + b.c_bleft;
+                above -= b.c_both;
+            }
+            // the reference prints "SCREWED!!" and exits here (kdtree.cc:283-301)
+            if (below != np || above != 0) return YR_ERR_BAD_TREE;
+            std::fill(bin.begin(), bin.end(), Bin());
+        }
+        return YR_OK;
+    }
+
+    // Exact sorted-edge SAH (kdTree_t::minimalCost, kdtree.cc:311-406).
+    // `clipped` holds per-position bounds (after clipping), else bounds_[prim].
+    void exact(const std::vector<uint32_t> &prims, const Box &nb, const std::vector<Box> *clipped,
+               float ebonus, Split &sp) {
+        const uint32_t np = (uint32_t)prims.size();
+        float d[3] = {nb.g[0] - nb.a[0], nb.g[1] - nb.a[1], nb.g[2] - nb.a[2]};
+        sp.old_cost = float(np);
+        sp.best_cost = std::numeric_limits<float>::infinity();
+        const float inv_sa = 1.0f / ((d[1] + d[2]) * d[0] + d[1] * d[2]);  // fast-math
+        for (int axis = 0; axis < 3; axis++) {
+            std::vector<Edge> &ed = edges_[axis];
+            ed.clear();
+            for (uint32_t i = 0; i < np; i++) {
+                const int pn = (int)prims[i];
+                const Box &bb = clipped ? (*clipped)[i] : bounds_[pn];
+                if (bb.a[axis] == bb.g[axis]) {
+                    ed.push_back({bb.a[axis], pn, kBoth});
+                } else {
+                    ed.push_back({bb.a[axis], pn, kLower});
+                    ed.push_back({bb.g[axis], pn, kUpper});
+                }
+            }
+            std::sort(ed.begin(), ed.end());
+            const int ne = (int)ed.size();
+            const float cap_area = d[(axis + 1) % 3] * d[(axis + 2) % 3];
+            const float cap_perim = d[(axis + 1) % 3] + d[(axis + 2) % 3];
+            uint32_t below = 0, above = np;
+            for (int i = 0; i < ne; ++i) {
+                if (ed[i].end == kUpper) --above;
+                const float et = ed[i].pos;
+                if (et > nb.a[axis] && et < nb.g[axis]) {
+                    const float l1 = et - nb.a[axis], l2 = nb.g[axis] - et;
+                    const float below_sa = cap_area + l1 * cap_perim;
+                    const float above_sa = cap_area + l2 * cap_perim;
+                    const float raw = below_sa * below + above_sa * above;
+                    // fast-math: folded as in the binned search, division kept here
+                    float net;
+                    if (above == 0) net = raw * (1.0f - (l2 / d[axis] + 0.1f) * ebonus);
+                    else if (below == 0) net = raw * (1.0f - (l1 / d[axis] + 0.1f) * ebonus);
+                    else net = raw;
+                    const float cost = cost_ratio_ + inv_sa * net;
+                    if (cost < sp.best_cost) {
+                        sp.best_cost = cost;
+                        sp.axis = axis;
+                        sp.offset = i;
+                        sp.n_edge = ne;
+                        sp.n_below = below;
+                        sp.n_above = above;
+                    }
+                }
+                if (ed[i].end != kUpper) {
+                    ++below;
+                    if (ed[i].end == kBoth) --above;
+                }
+            }
+        }
+    }
+
+    // kdTree_t::buildTree (kdtree.cc:416-582)
+    yr_status build(std::vector<uint32_t> &prims, const Box &nb, int depth, int bad_refines) {
+        std::vector<Box> clipped;
+        if (prims.size() <= kClipThresh) {
+            double bmin[3], bmax[3];
+            for (int i = 0; i < 3; ++i) {
+                const double half = (double)nb.g[i] - (double)nb.a[i];
+                const double tsize = (double)tree_.g[i] - (double)tree_.a[i];
+                const double grow = 0.021 * half + 0.00001 * tsize;  // fast-math
+                bmin[i] = (double)nb.a[i] - grow;
+                bmax[i] = (double)nb.g[i] + grow;
+            }
+            std::vector<uint32_t> kept;
+            kept.reserve(prims.size());
+            clipped.reserve(prims.size());
+            for (uint32_t pn : prims) {
+                double v[3][3];
+                for (int j = 0; j < 3; ++j) {
+                    v[0][j] = vtx(pn, 0)[j];
+                    v[1][j] = vtx(pn, 1)[j];
+                    v[2][j] = vtx(pn, 2)[j];
+                }
+                Box cb;
+                int res = clip_triangle(bmin, bmax, v, cb);
+                if (res == 0) {
+                    kept.push_back(pn);
+                    clipped.push_back(cb);
+                } else if (res == 2) {
+                    kept.push_back(pn);
+                    clipped.push_back(bounds_[pn]);
+                }
+            }
+            prims.swap(kept);
+        }
+        const uint32_t np = (uint32_t)prims.size();
+        if (np <= (uint32_t)max_leaf_ || depth >= max_depth_) {
+            make_leaf(prims);
+            return YR_OK;
+        }
+        Split sp;
+        const float eb = (float)(ebonus_ * (1.1 - (double)((float)depth / (float)max_depth_)));
+        if (np > kPigeonThresh) {
+            yr_status st = pigeon(prims, nb, eb, sp);
+            if (st != YR_OK) return st;
+        } else if (np > kClipThresh) {
+            exact(prims, nb, nullptr, eb, sp);
+        } else {
+            exact(prims, nb, &clipped, eb, sp);
+        }
+        if (sp.best_cost > sp.old_cost) ++bad_refines;
+        if ((sp.best_cost > 1.6f * sp.old_cost && np < 16) || sp.axis == -1 || bad_refines == 2) {
+            make_leaf(prims);
+            return YR_OK;
+        }
+        std::vector<uint32_t> left, right;
+        left.reserve(np);
+        right.reserve(np);
+        float split_pos;
+        const int ax = sp.axis;
+        if (np > kPigeonThresh) {
+            for (uint32_t pn : prims) {
+                if (bounds_[pn].a[ax] >= sp.t) {
+                    right.push_back(pn);
+                } else {
+                    left.push_back(pn);
+                    if (bounds_[pn].g[ax] > sp.t) right.push_back(pn);
+                }
+            }
+            split_pos = sp.t;
+        } else {
+            const std::vector<Edge> &ed = edges_[ax];
+            split_pos = ed[sp.offset].pos;
+            for (int i = 0; i < sp.offset; ++i)
+                if (ed[i].end != kUpper) left.push_back((uint32_t)ed[i].prim);
+            if (ed[sp.offset].end == kBoth) right.push_back((uint32_t)ed[sp.offset].prim);
+            for (int i = sp.offset + 1; i < sp.n_edge; ++i)
+                if (ed[i].end != kLower) right.push_back((uint32_t)ed[i].prim);
+        }
+        prims.clear();
+        prims.shrink_to_fit();
+        clipped.clear();
+        clipped.shrink_to_fit();
+
+        const size_t cur = out_.nodes.size();
+        yr_kd_node nd;
+        std::memcpy(&nd.word, &split_pos, 4);
+        nd.flags = (uint32_t)ax;
+        out_.nodes.push_back(nd);
+        Box bl = nb, br = nb;
+        bl.g[ax] = split_pos;
+        br.a[ax] = split_pos;
+        yr_status st = build(left, bl, depth + 1, bad_refines);
+        if (st != YR_OK) return st;
+        const size_t right_index = out_.nodes.size();
+        if (right_index >= (1u << 30)) return YR_ERR_TOO_LARGE;
+        out_.nodes[cur].flags = (out_.nodes[cur].flags & 3u) | ((uint32_t)right_index << 2);
+        return build(right, br, depth + 1, bad_refines);
+    }
+
+    const float *verts_;
+    const uint32_t *tris_;
+    uint32_t n_;
+    KdTree &out_;
+    std::vector<Box> bounds_;
+    Box tree_{};
+    float cost_ratio_ = 0.f, ebonus_ = 0.f;
+    int max_depth_ = 0, max_leaf_ = 0;
+    std::vector<Edge> edges_[3];
+};
+
+// --- object tree -----------------------------------------------------------
+
+float box_vol(const Box &b) { return (b.g[1] - b.a[1]) * (b.g[0] - b.a[0]) * (b.g[2] - b.a[2]); }
+
+Box box_union(const Box &r, const Box &l) {
+    Box o;
+    for (int k = 0; k < 3; k++) {
+        o.a[k] = (r.a[k] < l.a[k]) ? r.a[k] : l.a[k];
+        o.g[k] = (r.g[k] > l.g[k]) ? r.g[k] : l.g[k];
+    }
+    return o;
+}
+
+// b_intersect + bound_distance (bound.cc:61-83)
+float box_overlap(const Box &r, const Box &l) {
+    float minx = (r.a[0] > l.a[0]) ? r.a[0] : l.a[0];
+    float miny = (r.a[1] > l.a[1]) ? r.a[1] : l.a[1];
+    float minz = (r.a[2] > l.a[2]) ? r.a[2] : l.a[2];
+    float maxx = (r.g[0] < l.g[0]) ? r.g[0] : l.g[0];
+    float maxy = (r.g[1] < l.g[1]) ? r.g[1] : l.g[1];
+    float maxz = (r.g[2] < l.g[2]) ? r.g[2] : l.g[2];
+    if (maxx <= minx) return 0;
+    if (maxy <= miny) return 0;
+    if (maxz <= minz) return 0;
+    return (maxx - minx) * (maxy - miny) * (maxz - minz);
+}
+
+float box_distance(const Box &l, const Box &r) {
+    Box nb = box_union(l, r);
+    float voids = box_vol(nb) - box_vol(l) - box_vol(r) + box_overlap(l, r);
+    if (voids < 0) voids = 0;
+    return (float)((double)(voids + box_vol(nb)) + std::fabs((double)(box_vol(l) - box_vol(r))));
+}
+
+// Greedy nearest-pair clustering with lazily recomputed nearest neighbours
+// (treeBuilder_t, yafutils.h:10-190).  The neighbour bookkeeping decides
+// which pair merges first when distances tie, so it is kept as is.
+class Clusterer {
+  public:
+    explicit Clusterer(std::vector<ObjNode> &nodes, std::vector<Box> &boxes) : nodes_(nodes), boxes_(boxes) {}
+
+    void push(int obj) {
+        items_.push_front(Item(obj));
+        items_.front().nearest = items_.end();
+        calculate(items_.begin());
+        if (items_.size() > 1 && (items_.front().dist < mindist_ || best_ == items_.end())) {
+            best_ = items_.begin();
+            mindist_ = items_.begin()->dist;
+        }
+    }
+
+    void build() {
+        while (items_.size() >= 2) step();
+    }
+
+    int solution() const { return items_.front().obj; }
+
+  private:
+    struct Item;
+    using It = std::list<Item>::iterator;
+    struct Item {
+        explicit Item(int o) : obj(o) {}
+        int obj;
+        It nearest;
+        float dist = 0.f;
+        std::list<It> recalculate;
+    };
+
+    float distance(int a, int b) const { return box_distance(boxes_[a], boxes_[b]); }
+
+    void calculate(It n) {
+        if (items_.size() == 1) return;
+        if (items_.size() == 2) {
+            It a = items_.begin();
+            It b = a;
+            ++b;
+            a->nearest = b;
+            a->recalculate.push_back(b);
+            b->nearest = a;
+            b->recalculate.push_back(a);
+            mindist_ = a->dist = b->dist = distance(a->obj, b->obj);
+            best_ = a;
+            return;
+        }
+        It before = n->nearest;
+        Item &nu = *n;
+        for (It i = items_.begin(); i != items_.end(); ++i) {
+            if (i == n) continue;
+            float d = distance(nu.obj, i->obj);
+            if (i->nearest == items_.end()) {
+                i->nearest = n;
+                i->dist = d;
+                nu.recalculate.push_back(i);
+            }
+            bool old_useless = (nu.nearest == items_.end()) || (nu.nearest->dist < nu.dist);
+            bool new_useful = (d < i->dist);
+            if ((nu.nearest == items_.end()) || ((d < nu.dist) && (new_useful || old_useless)) ||
+                (old_useless && new_useful)) {
+                nu.nearest = i;
+                nu.dist = d;
+            }
+        }
+        if (nu.dist < nu.nearest->dist) {
+            nu.nearest->nearest->recalculate.remove(nu.nearest);
+            nu.nearest->nearest = n;
+            nu.nearest->dist = nu.dist;
+            nu.recalculate.push_back(nu.nearest);
+        }
+        if (before != items_.end()) before->recalculate.remove(n);
+        nu.nearest->recalculate.push_back(n);
+    }
+
+    void pop() {
+        best_->nearest->nearest->recalculate.remove(best_->nearest);
+        std::list<It> update = best_->recalculate;
+        best_->nearest->recalculate.remove(best_);
+        update.insert(update.end(), best_->nearest->recalculate.begin(), best_->nearest->recalculate.end());
+        items_.erase(best_->nearest);
+        items_.erase(best_);
+        if (!items_.empty()) {
+            best_ = items_.end();
+            for (It i : update) i->nearest = items_.end();
+            for (It i : update) calculate(i);
+            for (It i = items_.begin(); i != items_.end(); ++i)
+                if ((i->dist < mindist_) || (best_ == items_.end())) {
+                    best_ = i;
+                    mindist_ = i->dist;
+                }
+        }
+    }
+
+    void step() {
+        const int a = best_->obj, b = best_->nearest->obj;
+        // join (oTreeJoin_f, object3d.cc:22-28): left = a, right = b
+        ObjNode nd;
+        const Box u = box_union(boxes_[a], boxes_[b]);
+        for (int k = 0; k < 3; k++) {
+            nd.bmin[k] = u.a[k];
+            nd.bmax[k] = u.g[k];
+        }
+        nd.left = a;
+        nd.right = b;
+        nodes_.push_back(nd);
+        boxes_.push_back(u);
+        pop();
+        push((int)nodes_.size() - 1);
+    }
+
+    std::vector<ObjNode> &nodes_;
+    std::vector<Box> &boxes_;
+    std::list<Item> items_;
+    It best_ = items_.end();
+    float mindist_ = 0.f;
+};
+
+}  // namespace
+
+yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris, KdTree &out) {
+    if (!verts || !tris || ntris == 0) return YR_ERR_EMPTY_SCENE;
+    for (size_t i = 0; i < 3 * (size_t)ntris; i++)
+        if (tris[i] >= nverts) return YR_ERR_INVALID_ARG;
+    Builder b(verts, tris, ntris, out);
+    return b.run();
+}
+
+Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris) {
+    Box b;
+    const float *p0 = verts + 3 * (size_t)tris[0];
+    for (int k = 0; k < 3; k++) b.a[k] = b.g[k] = p0[k];
+    for (size_t t = 0; t < ntris; t++)
+        for (int v = 0; v < 3; v++) {
+            const float *p = verts + 3 * (size_t)tris[3 * t + v];
+            for (int k = 0; k < 3; k++) {
+                if (p[k] > b.g[k]) b.g[k] = p[k];
+                if (p[k] < b.a[k]) b.a[k] = p[k];
+            }
+        }
+    return b;
+}
+
+void build_object_tree(const std::vector<Box> &object_bounds, std::vector<ObjNode> &out) {
+    // Work list: leaves first (one per object, obj_list order), then joins.
+    std::vector<ObjNode> nodes;
+    std::vector<Box> boxes;
+    for (size_t i = 0; i < object_bounds.size(); i++) {
+        ObjNode nd;
+        for (int k = 0; k < 3; k++) {
+            nd.bmin[k] = object_bounds[i].a[k];
+            nd.bmax[k] = object_bounds[i].g[k];
+        }
+        nd.left = -1;
+        nd.right = (int32_t)i;
+        nodes.push_back(nd);
+        boxes.push_back(object_bounds[i]);
+    }
+    out.clear();
+    if (nodes.empty()) return;
+    Clusterer c(nodes, boxes);
+    for (size_t i = 0; i < object_bounds.size(); i++) c.push((int)i);
+    c.build();
+    const int root = c.solution();
+    // re-index depth first from the root so that node 0 is the root
+    std::vector<int> stack{root};
+    std::vector<int> order;
+    std::vector<int> newidx(nodes.size(), -1);
+    while (!stack.empty()) {
+        int n = stack.back();
+        stack.pop_back();
+        newidx[n] = (int)order.size();
+        order.push_back(n);
+        if (nodes[n].left >= 0) {
+            stack.push_back(nodes[n].right);
+            stack.push_back(nodes[n].left);
+        }
+    }
+    out.resize(order.size());
+    for (size_t i = 0; i < order.size(); i++) {
+        ObjNode nd = nodes[order[i]];
+        if (nd.left >= 0) {
+            nd.left = newidx[nd.left];
+            nd.right = newidx[nd.right];
+        }
+        out[i] = nd;
+    }
+}
+
+}  // namespace yr

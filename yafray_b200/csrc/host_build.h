@@ -1,0 +1,48 @@
+// Host-side scene preparation: SAH kd-tree per mesh and the object tree.
+// Internal header (not part of the C ABI).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "../../include/yr.h"
+
+namespace yr {
+
+struct Box {
+    float a[3];  // min corner (bound_t::a)
+    float g[3];  // max corner (bound_t::g)
+};
+
+// One mesh's kd-tree in the device format (see yr_kd_node in yr.h).
+struct KdTree {
+    std::vector<yr_kd_node> nodes;
+    std::vector<uint32_t> prims;
+    Box bound;
+    int max_depth = 0;
+    int max_leaf_size = 0;
+    float cost_ratio = 0.f;
+    float empty_bonus = 0.f;
+};
+
+// Build with meshObject_t's parameters (mesh.cc:162: depth -1, leaf -1,
+// cost 1.2, empty bonus 0.40).  Returns YR_OK or an error status.
+yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris,
+                       uint32_t ntris, KdTree &out);
+
+// meshObject_t::recalcBound (mesh.cc:343-374): bound of the triangles' vertices.
+Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris);
+
+// Flattened object tree node (geomeTree_t, geometree.h:8-32).
+struct ObjNode {
+    float bmin[3];
+    int32_t left;    // child index, -1 for a leaf
+    float bmax[3];
+    int32_t right;   // child index for interior, object index for a leaf
+};
+
+// buildObjectTree (object3d.cc:30-53): greedy agglomerative clustering with
+// the bound_distance metric (bound.cc:75-83), in the order of obj_list.
+// Node 0 is the root.
+void build_object_tree(const std::vector<Box> &object_bounds, std::vector<ObjNode> &out);
+
+}  // namespace yr

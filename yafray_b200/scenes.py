@@ -1,0 +1,422 @@
+"""Seeded synthetic scenes with the shapes of the benchmark configurations.
+
+A scene is what a YafRay host would hand to the C ABI: meshes (object list),
+genericShader_t parameters, light plugin parameters, the camera and render
+settings.  ``write_yrs`` stores it in the "YRS1" layout of include/yr.h.
+
+Configurations (sizes as in the benchmark definitions):
+  * ``config_small``   UV sphere (64 rings x 128 segments) on a 2-triangle
+                       ground plane, point light, 320x240, 1 spp, no GI.
+  * ``config_large``   16x16 jittered grid of those spheres on a 40x40 plane,
+                       4 area lights (16 samples), 1920x1080, 16 spp, path GI
+                       with 2 bounces.
+  * ``config_batch``   256 independent scenes (spheres + tori), uneven sizes.
+  * ``config_diff``    the small scene at 512x512 / 64 spp with 64 material
+                       groups and 8 area lights (264 parameters).
+  * ``config_diffnoise`` 32 inverse problems with fBm-modulated albedo.
+
+UV sphere construction (pinned, the benchmark text leaves it open): 64
+latitude bands and 128 segments; the two polar bands are triangle fans, the
+62 inner bands are quads split in two, which gives 128 + 128 + 62*256 =
+16,128 non-degenerate triangles and 63*128 + 2 = 8,066 vertices.
+"""
+from __future__ import annotations
+
+import math
+import struct
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import abi
+
+
+# --------------------------------------------------------------------- meshes
+def uv_sphere(center=(0.0, 0.0, 0.0), radius=1.0, rings=64, segments=128):
+    """Vertices (float32 [V,3]) and triangles (uint32 [T,3]) of a UV sphere."""
+    cx, cy, cz = center
+    verts = [(cx, cy + radius, cz)]
+    for k in range(1, rings):
+        th = math.pi * k / rings
+        y, rr = math.cos(th), math.sin(th)
+        for s in range(segments):
+            ph = 2.0 * math.pi * s / segments
+            verts.append((cx + radius * rr * math.cos(ph), cy + radius * y, cz + radius * rr * math.sin(ph)))
+    verts.append((cx, cy - radius, cz))
+    south = len(verts) - 1
+
+    def ring(k, s):  # k in 1..rings-1
+        return 1 + (k - 1) * segments + (s % segments)
+
+    tris = []
+    for s in range(segments):  # north fan, outward winding
+        tris.append((0, ring(1, s + 1), ring(1, s)))
+    for k in range(1, rings - 1):
+        for s in range(segments):
+            a, b = ring(k, s), ring(k, s + 1)
+            c, d = ring(k + 1, s), ring(k + 1, s + 1)
+            tris.append((a, b, d))
+            tris.append((a, d, c))
+    for s in range(segments):
+        tris.append((south, ring(rings - 1, s), ring(rings - 1, s + 1)))
+    return np.asarray(verts, dtype=np.float32), np.asarray(tris, dtype=np.uint32)
+
+
+def torus(center, R, r, nu=64, nv=32):
+    cx, cy, cz = center
+    verts = []
+    for i in range(nu):
+        u = 2 * math.pi * i / nu
+        for j in range(nv):
+            v = 2 * math.pi * j / nv
+            x = (R + r * math.cos(v)) * math.cos(u)
+            z = (R + r * math.cos(v)) * math.sin(u)
+            y = r * math.sin(v)
+            verts.append((cx + x, cy + y, cz + z))
+    tris = []
+    for i in range(nu):
+        for j in range(nv):
+            a = i * nv + j
+            b = ((i + 1) % nu) * nv + j
+            c = i * nv + (j + 1) % nv
+            d = ((i + 1) % nu) * nv + (j + 1) % nv
+            tris.append((a, c, d))
+            tris.append((a, d, b))
+    return np.asarray(verts, dtype=np.float32), np.asarray(tris, dtype=np.uint32)
+
+
+def ground_plane(half=20.0, y=-1.0):
+    v = np.array([(-half, y, -half), (half, y, -half), (half, y, half), (-half, y, half)], dtype=np.float32)
+    t = np.array([(0, 2, 1), (0, 3, 2)], dtype=np.uint32)
+    return v, t
+
+
+# ---------------------------------------------------------------------- scene
+@dataclass
+class Mesh:
+    verts: np.ndarray
+    tris: np.ndarray
+    shader: int = 0
+    tri_shaders: Optional[np.ndarray] = None
+    cast_shadows: bool = True
+
+
+@dataclass
+class Scene:
+    meshes: List[Mesh] = field(default_factory=list)
+    shaders: List[abi.YrShaderDesc] = field(default_factory=list)
+    lights: List[abi.YrLightDesc] = field(default_factory=list)
+    camera: abi.YrCameraDesc = field(default_factory=abi.YrCameraDesc)
+    render: abi.YrRenderParams = field(default_factory=abi.YrRenderParams)
+    name: str = ""
+
+    @property
+    def ntris(self) -> int:
+        return int(sum(m.tris.shape[0] for m in self.meshes))
+
+    @property
+    def resx(self) -> int:
+        return int(self.camera.resx)
+
+    @property
+    def resy(self) -> int:
+        return int(self.camera.resy)
+
+
+def shader(color, specular=(0.0, 0.0, 0.0), hard=1.0) -> abi.YrShaderDesc:
+    s = abi.YrShaderDesc()
+    s.color[:] = [float(c) for c in color]
+    s.specular[:] = [float(c) for c in specular]
+    s.hard = float(hard)
+    s.tex_type = abi.YR_TEX_NONE
+    s.mod_size[:] = [1.0, 1.0, 1.0]
+    return s
+
+
+def fbm_shader(color, color1, color2, intensity, size, octaves=6.0, lacunarity=2.0, H=1.0,
+               mod_color=1.0) -> abi.YrShaderDesc:
+    """genericShader_t whose albedo is mixed with a musgrave fBm texture."""
+    s = shader(color)
+    s.tex_type = abi.YR_TEX_MUSGRAVE_FBM
+    s.tex_color1[:] = [float(c) for c in color1]
+    s.tex_color2[:] = [float(c) for c in color2]
+    s.tex_H = float(H)
+    s.tex_lacunarity = float(lacunarity)
+    s.tex_octaves = float(octaves)
+    s.tex_size = float(size)
+    s.tex_intensity = float(intensity)
+    s.mod_color = float(mod_color)
+    s.tex_noise = 0
+    return s
+
+
+def point_light(pos, power=1.0, color=(1.0, 1.0, 1.0), cast_shadows=True) -> abi.YrLightDesc:
+    l = abi.YrLightDesc()
+    l.type = abi.YR_LIGHT_POINT
+    l.color[:] = [float(c) for c in color]
+    l.power = float(power)
+    l.p[0][:] = [float(c) for c in pos]
+    l.cast_shadows = 1 if cast_shadows else 0
+    return l
+
+
+def area_light(a, b, c, d, power=1.0, samples=16, color=(1.0, 1.0, 1.0)) -> abi.YrLightDesc:
+    l = abi.YrLightDesc()
+    l.type = abi.YR_LIGHT_AREA
+    l.color[:] = [float(x) for x in color]
+    l.power = float(power)
+    for i, p in enumerate((a, b, c, d)):
+        l.p[i][:] = [float(x) for x in p]
+    l.samples = int(samples)
+    l.cast_shadows = 1
+    return l
+
+
+def quad_light_down(cx, y, cz, w, h, power, samples=16, color=(1.0, 1.0, 1.0)) -> abi.YrLightDesc:
+    """Horizontal quad at height y facing down ((b-a)x(d-a) points to -y)."""
+    a = (cx - w / 2, y, cz - h / 2)
+    b = (cx + w / 2, y, cz - h / 2)
+    c = (cx + w / 2, y, cz + h / 2)
+    d = (cx - w / 2, y, cz + h / 2)
+    return area_light(a, b, c, d, power, samples, color)
+
+
+def hemi_light(samples=16, power=1.0, color=(1.0, 1.0, 1.0), maxdist=-1.0) -> abi.YrLightDesc:
+    l = abi.YrLightDesc()
+    l.type = abi.YR_LIGHT_HEMI
+    l.color[:] = [float(x) for x in color]
+    l.power = float(power)
+    l.samples = int(samples)
+    l.maxdist = float(maxdist)
+    return l
+
+
+def path_light(samples=1, depth=2, power=1.0) -> abi.YrLightDesc:
+    l = abi.YrLightDesc()
+    l.type = abi.YR_LIGHT_PATH
+    l.color[:] = [1.0, 1.0, 1.0]
+    l.power = float(power)
+    l.samples = int(samples)
+    l.depth = int(depth)
+    return l
+
+
+def camera(pos, look, up, resx, resy, fov_deg=45.0, aspect=1.0) -> abi.YrCameraDesc:
+    """Pinhole camera; focal = 0.5 / tan(fov/2) because camera_t puts a
+    width-1 image plane at distance `focal` (camera.cc:53-60)."""
+    c = abi.YrCameraDesc()
+    c.pos[:] = [float(x) for x in pos]
+    c.look[:] = [float(x) for x in look]
+    c.up[:] = [float(x) for x in up]
+    c.resx, c.resy = int(resx), int(resy)
+    c.aspect = float(aspect)
+    c.focal = float(0.5 / math.tan(math.radians(fov_deg) / 2.0))
+    return c
+
+
+def render_params(spp=1, seed=0, bias=0.1, raydepth=3, pixelwidth=1.0, background=(0.0, 0.0, 0.0)):
+    r = abi.YrRenderParams()
+    r.self_bias = float(bias)
+    r.raydepth = int(raydepth)
+    r.spp = int(spp)
+    r.aa_pixelwidth = float(pixelwidth)
+    r.seed = int(seed) & 0xFFFFFFFF
+    r.background[:] = [float(x) for x in background]
+    r.flags = 0
+    return r
+
+
+# -------------------------------------------------------------- configurations
+def config_small(resx=320, resy=240) -> Scene:
+    """UV sphere r=1 at the origin on a 2-triangle plane at y=-1; point light
+    (3,5,2) power 1; albedo 0.8; camera at (0,1,5) looking at the origin."""
+    sv, st = uv_sphere()
+    pv, pt = ground_plane(half=20.0, y=-1.0)
+    sc = Scene(name=f"small_{resx}x{resy}")
+    sc.shaders = [shader((0.8, 0.8, 0.8))]
+    sc.meshes = [Mesh(sv, st, 0), Mesh(pv, pt, 0)]
+    sc.lights = [point_light((3.0, 5.0, 2.0), 1.0)]
+    sc.camera = camera((0, 1, 5), (0, 0, 0), (0, 2, 5), resx, resy)
+    sc.render = render_params(spp=1)
+    return sc
+
+
+def config_large(seed=1, resx=1920, resy=1080, spp=16, grid=16) -> Scene:
+    """grid x grid jittered spheres (radius U(0.3,0.5), centre jitter
+    U(-0.2,0.2)) on a 40x40 plane, four area lights (power U(1,5), 16
+    samples), path GI with 2 bounces, albedos U(0.2,0.9)."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(name=f"large_g{grid}_{resx}x{resy}_spp{spp}")
+    spacing = 2.0
+    off = (grid - 1) / 2.0
+    sc.shaders.append(shader(tuple(rng.uniform(0.2, 0.9, 3))))
+    pv, pt = ground_plane(half=20.0, y=-1.0)
+    sc.meshes.append(Mesh(pv, pt, 0))
+    for i in range(grid):
+        for k in range(grid):
+            r = float(rng.uniform(0.3, 0.5))
+            jx, jz = rng.uniform(-0.2, 0.2, 2)
+            c = ((i - off) * spacing + jx, -1.0 + r, (k - off) * spacing + jz)
+            v, t = uv_sphere(c, r)
+            sc.shaders.append(shader(tuple(rng.uniform(0.2, 0.9, 3))))
+            sc.meshes.append(Mesh(v, t, len(sc.shaders) - 1))
+    for lx, lz in ((-8.0, -8.0), (8.0, -8.0), (-8.0, 8.0), (8.0, 8.0)):
+        sc.lights.append(quad_light_down(lx, 12.0, lz, 4.0, 4.0, float(rng.uniform(1.0, 5.0)) * 30.0, 16))
+    sc.lights.append(path_light(samples=1, depth=2, power=1.0))
+    sc.camera = camera((0.0, 14.0, 26.0), (0.0, -1.0, 0.0), (0.0, 15.0, 26.0), resx, resy)
+    sc.render = render_params(spp=spp, seed=seed)
+    return sc
+
+
+def _random_object(rng, tri_budget):
+    """A sphere or a torus with roughly tri_budget triangles."""
+    if rng.random() < 0.6:
+        seg = max(8, int(math.sqrt(tri_budget)))
+        rings = max(4, seg // 2)
+        seg = max(8, tri_budget // (2 * rings))
+        return "sphere", rings, seg
+    nu = max(8, int(math.sqrt(tri_budget)))
+    nv = max(4, tri_budget // (2 * nu))
+    return "torus", nu, nv
+
+
+def config_batch_scene(rng, idx, tri_lo=1_000, tri_hi=200_000) -> Scene:
+    ntri = int(math.exp(rng.uniform(math.log(tri_lo), math.log(tri_hi))))
+    nobj = int(rng.integers(1, 33))
+    size = int(rng.choice([64, 128, 256, 512]))
+    spp = int(rng.integers(4, 65))
+    bounces = int(rng.integers(1, 4))
+    sc = Scene(name=f"batch{idx}_t{ntri}_o{nobj}_{size}_spp{spp}_b{bounces}")
+    pv, pt = ground_plane(half=20.0, y=-1.0)
+    sc.shaders.append(shader(tuple(rng.uniform(0.2, 0.9, 3))))
+    sc.meshes.append(Mesh(pv, pt, 0))
+    per = max(64, ntri // nobj)
+    for o in range(nobj):
+        kind, a, b = _random_object(rng, per)
+        c = (float(rng.uniform(-4, 4)), float(rng.uniform(-0.5, 1.5)), float(rng.uniform(-4, 4)))
+        if kind == "sphere":
+            v, t = uv_sphere(c, float(rng.uniform(0.3, 1.0)), rings=a, segments=b)
+        else:
+            v, t = torus(c, float(rng.uniform(0.5, 1.0)), float(rng.uniform(0.1, 0.3)), nu=a, nv=b)
+        sc.shaders.append(shader(tuple(rng.uniform(0.2, 0.9, 3))))
+        sc.meshes.append(Mesh(v, t, len(sc.shaders) - 1))
+    for _ in range(int(rng.integers(1, 5))):
+        if rng.random() < 0.5:
+            sc.lights.append(point_light((rng.uniform(-6, 6), rng.uniform(6, 10), rng.uniform(-6, 6)),
+                                         float(rng.uniform(20, 60))))
+        else:
+            sc.lights.append(quad_light_down(float(rng.uniform(-5, 5)), float(rng.uniform(7, 10)),
+                                             float(rng.uniform(-5, 5)), 2.0, 2.0, float(rng.uniform(20, 60)),
+                                             int(rng.choice([4, 9, 16]))))
+    sc.lights.append(path_light(samples=1, depth=bounces, power=1.0))
+    sc.camera = camera((0.0, 5.0, 12.0), (0.0, 0.0, 0.0), (0.0, 6.0, 12.0), size, size)
+    sc.render = render_params(spp=spp, seed=idx + 1)
+    return sc
+
+
+def config_batch(seed=3, count=256, **kw) -> List[Scene]:
+    rng = np.random.default_rng(seed)
+    return [config_batch_scene(rng, i, **kw) for i in range(count)]
+
+
+def config_diff(seed=4, res=512, spp=64, groups=64, nlights=8, hidden=False) -> Scene:
+    """The small scene at res^2 with `groups` material groups on the sphere
+    (triangles assigned round-robin by latitude band), diffuse U(0.2,0.9),
+    specular weight U(0,0.5), and `nlights` area lights power U(1,5)."""
+    rng = np.random.default_rng(seed + (1000 if hidden else 0))
+    sv, st = uv_sphere()
+    pv, pt = ground_plane(half=20.0, y=-1.0)
+    sc = Scene(name=f"diff_{res}_spp{spp}")
+    for g in range(groups):
+        spec = float(rng.uniform(0.0, 0.5))
+        sc.shaders.append(shader(tuple(rng.uniform(0.2, 0.9, 3)), (spec, spec, spec), hard=20.0))
+    band = np.arange(st.shape[0]) // 256
+    tri_sh = (band % groups).astype(np.uint32)
+    sc.meshes = [Mesh(sv, st, abi.YR_PER_TRIANGLE, tri_sh), Mesh(pv, pt, 0)]
+    for i in range(nlights):
+        ang = 2 * math.pi * i / nlights
+        sc.lights.append(quad_light_down(4.0 * math.cos(ang), 6.0, 4.0 * math.sin(ang), 1.5, 1.5,
+                                         float(rng.uniform(1.0, 5.0)) * 10.0, 4))
+    sc.camera = camera((0, 1, 5), (0, 0, 0), (0, 2, 5), res, res)
+    sc.render = render_params(spp=spp, seed=seed)
+    return sc
+
+
+def config_diffnoise_scene(rng, idx, res=256, spp=32, tri_lo=20_000, tri_hi=500_000) -> Scene:
+    ntri = int(math.exp(rng.uniform(math.log(tri_lo), math.log(tri_hi))))
+    seg = max(16, int(math.sqrt(ntri)))
+    rings = max(8, ntri // (2 * seg))
+    sv, st = uv_sphere((0.0, 0.0, 0.0), 1.0, rings=rings, segments=seg)
+    pv, pt = ground_plane(half=20.0, y=-1.0)
+    sc = Scene(name=f"diffnoise{idx}_t{st.shape[0]}")
+    sc.shaders.append(fbm_shader(tuple(rng.uniform(0.2, 0.9, 3)), tuple(rng.uniform(0.2, 0.9, 3)),
+                                 (1.0, 1.0, 1.0), float(rng.uniform(0.3, 1.0)), float(rng.uniform(1, 8))))
+    sc.shaders.append(shader((0.8, 0.8, 0.8)))
+    sc.meshes = [Mesh(sv, st, 0), Mesh(pv, pt, 1)]
+    sc.lights = [quad_light_down(2.0, 6.0, 2.0, 2.0, 2.0, 40.0, 4)]
+    sc.camera = camera((0, 1, 5), (0, 0, 0), (0, 2, 5), res, res)
+    sc.render = render_params(spp=spp, seed=idx + 7)
+    return sc
+
+
+def config_diffnoise(seed=5, count=32, **kw) -> List[Scene]:
+    rng = np.random.default_rng(seed)
+    return [config_diffnoise_scene(rng, i, **kw) for i in range(count)]
+
+
+# ------------------------------------------------------------------ YRS1 file
+def write_yrs(sc: Scene, path: str) -> None:
+    with open(path, "wb") as f:
+        f.write(b"YRS1")
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 0))
+        f.write(bytes(sc.camera))
+        f.write(bytes(sc.render))
+        for s in sc.shaders:
+            f.write(bytes(s))
+        for l in sc.lights:
+            f.write(bytes(l))
+        for m in sc.meshes:
+            v = np.ascontiguousarray(m.verts, dtype=np.float32)
+            t = np.ascontiguousarray(m.tris, dtype=np.uint32)
+            f.write(struct.pack("<4I", v.shape[0], t.shape[0], m.shader & 0xFFFFFFFF, 1 if m.cast_shadows else 0))
+            f.write(v.tobytes())
+            f.write(t.tobytes())
+            if m.shader == abi.YR_PER_TRIANGLE:
+                f.write(np.ascontiguousarray(m.tri_shaders, dtype=np.uint32).tobytes())
+
+
+def read_yrs(path: str) -> Scene:
+    data = open(path, "rb").read()
+    assert data[:4] == b"YRS1", "bad magic"
+    nobj, nsh, nl, _ = struct.unpack_from("<4I", data, 4)
+    off = 20
+    sc = Scene()
+    sc.camera = abi.YrCameraDesc.from_buffer_copy(data, off)
+    off += C_sizeof(abi.YrCameraDesc)
+    sc.render = abi.YrRenderParams.from_buffer_copy(data, off)
+    off += C_sizeof(abi.YrRenderParams)
+    for _ in range(nsh):
+        sc.shaders.append(abi.YrShaderDesc.from_buffer_copy(data, off))
+        off += C_sizeof(abi.YrShaderDesc)
+    for _ in range(nl):
+        sc.lights.append(abi.YrLightDesc.from_buffer_copy(data, off))
+        off += C_sizeof(abi.YrLightDesc)
+    for _ in range(nobj):
+        nv, nt, shid, cast = struct.unpack_from("<4I", data, off)
+        off += 16
+        v = np.frombuffer(data, np.float32, 3 * nv, off).reshape(nv, 3).copy()
+        off += 12 * nv
+        t = np.frombuffer(data, np.uint32, 3 * nt, off).reshape(nt, 3).copy()
+        off += 12 * nt
+        ts = None
+        if shid == abi.YR_PER_TRIANGLE:
+            ts = np.frombuffer(data, np.uint32, nt, off).copy()
+            off += 4 * nt
+        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast)))
+    return sc
+
+
+def C_sizeof(t) -> int:
+    import ctypes
+    return ctypes.sizeof(t)
