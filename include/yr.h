@@ -91,6 +91,21 @@ YR_API yr_status yr_kdtree_build(const float *verts, uint32_t nverts,
                                  yr_kdtree **out);
 YR_API void yr_kdtree_free(yr_kdtree *tree);
 
+/* Object tree node (geomeTree_t, geometree.h:8-32): left < 0 marks a leaf
+ * whose `right` is the object index; node 0 is the root, children follow
+ * in depth-first order (left subtree first). */
+typedef struct yr_object_node {
+    float bmin[3];
+    int32_t left;
+    float bmax[3];
+    int32_t right;
+} yr_object_node;
+
+/* buildObjectTree (object3d.cc:30-53): greedy nearest-pair clustering of
+ * the objects' bounds (6 floats each: min xyz, max xyz) with the
+ * bound_distance metric, in object-list order.  `out` must hold 2n-1 nodes. */
+YR_API yr_status yr_object_tree_build(const float *bounds, uint32_t n, yr_object_node *out, uint32_t *nout);
+
 /* ------------------------------------------------------------------------
  * Scene description.  The records below are also the on-disk layout of the
  * "YRS1" scene files the tests and the benchmark exchange (little endian).

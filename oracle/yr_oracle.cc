@@ -1,0 +1,1035 @@
+// CPU ORACLE for the YafRay 0.0.9 ray-casting hot path - TEST INFRASTRUCTURE.
+//
+// A plain, single-threaded C++ restatement of the reference routines on the
+// path, used only by tests/, __graft_entry__.smoke() and bench.py's
+// cpu_baseline leg to check the CUDA library.  The product never links it.
+// It is pinned against the unmodified reference (oracle/_ref/yr_ref_harness,
+// built from the reference sources by oracle/Makefile) through the golden
+// vectors in tests/golden/.
+//
+// Arithmetic follows the reference's shipped build (-O3 -ffast-math): where
+// g++ evaluates an expression in a rewritten form that changes the rounding
+// (the slab test, Halton::getNext), the rewritten form is used ("fast-math").
+// Everything else is evaluated in source order, IEEE single precision, no
+// FMA contraction (built with -ffp-contract=off).
+//
+// Inputs are a YRS1 scene file (include/yr.h layout) plus the flattened
+// kd-trees and object tree (yr_kdtree layout), so the traversal can be run
+// on the reference's own trees.
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <limits>
+#include <vector>
+
+#include "../include/yr.h"
+
+namespace {
+
+const float kMinRay = 0.00005f;  // MIN_RAYDIST (configio.py:8-11)
+const float kInf = std::numeric_limits<float>::infinity();
+
+struct V {
+    float x, y, z;
+    V() : x(0), y(0), z(0) {}
+    V(float a, float b, float c) : x(a), y(b), z(c) {}
+    float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+    float &operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
+};
+V operator+(const V &a, const V &b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+V operator-(const V &a, const V &b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+V operator-(const V &a) { return V(-a.x, -a.y, -a.z); }
+V operator*(const V &a, float f) { return V(f * a.x, f * a.y, f * a.z); }  // vector3d.h:121-129
+V operator*(float f, const V &a) { return V(f * a.x, f * a.y, f * a.z); }
+V operator/(const V &a, float f) { return V(a.x / f, a.y / f, a.z / f); }
+float operator*(const V &a, const V &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }  // dot (vector3d.h:116)
+V operator^(const V &a, const V &b) {                                                // cross (vector3d.h:156)
+    return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+float length(const V &a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+V normalize(V a) {  // vector3d.h:207-217, 1/sqrt in double
+    float l = a.x * a.x + a.y * a.y + a.z * a.z;
+    if (l != 0) {
+        float k = (float)(1.0 / sqrt((double)l));
+        a.x *= k;
+        a.y *= k;
+        a.z *= k;
+    }
+    return a;
+}
+float normLenSqr(V &a) {  // vector3d.h:60-68
+    float l = a.x * a.x + a.y * a.y + a.z * a.z;
+    if (l != 0) {
+        float k = (float)(1.0 / sqrt((double)l));
+        a.x *= k;
+        a.y *= k;
+        a.z *= k;
+    }
+    return l;
+}
+
+struct C {
+    float r, g, b;
+    C() : r(0), g(0), b(0) {}
+    C(float a, float b_, float c) : r(a), g(b_), b(c) {}
+};
+C operator+(const C &a, const C &b) { return C(a.r + b.r, a.g + b.g, a.b + b.b); }
+C operator-(const C &a, const C &b) { return C(a.r - b.r, a.g - b.g, a.b - b.b); }
+C operator*(const C &a, const C &b) { return C(a.r * b.r, a.g * b.g, a.b * b.b); }
+C operator*(const C &a, float f) { return C(a.r * f, a.g * f, a.b * f); }
+C operator*(float f, const C &a) { return C(f * a.r, f * a.g, f * a.b); }
+C operator/(const C &a, float f) { return C(a.r / f, a.g / f, a.b / f); }
+float energy(const C &c) { return (c.r + c.g + c.b) * 0.333333f; }  // color.h:67
+
+struct Box {
+    float a[3], g[3];
+};
+
+// bound_t::cross(from, ray, enter, leave, dist), shipped (fast-math) form (bound.cc:389-436)
+bool cross_el(const Box &b, const V &from, const V &ray, float dist, float &enter, float &leave) {
+    float lmin = -1, lmax = -1;
+    for (int k = 0; k < 3; k++) {
+        if (ray[k] == 0) continue;
+        float t1 = (b.a[k] - from[k]) / ray[k], t2 = (b.g[k] - from[k]) / ray[k];
+        if (t1 > t2) {
+            float s = t1;
+            t1 = t2;
+            t2 = s;
+        }
+        if (k == 0) {
+            lmin = t1;
+            lmax = t2;
+        } else {
+            if (t1 > lmin) lmin = t1;
+            if ((t2 < lmax) || (lmax < 0)) lmax = t2;
+        }
+        if (k < 2 && ((lmax < 0) || (lmin > dist))) return false;
+    }
+    if ((lmin <= lmax) && (lmax >= 0) && (lmin <= dist)) {
+        enter = lmin;
+        leave = lmax;
+        return true;
+    }
+    return false;
+}
+// cross(from, ray, where, dist) (bound.cc:340-387)
+bool cross_w(const Box &b, const V &from, const V &ray, float dist, float &where) {
+    float e, l;
+    if (!cross_el(b, from, ray, dist, e, l)) return false;
+    where = (e > 0) ? e : 0;
+    return true;
+}
+
+struct Obj {
+    std::vector<V> tri_a, tri_b, tri_c, tri_n;
+    std::vector<uint32_t> tri_shader;
+    std::vector<yr_kd_node> nodes;
+    std::vector<uint32_t> prims;
+    Box tb, ob;
+    bool cast;
+};
+
+struct ONode {
+    Box b;
+    int left, right;  // left < 0: leaf, right = object
+};
+
+struct Light {
+    yr_light_desc d;
+    int samples;
+    C color;
+    V from, direction, corner, tox, toy;
+    std::vector<V> pts, jit1, jit2;
+    float sampdiv;
+};
+
+struct Cam {
+    V pos, vright, vup, vto;
+    int resx, resy;
+};
+
+struct Stats {
+    uint64_t primary, shadow, bounce, nodes, tests;
+};
+
+struct Scene {
+    std::vector<Obj> objs;
+    std::vector<ONode> otree;
+    std::vector<yr_shader_desc> shaders;
+    std::vector<Light> lights;
+    Cam cam;
+    yr_render_params rp;
+    Stats st;
+};
+
+// ------------------------------------------------------------- triangles
+// triangle_t::hit + intersect (triangle.h:48-86)
+bool tri_hit(const Obj &o, uint32_t t, const V &from, const V &ray, float &rt) {
+    const V va = o.tri_a[t] - from, vb = o.tri_b[t] - from, vc = o.tri_c[t] - from;
+    const V &N = o.tri_n[t];
+    V r = ((ray * N) < 0) ? -ray : ray;
+    if (((va ^ vb) * r) < 0) return false;
+    if (((vb ^ vc) * r) < 0) return false;
+    if (((vc ^ va) * r) < 0) return false;
+    rt = (N * va) / (N * ray);
+    return true;
+}
+
+// ---------------------------------------------------------------- kd-tree
+struct KdStackE {
+    uint32_t node;
+    float t;
+    V pb;
+    int prev;
+};
+
+// kdTree_t::Intersect (kdtree.cc:591-727) if !any, IntersectS (kdtree.cc:730-866) if any
+bool kd_intersect(Scene &S, const Obj &o, const V &from, const V &ray, float dist, uint32_t &tr, float &Z, bool any) {
+    float a, b, t;
+    if (!cross_el(o.tb, from, ray, dist, a, b)) return false;
+    const V invDir(1.f / ray.x, 1.f / ray.y, 1.f / ray.z);
+    bool hit = false;
+    KdStackE stack[64];
+    const uint32_t kNull = 0xffffffffu;
+    uint32_t curr = 0;
+    int enPt = 0;
+    stack[enPt].t = a;
+    stack[enPt].pb = (a >= 0.0) ? from + ray * a : from;
+    int exPt = 1;
+    stack[exPt].t = b;
+    stack[exPt].pb = from + ray * b;
+    stack[exPt].node = kNull;
+    stack[exPt].prev = 0;
+    while (curr != kNull) {
+        if (dist < stack[enPt].t) break;
+        while ((o.nodes[curr].flags & 3u) != 3u) {
+            S.st.nodes++;
+            const int axis = (int)(o.nodes[curr].flags & 3u);
+            float split;
+            memcpy(&split, &o.nodes[curr].word, 4);
+            const uint32_t right = o.nodes[curr].flags >> 2;
+            uint32_t far;
+            if (stack[enPt].pb[axis] <= split) {
+                if (stack[exPt].pb[axis] <= split) {
+                    curr++;
+                    continue;
+                }
+                if (stack[exPt].pb[axis] == split) {
+                    curr = right;
+                    continue;
+                }
+                far = right;
+                curr++;
+            } else {
+                if (split < stack[exPt].pb[axis]) {
+                    curr = right;
+                    continue;
+                }
+                far = curr + 1;
+                curr = right;
+            }
+            t = (split - from[axis]) * invDir[axis];
+            int tmp = exPt;
+            exPt++;
+            if (exPt == enPt) exPt++;
+            if (exPt >= 64) {
+                fprintf(stderr, "oracle: kd stack overflow\n");
+                abort();
+            }
+            const int nextAxis = (axis + 1) % 3, prevAxis = (axis + 2) % 3;
+            stack[exPt].prev = tmp;
+            stack[exPt].t = t;
+            stack[exPt].node = far;
+            stack[exPt].pb[axis] = split;
+            stack[exPt].pb[nextAxis] = from[nextAxis] + t * ray[nextAxis];
+            stack[exPt].pb[prevAxis] = from[prevAxis] + t * ray[prevAxis];
+        }
+        S.st.nodes++;
+        const uint32_t np = o.nodes[curr].flags >> 2;
+        for (uint32_t k = 0; k < np; k++) {
+            const uint32_t ti = (np == 1) ? o.nodes[curr].word : o.prims[o.nodes[curr].word + k];
+            S.st.tests++;
+            float rt;
+            if (tri_hit(o, ti, from, ray, rt)) {
+                if (any) {
+                    if (rt < dist && rt > 0.f) {
+                        tr = ti;
+                        return true;
+                    }
+                } else if (rt < Z && rt >= 0.f) {
+                    Z = rt;
+                    tr = ti;
+                    hit = true;
+                }
+            }
+        }
+        if (!any && hit && Z <= stack[exPt].t) return true;
+        enPt = exPt;
+        curr = stack[exPt].node;
+        exPt = stack[enPt].prev;
+    }
+    return hit;
+}
+
+// ------------------------------------------------------ object iterator
+// geomeIterator_t (geometree.h:36-157), front-to-back mode
+struct OIter {
+    const Scene &S;
+    const V from, ray;
+    std::vector<std::pair<int, float> > stack;
+    int current;
+    float maximun;
+    OIter(const Scene &s, float m, const V &f, const V &r) : S(s), from(f), ray(r), current(-1), maximun(m) {
+        if (S.otree.empty()) return;
+        float where = 0;
+        if (cross_w(S.otree[0].b, from, ray, maximun, where)) down(0);
+    }
+    void down(int node) {
+        while (S.otree[node].left >= 0) {
+            float hl = kInf, hr = kInf;
+            const ONode &n = S.otree[node];
+            bool hitl = cross_w(S.otree[n.left].b, from, ray, maximun, hl);
+            bool hitr = cross_w(S.otree[n.right].b, from, ray, maximun, hr);
+            if (!hitl && !hitr) {
+                if (stack.empty()) {
+                    current = -1;
+                    return;
+                }
+                node = stack.back().first;
+                stack.pop_back();
+                continue;
+            }
+            if (hl < hr) {
+                if (hitr) stack.push_back(std::make_pair(n.right, hr));
+                node = n.left;
+            } else {
+                if (hitl) stack.push_back(std::make_pair(n.left, hl));
+                node = n.right;
+            }
+        }
+        current = S.otree[node].right;
+    }
+    void next() {
+        current = -1;
+        while (!stack.empty() && stack.back().second > maximun) stack.pop_back();
+        if (!stack.empty()) {
+            int n = stack.back().first;
+            stack.pop_back();
+            down(n);
+        }
+    }
+    void limit(float z) {
+        if (z < maximun) maximun = z;
+    }
+};
+
+struct Hit {
+    int obj;
+    uint32_t tri;
+    float Z;
+};
+
+// closest hit: raytrace (limit passed to shoot) or firstHit (scene.cc:200-258, 688-721)
+Hit closest(Scene &S, const V &f, const V &ray, bool pass_limit, bool shadow_only) {
+    Hit best = {-1, 0, 0};
+    float limit = kInf;
+    OIter it(S, kInf, f, ray);
+    while (it.current >= 0) {
+        const Obj &o = S.objs[it.current];
+        if (!(shadow_only && !o.cast)) {
+            float dis = pass_limit ? limit : kInf;
+            float Z = dis;
+            uint32_t tr = 0;
+            if (kd_intersect(S, o, f, ray, dis, tr, Z, false) && Z > 0) {
+                if (pass_limit) limit = Z;
+                it.limit(Z);
+                if (best.obj < 0 || Z < best.Z) {
+                    best.obj = it.current;
+                    best.tri = tr;
+                    best.Z = Z;
+                }
+            }
+        }
+        it.next();
+    }
+    return best;
+}
+
+// scene_t::isShadowed (scene.cc:107-185)
+bool shadowed(Scene &S, const V &p, int own, const V &ray, float dist) {
+    const V self = p + ray * S.rp.self_bias;
+    const V p2 = p + ray * kMinRay;
+    OIter it(S, dist, p2, ray);
+    while (it.current >= 0) {
+        const Obj &o = S.objs[it.current];
+        if (o.cast) {
+            float Z = dist;
+            uint32_t tr;
+            if (kd_intersect(S, o, it.current == own ? self : p2, ray, dist, tr, Z, true)) return true;
+        }
+        it.next();
+    }
+    return false;
+}
+
+bool shadowed_point(Scene &S, const V &p, int own, const V &l) {
+    S.st.shadow++;
+    V ray = l - p;
+    float dist = length(ray);
+    ray = normalize(ray);
+    return shadowed(S, p, own, ray, dist);
+}
+
+bool shadowed_dir(Scene &S, const V &p, int own, const V &dir) {
+    S.st.shadow++;
+    return shadowed(S, p, own, normalize(dir), kInf);
+}
+
+// ------------------------------------------------------------------- QMC
+// Halton setStart(n) + getNext() (mcqmc.h:24-49), shipped (fast-math) form
+float halton(unsigned base, unsigned n) {
+    const double inv = 1.0 / double(base);
+    double value = 0.0, factor = inv;
+    unsigned i = n;
+    while (i > 0) {
+        value += double(i % base) * factor;
+        i /= base;
+        factor *= inv;
+    }
+    const double r = (1.0 - 0.0000000001) - value;
+    if (inv < r) {
+        value = value + inv;
+    } else {
+        double hh, h = inv;
+        do {
+            hh = h;
+            h *= inv;
+        } while (h >= r);
+        value = (hh + h) + (value - 1.0);
+    }
+    return (float)value;
+}
+
+uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+// per-pixel Cranley-Patterson rotation (the library's documented hash)
+float cp_rot(uint32_t seed, uint32_t pixel, uint32_t dim) {
+    uint32_t h = fmix32(seed * 0x9e3779b9u + 0x632be5abu);
+    h = fmix32(h ^ (pixel * 0x85ebca77u));
+    h = fmix32(h ^ (dim * 0xc2b2ae3du + 0x27d4eb2fu));
+    return (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+float cp_add(float v, float r) {
+    float u = v + r;
+    if (u >= 1.0f) u -= 1.0f;
+    return u;
+}
+const unsigned kPrimes[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+uint32_t light_dim(int k, int v) { return 64u + 16u * (uint32_t)k + 2u * (uint32_t)v; }
+
+// RI_LP (mcqmc.h:73-78)
+float ri_lp(unsigned i) {
+    unsigned r = 0;
+    for (unsigned v = 1u << 31; i; i >>= 1, v |= v >> 1)
+        if (i & 1) r ^= v;
+    return (float)(double(r) / 4294967296.0);
+}
+
+// ----------------------------------------------------------------- noise
+// Blender permutation (noise.cc:118-127, first half)
+const unsigned char kPerm[256] = {
+    162, 160, 25,  59,  248, 235, 170, 238, 243, 28,  103, 40,  29,  237, 0,   222, 149, 46,  220, 63,  58,  130,
+    53,  77,  108, 186, 54,  208, 246, 12,  121, 50,  209, 89,  244, 8,   139, 99,  137, 47,  184, 180, 151, 131,
+    242, 143, 24,  199, 81,  20,  101, 135, 72,  32,  66,  168, 128, 181, 64,  19,  178, 34,  126, 87,  188, 127,
+    107, 157, 134, 76,  200, 219, 124, 213, 37,  78,  90,  85,  116, 80,  205, 179, 122, 187, 195, 203, 182, 226,
+    228, 236, 253, 152, 11,  150, 211, 158, 92,  161, 100, 241, 129, 97,  225, 196, 36,  114, 73,  140, 144, 75,
+    132, 52,  56,  171, 120, 202, 31,  1,   215, 147, 17,  193, 88,  169, 49,  249, 68,  109, 191, 51,  156, 95,
+    9,   148, 163, 133, 6,   198, 154, 30,  123, 70,  21,  48,  39,  43,  27,  113, 60,  91,  214, 111, 98,  172,
+    79,  194, 192, 14,  177, 35,  167, 223, 71,  176, 119, 105, 5,   233, 230, 231, 118, 115, 15,  254, 110, 155,
+    86,  239, 18,  165, 55,  252, 174, 217, 3,   142, 221, 16,  185, 206, 201, 141, 218, 42,  189, 104, 23,  159,
+    190, 212, 10,  204, 210, 232, 67,  61,  112, 183, 2,   125, 153, 216, 13,  96,  138, 4,   44,  62,  146, 229,
+    175, 83,  7,   224, 41,  166, 197, 227, 245, 247, 74,  65,  38,  106, 22,  94,  82,  45,  33,  173, 240, 145,
+    255, 234, 84,  250, 102, 26,  69,  57,  207, 117, 164, 136, 251, 93};
+int hsh(int i) { return kPerm[i & 255]; }
+float fade(float t) { return t * t * t * (t * (t * 6 - 15) + 10); }
+float lerp(float t, float a, float b) { return a + t * (b - a); }
+float grad(int hash, float x, float y, float z) {
+    int h = hash & 15;
+    float u = h < 8 ? x : y, v = h < 4 ? y : h == 12 || h == 14 ? x : z;
+    return ((h & 1) == 0 ? u : -u) + ((h & 2) == 0 ? v : -v);
+}
+// newPerlin_t::operator() (noise.cc:161-183), source order
+float perlin(const V &pt) {
+    float x = pt.x, y = pt.y, z = pt.z;
+    float u = floorf(x), v = floorf(y), w = floorf(z);
+    int X = ((int)u) & 255, Y = ((int)v) & 255, Z = ((int)w) & 255;
+    x -= u;
+    y -= v;
+    z -= w;
+    u = fade(x);
+    v = fade(y);
+    w = fade(z);
+    int A = hsh(X) + Y, AA = hsh(A) + Z, AB = hsh(A + 1) + Z, B = hsh(X + 1) + Y, BA = hsh(B) + Z, BB = hsh(B + 1) + Z;
+    float nv = lerp(w,
+                    lerp(v, lerp(u, grad(hsh(AA), x, y, z), grad(hsh(BA), x - 1, y, z)),
+                         lerp(u, grad(hsh(AB), x, y - 1, z), grad(hsh(BB), x - 1, y - 1, z))),
+                    lerp(v, lerp(u, grad(hsh(AA + 1), x, y, z - 1), grad(hsh(BA + 1), x - 1, y, z - 1)),
+                         lerp(u, grad(hsh(AB + 1), x, y - 1, z - 1), grad(hsh(BB + 1), x - 1, y - 1, z - 1))));
+    return (float)(0.5 + 0.5 * (double)nv);
+}
+// fBm_t::operator() (noise.cc:638-650)
+float fbm(V tp, float H, float lac, float oct) {
+    float value = 0, pwr = 1, pwHL = (float)pow((double)lac, (double)-H);
+    for (int i = 0; i < (int)oct; i++) {
+        value += ((float)2.0 * perlin(tp) - (float)1.0) * pwr;
+        pwr *= pwHL;
+        tp = V(tp.x * lac, tp.y * lac, tp.z * lac);
+    }
+    float rmd = oct - floorf(oct);
+    if (rmd != 0.f) value += rmd * ((float)2.0 * perlin(tp) - (float)1.0) * pwr;
+    return value;
+}
+// turbulence (noise.cc:808-819)
+float turbulence(const V &pt, int oct, float size, bool hard) {
+    float amp = 1, sum = 0;
+    V tp(pt.x * size, pt.y * size, pt.z * size);
+    for (int i = 0; i <= oct; i++, amp *= 0.5f, tp = V(tp.x * 2.0f, tp.y * 2.0f, tp.z * 2.0f)) {
+        float val = perlin(tp);
+        if (hard) val = (float)fabs(2.0 * (double)val - 1.0);
+        sum += amp * val;
+    }
+    return sum * ((float)(1 << oct) / (float)((1 << (oct + 1)) - 1));
+}
+
+// --------------------------------------------------------------- shading
+struct SP {
+    V P, N, Ng, NU, NV;
+    int obj;
+    int shader;
+};
+
+void createCS(const V &N, V &u, V &v) {  // vector3d.h:240-258
+    if ((N.x == 0) && (N.y == 0)) {
+        u = (N.z < 0) ? V(-1, 0, 0) : V(1, 0, 0);
+        v = V(0, 1, 0);
+    } else {
+        const float d = (float)(1.0 / sqrt((double)(N.y * N.y + N.x * N.x)));
+        u = V(N.y * d, -N.x * d, 0);
+        v = N ^ u;
+    }
+}
+V faceForward(const V &Ng, const V &N, const V &I) { return ((Ng * I) < 0) ? -N : N; }
+V reflectv(const V &n, const V &v) {
+    const float vn = v * n;
+    if (vn < 0) return -v;
+    return (2 * vn) * n - v;
+}
+
+SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from, const V &ray) {
+    SP s;
+    s.P = from + Z * ray;
+    const Obj &o = S.objs[obj];
+    s.N = s.Ng = o.tri_n[tri];
+    createCS(s.N, s.NU, s.NV);
+    s.obj = obj;
+    s.shader = (int)o.tri_shader[tri];
+    return s;
+}
+
+C col3(const float *p) { return C(p[0], p[1], p[2]); }
+
+// modulator "mix" of a musgrave/clouds texture into the diffuse colour
+C diffuse(const Scene &S, const SP &sp) {
+    const yr_shader_desc &d = S.shaders[sp.shader];
+    C c = col3(d.color);
+    if (d.tex_type == YR_TEX_NONE || !(d.mod_color > 0)) return c;
+    V tp(d.mod_size[0] * (sp.P.x + d.mod_ofs[0]), d.mod_size[1] * (sp.P.y + d.mod_ofs[1]),
+         d.mod_size[2] * (sp.P.z + d.mod_ofs[2]));
+    float f;
+    if (d.tex_type == YR_TEX_MUSGRAVE_FBM)
+        f = d.tex_intensity * fbm(V(tp.x * d.tex_size, tp.y * d.tex_size, tp.z * d.tex_size), d.tex_H,
+                                  d.tex_lacunarity, d.tex_octaves);
+    else
+        f = turbulence(tp, d.tex_depth, d.tex_size, d.tex_hard != 0);
+    C tex = col3(d.tex_color1) + f * (col3(d.tex_color2) - col3(d.tex_color1));
+    float w = d.mod_color;
+    if (w > 1.0f) return tex;
+    return tex * w + (1 - w) * c;
+}
+
+// genericShader_t::fromLight (basicshaders.cc:46-70)
+C fromLight(const Scene &S, const SP &sp, const V &ldir, const C &lcol, const V &eye) {
+    const yr_shader_desc &d = S.shaders[sp.shader];
+    V edir = normalize(eye);
+    V N = faceForward(sp.Ng, sp.N, edir);
+    float inte = N * ldir;
+    if (inte < 0) return C();
+    C lkc = diffuse(S, sp), lks = col3(d.specular);
+    edir = reflectv(N, edir);
+    float refle = edir * ldir;
+    if (refle < 0) refle = 0;
+    else refle = (float)pow((double)refle, (double)d.hard);
+    return ((C(1.f * inte, 1.f * inte, 1.f * inte) * lcol) * lkc) + (lks * refle) * lcol;
+}
+
+// --------------------------------------------------------------- lights
+struct Ctx {
+    uint32_t pixel, s, pi;  // pixel, camera sample, path index
+    int npath;
+};
+
+C illum_point(Scene &S, const Light &L, const SP &sp, const V &eye) {
+    V Lv = L.from - sp.P;
+    V dir = normalize(Lv);
+    float id2 = Lv * Lv;
+    if (id2 != 0.f) id2 = 1.f / id2;
+    C col;
+    if (L.d.cast_shadows ? !shadowed_point(S, sp.P, sp.obj, L.from) : true)
+        col = fromLight(S, sp, dir, L.color * id2, eye);
+    return col;
+}
+
+C illum_area(Scene &S, int k, const Light &L, const SP &sp, const V &eye, int v, uint32_t m0, const Ctx &cx) {
+    V edir = normalize(eye);
+    V N = faceForward(sp.Ng, sp.N, edir);
+    float plane_at = (sp.P - L.from) * L.direction;
+    if (plane_at <= 0) return C();
+    const uint32_t d = light_dim(k, v);
+    const float r0 = cp_rot(S.rp.seed, cx.pixel, d), r1 = cp_rot(S.rp.seed, cx.pixel, d + 1);
+    C resul;
+    for (int i = 0; i < L.samples; i++) {
+        const uint32_t m = m0 * (uint32_t)L.samples + (uint32_t)i;
+        const float h2 = cp_add(halton(2, m), r0), h3 = cp_add(halton(3, m), r1);
+        V sampleP;
+        if (L.samples == 1) sampleP = (L.corner + L.tox * h2) + L.toy * h3;
+        else sampleP = (L.pts[i] + L.jit1[i] * (h2 - 0.5f)) + L.jit2[i] * (h3 - 0.5f);
+        V Lv = sampleP - sp.P;
+        if ((Lv * N) < 0) continue;
+        if (!shadowed_point(S, sp.P, sp.obj, sampleP)) {
+            V dir = Lv;
+            float ld2 = normLenSqr(dir);
+            ld2 = (ld2 != 0) ? (1.f / ld2) : 1.f;
+            resul = resul + fromLight(S, sp, dir, (L.d.power * L.color) * ld2, eye);
+        }
+    }
+    return (plane_at * resul) / (float)L.samples;
+}
+
+V uniHemi(const V &N, const V &Ru, const V &Rv, float z1, float z2) {  // hemilight.cc:103-114
+    z2 = (float)((double)z2 * 6.283185307179586);
+    const float c = (float)cos((double)z2), s = (float)sin((double)z2);
+    return (Ru * c + Rv * s) * (float)sqrt(1.0 - (double)(z1 * z1)) + N * z1;
+}
+
+C illum_hemi(Scene &S, int k, const Light &L, const SP &sp, const V &eye, int v, uint32_t m0, const Ctx &cx) {
+    V N = faceForward(sp.Ng, sp.N, eye);
+    C fl = fromLight(S, sp, N, C(1, 1, 1), eye);
+    float mad = fabsf(fl.r);
+    if (fabsf(fl.g) > mad) mad = fabsf(fl.g);
+    if (fabsf(fl.b) > mad) mad = fabsf(fl.b);
+    if (mad < 0.05f) return C();
+    const uint32_t d = light_dim(k, v);
+    const float r0 = cp_rot(S.rp.seed, cx.pixel, d), r1 = cp_rot(S.rp.seed, cx.pixel, d + 1);
+    C total;
+    for (int sm = 0; sm < L.samples; sm++) {
+        const uint32_t m = m0 * (uint32_t)L.samples + (uint32_t)sm;
+        V dir = uniHemi(N, sp.NU, sp.NV, cp_add(halton(2, m), r0), cp_add(halton(3, m), r1));
+        float occ = dir * N;
+        if (occ > 0) {
+            bool sh = (L.d.maxdist > 0) ? shadowed_point(S, sp.P, sp.obj, sp.P + L.d.maxdist * dir)
+                                        : shadowed_dir(S, sp.P, sp.obj, dir);
+            if (!sh) total = total + L.color * occ;
+        }
+    }
+    return (L.sampdiv * total) * fl;
+}
+
+V cosHemi(const V &N, const V &Ru, const V &Rv, float z1, float z2) {  // pathtools.cc:32-43
+    if (z1 > 1.0f) z1 = 1.0f;
+    z2 = (float)((double)z2 * 6.283185307179586);
+    const float c = (float)cos((double)z2), s = (float)sin((double)z2);
+    return (Ru * c + Rv * s) * (float)sqrt(1.0 - (double)z1) + N * sqrtf(z1);
+}
+
+// scene_t::light (scene.cc:260-277) without the path light (indirect) or
+// with it (camera vertex); v = QMC vertex level, m0 = QMC sample index.
+C light_sum(Scene &S, const SP &sp, const V &eye, bool indirect, int v, uint32_t m0, const Ctx &cx);
+
+// pathLight_t::normalSample + takeSample (pathlight.cc:223-403), explicit indices
+C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx) {
+    V N = faceForward(sp.Ng, sp.N, eye);
+    C dif = diffuse(S, sp);
+    if (energy(dif) < 0.05f) return C();
+    const int P = L.d.samples, depth = L.d.depth;
+    C total;
+    for (int i = 0; i < P; i++) {
+        const uint32_t n = cx.s * (uint32_t)P + (uint32_t)i;
+        V ray = cosHemi(N, sp.NU, sp.NV, cp_add(halton(kPrimes[0], n), cp_rot(S.rp.seed, cx.pixel, 0)),
+                        cp_add(halton(kPrimes[1], n), cp_rot(S.rp.seed, cx.pixel, 1)));
+        const V startray = ray;
+        V where = sp.P;
+        C raycolor(1, 1, 1);
+        const float startN = startray * N;
+        for (int j = 0; j < depth; ++j) {
+            if (energy(raycolor) < 0.05f) break;
+            S.st.bounce++;
+            const V f = where + ray * kMinRay;
+            Hit h = closest(S, f, ray, false, true);
+            if (h.obj < 0) {
+                total = total + (startN * raycolor) * col3(S.rp.background);
+                break;
+            }
+            SP t = surface(S, h.obj, h.tri, h.Z, f, ray);
+            Ctx c2 = cx;
+            c2.pi = (uint32_t)i;
+            const V eye2 = (t.P + (-ray)) - t.P;
+            C light = light_sum(S, t, eye2, true, j + 1, n, c2);
+            total = total + (startN * raycolor) * light;
+            const V HN = faceForward(t.Ng, t.N, -ray);
+            raycolor = raycolor * diffuse(S, t);
+            if (j + 1 < depth) {
+                const int lev = j + 1;
+                ray = cosHemi(HN, t.NU, t.NV,
+                              cp_add(halton(kPrimes[2 * lev], n), cp_rot(S.rp.seed, cx.pixel, 2 * lev)),
+                              cp_add(halton(kPrimes[2 * lev + 1], n), cp_rot(S.rp.seed, cx.pixel, 2 * lev + 1)));
+            }
+            where = t.P;
+        }
+    }
+    total = total * ((float)(1.0 / (double)(float)P) / 1.0f);
+    return (dif * total) * L.d.power;
+}
+
+C light_sum(Scene &S, const SP &sp, const V &eye, bool indirect, int v, uint32_t m0, const Ctx &cx) {
+    C fl;
+    for (size_t k = 0; k < S.lights.size(); k++) {
+        const Light &L = S.lights[k];
+        switch (L.d.type) {
+        case YR_LIGHT_POINT: fl = fl + illum_point(S, L, sp, eye); break;
+        case YR_LIGHT_AREA: fl = fl + illum_area(S, (int)k, L, sp, eye, v, m0, cx); break;
+        case YR_LIGHT_HEMI: fl = fl + illum_hemi(S, (int)k, L, sp, eye, v, m0, cx); break;
+        case YR_LIGHT_PATH:
+            if (!indirect) fl = fl + illum_path(S, L, sp, eye, cx);
+            break;
+        }
+    }
+    return fl;
+}
+
+// camera_t ctor + shootRay (camera.cc:27-87, 146-210)
+void make_camera(const yr_camera_desc &c, Cam &o) {
+    const V pos(c.pos[0], c.pos[1], c.pos[2]);
+    V vup = V(c.up[0], c.up[1], c.up[2]) - pos;
+    V vto = V(c.look[0], c.look[1], c.look[2]) - pos;
+    V vright = vup ^ vto;
+    vup = vright ^ vto;
+    vup = normalize(vup);
+    vright = normalize(vright);
+    vright = vright * -1.0f;
+    float vl = vto * vto;
+    if (vl != 0) {
+        vl = sqrtf(vl);
+        const float d = (float)(1.0 / vl);
+        vto = V(vto.x * d, vto.y * d, vto.z * d);
+    }
+    vup = vup * (c.aspect * (float)c.resy / (float)c.resx);
+    vto = (vto * c.focal) - 0.5f * (vup + vright);
+    vup = vup / (float)c.resy;
+    vright = vright / (float)c.resx;
+    o.pos = pos;
+    o.vright = vright;
+    o.vup = vup;
+    o.vto = vto;
+    o.resx = c.resx;
+    o.resy = c.resy;
+}
+V shoot(const Cam &c, float px, float py) { return normalize(c.vto + (c.vright * px + c.vup * py)); }
+
+// one camera sample: scene_t::raytrace (scene.cc:200-258)
+void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
+    const uint32_t spp = S.rp.spp ? S.rp.spp : 1;
+    const int x = (int)(pixel % (uint32_t)S.cam.resx), y = (int)(pixel / (uint32_t)S.cam.resx);
+    float fx = 0.5f, fy = 0.5f;
+    if (s > 0) {
+        const uint32_t c = s - 1;
+        const float tsd = (float)(1.0 / (float)(spp - 1));
+        fx = (float)(0.5 + (double)S.rp.aa_pixelwidth * ((double)ri_lp(c + pixel) - 0.5));
+        fy = (float)(0.5 + (double)S.rp.aa_pixelwidth * ((double)((float)c * tsd) - 0.5));
+    }
+    const V ray = shoot(S.cam, (float)x + fx, (float)y + fy);
+    S.st.primary++;
+    if (S.rp.raydepth <= 0) {
+        rgba[0] = rgba[1] = rgba[2] = rgba[3] = 0.f;
+        return;
+    }
+    const V f = S.cam.pos + ray * kMinRay;
+    Hit h = closest(S, f, ray, true, false);
+    if (h.obj < 0) {
+        rgba[0] = S.rp.background[0];
+        rgba[1] = S.rp.background[1];
+        rgba[2] = S.rp.background[2];
+        rgba[3] = 0.f;
+        return;
+    }
+    SP sp = surface(S, h.obj, h.tri, h.Z, f, ray);
+    Ctx cx;
+    cx.pixel = pixel;
+    cx.s = s;
+    cx.pi = 0;
+    C c = light_sum(S, sp, S.cam.pos - sp.P, false, 0, s, cx);
+    rgba[0] = c.r;
+    rgba[1] = c.g;
+    rgba[2] = c.b;
+    rgba[3] = 1.f;
+}
+
+// ----------------------------------------------------------- scene load
+template <class T>
+bool rdv(FILE *f, T *p, size_t n) {
+    return n == 0 || fread(p, sizeof(T), n, f) == n;
+}
+
+V vtx(const std::vector<float> &v, uint32_t i) { return V(v[3 * i], v[3 * i + 1], v[3 * i + 2]); }
+
+}  // namespace
+
+extern "C" {
+
+typedef struct orc_scene orc_scene;
+struct orc_scene {
+    Scene s;
+};
+
+// Load a YRS1 file.  Trees are added with orc_set_tree / orc_set_object_tree.
+orc_scene *orc_load(const char *path) {
+    FILE *f = fopen(path, "rb");
+    if (!f) return NULL;
+    char magic[4];
+    uint32_t hdr[4];
+    orc_scene *o = new orc_scene;
+    Scene &S = o->s;
+    yr_camera_desc cam;
+    bool ok = rdv(f, magic, 4) && memcmp(magic, "YRS1", 4) == 0 && rdv(f, hdr, 4) && rdv(f, &cam, 1) &&
+              rdv(f, &S.rp, 1);
+    S.shaders.resize(hdr[1]);
+    std::vector<yr_light_desc> ld(hdr[2]);
+    ok = ok && rdv(f, S.shaders.data(), hdr[1]) && rdv(f, ld.data(), hdr[2]);
+    S.objs.resize(hdr[0]);
+    for (uint32_t i = 0; ok && i < hdr[0]; i++) {
+        uint32_t oh[4];
+        ok = rdv(f, oh, 4);
+        if (!ok) break;
+        std::vector<float> v(3 * (size_t)oh[0]);
+        std::vector<uint32_t> t(3 * (size_t)oh[1]), ts;
+        ok = rdv(f, v.data(), v.size()) && rdv(f, t.data(), t.size());
+        if (ok && oh[2] == YR_PER_TRIANGLE) {
+            ts.resize(oh[1]);
+            ok = rdv(f, ts.data(), ts.size());
+        }
+        Obj &ob = S.objs[i];
+        ob.cast = oh[3] != 0;
+        for (uint32_t k = 0; ok && k < oh[1]; k++) {
+            V a = vtx(v, t[3 * k]), b = vtx(v, t[3 * k + 1]), c = vtx(v, t[3 * k + 2]);
+            ob.tri_a.push_back(a);
+            ob.tri_b.push_back(b);
+            ob.tri_c.push_back(c);
+            ob.tri_n.push_back(normalize((b - a) ^ (c - a)));  // triangle.cc:30-43
+            ob.tri_shader.push_back(oh[2] == YR_PER_TRIANGLE ? ts[k] : oh[2]);
+        }
+    }
+    fclose(f);
+    if (!ok) {
+        delete o;
+        return NULL;
+    }
+    make_camera(cam, S.cam);
+    for (size_t k = 0; k < ld.size(); k++) {
+        Light L;
+        L.d = ld[k];
+        L.samples = ld[k].samples;
+        L.color = col3(ld[k].color);
+        L.sampdiv = 0;
+        const V a(ld[k].p[0][0], ld[k].p[0][1], ld[k].p[0][2]), b(ld[k].p[1][0], ld[k].p[1][1], ld[k].p[1][2]),
+            c(ld[k].p[2][0], ld[k].p[2][1], ld[k].p[2][2]), d(ld[k].p[3][0], ld[k].p[3][1], ld[k].p[3][2]);
+        if (L.d.type == YR_LIGHT_POINT) {
+            L.from = a;
+            L.color = L.color * ld[k].power;
+        } else if (L.d.type == YR_LIGHT_AREA) {
+            // areaLight_t ctor + fillQuad (arealight.cc:31-91)
+            const int nsam = ld[k].samples;
+            float ab = length(b - a), bc = length(c - b), cd = length(d - c), da = length(a - d);
+            float max_v = (bc > da) ? bc : da, max_h = (ab > cd) ? ab : cd;
+            int v_samp = (int)((max_v / (max_v + max_h)) * 2.0 * (double)sqrtf((float)nsam));
+            int h_samp = (int)((max_h / (max_v + max_h)) * 2.0 * (double)sqrtf((float)nsam));
+            if (nsam == 1) {
+                L.samples = 1;
+            } else {
+                V inc_v_a = (d - a) / (float)v_samp, inc_v_b = (c - b) / (float)v_samp;
+                V line_a = a + 0.5f * inc_v_a, line_b = b + 0.5f * inc_v_b;
+                for (int i = 0; i < v_samp; ++i) {
+                    V inc_h = (line_b - line_a) / (float)h_samp;
+                    V point = line_a + 0.5f * inc_h;
+                    for (int j = 0; j < h_samp; ++j) {
+                        float vf = ((float)j) / ((float)h_samp);
+                        V inc_v = inc_v_a * (float)(1.0 - vf) + inc_v_b * vf;
+                        L.pts.push_back(point);
+                        L.jit1.push_back(inc_h);
+                        L.jit2.push_back(inc_v);
+                        point = point + inc_h;
+                    }
+                    line_a = line_a + inc_v_a;
+                    line_b = line_b + inc_v_b;
+                }
+                L.samples = (int)L.pts.size();
+            }
+            L.direction = normalize((b - a) ^ (d - a));
+            L.from = (((a + b) + c) + d) * 0.25f;
+            L.corner = a;
+            L.tox = b - a;
+            L.toy = d - a;
+        } else if (L.d.type == YR_LIGHT_HEMI) {
+            L.sampdiv = ld[k].power / (float)ld[k].samples;
+        }
+        S.lights.push_back(L);
+    }
+    memset(&S.st, 0, sizeof(S.st));
+    return o;
+}
+
+void orc_free(orc_scene *o) { delete o; }
+
+int orc_set_tree(orc_scene *o, uint32_t obj, const yr_kd_node *nodes, uint32_t nnodes, const uint32_t *prims,
+                 uint32_t nprims, const float *tree_bound, const float *obj_bound) {
+    if (!o || obj >= o->s.objs.size()) return 1;
+    Obj &ob = o->s.objs[obj];
+    ob.nodes.assign(nodes, nodes + nnodes);
+    ob.prims.assign(prims, prims + nprims);
+    memcpy(ob.tb.a, tree_bound, 12);
+    memcpy(ob.tb.g, tree_bound + 3, 12);
+    memcpy(ob.ob.a, obj_bound, 12);
+    memcpy(ob.ob.g, obj_bound + 3, 12);
+    return 0;
+}
+
+// node records: bmin[3], left, bmax[3], right (left < 0: leaf, right = object)
+int orc_set_object_tree(orc_scene *o, const float *recs, uint32_t n) {
+    o->s.otree.resize(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const float *r = recs + 8 * (size_t)i;
+        ONode &nd = o->s.otree[i];
+        memcpy(nd.b.a, r, 12);
+        memcpy(&nd.left, r + 3, 4);
+        memcpy(nd.b.g, r + 4, 12);
+        memcpy(&nd.right, r + 7, 4);
+    }
+    return 0;
+}
+
+// rays: org[3], tmax, dir[3], flags (yr_ray); hits: t, object, triangle, nodes
+void orc_trace_closest(orc_scene *o, const float *rays, uint32_t n, uint32_t *hits, int shadow_only) {
+    for (uint32_t i = 0; i < n; i++) {
+        const float *r = rays + 8 * (size_t)i;
+        const V org(r[0], r[1], r[2]), dir(r[4], r[5], r[6]);
+        const uint64_t n0 = o->s.st.nodes;
+        Hit h = closest(o->s, org + dir * kMinRay, dir, false, shadow_only != 0);
+        float t = h.obj >= 0 ? h.Z : 0.f;
+        memcpy(&hits[4 * i], &t, 4);
+        hits[4 * i + 1] = h.obj >= 0 ? (uint32_t)h.obj : 0xffffffffu;
+        hits[4 * i + 2] = h.obj >= 0 ? h.tri : 0xffffffffu;
+        hits[4 * i + 3] = (uint32_t)(o->s.st.nodes - n0);
+    }
+}
+
+// shadow rays: p[3], object, l[3], flags (yr_shadow_ray)
+void orc_trace_shadow(orc_scene *o, const float *rays, uint32_t n, uint8_t *occ) {
+    for (uint32_t i = 0; i < n; i++) {
+        const float *r = rays + 8 * (size_t)i;
+        int own;
+        uint32_t flags;
+        memcpy(&own, r + 3, 4);
+        memcpy(&flags, r + 7, 4);
+        const V p(r[0], r[1], r[2]), l(r[4], r[5], r[6]);
+        occ[i] = (flags & 1u) ? shadowed_dir(o->s, p, own, l) : shadowed_point(o->s, p, own, l);
+    }
+}
+
+// Kd traversal of one object only (kdTree_t::Intersect / IntersectS):
+// out: hit, tri, Z bits, nodes visited
+void orc_kd(orc_scene *o, uint32_t obj, const float *from, const float *dir, float dist, int any, uint32_t *out) {
+    const uint64_t n0 = o->s.st.nodes;
+    uint32_t tr = 0;
+    float Z = dist < 0 ? kInf : dist;
+    bool h = kd_intersect(o->s, o->s.objs[obj], V(from[0], from[1], from[2]), V(dir[0], dir[1], dir[2]),
+                          dist < 0 ? kInf : dist, tr, Z, any != 0);
+    out[0] = h;
+    out[1] = h ? tr : 0xffffffffu;
+    float z = (h && !any) ? Z : 0.f;
+    memcpy(&out[2], &z, 4);
+    out[3] = (uint32_t)(o->s.st.nodes - n0);
+}
+
+// Render pixels [x0,x1) x [y0,y1) into rgba (full image layout, resx*resy*4).
+// stats: primary, shadow, bounce, nodes, tests
+void orc_render(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint64_t *stats) {
+    Scene &S = o->s;
+    const uint32_t spp = S.rp.spp ? S.rp.spp : 1;
+    memset(&S.st, 0, sizeof(S.st));
+    for (int y = y0; y < y1; y++)
+        for (int x = x0; x < x1; x++) {
+            const uint32_t pixel = (uint32_t)(y * S.cam.resx + x);
+            float first[4], tot[4] = {0, 0, 0, 0}, c[4];
+            for (uint32_t s = 0; s < spp; s++) {
+                camera_sample(S, pixel, s, c);
+                if (s == 0) memcpy(first, c, 16);
+                else
+                    for (int k = 0; k < 4; k++) tot[k] += c[k];
+            }
+            float *px = rgba + 4 * (size_t)pixel;
+            if (spp > 1) {
+                const float d = (float)(1 + (spp - 1));
+                for (int k = 0; k < 4; k++) px[k] = (first[k] + tot[k]) / d;
+            } else {
+                memcpy(px, first, 16);
+            }
+        }
+    if (stats) {
+        stats[0] = S.st.primary;
+        stats[1] = S.st.shadow;
+        stats[2] = S.st.bounce;
+        stats[3] = S.st.nodes;
+        stats[4] = S.st.tests;
+    }
+}
+
+// primary ray directions of pixel centres (camera_t::shootRay)
+void orc_camera_rays(orc_scene *o, float *dirs) {
+    const Cam &c = o->s.cam;
+    for (int y = 0; y < c.resy; y++)
+        for (int x = 0; x < c.resx; x++) {
+            V d = shoot(c, (float)x + 0.5f, (float)y + 0.5f);
+            float *p = dirs + 3 * ((size_t)y * c.resx + x);
+            p[0] = d.x;
+            p[1] = d.y;
+            p[2] = d.z;
+        }
+}
+
+float orc_halton(uint32_t base, uint32_t n) { return halton(base, n); }
+float orc_ri_lp(uint32_t i) { return ri_lp(i); }
+float orc_cp_rot(uint32_t seed, uint32_t pixel, uint32_t dim) { return cp_rot(seed, pixel, dim); }
+float orc_perlin(float x, float y, float z) { return perlin(V(x, y, z)); }
+float orc_fbm(float x, float y, float z, float H, float lac, float oct) { return fbm(V(x, y, z), H, lac, oct); }
+float orc_turbulence(float x, float y, float z, int oct, float size, int hard) {
+    return turbulence(V(x, y, z), oct, size, hard != 0);
+}
+
+}  // extern "C"

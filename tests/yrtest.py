@@ -1,0 +1,275 @@
+"""Shared helpers for the tests: the CPU oracle (ctypes), the reference
+harness (oracle/_ref, present only where the reference was built), and
+host-side tree extraction through the product's C ABI."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from yafray_b200 import abi, scenes  # noqa: E402
+
+ORACLE_LIB = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "yr_ref_harness")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+_orc = None
+
+
+def oracle() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_LIB):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True,
+                           capture_output=True)
+        lib = C.CDLL(ORACLE_LIB)
+        P, F, U = C.c_void_p, C.c_float, C.c_uint32
+        sig = {
+            "orc_load": (P, [C.c_char_p]),
+            "orc_free": (None, [P]),
+            "orc_set_tree": (C.c_int, [P, U, P, U, P, U, P, P]),
+            "orc_set_object_tree": (C.c_int, [P, P, U]),
+            "orc_trace_closest": (None, [P, P, U, P, C.c_int]),
+            "orc_trace_shadow": (None, [P, P, U, P]),
+            "orc_kd": (None, [P, U, P, P, F, C.c_int, P]),
+            "orc_render": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
+            "orc_camera_rays": (None, [P, P]),
+            "orc_halton": (F, [U, U]),
+            "orc_ri_lp": (F, [U]),
+            "orc_cp_rot": (F, [U, U, U]),
+            "orc_perlin": (F, [F, F, F]),
+            "orc_fbm": (F, [F, F, F, F, F, F]),
+            "orc_turbulence": (F, [F, F, F, C.c_int, F, C.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _orc = lib
+    return _orc
+
+
+def has_harness() -> bool:
+    return os.path.exists(HARNESS)
+
+
+def ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+# ----------------------------------------------------------- product trees
+def product_tree(mesh: scenes.Mesh) -> dict:
+    lib = abi.load()
+    v = np.ascontiguousarray(mesh.verts, np.float32)
+    t = np.ascontiguousarray(mesh.tris, np.uint32)
+    p = C.POINTER(abi.YrKdTree)()
+    st = lib.yr_kdtree_build(v.ctypes.data_as(C.POINTER(C.c_float)), v.shape[0],
+                             t.ctypes.data_as(C.POINTER(C.c_uint32)), t.shape[0], C.byref(p))
+    abi.check(st, "yr_kdtree_build")
+    tr = p.contents
+    nodes = np.ctypeslib.as_array(C.cast(tr.nodes, C.POINTER(C.c_uint32)), (2 * tr.nnodes,)).reshape(-1, 2).copy()
+    prims = np.ctypeslib.as_array(tr.prims, (max(tr.nprims, 1),))[:tr.nprims].copy()
+    out = dict(nodes=nodes, prims=prims, tb=np.array(tr.bound[:], np.float32), max_depth=tr.max_depth,
+               max_leaf=tr.max_leaf_size, cost_ratio=np.float32(tr.cost_ratio))
+    lib.yr_kdtree_free(p)
+    return out
+
+
+def mesh_bound(mesh: scenes.Mesh) -> np.ndarray:
+    """meshObject_t::recalcBound: vertex bound grown by BOX_MIN = 1e-5 in double."""
+    v = mesh.verts[mesh.tris.reshape(-1)].astype(np.float32)
+    lo = (v.min(0).astype(np.float64) - 0.00001).astype(np.float32)
+    hi = (v.max(0).astype(np.float64) + 0.00001).astype(np.float32)
+    return np.concatenate([lo, hi]).astype(np.float32)
+
+
+def product_object_tree(sc: scenes.Scene) -> np.ndarray:
+    """(n, 8) float32 records bmin[3], left(int bits), bmax[3], right(int bits)."""
+    lib = abi.load()
+    b = np.ascontiguousarray(np.stack([mesh_bound(m) for m in sc.meshes]), np.float32)
+    n = len(sc.meshes)
+    out = (abi.YrObjectNode * (2 * n - 1))()
+    nout = C.c_uint32()
+    st = lib.yr_object_tree_build(b.ctypes.data_as(C.POINTER(C.c_float)), n, out, C.byref(nout))
+    abi.check(st, "yr_object_tree_build")
+    return np.frombuffer(bytes(out), np.float32).reshape(-1, 8)[: nout.value].copy()
+
+
+# ------------------------------------------------------------------ oracle
+class OracleScene:
+    """The oracle loaded with a scene and the given (or product-built) trees."""
+
+    def __init__(self, sc: scenes.Scene, trees=None, otree=None):
+        self.sc = sc
+        fd, self.path = tempfile.mkstemp(suffix=".yrs")
+        os.close(fd)
+        scenes.write_yrs(sc, self.path)
+        self.lib = oracle()
+        self.h = self.lib.orc_load(self.path.encode())
+        assert self.h, "oracle could not load the scene"
+        trees = trees if trees is not None else [product_tree(m) for m in sc.meshes]
+        self._keep = []
+        for i, (m, t) in enumerate(zip(sc.meshes, trees)):
+            nodes = np.ascontiguousarray(t["nodes"], np.uint32)
+            prims = np.ascontiguousarray(t["prims"], np.uint32) if len(t["prims"]) else np.zeros(1, np.uint32)
+            tb = np.ascontiguousarray(t["tb"], np.float32)
+            ob = mesh_bound(m)
+            self._keep += [nodes, prims, tb, ob]
+            self.lib.orc_set_tree(self.h, i, ptr(nodes), nodes.shape[0], ptr(prims), len(t["prims"]), ptr(tb), ptr(ob))
+        ot = otree if otree is not None else product_object_tree(sc)
+        ot = np.ascontiguousarray(ot, np.float32)
+        self._keep.append(ot)
+        self.lib.orc_set_object_tree(self.h, ptr(ot), ot.shape[0])
+
+    def close(self):
+        if self.h:
+            self.lib.orc_free(self.h)
+            self.h = None
+        if os.path.exists(self.path):
+            os.unlink(self.path)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def trace_closest(self, rays: np.ndarray, shadow_only=False) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.zeros((rays.shape[0], 4), np.uint32)
+        self.lib.orc_trace_closest(self.h, ptr(rays), rays.shape[0], ptr(hits), int(shadow_only))
+        return hits
+
+    def trace_shadow(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        occ = np.zeros(rays.shape[0], np.uint8)
+        self.lib.orc_trace_shadow(self.h, ptr(rays), rays.shape[0], ptr(occ))
+        return occ
+
+    def kd(self, obj, frm, d, dist, any_hit):
+        out = np.zeros(4, np.uint32)
+        f = np.ascontiguousarray(frm, np.float32)
+        dd = np.ascontiguousarray(d, np.float32)
+        self.lib.orc_kd(self.h, obj, ptr(f), ptr(dd), float(dist), int(any_hit), ptr(out))
+        return out
+
+    def render(self, x0=0, x1=None, y0=0, y1=None):
+        sc = self.sc
+        x1 = sc.resx if x1 is None else x1
+        y1 = sc.resy if y1 is None else y1
+        img = np.zeros((sc.resy, sc.resx, 4), np.float32)
+        stats = np.zeros(5, np.uint64)
+        self.lib.orc_render(self.h, ptr(img), x0, x1, y0, y1, ptr(stats))
+        return img, stats
+
+    def camera_rays(self):
+        d = np.zeros((self.sc.resy, self.sc.resx, 3), np.float32)
+        self.lib.orc_camera_rays(self.h, ptr(d))
+        return d
+
+
+# ----------------------------------------------------------------- harness
+def run_harness(*args, timeout=600):
+    r = subprocess.run([HARNESS] + [str(a) for a in args], capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"harness {args[0]} failed: {r.stderr[-2000:]}")
+    return r.stdout
+
+
+def harness_trees(sc: scenes.Scene):
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "t.bin")
+        scenes.write_yrs(sc, sp)
+        run_harness("tree", sp, op)
+        data = open(op, "rb").read()
+    off = 0
+    n, = struct.unpack_from("<I", data, off)
+    off += 4
+    trees = []
+    for _ in range(n):
+        nn, npr = struct.unpack_from("<2I", data, off)
+        off += 8
+        tb = np.frombuffer(data, np.float32, 6, off).copy()
+        off += 24
+        md, ml = struct.unpack_from("<2i", data, off)
+        off += 8
+        cr, eb = struct.unpack_from("<2f", data, off)
+        off += 8
+        ob = np.frombuffer(data, np.float32, 6, off).copy()
+        off += 24
+        nodes = np.frombuffer(data, np.uint32, 2 * nn, off).reshape(nn, 2).copy()
+        off += 8 * nn
+        prims = np.frombuffer(data, np.uint32, npr, off).copy()
+        off += 4 * npr
+        trees.append(dict(nodes=nodes, prims=prims, tb=tb, max_depth=md, max_leaf=ml, cost_ratio=np.float32(cr),
+                          ob=ob))
+    nn, = struct.unpack_from("<I", data, off)
+    off += 4
+    raw = np.frombuffer(data, np.float32, 8 * nn, off).reshape(nn, 8)
+    # harness record: bmin[3], bmax[3], left, right -> yr_object_node order
+    otree = np.ascontiguousarray(raw[:, [0, 1, 2, 6, 3, 4, 5, 7]])
+    return trees, otree
+
+
+RAY_REC = np.dtype([("mode", "<u4"), ("object", "<u4"), ("frm", "<f4", 3), ("dir", "<f4", 3), ("dist", "<f4"),
+                    ("l", "<f4", 3)])
+
+
+def harness_rays(sc: scenes.Scene, recs: np.ndarray) -> np.ndarray:
+    """Run ray records (RAY_REC) through the reference; returns (n,4) uint32."""
+    with tempfile.TemporaryDirectory() as d:
+        sp, rp, op = os.path.join(d, "s.yrs"), os.path.join(d, "r.bin"), os.path.join(d, "o.bin")
+        scenes.write_yrs(sc, sp)
+        with open(rp, "wb") as f:
+            f.write(struct.pack("<I", recs.shape[0]))
+            f.write(np.ascontiguousarray(recs, RAY_REC).tobytes())
+        run_harness("rays", sp, rp, op)
+        return np.fromfile(op, np.uint32).reshape(-1, 4)
+
+
+def harness_render(sc: scenes.Scene, threads=1, crop=None):
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "o.bin")
+        scenes.write_yrs(sc, sp)
+        args = ["render", sp, op, threads] + (list(crop) if crop else [])
+        out = run_harness(*args)
+        img = np.fromfile(op, np.float32).reshape(sc.resy, sc.resx, 4)
+    import json
+    return img, json.loads(out.strip().splitlines()[-1])
+
+
+def harness_camera(sc: scenes.Scene) -> np.ndarray:
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "o.bin")
+        scenes.write_yrs(sc, sp)
+        run_harness("camera", sp, op)
+        return np.fromfile(op, np.float32).reshape(sc.resy, sc.resx, 3)
+
+
+# ------------------------------------------------------------------- rays
+def random_rays(sc: scenes.Scene, n: int, seed: int, spread=1.0) -> np.ndarray:
+    """Rays from around the camera / scene towards random scene points,
+    as yr_ray records (n, 8) float32."""
+    rng = np.random.default_rng(seed)
+    allv = np.concatenate([m.verts for m in sc.meshes])
+    lo, hi = allv.min(0), allv.max(0)
+    c = (lo + hi) / 2
+    ext = (hi - lo) / 2 * 1.2
+    org = c + rng.uniform(-1, 1, (n, 3)) * ext * spread
+    tgt = c + rng.uniform(-1, 1, (n, 3)) * ext * 0.5
+    d = tgt - org
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = org
+    rays[:, 3] = -1.0
+    rays[:, 4:7] = d
+    return rays

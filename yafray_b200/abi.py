@@ -42,6 +42,10 @@ class YrKdTree(C.Structure):
     ]
 
 
+class YrObjectNode(C.Structure):
+    _fields_ = [("bmin", f3), ("left", C.c_int32), ("bmax", f3), ("right", C.c_int32)]
+
+
 class YrCameraDesc(C.Structure):
     _fields_ = [("pos", f3), ("look", f3), ("up", f3), ("resx", C.c_int32), ("resy", C.c_int32),
                 ("aspect", C.c_float), ("focal", C.c_float)]
@@ -127,6 +131,8 @@ SIGNATURES = {
     "yr_kdtree_build": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32,
                                   C.POINTER(C.POINTER(YrKdTree))]),
     "yr_kdtree_free": (None, [C.POINTER(YrKdTree)]),
+    "yr_object_tree_build": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(YrObjectNode),
+                                       C.POINTER(C.c_uint32)]),
     "yr_scene_create": (C.c_int, [C.POINTER(YrSceneDesc), C.c_int, C.POINTER(_P)]),
     "yr_scene_destroy": (C.c_int, [_P]),
     "yr_scene_info_get": (C.c_int, [_P, C.POINTER(YrSceneInfo)]),

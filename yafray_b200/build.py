@@ -27,7 +27,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC
 def _compile(src: str) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(
-            [os.path.getmtime(src)] + [os.path.getmtime(h) for h in glob.glob(os.path.join(CSRC, "*.h*"))]
+            [os.path.getmtime(src)] + [os.path.getmtime(h) for h in glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))]
             + [os.path.getmtime(os.path.join(HERE, "..", "include", "yr.h"))]):
         return obj
     cmd = [NVCC] + ARCH + COMMON + ["-c", src, "-o", obj]

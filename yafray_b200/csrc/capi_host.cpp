@@ -1,6 +1,7 @@
 // Host-only entry points of the C ABI (no CUDA calls).
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "host_build.h"
 
@@ -58,6 +59,25 @@ YR_API yr_status yr_kdtree_build(const float *verts, uint32_t nverts, const uint
     r->cost_ratio = t.cost_ratio;
     r->empty_bonus = t.empty_bonus;
     *out = r;
+    return YR_OK;
+}
+
+YR_API yr_status yr_object_tree_build(const float *bounds, uint32_t n, yr_object_node *out, uint32_t *nout) {
+    if (!bounds || !out || !nout || n == 0) return YR_ERR_INVALID_ARG;
+    std::vector<yr::Box> b(n);
+    for (uint32_t i = 0; i < n; i++) {
+        std::memcpy(b[i].a, bounds + 6 * (size_t)i, 12);
+        std::memcpy(b[i].g, bounds + 6 * (size_t)i + 3, 12);
+    }
+    std::vector<yr::ObjNode> t;
+    try {
+        yr::build_object_tree(b, t);
+    } catch (const std::bad_alloc &) {
+        return YR_ERR_OUT_OF_MEMORY;
+    }
+    static_assert(sizeof(yr::ObjNode) == sizeof(yr_object_node), "object node layout");
+    std::memcpy(out, t.data(), sizeof(yr_object_node) * t.size());
+    *nout = (uint32_t)t.size();
     return YR_OK;
 }
 

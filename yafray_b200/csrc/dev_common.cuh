@@ -1,0 +1,123 @@
+// Device data layout and exact-rounding vector helpers.
+//
+// All single-precision arithmetic on the parity path is written operation
+// by operation in the order the reference evaluates it (x86-64 SSE, no FMA
+// contraction; the library is compiled with --fmad=false).  Where the
+// shipped reference build (-O3 -ffast-math) evaluates an expression in a
+// different but fixed form, that form is used and marked "fast-math".
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/yr.h"
+
+namespace yr {
+
+constexpr float kMinRayDist = 0.00005f;     // MIN_RAYDIST (configio.py:8-11)
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr int kMaxKdStack = 64;             // MAX_STACK (kdtree.cc:603)
+constexpr int kMaxObjStack = 64;
+constexpr uint32_t kMaxLeafVisits = 1u << 22;  // iteration cap per ray
+
+// device status word bits (first error wins; read back after each launch)
+enum DevError : int {
+    kDevOk = 0,
+    kDevIterationCap = YR_ERR_ITERATION_CAP,
+    kDevStackOverflow = YR_ERR_STACK_OVERFLOW,
+    kDevBadTree = YR_ERR_BAD_TREE,
+};
+
+struct V3 {
+    float x, y, z;
+};
+
+__host__ __device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__host__ __device__ __forceinline__ float comp(const V3 &v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+__host__ __device__ __forceinline__ V3 operator+(const V3 &a, const V3 &b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__host__ __device__ __forceinline__ V3 operator-(const V3 &a, const V3 &b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__host__ __device__ __forceinline__ V3 operator-(const V3 &a) { return V3{-a.x, -a.y, -a.z}; }
+// vector3d_t operator*(vector, PFLOAT f) returns (f*x, f*y, f*z) (vector3d.h:121-129)
+__host__ __device__ __forceinline__ V3 operator*(const V3 &a, float f) { return V3{f * a.x, f * a.y, f * a.z}; }
+__host__ __device__ __forceinline__ V3 operator*(float f, const V3 &a) { return V3{f * a.x, f * a.y, f * a.z}; }
+// dot product, left to right (vector3d.h:116-119)
+__host__ __device__ __forceinline__ float dot(const V3 &a, const V3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// cross product (vector3d.h:156-159)
+__host__ __device__ __forceinline__ V3 cross(const V3 &a, const V3 &b) {
+    return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+// vector3d_t::length: sqrt of the float sum (sqrtf after g++ narrows it)
+__device__ __forceinline__ float length(const V3 &a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+// vector3d_t::normalize (vector3d.h:207-217): 1/sqrt taken in double
+__device__ __forceinline__ V3 normalize(const V3 &a) {
+    float l = a.x * a.x + a.y * a.y + a.z * a.z;
+    if (l != 0.f) {
+        float k = (float)(1.0 / sqrt((double)l));
+        return V3{a.x * k, a.y * k, a.z * k};
+    }
+    return a;
+}
+// vector3d_t::normLenSqr (vector3d.h:60-68): normalizes, returns the squared length
+__device__ __forceinline__ float norm_len_sqr(V3 &a) {
+    float l = a.x * a.x + a.y * a.y + a.z * a.z;
+    if (l != 0.f) {
+        float k = (float)(1.0 / sqrt((double)l));
+        a.x *= k;
+        a.y *= k;
+        a.z *= k;
+    }
+    return l;
+}
+
+struct C3 {
+    float r, g, b;
+};
+__host__ __device__ __forceinline__ C3 c3(float r, float g, float b) { return C3{r, g, b}; }
+__host__ __device__ __forceinline__ C3 operator+(const C3 &a, const C3 &b) { return C3{a.r + b.r, a.g + b.g, a.b + b.b}; }
+__host__ __device__ __forceinline__ C3 operator-(const C3 &a, const C3 &b) { return C3{a.r - b.r, a.g - b.g, a.b - b.b}; }
+__host__ __device__ __forceinline__ C3 operator*(const C3 &a, const C3 &b) { return C3{a.r * b.r, a.g * b.g, a.b * b.b}; }
+// color_t * CFLOAT (color.h)
+__host__ __device__ __forceinline__ C3 operator*(const C3 &a, float f) { return C3{a.r * f, a.g * f, a.b * f}; }
+__host__ __device__ __forceinline__ C3 operator*(float f, const C3 &a) { return C3{f * a.r, f * a.g, f * a.b}; }
+__host__ __device__ __forceinline__ C3 operator/(const C3 &a, float f) { return C3{a.r / f, a.g / f, a.b / f}; }
+// color_t::energy (color.h:67)
+__host__ __device__ __forceinline__ float energy(const C3 &c) { return (c.r + c.g + c.b) * 0.333333f; }
+
+// ----------------------------------------------------------------- layout
+// kd node: x = word (split bits / triangle / prim offset), y = flags.
+// Indices are global: right child and triangle / prim offsets already
+// include the owning object's base.
+struct DevObject {
+    float tb[6];        // kdTree_t::treeBound (min xyz, max xyz)
+    uint32_t root;      // global index of the root kd node
+    uint32_t tri_base;  // first global triangle index
+    uint32_t ntris;
+    uint32_t flags;     // bit0: casts shadows
+};
+
+struct DevObjNode {     // object tree (geomeTree_t), node 0 = root
+    float bmin[3];
+    int32_t left;       // -1 = leaf
+    float bmax[3];
+    int32_t right;      // child, or object index for a leaf
+};
+
+struct DevScene {
+    const float4 *tris;         // 3 per triangle: {a, N.x}, {b, N.y}, {c, N.z}
+    const uint2 *nodes;
+    const uint32_t *prims;
+    const DevObject *objects;
+    const DevObjNode *otree;
+    uint32_t nobjects;
+    uint32_t ntris;
+    uint32_t nnodes;
+    uint32_t nprims;
+    uint32_t notree;
+    int32_t kd_stack;           // stack entries needed (max tree depth + 3, <= 64)
+    int *status;                // device status word
+};
+
+__device__ __forceinline__ void dev_fail(int *status, int code) {
+    if (status) atomicCAS(status, 0, code);
+}
+
+}  // namespace yr

@@ -1,0 +1,251 @@
+// Shading on the device: explicit-index Halton QMC with per-pixel
+// Cranley-Patterson rotation, improved Perlin noise / fBm / turbulence,
+// genericShader_t with its texture modulator, and the per-sample parts of
+// the point, area, hemi and path lights.
+#pragma once
+#include "dev_common.cuh"
+#include "scene.h"
+
+namespace yr {
+
+// ------------------------------------------------------------------ QMC
+// Halton::setStart(n) followed by Halton::getNext() (mcqmc.h:24-49), i.e.
+// the radical inverse of n+1, as the shipped build evaluates it
+// (fast-math: r = (1 - 1e-10) - value, value = (hh + h) + (value - 1)).
+__device__ __forceinline__ float halton(uint32_t base, uint32_t n) {
+    const double inv = 1.0 / (double)base;
+    double value = 0.0, factor = inv;
+    uint32_t i = n;
+    while (i > 0) {
+        value += (double)(i % base) * factor;
+        i /= base;
+        factor *= inv;
+    }
+    const double r = (1.0 - 0.0000000001) - value;
+    if (inv < r) {
+        value = value + inv;
+    } else {
+        double hh, h = inv;
+        do {
+            hh = h;
+            h *= inv;
+        } while (h >= r);
+        value = (hh + h) + (value - 1.0);
+    }
+    return (float)value;
+}
+
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// Cranley-Patterson rotation offset of (pixel, dimension) in [0,1).
+__host__ __device__ __forceinline__ float cp_rot(uint32_t seed, uint32_t pixel, uint32_t dim) {
+    uint32_t h = fmix32(seed * 0x9e3779b9u + 0x632be5abu);
+    h = fmix32(h ^ (pixel * 0x85ebca77u));
+    h = fmix32(h ^ (dim * 0xc2b2ae3du + 0x27d4eb2fu));
+    return (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+
+__host__ __device__ __forceinline__ float cp_add(float v, float r) {
+    float u = v + r;
+    if (u >= 1.0f) u -= 1.0f;
+    return u;
+}
+
+__device__ __constant__ uint32_t kPrimes[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+
+// QMC dimensions: path level l uses dims (2l, 2l+1) with the l-th pair of
+// primes (pathtools.cc:9-19); light k at vertex v uses dims 64+16k+2v (+1)
+// with bases 2 and 3.
+__device__ __forceinline__ uint32_t light_dim(int k, int v) { return 64u + 16u * (uint32_t)k + 2u * (uint32_t)v; }
+
+// ---------------------------------------------------------------- noise
+// The 256-entry permutation of Blender's noise (the first half of hash[512]
+// in noise.cc:118-127; the second half repeats it), indexed modulo 256.
+__device__ const uint8_t kPerm[256] = {
+    162, 160,  25,  59, 248, 235, 170, 238, 243,  28, 103,  40,  29, 237,   0, 222,
+    149,  46, 220,  63,  58, 130,  53,  77, 108, 186,  54, 208, 246,  12, 121,  50,
+    209,  89, 244,   8, 139,  99, 137,  47, 184, 180, 151, 131, 242, 143,  24, 199,
+     81,  20, 101, 135,  72,  32,  66, 168, 128, 181,  64,  19, 178,  34, 126,  87,
+    188, 127, 107, 157, 134,  76, 200, 219, 124, 213,  37,  78,  90,  85, 116,  80,
+    205, 179, 122, 187, 195, 203, 182, 226, 228, 236, 253, 152,  11, 150, 211, 158,
+     92, 161, 100, 241, 129,  97, 225, 196,  36, 114,  73, 140, 144,  75, 132,  52,
+     56, 171, 120, 202,  31,   1, 215, 147,  17, 193,  88, 169,  49, 249,  68, 109,
+    191,  51, 156,  95,   9, 148, 163, 133,   6, 198, 154,  30, 123,  70,  21,  48,
+     39,  43,  27, 113,  60,  91, 214, 111,  98, 172,  79, 194, 192,  14, 177,  35,
+    167, 223,  71, 176, 119, 105,   5, 233, 230, 231, 118, 115,  15, 254, 110, 155,
+     86, 239,  18, 165,  55, 252, 174, 217,   3, 142, 221,  16, 185, 206, 201, 141,
+    218,  42, 189, 104,  23, 159, 190, 212,  10, 204, 210, 232,  67,  61, 112, 183,
+      2, 125, 153, 216,  13,  96, 138,   4,  44,  62, 146, 229, 175,  83,   7, 224,
+     41, 166, 197, 227, 245, 247,  74,  65,  38, 106,  22,  94,  82,  45,  33, 173,
+    240, 145, 255, 234,  84, 250, 102,  26,  69,  57, 207, 117, 164, 136, 251,  93,};
+
+__device__ __forceinline__ int perm(int i) { return (int)__ldg(&kPerm[i & 255]); }
+
+__device__ __forceinline__ float nfade(float t) { return t * t * t * (t * (t * 6 - 15) + 10); }
+__device__ __forceinline__ float nlerp(float t, float a, float b) { return a + t * (b - a); }
+__device__ __forceinline__ float ngrad(int hash, float x, float y, float z) {
+    const int h = hash & 15;
+    const float u = h < 8 ? x : y, v = h < 4 ? y : (h == 12 || h == 14 ? x : z);
+    return ((h & 1) == 0 ? u : -u) + ((h & 2) == 0 ? v : -v);
+}
+
+// newPerlin_t::operator() (noise.cc:161-183): improved Perlin noise in [0,1]
+__device__ __forceinline__ float perlin(const V3 &pt) {
+    float x = pt.x, y = pt.y, z = pt.z;
+    float u = floorf(x), v = floorf(y), w = floorf(z);
+    const int X = ((int)u) & 255, Y = ((int)v) & 255, Z = ((int)w) & 255;
+    x -= u;
+    y -= v;
+    z -= w;
+    u = nfade(x);
+    v = nfade(y);
+    w = nfade(z);
+    const int A = perm(X) + Y, AA = perm(A) + Z, AB = perm(A + 1) + Z;
+    const int B = perm(X + 1) + Y, BA = perm(B) + Z, BB = perm(B + 1) + Z;
+    const float nv =
+        nlerp(w,
+              nlerp(v, nlerp(u, ngrad(perm(AA), x, y, z), ngrad(perm(BA), x - 1, y, z)),
+                    nlerp(u, ngrad(perm(AB), x, y - 1, z), ngrad(perm(BB), x - 1, y - 1, z))),
+              nlerp(v, nlerp(u, ngrad(perm(AA + 1), x, y, z - 1), ngrad(perm(BA + 1), x - 1, y, z - 1)),
+                    nlerp(u, ngrad(perm(AB + 1), x, y - 1, z - 1), ngrad(perm(BB + 1), x - 1, y - 1, z - 1))));
+    return (float)(0.5 + 0.5 * (double)nv);
+}
+
+// fBm_t::operator() (noise.cc:638-650) over newPerlin with getSignedNoise
+// (noise.h:245-248).  pwHL = lacunarity^-H.
+__device__ __forceinline__ float fbm(V3 tp, float H, float lacunarity, float octaves) {
+    float value = 0, pwr = 1;
+    const float pwHL = (float)pow((double)lacunarity, (double)-H);
+    for (int i = 0; i < (int)octaves; i++) {
+        value += ((float)2.0 * perlin(tp) - (float)1.0) * pwr;
+        pwr *= pwHL;
+        tp = V3{tp.x * lacunarity, tp.y * lacunarity, tp.z * lacunarity};
+    }
+    const float rmd = octaves - floorf(octaves);
+    if (rmd != 0.f) value += rmd * ((float)2.0 * perlin(tp) - (float)1.0) * pwr;
+    return value;
+}
+
+// turbulence (noise.cc:808-819), newPerlin (no offset)
+__device__ __forceinline__ float turbulence(const V3 &pt, int oct, float size, bool hard) {
+    float amp = 1, sum = 0;
+    V3 tp = V3{pt.x * size, pt.y * size, pt.z * size};
+    for (int i = 0; i <= oct; i++, amp *= 0.5f, tp = V3{tp.x * 2.0f, tp.y * 2.0f, tp.z * 2.0f}) {
+        float val = perlin(tp);
+        if (hard) val = (float)fabs(2.0 * (double)val - 1.0);
+        sum += amp * val;
+    }
+    return sum * ((float)(1 << oct) / (float)((1 << (oct + 1)) - 1));
+}
+
+// --------------------------------------------------------------- shading
+struct Surf {
+    V3 P, N, Ng, NU, NV;
+    int object;
+    int shader;
+    float Z;
+};
+
+// createCS (vector3d.h:240-258)
+__device__ __forceinline__ void create_cs(const V3 &N, V3 &u, V3 &v) {
+    if ((N.x == 0.f) && (N.y == 0.f)) {
+        u = (N.z < 0.f) ? v3(-1.f, 0.f, 0.f) : v3(1.f, 0.f, 0.f);
+        v = v3(0.f, 1.f, 0.f);
+    } else {
+        const float d = (float)(1.0 / sqrt((double)(N.y * N.y + N.x * N.x)));
+        u = v3(N.y * d, -N.x * d, 0.f);
+        v = cross(N, u);
+    }
+}
+
+// FACE_FORWARD(Ng, N, I) (shader.h:157)
+__device__ __forceinline__ V3 face_forward(const V3 &Ng, const V3 &N, const V3 &I) {
+    return (dot(Ng, I) < 0.f) ? -N : N;
+}
+
+// reflect (vector3d.h:221-226)
+__device__ __forceinline__ V3 reflect(const V3 &n, const V3 &v) {
+    const float vn = dot(v, n);
+    if (vn < 0.f) return -v;
+    return (2 * vn) * n - v;
+}
+
+// meshObject_t::shoot + triangle_t::getSurface for a flat triangle
+// (mesh.cc:570-576, triangle.cc:138-141): P = from + Z*ray, N = Ng.
+__device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender &R, int object, uint32_t tri,
+                                             float Z, const V3 &from, const V3 &ray) {
+    Surf s;
+    s.P = from + Z * ray;
+    const float4 p = __ldg(S.tris + 3 * (size_t)tri), q = __ldg(S.tris + 3 * (size_t)tri + 1),
+                 r = __ldg(S.tris + 3 * (size_t)tri + 2);
+    s.N = v3(p.w, q.w, r.w);
+    s.Ng = s.N;
+    create_cs(s.N, s.NU, s.NV);
+    s.object = object;
+    s.shader = (int)__ldg(R.tri_shader + tri);
+    s.Z = Z;
+    return s;
+}
+
+// modulator_t::modulate (texture.cc:499-534) in "mix" mode with procedural
+// texture coordinates size*(P + ofs) (texture.cc:307-312), applied to the
+// diffuse colour only.
+__device__ __forceinline__ C3 modulated_color(const DevShader &sh, const V3 &P) {
+    C3 C = sh.color;
+    if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f)) return C;
+    const V3 tp = v3(sh.msize[0] * (P.x + sh.mofs[0]), sh.msize[1] * (P.y + sh.mofs[1]), sh.msize[2] * (P.z + sh.mofs[2]));
+    float f;
+    if (sh.tex_type == YR_TEX_MUSGRAVE_FBM)  // textureMusgrave_t::getFloat (basictex.cc:677-680)
+        f = sh.intensity * fbm(V3{tp.x * sh.tsize, tp.y * sh.tsize, tp.z * sh.tsize}, sh.H, sh.lacunarity, sh.octaves);
+    else  // textureClouds_t::getFloat (basictex.cc:83-91), no bias
+        f = turbulence(tp, sh.tdepth, sh.tsize, sh.thard != 0);
+    const C3 tex = sh.tc1 + f * (sh.tc2 - sh.tc1);
+    // mix(texcolor, C, w) (color.cc:103-109)
+    const float w = sh.mod_color;
+    if (w > 1.0f) return tex;
+    return tex * w + (1 - w) * C;
+}
+
+// genericShader_t::fromLight (basicshaders.cc:46-70) with edif = 1.
+// `lkc` is the (modulated) diffuse colour.
+__device__ __forceinline__ C3 from_light(const DevShader &sh, const C3 &lkc, const Surf &sp, const V3 &ldir,
+                                         const C3 &lcol, const V3 &eye) {
+    V3 edir = normalize(eye);
+    const V3 N = face_forward(sp.Ng, sp.N, edir);
+    const float inte = dot(N, ldir);
+    if (inte < 0.f) return c3(0.f, 0.f, 0.f);
+    edir = reflect(N, edir);
+    float refle = dot(edir, ldir);
+    if (refle < 0.f) refle = 0.f;
+    else refle = (float)pow((double)refle, (double)sh.hard);
+    const C3 edif_inte = c3(1.f * inte, 1.f * inte, 1.f * inte);
+    return ((edif_inte * lcol) * lkc) + (sh.specular * refle) * lcol;
+}
+
+// haltonSampler_t::nextDirection (pathtools.cc:32-43) for explicit z1, z2
+// in [0,1): cosine-weighted direction around N.
+__device__ __forceinline__ V3 cos_hemi_dir(const V3 &N, const V3 &Ru, const V3 &Rv, float z1, float z2) {
+    if (z1 > 1.0f) z1 = 1.0f;
+    z2 = (float)((double)z2 * 6.283185307179586);
+    const float c = (float)cos((double)z2), s = (float)sin((double)z2);
+    const float s1 = (float)sqrt(1.0 - (double)z1);
+    const float s2 = sqrtf(z1);
+    return (Ru * c + Rv * s) * s1 + N * s2;
+}
+
+// hemiLight_t::getNext (hemilight.cc:103-114): uniform direction
+__device__ __forceinline__ V3 uni_hemi_dir(const V3 &N, const V3 &Ru, const V3 &Rv, float z1, float z2) {
+    z2 = (float)((double)z2 * 6.283185307179586);
+    const float c = (float)cos((double)z2), s = (float)sin((double)z2);
+    const float s1 = (float)sqrt(1.0 - (double)(z1 * z1));
+    return (Ru * c + Rv * s) * s1 + N * z1;
+}
+
+}  // namespace yr

@@ -1,0 +1,387 @@
+// Ray queries on the device: slab test, kd-tree traversal (closest and any
+// hit), triangle test, and the front-to-back object-tree iterator.
+//
+// Each function restates one reference routine; the traversal order, the
+// comparisons (strict vs non-strict) and the float expressions are the
+// reference's, so a ray visits the same nodes and reports the same triangle
+// as kdTree_t::Intersect / IntersectS on the same tree.
+#pragma once
+#include "dev_common.cuh"
+
+namespace yr {
+
+// bound_t::cross(from, ray, enter, leave, dist) (bound.cc:389-436) as the
+// shipped build evaluates it (fast-math: (g - from)/ray instead of
+// ((g - a) - (from - a))/ray).
+__device__ __forceinline__ bool box_enter_leave(const float *bmin, const float *bmax, const V3 &from,
+                                                const V3 &ray, float dist, float &enter, float &leave) {
+    float lmin = -1.f, lmax = -1.f;
+    if (ray.x != 0.f) {
+        float t1 = (bmin[0] - from.x) / ray.x, t2 = (bmax[0] - from.x) / ray.x;
+        if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+        lmin = t1;
+        lmax = t2;
+        if ((lmax < 0.f) || (lmin > dist)) return false;
+    }
+    if (ray.y != 0.f) {
+        float t1 = (bmin[1] - from.y) / ray.y, t2 = (bmax[1] - from.y) / ray.y;
+        if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+        if (t1 > lmin) lmin = t1;
+        if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;
+        if ((lmax < 0.f) || (lmin > dist)) return false;
+    }
+    if (ray.z != 0.f) {
+        float t1 = (bmin[2] - from.z) / ray.z, t2 = (bmax[2] - from.z) / ray.z;
+        if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+        if (t1 > lmin) lmin = t1;
+        if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;
+    }
+    if ((lmin <= lmax) && (lmax >= 0.f) && (lmin <= dist)) {
+        enter = lmin;
+        leave = lmax;
+        return true;
+    }
+    return false;
+}
+
+// bound_t::cross(from, ray, where, dist) (bound.cc:340-387): where = max(enter, 0)
+__device__ __forceinline__ bool box_where(const float *bmin, const float *bmax, const V3 &from, const V3 &ray,
+                                          float dist, float &where) {
+    float e, l;
+    if (!box_enter_leave(bmin, bmax, from, ray, dist, e, l)) return false;
+    where = (e > 0.f) ? e : 0.f;
+    return true;
+}
+
+struct Tri {
+    V3 a, b, c, n;
+};
+
+// 3 x 128-bit read-only loads per triangle
+__device__ __forceinline__ Tri load_tri(const float4 *tris, uint32_t i) {
+    const float4 p = __ldg(tris + 3 * (size_t)i);
+    const float4 q = __ldg(tris + 3 * (size_t)i + 1);
+    const float4 r = __ldg(tris + 3 * (size_t)i + 2);
+    Tri t;
+    t.a = v3(p.x, p.y, p.z);
+    t.b = v3(q.x, q.y, q.z);
+    t.c = v3(r.x, r.y, r.z);
+    t.n = v3(p.w, q.w, r.w);
+    return t;
+}
+
+// triangle_t::hit (triangle.h:48-58): edge signs, no epsilon.  Returns the
+// hit distance triangle_t::intersect (triangle.h:83-86) through `t`.
+__device__ __forceinline__ bool tri_hit(const Tri &tr, const V3 &from, const V3 &ray, float &t) {
+    const V3 va = tr.a - from, vb = tr.b - from, vc = tr.c - from;
+    const float rn = dot(ray, tr.n);
+    const V3 r = (rn < 0.f) ? -ray : ray;
+    if (dot(cross(va, vb), r) < 0.f) return false;
+    if (dot(cross(vb, vc), r) < 0.f) return false;
+    if (dot(cross(vc, va), r) < 0.f) return false;
+    t = dot(tr.n, va) / rn;
+    return true;
+}
+
+// Per-thread kd stack entry: far child, signed distance of the exit point,
+// the split plane that produced it, and the link to the previous exit.  The
+// exit point's coordinates are recomputed from (t, split, axis) exactly as
+// they were first computed, so 16 bytes replace KdStack's 24.
+struct KdStack {
+    uint4 *e;     // entries, strided by `stride` (one column per thread)
+    int stride;
+    int cap;
+    __device__ __forceinline__ uint4 &at(int i) const { return e[(size_t)i * stride]; }
+};
+
+__device__ __forceinline__ void exit_point(const uint4 &en, const V3 &from, const V3 &ray, float *pb) {
+    const float t = __uint_as_float(en.y);
+    const int axis = (int)((en.w >> 8) & 3u);
+    if (axis == 3) {  // initial exit: from + ray*t on every axis
+        pb[0] = from.x + t * ray.x;
+        pb[1] = from.y + t * ray.y;
+        pb[2] = from.z + t * ray.z;
+    } else {
+        const int na = axis == 2 ? 0 : axis + 1, pa = axis == 0 ? 2 : axis - 1;
+        pb[axis] = __uint_as_float(en.z);
+        pb[na] = comp(from, na) + t * comp(ray, na);
+        pb[pa] = comp(from, pa) + t * comp(ray, pa);
+    }
+}
+
+struct KdResult {
+    uint32_t tri;
+    uint32_t nodes;   // interior + leaf nodes visited
+    uint32_t tests;   // triangle tests
+};
+
+// kdTree_t::Intersect (kdtree.cc:591-727, ANY=false) and IntersectS
+// (kdtree.cc:730-866, ANY=true).  Z is in/out (closest hit only).
+template <bool ANY>
+__device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V3 &from, const V3 &ray, float dist,
+                         float &Z, KdResult &res, const KdStack &stk) {
+    float a, b;
+    if (!box_enter_leave(obj.tb, obj.tb + 3, from, ray, dist, a, b)) return false;
+    // 1.0/ray in double narrowed to float == 1.f/ray (both correctly rounded)
+    const float inv[3] = {1.f / ray.x, 1.f / ray.y, 1.f / ray.z};
+    const float fr[3] = {from.x, from.y, from.z};
+    const float rr[3] = {ray.x, ray.y, ray.z};
+    bool hit = false;
+    uint32_t curr = obj.root;
+    int en = 0, ex = 1;
+    float en_t = a, en_pb[3];
+    if (a >= 0.f) {
+        en_pb[0] = fr[0] + a * rr[0];
+        en_pb[1] = fr[1] + a * rr[1];
+        en_pb[2] = fr[2] + a * rr[2];
+    } else {
+        en_pb[0] = fr[0];
+        en_pb[1] = fr[1];
+        en_pb[2] = fr[2];
+    }
+    float ex_t = b, ex_pb[3];
+    ex_pb[0] = fr[0] + b * rr[0];
+    ex_pb[1] = fr[1] + b * rr[1];
+    ex_pb[2] = fr[2] + b * rr[2];
+    stk.at(1) = make_uint4(kNone, __float_as_uint(b), 0u, (3u << 8));
+    uint32_t leaves = 0;
+    while (curr != kNone) {
+        if (dist < en_t) break;
+        if (++leaves > kMaxLeafVisits) {
+            dev_fail(S.status, kDevIterationCap);
+            return false;
+        }
+        if (curr >= S.nnodes) {
+            dev_fail(S.status, kDevBadTree);
+            return false;
+        }
+        uint2 nd = __ldg(S.nodes + curr);
+        while ((nd.y & 3u) != 3u) {
+            res.nodes++;
+            const int axis = (int)(nd.y & 3u);
+            const float split = __uint_as_float(nd.x);
+            const uint32_t right = nd.y >> 2;
+            uint32_t far_child;
+            if (curr + 1 >= S.nnodes || right >= S.nnodes) {
+                dev_fail(S.status, kDevBadTree);
+                return false;
+            }
+            if (en_pb[axis] <= split) {
+                if (ex_pb[axis] <= split) {
+                    curr = curr + 1;
+                    nd = __ldg(S.nodes + curr);
+                    continue;
+                }
+                far_child = right;
+                curr = curr + 1;
+            } else {
+                if (split < ex_pb[axis]) {
+                    curr = right;
+                    nd = __ldg(S.nodes + curr);
+                    continue;
+                }
+                far_child = curr + 1;
+                curr = right;
+            }
+            const float t = (split - fr[axis]) * inv[axis];
+            const int tmp = ex;
+            ex++;
+            if (ex == en) ex++;
+            if (ex >= stk.cap) {
+                dev_fail(S.status, kDevStackOverflow);
+                return false;
+            }
+            stk.at(ex) = make_uint4(far_child, __float_as_uint(t), __float_as_uint(split),
+                                    (uint32_t)tmp | ((uint32_t)axis << 8));
+            const int na = axis == 2 ? 0 : axis + 1, pa = axis == 0 ? 2 : axis - 1;
+            ex_t = t;
+            ex_pb[axis] = split;
+            ex_pb[na] = fr[na] + t * rr[na];
+            ex_pb[pa] = fr[pa] + t * rr[pa];
+            nd = __ldg(S.nodes + curr);
+        }
+        res.nodes++;
+        // leaf
+        const uint32_t np = nd.y >> 2;
+        for (uint32_t k = 0; k < np; k++) {
+            const uint32_t ti = (np == 1) ? nd.x : __ldg(S.prims + nd.x + k);
+            if (ti >= S.ntris) {
+                dev_fail(S.status, kDevBadTree);
+                return false;
+            }
+            res.tests++;
+            const Tri tr = load_tri(S.tris, ti);
+            float rt;
+            if (tri_hit(tr, from, ray, rt)) {
+                if (ANY) {
+                    if (rt < dist && rt > 0.f) {
+                        res.tri = ti;
+                        return true;
+                    }
+                } else if (rt < Z && rt >= 0.f) {
+                    Z = rt;
+                    res.tri = ti;
+                    hit = true;
+                }
+            }
+        }
+        if (!ANY && hit && Z <= ex_t) return true;
+        // pop: the exit point becomes the entry point
+        en = ex;
+        en_t = ex_t;
+        en_pb[0] = ex_pb[0];
+        en_pb[1] = ex_pb[1];
+        en_pb[2] = ex_pb[2];
+        const uint4 top = stk.at(ex);
+        curr = top.x;
+        ex = (int)(top.w & 0xffu);
+        if (curr != kNone) {
+            const uint4 nx = stk.at(ex);
+            ex_t = __uint_as_float(nx.y);
+            exit_point(nx, from, ray, ex_pb);
+        }
+    }
+    return hit;
+}
+
+// geomeIterator_t (geometree.h:36-157) in its front-to-back mode: yields
+// objects whose bound the ray crosses before `maximun`, nearest entry first.
+struct ObjIter {
+    int2 st[kMaxObjStack];   // (node, bits of the entry distance)
+    int sp;
+    int current;             // object index or -1
+    float maximun;
+
+    __device__ __forceinline__ void down(const DevScene &S, int node, const V3 &from, const V3 &ray) {
+        for (;;) {
+            const DevObjNode nd = S.otree[node];
+            if (nd.left < 0) {
+                current = nd.right;
+                return;
+            }
+            const DevObjNode L = S.otree[nd.left], R = S.otree[nd.right];
+            float hl = __int_as_float(0x7f800000), hr = __int_as_float(0x7f800000);
+            const bool hitl = box_where(L.bmin, L.bmax, from, ray, maximun, hl);
+            const bool hitr = box_where(R.bmin, R.bmax, from, ray, maximun, hr);
+            if (!hitl && !hitr) {
+                if (sp == 0) {
+                    current = -1;
+                    return;
+                }
+                node = st[--sp].x;
+                continue;
+            }
+            if (sp >= kMaxObjStack) {
+                dev_fail(S.status, kDevStackOverflow);
+                current = -1;
+                return;
+            }
+            if (hl < hr) {
+                if (hitr) st[sp++] = make_int2(nd.right, __float_as_int(hr));
+                node = nd.left;
+            } else {
+                if (hitl) st[sp++] = make_int2(nd.left, __float_as_int(hl));
+                node = nd.right;
+            }
+        }
+    }
+
+    __device__ __forceinline__ void start(const DevScene &S, const V3 &from, const V3 &ray, float maxd) {
+        maximun = maxd;
+        sp = 0;
+        current = -1;
+        if (S.notree == 0) return;
+        const DevObjNode r = S.otree[0];
+        float w = 0.f;
+        if (box_where(r.bmin, r.bmax, from, ray, maximun, w)) down(S, 0, from, ray);
+    }
+
+    __device__ __forceinline__ void next(const DevScene &S, const V3 &from, const V3 &ray) {
+        current = -1;
+        while (sp > 0 && __int_as_float(st[sp - 1].y) > maximun) sp--;
+        if (sp > 0) {
+            const int node = st[--sp].x;
+            down(S, node, from, ray);
+        }
+    }
+
+    __device__ __forceinline__ void limit(float z) {
+        if (z < maximun) maximun = z;
+    }
+};
+
+struct SceneHit {
+    float t;
+    int object;       // -1 = miss
+    uint32_t tri;     // global triangle index
+    uint32_t nodes;
+    uint32_t tests;
+};
+
+// Closest hit over all objects.  `f` is the already offset origin.
+//   pass_limit = true : scene_t::raytrace (scene.cc:210-233) - each object
+//                       is shot with the current closest distance
+//   pass_limit = false: scene_t::firstHit (scene.cc:688-707)
+//   shadow_only: skip objects that do not cast shadows (firstHit's shadow arg)
+__device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V3 &ray, bool pass_limit, bool shadow_only,
+                                  const KdStack &stk) {
+    SceneHit best;
+    best.t = 0.f;
+    best.object = -1;
+    best.tri = kNone;
+    best.nodes = 0;
+    best.tests = 0;
+    const float inf = __int_as_float(0x7f800000);
+    float limit = inf;
+    ObjIter it;
+    it.start(S, f, ray, inf);
+    while (it.current >= 0) {
+        const int o = it.current;
+        const DevObject obj = S.objects[o];
+        if (!(shadow_only && !(obj.flags & 1u))) {
+            const float dis = pass_limit ? limit : inf;
+            float Z = dis;
+            KdResult r{kNone, 0, 0};
+            const bool h = kd_trace<false>(S, obj, f, ray, dis, Z, r, stk);
+            best.nodes += r.nodes;
+            best.tests += r.tests;
+            if (h && Z > 0.f) {
+                if (pass_limit) limit = Z;
+                it.limit(Z);
+                if (best.object < 0 || Z < best.t) {
+                    best.t = Z;
+                    best.object = o;
+                    best.tri = r.tri;
+                }
+            }
+        }
+        it.next(S, f, ray);
+    }
+    return best;
+}
+
+// scene_t::isShadowed (scene.cc:107-185).  p: shading point, own: its
+// object, ray: unit direction, dist: |l - p| (or infinity).
+__device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &ray, float dist, float self_bias,
+                               const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+    const V3 self = p + ray * self_bias;
+    const V3 p2 = p + ray * kMinRayDist;
+    ObjIter it;
+    it.start(S, p2, ray, dist);
+    while (it.current >= 0) {
+        const int o = it.current;
+        const DevObject obj = S.objects[o];
+        if (obj.flags & 1u) {
+            float Z = dist;
+            KdResult r{kNone, 0, 0};
+            const bool h = kd_trace<true>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
+            nodes += r.nodes;
+            tests += r.tests;
+            if (h) return true;
+        }
+        it.next(S, p2, ray);
+    }
+    return false;
+}
+
+}  // namespace yr

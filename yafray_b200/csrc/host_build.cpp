@@ -653,6 +653,11 @@ Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris) {
                 if (p[k] < b.a[k]) b.a[k] = p[k];
             }
         }
+    // grown by BOX_MIN = 0.00001 (mesh.cc:32, 373-379), in double
+    for (int k = 0; k < 3; k++) {
+        b.a[k] = (float)((double)b.a[k] - 0.00001);
+        b.g[k] = (float)((double)b.g[k] + 0.00001);
+    }
     return b;
 }
 

@@ -29,7 +29,8 @@ struct KdTree {
 yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris,
                        uint32_t ntris, KdTree &out);
 
-// meshObject_t::recalcBound (mesh.cc:343-374): bound of the triangles' vertices.
+// meshObject_t::recalcBound (mesh.cc:343-379): bound of the triangles'
+// vertices grown by BOX_MIN.
 Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris);
 
 // Flattened object tree node (geomeTree_t, geometree.h:8-32).

@@ -1,0 +1,467 @@
+// yr_scene_create / yr_scene_destroy: host flattening and device upload.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "scene.h"
+
+namespace yr {
+namespace {
+
+V3 hv(const float *p) { return V3{p[0], p[1], p[2]}; }
+
+// vector3d_t::normalize on the host (1/sqrt in double, vector3d.h:207-217)
+V3 h_normalize(V3 a) {
+    float l = a.x * a.x + a.y * a.y + a.z * a.z;
+    if (l != 0.f) {
+        float k = (float)(1.0 / std::sqrt((double)l));
+        a.x *= k;
+        a.y *= k;
+        a.z *= k;
+    }
+    return a;
+}
+float h_length(const V3 &a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+V3 h_div(const V3 &a, float f) { return V3{a.x / f, a.y / f, a.z / f}; }
+
+template <class T>
+yr_status dev_upload(yr_scene *s, const T *host, size_t count, T **out) {
+    *out = nullptr;
+    if (count == 0) return YR_OK;
+    DevBuf b;
+    b.bytes = sizeof(T) * count;
+    if (cudaMalloc(&b.p, b.bytes) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
+    s->bufs.push_back(b);
+    if (cudaMemcpy(b.p, host, b.bytes, cudaMemcpyHostToDevice) != cudaSuccess) return YR_ERR_CUDA;
+    *out = (T *)b.p;
+    return YR_OK;
+}
+
+}  // namespace
+
+void make_shader(const yr_shader_desc &d, DevShader &o) {
+    o.color = c3(d.color[0], d.color[1], d.color[2]);
+    o.specular = c3(d.specular[0], d.specular[1], d.specular[2]);
+    o.hard = d.hard;
+    o.tex_type = (int)d.tex_type;
+    o.tc1 = c3(d.tex_color1[0], d.tex_color1[1], d.tex_color1[2]);
+    o.tc2 = c3(d.tex_color2[0], d.tex_color2[1], d.tex_color2[2]);
+    o.H = d.tex_H;
+    o.lacunarity = d.tex_lacunarity;
+    o.octaves = d.tex_octaves;
+    o.tsize = d.tex_size;
+    o.intensity = d.tex_intensity;
+    o.mod_color = d.mod_color;
+    for (int k = 0; k < 3; k++) {
+        o.msize[k] = d.mod_size[k];
+        o.mofs[k] = d.mod_ofs[k];
+    }
+    o.tdepth = d.tex_depth;
+    o.thard = (int)d.tex_hard;
+}
+
+// areaLight_t::fillQuad (arealight.cc:31-73): sample grid and jitter axes.
+static yr_status fill_quad(const yr_light_desc &d, DevLight &L, std::vector<float> &pts) {
+    const V3 a = hv(d.p[0]), b = hv(d.p[1]), c = hv(d.p[2]), dd = hv(d.p[3]);
+    const int nsam = d.samples;
+    if (nsam < 1) return YR_ERR_INVALID_ARG;
+    const float ab = h_length(b - a), bc = h_length(c - b), cd = h_length(dd - c), da = h_length(a - dd);
+    const float max_v = (bc > da) ? bc : da;
+    const float max_h = (ab > cd) ? ab : cd;
+    const int v_samp = (int)((max_v / (max_v + max_h)) * 2.0 * (double)std::sqrt((float)nsam));
+    const int h_samp = (int)((max_h / (max_v + max_h)) * 2.0 * (double)std::sqrt((float)nsam));
+    L.pt_base = (int)(pts.size() / 9);
+    if (nsam == 1) {
+        // fillQuad returns 1 without filling; illuminate() then samples the
+        // whole quad (arealight.cc:115-130)
+        L.samples = 1;
+        return YR_OK;
+    }
+    if (v_samp * h_samp > nsam) return YR_ERR_UNSUPPORTED;  // the reference would write past its array
+    const V3 inc_v_a = h_div(dd - a, (float)v_samp), inc_v_b = h_div(c - b, (float)v_samp);
+    V3 line_a = a + 0.5f * inc_v_a, line_b = b + 0.5f * inc_v_b;
+    int index = 0;
+    for (int i = 0; i < v_samp; ++i) {
+        const V3 inc_h = h_div(line_b - line_a, (float)h_samp);
+        V3 point = line_a + 0.5f * inc_h;
+        for (int j = 0; j < h_samp; ++j) {
+            const float vf = ((float)j) / ((float)h_samp);
+            const V3 inc_v = inc_v_a * (float)(1.0 - vf) + inc_v_b * vf;
+            const float rec[9] = {point.x, point.y, point.z, inc_h.x, inc_h.y, inc_h.z, inc_v.x, inc_v.y, inc_v.z};
+            pts.insert(pts.end(), rec, rec + 9);
+            index++;
+            point = point + inc_h;
+        }
+        line_a = line_a + inc_v_a;
+        line_b = line_b + inc_v_b;
+    }
+    L.samples = index;
+    return YR_OK;
+}
+
+yr_status make_lights(const std::vector<yr_light_desc> &in, std::vector<DevLight> &out, std::vector<float> &pts) {
+    out.clear();
+    pts.clear();
+    for (const yr_light_desc &d : in) {
+        DevLight L;
+        std::memset(&L, 0, sizeof(L));
+        L.type = (int)d.type;
+        L.color = c3(d.color[0], d.color[1], d.color[2]);
+        L.power = d.power;
+        L.samples = d.samples;
+        L.depth = d.depth;
+        L.cast = d.cast_shadows ? 1 : 0;
+        L.maxdist = d.maxdist;
+        switch (d.type) {
+        case YR_LIGHT_POINT:
+            L.from = hv(d.p[0]);
+            L.color = L.color * d.power;  // pointLight_t ctor: color = c*inte
+            break;
+        case YR_LIGHT_AREA: {
+            yr_status st = fill_quad(d, L, pts);
+            if (st != YR_OK) return st;
+            const V3 a = hv(d.p[0]), b = hv(d.p[1]), c = hv(d.p[2]), dd = hv(d.p[3]);
+            L.direction = h_normalize(cross(b - a, dd - a));
+            L.from = (((a + b) + c) + dd) * 0.25f;
+            L.corner = a;
+            L.tox = b - a;
+            L.toy = dd - a;
+            break;
+        }
+        case YR_LIGHT_HEMI:
+            if (d.samples < 1) return YR_ERR_INVALID_ARG;
+            L.sampdiv = d.power / (float)d.samples;
+            break;
+        case YR_LIGHT_PATH:
+            if (d.samples < 1 || d.depth < 0) return YR_ERR_INVALID_ARG;
+            break;
+        default:
+            return YR_ERR_UNSUPPORTED;
+        }
+        out.push_back(L);
+    }
+    return YR_OK;
+}
+
+// camera_t ctor for CM_PERSPECTIVE (camera.cc:27-87)
+void make_camera(const yr_camera_desc &c, DevCamera &o) {
+    const V3 pos = hv(c.pos);
+    V3 vup = hv(c.up) - pos;
+    V3 vto = hv(c.look) - pos;
+    V3 vright = cross(vup, vto);
+    vup = cross(vright, vto);
+    vup = h_normalize(vup);
+    vright = h_normalize(vright);
+    vright = vright * -1.0f;
+    // fdist = vto.normLen()
+    {
+        float vl = vto.x * vto.x + vto.y * vto.y + vto.z * vto.z;
+        if (vl != 0.f) {
+            vl = std::sqrt(vl);
+            const float dv = (float)(1.0 / vl);
+            vto.x *= dv;
+            vto.y *= dv;
+            vto.z *= dv;
+        }
+    }
+    vup = vup * (c.aspect * (float)c.resy / (float)c.resx);
+    vto = (vto * c.focal) - 0.5f * (vup + vright);
+    vup = h_div(vup, (float)c.resy);
+    vright = h_div(vright, (float)c.resx);
+    o.pos = pos;
+    o.vright = vright;
+    o.vup = vup;
+    o.vto = vto;
+    o.resx = c.resx;
+    o.resy = c.resy;
+}
+
+yr_status upload_params(yr_scene *s) {
+    if (!s->shaders.empty() &&
+        cudaMemcpy(s->d_shaders, s->shaders.data(), sizeof(DevShader) * s->shaders.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+        return YR_ERR_CUDA;
+    if (!s->lights.empty() &&
+        cudaMemcpy(s->d_lights, s->lights.data(), sizeof(DevLight) * s->lights.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+        return YR_ERR_CUDA;
+    return YR_OK;
+}
+
+yr_status take_status(yr_scene *s, cudaStream_t stream) {
+    if (cudaMemcpyAsync(s->status_host, s->status, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+        return YR_ERR_CUDA;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return YR_ERR_CUDA;
+    const int code = *s->status_host;
+    if (code != 0) {
+        if (cudaMemsetAsync(s->status, 0, sizeof(int), stream) != cudaSuccess) return YR_ERR_CUDA;
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return YR_ERR_CUDA;
+        return (yr_status)code;
+    }
+    return YR_OK;
+}
+
+}  // namespace yr
+
+using namespace yr;
+
+static void destroy_scene(yr_scene *s) {
+    if (!s) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    for (DevBuf &b : s->bufs) cudaFree(b.p);
+    for (DevBuf &b : s->scratch) cudaFree(b.p);
+    if (s->status) cudaFree(s->status);
+    if (s->status_host) cudaFreeHost(s->status_host);
+    cudaSetDevice(prev);
+    delete s;
+}
+
+extern "C" {
+
+YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene **out) {
+    if (!desc || !out) return YR_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (desc->nobjects == 0 || !desc->objects) return YR_ERR_EMPTY_SCENE;
+    if (desc->nshaders == 0 || !desc->shaders) return YR_ERR_INVALID_ARG;
+    if (desc->nlights && !desc->lights) return YR_ERR_INVALID_ARG;
+    if (desc->camera.resx <= 0 || desc->camera.resy <= 0) return YR_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return YR_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return YR_ERR_INVALID_ARG;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return YR_ERR_CUDA;
+
+    yr_scene *s = new (std::nothrow) yr_scene;
+    if (!s) return YR_ERR_OUT_OF_MEMORY;
+    s->device = device;
+    yr_status st = YR_OK;
+    auto fail = [&](yr_status e) {
+        destroy_scene(s);
+        cudaSetDevice(prev);
+        return e;
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+
+    // ---- geometry: per-object trees flattened into global arrays
+    std::vector<float4> tris;
+    std::vector<uint2> nodes;
+    std::vector<uint32_t> prims, tri_shader;
+    std::vector<DevObject> objects;
+    std::vector<Box> obounds;
+    size_t total_tris = 0;
+    for (uint32_t o = 0; o < desc->nobjects; o++) total_tris += desc->objects[o].ntris;
+    if (total_tris == 0) return fail(YR_ERR_EMPTY_SCENE);
+    if (total_tris >= (1u << 30)) return fail(YR_ERR_TOO_LARGE);
+    tris.reserve(3 * total_tris);
+    tri_shader.reserve(total_tris);
+    for (uint32_t o = 0; o < desc->nobjects; o++) {
+        const yr_object_desc &od = desc->objects[o];
+        if (od.ntris == 0 || !od.verts || !od.tris) return fail(YR_ERR_EMPTY_SCENE);
+        if (od.shader != YR_PER_TRIANGLE && od.shader >= desc->nshaders) return fail(YR_ERR_INVALID_ARG);
+        if (od.shader == YR_PER_TRIANGLE && !od.tri_shaders) return fail(YR_ERR_INVALID_ARG);
+        KdTree tree;
+        if (od.tree) {
+            tree.nodes.assign(od.tree->nodes, od.tree->nodes + od.tree->nnodes);
+            tree.prims.assign(od.tree->prims, od.tree->prims + od.tree->nprims);
+            std::memcpy(tree.bound.a, od.tree->bound, 12);
+            std::memcpy(tree.bound.g, od.tree->bound + 3, 12);
+            tree.max_depth = od.tree->max_depth;
+        } else {
+            st = build_kdtree(od.verts, od.nverts, od.tris, od.ntris, tree);
+            if (st != YR_OK) return fail(st);
+        }
+        if (tree.max_depth > s->max_tree_depth) s->max_tree_depth = tree.max_depth;
+        const uint32_t tri_base = (uint32_t)(tris.size() / 3);
+        const uint32_t node_base = (uint32_t)nodes.size();
+        const uint32_t prim_base = (uint32_t)prims.size();
+        for (uint32_t t = 0; t < od.ntris; t++) {
+            uint32_t vi[3];
+            for (int k = 0; k < 3; k++) {
+                vi[k] = od.tris[3 * (size_t)t + k];
+                if (vi[k] >= od.nverts) return fail(YR_ERR_INVALID_ARG);
+            }
+            const V3 a = hv(od.verts + 3 * (size_t)vi[0]);
+            const V3 b = hv(od.verts + 3 * (size_t)vi[1]);
+            const V3 c = hv(od.verts + 3 * (size_t)vi[2]);
+            // triangle_t ctor: normal = normalize((b-a)^(c-a)) (triangle.cc:30-43)
+            const V3 n = h_normalize(cross(b - a, c - a));
+            tris.push_back(make_float4(a.x, a.y, a.z, n.x));
+            tris.push_back(make_float4(b.x, b.y, b.z, n.y));
+            tris.push_back(make_float4(c.x, c.y, c.z, n.z));
+            const uint32_t sh = od.shader == YR_PER_TRIANGLE ? od.tri_shaders[t] : od.shader;
+            if (sh >= desc->nshaders) return fail(YR_ERR_INVALID_ARG);
+            tri_shader.push_back(sh);
+        }
+        for (const yr_kd_node &nd : tree.nodes) {
+            uint2 g;
+            g.y = nd.flags;
+            g.x = nd.word;
+            if ((nd.flags & 3u) != 3u) {
+                const uint32_t right = (nd.flags >> 2) + node_base;
+                if ((nd.flags >> 2) >= tree.nodes.size() || right >= (1u << 30)) return fail(YR_ERR_BAD_TREE);
+                g.y = (nd.flags & 3u) | (right << 2);
+            } else {
+                const uint32_t np = nd.flags >> 2;
+                if (np == 1) {
+                    if (nd.word >= od.ntris) return fail(YR_ERR_BAD_TREE);
+                    g.x = nd.word + tri_base;
+                } else if (np > 1) {
+                    if ((size_t)nd.word + np > tree.prims.size()) return fail(YR_ERR_BAD_TREE);
+                    g.x = nd.word + prim_base;
+                }
+            }
+            nodes.push_back(g);
+        }
+        for (uint32_t p : tree.prims) {
+            if (p >= od.ntris) return fail(YR_ERR_BAD_TREE);
+            prims.push_back(p + tri_base);
+        }
+        DevObject dob;
+        std::memcpy(dob.tb, tree.bound.a, 12);
+        std::memcpy(dob.tb + 3, tree.bound.g, 12);
+        dob.root = node_base;
+        dob.tri_base = tri_base;
+        dob.ntris = od.ntris;
+        dob.flags = od.cast_shadows ? 1u : 0u;
+        objects.push_back(dob);
+        obounds.push_back(mesh_bound(od.verts, od.tris, od.ntris));
+    }
+    std::vector<ObjNode> otree;
+    build_object_tree(obounds, otree);
+    const auto t1 = std::chrono::steady_clock::now();
+
+    // ---- upload
+    const float4 *d_tris;
+    const uint2 *d_nodes;
+    const uint32_t *d_prims, *d_tri_shader;
+    const DevObject *d_objects;
+    const DevObjNode *d_otree;
+    static_assert(sizeof(ObjNode) == sizeof(DevObjNode), "object node layout");
+    if ((st = dev_upload(s, tris.data(), tris.size(), (float4 **)&d_tris)) != YR_OK) return fail(st);
+    if ((st = dev_upload(s, nodes.data(), nodes.size(), (uint2 **)&d_nodes)) != YR_OK) return fail(st);
+    if (!prims.empty() && (st = dev_upload(s, prims.data(), prims.size(), (uint32_t **)&d_prims)) != YR_OK)
+        return fail(st);
+    if (prims.empty()) d_prims = nullptr;
+    if ((st = dev_upload(s, tri_shader.data(), tri_shader.size(), (uint32_t **)&d_tri_shader)) != YR_OK)
+        return fail(st);
+    if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
+    if ((st = dev_upload(s, (const DevObjNode *)otree.data(), otree.size(), (DevObjNode **)&d_otree)) != YR_OK)
+        return fail(st);
+    if (cudaMalloc(&s->status, sizeof(int)) != cudaSuccess) return fail(YR_ERR_OUT_OF_MEMORY);
+    if (cudaMemset(s->status, 0, sizeof(int)) != cudaSuccess) return fail(YR_ERR_CUDA);
+    if (cudaMallocHost(&s->status_host, sizeof(int)) != cudaSuccess) return fail(YR_ERR_OUT_OF_MEMORY);
+
+    DevScene &D = s->dev;
+    D.tris = d_tris;
+    D.nodes = d_nodes;
+    D.prims = d_prims;
+    D.objects = d_objects;
+    D.otree = d_otree;
+    D.nobjects = desc->nobjects;
+    D.ntris = (uint32_t)total_tris;
+    D.nnodes = (uint32_t)nodes.size();
+    D.nprims = (uint32_t)prims.size();
+    D.notree = (uint32_t)otree.size();
+    D.kd_stack = kMaxKdStack;
+    D.status = s->status;
+
+    // ---- shading records
+    s->shader_desc.assign(desc->shaders, desc->shaders + desc->nshaders);
+    s->light_desc.assign(desc->lights, desc->lights + desc->nlights);
+    s->shaders.resize(desc->nshaders);
+    for (uint32_t i = 0; i < desc->nshaders; i++) make_shader(desc->shaders[i], s->shaders[i]);
+    if ((st = make_lights(s->light_desc, s->lights, s->area_pts)) != YR_OK) return fail(st);
+    if ((st = dev_upload(s, s->shaders.data(), s->shaders.size(), &s->d_shaders)) != YR_OK) return fail(st);
+    if (!s->lights.empty() && (st = dev_upload(s, s->lights.data(), s->lights.size(), &s->d_lights)) != YR_OK)
+        return fail(st);
+    const float *d_pts = nullptr;
+    if (!s->area_pts.empty() && (st = dev_upload(s, s->area_pts.data(), s->area_pts.size(), (float **)&d_pts)) != YR_OK)
+        return fail(st);
+    s->camera = desc->camera;
+    s->render = desc->render;
+    DevRender &R = s->rdr;
+    make_camera(desc->camera, R.cam);
+    R.shaders = s->d_shaders;
+    R.lights = s->d_lights;
+    R.area_pts = d_pts;
+    R.tri_shader = d_tri_shader;
+    R.nlights = (int)s->lights.size();
+    R.nshaders = (int)s->shaders.size();
+    R.spp = desc->render.spp ? desc->render.spp : 1;
+    R.pw = desc->render.aa_pixelwidth;
+    R.totsamdiv = R.spp > 1 ? (float)(1.0 / (float)(R.spp - 1)) : 0.f;
+    R.seed = desc->render.seed;
+    R.self_bias = desc->render.self_bias;
+    R.raydepth = desc->render.raydepth;
+    R.background = c3(desc->render.background[0], desc->render.background[1], desc->render.background[2]);
+    R.path_light = -1;
+    for (int i = 0; i < R.nlights; i++)
+        if (s->lights[i].type == YR_LIGHT_PATH) {
+            if (R.path_light >= 0) return fail(YR_ERR_UNSUPPORTED);  // one path light per scene
+            R.path_light = i;
+            R.path_samples = s->lights[i].samples;
+            R.path_depth = s->lights[i].depth;
+        }
+
+    yr_scene_info &I = s->info;
+    I.nobjects = desc->nobjects;
+    I.ntriangles = (uint32_t)total_tris;
+    I.nnodes = (uint32_t)nodes.size();
+    I.nprims = (uint32_t)prims.size();
+    I.nlights = desc->nlights;
+    I.device_bytes = 0;
+    for (const DevBuf &b : s->bufs) I.device_bytes += b.bytes;
+    I.build_seconds = std::chrono::duration<double>(t1 - t0).count();
+    cudaSetDevice(prev);
+    *out = s;
+    return YR_OK;
+}
+
+YR_API yr_status yr_scene_destroy(yr_scene *scene) {
+    if (!scene) return YR_ERR_INVALID_ARG;
+    destroy_scene(scene);
+    return YR_OK;
+}
+
+YR_API yr_status yr_scene_info_get(const yr_scene *scene, yr_scene_info *info) {
+    if (!scene || !info) return YR_ERR_INVALID_ARG;
+    *info = scene->info;
+    return YR_OK;
+}
+
+YR_API yr_status yr_scene_set_params(yr_scene *scene, const yr_shader_desc *shaders, const yr_light_desc *lights) {
+    if (!scene) return YR_ERR_INVALID_ARG;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(scene->device);
+    if (shaders) {
+        scene->shader_desc.assign(shaders, shaders + scene->shader_desc.size());
+        for (size_t i = 0; i < scene->shaders.size(); i++) make_shader(shaders[i], scene->shaders[i]);
+    }
+    if (lights) {
+        // geometry of the lights must not change (sample grids are fixed)
+        std::vector<yr_light_desc> ld(lights, lights + scene->light_desc.size());
+        std::vector<DevLight> nl;
+        std::vector<float> pts;
+        yr_status st = make_lights(ld, nl, pts);
+        if (st != YR_OK) {
+            cudaSetDevice(prev);
+            return st;
+        }
+        if (pts != scene->area_pts) {
+            cudaSetDevice(prev);
+            return YR_ERR_INVALID_ARG;
+        }
+        scene->light_desc = ld;
+        scene->lights = nl;
+    }
+    yr_status st = upload_params(scene);
+    cudaSetDevice(prev);
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// Host-side scene object behind the opaque yr_scene handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "dev_common.cuh"
+#include "host_build.h"
+
+namespace yr {
+
+// genericShader_t colour parameters + one musgrave/clouds modulator
+struct DevShader {
+    C3 color;        // scolor
+    C3 specular;     // ks
+    float hard;
+    int tex_type;    // YR_TEX_*
+    C3 tc1, tc2;     // texture color1 / color2
+    float H, lacunarity, octaves, tsize, intensity;
+    float mod_color;
+    float msize[3], mofs[3];
+    int tdepth, thard;
+};
+
+struct DevLight {
+    int type;            // YR_LIGHT_*
+    int samples;         // area: filled quad samples; hemi/path: samples
+    int depth;           // path: maxdepth
+    int cast;            // point: cast_shadows
+    C3 color;            // point: color*power (pointLight_t ctor); others: color
+    float power;         // area "pow", hemi/path power
+    V3 from;             // point position / area centre
+    V3 direction;        // area: unit normal of the quad
+    V3 corner, tox, toy; // area: corner a, b-a, d-a
+    float maxdist;       // hemi
+    float sampdiv;       // hemi: power/samples
+    int pt_base;         // area: first entry in DevRender::area_pts
+    int pad;
+};
+
+struct DevCamera {
+    V3 pos, vright, vup, vto;
+    int resx, resy;
+};
+
+struct DevRender {
+    DevCamera cam;
+    const DevShader *shaders;
+    const DevLight *lights;
+    const float *area_pts;      // per area sample: point, jit.first, jit.second (9 floats)
+    const uint32_t *tri_shader; // shader per global triangle
+    int nlights;
+    int nshaders;
+    uint32_t spp;
+    float pw;                   // AA pixel width
+    float totsamdiv;            // 1/(spp-1) as PFLOAT (scene.cc:776-777)
+    uint32_t seed;
+    float self_bias;
+    int raydepth;
+    C3 background;
+    int path_light;             // index of the path light or -1
+    int path_samples;
+    int path_depth;
+};
+
+// Device allocation tracked by the scene (freed in yr_scene_destroy).
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace yr
+
+struct yr_scene {
+    int device = 0;
+    yr::DevScene dev{};
+    yr::DevRender rdr{};
+    std::vector<yr::DevBuf> bufs;
+    std::vector<yr::DevShader> shaders;
+    std::vector<yr::DevLight> lights;
+    std::vector<yr_shader_desc> shader_desc;
+    std::vector<yr_light_desc> light_desc;
+    std::vector<float> area_pts;
+    yr_camera_desc camera{};
+    yr_render_params render{};
+    yr_scene_info info{};
+    int max_tree_depth = 0;
+    int *status = nullptr;          // device status word
+    int *status_host = nullptr;     // pinned mirror
+    yr::DevShader *d_shaders = nullptr;
+    yr::DevLight *d_lights = nullptr;
+    // render scratch (grown on demand)
+    std::vector<yr::DevBuf> scratch;
+};
+
+namespace yr {
+// derived device records from the ABI descriptors (scene.cu)
+void make_shader(const yr_shader_desc &d, DevShader &o);
+yr_status make_lights(const std::vector<yr_light_desc> &in, std::vector<DevLight> &out, std::vector<float> &pts);
+void make_camera(const yr_camera_desc &c, DevCamera &o);
+yr_status upload_params(yr_scene *s);
+// read and clear the device status word (synchronizes `stream`)
+yr_status take_status(yr_scene *s, cudaStream_t stream);
+}  // namespace yr
