@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark: Mrays/s of the ray-casting hot path on the large plain scene.
+
+Workload (the largest single-GPU configuration of the benchmark set):
+16x16 jittered grid of UV spheres (64 rings x 128 segments, 4,128,770
+triangles with the ground plane, 257 objects), four area lights with 16
+samples each, path-traced GI with 2 bounces (pathlight, 1 path per camera
+sample), 1920x1080, 16 camera samples per pixel, seeded synthetic geometry.
+One step = one full render of that frame.  Mrays/s counts every traced ray
+(primary + shadow + bounce) over the device time of the render.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU (torchrun), every rank renders its own frame
+replica (the path shards by frame/tile with no exchange): weak scaling,
+value = all rays of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import csv
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from yafray_b200 import abi, scenes  # noqa: E402
+
+METRIC = "Mrays/s"
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "yr_ref_harness")
+
+
+def workload(args):
+    if args.config == "small":
+        sc = scenes.config_small()
+        name = "small: UV sphere 16,128 tris + plane, point light, 320x240, 1 spp"
+    else:
+        sc = scenes.config_large(seed=args.seed, resx=args.resx, resy=args.resy, spp=args.spp, grid=args.grid)
+        name = (f"large: {args.grid}x{args.grid} spheres + plane ({sc.ntris:,} tris, {len(sc.meshes)} objects), "
+                f"4 area lights x16, path GI depth 2, {args.resx}x{args.resy}, {args.spp} spp")
+    return sc, name
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for r in csv.reader(fh):
+                if len(r) >= 9:
+                    rows.append([x.strip() for x in r])
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------- CPU legs
+def reference_render(sc, threads, rows, reps, timeout=900):
+    """Run the unmodified reference (oracle/_ref) on full-width rows [0, rows)
+    of the frame; returns per-render dicts (render_s, primary, shadow, bounce)."""
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "o.bin")
+        scenes.write_yrs(sc, sp)
+        cmd = [HARNESS, "render", sp, op, str(threads), "0", str(sc.resx), "0", str(rows), str(reps)]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr[-2000:])
+        return [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
+
+
+def cpu_sample_rows(sc, threads):
+    """Full-width band sized for ~10 s of wall time on `threads` cores
+    (~1000 px/s per core at 16 spp); at least one 64-pixel block row."""
+    spp = max(1, sc.render.spp)
+    px = 10.0 * 1000.0 * threads * 16.0 / spp
+    rows = int(min(sc.resy, max(64, px / sc.resx)))
+    return rows
+
+
+def cpu_baseline(sc):
+    threads = host_cores()
+    if os.path.exists(HARNESS):
+        # threadedscene_t aborts when threads exceed the 64x64 blocks that hold work
+        rows = cpu_sample_rows(sc, threads)
+        blocks = ((sc.resx + 63) // 64) * ((rows + 63) // 64)
+        thr = max(1, min(threads, blocks))
+        res = reference_render(sc, thr, rows, 1)[-1]
+        rays = res["primary"] + res["shadow"] + res["bounce"]
+        return {"value": rays / res["render_s"] / 1e6, "unit": METRIC, "cores": thr, "kind": "reference",
+                "sample": f"unmodified reference (threadedscene_t, {thr} threads) on rows 0-{rows} of the frame "
+                          f"({sc.resx}x{rows} px x {sc.render.spp} spp, {rays:,} rays counted at "
+                          f"scene_t::isShadowed/firstHit + camera rays), render phase only; kd build excluded"}
+    import yrtest as T
+    O = T.OracleScene(sc)
+    t0 = time.perf_counter()
+    _, st = O.render(0, min(sc.resx, 64), 0, 8)
+    dt = time.perf_counter() - t0
+    rays = int(st[0] + st[1] + st[2])
+    return {"value": rays / dt / 1e6, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"oracle port, 1 thread, pixels 64x8 of the frame ({rays:,} rays)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc, name = workload(args)
+    if not os.path.exists(HARNESS):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/yr_ref_harness was not built"}))
+        return
+    threads = host_cores()
+    rows = cpu_sample_rows(sc, threads)
+    blocks = ((sc.resx + 63) // 64) * ((rows + 63) // 64)
+    thr = max(1, min(threads, blocks))
+    res = reference_render(sc, thr, rows, args.warmup + args.steps, timeout=1800)
+    timed = res[args.warmup:]
+    rays = sum(r["primary"] + r["shadow"] + r["bounce"] for r in timed)
+    secs = sum(r["render_s"] for r in timed)
+    value = rays / secs / 1e6
+    sample = (f"unmodified reference (threadedscene_t, {thr} threads) rendering rows 0-{rows} of the frame "
+              f"per step ({sc.resx}x{rows} px x {sc.render.spp} spp); rays counted at scene_t::isShadowed/firstHit "
+              f"+ camera rays; render phase timed, kd build excluded")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / max(1, len(timed)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "sample_rows": rows},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": thr, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ------------------------------------------------------------------ GPU leg
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return {}
+    return {}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="large", choices=["large", "small"])
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--resx", type=int, default=1920)
+    ap.add_argument("--resy", type=int, default=1080)
+    ap.add_argument("--spp", type=int, default=16)
+    ap.add_argument("--grid", type=int, default=16)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from yafray_b200 import api
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    sc, name = workload(args)
+    t0 = time.perf_counter()
+    ds = api.DeviceScene(sc, device=local)
+    info = ds.info()
+    build_s = time.perf_counter() - t0
+    out = torch.empty((sc.resy, sc.resx, 4), dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        ds.render_into(out.data_ptr())
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    agg = {"rays": 0, "kms": np.zeros(abi.YR_K_COUNT), "launch": np.zeros(abi.YR_K_COUNT),
+           "krays": np.zeros(abi.YR_K_COUNT), "knodes": np.zeros(abi.YR_K_COUNT), "ktests": np.zeros(abi.YR_K_COUNT)}
+    for _ in range(args.steps):
+        st = abi.YrRenderStats()
+        st.want_kernel_stats = 1
+        abi.check(ds.lib.yr_render(ds.handle, C.c_void_p(out.data_ptr()), 0, C.byref(st), C.c_void_p(0)), "yr_render")
+        agg["rays"] += st.rays_primary + st.rays_shadow + st.rays_bounce
+        agg["kms"] += np.array(st.kernel_ms[:])
+        agg["launch"] += np.array(st.kernel_launches[:])
+        agg["krays"] += np.array(st.kernel_rays[:], dtype=np.float64)
+        agg["knodes"] += np.array(st.kernel_nodes[:], dtype=np.float64)
+        agg["ktests"] += np.array(st.kernel_tests[:], dtype=np.float64)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    rays_all = torch.tensor([float(agg["rays"])], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(rays_all, op=dist.ReduceOp.SUM)
+    ms_max = float(t_max.item())
+    value = float(rays_all.item()) / (ms_max / 1000.0) / 1e6
+    gpu_launches = int(agg["launch"].sum())
+
+    # end to end through the C ABI: per step the shader/light parameters go
+    # host -> device (yr_scene_set_params) and the image comes back to a
+    # pinned host buffer (yr_render with a host destination)
+    host_img = torch.empty((sc.resy, sc.resx, 4), dtype=torch.float32).pin_memory()
+    h2d = len(sc.shaders) * C.sizeof(abi.YrShaderDesc) + len(sc.lights) * C.sizeof(abi.YrLightDesc)
+    d2h = host_img.numel() * 4
+    e2e_rays = 0
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ds.set_params(sc.shaders, sc.lights)
+        st = ds.render_into(host_img.data_ptr(), on_host=True)
+        e2e_rays += st.rays_primary + st.rays_shadow + st.rays_bounce
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    e2e_r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(e2e_r, op=dist.ReduceOp.SUM)
+    e2e_value = float(e2e_r.item()) / float(e2e_t.item()) / 1e6
+
+    # roofline of the dominant kernel class: algorithmic bytes per ray =
+    # 32 (ray) + 16 (hit / occlusion record) + 8 per kd or object-tree node
+    # + 52 per triangle test (48-byte triangle + 4-byte leaf index)
+    kms = agg["kms"]
+    dom = int(np.argmax(kms))
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    alg_bytes = 48.0 * agg["krays"][dom] + 8.0 * agg["knodes"][dom] + 52.0 * agg["ktests"][dom]
+    achieved = alg_bytes / (kms[dom] / 1000.0) / 1e9 if kms[dom] > 0 else 0.0
+    traffic = load_traffic().get(abi.KERNEL_CLASSES[dom])
+    launches = max(1.0, agg["launch"][dom])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "kernel": abi.KERNEL_CLASSES[dom],
+                "bytes_per_launch": alg_bytes / launches, "ms_per_launch": kms[dom] / launches,
+                "peak_source": peak_src,
+                "nodes_per_ray": agg["knodes"][dom] / max(1.0, agg["krays"][dom]),
+                "tests_per_ray": agg["ktests"][dom] / max(1.0, agg["krays"][dom])}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": name, "triangles": int(info.ntriangles), "objects": int(info.nobjects),
+                   "kd_nodes": int(info.nnodes), "l2": "inputs larger than L2 (scene arrays "
+                   f"{info.device_bytes / 1e6:.0f} MB on the device)",
+                   "host_build_s": round(info.build_seconds, 3), "scene_setup_s": round(build_s, 3),
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": gpu_launches,
+        "roofline": roofline,
+        "kernels_ms": {abi.KERNEL_CLASSES[k]: round(float(kms[k]), 3) for k in range(abi.YR_K_COUNT) if kms[k] > 0},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline(sc)
+        except Exception as ex:  # the GPU number stands without it
+            line["cpu_baseline"] = {"value": None, "error": str(ex)[:300]}
+    ds.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

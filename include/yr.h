@@ -181,6 +181,9 @@ typedef struct yr_render_params {
     uint32_t seed;           /* Cranley-Patterson rotation seed               */
     float background[3];     /* constant background colour (black = none)     */
     uint32_t flags;          /* reserved, 0                                    */
+    int32_t region[4];       /* x0, x1, y0, y1: render only these pixels
+                                (scene_t::setRegion / the loader's -r option);
+                                all zero = the whole image                    */
 } yr_render_params;
 
 typedef struct yr_object_desc {
@@ -271,11 +274,33 @@ YR_API yr_status yr_trace_shadow(yr_scene *scene, const yr_shadow_ray *rays, uin
 /* ------------------------------------------------------------------------
  * Rendering.
  * ------------------------------------------------------------------------ */
+/* Kernel classes reported in yr_render_stats (per-class arrays). */
+enum {
+    YR_K_PRIMARY = 0,        /* camera rays + closest hit                     */
+    YR_K_SHADE_CAMERA = 1,   /* light sampling at camera hits                 */
+    YR_K_SHADOW = 2,         /* shadow-ray queue traversal (any hit)          */
+    YR_K_GATHER = 3,         /* per-vertex light sums                         */
+    YR_K_BOUNCE = 4,         /* bounce-ray queue traversal (closest hit)      */
+    YR_K_SHADE_PATH = 5,     /* light sampling at bounce vertices            */
+    YR_K_OTHER = 6,          /* finish, queue bookkeeping                     */
+    YR_K_COUNT = 8
+};
+
 typedef struct yr_render_stats {
     uint64_t rays_primary;
     uint64_t rays_shadow;
     uint64_t rays_bounce;
     double ms;               /* device time of the render (CUDA events)      */
+    /* input: nonzero = time every kernel class with CUDA events and count
+     * kd nodes / triangle tests per class (costs a few microseconds per
+     * launch) */
+    uint32_t want_kernel_stats;
+    uint32_t reserved;
+    double kernel_ms[YR_K_COUNT];        /* summed event time per class       */
+    uint32_t kernel_launches[YR_K_COUNT];
+    uint64_t kernel_rays[YR_K_COUNT];    /* rays traversed per class          */
+    uint64_t kernel_nodes[YR_K_COUNT];   /* kd + object-tree nodes visited    */
+    uint64_t kernel_tests[YR_K_COUNT];   /* ray-triangle tests                */
 } yr_render_stats;
 
 /* Render the whole image: RGBA float, resy rows of resx pixels, row 0 at the

@@ -8,13 +8,11 @@
 //   yr_ref_harness tree    SCENE OUT           kd-trees + object tree
 //   yr_ref_harness rays    SCENE RAYS OUT      kd / scene ray queries
 //   yr_ref_harness camera  SCENE OUT           primary ray directions
-//   yr_ref_harness render  SCENE OUT THREADS [x0 x1 y0 y1]
-//                                              stock scene_t::render, float sink
-//   yr_ref_harness explicit SCENE OUT [x0 x1 y0 y1]
-//                                              index-explicit GI estimator
+//   yr_ref_harness render  SCENE OUT THREADS [x0 x1 y0 y1 [REPEATS]]
+//                                              stock scene_t::render, float sink,
+//                                              ray counts, one JSON line per render
 //   yr_ref_harness noise   POINTS OUT          newPerlin / fBm / turbulence
 //   yr_ref_harness halton  OUT                 Halton setStart+getNext values
-//   yr_ref_harness shade   SCENE OUT           getSurface / fromLight probes
 //
 // Private members (kdTree_t::nodes, meshObject_t::triangles, scene_t::BTree)
 // are read by compiling the reference headers with private/protected
@@ -59,6 +57,37 @@ namespace yafray {
 // image textures are not on the path.
 cBuffer_t *load_jpeg(const char *name) { return NULL; }
 geomeTree_t<object3d_t> *buildObjectTree(std::list<object3d_t *> &obj_list);
+}
+
+// Ray counters: the reference has none (mesh.cc:409-412 are unused), so
+// the calls that plugins make into scene_t::isShadowed / firstHit are
+// counted through link-time wrappers (-Wl,--wrap in oracle/Makefile).
+static volatile long g_shadow_rays = 0, g_bounce_rays = 0;
+extern "C" {
+bool __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_9point3d_tE(
+    const scene_t *, renderState_t &, const surfacePoint_t &, const point3d_t &);
+bool __wrap__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_9point3d_tE(
+    const scene_t *s, renderState_t &st, const surfacePoint_t &sp, const point3d_t &l) {
+    __sync_fetch_and_add(&g_shadow_rays, 1);
+    return __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_9point3d_tE(s, st, sp,
+                                                                                                           l);
+}
+bool __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_10vector3d_tE(
+    const scene_t *, renderState_t &, const surfacePoint_t &, const vector3d_t &);
+bool __wrap__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_10vector3d_tE(
+    const scene_t *s, renderState_t &st, const surfacePoint_t &sp, const vector3d_t &d) {
+    __sync_fetch_and_add(&g_shadow_rays, 1);
+    return __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_10vector3d_tE(s, st,
+                                                                                                            sp, d);
+}
+bool __real__ZNK6yafray7scene_t8firstHitERNS_13renderState_tERNS_14surfacePoint_tERKNS_9point3d_tERKNS_10vector3d_tEb(
+    const scene_t *, renderState_t &, surfacePoint_t &, const point3d_t &, const vector3d_t &, bool);
+bool __wrap__ZNK6yafray7scene_t8firstHitERNS_13renderState_tERNS_14surfacePoint_tERKNS_9point3d_tERKNS_10vector3d_tEb(
+    const scene_t *s, renderState_t &st, surfacePoint_t &sp, const point3d_t &p, const vector3d_t &r, bool sh) {
+    __sync_fetch_and_add(&g_bounce_rays, 1);
+    return __real__ZNK6yafray7scene_t8firstHitERNS_13renderState_tERNS_14surfacePoint_tERKNS_9point3d_tERKNS_10vector3d_tEb(
+        s, st, sp, p, r, sh);
+}
 }
 
 static double now_s() {
@@ -417,7 +446,7 @@ class floatSink_t : public colorOutput_t {
     std::vector<float> img;
 };
 
-static void cmd_render(const SceneFile &s, const char *out, int threads, const int *crop) {
+static void cmd_render(const SceneFile &s, const char *out, int threads, const int *crop, int reps) {
     RefScene r;
     build_ref(s, r, true);
     scene_t *sc = r.scene;
@@ -441,20 +470,29 @@ static void cmd_render(const SceneFile &s, const char *out, int threads, const i
     const uint32_t spp = s.rp.spp ? s.rp.spp : 1;
     // every pixel resampled: AA_threshold 0 (renderblock.cc:22-66 uses >=)
     sc->setAASamples(spp > 1 ? 1 : 0, spp > 1 ? (int)spp - 1 : 1, s.rp.aa_pixelwidth, 0.0, false);
+    long region_px = (long)s.cam.resx * s.cam.resy;
     if (crop) {
         // screen-space region in [-1,1] (scene.cc:745-747), from pixel bounds
+        // (pixel centres, so a pixel is inside exactly when x0 <= x < x1)
         PFLOAT rx = (PFLOAT)s.cam.resx, ry = (PFLOAT)s.cam.resy;
         sc->setRegion(2.0 * crop[0] / rx - 1.0, 2.0 * crop[1] / rx - 1.0, 1.0 - 2.0 * crop[3] / ry,
                       1.0 - 2.0 * crop[2] / ry);
+        region_px = (long)(crop[1] - crop[0]) * (crop[3] - crop[2]);
     }
     floatSink_t sink(s.cam.resx, s.cam.resy);
-    double t0 = now_s();
-    sc->render(sink);
-    double t1 = now_s();
+    // repeated renders share one scene (and one kd-tree build); each prints a line
+    for (int rep = 0; rep < reps; rep++) {
+        g_shadow_rays = g_bounce_rays = 0;
+        double t0 = now_s();
+        sc->render(sink);
+        double t1 = now_s();
+        printf("{\"render_s\": %.6f, \"threads\": %d, \"primary\": %ld, \"shadow\": %ld, \"bounce\": %ld}\n",
+               t1 - t0, threads, region_px * (long)spp, (long)g_shadow_rays, (long)g_bounce_rays);
+        fflush(stdout);
+    }
     FILE *f = fopen(out, "wb");
     wr(f, &sink.img[0], 4 * sink.img.size());
     fclose(f);
-    printf("{\"render_s\": %.6f, \"threads\": %d}\n", t1 - t0, threads);
 }
 
 // ------------------------------------------------------------------- noise
@@ -523,12 +561,13 @@ int main(int argc, char **argv) {
     } else if (cmd == "camera") {
         cmd_camera(s, argv[3]);
     } else if (cmd == "render") {
-        if (argc < 5) die("render SCENE OUT THREADS [x0 x1 y0 y1]");
+        if (argc < 5) die("render SCENE OUT THREADS [x0 x1 y0 y1 [REPEATS]]");
         int crop[4];
         bool has_crop = argc >= 9;
         if (has_crop)
             for (int k = 0; k < 4; k++) crop[k] = atoi(argv[5 + k]);
-        cmd_render(s, argv[3], atoi(argv[4]), has_crop ? crop : NULL);
+        const int reps = argc >= 10 ? atoi(argv[9]) : 1;
+        cmd_render(s, argv[3], atoi(argv[4]), has_crop ? crop : NULL, reps < 1 ? 1 : reps);
     } else {
         die("unknown command");
     }

@@ -1,0 +1,105 @@
+"""Regenerate the golden vectors in this folder from the UNMODIFIED reference.
+
+Run in the build container (needs oracle/_ref/yr_ref_harness, built from the
+reference sources by `make -C oracle`):
+
+    python tests/golden/make_golden.py
+
+Every fixture is produced by the reference harness on seeded inputs; the
+inputs themselves are either stored alongside or regenerated from the seeds
+by yafray_b200.scenes.
+"""
+import os
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+import yrtest as T  # noqa: E402
+from yafray_b200 import scenes  # noqa: E402
+
+
+def small_sphere_scene():
+    sv, st = scenes.uv_sphere((0.0, 0.0, 0.0), 1.0, rings=16, segments=32)
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    sc = scenes.config_small(80, 60)
+    sc.meshes = [scenes.Mesh(sv, st, 0), scenes.Mesh(pv, pt, 0)]
+    return sc
+
+
+def random_mesh_scene(n, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-5, 5, (n, 1, 3))
+    v = (c + 0.3 * rng.uniform(-1, 1, (n, 3, 3))).reshape(-1, 3).astype(np.float32)
+    t = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
+    sc = scenes.config_small(80, 60)
+    sc.meshes = [scenes.Mesh(v, t, 0)]
+    return sc
+
+
+def trees():
+    out = {}
+    for name, sc in (("sphere16", small_sphere_scene()), ("random3000", random_mesh_scene(3000, 11))):
+        tr, ot = T.harness_trees(sc)
+        for i, t in enumerate(tr):
+            for k in ("nodes", "prims", "tb", "ob"):
+                out[f"{name}_{i}_{k}"] = t[k]
+            out[f"{name}_{i}_params"] = np.array([t["max_depth"], t["max_leaf"]], np.int32)
+            out[f"{name}_{i}_cost"] = np.array([t["cost_ratio"]], np.float32)
+        out[f"{name}_otree"] = ot
+    np.savez_compressed(os.path.join(HERE, "trees.npz"), **out)
+
+
+def rays():
+    sc = scenes.config_small()
+    n = 8192
+    rng = np.random.default_rng(2)
+    base = T.random_rays(sc, n, 1)
+    recs = np.zeros(n, T.RAY_REC)
+    recs["mode"] = rng.integers(0, 5, n)
+    recs["object"] = rng.integers(0, 2, n)
+    recs["frm"] = base[:, :3]
+    recs["dir"] = base[:, 4:7]
+    recs["dist"] = np.where(rng.random(n) < 0.5, -1.0, rng.uniform(0.5, 10, n))
+    recs["l"] = base[:, :3] + base[:, 4:7] * rng.uniform(0.5, 8, (n, 1))
+    res = T.harness_rays(sc, recs)
+    np.savez_compressed(os.path.join(HERE, "rays_small.npz"), recs=recs, res=res)
+
+
+def camera_and_render():
+    sc = scenes.config_small(160, 120)
+    cam = T.harness_camera(sc)
+    img, _ = T.harness_render(sc)
+    np.savez_compressed(os.path.join(HERE, "render_small_160x120.npz"), camera=cam, image=img)
+
+
+def halton_noise():
+    with tempfile.TemporaryDirectory() as d:
+        hp = os.path.join(d, "h.bin")
+        T.run_harness("halton", hp)
+        raw = np.fromfile(hp, np.float32)
+        hal = raw[: 12 * 4096].reshape(12, 4096)
+        ri = raw[12 * 4096:].reshape(4096, 3)
+        rng = np.random.default_rng(5)
+        pts = np.concatenate([rng.uniform(-300, 300, (2048, 3)), rng.uniform(-4, 4, (2048, 3))]).astype(np.float32)
+        pp, op = os.path.join(d, "p.bin"), os.path.join(d, "n.bin")
+        with open(pp, "wb") as f:
+            f.write(struct.pack("<I", pts.shape[0]))
+            f.write(pts.tobytes())
+        T.run_harness("noise", pp, op)
+        noise = np.fromfile(op, np.float32).reshape(-1, 5)
+    np.savez_compressed(os.path.join(HERE, "qmc_noise.npz"), halton=hal, ri=ri, pts=pts, noise=noise)
+
+
+if __name__ == "__main__":
+    assert T.has_harness(), "build the reference first: make -C oracle"
+    trees()
+    rays()
+    camera_and_render()
+    halton_noise()
+    for f in sorted(os.listdir(HERE)):
+        print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,117 @@
+"""The CPU oracle and the host-side builders against golden vectors produced
+by the unmodified reference (tests/golden/make_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+import yrtest as T
+from yafray_b200 import scenes
+
+G = T.GOLDEN
+
+
+def load(name):
+    return np.load(os.path.join(G, name))
+
+
+def _scenes():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mg", os.path.join(G, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return {"sphere16": mg.small_sphere_scene(), "random3000": mg.random_mesh_scene(3000, 11)}
+
+
+@pytest.mark.parametrize("name", ["sphere16", "random3000"])
+def test_kdtree_build_matches_reference(name):
+    """yr_kdtree_build reproduces kdTree_t node for node (kdtree.cc:57-582)."""
+    g = load("trees.npz")
+    sc = _scenes()[name]
+    for i, m in enumerate(sc.meshes):
+        t = T.product_tree(m)
+        assert np.array_equal(t["nodes"], g[f"{name}_{i}_nodes"])
+        assert np.array_equal(t["prims"], g[f"{name}_{i}_prims"])
+        assert np.array_equal(t["tb"].view(np.uint32), g[f"{name}_{i}_tb"].view(np.uint32))
+        assert [t["max_depth"], t["max_leaf"]] == list(g[f"{name}_{i}_params"])
+        assert t["cost_ratio"] == g[f"{name}_{i}_cost"][0]
+        assert np.array_equal(T.mesh_bound(m).view(np.uint32), g[f"{name}_{i}_ob"].view(np.uint32))
+
+
+def test_object_tree_matches_reference():
+    g = load("trees.npz")
+    sc = _scenes()["sphere16"]
+    assert np.array_equal(T.product_object_tree(sc).view(np.uint32), g["sphere16_otree"].view(np.uint32))
+
+
+def test_oracle_rays_match_reference():
+    """kdTree_t::Intersect / IntersectS, scene_t::firstHit and isShadowed on
+    8192 seeded queries: hit flag, triangle and distance bit for bit."""
+    g = load("rays_small.npz")
+    recs, res = g["recs"], g["res"]
+    sc = scenes.config_small()
+    O = T.OracleScene(sc)
+    bad = []
+    for i in range(recs.shape[0]):
+        m = int(recs["mode"][i])
+        if m in (0, 1):
+            o = O.kd(int(recs["object"][i]), recs["frm"][i], recs["dir"][i], float(recs["dist"][i]), m == 1)
+            ok = o[0] == res[i, 0] and (not o[0] or (o[1] == res[i, 2] and o[2] == res[i, 3]))
+        elif m in (2, 4):
+            r = np.zeros((1, 8), np.float32)
+            r[0, :3], r[0, 4:7] = recs["frm"][i], recs["dir"][i]
+            h = O.trace_closest(r, shadow_only=(m == 4))[0]
+            if res[i, 0]:
+                ok = h[1] == res[i, 1] and h[2] == res[i, 2] and h[0] == res[i, 3]
+            else:
+                ok = h[1] == 0xFFFFFFFF
+        else:
+            r = np.zeros((1, 8), np.float32)
+            r[0, :3] = recs["frm"][i]
+            r[0, 3] = np.array([recs["object"][i]], np.uint32).view(np.float32)[0]
+            r[0, 4:7] = recs["l"][i]
+            ok = O.trace_shadow(r)[0] == res[i, 0]
+        if not ok:
+            bad.append(i)
+    assert not bad, f"{len(bad)} mismatches, first {bad[:5]}"
+    assert (res[:, 0] == 1).sum() > 500  # the set exercises real hits
+
+
+def test_oracle_camera_and_render_match_reference():
+    g = load("render_small_160x120.npz")
+    sc = scenes.config_small(160, 120)
+    O = T.OracleScene(sc)
+    cam = O.camera_rays()
+    assert np.array_equal(cam.view(np.uint32), g["camera"].view(np.uint32))
+    img, stats = O.render()
+    ref = g["image"]
+    assert np.array_equal(img[..., 3], ref[..., 3])  # same pixels hit
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
+    assert stats[0] == 160 * 120
+
+
+def test_oracle_halton_and_ri_match_reference():
+    g = load("qmc_noise.npz")
+    lib = T.oracle()
+    primes = [2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37]
+    for b, p in enumerate(primes):
+        got = np.array([lib.orc_halton(p, i) for i in range(4096)], np.float32)
+        assert np.array_equal(got.view(np.uint32), g["halton"][b].view(np.uint32)), p
+    lp = np.array([lib.orc_ri_lp((i * 7919) & 0xFFFFFFFF) for i in range(4096)], np.float32)
+    assert np.array_equal(lp.view(np.uint32), g["ri"][:, 2].view(np.uint32))
+
+
+def test_oracle_noise_matches_reference():
+    """newPerlin, fBm and turbulence within 2 ulp-scale absolute error (the
+    shipped build reassociates the lerp chain under -ffast-math)."""
+    g = load("qmc_noise.npz")
+    lib = T.oracle()
+    pts, ref = g["pts"], g["noise"]
+    got = np.zeros_like(ref)
+    for i, p in enumerate(pts):
+        x, y, z = (float(v) for v in p)
+        got[i] = [lib.orc_perlin(x, y, z), lib.orc_fbm(x, y, z, 1.0, 2.0, 6.0), lib.orc_fbm(x, y, z, 0.8, 2.5, 3.5),
+                  lib.orc_turbulence(x, y, z, 2, 1.0, 0), lib.orc_turbulence(x, y, z, 3, 2.5, 1)]
+    err = np.abs(got - ref)
+    assert err.max() < 2e-6, err.max(0)

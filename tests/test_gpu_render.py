@@ -1,0 +1,75 @@
+"""yr_render against the oracle on the same scenes and QMC indices.
+
+Tolerances (from the specification of this path): radiance within 1e-4
+relative; pixel coverage (alpha) identical."""
+import numpy as np
+import pytest
+
+import yrtest as T
+from yafray_b200 import api, scenes
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+
+
+def _cmp(img, ref, frac=1.0):
+    assert img.shape == ref.shape
+    assert np.isfinite(img).all()
+    rel = np.abs(img[..., :3] - ref[..., :3]) / np.maximum(np.abs(ref[..., :3]), 1e-3)
+    ok = (rel <= RTOL).all(-1)
+    assert ok.mean() >= frac, f"{(~ok).sum()} pixels beyond {RTOL}; worst {rel.max()}"
+    return rel
+
+
+def test_render_small_point_light(cuda):
+    """320x240 point light, 1 spp: the benchmark's CPU-runnable case."""
+    sc = scenes.config_small()
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    ref, stats = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref)
+    st = ds.last_stats
+    assert st.rays_primary == stats[0] and st.rays_shadow == stats[1]
+
+
+def test_render_small_aa(cuda):
+    sc = scenes.config_small(96, 72)
+    sc.render.spp = 5
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    ref, _ = T.OracleScene(sc).render()
+    _cmp(img, ref)
+
+
+def test_render_gi_area_lights(cuda):
+    """Area lights + path GI with 2 bounces on a small sphere grid."""
+    sc = scenes.config_large(seed=2, resx=64, resy=40, spp=4, grid=2)
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    ref, stats = T.OracleScene(sc).render()
+    _cmp(img, ref, frac=0.995)
+    st = ds.last_stats
+    assert st.rays_primary == stats[0]
+    assert abs(int(st.rays_shadow) - int(stats[1])) <= 0.001 * stats[1] + 4
+    assert abs(int(st.rays_bounce) - int(stats[2])) <= 0.001 * stats[2] + 4
+
+
+def test_render_hemi_and_texture(cuda):
+    sc = scenes.config_small(64, 48)
+    sc.shaders[0] = scenes.fbm_shader((0.8, 0.8, 0.8), (0.2, 0.5, 0.7), (1.0, 1.0, 1.0), 0.7, 3.0)
+    sc.lights.append(scenes.hemi_light(samples=8, power=0.5))
+    sc.render.spp = 2
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    ref, _ = T.OracleScene(sc).render()
+    _cmp(img, ref, frac=0.995)
+
+
+def test_render_per_triangle_materials(cuda):
+    sc = scenes.config_diff(res=48, spp=2, groups=8, nlights=2)
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    ref, _ = T.OracleScene(sc).render()
+    _cmp(img, ref, frac=0.995)

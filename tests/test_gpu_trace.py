@@ -1,0 +1,91 @@
+"""CUDA ray queries against the oracle, through the C ABI (yr_trace_closest,
+yr_trace_shadow).  Integer results (object, triangle, node counts) must be
+identical; hit distances bit for bit."""
+import numpy as np
+import pytest
+
+import yrtest as T
+from yafray_b200 import api, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_closest(torch, ds, rays, shadow_only=False):
+    n = rays.shape[0]
+    d_rays = torch.from_numpy(np.ascontiguousarray(rays, np.float32)).cuda()
+    d_hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    api.trace_closest(ds, d_rays.data_ptr(), n, d_hits.data_ptr(), shadow_only)
+    torch.cuda.synchronize()
+    return d_hits.cpu().numpy().view(np.uint32)
+
+
+def _run_shadow(torch, ds, srays):
+    n = srays.shape[0]
+    d_rays = torch.from_numpy(np.ascontiguousarray(srays, np.float32)).cuda()
+    d_occ = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    api.trace_shadow(ds, d_rays.data_ptr(), n, d_occ.data_ptr())
+    torch.cuda.synchronize()
+    return d_occ.cpu().numpy()
+
+
+def _shadow_rays(sc, n, seed):
+    rng = np.random.default_rng(seed)
+    base = T.random_rays(sc, n, seed)
+    s = np.zeros((n, 8), np.float32)
+    s[:, :3] = base[:, :3]
+    s[:, 3] = rng.integers(0, len(sc.meshes), n).astype(np.uint32).view(np.float32)
+    s[:, 4:7] = base[:, :3] + base[:, 4:7] * rng.uniform(0.5, 8, (n, 1)).astype(np.float32)
+    dirmode = rng.random(n) < 0.25
+    s[dirmode, 4:7] = base[dirmode, 4:7]
+    s[:, 7] = dirmode.astype(np.uint32).view(np.float32)
+    return s
+
+
+@pytest.mark.parametrize("shadow_only", [False, True])
+def test_closest_small_scene(cuda, shadow_only):
+    sc = scenes.config_small()
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    rays = T.random_rays(sc, 60000, 7)
+    got = _run_closest(cuda, ds, rays, shadow_only)
+    ref = O.trace_closest(rays, shadow_only)
+    assert np.array_equal(got[:, 1], ref[:, 1]), "object ids differ"
+    assert np.array_equal(got[:, 2], ref[:, 2]), "triangle ids differ"
+    assert np.array_equal(got[:, 0], ref[:, 0]), "hit distances differ"
+    assert np.array_equal(got[:, 3], ref[:, 3]), "node visit counts differ"
+    assert (ref[:, 1] != 0xFFFFFFFF).sum() > 5000
+
+
+def test_closest_many_objects(cuda):
+    sc = scenes.config_large(seed=3, resx=64, resy=48, spp=1, grid=4)
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    rays = T.random_rays(sc, 40000, 9)
+    got = _run_closest(cuda, ds, rays)
+    ref = O.trace_closest(rays)
+    assert np.array_equal(got[:, :3], ref[:, :3])
+
+
+def test_shadow_small_scene(cuda):
+    sc = scenes.config_small()
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    s = _shadow_rays(sc, 60000, 5)
+    assert np.array_equal(_run_shadow(cuda, ds, s), O.trace_shadow(s))
+
+
+def test_shadow_many_objects(cuda):
+    sc = scenes.config_large(seed=3, resx=64, resy=48, spp=1, grid=4)
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    s = _shadow_rays(sc, 40000, 6)
+    occ = _run_shadow(cuda, ds, s)
+    ref = O.trace_shadow(s)
+    assert np.array_equal(occ, ref)
+    assert 0 < ref.sum() < len(ref)
+
+
+def test_empty_query(cuda):
+    sc = scenes.config_small(32, 24)
+    ds = api.DeviceScene(sc)
+    assert _run_closest(cuda, ds, np.zeros((0, 8), np.float32)).shape == (0, 4)

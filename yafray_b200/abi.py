@@ -72,7 +72,7 @@ class YrLightDesc(C.Structure):
 class YrRenderParams(C.Structure):
     _fields_ = [("self_bias", C.c_float), ("raydepth", C.c_int32), ("spp", C.c_uint32),
                 ("aa_pixelwidth", C.c_float), ("seed", C.c_uint32), ("background", f3),
-                ("flags", C.c_uint32)]
+                ("flags", C.c_uint32), ("region", C.c_int32 * 4)]
 
 
 class YrObjectDesc(C.Structure):
@@ -108,9 +108,17 @@ class YrShadowRay(C.Structure):
     _fields_ = [("p", f3), ("object", C.c_uint32), ("l", f3), ("flags", C.c_uint32)]
 
 
+YR_K_COUNT = 8
+KERNEL_CLASSES = ["primary", "shade_camera", "shadow", "gather", "bounce", "shade_path", "other", "unused"]
+
+
 class YrRenderStats(C.Structure):
     _fields_ = [("rays_primary", C.c_uint64), ("rays_shadow", C.c_uint64),
-                ("rays_bounce", C.c_uint64), ("ms", C.c_double)]
+                ("rays_bounce", C.c_uint64), ("ms", C.c_double),
+                ("want_kernel_stats", C.c_uint32), ("reserved", C.c_uint32),
+                ("kernel_ms", C.c_double * YR_K_COUNT), ("kernel_launches", C.c_uint32 * YR_K_COUNT),
+                ("kernel_rays", C.c_uint64 * YR_K_COUNT), ("kernel_nodes", C.c_uint64 * YR_K_COUNT),
+                ("kernel_tests", C.c_uint64 * YR_K_COUNT)]
 
 
 class YrBatchParams(C.Structure):

@@ -1,0 +1,101 @@
+"""Python host interface over the C ABI (include/yr.h).
+
+Mirrors the reference's front door for this path: a scene is assembled from
+meshes, shaders and lights (yafrayInterface_t::addObject_trimesh /
+addLight / addCamera, interface/external.h:144-183), then rendered
+(yafrayInterface_t::render, interface_impl.cc:677-835) or queried ray by ray
+(scene_t::firstHit / isShadowed, scene.cc:107-185, 688-721).  All compute
+runs in the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional
+
+import numpy as np
+
+from . import abi, scenes
+
+
+class DeviceScene:
+    """A scene uploaded to one GPU (yr_scene_create)."""
+
+    def __init__(self, sc: scenes.Scene, device: int = 0):
+        self.lib = abi.load()
+        self.sc = sc
+        self._keep = []
+        objs = (abi.YrObjectDesc * len(sc.meshes))()
+        for i, m in enumerate(sc.meshes):
+            v = np.ascontiguousarray(m.verts, np.float32)
+            t = np.ascontiguousarray(m.tris, np.uint32)
+            self._keep += [v, t]
+            objs[i].verts = v.ctypes.data_as(C.POINTER(C.c_float))
+            objs[i].nverts = v.shape[0]
+            objs[i].tris = t.ctypes.data_as(C.POINTER(C.c_uint32))
+            objs[i].ntris = t.shape[0]
+            objs[i].shader = m.shader & 0xFFFFFFFF
+            objs[i].cast_shadows = 1 if m.cast_shadows else 0
+            if m.shader == abi.YR_PER_TRIANGLE:
+                ts = np.ascontiguousarray(m.tri_shaders, np.uint32)
+                self._keep.append(ts)
+                objs[i].tri_shaders = ts.ctypes.data_as(C.POINTER(C.c_uint32))
+        shaders = (abi.YrShaderDesc * len(sc.shaders))(*sc.shaders)
+        lights = (abi.YrLightDesc * max(1, len(sc.lights)))(*sc.lights)
+        desc = abi.YrSceneDesc()
+        desc.objects = objs
+        desc.nobjects = len(sc.meshes)
+        desc.shaders = shaders
+        desc.nshaders = len(sc.shaders)
+        desc.lights = lights
+        desc.nlights = len(sc.lights)
+        desc.camera = sc.camera
+        desc.render = sc.render
+        self._keep += [objs, shaders, lights, desc]
+        h = C.c_void_p()
+        abi.check(self.lib.yr_scene_create(C.byref(desc), device, C.byref(h)), "yr_scene_create")
+        self.handle = h
+        self._keep = [v for v in self._keep if isinstance(v, np.ndarray)]  # descriptors no longer needed
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.yr_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> abi.YrSceneInfo:
+        inf = abi.YrSceneInfo()
+        abi.check(self.lib.yr_scene_info_get(self.handle, C.byref(inf)), "yr_scene_info_get")
+        return inf
+
+    # ------------------------------------------------------------ rendering
+    def render_into(self, out_ptr: int, on_host: bool = False, stream: int = 0) -> abi.YrRenderStats:
+        st = abi.YrRenderStats()
+        abi.check(self.lib.yr_render(self.handle, C.c_void_p(out_ptr), int(on_host), C.byref(st),
+                                     C.c_void_p(stream)), "yr_render")
+        return st
+
+    def render(self) -> np.ndarray:
+        """Render to a host RGBA float image (resy, resx, 4)."""
+        img = np.zeros((self.sc.resy, self.sc.resx, 4), np.float32)
+        self.last_stats = self.render_into(img.ctypes.data, on_host=True)
+        return img
+
+    def set_params(self, shaders=None, lights=None):
+        sh = (abi.YrShaderDesc * len(shaders))(*shaders) if shaders is not None else None
+        li = (abi.YrLightDesc * len(lights))(*lights) if lights is not None else None
+        abi.check(self.lib.yr_scene_set_params(self.handle, sh, li), "yr_scene_set_params")
+
+
+def trace_closest(ds: DeviceScene, rays_dev_ptr: int, n: int, hits_dev_ptr: int, shadow_only=False, stream=0):
+    abi.check(ds.lib.yr_trace_closest(ds.handle, C.c_void_p(rays_dev_ptr), n, C.c_void_p(hits_dev_ptr),
+                                      int(shadow_only), C.c_void_p(stream)), "yr_trace_closest")
+
+
+def trace_shadow(ds: DeviceScene, rays_dev_ptr: int, n: int, occ_dev_ptr: int, stream=0):
+    abi.check(ds.lib.yr_trace_shadow(ds.handle, C.c_void_p(rays_dev_ptr), n, C.c_void_p(occ_dev_ptr),
+                                     C.c_void_p(stream)), "yr_trace_shadow")

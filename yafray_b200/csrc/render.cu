@@ -17,6 +17,7 @@
 // per-vertex slots, so every sum is formed in the reference's order.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "dev_shade.cuh"
 #include "dev_trace.cuh"
@@ -58,8 +59,29 @@ struct Wave {
     uint32_t *counters;  // [0] shadow queue, [1] bounce queue, [2] next bounce queue,
                          // [3..5] ray totals (primary, shadow, bounce) as 2x u32 lo/hi pairs
     unsigned long long *rays;  // [3] primary, shadow, bounce
+    unsigned long long *kst;   // [YR_K_COUNT][3]: rays, nodes, tests per kernel class
     float *out;          // RGBA image (device)
 };
+
+// warp-reduced traversal counters, one atomic per warp (all lanes must call)
+__device__ __forceinline__ void count_work(const Wave &W, int cls, uint32_t rays, uint32_t nodes, uint32_t tests) {
+    const uint32_t r = __reduce_add_sync(0xffffffffu, rays);
+    const uint32_t n = __reduce_add_sync(0xffffffffu, nodes);
+    const uint32_t t = __reduce_add_sync(0xffffffffu, tests);
+    if ((threadIdx.x & 31) == 0 && r) {
+        atomicAdd(&W.kst[3 * cls + 0], (unsigned long long)r);
+        atomicAdd(&W.kst[3 * cls + 1], (unsigned long long)n);
+        atomicAdd(&W.kst[3 * cls + 2], (unsigned long long)t);
+    }
+}
+
+// camera sample cs -> image pixel (row-major index) inside the region
+__device__ __forceinline__ uint32_t cs_pixel(const DevRender &R, uint32_t cs, int &x, int &y) {
+    const uint32_t lp = cs / R.spp;
+    x = R.rx0 + (int)(lp % (uint32_t)R.rw);
+    y = R.ry0 + (int)(lp / (uint32_t)R.rw);
+    return (uint32_t)y * (uint32_t)R.cam.resx + (uint32_t)x;
+}
 
 // ---------------------------------------------------------------- camera
 // camera_t::shootRay, CM_PERSPECTIVE (camera.cc:184-188)
@@ -113,16 +135,21 @@ __global__ void __launch_bounds__(kBlock) k_primary(DevScene S, DevRender R, Wav
     uint4 stack[kMaxKdStack];
     const KdStack stk{stack, 1, kMaxKdStack};
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= W.count) return;
-    const uint32_t cs = W.base + i;
-    const uint32_t pixel = cs / R.spp, s = cs % R.spp;
-    const int x = (int)(pixel % (uint32_t)R.cam.resx), y = (int)(pixel / (uint32_t)R.cam.resx);
-    float fx, fy;
-    sample_pos(R, pixel, s, fx, fy);
-    const V3 ray = camera_ray(R.cam, (float)x + fx, (float)y + fy);
-    const V3 f = R.cam.pos + ray * kMinRayDist;  // scene.cc:211
-    const SceneHit h = scene_closest(S, f, ray, true, false, stk);
-    W.hit0[i] = make_float4(h.t, __int_as_float(h.object), __uint_as_float(h.tri), 0.f);
+    uint32_t nodes = 0, tests = 0;
+    if (i < W.count) {
+        const uint32_t cs = W.base + i;
+        int x, y;
+        const uint32_t pixel = cs_pixel(R, cs, x, y), s = cs % R.spp;
+        float fx, fy;
+        sample_pos(R, pixel, s, fx, fy);
+        const V3 ray = camera_ray(R.cam, (float)x + fx, (float)y + fy);
+        const V3 f = R.cam.pos + ray * kMinRayDist;  // scene.cc:211
+        const SceneHit h = scene_closest(S, f, ray, true, false, stk);
+        W.hit0[i] = make_float4(h.t, __int_as_float(h.object), __uint_as_float(h.tri), 0.f);
+        nodes = h.nodes;
+        tests = h.tests;
+    }
+    count_work(W, YR_K_PRIMARY, i < W.count ? 1u : 0u, nodes, tests);
 }
 
 // per-light sampling at one shading vertex; writes slots, aux and queue
@@ -317,7 +344,8 @@ __global__ void __launch_bounds__(kBlock) k_shade_camera(DevScene S, DevRender R
     if (i >= W.count && (i & ~31u) >= W.count) return;  // whole warps past the end leave
     const bool inb = i < W.count;
     const uint32_t cs = W.base + (inb ? i : 0);
-    const uint32_t pixel = cs / R.spp, s = cs % R.spp;
+    int x, y;
+    const uint32_t pixel = cs_pixel(R, cs, x, y), s = cs % R.spp;
     bool active = false;
     Surf sp;
     V3 eye = v3(0.f, 0.f, 0.f);
@@ -325,7 +353,6 @@ __global__ void __launch_bounds__(kBlock) k_shade_camera(DevScene S, DevRender R
         const float4 h = W.hit0[i];
         const int obj = __float_as_int(h.y);
         if (obj >= 0) {
-            const int x = (int)(pixel % (uint32_t)R.cam.resx), y = (int)(pixel / (uint32_t)R.cam.resx);
             float fx, fy;
             sample_pos(R, pixel, s, fx, fy);
             const V3 ray = camera_ray(R.cam, (float)x + fx, (float)y + fy);
@@ -373,13 +400,15 @@ __global__ void __launch_bounds__(kBlock) k_trace_shadow_q(DevScene S, Wave W, f
     uint4 stack[kMaxKdStack];
     const KdStack stk{stack, 1, kMaxKdStack};
     const uint32_t n = W.counters[0];
+    uint32_t rays = 0, nodes = 0, tests = 0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const float4 a = W.shq0[q], b = W.shq1[q];
-        uint32_t nodes = 0, tests = 0;
         const bool occ = scene_occluded(S, v3(a.x, a.y, a.z), __float_as_int(a.w), v3(b.x, b.y, b.z), b.w,
                                         self_bias, stk, nodes, tests);
         W.slot_f[W.shq_slot[q]] = occ ? kSlotShadowed : kSlotLit;
+        rays++;
     }
+    count_work(W, YR_K_SHADOW, rays, nodes, tests);
 }
 
 __global__ void __launch_bounds__(kBlock) k_gather_camera(DevRender R, Wave W) {
@@ -401,6 +430,7 @@ __global__ void __launch_bounds__(kBlock) k_trace_bounce(DevScene S, Wave W) {
     uint4 stack[kMaxKdStack];
     const KdStack stk{stack, 1, kMaxKdStack};
     const uint32_t n = W.counters[1];
+    uint32_t rays = 0, nodes = 0, tests = 0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const uint32_t p = W.bq[q];
         const float4 wh = W.p_where[p], rr = W.p_ray[p];
@@ -408,7 +438,11 @@ __global__ void __launch_bounds__(kBlock) k_trace_bounce(DevScene S, Wave W) {
         const V3 f = v3(wh.x, wh.y, wh.z) + ray * kMinRayDist;  // scene.cc:693
         const SceneHit h = scene_closest(S, f, ray, false, true, stk);
         W.p_hit[p] = make_float4(h.t, __int_as_float(h.object), __uint_as_float(h.tri), 0.f);
+        rays++;
+        nodes += h.nodes;
+        tests += h.tests;
     }
+    count_work(W, YR_K_BOUNCE, rays, nodes, tests);
 }
 
 // shading at bounce vertex j (pathlight.cc:313-346): light samples, next
@@ -421,7 +455,8 @@ __global__ void __launch_bounds__(kBlock) k_shade_path(DevScene S, DevRender R, 
     const uint32_t p = inq ? W.bq[q] : 0;
     const uint32_t i = p / W.npath, pi = p % W.npath;
     const uint32_t cs = W.base + i;
-    const uint32_t pixel = cs / R.spp, s = cs % R.spp;
+    int px_x, px_y;
+    const uint32_t pixel = cs_pixel(R, cs, px_x, px_y), s = cs % R.spp;
     bool active = false;
     Surf sp;
     V3 eye = v3(0.f, 0.f, 0.f), ray = v3(0.f, 0.f, 1.f);
@@ -558,7 +593,8 @@ __global__ void __launch_bounds__(kBlock) k_finish(DevRender R, Wave W) {
         const float d = (float)(1 + (R.spp - 1));
         o = make_float4((first.x + tot.x) / d, (first.y + tot.y) / d, (first.z + tot.z) / d, (first.w + tot.w) / d);
     }
-    const uint32_t pixel = W.base / R.spp + px;
+    int x, y;
+    const uint32_t pixel = cs_pixel(R, W.base + px * R.spp, x, y);
     reinterpret_cast<float4 *>(W.out)[pixel] = o;
 }
 
@@ -607,8 +643,9 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
     cudaSetDevice(scene->device);
     cudaStream_t st = (cudaStream_t)stream;
     DevRender &R = scene->rdr;
-    const uint32_t npix = (uint32_t)R.cam.resx * (uint32_t)R.cam.resy;
-    const uint64_t total = (uint64_t)npix * R.spp;
+    const uint32_t npix = (uint32_t)R.cam.resx * (uint32_t)R.cam.resy;  // image
+    const uint32_t rpix = (uint32_t)R.rw * (uint32_t)R.rh;              // region
+    const uint64_t total = (uint64_t)rpix * R.spp;
     yr_status ret = YR_OK;
     auto done = [&](yr_status e) {
         cudaSetDevice(prev);
@@ -625,7 +662,7 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
     // wave: whole pixels, bounded so that the slot arrays stay near 1.5 GB
     const uint64_t per_cs = (uint64_t)std::max<uint32_t>(1, std::max(1u, npath)) * std::max(ns, 1u) * 64 + 512;
     uint64_t wave_px = std::max<uint64_t>(1, (1536ull << 20) / (per_cs * R.spp));
-    wave_px = std::min<uint64_t>(wave_px, npix);
+    wave_px = std::min<uint64_t>(wave_px, rpix);
     const uint32_t wcap = (uint32_t)(wave_px * R.spp);
     const uint32_t nl = std::max(1, R.nlights);
     const uint32_t pcap = wcap * std::max(1u, npath);
@@ -662,6 +699,7 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
     YR_SCRATCH(bq2, sizeof(uint32_t) * pcap);
     YR_SCRATCH(counters, sizeof(uint32_t) * 8);
     YR_SCRATCH(rays, sizeof(unsigned long long) * 4);
+    YR_SCRATCH(kst, sizeof(unsigned long long) * 3 * YR_K_COUNT);
 #undef YR_SCRATCH
     float *out = rgba;
     if (rgba_on_host) {
@@ -671,58 +709,97 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
     W.out = out;
     W.ns = ns;
     W.npath = npath;
+    const bool kstats = stats && stats->want_kernel_stats;
+    double kms[YR_K_COUNT] = {0};
+    uint32_t klaunch[YR_K_COUNT] = {0};
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> kev;
+    auto timed = [&](int cls, auto &&launch) {
+        klaunch[cls]++;
+        if (!kstats) {
+            launch();
+            return;
+        }
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, st);
+        launch();
+        cudaEventRecord(b, st);
+        kev.push_back({cls, {a, b}});
+    };
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st);
     cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
+    cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
+    // pixels outside the region are written as 0 (scene.cc:773)
+    if (rpix != npix) cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)npix, st);
     if (R.raydepth <= 0) {
         // raytrace() returns black at the ray-level cap (scene.cc:204-209)
         cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)npix, st);
     } else {
         const int gq = grid_for(vcap * std::max(ns, 1u), kBlock);
+        const DevScene &D = scene->dev;
         for (uint64_t b = 0; b < total; b += wcap) {
             W.base = (uint32_t)b;
             W.count = (uint32_t)std::min<uint64_t>(wcap, total - b);
             const int g = (int)((W.count + kBlock - 1) / kBlock);
             cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
-            k_primary<<<g, kBlock, 0, st>>>(scene->dev, R, W);
-            k_shade_camera<<<g, kBlock, 0, st>>>(scene->dev, R, W);
-            k_count<<<1, 1, 0, st>>>(W, 0);
-            k_trace_shadow_q<<<gq, kBlock, 0, st>>>(scene->dev, W, R.self_bias);
-            k_gather_camera<<<g, kBlock, 0, st>>>(R, W);
+            timed(YR_K_PRIMARY, [&] { k_primary<<<g, kBlock, 0, st>>>(D, R, W); });
+            timed(YR_K_SHADE_CAMERA, [&] { k_shade_camera<<<g, kBlock, 0, st>>>(D, R, W); });
+            timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
+            timed(YR_K_SHADOW, [&] { k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+            timed(YR_K_GATHER, [&] { k_gather_camera<<<g, kBlock, 0, st>>>(R, W); });
             if (npath > 0) {
                 const size_t nc = (size_t)W.count * npath * depth;
-                k_clear_contri<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(W, nc);
+                timed(YR_K_OTHER, [&] {
+                    k_clear_contri<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(W, nc);
+                });
                 const int gp = (int)(((size_t)W.count * npath + kBlock - 1) / kBlock);
                 for (int j = 0; j < R.path_depth; j++) {
-                    k_count<<<1, 1, 0, st>>>(W, 1);
-                    k_trace_bounce<<<gq, kBlock, 0, st>>>(scene->dev, W);
+                    timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 1); });
+                    timed(YR_K_BOUNCE, [&] { k_trace_bounce<<<gq, kBlock, 0, st>>>(D, W); });
                     cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
-                    k_shade_path<<<gp, kBlock, 0, st>>>(scene->dev, R, W, j);
-                    k_count<<<1, 1, 0, st>>>(W, 0);
-                    k_trace_shadow_q<<<gq, kBlock, 0, st>>>(scene->dev, W, R.self_bias);
-                    k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background);
+                    timed(YR_K_SHADE_PATH, [&] { k_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j); });
+                    timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
+                    timed(YR_K_SHADOW, [&] { k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+                    timed(YR_K_GATHER, [&] { k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background); });
                     std::swap(W.bq, W.bq2);
-                    k_swap_queues<<<1, 1, 0, st>>>(W);
+                    timed(YR_K_OTHER, [&] { k_swap_queues<<<1, 1, 0, st>>>(W); });
                 }
             }
             const int gf = (int)((W.count / R.spp + kBlock - 1) / kBlock);
-            k_finish<<<gf, kBlock, 0, st>>>(R, W);
+            timed(YR_K_OTHER, [&] { k_finish<<<gf, kBlock, 0, st>>>(R, W); });
         }
     }
     cudaEventRecord(e1, st);
     if (cudaGetLastError() != cudaSuccess) return done(YR_ERR_CUDA);
     if ((ret = take_status(scene, st)) != YR_OK) return done(ret);
     if (stats) {
-        unsigned long long r[4] = {0, 0, 0, 0};
+        unsigned long long r[4] = {0, 0, 0, 0}, k[3 * YR_K_COUNT];
         cudaMemcpy(r, W.rays, sizeof(r), cudaMemcpyDeviceToHost);
+        cudaMemcpy(k, W.kst, sizeof(k), cudaMemcpyDeviceToHost);
         stats->rays_primary = (R.raydepth > 0) ? total : 0;
         stats->rays_shadow = r[1];
         stats->rays_bounce = r[2];
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         stats->ms = ms;
+        for (auto &e : kev) {
+            float m = 0.f;
+            cudaEventElapsedTime(&m, e.second.first, e.second.second);
+            kms[e.first] += m;
+            cudaEventDestroy(e.second.first);
+            cudaEventDestroy(e.second.second);
+        }
+        for (int c = 0; c < YR_K_COUNT; c++) {
+            stats->kernel_ms[c] = kms[c];
+            stats->kernel_launches[c] = klaunch[c];
+            stats->kernel_rays[c] = k[3 * c];
+            stats->kernel_nodes[c] = k[3 * c + 1];
+            stats->kernel_tests[c] = k[3 * c + 2];
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -1,5 +1,8 @@
 // yr_scene_create / yr_scene_destroy: host flattening and device upload.
+#include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -263,17 +266,45 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         if (od.ntris == 0 || !od.verts || !od.tris) return fail(YR_ERR_EMPTY_SCENE);
         if (od.shader != YR_PER_TRIANGLE && od.shader >= desc->nshaders) return fail(YR_ERR_INVALID_ARG);
         if (od.shader == YR_PER_TRIANGLE && !od.tri_shaders) return fail(YR_ERR_INVALID_ARG);
-        KdTree tree;
-        if (od.tree) {
-            tree.nodes.assign(od.tree->nodes, od.tree->nodes + od.tree->nnodes);
-            tree.prims.assign(od.tree->prims, od.tree->prims + od.tree->nprims);
-            std::memcpy(tree.bound.a, od.tree->bound, 12);
-            std::memcpy(tree.bound.g, od.tree->bound + 3, 12);
-            tree.max_depth = od.tree->max_depth;
-        } else {
-            st = build_kdtree(od.verts, od.nverts, od.tris, od.ntris, tree);
-            if (st != YR_OK) return fail(st);
-        }
+    }
+    // kd-trees of different objects are independent: build them on all host
+    // cores (each tree is the same as a sequential build)
+    std::vector<KdTree> trees(desc->nobjects);
+    std::vector<yr_status> tree_st(desc->nobjects, YR_OK);
+    {
+        std::atomic<uint32_t> next{0};
+        auto worker = [&] {
+            for (;;) {
+                const uint32_t o = next.fetch_add(1);
+                if (o >= desc->nobjects) return;
+                const yr_object_desc &od = desc->objects[o];
+                KdTree &tree = trees[o];
+                try {
+                    if (od.tree) {
+                        tree.nodes.assign(od.tree->nodes, od.tree->nodes + od.tree->nnodes);
+                        tree.prims.assign(od.tree->prims, od.tree->prims + od.tree->nprims);
+                        std::memcpy(tree.bound.a, od.tree->bound, 12);
+                        std::memcpy(tree.bound.g, od.tree->bound + 3, 12);
+                        tree.max_depth = od.tree->max_depth;
+                    } else {
+                        tree_st[o] = build_kdtree(od.verts, od.nverts, od.tris, od.ntris, tree);
+                    }
+                } catch (const std::bad_alloc &) {
+                    tree_st[o] = YR_ERR_OUT_OF_MEMORY;
+                }
+            }
+        };
+        unsigned nth = std::thread::hardware_concurrency();
+        nth = std::max(1u, std::min(nth ? nth : 1u, desc->nobjects));
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nth; t++) pool.emplace_back(worker);
+        worker();
+        for (std::thread &t : pool) t.join();
+    }
+    for (uint32_t o = 0; o < desc->nobjects; o++) {
+        const yr_object_desc &od = desc->objects[o];
+        if (tree_st[o] != YR_OK) return fail(tree_st[o]);
+        KdTree tree = std::move(trees[o]);
         if (tree.max_depth > s->max_tree_depth) s->max_tree_depth = tree.max_depth;
         const uint32_t tri_base = (uint32_t)(tris.size() / 3);
         const uint32_t node_base = (uint32_t)nodes.size();
@@ -398,6 +429,23 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     R.self_bias = desc->render.self_bias;
     R.raydepth = desc->render.raydepth;
     R.background = c3(desc->render.background[0], desc->render.background[1], desc->render.background[2]);
+    {
+        const int32_t *rg = desc->render.region;
+        if (rg[0] == 0 && rg[1] == 0 && rg[2] == 0 && rg[3] == 0) {
+            R.rx0 = 0;
+            R.ry0 = 0;
+            R.rw = desc->camera.resx;
+            R.rh = desc->camera.resy;
+        } else {
+            if (rg[0] < 0 || rg[1] > desc->camera.resx || rg[0] >= rg[1] || rg[2] < 0 || rg[3] > desc->camera.resy ||
+                rg[2] >= rg[3])
+                return fail(YR_ERR_INVALID_ARG);
+            R.rx0 = rg[0];
+            R.ry0 = rg[2];
+            R.rw = rg[1] - rg[0];
+            R.rh = rg[3] - rg[2];
+        }
+    }
     R.path_light = -1;
     for (int i = 0; i < R.nlights; i++)
         if (s->lights[i].type == YR_LIGHT_PATH) {

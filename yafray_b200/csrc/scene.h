@@ -59,6 +59,7 @@ struct DevRender {
     float self_bias;
     int raydepth;
     C3 background;
+    int rx0, ry0, rw, rh;       // pixel region (x0, y0, width, height)
     int path_light;             // index of the path light or -1
     int path_samples;
     int path_depth;

@@ -36,31 +36,29 @@ from . import abi
 def uv_sphere(center=(0.0, 0.0, 0.0), radius=1.0, rings=64, segments=128):
     """Vertices (float32 [V,3]) and triangles (uint32 [T,3]) of a UV sphere."""
     cx, cy, cz = center
-    verts = [(cx, cy + radius, cz)]
-    for k in range(1, rings):
-        th = math.pi * k / rings
-        y, rr = math.cos(th), math.sin(th)
-        for s in range(segments):
-            ph = 2.0 * math.pi * s / segments
-            verts.append((cx + radius * rr * math.cos(ph), cy + radius * y, cz + radius * rr * math.sin(ph)))
-    verts.append((cx, cy - radius, cz))
-    south = len(verts) - 1
+    k = np.arange(1, rings, dtype=np.float64)
+    th = np.pi * k / rings
+    ph = 2.0 * np.pi * np.arange(segments, dtype=np.float64) / segments
+    y = np.cos(th)[:, None] * np.ones_like(ph)[None, :]
+    rr = np.sin(th)[:, None]
+    ring_v = np.stack([cx + radius * rr * np.cos(ph)[None, :], cy + radius * y,
+                       cz + radius * rr * np.sin(ph)[None, :]], -1).reshape(-1, 3)
+    verts = np.concatenate([[[cx, cy + radius, cz]], ring_v, [[cx, cy - radius, cz]]])
+    south = verts.shape[0] - 1
+    s = np.arange(segments)
+    s1 = (s + 1) % segments
 
-    def ring(k, s):  # k in 1..rings-1
-        return 1 + (k - 1) * segments + (s % segments)
+    def ring(kk, ss):  # kk in 1..rings-1
+        return 1 + (kk - 1) * segments + ss
 
-    tris = []
-    for s in range(segments):  # north fan, outward winding
-        tris.append((0, ring(1, s + 1), ring(1, s)))
-    for k in range(1, rings - 1):
-        for s in range(segments):
-            a, b = ring(k, s), ring(k, s + 1)
-            c, d = ring(k + 1, s), ring(k + 1, s + 1)
-            tris.append((a, b, d))
-            tris.append((a, d, c))
-    for s in range(segments):
-        tris.append((south, ring(rings - 1, s), ring(rings - 1, s + 1)))
-    return np.asarray(verts, dtype=np.float32), np.asarray(tris, dtype=np.uint32)
+    north = np.stack([np.zeros(segments, np.int64), ring(1, s1), ring(1, s)], -1)
+    kk = np.arange(1, rings - 1)[:, None]
+    a, b = ring(kk, s[None, :]), ring(kk, s1[None, :])
+    c, d = ring(kk + 1, s[None, :]), ring(kk + 1, s1[None, :])
+    band = np.stack([np.stack([a, b, d], -1), np.stack([a, d, c], -1)], 2).reshape(-1, 3)
+    southf = np.stack([np.full(segments, south), ring(rings - 1, s), ring(rings - 1, s1)], -1)
+    tris = np.concatenate([north, band, southf])
+    return verts.astype(np.float32), tris.astype(np.uint32)
 
 
 def torus(center, R, r, nu=64, nv=32):
