@@ -89,3 +89,14 @@ def test_empty_query(cuda):
     sc = scenes.config_small(32, 24)
     ds = api.DeviceScene(sc)
     assert _run_closest(cuda, ds, np.zeros((0, 8), np.float32)).shape == (0, 4)
+
+
+def test_reciprocal_division_is_exact(cuda):
+    """The slab tests' reciprocal + Markstein-correction division returns the
+    IEEE quotient bit for bit (200 M operand pairs)."""
+    import ctypes as C
+    from yafray_b200 import abi
+    lib = abi.load()
+    bad = C.c_uint64(123)
+    abi.check(lib.yr_selftest_division(200_000_000, 12345, C.byref(bad)), "yr_selftest_division")
+    assert bad.value == 0

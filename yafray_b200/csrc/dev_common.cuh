@@ -15,8 +15,7 @@ namespace yr {
 
 constexpr float kMinRayDist = 0.00005f;     // MIN_RAYDIST (configio.py:8-11)
 constexpr uint32_t kNone = 0xffffffffu;
-constexpr int kMaxKdStack = 64;             // MAX_STACK (kdtree.cc:603)
-constexpr int kMaxObjStack = 64;
+constexpr int kMaxObjStack = 32;            // object-tree depth cap (checked at scene creation)
 constexpr uint32_t kMaxLeafVisits = 1u << 22;  // iteration cap per ray
 
 // device status word bits (first error wins; read back after each launch)
@@ -112,7 +111,6 @@ struct DevScene {
     uint32_t nnodes;
     uint32_t nprims;
     uint32_t notree;
-    int32_t kd_stack;           // stack entries needed (max tree depth + 3, <= 64)
     int *status;                // device status word
 };
 

@@ -10,28 +10,64 @@
 
 namespace yr {
 
+// a/b rounded to nearest, given y = RN(1/b): one correction step of
+// Markstein's method (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. R&D 34(1), 1990; Theorem 4.10
+// of the Handbook of Floating-Point Arithmetic): with q0 = RN(a*y) within
+// one ulp of a/b and r = a - b*q0 exact through an FMA, RN(q0 + r*y) is the
+// correctly rounded quotient.  The slab tests divide by the same three ray
+// components many times per ray, so the three reciprocals are formed once
+// (with IEEE division) and every quotient costs a multiply and two FMAs on
+// the FMA pipe instead of a MUFU-based division.  Operands outside
+// [2^-60, 2^60] (where an intermediate could leave the normal range) take
+// the IEEE division; a zero dividend returns the correctly signed zero.
+__device__ __forceinline__ float div_rcp(float a, float b, float y) {
+    const float q0 = __fmul_rn(a, y);
+    if (a == 0.f) return q0;
+    const float aa = fabsf(a), ab = fabsf(b);
+    if (aa < 0x1p-60f || aa > 0x1p60f || ab < 0x1p-60f || ab > 0x1p60f) return __fdiv_rn(a, b);
+    const float r = __fmaf_rn(-q0, b, a);
+    return __fmaf_rn(r, y, q0);
+}
+
+// A ray with the reciprocals of its direction (1.f/d, correctly rounded,
+// which is also kdTree_t::Intersect's invDir: 1.0/d in double narrowed to
+// float rounds to the same value).
+struct RayR {
+    V3 d;
+    V3 inv;
+};
+
+__device__ __forceinline__ RayR make_rayr(const V3 &d) {
+    RayR r;
+    r.d = d;
+    r.inv = v3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+    return r;
+}
+
 // bound_t::cross(from, ray, enter, leave, dist) (bound.cc:389-436) as the
 // shipped build evaluates it (fast-math: (g - from)/ray instead of
 // ((g - a) - (from - a))/ray).
 __device__ __forceinline__ bool box_enter_leave(const float *bmin, const float *bmax, const V3 &from,
-                                                const V3 &ray, float dist, float &enter, float &leave) {
+                                                const RayR &R, float dist, float &enter, float &leave) {
     float lmin = -1.f, lmax = -1.f;
+    const V3 &ray = R.d;
     if (ray.x != 0.f) {
-        float t1 = (bmin[0] - from.x) / ray.x, t2 = (bmax[0] - from.x) / ray.x;
+        float t1 = div_rcp(bmin[0] - from.x, ray.x, R.inv.x), t2 = div_rcp(bmax[0] - from.x, ray.x, R.inv.x);
         if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
         lmin = t1;
         lmax = t2;
         if ((lmax < 0.f) || (lmin > dist)) return false;
     }
     if (ray.y != 0.f) {
-        float t1 = (bmin[1] - from.y) / ray.y, t2 = (bmax[1] - from.y) / ray.y;
+        float t1 = div_rcp(bmin[1] - from.y, ray.y, R.inv.y), t2 = div_rcp(bmax[1] - from.y, ray.y, R.inv.y);
         if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
         if (t1 > lmin) lmin = t1;
         if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;
         if ((lmax < 0.f) || (lmin > dist)) return false;
     }
     if (ray.z != 0.f) {
-        float t1 = (bmin[2] - from.z) / ray.z, t2 = (bmax[2] - from.z) / ray.z;
+        float t1 = div_rcp(bmin[2] - from.z, ray.z, R.inv.z), t2 = div_rcp(bmax[2] - from.z, ray.z, R.inv.z);
         if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
         if (t1 > lmin) lmin = t1;
         if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;
@@ -45,10 +81,10 @@ __device__ __forceinline__ bool box_enter_leave(const float *bmin, const float *
 }
 
 // bound_t::cross(from, ray, where, dist) (bound.cc:340-387): where = max(enter, 0)
-__device__ __forceinline__ bool box_where(const float *bmin, const float *bmax, const V3 &from, const V3 &ray,
+__device__ __forceinline__ bool box_where(const float *bmin, const float *bmax, const V3 &from, const RayR &R,
                                           float dist, float &where) {
     float e, l;
-    if (!box_enter_leave(bmin, bmax, from, ray, dist, e, l)) return false;
+    if (!box_enter_leave(bmin, bmax, from, R, dist, e, l)) return false;
     where = (e > 0.f) ? e : 0.f;
     return true;
 }
@@ -83,29 +119,34 @@ __device__ __forceinline__ bool tri_hit(const Tri &tr, const V3 &from, const V3 
     return true;
 }
 
-// Per-thread kd stack entry: far child, signed distance of the exit point,
-// the split plane that produced it, and the link to the previous exit.  The
-// exit point's coordinates are recomputed from (t, split, axis) exactly as
-// they were first computed, so 16 bytes replace KdStack's 24.
+// Per-thread kd stack.  kdTree_t keeps exit points in an array linked by
+// `prev` indices and protects the current entry slot (kdtree.cc:606-624,
+// 660-676, 720-723); the links always form a last-in first-out chain whose
+// head is the current exit, so a plain stack of exits reproduces it: push a
+// far child's exit, and on leaving a leaf the head becomes the entry point
+// and the next exit is the new head.  The current exit point lives in
+// registers; an entry keeps (far node | axis << 30, t) and the split, from
+// which the exit point is recomputed exactly as it was first computed.
+// Capacity: one entry per level of the deepest tree plus the initial exit.
+constexpr int kKdStackCap = 66;
+
 struct KdStack {
-    uint4 *e;     // entries, strided by `stride` (one column per thread)
-    int stride;
-    int cap;
-    __device__ __forceinline__ uint4 &at(int i) const { return e[(size_t)i * stride]; }
+    uint2 *nt;     // far node | axis << 30, bits of t
+    float *split;
 };
 
-__device__ __forceinline__ void exit_point(const uint4 &en, const V3 &from, const V3 &ray, float *pb) {
-    const float t = __uint_as_float(en.y);
-    const int axis = (int)((en.w >> 8) & 3u);
-    if (axis == 3) {  // initial exit: from + ray*t on every axis
-        pb[0] = from.x + t * ray.x;
-        pb[1] = from.y + t * ray.y;
-        pb[2] = from.z + t * ray.z;
+__device__ __forceinline__ void exit_point(uint32_t node_axis, float t, float split, const float *fr,
+                                           const float *rr, float *pb) {
+    const uint32_t axis = node_axis >> 30;
+    if (axis == 3u) {  // initial exit: from + ray*t on every axis
+        pb[0] = fr[0] + t * rr[0];
+        pb[1] = fr[1] + t * rr[1];
+        pb[2] = fr[2] + t * rr[2];
     } else {
-        const int na = axis == 2 ? 0 : axis + 1, pa = axis == 0 ? 2 : axis - 1;
-        pb[axis] = __uint_as_float(en.z);
-        pb[na] = comp(from, na) + t * comp(ray, na);
-        pb[pa] = comp(from, pa) + t * comp(ray, pa);
+        const int ax = (int)axis, na = ax == 2 ? 0 : ax + 1, pa = ax == 0 ? 2 : ax - 1;
+        pb[ax] = split;
+        pb[na] = fr[na] + t * rr[na];
+        pb[pa] = fr[pa] + t * rr[pa];
     }
 }
 
@@ -115,20 +156,21 @@ struct KdResult {
     uint32_t tests;   // triangle tests
 };
 
+constexpr uint32_t kNodeMask = 0x3fffffffu;
+
 // kdTree_t::Intersect (kdtree.cc:591-727, ANY=false) and IntersectS
 // (kdtree.cc:730-866, ANY=true).  Z is in/out (closest hit only).
 template <bool ANY>
-__device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V3 &from, const V3 &ray, float dist,
-                         float &Z, KdResult &res, const KdStack &stk) {
+__device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V3 &from, const RayR &R, float dist,
+                                float &Z, KdResult &res, const KdStack &stk) {
     float a, b;
-    if (!box_enter_leave(obj.tb, obj.tb + 3, from, ray, dist, a, b)) return false;
-    // 1.0/ray in double narrowed to float == 1.f/ray (both correctly rounded)
-    const float inv[3] = {1.f / ray.x, 1.f / ray.y, 1.f / ray.z};
+    if (!box_enter_leave(obj.tb, obj.tb + 3, from, R, dist, a, b)) return false;
+    const V3 &ray = R.d;
+    const float inv[3] = {R.inv.x, R.inv.y, R.inv.z};
     const float fr[3] = {from.x, from.y, from.z};
     const float rr[3] = {ray.x, ray.y, ray.z};
     bool hit = false;
     uint32_t curr = obj.root;
-    int en = 0, ex = 1;
     float en_t = a, en_pb[3];
     if (a >= 0.f) {
         en_pb[0] = fr[0] + a * rr[0];
@@ -143,9 +185,11 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
     ex_pb[0] = fr[0] + b * rr[0];
     ex_pb[1] = fr[1] + b * rr[1];
     ex_pb[2] = fr[2] + b * rr[2];
-    stk.at(1) = make_uint4(kNone, __float_as_uint(b), 0u, (3u << 8));
+    // stack[0] = initial exit (no node); sp = number of exits on the stack
+    stk.nt[0] = make_uint2(kNodeMask | (3u << 30), __float_as_uint(b));
+    int sp = 1;
     uint32_t leaves = 0;
-    while (curr != kNone) {
+    while (curr != kNodeMask) {
         if (dist < en_t) break;
         if (++leaves > kMaxLeafVisits) {
             dev_fail(S.status, kDevIterationCap);
@@ -184,15 +228,13 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
                 curr = right;
             }
             const float t = (split - fr[axis]) * inv[axis];
-            const int tmp = ex;
-            ex++;
-            if (ex == en) ex++;
-            if (ex >= stk.cap) {
+            if (sp >= kKdStackCap) {
                 dev_fail(S.status, kDevStackOverflow);
                 return false;
             }
-            stk.at(ex) = make_uint4(far_child, __float_as_uint(t), __float_as_uint(split),
-                                    (uint32_t)tmp | ((uint32_t)axis << 8));
+            stk.nt[sp] = make_uint2(far_child | ((uint32_t)axis << 30), __float_as_uint(t));
+            stk.split[sp] = split;
+            sp++;
             const int na = axis == 2 ? 0 : axis + 1, pa = axis == 0 ? 2 : axis - 1;
             ex_t = t;
             ex_pb[axis] = split;
@@ -226,19 +268,17 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             }
         }
         if (!ANY && hit && Z <= ex_t) return true;
-        // pop: the exit point becomes the entry point
-        en = ex;
+        // the exit point becomes the entry point; descend into its far node
         en_t = ex_t;
         en_pb[0] = ex_pb[0];
         en_pb[1] = ex_pb[1];
         en_pb[2] = ex_pb[2];
-        const uint4 top = stk.at(ex);
-        curr = top.x;
-        ex = (int)(top.w & 0xffu);
-        if (curr != kNone) {
-            const uint4 nx = stk.at(ex);
+        sp--;
+        curr = stk.nt[sp].x & kNodeMask;
+        if (curr != kNodeMask) {
+            const uint2 nx = stk.nt[sp - 1];
             ex_t = __uint_as_float(nx.y);
-            exit_point(nx, from, ray, ex_pb);
+            exit_point(nx.x, ex_t, stk.split[sp - 1], fr, rr, ex_pb);
         }
     }
     return hit;
@@ -247,12 +287,12 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
 // geomeIterator_t (geometree.h:36-157) in its front-to-back mode: yields
 // objects whose bound the ray crosses before `maximun`, nearest entry first.
 struct ObjIter {
-    int2 st[kMaxObjStack];   // (node, bits of the entry distance)
+    int2 st[kMaxObjStack];   // (node, bits of the entry distance)  (host checks the tree depth)
     int sp;
     int current;             // object index or -1
     float maximun;
 
-    __device__ __forceinline__ void down(const DevScene &S, int node, const V3 &from, const V3 &ray) {
+    __device__ __forceinline__ void down(const DevScene &S, int node, const V3 &from, const RayR &ray) {
         for (;;) {
             const DevObjNode nd = S.otree[node];
             if (nd.left < 0) {
@@ -286,7 +326,7 @@ struct ObjIter {
         }
     }
 
-    __device__ __forceinline__ void start(const DevScene &S, const V3 &from, const V3 &ray, float maxd) {
+    __device__ __forceinline__ void start(const DevScene &S, const V3 &from, const RayR &ray, float maxd) {
         maximun = maxd;
         sp = 0;
         current = -1;
@@ -296,7 +336,7 @@ struct ObjIter {
         if (box_where(r.bmin, r.bmax, from, ray, maximun, w)) down(S, 0, from, ray);
     }
 
-    __device__ __forceinline__ void next(const DevScene &S, const V3 &from, const V3 &ray) {
+    __device__ __forceinline__ void next(const DevScene &S, const V3 &from, const RayR &ray) {
         current = -1;
         while (sp > 0 && __int_as_float(st[sp - 1].y) > maximun) sp--;
         if (sp > 0) {
@@ -323,8 +363,9 @@ struct SceneHit {
 //                       is shot with the current closest distance
 //   pass_limit = false: scene_t::firstHit (scene.cc:688-707)
 //   shadow_only: skip objects that do not cast shadows (firstHit's shadow arg)
-__device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V3 &ray, bool pass_limit, bool shadow_only,
-                                  const KdStack &stk) {
+__device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V3 &dir, bool pass_limit,
+                                         bool shadow_only, const KdStack &stk) {
+    const RayR ray = make_rayr(dir);
     SceneHit best;
     best.t = 0.f;
     best.object = -1;
@@ -362,10 +403,11 @@ __device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V
 
 // scene_t::isShadowed (scene.cc:107-185).  p: shading point, own: its
 // object, ray: unit direction, dist: |l - p| (or infinity).
-__device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &ray, float dist, float self_bias,
-                               const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
-    const V3 self = p + ray * self_bias;
-    const V3 p2 = p + ray * kMinRayDist;
+__device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
+                                      float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+    const V3 self = p + dir * self_bias;
+    const V3 p2 = p + dir * kMinRayDist;
+    const RayR ray = make_rayr(dir);
     ObjIter it;
     it.start(S, p2, ray, dist);
     while (it.current >= 0) {

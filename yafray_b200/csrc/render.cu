@@ -132,8 +132,9 @@ __device__ __forceinline__ void emit_shadow(const Wave &W, bool pred, const V3 &
 
 // --------------------------------------------------------------- kernels
 __global__ void __launch_bounds__(kBlock) k_primary(DevScene S, DevRender R, Wave W) {
-    uint4 stack[kMaxKdStack];
-    const KdStack stk{stack, 1, kMaxKdStack};
+    uint2 stk_nt[kKdStackCap];
+    float stk_split[kKdStackCap];
+    const KdStack stk{stk_nt, stk_split};
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t nodes = 0, tests = 0;
     if (i < W.count) {
@@ -397,8 +398,9 @@ __global__ void __launch_bounds__(kBlock) k_shade_camera(DevScene S, DevRender R
 }
 
 __global__ void __launch_bounds__(kBlock) k_trace_shadow_q(DevScene S, Wave W, float self_bias) {
-    uint4 stack[kMaxKdStack];
-    const KdStack stk{stack, 1, kMaxKdStack};
+    uint2 stk_nt[kKdStackCap];
+    float stk_split[kKdStackCap];
+    const KdStack stk{stk_nt, stk_split};
     const uint32_t n = W.counters[0];
     uint32_t rays = 0, nodes = 0, tests = 0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -427,8 +429,9 @@ __global__ void __launch_bounds__(kBlock) k_gather_camera(DevRender R, Wave W) {
 }
 
 __global__ void __launch_bounds__(kBlock) k_trace_bounce(DevScene S, Wave W) {
-    uint4 stack[kMaxKdStack];
-    const KdStack stk{stack, 1, kMaxKdStack};
+    uint2 stk_nt[kKdStackCap];
+    float stk_split[kKdStackCap];
+    const KdStack stk{stk_nt, stk_split};
     const uint32_t n = W.counters[1];
     uint32_t rays = 0, nodes = 0, tests = 0;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {

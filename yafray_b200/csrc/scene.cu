@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 
+#include "dev_trace.cuh"
 #include "scene.h"
 
 namespace yr {
@@ -363,6 +364,23 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     }
     std::vector<ObjNode> otree;
     build_object_tree(obounds, otree);
+    // traversal state is sized for these limits (kd stack: depth + 2 exits)
+    if (nodes.size() >= kNodeMask) return fail(YR_ERR_TOO_LARGE);
+    if (s->max_tree_depth + 2 > kKdStackCap) return fail(YR_ERR_TOO_LARGE);
+    {
+        int depth = 0;
+        std::vector<std::pair<int, int>> st{{0, 0}};
+        while (!st.empty()) {
+            auto [n, d] = st.back();
+            st.pop_back();
+            depth = std::max(depth, d);
+            if (otree[n].left >= 0) {
+                st.push_back({otree[n].left, d + 1});
+                st.push_back({otree[n].right, d + 1});
+            }
+        }
+        if (depth > kMaxObjStack) return fail(YR_ERR_UNSUPPORTED);
+    }
     const auto t1 = std::chrono::steady_clock::now();
 
     // ---- upload
@@ -397,7 +415,6 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.nnodes = (uint32_t)nodes.size();
     D.nprims = (uint32_t)prims.size();
     D.notree = (uint32_t)otree.size();
-    D.kd_stack = kMaxKdStack;
     D.status = s->status;
 
     // ---- shading records
