@@ -202,6 +202,8 @@ def main():
     ap.add_argument("--spp", type=int, default=16)
     ap.add_argument("--grid", type=int, default=16)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--reference-shadows", action="store_true",
+                    help="shadow rays walk the object tree in the reference's order (slower)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -223,6 +225,9 @@ def main():
             dist.barrier()
 
     sc, name = workload(args)
+    if args.reference_shadows:
+        sc.render.flags |= 1
+        name += ", shadow rays through the object tree"
     t0 = time.perf_counter()
     ds = api.DeviceScene(sc, device=local)
     info = ds.info()

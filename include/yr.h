@@ -91,6 +91,22 @@ YR_API yr_status yr_kdtree_build(const float *verts, uint32_t nverts,
                                  yr_kdtree **out);
 YR_API void yr_kdtree_free(yr_kdtree *tree);
 
+/* kdTree_t::kdTree_t(prims, n, depth, leafSize, cost_ratio, emptyBonus)
+ * with explicit parameters (kdtree.h:127-128; <= 0 depth / leaf size pick
+ * the ctor's defaults) and `nthreads` host threads (subtrees below the top
+ * levels are built concurrently; the tree is the same as with 1 thread). */
+typedef struct yr_kdtree_params {
+    int32_t max_depth;
+    int32_t max_leaf_size;
+    float cost_ratio;
+    float empty_bonus;
+    int32_t large_scene_penalty;  /* kdtree.cc:79-80 cost ratio penalty      */
+    int32_t reserved;
+} yr_kdtree_params;
+
+YR_API yr_status yr_kdtree_build_ex(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris,
+                                    const yr_kdtree_params *params, int nthreads, yr_kdtree **out);
+
 /* Object tree node (geomeTree_t, geometree.h:8-32): left < 0 marks a leaf
  * whose `right` is the object index; node 0 is the root, children follow
  * in depth-first order (left subtree first). */
@@ -180,11 +196,16 @@ typedef struct yr_render_params {
     float aa_pixelwidth;     /* AA_pixelwidth (default 1)                      */
     uint32_t seed;           /* Cranley-Patterson rotation seed               */
     float background[3];     /* constant background colour (black = none)     */
-    uint32_t flags;          /* reserved, 0                                    */
+    uint32_t flags;          /* YR_RENDER_* bits                               */
     int32_t region[4];       /* x0, x1, y0, y1: render only these pixels
                                 (scene_t::setRegion / the loader's -r option);
                                 all zero = the whole image                    */
 } yr_render_params;
+
+/* yr_render_params.flags: shadow rays walk the object tree front to back
+ * as scene_t::isShadowed does (the same answers as the default shadow-ray
+ * tree, with the reference's node counts; slower). */
+#define YR_RENDER_REFERENCE_SHADOWS 1u
 
 typedef struct yr_object_desc {
     const float *verts;      /* 3*nverts                                       */

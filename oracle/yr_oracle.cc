@@ -88,8 +88,14 @@ struct Box {
     float a[3], g[3];
 };
 
+struct Stats {
+    uint64_t primary, shadow, bounce, nodes, tests, boxes, roots;
+};
+Stats *g_stats = NULL;  // the scene being traced (for the slab-test counter)
+
 // bound_t::cross(from, ray, enter, leave, dist), shipped (fast-math) form (bound.cc:389-436)
 bool cross_el(const Box &b, const V &from, const V &ray, float dist, float &enter, float &leave) {
+    if (g_stats) g_stats->boxes++;
     float lmin = -1, lmax = -1;
     for (int k = 0; k < 3; k++) {
         if (ray[k] == 0) continue;
@@ -151,9 +157,6 @@ struct Cam {
     int resx, resy;
 };
 
-struct Stats {
-    uint64_t primary, shadow, bounce, nodes, tests;
-};
 
 struct Scene {
     std::vector<Obj> objs;
@@ -189,6 +192,7 @@ struct KdStackE {
 // kdTree_t::Intersect (kdtree.cc:591-727) if !any, IntersectS (kdtree.cc:730-866) if any
 bool kd_intersect(Scene &S, const Obj &o, const V &from, const V &ray, float dist, uint32_t &tr, float &Z, bool any) {
     float a, b, t;
+    S.st.roots++;
     if (!cross_el(o.tb, from, ray, dist, a, b)) return false;
     const V invDir(1.f / ray.x, 1.f / ray.y, 1.f / ray.z);
     bool hit = false;
@@ -978,11 +982,12 @@ void orc_kd(orc_scene *o, uint32_t obj, const float *from, const float *dir, flo
 }
 
 // Render pixels [x0,x1) x [y0,y1) into rgba (full image layout, resx*resy*4).
-// stats: primary, shadow, bounce, nodes, tests
+// stats: primary, shadow, bounce, nodes, tests, slab tests, kd roots tried
 void orc_render(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint64_t *stats) {
     Scene &S = o->s;
     const uint32_t spp = S.rp.spp ? S.rp.spp : 1;
     memset(&S.st, 0, sizeof(S.st));
+    g_stats = &S.st;
     for (int y = y0; y < y1; y++)
         for (int x = x0; x < x1; x++) {
             const uint32_t pixel = (uint32_t)(y * S.cam.resx + x);
@@ -1007,7 +1012,10 @@ void orc_render(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint6
         stats[2] = S.st.bounce;
         stats[3] = S.st.nodes;
         stats[4] = S.st.tests;
+        stats[5] = S.st.boxes;
+        stats[6] = S.st.roots;
     }
+    g_stats = NULL;
 }
 
 // primary ray directions of pixel centres (camera_t::shootRay)

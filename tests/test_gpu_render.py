@@ -73,3 +73,13 @@ def test_render_per_triangle_materials(cuda):
     img = ds.render()
     ref, _ = T.OracleScene(sc).render()
     _cmp(img, ref, frac=0.995)
+
+
+def test_render_gi_reference_shadow_order(cuda):
+    """The same image and ray counts with shadow rays walking the object tree."""
+    sc = scenes.config_large(seed=2, resx=48, resy=32, spp=2, grid=2)
+    a = api.DeviceScene(sc).render()
+    sc.render.flags = 1
+    ds = api.DeviceScene(sc)
+    b = ds.render()
+    assert np.array_equal(a, b)

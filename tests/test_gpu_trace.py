@@ -66,16 +66,22 @@ def test_closest_many_objects(cuda):
     assert np.array_equal(got[:, :3], ref[:, :3])
 
 
-def test_shadow_small_scene(cuda):
+@pytest.mark.parametrize("reference_order", [False, True])
+def test_shadow_small_scene(cuda, reference_order):
+    """Shadow-ray tree (default) and the reference's object-tree walk give
+    the oracle's answers bit for bit."""
     sc = scenes.config_small()
+    sc.render.flags = 1 if reference_order else 0
     ds = api.DeviceScene(sc)
     O = T.OracleScene(sc)
     s = _shadow_rays(sc, 60000, 5)
     assert np.array_equal(_run_shadow(cuda, ds, s), O.trace_shadow(s))
 
 
-def test_shadow_many_objects(cuda):
+@pytest.mark.parametrize("reference_order", [False, True])
+def test_shadow_many_objects(cuda, reference_order):
     sc = scenes.config_large(seed=3, resx=64, resy=48, spp=1, grid=4)
+    sc.render.flags = 1 if reference_order else 0
     ds = api.DeviceScene(sc)
     O = T.OracleScene(sc)
     s = _shadow_rays(sc, 40000, 6)
@@ -100,3 +106,25 @@ def test_reciprocal_division_is_exact(cuda):
     bad = C.c_uint64(123)
     abi.check(lib.yr_selftest_division(200_000_000, 12345, C.byref(bad)), "yr_selftest_division")
     assert bad.value == 0
+
+
+def test_shadow_bias_below_min_raydist(cuda):
+    """self_bias smaller than MIN_RAYDIST: the shadow-ray tree starts its walk
+    at the earlier origin and still matches the oracle."""
+    sc = scenes.config_large(seed=4, resx=64, resy=48, spp=1, grid=3)
+    sc.render.self_bias = 0.00001
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    s = _shadow_rays(sc, 30000, 8)
+    assert np.array_equal(_run_shadow(cuda, ds, s), O.trace_shadow(s))
+
+
+def test_no_shadow_casters(cuda):
+    sc = scenes.config_small(32, 24)
+    for m in sc.meshes:
+        m.cast_shadows = False
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    s = _shadow_rays(sc, 5000, 9)
+    occ = _run_shadow(cuda, ds, s)
+    assert np.array_equal(occ, O.trace_shadow(s)) and occ.sum() == 0

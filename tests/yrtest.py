@@ -67,13 +67,14 @@ def ptr(a: np.ndarray) -> C.c_void_p:
 
 
 # ----------------------------------------------------------- product trees
-def product_tree(mesh: scenes.Mesh) -> dict:
+def product_tree(mesh: scenes.Mesh, params=None, nthreads=1) -> dict:
     lib = abi.load()
     v = np.ascontiguousarray(mesh.verts, np.float32)
     t = np.ascontiguousarray(mesh.tris, np.uint32)
     p = C.POINTER(abi.YrKdTree)()
-    st = lib.yr_kdtree_build(v.ctypes.data_as(C.POINTER(C.c_float)), v.shape[0],
-                             t.ctypes.data_as(C.POINTER(C.c_uint32)), t.shape[0], C.byref(p))
+    st = lib.yr_kdtree_build_ex(v.ctypes.data_as(C.POINTER(C.c_float)), v.shape[0],
+                                t.ctypes.data_as(C.POINTER(C.c_uint32)), t.shape[0],
+                                C.byref(params) if params is not None else None, nthreads, C.byref(p))
     abi.check(st, "yr_kdtree_build")
     tr = p.contents
     nodes = np.ctypeslib.as_array(C.cast(tr.nodes, C.POINTER(C.c_uint32)), (2 * tr.nnodes,)).reshape(-1, 2).copy()
@@ -167,7 +168,7 @@ class OracleScene:
         x1 = sc.resx if x1 is None else x1
         y1 = sc.resy if y1 is None else y1
         img = np.zeros((sc.resy, sc.resx, 4), np.float32)
-        stats = np.zeros(5, np.uint64)
+        stats = np.zeros(7, np.uint64)
         self.lib.orc_render(self.h, ptr(img), x0, x1, y0, y1, ptr(stats))
         return img, stats
 

@@ -46,6 +46,11 @@ class YrObjectNode(C.Structure):
     _fields_ = [("bmin", f3), ("left", C.c_int32), ("bmax", f3), ("right", C.c_int32)]
 
 
+class YrKdTreeParams(C.Structure):
+    _fields_ = [("max_depth", C.c_int32), ("max_leaf_size", C.c_int32), ("cost_ratio", C.c_float),
+                ("empty_bonus", C.c_float), ("large_scene_penalty", C.c_int32), ("reserved", C.c_int32)]
+
+
 class YrCameraDesc(C.Structure):
     _fields_ = [("pos", f3), ("look", f3), ("up", f3), ("resx", C.c_int32), ("resy", C.c_int32),
                 ("aspect", C.c_float), ("focal", C.c_float)]
@@ -139,6 +144,8 @@ SIGNATURES = {
     "yr_kdtree_build": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32,
                                   C.POINTER(C.POINTER(YrKdTree))]),
     "yr_kdtree_free": (None, [C.POINTER(YrKdTree)]),
+    "yr_kdtree_build_ex": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32,
+                                     C.POINTER(YrKdTreeParams), C.c_int, C.POINTER(C.POINTER(YrKdTree))]),
     "yr_object_tree_build": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(YrObjectNode),
                                        C.POINTER(C.c_uint32)]),
     "yr_scene_create": (C.c_int, [C.POINTER(YrSceneDesc), C.c_int, C.POINTER(_P)]),

@@ -29,12 +29,25 @@ YR_API const char *yr_version(void) { return "yafray_b200 0.1 (YafRay 0.0.9 hot 
 
 YR_API yr_status yr_kdtree_build(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris,
                                  yr_kdtree **out) {
+    return yr_kdtree_build_ex(verts, nverts, tris, ntris, nullptr, 1, out);
+}
+
+YR_API yr_status yr_kdtree_build_ex(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris,
+                                    const yr_kdtree_params *params, int nthreads, yr_kdtree **out) {
     if (!out) return YR_ERR_INVALID_ARG;
     *out = nullptr;
+    yr::KdParams kp;
+    if (params) {
+        kp.max_depth = params->max_depth;
+        kp.max_leaf = params->max_leaf_size;
+        kp.cost_ratio = params->cost_ratio;
+        kp.empty_bonus = params->empty_bonus;
+        kp.large_scene_penalty = params->large_scene_penalty != 0;
+    }
     yr::KdTree t;
     yr_status st;
     try {
-        st = yr::build_kdtree(verts, nverts, tris, ntris, t);
+        st = yr::build_kdtree(verts, nverts, tris, ntris, t, kp, nthreads < 1 ? 1 : nthreads);
     } catch (const std::bad_alloc &) {
         return YR_ERR_OUT_OF_MEMORY;
     }

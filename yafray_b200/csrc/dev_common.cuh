@@ -111,6 +111,15 @@ struct DevScene {
     uint32_t nnodes;
     uint32_t nprims;
     uint32_t notree;
+    // shadow-ray tree: one kd-tree over the triangles of every object that
+    // casts shadows (global triangle indices), plus each triangle's object
+    const uint2 *sh_nodes;
+    const uint32_t *sh_prims;
+    const uint32_t *tri_obj;
+    uint32_t sh_nnodes;
+    uint32_t sh_nprims;
+    float sh_tb[6];
+    int use_sh_tree;            // 0: shadow rays walk the object tree (reference order)
     int *status;                // device status word
 };
 

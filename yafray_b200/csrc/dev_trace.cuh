@@ -350,6 +350,149 @@ struct ObjIter {
     }
 };
 
+// scene_t::isShadowed answered with the shadow-ray tree.  The reference
+// shoots each shadow-casting object whose bound the ray crosses, from
+// p + dir*self_bias for the point's own object and from p + dir*MIN_RAYDIST
+// for the others, and reports whether any kdTree_t::IntersectS finds a
+// triangle with 0 < t < dist (scene.cc:107-185, kdtree.cc:730-866).  That
+// is a yes/no question about single triangles, so it does not depend on
+// the order in which objects or leaves are visited: here one traversal of
+// the merged tree covers the segment that both origins can reach (from the
+// earlier origin, up to dist plus the gap between the two offsets), and
+// each triangle is tested from its own object's origin with the same
+// triangle_t::hit / intersect arithmetic - the answer is bit-identical.
+__device__ inline bool scene_occluded_merged(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
+                                             float self_bias, const KdStack &stk, uint32_t &nodes_out,
+                                             uint32_t &tests_out) {
+    const V3 self = p + dir * self_bias;
+    const V3 p2 = p + dir * kMinRayDist;
+    const bool self_first = self_bias < kMinRayDist;
+    const V3 q = self_first ? self : p2;
+    const float tdist = (dist + fabsf(self_bias - kMinRayDist)) * 1.000001f + 1e-6f;
+    const RayR R = make_rayr(dir);
+    float a, b;
+    if (!box_enter_leave(S.sh_tb, S.sh_tb + 3, q, R, tdist, a, b)) return false;
+    const V3 &ray = R.d;
+    const float inv[3] = {R.inv.x, R.inv.y, R.inv.z};
+    const float fr[3] = {q.x, q.y, q.z};
+    const float rr[3] = {ray.x, ray.y, ray.z};
+    uint32_t curr = 0;
+    float en_t = a, en_pb[3];
+    if (a >= 0.f) {
+        en_pb[0] = fr[0] + a * rr[0];
+        en_pb[1] = fr[1] + a * rr[1];
+        en_pb[2] = fr[2] + a * rr[2];
+    } else {
+        en_pb[0] = fr[0];
+        en_pb[1] = fr[1];
+        en_pb[2] = fr[2];
+    }
+    float ex_pb[3];
+    ex_pb[0] = fr[0] + b * rr[0];
+    ex_pb[1] = fr[1] + b * rr[1];
+    ex_pb[2] = fr[2] + b * rr[2];
+    float ex_t = b;
+    stk.nt[0] = make_uint2(kNodeMask | (3u << 30), __float_as_uint(b));
+    int sp = 1;
+    uint32_t leaves = 0, nodes = 0, tests = 0;
+    bool occluded = false;
+    while (curr != kNodeMask) {
+        if (tdist < en_t) break;
+        if (++leaves > kMaxLeafVisits) {
+            dev_fail(S.status, kDevIterationCap);
+            break;
+        }
+        if (curr >= S.sh_nnodes) {
+            dev_fail(S.status, kDevBadTree);
+            break;
+        }
+        uint2 nd = __ldg(S.sh_nodes + curr);
+        bool bad = false;
+        while ((nd.y & 3u) != 3u) {
+            nodes++;
+            const int axis = (int)(nd.y & 3u);
+            const float split = __uint_as_float(nd.x);
+            const uint32_t right = nd.y >> 2;
+            uint32_t far_child;
+            if (curr + 1 >= S.sh_nnodes || right >= S.sh_nnodes) {
+                bad = true;
+                break;
+            }
+            if (en_pb[axis] <= split) {
+                if (ex_pb[axis] <= split) {
+                    curr = curr + 1;
+                    nd = __ldg(S.sh_nodes + curr);
+                    continue;
+                }
+                far_child = right;
+                curr = curr + 1;
+            } else {
+                if (split < ex_pb[axis]) {
+                    curr = right;
+                    nd = __ldg(S.sh_nodes + curr);
+                    continue;
+                }
+                far_child = curr + 1;
+                curr = right;
+            }
+            const float t = (split - fr[axis]) * inv[axis];
+            if (sp >= kKdStackCap) {
+                bad = true;
+                break;
+            }
+            stk.nt[sp] = make_uint2(far_child | ((uint32_t)axis << 30), __float_as_uint(t));
+            stk.split[sp] = split;
+            sp++;
+            const int na = axis == 2 ? 0 : axis + 1, pa = axis == 0 ? 2 : axis - 1;
+            ex_t = t;
+            ex_pb[axis] = split;
+            ex_pb[na] = fr[na] + t * rr[na];
+            ex_pb[pa] = fr[pa] + t * rr[pa];
+            nd = __ldg(S.sh_nodes + curr);
+        }
+        if (bad) {
+            dev_fail(S.status, sp >= kKdStackCap ? kDevStackOverflow : kDevBadTree);
+            break;
+        }
+        nodes++;
+        const uint32_t np = nd.y >> 2;
+        for (uint32_t k = 0; k < np; k++) {
+            const uint32_t ti = (np == 1) ? nd.x : __ldg(S.sh_prims + nd.x + k);
+            if (ti >= S.ntris) {
+                bad = true;
+                break;
+            }
+            tests++;
+            const Tri tr = load_tri(S.tris, ti);
+            const int obj = (int)__ldg(S.tri_obj + ti);
+            float rt;
+            if (tri_hit(tr, obj == own ? self : p2, ray, rt) && rt < dist && rt > 0.f) {
+                occluded = true;
+                break;
+            }
+        }
+        if (bad) {
+            dev_fail(S.status, kDevBadTree);
+            break;
+        }
+        if (occluded) break;
+        en_t = ex_t;
+        en_pb[0] = ex_pb[0];
+        en_pb[1] = ex_pb[1];
+        en_pb[2] = ex_pb[2];
+        sp--;
+        curr = stk.nt[sp].x & kNodeMask;
+        if (curr != kNodeMask) {
+            const uint2 nx = stk.nt[sp - 1];
+            ex_t = __uint_as_float(nx.y);
+            exit_point(nx.x, ex_t, stk.split[sp - 1], fr, rr, ex_pb);
+        }
+    }
+    nodes_out += nodes;
+    tests_out += tests;
+    return occluded;
+}
+
 struct SceneHit {
     float t;
     int object;       // -1 = miss
@@ -403,8 +546,8 @@ __device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V
 
 // scene_t::isShadowed (scene.cc:107-185).  p: shading point, own: its
 // object, ray: unit direction, dist: |l - p| (or infinity).
-__device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
-                                      float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+__device__ inline bool scene_occluded_ref(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
+                                          float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     const V3 self = p + dir * self_bias;
     const V3 p2 = p + dir * kMinRayDist;
     const RayR ray = make_rayr(dir);
@@ -424,6 +567,17 @@ __device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, c
         it.next(S, p2, ray);
     }
     return false;
+}
+
+// isShadowed through the shadow-ray tree, or through the object tree in the
+// reference's order when the scene asks for it (yr_render_params.flags)
+__device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
+                                      float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+    if (S.use_sh_tree) {
+        if (S.sh_nnodes == 0) return false;  // nothing casts shadows
+        return scene_occluded_merged(S, p, own, dir, dist, self_bias, stk, nodes, tests);
+    }
+    return scene_occluded_ref(S, p, own, dir, dist, self_bias, stk, nodes, tests);
 }
 
 }  // namespace yr

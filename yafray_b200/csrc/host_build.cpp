@@ -24,7 +24,9 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <atomic>
 #include <list>
+#include <thread>
 
 namespace yr {
 namespace {
@@ -148,16 +150,39 @@ class Builder {
     Builder(const float *verts, const uint32_t *tris, uint32_t ntris, KdTree &out)
         : verts_(verts), tris_(tris), n_(ntris), out_(out) {}
 
-    yr_status run() {
+    // a builder for one deferred subtree, sharing the parent's inputs
+    Builder(const Builder &parent, KdTree &out)
+        : verts_(parent.verts_), tris_(parent.tris_), n_(parent.n_), out_(out), shared_bounds_(&parent.bounds()),
+          tree_(parent.tree_), cost_ratio_(parent.cost_ratio_), ebonus_(parent.ebonus_),
+          max_depth_(parent.max_depth_), max_leaf_(parent.max_leaf_) {}
+
+    struct Task {
+        std::vector<uint32_t> prims;
+        Box nb;
+        int depth;
+        int bad_refines;
+        size_t node;  // placeholder position in the parent's node array
+    };
+
+    yr_status run(const KdParams &kp, int nthreads) {
         // kdTree_t ctor parameter defaults (kdtree.cc:57-80)
-        cost_ratio_ = 1.2f;
-        ebonus_ = 0.40f;
-        max_depth_ = int(6.0f + 1.66f * std::log(float(n_)));
+        cost_ratio_ = kp.cost_ratio;
+        ebonus_ = kp.empty_bonus;
+        max_depth_ = kp.max_depth;
+        max_leaf_ = kp.max_leaf;
+        if (max_depth_ <= 0) max_depth_ = int(6.0f + 1.66f * std::log(float(n_)));
         const double log_leaves = 1.442695f * std::log(double(n_));
-        max_leaf_ = int(log_leaves - 16.0);
-        if (max_leaf_ <= 0) max_leaf_ = 1;
+        if (max_leaf_ <= 0) {
+            max_leaf_ = int(log_leaves - 16.0);
+            if (max_leaf_ <= 0) max_leaf_ = 1;
+        }
         if (max_depth_ > 64) max_depth_ = 64;
-        if (log_leaves > 16.0) cost_ratio_ = (float)(cost_ratio_ + 0.25 * (log_leaves - 16.0));
+        if (kp.large_scene_penalty && log_leaves > 16.0)
+            cost_ratio_ = (float)(cost_ratio_ + 0.25 * (log_leaves - 16.0));
+        if (nthreads > 1 && n_ > 4096) {
+            defer_depth_ = 0;
+            while ((1 << defer_depth_) < 4 * nthreads && defer_depth_ < 12) defer_depth_++;
+        }
 
         bounds_.resize(n_);
         for (uint32_t i = 0; i < n_; i++) {
@@ -191,6 +216,7 @@ class Builder {
         out_.nodes.reserve(2 * (size_t)n_ + 16);
         Box root = tree_;
         yr_status st = build(all, root, 0, 0);
+        if (st == YR_OK && !tasks_.empty()) st = run_tasks(nthreads);
         out_.bound = tree_;
         out_.max_depth = max_depth_;
         out_.max_leaf_size = max_leaf_;
@@ -199,8 +225,77 @@ class Builder {
         return st;
     }
 
+    const std::vector<Box> &bounds() const { return shared_bounds_ ? *shared_bounds_ : bounds_; }
+
+    // kdTree_t::buildTree (kdtree.cc:416-582)
+    yr_status build(std::vector<uint32_t> &prims, const Box &nb, int depth, int bad_refines);
+
   private:
     const float *vtx(uint32_t tri, int k) const { return verts_ + 3 * (size_t)tris_[3 * (size_t)tri + k]; }
+
+    // Build the deferred subtrees in parallel and splice each one in place of
+    // its placeholder: the node order is then the sequential build's
+    // depth-first order (right-child links and prim offsets relocated).
+    yr_status run_tasks(int nthreads) {
+        std::vector<KdTree> sub(tasks_.size());
+        std::vector<yr_status> st(tasks_.size(), YR_OK);
+        std::atomic<size_t> next{0};
+        auto worker = [&] {
+            for (;;) {
+                const size_t k = next.fetch_add(1);
+                if (k >= tasks_.size()) return;
+                Builder b(*this, sub[k]);
+                Task &t = tasks_[k];
+                try {
+                    st[k] = b.build(t.prims, t.nb, t.depth, t.bad_refines);
+                } catch (const std::bad_alloc &) {
+                    st[k] = YR_ERR_OUT_OF_MEMORY;
+                }
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+        worker();
+        for (std::thread &th : pool) th.join();
+        for (yr_status e : st)
+            if (e != YR_OK) return e;
+        // new position of every node of the serial part
+        const size_t n0 = out_.nodes.size();
+        std::vector<size_t> newpos(n0 + 1);
+        std::vector<int> task_at(n0, -1);
+        for (size_t k = 0; k < tasks_.size(); k++) task_at[tasks_[k].node] = (int)k;
+        size_t shift = 0;
+        for (size_t i = 0; i < n0; i++) {
+            newpos[i] = i + shift;
+            if (task_at[i] >= 0) shift += sub[task_at[i]].nodes.size() - 1;
+        }
+        newpos[n0] = n0 + shift;
+        if (n0 + shift >= (1u << 30)) return YR_ERR_TOO_LARGE;
+        std::vector<yr_kd_node> nodes(n0 + shift);
+        std::vector<uint32_t> prims = std::move(out_.prims);
+        for (size_t i = 0; i < n0; i++) {
+            const yr_kd_node nd = out_.nodes[i];
+            const int k = task_at[i];
+            if (k < 0) {
+                yr_kd_node o = nd;
+                if ((nd.flags & 3u) != 3u) o.flags = (nd.flags & 3u) | ((uint32_t)newpos[nd.flags >> 2] << 2);
+                nodes[newpos[i]] = o;
+                continue;
+            }
+            const KdTree &t = sub[k];
+            const uint32_t base = (uint32_t)newpos[i], pbase = (uint32_t)prims.size();
+            for (size_t j = 0; j < t.nodes.size(); j++) {
+                yr_kd_node o = t.nodes[j];
+                if ((o.flags & 3u) != 3u) o.flags = (o.flags & 3u) | (((o.flags >> 2) + base) << 2);
+                else if ((o.flags >> 2) > 1) o.word += pbase;
+                nodes[base + j] = o;
+            }
+            prims.insert(prims.end(), t.prims.begin(), t.prims.end());
+        }
+        out_.nodes.swap(nodes);
+        out_.prims.swap(prims);
+        return YR_OK;
+    }
 
     void make_leaf(const std::vector<uint32_t> &prims) {
         yr_kd_node nd;
@@ -229,7 +324,7 @@ class Builder {
             const float s = kBins / d[axis];
             const float lo = nb.a[axis];
             for (uint32_t i = 0; i < np; i++) {
-                const Box &bb = bounds_[prims[i]];
+                const Box &bb = bounds()[prims[i]];
                 const float tl = bb.a[axis], tu = bb.g[axis];
                 int bl = (int)((tl - lo) * s), br = (int)((tu - lo) * s);
                 bl = bl < 0 ? 0 : (bl > kBins ? kBins : bl);
@@ -309,7 +404,7 @@ class Builder {
     }
 
     // Exact sorted-edge SAH (kdTree_t::minimalCost, kdtree.cc:311-406).
-    // `clipped` holds per-position bounds (after clipping), else bounds_[prim].
+    // `clipped` holds per-position bounds (after clipping), else bounds()[prim].
     void exact(const std::vector<uint32_t> &prims, const Box &nb, const std::vector<Box> *clipped,
                float ebonus, Split &sp) {
         const uint32_t np = (uint32_t)prims.size();
@@ -322,7 +417,7 @@ class Builder {
             ed.clear();
             for (uint32_t i = 0; i < np; i++) {
                 const int pn = (int)prims[i];
-                const Box &bb = clipped ? (*clipped)[i] : bounds_[pn];
+                const Box &bb = clipped ? (*clipped)[i] : bounds()[pn];
                 if (bb.a[axis] == bb.g[axis]) {
                     ed.push_back({bb.a[axis], pn, kBoth});
                 } else {
@@ -366,8 +461,19 @@ class Builder {
         }
     }
 
-    // kdTree_t::buildTree (kdtree.cc:416-582)
-    yr_status build(std::vector<uint32_t> &prims, const Box &nb, int depth, int bad_refines) {
+  public:
+    yr_status build_node(std::vector<uint32_t> &prims, const Box &nb, int depth, int bad_refines) {
+        if (defer_depth_ >= 0 && depth == defer_depth_ && prims.size() > 4096) {
+            Task t;
+            t.prims.swap(prims);
+            t.nb = nb;
+            t.depth = depth;
+            t.bad_refines = bad_refines;
+            t.node = out_.nodes.size();
+            tasks_.push_back(std::move(t));
+            out_.nodes.push_back(yr_kd_node{0u, 3u});  // placeholder
+            return YR_OK;
+        }
         std::vector<Box> clipped;
         if (prims.size() <= kClipThresh) {
             double bmin[3], bmax[3];
@@ -395,7 +501,7 @@ class Builder {
                     clipped.push_back(cb);
                 } else if (res == 2) {
                     kept.push_back(pn);
-                    clipped.push_back(bounds_[pn]);
+                    clipped.push_back(bounds()[pn]);
                 }
             }
             prims.swap(kept);
@@ -427,11 +533,11 @@ class Builder {
         const int ax = sp.axis;
         if (np > kPigeonThresh) {
             for (uint32_t pn : prims) {
-                if (bounds_[pn].a[ax] >= sp.t) {
+                if (bounds()[pn].a[ax] >= sp.t) {
                     right.push_back(pn);
                 } else {
                     left.push_back(pn);
-                    if (bounds_[pn].g[ax] > sp.t) right.push_back(pn);
+                    if (bounds()[pn].g[ax] > sp.t) right.push_back(pn);
                 }
             }
             split_pos = sp.t;
@@ -457,24 +563,32 @@ class Builder {
         Box bl = nb, br = nb;
         bl.g[ax] = split_pos;
         br.a[ax] = split_pos;
-        yr_status st = build(left, bl, depth + 1, bad_refines);
+        yr_status st = build_node(left, bl, depth + 1, bad_refines);
         if (st != YR_OK) return st;
         const size_t right_index = out_.nodes.size();
         if (right_index >= (1u << 30)) return YR_ERR_TOO_LARGE;
         out_.nodes[cur].flags = (out_.nodes[cur].flags & 3u) | ((uint32_t)right_index << 2);
-        return build(right, br, depth + 1, bad_refines);
+        return build_node(right, br, depth + 1, bad_refines);
     }
+  private:
 
     const float *verts_;
     const uint32_t *tris_;
     uint32_t n_;
     KdTree &out_;
     std::vector<Box> bounds_;
+    const std::vector<Box> *shared_bounds_ = nullptr;
     Box tree_{};
     float cost_ratio_ = 0.f, ebonus_ = 0.f;
     int max_depth_ = 0, max_leaf_ = 0;
+    int defer_depth_ = -1;
+    std::vector<Task> tasks_;
     std::vector<Edge> edges_[3];
 };
+
+yr_status Builder::build(std::vector<uint32_t> &prims, const Box &nb, int depth, int bad_refines) {
+    return build_node(prims, nb, depth, bad_refines);
+}
 
 // --- object tree -----------------------------------------------------------
 
@@ -633,12 +747,13 @@ class Clusterer {
 
 }  // namespace
 
-yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris, KdTree &out) {
+yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris, KdTree &out,
+                       const KdParams &params, int nthreads) {
     if (!verts || !tris || ntris == 0) return YR_ERR_EMPTY_SCENE;
     for (size_t i = 0; i < 3 * (size_t)ntris; i++)
         if (tris[i] >= nverts) return YR_ERR_INVALID_ARG;
     Builder b(verts, tris, ntris, out);
-    return b.run();
+    return b.run(params, nthreads);
 }
 
 Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris) {

@@ -24,10 +24,23 @@ struct KdTree {
     float empty_bonus = 0.f;
 };
 
-// Build with meshObject_t's parameters (mesh.cc:162: depth -1, leaf -1,
-// cost 1.2, empty bonus 0.40).  Returns YR_OK or an error status.
+// Build parameters; the defaults are meshObject_t's (mesh.cc:162: depth -1,
+// leaf size -1, cost ratio 1.2, empty bonus 0.40, with kdTree_t's
+// large-scene cost penalty, kdtree.cc:68-80).
+struct KdParams {
+    int max_depth = -1;
+    int max_leaf = -1;
+    float cost_ratio = 1.2f;
+    float empty_bonus = 0.40f;
+    bool large_scene_penalty = true;
+};
+
+// Returns YR_OK or an error status.  With nthreads > 1 the subtrees below a
+// few top levels are built concurrently; the result is identical to the
+// sequential build.
 yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris,
-                       uint32_t ntris, KdTree &out);
+                       uint32_t ntris, KdTree &out, const KdParams &params = KdParams(),
+                       int nthreads = 1);
 
 // meshObject_t::recalcBound (mesh.cc:343-379): bound of the triangles'
 // vertices grown by BOX_MIN.

@@ -362,6 +362,47 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         objects.push_back(dob);
         obounds.push_back(mesh_bound(od.verts, od.tris, od.ntris));
     }
+    // shadow-ray tree over the triangles of every shadow-casting object
+    std::vector<uint2> sh_nodes;
+    std::vector<uint32_t> sh_prims, tri_obj(total_tris);
+    float sh_tb[6] = {0, 0, 0, 0, 0, 0};
+    {
+        std::vector<float> mv;
+        std::vector<uint32_t> mt, remap;
+        for (uint32_t o = 0; o < desc->nobjects; o++) {
+            const yr_object_desc &od = desc->objects[o];
+            for (uint32_t t = 0; t < od.ntris; t++) tri_obj[objects[o].tri_base + t] = o;
+            if (!od.cast_shadows) continue;
+            const uint32_t vbase = (uint32_t)(mv.size() / 3);
+            mv.insert(mv.end(), od.verts, od.verts + 3 * (size_t)od.nverts);
+            for (size_t k = 0; k < 3 * (size_t)od.ntris; k++) mt.push_back(od.tris[k] + vbase);
+            for (uint32_t t = 0; t < od.ntris; t++) remap.push_back(objects[o].tri_base + t);
+        }
+        if (!remap.empty()) {
+            KdTree st_tree;
+            KdParams kp;
+            kp.max_leaf = 1;                   // deeper tree, fewer triangle tests
+            kp.large_scene_penalty = false;
+            unsigned nth = std::thread::hardware_concurrency();
+            st = build_kdtree(mv.data(), (uint32_t)(mv.size() / 3), mt.data(), (uint32_t)remap.size(), st_tree, kp,
+                              (int)std::max(1u, nth));
+            if (st != YR_OK) return fail(st);
+            if (st_tree.nodes.size() >= kNodeMask) return fail(YR_ERR_TOO_LARGE);
+            if (st_tree.max_depth + 2 > kKdStackCap) return fail(YR_ERR_TOO_LARGE);
+            sh_nodes.reserve(st_tree.nodes.size());
+            for (const yr_kd_node &nd : st_tree.nodes) {
+                uint2 g;
+                g.x = nd.word;
+                g.y = nd.flags;
+                if ((nd.flags & 3u) == 3u && (nd.flags >> 2) == 1) g.x = remap[nd.word];
+                sh_nodes.push_back(g);
+            }
+            sh_prims.reserve(st_tree.prims.size());
+            for (uint32_t p : st_tree.prims) sh_prims.push_back(remap[p]);
+            std::memcpy(sh_tb, st_tree.bound.a, 12);
+            std::memcpy(sh_tb + 3, st_tree.bound.g, 12);
+        }
+    }
     std::vector<ObjNode> otree;
     build_object_tree(obounds, otree);
     // traversal state is sized for these limits (kd stack: depth + 2 exits)
@@ -400,6 +441,11 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, (const DevObjNode *)otree.data(), otree.size(), (DevObjNode **)&d_otree)) != YR_OK)
         return fail(st);
+    const uint2 *d_sh_nodes = nullptr;
+    const uint32_t *d_sh_prims = nullptr, *d_tri_obj = nullptr;
+    if ((st = dev_upload(s, sh_nodes.data(), sh_nodes.size(), (uint2 **)&d_sh_nodes)) != YR_OK) return fail(st);
+    if ((st = dev_upload(s, sh_prims.data(), sh_prims.size(), (uint32_t **)&d_sh_prims)) != YR_OK) return fail(st);
+    if ((st = dev_upload(s, tri_obj.data(), tri_obj.size(), (uint32_t **)&d_tri_obj)) != YR_OK) return fail(st);
     if (cudaMalloc(&s->status, sizeof(int)) != cudaSuccess) return fail(YR_ERR_OUT_OF_MEMORY);
     if (cudaMemset(s->status, 0, sizeof(int)) != cudaSuccess) return fail(YR_ERR_CUDA);
     if (cudaMallocHost(&s->status_host, sizeof(int)) != cudaSuccess) return fail(YR_ERR_OUT_OF_MEMORY);
@@ -415,6 +461,13 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.nnodes = (uint32_t)nodes.size();
     D.nprims = (uint32_t)prims.size();
     D.notree = (uint32_t)otree.size();
+    D.sh_nodes = d_sh_nodes;
+    D.sh_prims = d_sh_prims;
+    D.tri_obj = d_tri_obj;
+    D.sh_nnodes = (uint32_t)sh_nodes.size();
+    D.sh_nprims = (uint32_t)sh_prims.size();
+    std::memcpy(D.sh_tb, sh_tb, sizeof(sh_tb));
+    D.use_sh_tree = (desc->render.flags & YR_RENDER_REFERENCE_SHADOWS) ? 0 : 1;
     D.status = s->status;
 
     // ---- shading records
