@@ -91,6 +91,7 @@ struct DevObject {
     uint32_t tri_base;  // first global triangle index
     uint32_t ntris;
     uint32_t flags;     // bit0: casts shadows
+    float ob[6];        // object bound (meshObject_t::getBound), the object tree's leaf box
 };
 
 struct DevObjNode {     // object tree (geomeTree_t), node 0 = root

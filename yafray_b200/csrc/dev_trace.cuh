@@ -467,8 +467,16 @@ __device__ inline bool scene_occluded_merged(const DevScene &S, const V3 &p, int
             const int obj = (int)__ldg(S.tri_obj + ti);
             float rt;
             if (tri_hit(tr, obj == own ? self : p2, ray, rt) && rt < dist && rt > 0.f) {
-                occluded = true;
-                break;
+                // the reference shoots an object only when the ray from p2
+                // crosses its bound before dist (geometree.h:86-135); the
+                // enclosing object-tree boxes then pass too (same ray, larger
+                // boxes, monotonic slab arithmetic)
+                const DevObject &ob = S.objects[obj];
+                float w;
+                if (box_where(ob.ob, ob.ob + 3, p2, R, dist, w)) {
+                    occluded = true;
+                    break;
+                }
             }
         }
         if (bad) {

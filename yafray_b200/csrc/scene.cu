@@ -359,8 +359,11 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         dob.tri_base = tri_base;
         dob.ntris = od.ntris;
         dob.flags = od.cast_shadows ? 1u : 0u;
+        const Box obb = mesh_bound(od.verts, od.tris, od.ntris);
+        std::memcpy(dob.ob, obb.a, 12);
+        std::memcpy(dob.ob + 3, obb.g, 12);
         objects.push_back(dob);
-        obounds.push_back(mesh_bound(od.verts, od.tris, od.ntris));
+        obounds.push_back(obb);
     }
     // shadow-ray tree over the triangles of every shadow-casting object
     std::vector<uint2> sh_nodes;
