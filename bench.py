@@ -202,8 +202,9 @@ def main():
     ap.add_argument("--spp", type=int, default=16)
     ap.add_argument("--grid", type=int, default=16)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--reference-shadows", action="store_true",
-                    help="shadow rays walk the object tree in the reference's order (slower)")
+    ap.add_argument("--exact-order", action="store_true",
+                    help="exact slab tests in the object tree (reference visiting order)")
+    ap.add_argument("--shadow-tree", action="store_true", help="answer shadow rays with the shadow-ray tree")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -225,9 +226,12 @@ def main():
             dist.barrier()
 
     sc, name = workload(args)
-    if args.reference_shadows:
+    if args.exact_order:
+        sc.render.flags |= 2
+        name += ", exact object-tree order"
+    if args.shadow_tree:
         sc.render.flags |= 1
-        name += ", shadow rays through the object tree"
+        name += ", shadow-ray tree"
     t0 = time.perf_counter()
     ds = api.DeviceScene(sc, device=local)
     info = ds.info()

@@ -202,10 +202,18 @@ typedef struct yr_render_params {
                                 all zero = the whole image                    */
 } yr_render_params;
 
-/* yr_render_params.flags: shadow rays walk the object tree front to back
- * as scene_t::isShadowed does (the same answers as the default shadow-ray
- * tree, with the reference's node counts; slower). */
-#define YR_RENDER_REFERENCE_SHADOWS 1u
+/* yr_render_params.flags:
+ * YR_RENDER_SHADOW_TREE: answer shadow rays with one kd-tree over all
+ *   shadow-casting triangles instead of walking the object tree
+ *   (scene_t::isShadowed order); the answers are identical, the walk
+ *   differs.  Built at scene creation only when requested.
+ * YR_RENDER_EXACT_ORDER: evaluate every object-tree slab test exactly as
+ *   bound_t::cross does, so that objects are visited in the reference's
+ *   order and node counts match it; by default the object tree uses a
+ *   conservative reciprocal-multiply slab test (same hits except between
+ *   exactly equidistant objects; faster). */
+#define YR_RENDER_SHADOW_TREE 1u
+#define YR_RENDER_EXACT_ORDER 2u
 
 typedef struct yr_object_desc {
     const float *verts;      /* 3*nverts                                       */

@@ -75,11 +75,11 @@ def test_render_per_triangle_materials(cuda):
     _cmp(img, ref, frac=0.995)
 
 
-def test_render_gi_reference_shadow_order(cuda):
-    """The same image and ray counts with shadow rays walking the object tree."""
+@pytest.mark.parametrize("flags", [1, 2, 3])
+def test_render_gi_traversal_variants(cuda, flags):
+    """The same image with the shadow-ray tree and/or the exact object order."""
     sc = scenes.config_large(seed=2, resx=48, resy=32, spp=2, grid=2)
     a = api.DeviceScene(sc).render()
-    sc.render.flags = 1
-    ds = api.DeviceScene(sc)
-    b = ds.render()
+    sc.render.flags = flags
+    b = api.DeviceScene(sc).render()
     assert np.array_equal(a, b)

@@ -41,9 +41,17 @@ def _shadow_rays(sc, n, seed):
     return s
 
 
+EXACT = 2        # YR_RENDER_EXACT_ORDER
+SHADOW_TREE = 1  # YR_RENDER_SHADOW_TREE
+
+
 @pytest.mark.parametrize("shadow_only", [False, True])
-def test_closest_small_scene(cuda, shadow_only):
+@pytest.mark.parametrize("exact", [False, True])
+def test_closest_small_scene(cuda, shadow_only, exact):
+    """Object, triangle and distance bit for bit; with the exact object-tree
+    order also the number of kd and object-tree nodes visited."""
     sc = scenes.config_small()
+    sc.render.flags = EXACT if exact else 0
     ds = api.DeviceScene(sc)
     O = T.OracleScene(sc)
     rays = T.random_rays(sc, 60000, 7)
@@ -52,36 +60,41 @@ def test_closest_small_scene(cuda, shadow_only):
     assert np.array_equal(got[:, 1], ref[:, 1]), "object ids differ"
     assert np.array_equal(got[:, 2], ref[:, 2]), "triangle ids differ"
     assert np.array_equal(got[:, 0], ref[:, 0]), "hit distances differ"
-    assert np.array_equal(got[:, 3], ref[:, 3]), "node visit counts differ"
+    if exact:
+        assert np.array_equal(got[:, 3], ref[:, 3]), "node visit counts differ"
     assert (ref[:, 1] != 0xFFFFFFFF).sum() > 5000
 
 
-def test_closest_many_objects(cuda):
+@pytest.mark.parametrize("exact", [False, True])
+def test_closest_many_objects(cuda, exact):
     sc = scenes.config_large(seed=3, resx=64, resy=48, spp=1, grid=4)
+    sc.render.flags = EXACT if exact else 0
     ds = api.DeviceScene(sc)
     O = T.OracleScene(sc)
     rays = T.random_rays(sc, 40000, 9)
     got = _run_closest(cuda, ds, rays)
     ref = O.trace_closest(rays)
     assert np.array_equal(got[:, :3], ref[:, :3])
+    if exact:
+        assert np.array_equal(got[:, 3], ref[:, 3])
 
 
-@pytest.mark.parametrize("reference_order", [False, True])
-def test_shadow_small_scene(cuda, reference_order):
-    """Shadow-ray tree (default) and the reference's object-tree walk give
+@pytest.mark.parametrize("flags", [0, SHADOW_TREE, EXACT])
+def test_shadow_small_scene(cuda, flags):
+    """Object-tree walk (default, exact order) and the shadow-ray tree give
     the oracle's answers bit for bit."""
     sc = scenes.config_small()
-    sc.render.flags = 1 if reference_order else 0
+    sc.render.flags = flags
     ds = api.DeviceScene(sc)
     O = T.OracleScene(sc)
     s = _shadow_rays(sc, 60000, 5)
     assert np.array_equal(_run_shadow(cuda, ds, s), O.trace_shadow(s))
 
 
-@pytest.mark.parametrize("reference_order", [False, True])
-def test_shadow_many_objects(cuda, reference_order):
+@pytest.mark.parametrize("flags", [0, SHADOW_TREE, EXACT])
+def test_shadow_many_objects(cuda, flags):
     sc = scenes.config_large(seed=3, resx=64, resy=48, spp=1, grid=4)
-    sc.render.flags = 1 if reference_order else 0
+    sc.render.flags = flags
     ds = api.DeviceScene(sc)
     O = T.OracleScene(sc)
     s = _shadow_rays(sc, 40000, 6)
@@ -108,19 +121,23 @@ def test_reciprocal_division_is_exact(cuda):
     assert bad.value == 0
 
 
-def test_shadow_bias_below_min_raydist(cuda):
+@pytest.mark.parametrize("flags", [0, SHADOW_TREE])
+def test_shadow_bias_below_min_raydist(cuda, flags):
     """self_bias smaller than MIN_RAYDIST: the shadow-ray tree starts its walk
     at the earlier origin and still matches the oracle."""
     sc = scenes.config_large(seed=4, resx=64, resy=48, spp=1, grid=3)
     sc.render.self_bias = 0.00001
+    sc.render.flags = flags
     ds = api.DeviceScene(sc)
     O = T.OracleScene(sc)
     s = _shadow_rays(sc, 30000, 8)
     assert np.array_equal(_run_shadow(cuda, ds, s), O.trace_shadow(s))
 
 
-def test_no_shadow_casters(cuda):
+@pytest.mark.parametrize("flags", [0, SHADOW_TREE])
+def test_no_shadow_casters(cuda, flags):
     sc = scenes.config_small(32, 24)
+    sc.render.flags = flags
     for m in sc.meshes:
         m.cast_shadows = False
     ds = api.DeviceScene(sc)

@@ -11,7 +11,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libyafray_b200.so")
+# YAFRAY_B200_LIB selects another build of the library (variant builds for A/B timing)
+LIB_PATH = os.environ.get("YAFRAY_B200_LIB", os.path.join(HERE, "libyafray_b200.so"))
 
 YR_OK = 0
 STATUS_NAMES = {

@@ -16,8 +16,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
-OUT = os.path.join(HERE, "libyafray_b200.so")
+BUILD = os.environ.get("YR_BUILD_DIR", os.path.join(HERE, "_build"))
+OUT = os.environ.get("YR_OUT", os.path.join(HERE, "libyafray_b200.so"))
+EXTRA = os.environ.get("YR_DEFINES", "").split()  # variant builds for A/B measurements
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
@@ -30,7 +31,7 @@ def _compile(src: str) -> str:
             [os.path.getmtime(src)] + [os.path.getmtime(h) for h in glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))]
             + [os.path.getmtime(os.path.join(HERE, "..", "include", "yr.h"))]):
         return obj
-    cmd = [NVCC] + ARCH + COMMON + ["-c", src, "-o", obj]
+    cmd = [NVCC] + ARCH + COMMON + EXTRA + ["-c", src, "-o", obj]
     if src.endswith(".cu"):
         cmd[1:1] = ["-Xptxas", "-v"] if os.environ.get("YR_PTXAS_V") else []
     else:

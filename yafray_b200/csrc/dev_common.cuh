@@ -120,7 +120,9 @@ struct DevScene {
     uint32_t sh_nnodes;
     uint32_t sh_nprims;
     float sh_tb[6];
-    int use_sh_tree;            // 0: shadow rays walk the object tree (reference order)
+    int use_sh_tree;            // 1: shadow rays use the shadow-ray tree
+    int exact_order;            // 1: exact slab tests in the object tree
+    float coord_max;            // max |coordinate| of the object tree's root box
     int *status;                // device status word
 };
 

@@ -22,6 +22,9 @@ namespace yr {
 // [2^-60, 2^60] (where an intermediate could leave the normal range) take
 // the IEEE division; a zero dividend returns the correctly signed zero.
 __device__ __forceinline__ float div_rcp(float a, float b, float y) {
+#ifdef YR_SLAB_IEEE
+    return __fdiv_rn(a, b);
+#endif
     const float q0 = __fmul_rn(a, y);
     if (a == 0.f) return q0;
     const float aa = fabsf(a), ab = fabsf(b);
@@ -87,6 +90,68 @@ __device__ __forceinline__ bool box_where(const float *bmin, const float *bmax, 
     if (!box_enter_leave(bmin, bmax, from, R, dist, e, l)) return false;
     where = (e > 0.f) ? e : 0.f;
     return true;
+}
+
+// A ray prepared for the object-tree walk.  Unless the scene asks for the
+// exact order, the walk uses a conservative slab test: t = b*y + (-f*y)
+// with one FMA per plane, widened by a bound on its rounding error so that
+// the interval contains the one bound_t::cross computes.  Crossing tests
+// then never reject a box that the exact test accepts, and entry distances
+// are lower bounds, so pruning by the closest hit so far stays safe; only
+// the visiting order of boxes whose entry distances agree to within that
+// error can differ (which changes the reported object only when two
+// objects are hit at exactly the same distance).
+struct ObjRay {
+    V3 from;
+    RayR R;
+    float nf[3];   // RN(-from*y)
+    float err[3];  // per-axis error bound of t
+    bool exact;
+};
+
+__device__ __forceinline__ ObjRay make_objray(const V3 &from, const RayR &R, float coord_max, bool exact) {
+    ObjRay q;
+    q.from = from;
+    q.R = R;
+    q.exact = exact;
+    const float f[3] = {from.x, from.y, from.z}, y[3] = {R.inv.x, R.inv.y, R.inv.z};
+    for (int k = 0; k < 3; k++) {
+        q.nf[k] = -f[k] * y[k];
+        // |t~ - t| <= 2u|t| + u|f y| (+ rounding) with |t| <= (M + |f|)|y|:
+        // 2^-21 = 8u on (M + 2|f|)|y| leaves a factor of ~2 of headroom
+        q.err[k] = (coord_max + 2.f * fabsf(f[k])) * fabsf(y[k]) * 0x1p-21f;
+    }
+    return q;
+}
+
+__device__ __forceinline__ bool box_where_obj(const float *bmin, const float *bmax, const ObjRay &q, float dist,
+                                              float &where) {
+    if (q.exact) return box_where(bmin, bmax, q.from, q.R, dist, where);
+    float lmin = -1.f, lmax = -1.f;
+    const float d[3] = {q.R.d.x, q.R.d.y, q.R.d.z}, y[3] = {q.R.inv.x, q.R.inv.y, q.R.inv.z};
+    bool first = true;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (d[k] == 0.f) continue;
+        float t1 = __fmaf_rn(bmin[k], y[k], q.nf[k]), t2 = __fmaf_rn(bmax[k], y[k], q.nf[k]);
+        if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+        t1 -= q.err[k];
+        t2 += q.err[k];
+        if (first) {
+            lmin = t1;
+            lmax = t2;
+            first = false;
+        } else {
+            if (t1 > lmin) lmin = t1;
+            if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;
+        }
+        if ((lmax < 0.f) || (lmin > dist)) return false;
+    }
+    if ((lmin <= lmax) && (lmax >= 0.f) && (lmin <= dist)) {
+        where = (lmin > 0.f) ? lmin : 0.f;
+        return true;
+    }
+    return false;
 }
 
 struct Tri {
@@ -292,7 +357,7 @@ struct ObjIter {
     int current;             // object index or -1
     float maximun;
 
-    __device__ __forceinline__ void down(const DevScene &S, int node, const V3 &from, const RayR &ray) {
+    __device__ __forceinline__ void down(const DevScene &S, int node, const ObjRay &ray) {
         for (;;) {
             const DevObjNode nd = S.otree[node];
             if (nd.left < 0) {
@@ -301,8 +366,8 @@ struct ObjIter {
             }
             const DevObjNode L = S.otree[nd.left], R = S.otree[nd.right];
             float hl = __int_as_float(0x7f800000), hr = __int_as_float(0x7f800000);
-            const bool hitl = box_where(L.bmin, L.bmax, from, ray, maximun, hl);
-            const bool hitr = box_where(R.bmin, R.bmax, from, ray, maximun, hr);
+            const bool hitl = box_where_obj(L.bmin, L.bmax, ray, maximun, hl);
+            const bool hitr = box_where_obj(R.bmin, R.bmax, ray, maximun, hr);
             if (!hitl && !hitr) {
                 if (sp == 0) {
                     current = -1;
@@ -326,22 +391,22 @@ struct ObjIter {
         }
     }
 
-    __device__ __forceinline__ void start(const DevScene &S, const V3 &from, const RayR &ray, float maxd) {
+    __device__ __forceinline__ void start(const DevScene &S, const ObjRay &ray, float maxd) {
         maximun = maxd;
         sp = 0;
         current = -1;
         if (S.notree == 0) return;
         const DevObjNode r = S.otree[0];
         float w = 0.f;
-        if (box_where(r.bmin, r.bmax, from, ray, maximun, w)) down(S, 0, from, ray);
+        if (box_where_obj(r.bmin, r.bmax, ray, maximun, w)) down(S, 0, ray);
     }
 
-    __device__ __forceinline__ void next(const DevScene &S, const V3 &from, const RayR &ray) {
+    __device__ __forceinline__ void next(const DevScene &S, const ObjRay &ray) {
         current = -1;
         while (sp > 0 && __int_as_float(st[sp - 1].y) > maximun) sp--;
         if (sp > 0) {
             const int node = st[--sp].x;
-            down(S, node, from, ray);
+            down(S, node, ray);
         }
     }
 
@@ -517,6 +582,7 @@ struct SceneHit {
 __device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V3 &dir, bool pass_limit,
                                          bool shadow_only, const KdStack &stk) {
     const RayR ray = make_rayr(dir);
+    const ObjRay oray = make_objray(f, ray, S.coord_max, S.exact_order != 0);
     SceneHit best;
     best.t = 0.f;
     best.object = -1;
@@ -526,10 +592,10 @@ __device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V
     const float inf = __int_as_float(0x7f800000);
     float limit = inf;
     ObjIter it;
-    it.start(S, f, ray, inf);
+    it.start(S, oray, inf);
     while (it.current >= 0) {
         const int o = it.current;
-        const DevObject obj = S.objects[o];
+        const DevObject &obj = S.objects[o];
         if (!(shadow_only && !(obj.flags & 1u))) {
             const float dis = pass_limit ? limit : inf;
             float Z = dis;
@@ -547,7 +613,7 @@ __device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V
                 }
             }
         }
-        it.next(S, f, ray);
+        it.next(S, oray);
     }
     return best;
 }
@@ -559,11 +625,12 @@ __device__ inline bool scene_occluded_ref(const DevScene &S, const V3 &p, int ow
     const V3 self = p + dir * self_bias;
     const V3 p2 = p + dir * kMinRayDist;
     const RayR ray = make_rayr(dir);
+    const ObjRay oray = make_objray(p2, ray, S.coord_max, S.exact_order != 0);
     ObjIter it;
-    it.start(S, p2, ray, dist);
+    it.start(S, oray, dist);
     while (it.current >= 0) {
         const int o = it.current;
-        const DevObject obj = S.objects[o];
+        const DevObject &obj = S.objects[o];
         if (obj.flags & 1u) {
             float Z = dist;
             KdResult r{kNone, 0, 0};
@@ -572,7 +639,7 @@ __device__ inline bool scene_occluded_ref(const DevScene &S, const V3 &p, int ow
             tests += r.tests;
             if (h) return true;
         }
-        it.next(S, p2, ray);
+        it.next(S, oray);
     }
     return false;
 }

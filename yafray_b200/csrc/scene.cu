@@ -381,7 +381,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
             for (size_t k = 0; k < 3 * (size_t)od.ntris; k++) mt.push_back(od.tris[k] + vbase);
             for (uint32_t t = 0; t < od.ntris; t++) remap.push_back(objects[o].tri_base + t);
         }
-        if (!remap.empty()) {
+        if (!remap.empty() && (desc->render.flags & YR_RENDER_SHADOW_TREE)) {
             KdTree st_tree;
             KdParams kp;
             kp.max_leaf = 1;                   // deeper tree, fewer triangle tests
@@ -470,7 +470,12 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.sh_nnodes = (uint32_t)sh_nodes.size();
     D.sh_nprims = (uint32_t)sh_prims.size();
     std::memcpy(D.sh_tb, sh_tb, sizeof(sh_tb));
-    D.use_sh_tree = (desc->render.flags & YR_RENDER_REFERENCE_SHADOWS) ? 0 : 1;
+    D.use_sh_tree = (desc->render.flags & YR_RENDER_SHADOW_TREE) ? 1 : 0;
+    D.exact_order = (desc->render.flags & YR_RENDER_EXACT_ORDER) ? 1 : 0;
+    D.coord_max = 0.f;
+    if (!otree.empty())
+        for (int k = 0; k < 3; k++)
+            D.coord_max = std::max(D.coord_max, std::max(std::fabs(otree[0].bmin[k]), std::fabs(otree[0].bmax[k])));
     D.status = s->status;
 
     // ---- shading records
