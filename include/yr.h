@@ -377,16 +377,6 @@ YR_API yr_status yr_params_set(yr_scene *scene, const float *params);
 YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, float *dparams,
                              float *loss_out, void *stream);
 
-/* ------------------------------------------------------------------------
- * Diagnostics.
- * ------------------------------------------------------------------------ */
-/* Compare the reciprocal-based division used by the slab tests with IEEE
- * division on n pseudo-random operand pairs on the current device; the
- * number of results that differ in any bit is written to *mismatches
- * (expected: 0).  No reference counterpart: it verifies this library's own
- * arithmetic. */
-YR_API yr_status yr_selftest_division(uint64_t n, uint64_t seed, uint64_t *mismatches);
-
 #ifdef __cplusplus
 }
 #endif

@@ -108,40 +108,3 @@ def test_empty_query(cuda):
     sc = scenes.config_small(32, 24)
     ds = api.DeviceScene(sc)
     assert _run_closest(cuda, ds, np.zeros((0, 8), np.float32)).shape == (0, 4)
-
-
-def test_reciprocal_division_is_exact(cuda):
-    """The slab tests' reciprocal + Markstein-correction division returns the
-    IEEE quotient bit for bit (200 M operand pairs)."""
-    import ctypes as C
-    from yafray_b200 import abi
-    lib = abi.load()
-    bad = C.c_uint64(123)
-    abi.check(lib.yr_selftest_division(200_000_000, 12345, C.byref(bad)), "yr_selftest_division")
-    assert bad.value == 0
-
-
-@pytest.mark.parametrize("flags", [0, SHADOW_TREE])
-def test_shadow_bias_below_min_raydist(cuda, flags):
-    """self_bias smaller than MIN_RAYDIST: the shadow-ray tree starts its walk
-    at the earlier origin and still matches the oracle."""
-    sc = scenes.config_large(seed=4, resx=64, resy=48, spp=1, grid=3)
-    sc.render.self_bias = 0.00001
-    sc.render.flags = flags
-    ds = api.DeviceScene(sc)
-    O = T.OracleScene(sc)
-    s = _shadow_rays(sc, 30000, 8)
-    assert np.array_equal(_run_shadow(cuda, ds, s), O.trace_shadow(s))
-
-
-@pytest.mark.parametrize("flags", [0, SHADOW_TREE])
-def test_no_shadow_casters(cuda, flags):
-    sc = scenes.config_small(32, 24)
-    sc.render.flags = flags
-    for m in sc.meshes:
-        m.cast_shadows = False
-    ds = api.DeviceScene(sc)
-    O = T.OracleScene(sc)
-    s = _shadow_rays(sc, 5000, 9)
-    occ = _run_shadow(cuda, ds, s)
-    assert np.array_equal(occ, O.trace_shadow(s)) and occ.sum() == 0

@@ -162,7 +162,6 @@ SIGNATURES = {
     "yr_params_get": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "yr_params_set": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "yr_backward": (C.c_int, [_P, C.POINTER(YrBackwardDesc), _P, C.POINTER(C.c_float), _P]),
-    "yr_selftest_division": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
 }
 
 _lib = None

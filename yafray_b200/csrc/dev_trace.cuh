@@ -10,32 +10,11 @@
 
 namespace yr {
 
-// a/b rounded to nearest, given y = RN(1/b): one correction step of
-// Markstein's method (P. Markstein, "Computation of elementary functions on
-// the IBM RISC System/6000 processor", IBM J. R&D 34(1), 1990; Theorem 4.10
-// of the Handbook of Floating-Point Arithmetic): with q0 = RN(a*y) within
-// one ulp of a/b and r = a - b*q0 exact through an FMA, RN(q0 + r*y) is the
-// correctly rounded quotient.  The slab tests divide by the same three ray
-// components many times per ray, so the three reciprocals are formed once
-// (with IEEE division) and every quotient costs a multiply and two FMAs on
-// the FMA pipe instead of a MUFU-based division.  Operands outside
-// [2^-60, 2^60] (where an intermediate could leave the normal range) take
-// the IEEE division; a zero dividend returns the correctly signed zero.
-__device__ __forceinline__ float div_rcp(float a, float b, float y) {
-#ifdef YR_SLAB_IEEE
-    return __fdiv_rn(a, b);
-#endif
-    const float q0 = __fmul_rn(a, y);
-    if (a == 0.f) return q0;
-    const float aa = fabsf(a), ab = fabsf(b);
-    if (aa < 0x1p-60f || aa > 0x1p60f || ab < 0x1p-60f || ab > 0x1p60f) return __fdiv_rn(a, b);
-    const float r = __fmaf_rn(-q0, b, a);
-    return __fmaf_rn(r, y, q0);
-}
-
 // A ray with the reciprocals of its direction (1.f/d, correctly rounded,
 // which is also kdTree_t::Intersect's invDir: 1.0/d in double narrowed to
-// float rounds to the same value).
+// float rounds to the same value).  The exact slab test divides (IEEE) as
+// bound_t::cross does; the reciprocals serve the kd split distances and the
+// conservative object-tree test.
 struct RayR {
     V3 d;
     V3 inv;
@@ -56,21 +35,21 @@ __device__ __forceinline__ bool box_enter_leave(const float *bmin, const float *
     float lmin = -1.f, lmax = -1.f;
     const V3 &ray = R.d;
     if (ray.x != 0.f) {
-        float t1 = div_rcp(bmin[0] - from.x, ray.x, R.inv.x), t2 = div_rcp(bmax[0] - from.x, ray.x, R.inv.x);
+        float t1 = (bmin[0] - from.x) / ray.x, t2 = (bmax[0] - from.x) / ray.x;
         if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
         lmin = t1;
         lmax = t2;
         if ((lmax < 0.f) || (lmin > dist)) return false;
     }
     if (ray.y != 0.f) {
-        float t1 = div_rcp(bmin[1] - from.y, ray.y, R.inv.y), t2 = div_rcp(bmax[1] - from.y, ray.y, R.inv.y);
+        float t1 = (bmin[1] - from.y) / ray.y, t2 = (bmax[1] - from.y) / ray.y;
         if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
         if (t1 > lmin) lmin = t1;
         if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;
         if ((lmax < 0.f) || (lmin > dist)) return false;
     }
     if (ray.z != 0.f) {
-        float t1 = div_rcp(bmin[2] - from.z, ray.z, R.inv.z), t2 = div_rcp(bmax[2] - from.z, ray.z, R.inv.z);
+        float t1 = (bmin[2] - from.z) / ray.z, t2 = (bmax[2] - from.z) / ray.z;
         if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
         if (t1 > lmin) lmin = t1;
         if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;

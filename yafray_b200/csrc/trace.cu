@@ -6,15 +6,6 @@ namespace yr {
 
 constexpr int kTraceBlock = 128;
 
-__device__ __forceinline__ uint32_t fmix_u32(uint32_t h) {
-    h ^= h >> 16;
-    h *= 0x85ebca6bu;
-    h ^= h >> 13;
-    h *= 0xc2b2ae35u;
-    h ^= h >> 16;
-    return h;
-}
-
 __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(DevScene S, const yr_ray *__restrict__ rays, uint32_t n,
                                                                 yr_hit *__restrict__ hits, int shadow_only) {
     uint2 stk_nt[kKdStackCap];
@@ -62,30 +53,6 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(DevScene S, const 
     }
 }
 
-// Check div_rcp against IEEE division on n pseudo-random operand pairs whose
-// exponents span [-80, 80] (inside and outside the fast path's range) and
-// on operands drawn from the slab test's typical magnitudes.
-__global__ void k_selftest_division(uint64_t n, uint64_t seed, unsigned long long *bad) {
-    unsigned long long local = 0;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t h1 = fmix_u32((uint32_t)i ^ (uint32_t)seed), h2 = fmix_u32(h1 ^ 0x9e3779b9u ^ (uint32_t)(i >> 32));
-        const uint32_t h3 = fmix_u32(h2 + 0x7f4a7c15u), h4 = fmix_u32(h3 ^ (uint32_t)(seed >> 32));
-        float a, b;
-        if (i & 1) {  // wide exponent range
-            a = __uint_as_float((h1 & 0x807fffffu) | ((uint32_t)(127 - 80 + (h3 % 161)) << 23));
-            b = __uint_as_float((h2 & 0x807fffffu) | ((uint32_t)(127 - 80 + (h4 % 161)) << 23));
-        } else {      // box-coordinate differences over unit-vector components
-            a = (float)((int)(h1 % 2000001u) - 1000000) * 1e-4f;
-            b = ((float)(h2 >> 8) * (1.0f / 16777216.0f)) * 2.f - 1.f;
-            if (b == 0.f) b = 0.5f;
-        }
-        const float y = 1.f / b;
-        const float q1 = div_rcp(a, b, y), q2 = a / b;
-        if (__float_as_uint(q1) != __float_as_uint(q2) && !(q1 != q1 && q2 != q2)) local++;
-    }
-    if (local) atomicAdd(bad, local);
-}
-
 int grid_for(uint32_t n, int block) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -128,20 +95,6 @@ YR_API yr_status yr_trace_shadow(yr_scene *scene, const yr_shadow_ray *rays, uin
     yr_status r = cudaGetLastError() == cudaSuccess ? take_status(scene, st) : YR_ERR_CUDA;
     cudaSetDevice(prev);
     return r;
-}
-
-YR_API yr_status yr_selftest_division(uint64_t n, uint64_t seed, uint64_t *mismatches) {
-    if (!mismatches) return YR_ERR_INVALID_ARG;
-    unsigned long long *d = nullptr;
-    if (cudaMalloc(&d, sizeof(*d)) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
-    cudaMemset(d, 0, sizeof(*d));
-    k_selftest_division<<<148 * 8, 256>>>(n, seed, d);
-    unsigned long long h = 0;
-    const bool ok = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess;
-    cudaFree(d);
-    if (!ok) return YR_ERR_CUDA;
-    *mismatches = h;
-    return YR_OK;
 }
 
 }  // extern "C"
