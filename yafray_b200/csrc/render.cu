@@ -620,6 +620,107 @@ __global__ void k_count(Wave W, int which) {
 
 int grid_for(uint32_t n, int block);
 
+// ------------------------------------------------------------ wave layout
+// Shape of a render: slots per vertex, paths per camera sample, lights.
+struct Plan {
+    uint32_t npix;    // image pixels
+    uint32_t rpix;    // region pixels
+    uint64_t total;   // camera samples to render
+    uint32_t ns;      // shadow slots per vertex
+    uint32_t npath;   // path samples per camera sample
+    uint32_t nl;      // lights (>= 1 for sizing)
+    int depth;        // path depth (>= 1 for sizing)
+};
+
+static yr_status make_plan(const yr_scene *scene, Plan &P) {
+    const DevRender &R = scene->rdr;
+    P.npix = (uint32_t)R.cam.resx * (uint32_t)R.cam.resy;
+    P.rpix = (uint32_t)R.rw * (uint32_t)R.rh;
+    P.total = (uint64_t)P.rpix * R.spp;
+    if (P.total >= (1ull << 32)) return YR_ERR_TOO_LARGE;
+    if (R.path_light >= 0 && R.path_depth > 15) return YR_ERR_UNSUPPORTED;
+    P.ns = 0;
+    for (const DevLight &L : scene->lights) {
+        if (L.type == YR_LIGHT_POINT) P.ns += 1;
+        else if (L.type == YR_LIGHT_AREA || L.type == YR_LIGHT_HEMI) P.ns += (uint32_t)L.samples;
+    }
+    P.npath = R.path_light >= 0 ? (uint32_t)R.path_samples : 0;
+    P.nl = (uint32_t)std::max(1, R.nlights);
+    P.depth = std::max(1, R.path_depth);
+    return YR_OK;
+}
+
+constexpr int kNumBufs = 22;
+constexpr size_t kBufAlign = 256;
+
+// Bytes of each scratch buffer for a wave of `wcap` camera samples, in the
+// order assign_wave() hands them out.
+static void wave_sizes(const Plan &P, uint32_t wcap, size_t *b) {
+    const size_t w = wcap, pc = (size_t)wcap * std::max(1u, P.npath), vc = std::max(w, pc);
+    const size_t slots = vc * std::max(P.ns, 1u);
+    const size_t f4 = sizeof(float4);
+    size_t sizes[kNumBufs] = {f4 * w,  f4 * w * P.nl, f4 * w * P.nl, f4 * w,  f4 * pc, f4 * pc,
+                              f4 * pc, f4 * pc,       f4 * pc,       f4 * pc, f4 * pc * P.depth, f4 * pc * P.nl,
+                              f4 * slots, slots,      f4 * slots,    f4 * slots, 4 * slots, 4 * pc,
+                              4 * pc,  4 * 8,         8 * 4,         8 * 3 * YR_K_COUNT};
+    for (int i = 0; i < kNumBufs; i++) b[i] = sizes[i];
+}
+
+static size_t wave_bytes(const Plan &P, uint32_t wcap) {
+    size_t b[kNumBufs], t = 0;
+    wave_sizes(P, wcap, b);
+    for (int i = 0; i < kNumBufs; i++) t += (b[i] + kBufAlign - 1) / kBufAlign * kBufAlign;
+    return t;
+}
+
+// Point the wave's arrays into one block of at least wave_bytes(P, wcap).
+static void assign_wave(const Plan &P, uint32_t wcap, char *base, Wave &W) {
+    size_t b[kNumBufs];
+    wave_sizes(P, wcap, b);
+    void *ptr[kNumBufs];
+    size_t off = 0;
+    for (int i = 0; i < kNumBufs; i++) {
+        ptr[i] = base + off;
+        off += (b[i] + kBufAlign - 1) / kBufAlign * kBufAlign;
+    }
+    int k = 0;
+    W.hit0 = (float4 *)ptr[k++];
+    W.lterm = (float4 *)ptr[k++];
+    W.aux = (float4 *)ptr[k++];
+    W.diff0 = (float4 *)ptr[k++];
+    W.p_where = (float4 *)ptr[k++];
+    W.p_ray = (float4 *)ptr[k++];
+    W.p_col = (float4 *)ptr[k++];
+    W.p_next = (float4 *)ptr[k++];
+    W.p_nray = (float4 *)ptr[k++];
+    W.p_hit = (float4 *)ptr[k++];
+    W.p_contri = (float4 *)ptr[k++];
+    W.p_aux = (float4 *)ptr[k++];
+    W.slot_c = (float4 *)ptr[k++];
+    W.slot_f = (uint8_t *)ptr[k++];
+    W.shq0 = (float4 *)ptr[k++];
+    W.shq1 = (float4 *)ptr[k++];
+    W.shq_slot = (uint32_t *)ptr[k++];
+    W.bq = (uint32_t *)ptr[k++];
+    W.bq2 = (uint32_t *)ptr[k++];
+    W.counters = (uint32_t *)ptr[k++];
+    W.rays = (unsigned long long *)ptr[k++];
+    W.kst = (unsigned long long *)ptr[k++];
+    W.ns = P.ns;
+    W.npath = P.npath;
+}
+
+// Largest wave (whole pixels) whose scratch fits in `budget` bytes.
+static uint32_t wave_for_budget(const Plan &P, const DevRender &R, size_t budget) {
+    uint64_t lo = 0, hi = P.rpix;
+    while (lo < hi) {  // largest pixel count that fits
+        const uint64_t mid = (lo + hi + 1) / 2;
+        if (wave_bytes(P, (uint32_t)(mid * R.spp)) <= budget) lo = mid;
+        else hi = mid - 1;
+    }
+    return (uint32_t)(lo * R.spp);
+}
+
 static yr_status scratch(yr_scene *s, int i, size_t bytes, void **p) {
     if ((int)s->scratch.size() <= i) s->scratch.resize(i + 1);
     DevBuf &b = s->scratch[i];
@@ -634,85 +735,14 @@ static yr_status scratch(yr_scene *s, int i, size_t bytes, void **p) {
     return YR_OK;
 }
 
-}  // namespace yr
-
-using namespace yr;
-
-extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host, yr_render_stats *stats,
-                                      void *stream) {
-    if (!scene || !rgba) return YR_ERR_INVALID_ARG;
-    int prev = 0;
-    cudaGetDevice(&prev);
-    cudaSetDevice(scene->device);
-    cudaStream_t st = (cudaStream_t)stream;
+// All waves of one render on `st`.  `out` is the device RGBA image.
+// With `events` false no CUDA event is created (stats->ms and the kernel
+// times stay 0).
+static yr_status run_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out,
+                           yr_render_stats *stats, cudaStream_t st, bool events) {
     DevRender &R = scene->rdr;
-    const uint32_t npix = (uint32_t)R.cam.resx * (uint32_t)R.cam.resy;  // image
-    const uint32_t rpix = (uint32_t)R.rw * (uint32_t)R.rh;              // region
-    const uint64_t total = (uint64_t)rpix * R.spp;
-    yr_status ret = YR_OK;
-    auto done = [&](yr_status e) {
-        cudaSetDevice(prev);
-        return e;
-    };
-    if (total >= (1ull << 32)) return done(YR_ERR_TOO_LARGE);
-    if (R.path_light >= 0 && R.path_depth > 15) return done(YR_ERR_UNSUPPORTED);
-    uint32_t ns = 0;
-    for (const DevLight &L : scene->lights) {
-        if (L.type == YR_LIGHT_POINT) ns += 1;
-        else if (L.type == YR_LIGHT_AREA || L.type == YR_LIGHT_HEMI) ns += (uint32_t)L.samples;
-    }
-    const uint32_t npath = R.path_light >= 0 ? (uint32_t)R.path_samples : 0;
-    // wave: whole pixels, bounded so that the slot arrays stay near 1.5 GB
-    const uint64_t per_cs = (uint64_t)std::max<uint32_t>(1, std::max(1u, npath)) * std::max(ns, 1u) * 64 + 512;
-    uint64_t wave_px = std::max<uint64_t>(1, (1536ull << 20) / (per_cs * R.spp));
-    wave_px = std::min<uint64_t>(wave_px, rpix);
-    const uint32_t wcap = (uint32_t)(wave_px * R.spp);
-    const uint32_t nl = std::max(1, R.nlights);
-    const uint32_t pcap = wcap * std::max(1u, npath);
-    const uint32_t vcap = std::max(wcap, pcap);
-    const int depth = std::max(1, R.path_depth);
-
-    Wave W;
-    std::memset(&W, 0, sizeof(W));
-    void *ptr;
-    int si = 0;
-#define YR_SCRATCH(field, bytes)                                               \
-    do {                                                                       \
-        if ((ret = scratch(scene, si++, (bytes), &ptr)) != YR_OK) return done(ret); \
-        W.field = (decltype(W.field))ptr;                                      \
-    } while (0)
-    YR_SCRATCH(hit0, sizeof(float4) * wcap);
-    YR_SCRATCH(lterm, sizeof(float4) * wcap * nl);
-    YR_SCRATCH(aux, sizeof(float4) * wcap * nl);
-    YR_SCRATCH(diff0, sizeof(float4) * wcap);
-    YR_SCRATCH(p_where, sizeof(float4) * pcap);
-    YR_SCRATCH(p_ray, sizeof(float4) * pcap);
-    YR_SCRATCH(p_col, sizeof(float4) * pcap);
-    YR_SCRATCH(p_next, sizeof(float4) * pcap);
-    YR_SCRATCH(p_nray, sizeof(float4) * pcap);
-    YR_SCRATCH(p_hit, sizeof(float4) * pcap);
-    YR_SCRATCH(p_contri, sizeof(float4) * (size_t)pcap * depth);
-    YR_SCRATCH(p_aux, sizeof(float4) * (size_t)pcap * nl);
-    YR_SCRATCH(slot_c, sizeof(float4) * (size_t)vcap * std::max(ns, 1u));
-    YR_SCRATCH(slot_f, (size_t)vcap * std::max(ns, 1u));
-    YR_SCRATCH(shq0, sizeof(float4) * (size_t)vcap * std::max(ns, 1u));
-    YR_SCRATCH(shq1, sizeof(float4) * (size_t)vcap * std::max(ns, 1u));
-    YR_SCRATCH(shq_slot, sizeof(uint32_t) * (size_t)vcap * std::max(ns, 1u));
-    YR_SCRATCH(bq, sizeof(uint32_t) * pcap);
-    YR_SCRATCH(bq2, sizeof(uint32_t) * pcap);
-    YR_SCRATCH(counters, sizeof(uint32_t) * 8);
-    YR_SCRATCH(rays, sizeof(unsigned long long) * 4);
-    YR_SCRATCH(kst, sizeof(unsigned long long) * 3 * YR_K_COUNT);
-#undef YR_SCRATCH
-    float *out = rgba;
-    if (rgba_on_host) {
-        if ((ret = scratch(scene, si++, sizeof(float) * 4 * (size_t)npix, &ptr)) != YR_OK) return done(ret);
-        out = (float *)ptr;
-    }
     W.out = out;
-    W.ns = ns;
-    W.npath = npath;
-    const bool kstats = stats && stats->want_kernel_stats;
+    const bool kstats = events && stats && stats->want_kernel_stats;
     double kms[YR_K_COUNT] = {0};
     uint32_t klaunch[YR_K_COUNT] = {0};
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> kev;
@@ -730,23 +760,27 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
         cudaEventRecord(b, st);
         kev.push_back({cls, {a, b}});
     };
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (events) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, st);
+    }
     cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
     cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
     // pixels outside the region are written as 0 (scene.cc:773)
-    if (rpix != npix) cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)npix, st);
+    if (P.rpix != P.npix) cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
+    const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
     if (R.raydepth <= 0) {
         // raytrace() returns black at the ray-level cap (scene.cc:204-209)
-        cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)npix, st);
+        cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
     } else {
-        const int gq = grid_for(vcap * std::max(ns, 1u), kBlock);
+        const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
         const DevScene &D = scene->dev;
-        for (uint64_t b = 0; b < total; b += wcap) {
+        const uint32_t npath = P.npath;
+        for (uint64_t b = 0; b < P.total; b += wcap) {
             W.base = (uint32_t)b;
-            W.count = (uint32_t)std::min<uint64_t>(wcap, total - b);
+            W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
             const int g = (int)((W.count + kBlock - 1) / kBlock);
             cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
             timed(YR_K_PRIMARY, [&] { k_primary<<<g, kBlock, 0, st>>>(D, R, W); });
@@ -755,7 +789,7 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
             timed(YR_K_SHADOW, [&] { k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
             timed(YR_K_GATHER, [&] { k_gather_camera<<<g, kBlock, 0, st>>>(R, W); });
             if (npath > 0) {
-                const size_t nc = (size_t)W.count * npath * depth;
+                const size_t nc = (size_t)W.count * npath * P.depth;
                 timed(YR_K_OTHER, [&] {
                     k_clear_contri<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(W, nc);
                 });
@@ -776,25 +810,24 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
             timed(YR_K_OTHER, [&] { k_finish<<<gf, kBlock, 0, st>>>(R, W); });
         }
     }
-    cudaEventRecord(e1, st);
-    if (cudaGetLastError() != cudaSuccess) return done(YR_ERR_CUDA);
-    if ((ret = take_status(scene, st)) != YR_OK) return done(ret);
+    if (events) cudaEventRecord(e1, st);
+    if (cudaGetLastError() != cudaSuccess) return YR_ERR_CUDA;
+    yr_status ret = take_status(scene, st);
     if (stats) {
         unsigned long long r[4] = {0, 0, 0, 0}, k[3 * YR_K_COUNT];
-        cudaMemcpy(r, W.rays, sizeof(r), cudaMemcpyDeviceToHost);
-        cudaMemcpy(k, W.kst, sizeof(k), cudaMemcpyDeviceToHost);
-        stats->rays_primary = (R.raydepth > 0) ? total : 0;
+        cudaMemcpyAsync(r, W.rays, sizeof(r), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(k, W.kst, sizeof(k), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        stats->rays_primary = (R.raydepth > 0) ? P.total : 0;
         stats->rays_shadow = r[1];
         stats->rays_bounce = r[2];
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        if (events) cudaEventElapsedTime(&ms, e0, e1);
         stats->ms = ms;
         for (auto &e : kev) {
             float m = 0.f;
             cudaEventElapsedTime(&m, e.second.first, e.second.second);
             kms[e.first] += m;
-            cudaEventDestroy(e.second.first);
-            cudaEventDestroy(e.second.second);
         }
         for (int c = 0; c < YR_K_COUNT; c++) {
             stats->kernel_ms[c] = kms[c];
@@ -804,10 +837,52 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
             stats->kernel_tests[c] = k[3 * c + 2];
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    for (auto &e : kev) {
+        cudaEventDestroy(e.second.first);
+        cudaEventDestroy(e.second.second);
+    }
+    if (events) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return ret;
+}
+
+}  // namespace yr
+
+using namespace yr;
+
+extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host, yr_render_stats *stats,
+                                      void *stream) {
+    if (!scene || !rgba) return YR_ERR_INVALID_ARG;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(scene->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    auto done = [&](yr_status e) {
+        cudaSetDevice(prev);
+        return e;
+    };
+    Plan P;
+    yr_status ret = make_plan(scene, P);
+    if (ret != YR_OK) return done(ret);
+    // wave: whole pixels, scratch near 1.5 GB at most
+    const uint32_t wcap = std::max(scene->rdr.spp, wave_for_budget(P, scene->rdr, 1536ull << 20));
+    void *block = nullptr;
+    if ((ret = scratch(scene, 0, wave_bytes(P, wcap), &block)) != YR_OK) return done(ret);
+    Wave W;
+    std::memset(&W, 0, sizeof(W));
+    assign_wave(P, wcap, (char *)block, W);
+    float *out = rgba;
     if (rgba_on_host) {
-        if (cudaMemcpyAsync(rgba, out, sizeof(float) * 4 * (size_t)npix, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        void *ptr = nullptr;
+        if ((ret = scratch(scene, 1, sizeof(float) * 4 * (size_t)P.npix, &ptr)) != YR_OK) return done(ret);
+        out = (float *)ptr;
+    }
+    ret = run_waves(scene, P, wcap, W, out, stats, st, true);
+    if (ret != YR_OK) return done(ret);
+    if (rgba_on_host) {
+        if (cudaMemcpyAsync(rgba, out, sizeof(float) * 4 * (size_t)P.npix, cudaMemcpyDeviceToHost, st) != cudaSuccess)
             return done(YR_ERR_CUDA);
         if (cudaStreamSynchronize(st) != cudaSuccess) return done(YR_ERR_CUDA);
     }
