@@ -340,6 +340,27 @@ typedef struct yr_render_stats {
 YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
                            yr_render_stats *stats, void *stream);
 
+/* yr_render for callers that cannot allocate GPU memory at render time -
+ * for example a host that runs inside a memory pool it does not own, or a
+ * plugin that may not call cudaMalloc while the application holds a
+ * capture or a custom allocator.  It renders the same image as yr_render
+ * but draws its scratch from one fixed 64 MiB block that every GPU loading
+ * this library holds until the process exits, instead of allocating.
+ * (No counterpart in the reference: YafRay renders on the CPU.)
+ *   - `rgba` is a device pointer (resx*resy*4 floats); nothing is staged.
+ *   - The render runs in as many passes as the block needs; a render whose
+ *     single pixel (all its samples) needs more than the block fails with
+ *     YR_ERR_TOO_LARGE.
+ *   - The first call on a device looks the block's address up (once per
+ *     device, with that device current); make that first call before any
+ *     stream capture.
+ *   - All calls share the block and it keeps the last call's contents:
+ *     calls that overlap on the GPU (different streams or threads) race and
+ *     must be serialized by the caller.
+ *   - No CUDA events are created: stats->ms and the kernel times stay 0;
+ *     the ray counts are filled in. */
+YR_API yr_status yr_render_noalloc(yr_scene *scene, float *rgba, yr_render_stats *stats, void *stream);
+
 /* Render `count` independent scenes in one persistent launch with per-scene
  * ray queues.  outs[i] are device pointers (RGBA float, scene i's size). */
 typedef struct yr_batch_params {

@@ -156,6 +156,7 @@ SIGNATURES = {
     "yr_trace_closest": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_int, _P]),
     "yr_trace_shadow": (C.c_int, [_P, _P, C.c_uint32, _P, _P]),
     "yr_render": (C.c_int, [_P, _P, C.c_int, C.POINTER(YrRenderStats), _P]),
+    "yr_render_noalloc": (C.c_int, [_P, _P, C.POINTER(YrRenderStats), _P]),
     "yr_render_batch": (C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(_P), C.POINTER(YrBatchParams),
                                   C.POINTER(YrRenderStats), _P]),
     "yr_param_count": (C.c_uint32, [_P]),

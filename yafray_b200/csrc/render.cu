@@ -17,6 +17,7 @@
 // per-vertex slots, so every sum is formed in the reference's order.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "dev_shade.cuh"
@@ -848,9 +849,56 @@ static yr_status run_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &
     return ret;
 }
 
+// ------------------------------------------------- allocation-free render
+// Scratch of yr_render_noalloc: one fixed block in the global memory of
+// every GPU that loads this library, held until the process exits.  In host
+// code the symbol only stands for the block; its device address comes from
+// cudaGetSymbolAddress, taken once per device with that device current.
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_addr[kMaxDevices];
+
+static yr_status noalloc_scratch(int device, void **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (device < 0 || device >= kMaxDevices) return YR_ERR_INVALID_ARG;
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return YR_ERR_CUDA;
+        g_noalloc_addr[device] = p;
+    }
+    *out = g_noalloc_addr[device];
+    return YR_OK;
+}
+
 }  // namespace yr
 
 using namespace yr;
+
+extern "C" YR_API yr_status yr_render_noalloc(yr_scene *scene, float *rgba, yr_render_stats *stats, void *stream) {
+    if (!scene || !rgba) return YR_ERR_INVALID_ARG;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(scene->device) != cudaSuccess) return YR_ERR_CUDA;
+    auto done = [&](yr_status e) {
+        cudaSetDevice(prev);
+        return e;
+    };
+    Plan P;
+    yr_status ret = make_plan(scene, P);
+    if (ret != YR_OK) return done(ret);
+    // waves as large as the block allows; one pixel's samples must fit
+    const uint32_t wcap = wave_for_budget(P, scene->rdr, kNoAllocScratchBytes);
+    if (wcap < scene->rdr.spp) return done(YR_ERR_TOO_LARGE);
+    void *block = nullptr;
+    if ((ret = noalloc_scratch(scene->device, &block)) != YR_OK) return done(ret);
+    Wave W;
+    std::memset(&W, 0, sizeof(W));
+    assign_wave(P, wcap, (char *)block, W);
+    return done(run_waves(scene, P, wcap, W, rgba, stats, (cudaStream_t)stream, false));
+}
 
 extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host, yr_render_stats *stats,
                                       void *stream) {
