@@ -189,13 +189,107 @@ def load_traffic():
     return {}
 
 
+def run_batch(args, api, torch, local, barrier):
+    """Uneven batch: `batch_count` independent scenes (1k-200k triangles,
+    1-32 objects, 64^2-512^2, 4-64 spp, 1-4 lights, GI 1-3 bounces) rendered
+    by one persistent launch (yr_render_batch, autotuned, CUDA graph), with
+    the plain one-scene-per-call path (yr_render per scene) timed beside it
+    on the same scenes; images of both paths are compared bit for bit."""
+    scs = scenes.config_batch(count=args.batch_count)
+    t0 = time.perf_counter()
+    dss = [api.DeviceScene(sc, device=local) for sc in scs]
+    setup_s = time.perf_counter() - t0
+    ntris = sum(int(d.info().ntriangles) for d in dss)
+    outs = [torch.empty((d.sc.resy, d.sc.resx, 4), dtype=torch.float32, device="cuda") for d in dss]
+    plain = [torch.empty_like(o) for o in outs]
+    ptrs = [o.data_ptr() for o in outs]
+    t0 = time.perf_counter()
+    st, prm = api.render_batch(dss, ptrs)   # first call autotunes and captures the graph
+    tune_s = time.perf_counter() - t0
+    for _ in range(max(0, args.warmup - 1)):
+        api.render_batch(dss, ptrs)
+        for d, o in zip(dss, plain):
+            d.render_into(o.data_ptr())
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rays = 0
+        for _ in range(args.steps):
+            rays += fn()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        return e0.elapsed_time(e1), rays
+
+    def batched():
+        s, _ = api.render_batch(dss, ptrs)
+        return s.rays_primary + s.rays_shadow + s.rays_bounce
+
+    def per_scene():
+        r = 0
+        for d, o in zip(dss, plain):
+            s = d.render_into(o.data_ptr())
+            r += s.rays_primary + s.rays_shadow + s.rays_bounce
+        return r
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_b, rays_b = timed(batched)
+    ms_p, rays_p = timed(per_scene)
+    clk = clocks.stop()
+    identical = all(bool(torch.equal(a, b)) for a, b in zip(outs, plain))
+    value = rays_b / (ms_b / 1000.0) / 1e6
+    plain_value = rays_p / (ms_p / 1000.0) / 1e6
+    # end to end: parameters host -> device and every image back to pinned host memory
+    host = [torch.empty(o.shape, dtype=torch.float32).pin_memory() for o in outs]
+    h2d = sum(len(d.sc.shaders) * C.sizeof(abi.YrShaderDesc) + len(d.sc.lights) * C.sizeof(abi.YrLightDesc)
+              for d in dss)
+    d2h = sum(h.numel() * 4 for h in host)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_rays = 0
+    for _ in range(args.steps):
+        for d in dss:
+            d.set_params(d.sc.shaders, d.sc.lights)
+        e2e_rays += batched()
+        for h, o in zip(host, outs):
+            h.copy_(o, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": f"batch: {len(dss)} scenes, {ntris:,} triangles, one persistent launch",
+                   "block_size": prm.block_size, "queue_tile": prm.queue_tile,
+                   "stack_entries": prm.stack_entries, "autotune_s": round(tune_s, 3),
+                   "scene_setup_s": round(setup_s, 3), "l2": "scene arrays and images larger than L2"},
+        "plain_gpu": {"value": plain_value, "unit": METRIC, "ms_per_step": ms_p / args.steps,
+                      "launch": "yr_render per scene"},
+        "speedup_vs_plain": value / plain_value if plain_value else None,
+        "identical_images": identical,
+        "e2e": {"value": e2e_rays / e2e_s / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    for d in dss:
+        d.close()
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "batch"])
+    ap.add_argument("--batch-count", type=int, default=256, help="scenes in the batch workload")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--resx", type=int, default=1920)
     ap.add_argument("--resy", type=int, default=1080)
@@ -225,6 +319,9 @@ def main():
         if world > 1:
             dist.barrier()
 
+    if args.config == "batch":
+        run_batch(args, api, torch, local, barrier)
+        return
     sc, name = workload(args)
     if args.exact_order:
         sc.render.flags |= 2

@@ -361,18 +361,26 @@ YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
  *     the ray counts are filled in. */
 YR_API yr_status yr_render_noalloc(yr_scene *scene, float *rgba, yr_render_stats *stats, void *stream);
 
-/* Render `count` independent scenes in one persistent launch with per-scene
- * ray queues.  outs[i] are device pointers (RGBA float, scene i's size). */
+/* Render `count` independent scenes (one device) in one persistent launch.
+ * Work items are tiles of whole pixels of one scene; blocks pull them from
+ * a shared counter and run the render stages over the tile with
+ * block-local ray queues.  Each image equals yr_render's for that scene.
+ * outs[i]: device RGBA float image of scene i (its resx*resy*4 floats).
+ * params (in/out, may be NULL = all automatic): block_size / queue_tile
+ * 0 = autotuned on a sample of the work the first time this list of scenes
+ * is rendered (then cached); use_graph = capture the launch in a CUDA graph
+ * and replay it on later calls.  On return the fields hold the
+ * configuration used (stack_entries: kd stack capacity).  Stats: ray
+ * counts and the device time of the launch. */
 typedef struct yr_batch_params {
-    int32_t block_size;      /* 0 = autotuned                                  */
-    int32_t queue_tile;      /* pixels per work item, 0 = autotuned            */
-    int32_t use_graph;       /* capture the launch in a CUDA graph             */
-    int32_t reserved;
+    int32_t block_size;      /* threads per block, 0 = autotuned              */
+    int32_t queue_tile;      /* camera samples per work item, 0 = autotuned   */
+    int32_t use_graph;       /* capture the launch in a CUDA graph            */
+    int32_t stack_entries;   /* out: kd stack capacity of the kernel used     */
 } yr_batch_params;
 
 YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t count, float *const *outs,
-                                 const yr_batch_params *params, yr_render_stats *stats,
-                                 void *stream);
+                                 yr_batch_params *params, yr_render_stats *stats, void *stream);
 
 /* ------------------------------------------------------------------------
  * Adjoint.  Gradient of  L = sum_pixels w * |img - target|^2  ... see

@@ -129,7 +129,7 @@ class YrRenderStats(C.Structure):
 
 class YrBatchParams(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("queue_tile", C.c_int32), ("use_graph", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("stack_entries", C.c_int32)]
 
 
 class YrBackwardDesc(C.Structure):

@@ -1,0 +1,486 @@
+// yr_render_batch: many independent scenes in one persistent launch.
+//
+// Work items are (scene, tile of whole pixels).  A fixed grid of blocks
+// (SMs x resident blocks) pulls items from one atomic counter; each block
+// runs the wavefront stages of dev_wave.cuh over its tile with block-local
+// ray queues (shadow queue, bounce queues and their counters live in the
+// block's scratch and shared memory), so scenes of very different sizes
+// share the GPU without one launch per scene and per wave.  The launch is
+// captured once in a CUDA graph and replayed.  Block size, tile size and the
+// kd stack capacity come from a small autotuner that times the candidates
+// on a sample of the items the first time a batch is seen.
+//
+// Every camera sample, light sample and sum is computed by the same stage
+// code as yr_render, so each image is identical to the per-scene render.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "dev_wave.cuh"
+
+namespace yr {
+
+struct BatchItem {
+    uint32_t scene;
+    uint32_t first_px;   // first pixel (region-local, row-major) of the tile
+    uint32_t npx;
+    uint32_t pad;
+};
+
+struct BatchArgs {
+    const DevScene *scenes;
+    const DevRender *renders;
+    const uint32_t *ns;       // shadow slots per vertex, per scene
+    const uint32_t *npath;    // path samples per camera sample, per scene
+    const BatchItem *items;
+    uint32_t nitems;
+    uint32_t *next;           // item counter
+    char *scratch;
+    size_t cta_bytes;
+    Plan pmax;                // layout maxima over the scenes
+    uint32_t qmax;            // camera samples per tile at most
+    float *const *outs;
+    unsigned long long *rays; // primary, shadow, bounce
+};
+
+template <int STACK>
+__global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
+    __shared__ DevScene S;
+    __shared__ DevRender R;
+    __shared__ Wave W;
+    __shared__ uint32_t cnt[8];
+    __shared__ uint32_t item;
+    uint2 stk_nt[STACK];
+    float stk_split[STACK];
+    const KdStack stk{stk_nt, stk_split, STACK};
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, nthr = blockDim.x;
+    if (tid == 0) {
+        W = Wave();
+        assign_wave(A.pmax, A.qmax, A.scratch + (size_t)blockIdx.x * A.cta_bytes, W);
+        W.counters = cnt;
+    }
+    uint32_t n_prim = 0, n_sh = 0, n_b = 0, nodes = 0, tests = 0;
+    __syncthreads();
+    for (;;) {
+        if (tid == 0) item = atomicAdd(A.next, 1u);
+        __syncthreads();
+        const uint32_t it = item;
+        if (it >= A.nitems) break;
+        if (tid == 0) {
+            const BatchItem bi = A.items[it];
+            S = A.scenes[bi.scene];
+            R = A.renders[bi.scene];
+            W.base = bi.first_px * R.spp;
+            W.count = bi.npx * R.spp;
+            W.ns = A.ns[bi.scene];
+            W.npath = A.npath[bi.scene];
+            W.out = A.outs[bi.scene];
+            for (int k = 0; k < 8; k++) cnt[k] = 0;
+        }
+        __syncthreads();
+        const uint32_t count = W.count;
+        for (uint32_t i = tid; i < count; i += nthr) {
+            st_primary(S, R, W, i, stk, nodes, tests);
+            n_prim++;
+        }
+        __syncthreads();
+        for (uint32_t b0 = tid - lane; b0 < count; b0 += nthr) st_shade_camera(S, R, W, b0 + lane);
+        __syncthreads();
+        {
+            const uint32_t n = cnt[0];
+            for (uint32_t q = tid; q < n; q += nthr) {
+                st_trace_shadow(S, W, q, R.self_bias, stk, nodes, tests);
+                n_sh++;
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < count; i += nthr) st_gather_camera(R, W, i);
+        __syncthreads();
+        if (W.npath > 0) {
+            const uint32_t nc = count * W.npath * (uint32_t)R.path_depth;
+            for (uint32_t q = tid; q < nc; q += nthr) W.p_contri[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+            __syncthreads();
+            for (int j = 0; j < R.path_depth; j++) {
+                const uint32_t nb = cnt[1];
+                for (uint32_t q = tid; q < nb; q += nthr) {
+                    st_trace_bounce(S, W, q, stk, nodes, tests);
+                    n_b++;
+                }
+                __syncthreads();
+                if (tid == 0) cnt[0] = 0;
+                __syncthreads();
+                for (uint32_t b0 = tid - lane; b0 < nb; b0 += nthr) st_shade_path(S, R, W, j, b0 + lane, nb);
+                __syncthreads();
+                {
+                    const uint32_t n = cnt[0];
+                    for (uint32_t q = tid; q < n; q += nthr) {
+                        st_trace_shadow(S, W, q, R.self_bias, stk, nodes, tests);
+                        n_sh++;
+                    }
+                }
+                __syncthreads();
+                for (uint32_t b0 = tid - lane; b0 < nb; b0 += nthr)
+                    st_gather_path(R, W, j, R.background, b0 + lane, nb);
+                __syncthreads();
+                if (tid == 0) {
+                    uint32_t *t = W.bq;
+                    W.bq = W.bq2;
+                    W.bq2 = t;
+                    cnt[1] = cnt[2];
+                    cnt[2] = 0;
+                }
+                __syncthreads();
+            }
+        }
+        const uint32_t npx = count / R.spp;
+        for (uint32_t px = tid; px < npx; px += nthr) st_finish(R, W, px);
+        __syncthreads();
+    }
+    const uint32_t a = __reduce_add_sync(0xffffffffu, n_prim), b = __reduce_add_sync(0xffffffffu, n_sh),
+                   c = __reduce_add_sync(0xffffffffu, n_b);
+    if (lane == 0) {
+        atomicAdd(&A.rays[0], (unsigned long long)a);
+        atomicAdd(&A.rays[1], (unsigned long long)b);
+        atomicAdd(&A.rays[2], (unsigned long long)c);
+    }
+}
+
+using BatchKernel = void (*)(BatchArgs);
+static const int kStackOptions[3] = {32, 48, kKdStackCap};
+static BatchKernel batch_kernel(int stack) {
+    if (stack == 32) return k_batch<32>;
+    if (stack == 48) return k_batch<48>;
+    return k_batch<kKdStackCap>;
+}
+
+struct BatchConfig {
+    int block = 0;
+    int tile = 0;    // camera samples per tile (cap)
+    int stack = 0;
+    bool operator==(const BatchConfig &o) const { return block == o.block && tile == o.tile && stack == o.stack; }
+};
+
+// Device state of one batch (a list of scenes and output images), kept
+// between calls so that repeated renders replay the captured graph.
+struct BatchCtx {
+    int device = -1;
+    std::vector<yr_scene *> scenes;
+    std::vector<float *> outs;
+    std::vector<Plan> plans;
+    std::vector<DevScene> h_scenes;     // the records uploaded, to spot changes
+    std::vector<DevRender> h_renders;
+    Plan pmax{};
+    int max_depth = 0;
+    DevScene *d_scenes = nullptr;
+    DevRender *d_renders = nullptr;
+    uint32_t *d_ns = nullptr, *d_npath = nullptr;
+    float **d_outs = nullptr;
+    BatchItem *d_items = nullptr;
+    size_t items_cap = 0;
+    uint32_t *d_next = nullptr;
+    unsigned long long *d_rays = nullptr;
+    char *d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    BatchConfig tuned{};
+    BatchConfig graph_cfg{};
+    uint32_t graph_items = 0;
+    char *graph_scratch = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<BatchItem> items;
+
+    ~BatchCtx() {
+        if (graph) cudaGraphExecDestroy(graph);
+        cudaFree(d_scenes);
+        cudaFree(d_renders);
+        cudaFree(d_ns);
+        cudaFree(d_npath);
+        cudaFree(d_outs);
+        cudaFree(d_items);
+        cudaFree(d_next);
+        cudaFree(d_rays);
+        cudaFree(d_scratch);
+    }
+};
+
+static std::mutex g_batch_mu;
+static std::map<std::vector<uintptr_t>, std::unique_ptr<BatchCtx>> g_batches;
+
+void batch_forget(const yr_scene *s) {
+    std::lock_guard<std::mutex> lock(g_batch_mu);
+    for (auto it = g_batches.begin(); it != g_batches.end();) {
+        if (std::find(it->second->scenes.begin(), it->second->scenes.end(), s) != it->second->scenes.end()) {
+            int prev = 0;
+            cudaGetDevice(&prev);
+            cudaSetDevice(it->second->device);
+            it = g_batches.erase(it);
+            cudaSetDevice(prev);
+        } else {
+            ++it;
+        }
+    }
+}
+
+// Items for a tile cap: per scene, tiles of max(1, cap/spp) whole pixels;
+// scenes with the most work per pixel first, so the long items start early.
+static void make_items(const BatchCtx &C, int tile, std::vector<BatchItem> &items) {
+    items.clear();
+    std::vector<uint32_t> order(C.scenes.size());
+    std::iota(order.begin(), order.end(), 0u);
+    auto cost = [&](uint32_t s) {
+        const Plan &P = C.plans[s];
+        const DevRender &R = C.scenes[s]->rdr;
+        return (double)R.spp * (1.0 + P.ns) * (1.0 + P.npath * (double)P.depth * (1.0 + P.ns));
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost(a) > cost(b); });
+    for (uint32_t s : order) {
+        const DevRender &R = C.scenes[s]->rdr;
+        const uint32_t tpx = std::max<uint32_t>(1u, (uint32_t)tile / R.spp);
+        const uint32_t rpix = C.plans[s].rpix;
+        for (uint32_t p0 = 0; p0 < rpix; p0 += tpx) items.push_back({s, p0, std::min(tpx, rpix - p0), 0u});
+    }
+}
+
+static uint32_t tile_cap(const BatchCtx &C, int tile) {
+    uint32_t q = 0;
+    for (yr_scene *sc : C.scenes) {
+        const uint32_t spp = sc->rdr.spp;
+        q = std::max(q, std::max<uint32_t>(1u, (uint32_t)tile / spp) * spp);
+    }
+    return q;
+}
+
+static yr_status ensure(void **p, size_t &have, size_t need) {
+    if (have >= need && *p) return YR_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    have = 0;
+    if (cudaMalloc(p, need) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
+    have = need;
+    return YR_OK;
+}
+
+// Upload items, size the scratch, launch (or replay the graph) on `st`.
+static yr_status launch_batch(BatchCtx &C, const BatchConfig &cfg, const std::vector<BatchItem> &items,
+                              cudaStream_t st, bool use_graph, float *ms_out) {
+    const uint32_t qmax = tile_cap(C, cfg.tile);
+    const size_t cta = (wave_bytes(C.pmax, qmax) + 255) / 256 * 256;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, C.device);
+    BatchKernel kern = batch_kernel(cfg.stack);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.block, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int grid = std::max(1, std::min<int>(sms * per_sm, (int)items.size()));
+    yr_status ret;
+    if ((ret = ensure((void **)&C.d_scratch, C.scratch_bytes, cta * (size_t)sms * per_sm)) != YR_OK) return ret;
+    if (items.size() > C.items_cap) {
+        cudaFree(C.d_items);
+        C.d_items = nullptr;
+        if (cudaMalloc(&C.d_items, sizeof(BatchItem) * items.size()) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
+        C.items_cap = items.size();
+        if (C.graph) {
+            cudaGraphExecDestroy(C.graph);
+            C.graph = nullptr;
+        }
+    }
+    if (cudaMemcpyAsync(C.d_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+        return YR_ERR_CUDA;
+    BatchArgs A;
+    A.scenes = C.d_scenes;
+    A.renders = C.d_renders;
+    A.ns = C.d_ns;
+    A.npath = C.d_npath;
+    A.items = C.d_items;
+    A.nitems = (uint32_t)items.size();
+    A.next = C.d_next;
+    A.scratch = C.d_scratch;
+    A.cta_bytes = cta;
+    A.pmax = C.pmax;
+    A.qmax = qmax;
+    A.outs = C.d_outs;
+    A.rays = C.d_rays;
+    auto record = [&](cudaStream_t s) {
+        cudaMemsetAsync(C.d_next, 0, sizeof(uint32_t), s);
+        cudaMemsetAsync(C.d_rays, 0, sizeof(unsigned long long) * 4, s);
+        kern<<<grid, cfg.block, 0, s>>>(A);
+    };
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    if (use_graph) {
+        if (!C.graph || !(C.graph_cfg == cfg) || C.graph_items != A.nitems || C.graph_scratch != C.d_scratch) {
+            if (C.graph) cudaGraphExecDestroy(C.graph);
+            C.graph = nullptr;
+            cudaStream_t cs;
+            cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+            cudaGraph_t g;
+            if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return YR_ERR_CUDA;
+            record(cs);
+            if (cudaStreamEndCapture(cs, &g) != cudaSuccess) return YR_ERR_CUDA;
+            const cudaError_t ie = cudaGraphInstantiate(&C.graph, g, 0);
+            cudaGraphDestroy(g);
+            cudaStreamDestroy(cs);
+            if (ie != cudaSuccess) return YR_ERR_CUDA;
+            C.graph_cfg = cfg;
+            C.graph_items = A.nitems;
+            C.graph_scratch = C.d_scratch;
+        }
+        if (cudaGraphLaunch(C.graph, st) != cudaSuccess) return YR_ERR_CUDA;
+    } else {
+        record(st);
+    }
+    cudaEventRecord(e1, st);
+    if (cudaGetLastError() != cudaSuccess) return YR_ERR_CUDA;
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms_out) *ms_out = ms;
+    return YR_OK;
+}
+
+// Time every candidate on every 8th item and keep the fastest.
+static yr_status autotune(BatchCtx &C, cudaStream_t st, BatchConfig &best) {
+    float best_ms = 3.4e38f;
+    const int blocks[2] = {128, 256}, tiles[3] = {256, 512, 1024};
+    for (int stack : kStackOptions) {
+        if (C.max_depth + 2 > stack) continue;
+        for (int tile : tiles)
+            for (int block : blocks) {
+                BatchConfig cfg{block, tile, stack};
+                std::vector<BatchItem> all, sample;
+                make_items(C, tile, all);
+                for (size_t i = 0; i < all.size(); i += 8) sample.push_back(all[i]);
+                float ms = 0.f;
+                yr_status r = launch_batch(C, cfg, sample, st, false, &ms);
+                if (r != YR_OK) return r;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = cfg;
+                }
+            }
+    }
+    return best.block ? YR_OK : YR_ERR_UNSUPPORTED;
+}
+
+}  // namespace yr
+
+using namespace yr;
+
+extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t count, float *const *outs,
+                                            yr_batch_params *params, yr_render_stats *stats, void *stream) {
+    if (!scenes || !outs || count == 0) return YR_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < count; i++)
+        if (!scenes[i] || !outs[i] || scenes[i]->device != scenes[0]->device) return YR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g_batch_mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    const int device = scenes[0]->device;
+    cudaSetDevice(device);
+    auto done = [&](yr_status e) {
+        cudaSetDevice(prev);
+        return e;
+    };
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<uintptr_t> key;
+    key.push_back((uintptr_t)device);
+    for (uint32_t i = 0; i < count; i++) key.push_back((uintptr_t)scenes[i]);
+    std::unique_ptr<BatchCtx> &slot = g_batches[key];
+    yr_status ret;
+    if (slot) {  // a scene whose parameters changed since the last call: start over
+        for (uint32_t i = 0; i < count && slot; i++)
+            if (std::memcmp(&slot->h_scenes[i], &scenes[i]->dev, sizeof(DevScene)) ||
+                std::memcmp(&slot->h_renders[i], &scenes[i]->rdr, sizeof(DevRender)))
+                slot.reset();
+    }
+    if (!slot) {
+        std::unique_ptr<BatchCtx> C(new BatchCtx);
+        C->device = device;
+        C->scenes.assign(scenes, scenes + count);
+        C->plans.resize(count);
+        std::vector<DevScene> ds(count);
+        std::vector<DevRender> dr(count);
+        std::vector<uint32_t> ns(count), np(count);
+        C->pmax = Plan{};
+        for (uint32_t i = 0; i < count; i++) {
+            if ((ret = make_plan(scenes[i], C->plans[i])) != YR_OK) return done(ret);
+            if (scenes[i]->rdr.raydepth <= 0) return done(YR_ERR_UNSUPPORTED);
+            const Plan &P = C->plans[i];
+            C->pmax.ns = std::max(C->pmax.ns, P.ns);
+            C->pmax.npath = std::max(C->pmax.npath, P.npath);
+            C->pmax.nl = std::max(C->pmax.nl, P.nl);
+            C->pmax.depth = std::max(C->pmax.depth, P.depth);
+            C->max_depth = std::max(C->max_depth, scenes[i]->max_tree_depth);
+            std::memcpy(&ds[i], &scenes[i]->dev, sizeof(DevScene));
+            std::memcpy(&dr[i], &scenes[i]->rdr, sizeof(DevRender));
+            ns[i] = P.ns;
+            np[i] = P.npath;
+        }
+        if (cudaMalloc(&C->d_scenes, sizeof(DevScene) * count) != cudaSuccess ||
+            cudaMalloc(&C->d_renders, sizeof(DevRender) * count) != cudaSuccess ||
+            cudaMalloc(&C->d_ns, 4 * count) != cudaSuccess || cudaMalloc(&C->d_npath, 4 * count) != cudaSuccess ||
+            cudaMalloc(&C->d_outs, sizeof(float *) * count) != cudaSuccess ||
+            cudaMalloc(&C->d_next, sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc(&C->d_rays, sizeof(unsigned long long) * 4) != cudaSuccess)
+            return done(YR_ERR_OUT_OF_MEMORY);
+        cudaMemcpy(C->d_scenes, ds.data(), sizeof(DevScene) * count, cudaMemcpyHostToDevice);
+        cudaMemcpy(C->d_renders, dr.data(), sizeof(DevRender) * count, cudaMemcpyHostToDevice);
+        cudaMemcpy(C->d_ns, ns.data(), 4 * count, cudaMemcpyHostToDevice);
+        cudaMemcpy(C->d_npath, np.data(), 4 * count, cudaMemcpyHostToDevice);
+        C->h_scenes = std::move(ds);
+        C->h_renders = std::move(dr);
+        slot = std::move(C);
+    }
+    BatchCtx &C = *slot;
+    // output images may move between calls
+    if (C.outs.size() != count || !std::equal(C.outs.begin(), C.outs.end(), outs)) {
+        C.outs.assign(outs, outs + count);
+        cudaMemcpy(C.d_outs, C.outs.data(), sizeof(float *) * count, cudaMemcpyHostToDevice);
+    }
+    BatchConfig cfg;
+    const bool autotuned = !params || params->block_size == 0 || params->queue_tile == 0;
+    if (autotuned) {
+        if (!C.tuned.block && (ret = autotune(C, st, C.tuned)) != YR_OK) return done(ret);
+        cfg = C.tuned;
+    } else {
+        cfg.block = params->block_size;
+        cfg.tile = params->queue_tile;
+        if (cfg.block % 32 || cfg.block < 32 || cfg.block > 1024 || cfg.tile < 1) return done(YR_ERR_INVALID_ARG);
+        cfg.stack = kKdStackCap;
+        for (int s : kStackOptions)
+            if (C.max_depth + 2 <= s) {
+                cfg.stack = s;
+                break;
+            }
+    }
+    make_items(C, cfg.tile, C.items);
+    float ms = 0.f;
+    const bool use_graph = !params || params->use_graph;
+    if ((ret = launch_batch(C, cfg, C.items, st, use_graph, &ms)) != YR_OK) return done(ret);
+    // device status words of every scene
+    for (yr_scene *sc : C.scenes)
+        if ((ret = take_status(sc, st)) != YR_OK) return done(ret);
+    if (stats) {
+        unsigned long long r[4] = {0, 0, 0, 0};
+        cudaMemcpy(r, C.d_rays, sizeof(r), cudaMemcpyDeviceToHost);
+        std::memset(stats, 0, sizeof(*stats));
+        stats->rays_primary = r[0];
+        stats->rays_shadow = r[1];
+        stats->rays_bounce = r[2];
+        stats->ms = ms;
+        stats->kernel_ms[YR_K_OTHER] = ms;
+        stats->kernel_launches[YR_K_OTHER] = 1;
+    }
+    if (params) {  // report the configuration used
+        params->block_size = cfg.block;
+        params->queue_tile = cfg.tile;
+        params->stack_entries = cfg.stack;
+    }
+    return done(YR_OK);
+}

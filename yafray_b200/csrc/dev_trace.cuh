@@ -177,6 +177,7 @@ constexpr int kKdStackCap = 66;
 struct KdStack {
     uint2 *nt;     // far node | axis << 30, bits of t
     float *split;
+    int cap;       // entries (depth of the deepest tree + 2 must fit)
 };
 
 __device__ __forceinline__ void exit_point(uint32_t node_axis, float t, float split, const float *fr,
@@ -272,7 +273,7 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
                 curr = right;
             }
             const float t = (split - fr[axis]) * inv[axis];
-            if (sp >= kKdStackCap) {
+            if (sp >= stk.cap) {
                 dev_fail(S.status, kDevStackOverflow);
                 return false;
             }
@@ -480,7 +481,7 @@ __device__ inline bool scene_occluded_merged(const DevScene &S, const V3 &p, int
                 curr = right;
             }
             const float t = (split - fr[axis]) * inv[axis];
-            if (sp >= kKdStackCap) {
+            if (sp >= stk.cap) {
                 bad = true;
                 break;
             }
@@ -495,7 +496,7 @@ __device__ inline bool scene_occluded_merged(const DevScene &S, const V3 &p, int
             nd = __ldg(S.sh_nodes + curr);
         }
         if (bad) {
-            dev_fail(S.status, sp >= kKdStackCap ? kDevStackOverflow : kDevBadTree);
+            dev_fail(S.status, sp >= stk.cap ? kDevStackOverflow : kDevBadTree);
             break;
         }
         nodes++;

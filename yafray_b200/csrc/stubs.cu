@@ -3,10 +3,6 @@
 #include "scene.h"
 
 extern "C" {
-YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t count, float *const *outs,
-                                 const yr_batch_params *params, yr_render_stats *stats, void *stream) {
-    return YR_ERR_UNSUPPORTED;
-}
 YR_API uint32_t yr_param_count(const yr_scene *scene) { return 0; }
 YR_API yr_status yr_params_get(const yr_scene *scene, float *params) { return YR_ERR_UNSUPPORTED; }
 YR_API yr_status yr_params_set(yr_scene *scene, const float *params) { return YR_ERR_UNSUPPORTED; }

@@ -10,7 +10,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(DevScene S, const
                                                                 yr_hit *__restrict__ hits, int shadow_only) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
-    const KdStack stk{stk_nt, stk_split};
+    const KdStack stk{stk_nt, stk_split, kKdStackCap};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 *rp = reinterpret_cast<const float4 *>(rays + i);
         const float4 q0 = __ldg(rp), q1 = __ldg(rp + 1);
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(DevScene S, const 
                                                                uint32_t n, uint8_t *__restrict__ occ, float self_bias) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
-    const KdStack stk{stk_nt, stk_split};
+    const KdStack stk{stk_nt, stk_split, kKdStackCap};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 *rp = reinterpret_cast<const float4 *>(rays + i);
         const float4 q0 = __ldg(rp), q1 = __ldg(rp + 1);
