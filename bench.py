@@ -394,8 +394,8 @@ def main():
     e2e_value = float(e2e_r.item()) / float(e2e_t.item()) / 1e6
 
     # roofline of the dominant kernel class: algorithmic bytes per ray =
-    # 32 (ray) + 16 (hit / occlusion record) + 8 per kd or object-tree node
-    # + 52 per triangle test (48-byte triangle + 4-byte leaf index)
+    # 32 (ray) + 16 (hit / occlusion record) + 16 per node visited (the
+    # reference's kdTreeNode) + 48 per triangle tested (triangle_t a,b,c,N)
     kms = agg["kms"]
     dom = int(np.argmax(kms))
     peaks = {}
@@ -404,7 +404,7 @@ def main():
         peaks = json.load(open(pk_path))
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    alg_bytes = 48.0 * agg["krays"][dom] + 8.0 * agg["knodes"][dom] + 52.0 * agg["ktests"][dom]
+    alg_bytes = 48.0 * agg["krays"][dom] + 16.0 * agg["knodes"][dom] + 48.0 * agg["ktests"][dom]
     achieved = alg_bytes / (kms[dom] / 1000.0) / 1e9 if kms[dom] > 0 else 0.0
     traffic = load_traffic().get(abi.KERNEL_CLASSES[dom])
     launches = max(1.0, agg["launch"][dom])

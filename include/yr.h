@@ -336,7 +336,18 @@ typedef struct yr_render_stats {
  * top (colorOutput_t::putPixel(x, y) order).  `rgba` is a device pointer
  * unless `rgba_on_host` != 0, in which case the library stages it.
  * QMC: path, hemi and area-light samples use explicit Halton indices with a
- * per-pixel Cranley-Patterson rotation (documented in DESIGN.md). */
+ * per-pixel Cranley-Patterson rotation instead of the reference's
+ * sequential generator state.  halton(b, n) is the value that
+ * Halton::setStart(n) followed by getNext() returns (mcqmc.h:24-49);
+ * rot(pixel, dim) in [0,1) is a 32-bit hash of (seed, pixel, dim); a
+ * rotated value is u = halton + rot, minus 1 when u >= 1.  For camera
+ * sample s of a pixel, path sample i of P per camera sample:
+ *   bounce level l direction: bases (prime[2l], prime[2l+1]), index s*P+i,
+ *     dims (2l, 2l+1) (pathtools.cc:9-43);
+ *   area / hemi light k at path vertex v (0 = camera hit), sample j of J:
+ *     bases (2, 3), index m*J+j with m = s at the camera hit and s*P+i on
+ *     a path, dims 64+16k+2v (+1); area jitter = u - 0.5 along the cell
+ *     axes (arealight.cc:136-153). */
 YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
                            yr_render_stats *stats, void *stream);
 

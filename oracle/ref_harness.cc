@@ -1,5 +1,5 @@
 // Test harness around the UNMODIFIED YafRay 0.0.9 reference (linked from
-// objects built from /root/reference by oracle/Makefile).  Test
+// objects built from the reference sources by oracle/Makefile).  Test
 // infrastructure only: it generates golden vectors for tests/golden/ and is
 // the reference arm of bench.py; the product never links or runs it.
 //
