@@ -1,0 +1,131 @@
+"""yr_backward against central finite differences of the loss.
+
+L(theta) = sum over pixels and RGB of (render(theta) - target)^2, accumulated
+in FP64 from the FP32 images; FD step 1e-3 (the step actually taken in
+float32 is the denominator).  Tolerance: 1e-3 relative, plus an absolute
+floor of 1e-3 of the largest gradient for parameters whose gradient is
+near zero.  Scenes with a path light or a hemi light have energy cut-offs
+(paths stop below 0.05) that the adjoint treats as fixed; a parameter step
+can flip one of them for a few samples, so those scenes use 1e-2."""
+import numpy as np
+import pytest
+
+from yafray_b200 import api, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _loss(img, target):
+    d = img[..., :3].astype(np.float64) - target[..., :3].astype(np.float64)
+    return float((d * d).sum())
+
+
+def _render(torch, ds):
+    t = torch.zeros((ds.sc.resy, ds.sc.resx, 4), dtype=torch.float32, device="cuda")
+    ds.render_into(t.data_ptr())
+    torch.cuda.synchronize()
+    return t
+
+
+def _check(torch, sc, hidden_params_fn, nsample=16, rtol=1e-3, seed=0):
+    ds = api.DeviceScene(sc)
+    theta = ds.params_get().astype(np.float32)
+    n = theta.size
+    ds.params_set(hidden_params_fn(theta))
+    target = _render(torch, ds)
+    ds.params_set(theta)
+    img = _render(torch, ds)
+    grad = torch.zeros(n, dtype=torch.float32, device="cuda")
+    loss = ds.backward(img.data_ptr(), target.data_ptr(), grad.data_ptr(), 1.0)
+    g = grad.cpu().numpy().astype(np.float64)
+    tgt = target.cpu().numpy()
+    assert loss == pytest.approx(_loss(img.cpu().numpy(), tgt), rel=1e-5)
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(n, size=min(nsample, n), replace=False)
+    fd = np.zeros(idx.size)
+    for q, k in enumerate(idx):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] = np.float32(theta[k] + 1e-3)
+        tm[k] = np.float32(theta[k] - 1e-3)
+        ds.params_set(tp)
+        lp = _loss(_render(torch, ds).cpu().numpy(), tgt)
+        ds.params_set(tm)
+        lm = _loss(_render(torch, ds).cpu().numpy(), tgt)
+        fd[q] = (lp - lm) / (float(tp[k]) - float(tm[k]))
+    ds.params_set(theta)
+    floor = 1e-3 * np.abs(fd).max()
+    err = np.abs(g[idx] - fd)
+    bad = err > rtol * np.abs(fd) + floor
+    assert not bad.any(), (f"params {idx[bad]}: adjoint {g[idx][bad]} vs FD {fd[bad]} "
+                           f"(rel {(err / np.maximum(np.abs(fd), 1e-30))[bad]})")
+    return ds, g, fd
+
+
+def _hidden(seed):
+    def f(theta):
+        rng = np.random.default_rng(seed)
+        return (theta * rng.uniform(0.7, 1.3, theta.size)).astype(np.float32)
+    return f
+
+
+def test_param_layout_and_roundtrip(cuda):
+    sc = scenes.config_diff(res=32, spp=1, groups=64, nlights=8)
+    ds = api.DeviceScene(sc)
+    assert ds.param_count() == 64 * 4 + 8
+    p = ds.params_get()
+    assert np.allclose(p[0:3], sc.shaders[0].color[:])
+    assert p[3] == pytest.approx(max(sc.shaders[0].specular[:]))
+    assert p[-1] == pytest.approx(sc.lights[-1].power)
+    q = (p * 1.1).astype(np.float32)
+    ds.params_set(q)
+    assert np.allclose(ds.params_get(), q, rtol=1e-6)
+
+
+def test_grad_materials_and_area_lights(cuda):
+    """Config-4 shape at reduced size: 16 material groups (diffuse RGB +
+    specular weight) and 4 area lights."""
+    import torch
+    sc = scenes.config_diff(res=64, spp=4, groups=16, nlights=4)
+    _check(torch, sc, _hidden(1))
+
+
+def test_grad_point_light_and_specular(cuda):
+    import torch
+    sc = scenes.config_small(48, 36)
+    sc.shaders[0].specular[:] = [0.3, 0.3, 0.3]
+    sc.shaders[0].hard = 10.0
+    sc.lights.append(scenes.point_light((-3.0, 4.0, 3.0), 0.7, color=(1.0, 0.8, 0.6)))
+    sc.render.spp = 2
+    _check(torch, sc, _hidden(2), nsample=7)
+
+
+def test_grad_path_light_and_fbm_texture(cuda):
+    """Path GI (2 bounces) with an fBm-modulated albedo: amplitude and base
+    colour of the texture, the path light's power."""
+    import torch
+    sc = scenes.config_small(48, 36)
+    sc.shaders = [scenes.fbm_shader((0.6, 0.5, 0.4), (0.7, 0.3, 0.2), (1.0, 1.0, 1.0), 0.6, 3.0, mod_color=0.7),
+                  scenes.shader((0.8, 0.8, 0.8), (0.2, 0.2, 0.2), hard=8.0)]
+    sc.meshes[1].shader = 1
+    sc.lights = [scenes.quad_light_down(1.0, 5.0, 1.0, 2.0, 2.0, 30.0, 4),
+                 scenes.path_light(samples=2, depth=2, power=1.0)]
+    sc.render.spp = 4
+    ds, g, fd = _check(torch, sc, _hidden(3), nsample=14, rtol=1e-2)
+    assert ds.param_count() == 8 + 4 + 2
+
+
+def test_grad_hemi_light(cuda):
+    import torch
+    sc = scenes.config_small(40, 30)
+    sc.lights = [scenes.hemi_light(samples=8, power=0.8)]
+    sc.render.spp = 2
+    _check(torch, sc, _hidden(4), nsample=5, rtol=1e-2)
+
+
+def test_backward_rejects_bad_args(cuda):
+    import torch
+    from yafray_b200 import abi
+    ds = api.DeviceScene(scenes.config_small(16, 12))
+    img = _render(torch, ds)
+    with pytest.raises(abi.YrError):
+        ds.backward(img.data_ptr(), 0, 0)

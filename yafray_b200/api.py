@@ -85,6 +85,35 @@ class DeviceScene:
         self.last_stats = self.render_into(img.ctypes.data, on_host=True)
         return img
 
+    # ------------------------------------------------------------- adjoint
+    def param_count(self) -> int:
+        return int(self.lib.yr_param_count(self.handle))
+
+    def params_get(self) -> np.ndarray:
+        out = np.zeros(max(1, self.param_count()), np.float32)
+        abi.check(self.lib.yr_params_get(self.handle, out.ctypes.data_as(C.POINTER(C.c_float))), "yr_params_get")
+        return out[:self.param_count()]
+
+    def params_set(self, params) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.shape == (self.param_count(),)
+        abi.check(self.lib.yr_params_set(self.handle, p.ctypes.data_as(C.POINTER(C.c_float))), "yr_params_set")
+
+    def backward(self, image_ptr: int, target_ptr: int, dparams_ptr: int, loss_scale: float = 1.0,
+                 stream: int = 0) -> float:
+        """Gradient of loss_scale * sum over pixels and RGB of (image - target)^2
+        with respect to the parameter vector, written to dparams_ptr (device,
+        param_count floats).  image: this scene's forward render (device RGBA).
+        Returns the loss."""
+        d = abi.YrBackwardDesc()
+        d.target = target_ptr
+        d.image = image_ptr
+        d.loss_scale = float(loss_scale)
+        loss = C.c_float(0.0)
+        abi.check(self.lib.yr_backward(self.handle, C.byref(d), C.c_void_p(dparams_ptr), C.byref(loss),
+                                       C.c_void_p(stream)), "yr_backward")
+        return float(loss.value)
+
     def set_params(self, shaders=None, lights=None):
         sh = (abi.YrShaderDesc * len(shaders))(*shaders) if shaders is not None else None
         li = (abi.YrLightDesc * len(lights))(*lights) if lights is not None else None

@@ -1,0 +1,490 @@
+// yr_backward: gradient of an image loss with respect to the shaders'
+// colours, specular weights and texture parameters and the lights' powers.
+//
+// Geometry is fixed, so every ray, hit and shadow answer of the forward
+// render is a constant of the parameters; the pixel value is then a
+// polynomial in them.  For one camera sample with diffuse colour C0 and
+// specular colour S0 at its hit:
+//   c = sum_k pow_k (C0 . D_k + S0 . Sp_k)                  direct light k
+//     + pow_path / P * C0 . sum_paths sum_j cosN * (prod_{i<j} C_i) . G_j
+// where D_k / Sp_k are the diffuse / specular factors of light k per unit
+// power (fromLight split, basicshaders.cc:46-70), C_i the diffuse colour at
+// bounce vertex i and G_j the direct light at vertex j (or the background
+// on a miss), as pathLight_t::takeSample accumulates them
+// (pathlight.cc:303-347).  The adjoint re-runs the wavefront of yr_render
+// with the same QMC indices (the recompute stands in for stored paths),
+// keeps each light sample's D / Sp factors instead of its colour, and
+// accumulates dL/dparam: direct-light terms at the gather of each vertex,
+// the path products backwards (Horner) per camera sample at the end of the
+// wave.  Texture chain: C = mix(color1 + f (color2 - color1), C_base, w)
+// with f = intensity * fBm (basictex.cc:656-709, color.cc:103-109).
+//
+// The energy cut-offs of the forward (paths stop below 0.05; hemi lights
+// skip weak points) are treated as fixed decisions.  Gradients are
+// accumulated in FP32 per block in shared memory, then added to the global
+// vector with one atomic per parameter per block.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#define YR_WAVE_KERNELS 1
+#include "dev_wave.cuh"
+
+namespace yr {
+
+constexpr uint32_t kSmemParams = 8192;  // gradients kept in shared memory up to this many parameters
+
+struct GradAcc {
+    float *acc;  // shared-memory copy, or the global vector
+    __device__ __forceinline__ void add(int i, float v) const {
+        if (v != 0.f) atomicAdd(acc + i, v);
+    }
+};
+
+__device__ __forceinline__ GradAcc grad_begin(const AdjWave &A, float *smem) {
+    const bool use = A.nparams <= kSmemParams;
+    if (use)
+        for (uint32_t i = threadIdx.x; i < A.nparams; i += blockDim.x) smem[i] = 0.f;
+    __syncthreads();
+    return GradAcc{use ? smem : A.grad};
+}
+
+__device__ __forceinline__ void grad_end(const AdjWave &A, const GradAcc &g) {
+    __syncthreads();
+    if (g.acc != A.grad)
+        for (uint32_t i = threadIdx.x; i < A.nparams; i += blockDim.x) {
+            const float v = g.acc[i];
+            if (v != 0.f) atomicAdd(A.grad + i, v);
+        }
+}
+
+__device__ __forceinline__ float dot3(const C3 &a, const C3 &b) { return a.r * b.r + a.g * b.g + a.b * b.b; }
+
+// dL/dC and dL/dS at a vertex of shader `sid` -> the shader's parameters
+__device__ __forceinline__ void chain_shader(const DevRender &R, const AdjWave &A, const GradAcc &acc, int sid,
+                                             float m, const C3 &dC, const C3 &dS) {
+    const DevShader &sh = R.shaders[sid];
+    const int b = A.sh_pbase[sid];
+    C3 dCb = dC;
+    if (sh.tex_type != YR_TEX_NONE && sh.mod_color > 0.f) {
+        const float w = sh.mod_color;
+        const C3 dtex = w > 1.f ? dC : dC * w;
+        dCb = w > 1.f ? c3(0.f, 0.f, 0.f) : dC * (1.f - w);
+        const float f = sh.tex_type == YR_TEX_MUSGRAVE_FBM ? sh.intensity * m : m;
+        const C3 dtc1 = dtex * (1.f - f);
+        if (sh.tex_type == YR_TEX_MUSGRAVE_FBM) acc.add(b + 4, m * dot3(dtex, sh.tc2 - sh.tc1));
+        acc.add(b + 5, dtc1.r);
+        acc.add(b + 6, dtc1.g);
+        acc.add(b + 7, dtc1.b);
+    }
+    acc.add(b + 0, dCb.r);
+    acc.add(b + 1, dCb.g);
+    acc.add(b + 2, dCb.b);
+    const float4 sd = A.spec_dir[sid];
+    acc.add(b + 3, dS.r * sd.x + dS.g * sd.y + dS.b * sd.z);
+}
+
+// Direct light at one vertex from its slots (adjoint form of gather_term):
+// accumulates the light-power and shader gradients for adjoint weight Wv
+// and returns the direct light sum G.
+__device__ __forceinline__ C3 adj_vertex_direct(const DevRender &R, const Wave &W, const AdjWave &A,
+                                                const GradAcc &acc, uint32_t vtx, const float4 *aux, const C3 &lkc,
+                                                int sid, float m, const C3 &Wv) {
+    const C3 spec = R.shaders[sid].specular;
+    C3 Dt = c3(0.f, 0.f, 0.f), St = c3(0.f, 0.f, 0.f);
+    uint32_t off = 0;
+    for (int k = 0; k < R.nlights; k++) {
+        const DevLight L = R.lights[k];
+        C3 Dk = c3(0.f, 0.f, 0.f), Sk = c3(0.f, 0.f, 0.f);
+        if (L.type == YR_LIGHT_POINT) {
+            const uint32_t slot = vtx * W.ns + off;
+            if (W.slot_f[slot] == kSlotLit) {
+                const float4 d = W.slot_c[slot], e = A.slot_s[slot];
+                Dk = c3(d.x, d.y, d.z);
+                Sk = c3(e.x, e.y, e.z);
+            }
+        } else if (L.type == YR_LIGHT_AREA) {
+            const float4 a = aux[vtx * R.nlights + k];
+            if (a.y != 0.f) {
+                for (int jj = 0; jj < L.samples; jj++) {
+                    const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+                    if (W.slot_f[slot] == kSlotLit) {
+                        const float4 d = W.slot_c[slot], e = A.slot_s[slot];
+                        Dk = Dk + c3(d.x, d.y, d.z);
+                        Sk = Sk + c3(e.x, e.y, e.z);
+                    }
+                }
+                const float f = a.x / (float)L.samples;
+                Dk = Dk * f;
+                Sk = Sk * f;
+            }
+        } else if (L.type == YR_LIGHT_HEMI) {
+            const float4 a = aux[vtx * R.nlights + k];
+            if (a.w != 0.f) {
+                C3 total = c3(0.f, 0.f, 0.f);
+                for (int jj = 0; jj < L.samples; jj++) {
+                    const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+                    if (W.slot_f[slot] == kSlotLit) {
+                        const float4 d = W.slot_c[slot];
+                        total = total + c3(d.x, d.y, d.z);
+                    }
+                }
+                Dk = total * (a.x / (float)L.samples);
+                Sk = total * (a.y / (float)L.samples);
+            }
+        }
+        if (L.type != YR_LIGHT_PATH) {
+            acc.add(A.li_pidx[k], dot3(Wv, lkc * Dk + spec * Sk));
+            Dt = Dt + L.power * Dk;
+            St = St + L.power * Sk;
+        }
+        off += light_slots(L);
+    }
+    chain_shader(R, A, acc, sid, m, Wv * Dt, Wv * St);
+    return lkc * Dt + spec * St;
+}
+
+__device__ __forceinline__ C3 sample_weight(const DevRender &R, const AdjWave &A, uint32_t cs) {
+    int x, y;
+    const uint32_t pixel = cs_pixel(R, cs, x, y);
+    const float4 g = A.gpix[pixel];
+    const float inv = 1.f / (float)R.spp;  // the pixel is the mean of its spp samples
+    return c3(g.x * inv, g.y * inv, g.z * inv);
+}
+
+// --------------------------------------------------------------- kernels
+// dL/dpixel = 2 * scale * (img - target) over RGB; loss in double
+__global__ void __launch_bounds__(kBlock) k_adj_loss(const float4 *img, const float4 *target, uint32_t npix,
+                                                      float scale, float4 *gpix, double *loss) {
+    double part = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        const float4 a = img[i], b = target[i];
+        const float r = a.x - b.x, g = a.y - b.y, bl = a.z - b.z;
+        part += (double)scale * ((double)r * r + (double)g * g + (double)bl * bl);
+        gpix[i] = make_float4(2.f * scale * r, 2.f * scale * g, 2.f * scale * bl, 0.f);
+    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0 && part != 0.0) atomicAdd(loss, part);
+}
+
+__global__ void __launch_bounds__(kBlock) k_adj_shade_camera(DevScene S, DevRender R, Wave W, AdjWave A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W.count && (i & ~31u) >= W.count) return;  // whole warps past the end leave
+    st_shade_camera<true>(S, R, W, i, &A);
+}
+
+__global__ void __launch_bounds__(kBlock) k_adj_gather_camera(DevRender R, Wave W, AdjWave A) {
+    extern __shared__ float smem[];
+    const GradAcc acc = grad_begin(A, smem);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < W.count) {
+        const float4 h = W.hit0[i];
+        if (__float_as_int(h.y) >= 0) {
+            const float4 v = A.v0[i];
+            adj_vertex_direct(R, W, A, acc, i, W.aux, c3(v.x, v.y, v.z), __float_as_int(v.w), A.v0m[i],
+                              sample_weight(R, A, W.base + i));
+        }
+    }
+    grad_end(A, acc);
+}
+
+__global__ void k_adj_clear(AdjWave A, size_t n) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        A.pG[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        A.pv[q] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_adj_shade_path(DevScene S, DevRender R, Wave W, int j, AdjWave A) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = W.counters[1];
+    if (q >= n && (q & ~31u) >= n) return;
+    st_shade_path<true>(S, R, W, j, q, n, &A);
+}
+
+// adjoint of st_gather_path: direct-light gradients at bounce vertex j,
+// the vertex's direct light kept for the backward pass, and the same
+// continuation decision as the forward
+__global__ void __launch_bounds__(kBlock) k_adj_gather_path(DevRender R, Wave W, int j, C3 bg, AdjWave A) {
+    extern __shared__ float smem[];
+    const GradAcc acc = grad_begin(A, smem);
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = W.counters[1];
+    if (q < n || (q & ~31u) < n) {
+        const bool inq = q < n;
+        const uint32_t p = inq ? W.bq[q] : 0;
+        bool requeue = false;
+        if (inq) {
+            const uint32_t i = p / W.npath;
+            const float4 h = W.p_hit[p];
+            const float4 col = W.p_col[p];
+            const float startN = W.p_where[p].w;
+            const size_t ci = (size_t)p * R.path_depth + j;
+            if (__float_as_int(h.y) < 0) {
+                A.pG[ci] = make_float4(bg.r, bg.g, bg.b, 1.f);
+            } else {
+                const float4 d0 = W.diff0[i];
+                const float mult = (float)(1.0 / (double)(float)W.npath);
+                const C3 g = sample_weight(R, A, W.base + i);
+                const C3 Wv = ((g * c3(d0.x, d0.y, d0.z)) * (d0.w * mult * startN)) * c3(col.x, col.y, col.z);
+                const float4 v = A.pv[ci];
+                const C3 G = adj_vertex_direct(R, W, A, acc, p, W.p_aux, c3(v.x, v.y, v.z), __float_as_int(v.w),
+                                               A.pm[ci], Wv);
+                A.pG[ci] = make_float4(G.r, G.g, G.b, 1.f);
+                const float4 nc = W.p_next[p];
+                const C3 ncol = c3(nc.x, nc.y, nc.z);
+                W.p_col[p] = make_float4(ncol.r, ncol.g, ncol.b, 0.f);
+                if (j + 1 < R.path_depth && !(energy(ncol) < 0.05f)) {
+                    const float4 nr = W.p_nray[p];
+                    W.p_ray[p] = make_float4(nr.x, nr.y, nr.z, 1.f);
+                    requeue = true;
+                }
+            }
+        }
+        const uint32_t nq = warp_append(&W.counters[2], requeue);
+        if (requeue) W.bq2[nq] = p;
+    }
+    grad_end(A, acc);
+}
+
+// per camera sample: path products backwards, the camera vertex's diffuse
+// colour and the path light's power
+__global__ void __launch_bounds__(kBlock) k_adj_finish(DevRender R, Wave W, AdjWave A) {
+    extern __shared__ float smem[];
+    const GradAcc acc = grad_begin(A, smem);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < W.count && R.path_light >= 0) {
+        const float4 h = W.hit0[i], d0 = W.diff0[i];
+        if (__float_as_int(h.y) >= 0 && d0.w != 0.f) {
+            const C3 g = sample_weight(R, A, W.base + i), dif0 = c3(d0.x, d0.y, d0.z);
+            const float mult = (float)(1.0 / (double)(float)W.npath);
+            const C3 Acol = (g * dif0) * (d0.w * mult);
+            C3 Tsum = c3(0.f, 0.f, 0.f);
+            C3 rc[16];
+            for (uint32_t pi = 0; pi < W.npath; pi++) {
+                const uint32_t p = i * W.npath + pi;
+                const float startN = W.p_where[p].w;
+                const size_t c0 = (size_t)p * R.path_depth;
+                int J = 0;
+                rc[0] = c3(1.f, 1.f, 1.f);
+                while (J < R.path_depth && A.pG[c0 + J].w != 0.f) {
+                    const float4 v = A.pv[c0 + J];
+                    rc[J + 1] = __float_as_int(v.w) >= 0 ? rc[J] * c3(v.x, v.y, v.z) : c3(0.f, 0.f, 0.f);
+                    J++;
+                }
+                C3 U = c3(0.f, 0.f, 0.f);  // sum over later vertices, Horner form
+                for (int jj = J - 1; jj >= 0; jj--) {
+                    const float4 v = A.pv[c0 + jj], G = A.pG[c0 + jj];
+                    const int sid = __float_as_int(v.w);
+                    if (sid >= 0) {
+                        if (U.r != 0.f || U.g != 0.f || U.b != 0.f)
+                            chain_shader(R, A, acc, sid, A.pm[c0 + jj], (Acol * startN) * (rc[jj] * U),
+                                         c3(0.f, 0.f, 0.f));
+                        U = c3(G.x, G.y, G.z) + c3(v.x, v.y, v.z) * U;
+                    } else {
+                        U = c3(G.x, G.y, G.z);
+                    }
+                }
+                Tsum = Tsum + startN * U;
+            }
+            const float4 v = A.v0[i];
+            chain_shader(R, A, acc, __float_as_int(v.w), A.v0m[i], g * (Tsum * (d0.w * mult)), c3(0.f, 0.f, 0.f));
+            acc.add(A.li_pidx[R.path_light], dot3(g, dif0 * (Tsum * mult)));
+        }
+    }
+    grad_end(A, acc);
+}
+
+// ------------------------------------------------------------ layout
+constexpr int kNumAdjBufs = 7;
+
+static void adj_sizes(const Plan &P, uint32_t wcap, uint32_t npix, size_t *b) {
+    const size_t w = wcap, pc = (size_t)wcap * (P.npath > 1u ? P.npath : 1u), vc = w > pc ? w : pc;
+    const size_t slots = vc * (P.ns > 1u ? P.ns : 1u), pd = pc * (size_t)P.depth;
+    const size_t f4 = sizeof(float4);
+    const size_t sizes[kNumAdjBufs] = {f4 * slots, f4 * w, 4 * w, f4 * pd, 4 * pd, f4 * pd, f4 * (size_t)npix};
+    for (int i = 0; i < kNumAdjBufs; i++) b[i] = sizes[i];
+}
+
+static size_t adj_bytes(const Plan &P, uint32_t wcap, uint32_t npix) {
+    size_t b[kNumAdjBufs], t = 0;
+    adj_sizes(P, wcap, npix, b);
+    for (int i = 0; i < kNumAdjBufs; i++) t += (b[i] + kBufAlign - 1) / kBufAlign * kBufAlign;
+    return t;
+}
+
+static void assign_adj(const Plan &P, uint32_t wcap, uint32_t npix, char *base, AdjWave &A) {
+    size_t b[kNumAdjBufs];
+    adj_sizes(P, wcap, npix, b);
+    void *ptr[kNumAdjBufs];
+    size_t off = 0;
+    for (int i = 0; i < kNumAdjBufs; i++) {
+        ptr[i] = base + off;
+        off += (b[i] + kBufAlign - 1) / kBufAlign * kBufAlign;
+    }
+    A.slot_s = (float4 *)ptr[0];
+    A.v0 = (float4 *)ptr[1];
+    A.v0m = (float *)ptr[2];
+    A.pv = (float4 *)ptr[3];
+    A.pm = (float *)ptr[4];
+    A.pG = (float4 *)ptr[5];
+    A.gpix = (const float4 *)ptr[6];
+}
+
+static yr_status adj_scratch(yr_scene *s, size_t bytes, void **p) {
+    constexpr int kSlot = 2;  // 0: render waves, 1: host staging
+    if ((int)s->scratch.size() <= kSlot) s->scratch.resize(kSlot + 1);
+    DevBuf &b = s->scratch[kSlot];
+    if (b.bytes < bytes) {
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+        if (cudaMalloc(&b.p, bytes) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
+        b.bytes = bytes;
+    }
+    *p = b.p;
+    return YR_OK;
+}
+
+int grid_for(uint32_t n, int block);
+
+}  // namespace yr
+
+using namespace yr;
+
+extern "C" {
+
+YR_API uint32_t yr_param_count(const yr_scene *scene) { return scene ? scene->nparams : 0u; }
+
+YR_API yr_status yr_params_get(const yr_scene *scene, float *params) {
+    if (!scene || !params) return YR_ERR_INVALID_ARG;
+    for (size_t i = 0; i < scene->shader_desc.size(); i++) {
+        const yr_shader_desc &d = scene->shader_desc[i];
+        float *o = params + scene->sh_pbase[i];
+        o[0] = d.color[0];
+        o[1] = d.color[1];
+        o[2] = d.color[2];
+        o[3] = std::max(d.specular[0], std::max(d.specular[1], d.specular[2]));
+        if (d.tex_type != YR_TEX_NONE) {
+            o[4] = d.tex_intensity;
+            o[5] = d.tex_color1[0];
+            o[6] = d.tex_color1[1];
+            o[7] = d.tex_color1[2];
+        }
+    }
+    for (size_t k = 0; k < scene->light_desc.size(); k++) params[scene->li_pidx[k]] = scene->light_desc[k].power;
+    return YR_OK;
+}
+
+YR_API yr_status yr_params_set(yr_scene *scene, const float *params) {
+    if (!scene || !params) return YR_ERR_INVALID_ARG;
+    std::vector<yr_shader_desc> sh = scene->shader_desc;
+    std::vector<yr_light_desc> li = scene->light_desc;
+    for (size_t i = 0; i < sh.size(); i++) {
+        const float *o = params + scene->sh_pbase[i];
+        for (int c = 0; c < 3; c++) {
+            sh[i].color[c] = o[c];
+            sh[i].specular[c] = o[3] * scene->spec_dir[4 * i + c];
+        }
+        if (sh[i].tex_type != YR_TEX_NONE) {
+            sh[i].tex_intensity = o[4];
+            for (int c = 0; c < 3; c++) sh[i].tex_color1[c] = o[5 + c];
+        }
+    }
+    for (size_t k = 0; k < li.size(); k++) li[k].power = params[scene->li_pidx[k]];
+    return yr_scene_set_params(scene, sh.empty() ? nullptr : sh.data(), li.empty() ? nullptr : li.data());
+}
+
+YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, float *dparams, float *loss_out,
+                             void *stream) {
+    if (!scene || !desc || !desc->target || !desc->image || (!dparams && scene->nparams)) return YR_ERR_INVALID_ARG;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(scene->device);
+    auto done = [&](yr_status e) {
+        cudaSetDevice(prev);
+        return e;
+    };
+    cudaStream_t st = (cudaStream_t)stream;
+    const DevRender &R = scene->rdr;
+    Plan P;
+    yr_status ret = make_plan(scene, P);
+    if (ret != YR_OK) return done(ret);
+    if (R.raydepth <= 0) return done(YR_ERR_UNSUPPORTED);
+    // one block: loss (double, padded), wave buffers, adjoint buffers
+    const size_t budget = 1536ull << 20;
+    uint32_t wcap = std::max<uint32_t>(R.spp, 1u);
+    {
+        uint64_t lo = 1, hi = P.rpix;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi + 1) / 2;
+            const uint32_t w = (uint32_t)(mid * R.spp);
+            if (wave_bytes(P, w) + adj_bytes(P, w, P.npix) <= budget) lo = mid;
+            else hi = mid - 1;
+        }
+        wcap = (uint32_t)(lo * R.spp);
+    }
+    const size_t wb = (wave_bytes(P, wcap) + 255) / 256 * 256;
+    void *blk = nullptr;
+    if ((ret = adj_scratch(scene, 256 + wb + adj_bytes(P, wcap, P.npix), &blk)) != YR_OK) return done(ret);
+    double *d_loss = (double *)blk;
+    Wave W;
+    std::memset(&W, 0, sizeof(W));
+    assign_wave(P, wcap, (char *)blk + 256, W);
+    AdjWave A;
+    std::memset(&A, 0, sizeof(A));
+    assign_adj(P, wcap, P.npix, (char *)blk + 256 + wb, A);
+    A.grad = dparams;
+    A.sh_pbase = scene->d_sh_pbase;
+    A.li_pidx = scene->d_li_pidx;
+    A.spec_dir = scene->d_spec_dir;
+    A.nparams = scene->nparams;
+    const size_t smem = A.nparams <= kSmemParams ? sizeof(float) * std::max<uint32_t>(A.nparams, 1u) : 0;
+
+    if (scene->nparams) cudaMemsetAsync(dparams, 0, sizeof(float) * scene->nparams, st);
+    cudaMemsetAsync(d_loss, 0, sizeof(double), st);
+    cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
+    cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
+    k_adj_loss<<<grid_for(P.npix, kBlock), kBlock, 0, st>>>((const float4 *)desc->image,
+                                                             (const float4 *)desc->target, P.npix, desc->loss_scale,
+                                                             (float4 *)A.gpix, d_loss);
+    const DevScene &D = scene->dev;
+    const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
+    const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
+    for (uint64_t b = 0; b < P.total; b += wcap) {
+        W.base = (uint32_t)b;
+        W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
+        const int g = (int)((W.count + kBlock - 1) / kBlock);
+        cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
+        k_primary<<<g, kBlock, 0, st>>>(D, R, W);
+        k_adj_shade_camera<<<g, kBlock, 0, st>>>(D, R, W, A);
+        k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
+        k_adj_gather_camera<<<g, kBlock, smem, st>>>(R, W, A);
+        if (P.npath > 0) {
+            const size_t nc = (size_t)W.count * P.npath * P.depth;
+            k_adj_clear<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(A, nc);
+            const int gp = (int)(((size_t)W.count * P.npath + kBlock - 1) / kBlock);
+            for (int j = 0; j < R.path_depth; j++) {
+                k_trace_bounce<<<gq, kBlock, 0, st>>>(D, W);
+                cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
+                k_adj_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j, A);
+                k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
+                k_adj_gather_path<<<gp, kBlock, smem, st>>>(R, W, j, R.background, A);
+                std::swap(W.bq, W.bq2);
+                k_swap_queues<<<1, 1, 0, st>>>(W);
+            }
+            k_adj_finish<<<g, kBlock, smem, st>>>(R, W, A);
+        }
+    }
+    if (cudaGetLastError() != cudaSuccess) return done(YR_ERR_CUDA);
+    if (loss_out) {
+        double l = 0.0;
+        if (cudaMemcpyAsync(&l, d_loss, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return done(YR_ERR_CUDA);
+        *loss_out = (float)l;
+    }
+    return done(take_status(scene, st));
+}
+
+}  // extern "C"

@@ -197,15 +197,21 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
 // modulator_t::modulate (texture.cc:499-534) in "mix" mode with procedural
 // texture coordinates size*(P + ofs) (texture.cc:307-312), applied to the
 // diffuse colour only.
-__device__ __forceinline__ C3 modulated_color(const DevShader &sh, const V3 &P) {
+// `m_out` (optional) receives the noise value before the intensity scale
+// (the fBm sum, or the clouds turbulence), which the adjoint needs.
+__device__ __forceinline__ C3 modulated_color(const DevShader &sh, const V3 &P, float *m_out = nullptr) {
     C3 C = sh.color;
     if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f)) return C;
     const V3 tp = v3(sh.msize[0] * (P.x + sh.mofs[0]), sh.msize[1] * (P.y + sh.mofs[1]), sh.msize[2] * (P.z + sh.mofs[2]));
     float f;
-    if (sh.tex_type == YR_TEX_MUSGRAVE_FBM)  // textureMusgrave_t::getFloat (basictex.cc:677-680)
-        f = sh.intensity * fbm(V3{tp.x * sh.tsize, tp.y * sh.tsize, tp.z * sh.tsize}, sh.H, sh.lacunarity, sh.octaves);
-    else  // textureClouds_t::getFloat (basictex.cc:83-91), no bias
+    if (sh.tex_type == YR_TEX_MUSGRAVE_FBM) {  // textureMusgrave_t::getFloat (basictex.cc:677-680)
+        const float m = fbm(V3{tp.x * sh.tsize, tp.y * sh.tsize, tp.z * sh.tsize}, sh.H, sh.lacunarity, sh.octaves);
+        if (m_out) *m_out = m;
+        f = sh.intensity * m;
+    } else {  // textureClouds_t::getFloat (basictex.cc:83-91), no bias
         f = turbulence(tp, sh.tdepth, sh.tsize, sh.thard != 0);
+        if (m_out) *m_out = f;
+    }
     const C3 tex = sh.tc1 + f * (sh.tc2 - sh.tc1);
     // mix(texcolor, C, w) (color.cc:103-109)
     const float w = sh.mod_color;
@@ -227,6 +233,25 @@ __device__ __forceinline__ C3 from_light(const DevShader &sh, const C3 &lkc, con
     else refle = (float)pow((double)refle, (double)sh.hard);
     const C3 edif_inte = c3(1.f * inte, 1.f * inte, 1.f * inte);
     return ((edif_inte * lcol) * lkc) + (sh.specular * refle) * lcol;
+}
+
+// from_light split into the factor of the diffuse colour (D) and of the
+// specular colour (Sp): from_light = D * lkc + specular * Sp.
+__device__ __forceinline__ void from_light_parts(const DevShader &sh, const Surf &sp, const V3 &ldir,
+                                                 const C3 &lcol, const V3 &eye, C3 &D, C3 &Sp) {
+    V3 edir = normalize(eye);
+    const V3 N = face_forward(sp.Ng, sp.N, edir);
+    const float inte = dot(N, ldir);
+    if (inte < 0.f) {
+        D = Sp = c3(0.f, 0.f, 0.f);
+        return;
+    }
+    edir = reflect(N, edir);
+    float refle = dot(edir, ldir);
+    if (refle < 0.f) refle = 0.f;
+    else refle = (float)pow((double)refle, (double)sh.hard);
+    D = inte * lcol;
+    Sp = refle * lcol;
 }
 
 // haltonSampler_t::nextDirection (pathtools.cc:32-43) for explicit z1, z2

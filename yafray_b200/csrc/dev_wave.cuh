@@ -48,6 +48,22 @@ struct Wave {
     float *out;          // RGBA image (device)
 };
 
+// Extra per-wave state of the adjoint recompute (yr_backward).
+struct AdjWave {
+    float4 *slot_s;        // [slots] specular factor per light sample (slot_c: diffuse factor)
+    float4 *v0;            // [count] camera vertex: diffuse colour, shader (bits)
+    float *v0m;            // [count] noise value at the camera vertex
+    float4 *pv;            // [count*npath*depth] path vertex: diffuse colour, shader (bits); w = -1: none
+    float *pm;             // [count*npath*depth] noise value at the path vertex
+    float4 *pG;            // [count*npath*depth] direct light (or background) at the vertex; w = 1: present
+    const float4 *gpix;    // per image pixel: dL/d(pixel rgb)
+    float *grad;           // parameter gradient (global)
+    const int *sh_pbase;   // first parameter of each shader
+    const int *li_pidx;    // parameter of each light (its power)
+    const float4 *spec_dir;// unit specular direction of each shader
+    uint32_t nparams;
+};
+
 // warp-reduced traversal counters, one atomic per warp (all lanes must call)
 __device__ __forceinline__ void count_work(const Wave &W, int cls, uint32_t rays, uint32_t nodes, uint32_t tests) {
     const uint32_t r = __reduce_add_sync(0xffffffffu, rays);
@@ -137,7 +153,7 @@ __device__ __forceinline__ void st_primary(const DevScene &S, const DevRender &R
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_primary(DevScene S, DevRender R, Wave W) {
+static __global__ void __launch_bounds__(kBlock) k_primary(DevScene S, DevRender R, Wave W) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
@@ -151,14 +167,21 @@ __global__ void __launch_bounds__(kBlock) k_primary(DevScene S, DevRender R, Wav
 // per-light sampling at one shading vertex; writes slots, aux and queue
 // entries.  vtx = vertex index for slots/aux, v = QMC vertex level,
 // m0 = QMC sample index of this vertex.
+// ADJ (adjoint recompute): slot_c / slot_s receive the diffuse and specular
+// factors per unit light power instead of the light sample's colour, hemi
+// aux holds (diffuse factor, specular factor, 0, go), and the vertex's
+// diffuse colour and noise value are returned.
+template <bool ADJ = false>
 __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender &R, const Wave &W, bool active,
                                              const Surf &sp, const V3 &eye, uint32_t vtx, int v, uint32_t m0,
-                                             uint32_t pixel, float4 *aux) {
+                                             uint32_t pixel, float4 *aux, float4 *slot_s = nullptr,
+                                             C3 *lkc_out = nullptr, float *m_out = nullptr) {
     DevShader sh;
     C3 lkc = c3(0.f, 0.f, 0.f);
     if (active) {
         sh = R.shaders[sp.shader];
-        lkc = modulated_color(sh, sp.P);
+        lkc = modulated_color(sh, sp.P, ADJ ? m_out : nullptr);
+        if (ADJ) *lkc_out = lkc;
     }
     V3 N = sp.N;
     if (active) N = face_forward(sp.Ng, sp.N, normalize(eye));
@@ -176,8 +199,15 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                 const V3 dir = normalize(Lv);
                 float id2 = dot(Lv, Lv);
                 if (id2 != 0.f) id2 = 1.f / id2;
-                const C3 c = from_light(sh, lkc, sp, dir, L.color * id2, eye);
-                W.slot_c[slot] = make_float4(c.r, c.g, c.b, 0.f);
+                if (ADJ) {
+                    C3 D, Sp;
+                    from_light_parts(sh, sp, dir, L.rawc * id2, eye, D, Sp);
+                    W.slot_c[slot] = make_float4(D.r, D.g, D.b, 0.f);
+                    slot_s[slot] = make_float4(Sp.r, Sp.g, Sp.b, 0.f);
+                } else {
+                    const C3 c = from_light(sh, lkc, sp, dir, L.color * id2, eye);
+                    W.slot_c[slot] = make_float4(c.r, c.g, c.b, 0.f);
+                }
                 if (L.cast) {
                     // isShadowed(sp, from): ray = l - p, dist = |l - p|
                     rdir = L.from - sp.P;
@@ -227,8 +257,15 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                             V3 dir = Lv;
                             float ld2 = norm_len_sqr(dir);
                             ld2 = (ld2 != 0.f) ? (1.f / ld2) : 1.f;
-                            const C3 c = from_light(sh, lkc, sp, dir, (L.power * L.color) * ld2, eye);
-                            W.slot_c[slot] = make_float4(c.r, c.g, c.b, 0.f);
+                            if (ADJ) {
+                                C3 D, Sp;
+                                from_light_parts(sh, sp, dir, L.color * ld2, eye, D, Sp);
+                                W.slot_c[slot] = make_float4(D.r, D.g, D.b, 0.f);
+                                slot_s[slot] = make_float4(Sp.r, Sp.g, Sp.b, 0.f);
+                            } else {
+                                const C3 c = from_light(sh, lkc, sp, dir, (L.power * L.color) * ld2, eye);
+                                W.slot_c[slot] = make_float4(c.r, c.g, c.b, 0.f);
+                            }
                             W.slot_f[slot] = kSlotPending;
                             rdir = sampleP - sp.P;
                             dist = length(rdir);
@@ -250,7 +287,13 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                 fl = from_light(sh, lkc, sp, Nh, c3(1.f, 1.f, 1.f), eye);
                 const float mad = fmaxf(fabsf(fl.r), fmaxf(fabsf(fl.g), fabsf(fl.b)));
                 go = !(mad < 0.05f);
-                aux[vtx * R.nlights + k] = make_float4(fl.r, fl.g, fl.b, go ? 1.f : 0.f);
+                if (ADJ) {
+                    C3 D, Sp;
+                    from_light_parts(sh, sp, Nh, c3(1.f, 1.f, 1.f), eye, D, Sp);
+                    aux[vtx * R.nlights + k] = make_float4(D.r, Sp.r, 0.f, go ? 1.f : 0.f);
+                } else {
+                    aux[vtx * R.nlights + k] = make_float4(fl.r, fl.g, fl.b, go ? 1.f : 0.f);
+                }
             }
             const uint32_t d = light_dim(k, v);
             const float r0 = cp_rot(R.seed, pixel, d), r1 = cp_rot(R.seed, pixel, d + 1);
@@ -336,7 +379,9 @@ __device__ __forceinline__ uint32_t light_slots(const DevLight &L) {
 }
 
 // whole warp
-__device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRender &R, const Wave &W, uint32_t i) {
+template <bool ADJ = false>
+__device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRender &R, const Wave &W, uint32_t i,
+                                                const AdjWave *A = nullptr) {
     const bool inb = i < W.count;
     const uint32_t cs = W.base + (inb ? i : 0);
     int x, y;
@@ -357,7 +402,17 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
             active = true;
         }
     }
-    shade_lights(S, R, W, active, sp, eye, inb ? i : 0, 0, s, pixel, W.aux);
+    if (ADJ) {
+        C3 lkc = c3(0.f, 0.f, 0.f);
+        float m = 0.f;
+        shade_lights<true>(S, R, W, active, sp, eye, inb ? i : 0, 0, s, pixel, W.aux, A->slot_s, &lkc, &m);
+        if (active) {
+            A->v0[i] = make_float4(lkc.r, lkc.g, lkc.b, __int_as_float(sp.shader));
+            A->v0m[i] = m;
+        }
+    } else {
+        shade_lights(S, R, W, active, sp, eye, inb ? i : 0, 0, s, pixel, W.aux);
+    }
     if (!inb || R.path_light < 0) return;
     // pathLight_t::normalSample (pathlight.cc:389-403) + the first
     // directions of takeSample (pathlight.cc:305-312)
@@ -392,7 +447,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_shade_camera(DevScene S, DevRender R, Wave W) {
+static __global__ void __launch_bounds__(kBlock) k_shade_camera(DevScene S, DevRender R, Wave W) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= W.count && (i & ~31u) >= W.count) return;  // whole warps past the end leave
     st_shade_camera(S, R, W, i);
@@ -408,7 +463,7 @@ __device__ __forceinline__ void st_trace_shadow(const DevScene &S, const Wave &W
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_trace_shadow_q(DevScene S, Wave W, float self_bias) {
+static __global__ void __launch_bounds__(kBlock) k_trace_shadow_q(DevScene S, Wave W, float self_bias) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
@@ -436,7 +491,7 @@ __device__ __forceinline__ void st_gather_camera(const DevRender &R, const Wave 
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_gather_camera(DevRender R, Wave W) {
+static __global__ void __launch_bounds__(kBlock) k_gather_camera(DevRender R, Wave W) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < W.count) st_gather_camera(R, W, i);
 }
@@ -455,7 +510,7 @@ __device__ __forceinline__ void st_trace_bounce(const DevScene &S, const Wave &W
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_trace_bounce(DevScene S, Wave W) {
+static __global__ void __launch_bounds__(kBlock) k_trace_bounce(DevScene S, Wave W) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
@@ -472,8 +527,9 @@ __global__ void __launch_bounds__(kBlock) k_trace_bounce(DevScene S, Wave W) {
 // shading at bounce vertex j (pathlight.cc:313-346): light samples, next
 // direction and pending raycolor
 // whole warp; q indexes the bounce queue (lanes past its end are inactive)
+template <bool ADJ = false>
 __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender &R, const Wave &W, int j,
-                                              uint32_t q, uint32_t n) {
+                                              uint32_t q, uint32_t n, const AdjWave *A = nullptr) {
     const bool inq = q < n;
     const uint32_t p = inq ? W.bq[q] : 0;
     const uint32_t i = p / W.npath, pi = p % W.npath;
@@ -497,10 +553,21 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
             active = true;
         }
     }
-    shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux);
+    C3 dif = c3(0.f, 0.f, 0.f);
+    if (ADJ) {
+        float m = 0.f;
+        shade_lights<true>(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux, A->slot_s, &dif,
+                           &m);
+        if (active) {
+            const size_t ci = (size_t)p * R.path_depth + j;
+            A->pv[ci] = make_float4(dif.r, dif.g, dif.b, __int_as_float(sp.shader));
+            A->pm[ci] = m;
+        }
+    } else {
+        shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux);
+    }
     if (active) {
-        const DevShader sh = R.shaders[sp.shader];
-        const C3 dif = modulated_color(sh, sp.P);
+        if (!ADJ) dif = modulated_color(R.shaders[sp.shader], sp.P);
         const float4 col = W.p_col[p];
         const C3 nc = c3(col.x, col.y, col.z) * dif;
         W.p_next[p] = make_float4(nc.r, nc.g, nc.b, 0.f);
@@ -519,7 +586,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_shade_path(DevScene S, DevRender R, Wave W, int j) {
+static __global__ void __launch_bounds__(kBlock) k_shade_path(DevScene S, DevRender R, Wave W, int j) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = W.counters[1];
     if (q >= n && (q & ~31u) >= n) return;
@@ -568,7 +635,7 @@ __device__ __forceinline__ void st_gather_path(const DevRender &R, const Wave &W
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_gather_path(DevRender R, Wave W, int j, C3 bg) {
+static __global__ void __launch_bounds__(kBlock) k_gather_path(DevRender R, Wave W, int j, C3 bg) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = W.counters[1];
     if (q >= n && (q & ~31u) >= n) return;
@@ -636,21 +703,21 @@ __device__ __forceinline__ void st_finish(const DevRender &R, const Wave &W, uin
 }
 
 #ifdef YR_WAVE_KERNELS
-__global__ void __launch_bounds__(kBlock) k_finish(DevRender R, Wave W) {
+static __global__ void __launch_bounds__(kBlock) k_finish(DevRender R, Wave W) {
     const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
     if (px < W.count / R.spp) st_finish(R, W, px);
 }
 #endif
 
 #ifdef YR_WAVE_KERNELS
-__global__ void k_clear_contri(Wave W, size_t n) {
+static __global__ void k_clear_contri(Wave W, size_t n) {
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
         W.p_contri[q] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 #endif
 
 #ifdef YR_WAVE_KERNELS
-__global__ void k_swap_queues(Wave W) {
+static __global__ void k_swap_queues(Wave W) {
     // bounce queue <- next queue (the caller swaps the pointers)
     W.counters[1] = W.counters[2];
     W.counters[2] = 0;
@@ -658,7 +725,7 @@ __global__ void k_swap_queues(Wave W) {
 #endif
 
 #ifdef YR_WAVE_KERNELS
-__global__ void k_count(Wave W, int which) {
+static __global__ void k_count(Wave W, int which) {
     // accumulate queue lengths into the 64-bit ray totals
     if (which == 0) W.rays[1] += W.counters[0];
     if (which == 1) W.rays[2] += W.counters[1];

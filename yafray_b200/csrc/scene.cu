@@ -112,6 +112,7 @@ yr_status make_lights(const std::vector<yr_light_desc> &in, std::vector<DevLight
         std::memset(&L, 0, sizeof(L));
         L.type = (int)d.type;
         L.color = c3(d.color[0], d.color[1], d.color[2]);
+        L.rawc = L.color;
         L.power = d.power;
         L.samples = d.samples;
         L.depth = d.depth;
@@ -532,6 +533,30 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
             R.path_samples = s->lights[i].samples;
             R.path_depth = s->lights[i].depth;
         }
+
+    // ---- adjoint parameter vector (yr_param_count): per shader color[3] and
+    // specular weight, plus amplitude and base colour for textured shaders;
+    // per light its power
+    {
+        uint32_t n = 0;
+        s->sh_pbase.resize(s->shaders.size());
+        s->spec_dir.assign(4 * s->shaders.size(), 0.f);
+        for (size_t i = 0; i < s->shaders.size(); i++) {
+            s->sh_pbase[i] = (int)n;
+            n += 4 + (s->shader_desc[i].tex_type != YR_TEX_NONE ? 4 : 0);
+            const float *ks = s->shader_desc[i].specular;
+            const float w = std::max(ks[0], std::max(ks[1], ks[2]));
+            for (int k = 0; k < 3; k++) s->spec_dir[4 * i + k] = w > 0.f ? ks[k] / w : 1.f;
+        }
+        s->li_pidx.resize(s->lights.size());
+        for (size_t i = 0; i < s->lights.size(); i++) s->li_pidx[i] = (int)n++;
+        s->nparams = n;
+        if ((st = dev_upload(s, s->sh_pbase.data(), s->sh_pbase.size(), &s->d_sh_pbase)) != YR_OK) return fail(st);
+        if (!s->li_pidx.empty() && (st = dev_upload(s, s->li_pidx.data(), s->li_pidx.size(), &s->d_li_pidx)) != YR_OK)
+            return fail(st);
+        if ((st = dev_upload(s, (const float4 *)s->spec_dir.data(), s->shaders.size(), &s->d_spec_dir)) != YR_OK)
+            return fail(st);
+    }
 
     yr_scene_info &I = s->info;
     I.nobjects = desc->nobjects;

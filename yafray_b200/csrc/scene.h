@@ -37,6 +37,7 @@ struct DevLight {
     float sampdiv;       // hemi: power/samples
     int pt_base;         // area: first entry in DevRender::area_pts
     int pad;
+    C3 rawc;             // the light's "color" parameter (before any power scale)
 };
 
 struct DevCamera {
@@ -93,6 +94,13 @@ struct yr_scene {
     yr::DevLight *d_lights = nullptr;
     // render scratch (grown on demand)
     std::vector<yr::DevBuf> scratch;
+    // adjoint parameter vector: first index of each shader's and light's
+    // parameters; unit specular direction of each shader
+    uint32_t nparams = 0;
+    std::vector<int> sh_pbase, li_pidx;
+    std::vector<float> spec_dir;      // 4 per shader
+    int *d_sh_pbase = nullptr, *d_li_pidx = nullptr;
+    float4 *d_spec_dir = nullptr;
 };
 
 namespace yr {
