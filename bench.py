@@ -189,10 +189,87 @@ def load_traffic():
     return {}
 
 
+def run_diff(args, api, torch, local, fd_params=16):
+    """Adjoint workload: the small scene at 512x512, 64 spp, 64 material
+    groups (diffuse RGB + specular weight) and 8 area lights = 264
+    parameters; target rendered from hidden parameters.  One step = one
+    forward render + one yr_backward.  Reports the adjoint / forward time
+    ratio and a check of the gradient against FP64-accumulated central
+    differences (step 1e-3) on `fd_params` sampled parameters."""
+    sc = scenes.config_diff()
+    hid = scenes.config_diff(hidden=True)
+    ds = api.DeviceScene(sc, device=local)
+    n = ds.param_count()
+    theta = ds.params_get()
+    dh = api.DeviceScene(hid, device=local)
+    target = torch.empty((sc.resy, sc.resx, 4), dtype=torch.float32, device="cuda")
+    dh.render_into(target.data_ptr())
+    dh.close()
+    img = torch.empty_like(target)
+    grad = torch.empty(n, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        ds.render_into(img.data_ptr())
+        ds.backward(img.data_ptr(), target.data_ptr(), grad.data_ptr())
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd_ms = bwd_ms = 0.0
+    rays = 0
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.steps):
+        ev[0].record()
+        st = ds.render_into(img.data_ptr())
+        ev[1].record()
+        loss = ds.backward(img.data_ptr(), target.data_ptr(), grad.data_ptr())
+        ev[2].record()
+        torch.cuda.synchronize()
+        fwd_ms += ev[0].elapsed_time(ev[1])
+        bwd_ms += ev[1].elapsed_time(ev[2])
+        rays += st.rays_primary + st.rays_shadow + st.rays_bounce
+    clk = clocks.stop()
+    g = grad.cpu().numpy().astype(np.float64)
+    tgt = target.cpu().numpy()
+
+    def loss64(t):
+        d = t.cpu().numpy()[..., :3].astype(np.float64) - tgt[..., :3].astype(np.float64)
+        return float((d * d).sum())
+
+    rng = np.random.default_rng(0)
+    idx = rng.choice(n, size=min(fd_params, n), replace=False)
+    rel = []
+    for k in idx:
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] = np.float32(theta[k] + 1e-3)
+        tm[k] = np.float32(theta[k] - 1e-3)
+        ds.params_set(tp)
+        ds.render_into(img.data_ptr())
+        lp = loss64(img)
+        ds.params_set(tm)
+        ds.render_into(img.data_ptr())
+        lm = loss64(img)
+        fd = (lp - lm) / (float(tp[k]) - float(tm[k]))
+        rel.append(abs(g[k] - fd) / max(abs(fd), 1e-30))
+    ds.params_set(theta)
+    ds.close()
+    value = rays / ((fwd_ms + bwd_ms) / 1000.0) / 1e6 if fwd_ms + bwd_ms > 0 else 0.0
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": (fwd_ms + bwd_ms) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": f"adjoint: small scene 512x512, 64 spp, 64 material groups, 8 area lights, "
+                               f"{n} parameters", "parameters": n},
+        "forward_ms": fwd_ms / args.steps, "adjoint_ms": bwd_ms / args.steps,
+        "adjoint_over_forward": bwd_ms / fwd_ms if fwd_ms else None, "loss": loss,
+        "fd_check": {"params": [int(k) for k in idx], "max_rel_err": float(max(rel)),
+                     "median_rel_err": float(np.median(rel)), "step": 1e-3, "accumulation": "fp64"},
+        "gpu_launches": None, "clocks": clk,
+    }))
+
+
 def run_batch(args, api, torch, local, barrier):
     """Uneven batch: `batch_count` independent scenes (1k-200k triangles,
     1-32 objects, 64^2-512^2, 4-64 spp, 1-4 lights, GI 1-3 bounces) rendered
-    by one persistent launch (yr_render_batch, autotuned, CUDA graph), with
+    as one launch (yr_render_batch: autotuned schedule, CUDA graph), with
     the plain one-scene-per-call path (yr_render per scene) timed beside it
     on the same scenes; images of both paths are compared bit for bit."""
     scs = scenes.config_batch(count=args.batch_count)
@@ -264,7 +341,8 @@ def run_batch(args, api, torch, local, barrier):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-        "config": {"workload": f"batch: {len(dss)} scenes, {ntris:,} triangles, one persistent launch",
+        "config": {"workload": f"batch: {len(dss)} scenes, {ntris:,} triangles, one graph launch",
+                   "schedule": {1: "tiles", 2: "waves"}.get(prm.mode, prm.mode), "streams": prm.streams,
                    "block_size": prm.block_size, "queue_tile": prm.queue_tile,
                    "stack_entries": prm.stack_entries, "autotune_s": round(tune_s, 3),
                    "scene_setup_s": round(setup_s, 3), "l2": "scene arrays and images larger than L2"},
@@ -288,7 +366,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small", "batch"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "batch", "diff"])
     ap.add_argument("--batch-count", type=int, default=256, help="scenes in the batch workload")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--resx", type=int, default=1920)
@@ -321,6 +399,9 @@ def main():
 
     if args.config == "batch":
         run_batch(args, api, torch, local, barrier)
+        return
+    if args.config == "diff":
+        run_diff(args, api, torch, local)
         return
     sc, name = workload(args)
     if args.exact_order:

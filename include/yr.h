@@ -372,22 +372,29 @@ YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
  *     the ray counts are filled in. */
 YR_API yr_status yr_render_noalloc(yr_scene *scene, float *rgba, yr_render_stats *stats, void *stream);
 
-/* Render `count` independent scenes (one device) in one persistent launch.
- * Work items are tiles of whole pixels of one scene; blocks pull them from
- * a shared counter and run the render stages over the tile with
- * block-local ray queues.  Each image equals yr_render's for that scene.
+/* Render `count` independent scenes (one device) as one launch.  Two
+ * schedules, both giving each scene exactly yr_render's image:
+ *   YR_BATCH_TILES: one persistent kernel; work items are tiles of whole
+ *     pixels of one scene, pulled from a shared counter, and each block runs
+ *     the render stages over its tile with block-local ray queues;
+ *   YR_BATCH_WAVES: every scene's own wavefront (per-scene ray queues, the
+ *     kernels of yr_render) on one of `streams` concurrent streams, the
+ *     whole batch captured as one CUDA graph.
  * outs[i]: device RGBA float image of scene i (its resx*resy*4 floats).
- * params (in/out, may be NULL = all automatic): block_size / queue_tile
- * 0 = autotuned on a sample of the work the first time this list of scenes
- * is rendered (then cached); use_graph = capture the launch in a CUDA graph
- * and replay it on later calls.  On return the fields hold the
- * configuration used (stack_entries: kd stack capacity).  Stats: ray
- * counts and the device time of the launch. */
+ * params (in/out, may be NULL = all automatic): mode 0 and block_size /
+ * queue_tile / streams 0 = autotuned the first time this list of scenes is
+ * rendered (timed on the device, then cached); use_graph = capture the
+ * launch in a CUDA graph and replay it on later calls (the waves schedule
+ * always uses a graph).  On return the fields hold the configuration used.
+ * Stats: ray counts and the device time of the launch. */
+enum { YR_BATCH_AUTO = 0, YR_BATCH_TILES = 1, YR_BATCH_WAVES = 2 };
 typedef struct yr_batch_params {
-    int32_t block_size;      /* threads per block, 0 = autotuned              */
-    int32_t queue_tile;      /* camera samples per work item, 0 = autotuned   */
+    int32_t block_size;      /* tiles: threads per block, 0 = autotuned       */
+    int32_t queue_tile;      /* tiles: camera samples per item, 0 = autotuned */
     int32_t use_graph;       /* capture the launch in a CUDA graph            */
     int32_t stack_entries;   /* out: kd stack capacity of the kernel used     */
+    int32_t mode;            /* YR_BATCH_*                                    */
+    int32_t streams;         /* waves: concurrent streams, 0 = autotuned      */
 } yr_batch_params;
 
 YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t count, float *const *outs,

@@ -42,7 +42,9 @@ def _batched(torch, dss, **kw):
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(use_graph=False), dict(block_size=128, queue_tile=64),
-                                dict(block_size=256, queue_tile=1000, use_graph=True)])
+                                dict(block_size=256, queue_tile=1000, use_graph=True),
+                                dict(mode=abi.YR_BATCH_TILES), dict(mode=abi.YR_BATCH_WAVES),
+                                dict(mode=abi.YR_BATCH_WAVES, streams=3)])
 def test_batch_matches_per_scene(cuda, kw):
     import torch
     dss = [api.DeviceScene(sc) for sc in _small_batch(10)]
@@ -51,7 +53,13 @@ def test_batch_matches_per_scene(cuda, kw):
         got, st, p = _batched(torch, dss, **kw)
         for a, b in zip(got, ref):
             assert np.array_equal(a, b)
-        assert p.block_size in (32 * k for k in range(1, 33)) and p.queue_tile > 0
+        assert p.mode in (abi.YR_BATCH_TILES, abi.YR_BATCH_WAVES)
+        if "mode" in kw:
+            assert p.mode == kw["mode"]
+        if p.mode == abi.YR_BATCH_TILES:
+            assert p.block_size in (32 * k for k in range(1, 33)) and p.queue_tile > 0
+        else:
+            assert p.streams == kw.get("streams", p.streams) and p.streams >= 1
         assert p.stack_entries >= 32
     tot = sum(d.sc.resx * d.sc.resy * d.sc.render.spp for d in dss)
     assert st.rays_primary == tot

@@ -24,6 +24,7 @@ STATUS_NAMES = {
 
 YR_TEX_NONE, YR_TEX_MUSGRAVE_FBM, YR_TEX_CLOUDS = 0, 1, 2
 YR_LIGHT_POINT, YR_LIGHT_AREA, YR_LIGHT_HEMI, YR_LIGHT_PATH = 0, 1, 2, 3
+YR_BATCH_AUTO, YR_BATCH_TILES, YR_BATCH_WAVES = 0, 1, 2
 YR_PER_TRIANGLE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
 
@@ -129,7 +130,7 @@ class YrRenderStats(C.Structure):
 
 class YrBatchParams(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("queue_tile", C.c_int32), ("use_graph", C.c_int32),
-                ("stack_entries", C.c_int32)]
+                ("stack_entries", C.c_int32), ("mode", C.c_int32), ("streams", C.c_int32)]
 
 
 class YrBackwardDesc(C.Structure):

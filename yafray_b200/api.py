@@ -131,15 +131,18 @@ def trace_shadow(ds: DeviceScene, rays_dev_ptr: int, n: int, occ_dev_ptr: int, s
 
 
 def render_batch(dss: List[DeviceScene], out_ptrs: List[int], block_size: int = 0, queue_tile: int = 0,
-                 use_graph: bool = True, stream: int = 0):
-    """Render several scenes of one GPU in one persistent launch
-    (yr_render_batch).  out_ptrs: device RGBA float images, one per scene.
-    block_size / queue_tile 0 = autotuned.  Returns (stats, params used)."""
+                 use_graph: bool = True, stream: int = 0, mode: int = 0, streams: int = 0):
+    """Render several scenes of one GPU as one launch (yr_render_batch).
+    out_ptrs: device RGBA float images, one per scene.  mode: 0 = autotuned,
+    abi.YR_BATCH_TILES (persistent tile kernel; block_size / queue_tile 0 =
+    autotuned) or abi.YR_BATCH_WAVES (per-scene wavefronts on `streams`
+    concurrent streams in one CUDA graph; 0 = autotuned).  Returns (stats,
+    params used)."""
     lib = abi.load()
     n = len(dss)
     hs = (C.c_void_p * n)(*[d.handle.value for d in dss])
     outs = (C.c_void_p * n)(*out_ptrs)
-    p = abi.YrBatchParams(int(block_size), int(queue_tile), int(use_graph), 0)
+    p = abi.YrBatchParams(int(block_size), int(queue_tile), int(use_graph), 0, int(mode), int(streams))
     st = abi.YrRenderStats()
     abi.check(lib.yr_render_batch(hs, n, outs, C.byref(p), C.byref(st), C.c_void_p(stream)), "yr_render_batch")
     return st, p

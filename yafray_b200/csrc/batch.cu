@@ -158,10 +158,24 @@ static BatchKernel batch_kernel(int stack) {
 }
 
 struct BatchConfig {
+    int mode = 0;    // YR_BATCH_TILES / YR_BATCH_WAVES
     int block = 0;
     int tile = 0;    // camera samples per tile (cap)
     int stack = 0;
-    bool operator==(const BatchConfig &o) const { return block == o.block && tile == o.tile && stack == o.stack; }
+    int streams = 0;
+    bool operator==(const BatchConfig &o) const {
+        return mode == o.mode && block == o.block && tile == o.tile && stack == o.stack && streams == o.streams;
+    }
+};
+
+// One stream of the waves schedule: its scenes run one after another
+// through one scratch block.
+struct WaveLane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<uint32_t> scenes;
+    char *scratch = nullptr;
+    size_t bytes = 0;
 };
 
 // Device state of one batch (a list of scenes and output images), kept
@@ -175,6 +189,7 @@ struct BatchCtx {
     std::vector<DevRender> h_renders;
     Plan pmax{};
     int max_depth = 0;
+    uint64_t primary = 0;               // camera samples of all scenes
     DevScene *d_scenes = nullptr;
     DevRender *d_renders = nullptr;
     uint32_t *d_ns = nullptr, *d_npath = nullptr;
@@ -182,7 +197,8 @@ struct BatchCtx {
     BatchItem *d_items = nullptr;
     size_t items_cap = 0;
     uint32_t *d_next = nullptr;
-    unsigned long long *d_rays = nullptr;
+    unsigned long long *d_rays = nullptr;   // tiles: 4; waves: 4 per scene
+    unsigned long long *d_kst = nullptr;    // waves: shared kernel-class counters
     char *d_scratch = nullptr;
     size_t scratch_bytes = 0;
     BatchConfig tuned{};
@@ -191,9 +207,27 @@ struct BatchCtx {
     char *graph_scratch = nullptr;
     cudaGraphExec_t graph = nullptr;
     std::vector<BatchItem> items;
+    std::vector<WaveLane> lanes;
+    int lanes_n = 0;
+    cudaEvent_t fork = nullptr;
 
-    ~BatchCtx() {
+    void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+    void drop_lanes() {
+        for (WaveLane &l : lanes) {
+            if (l.stream) cudaStreamDestroy(l.stream);
+            if (l.done) cudaEventDestroy(l.done);
+            cudaFree(l.scratch);
+        }
+        lanes.clear();
+        lanes_n = 0;
+    }
+    ~BatchCtx() {
+        drop_graph();
+        drop_lanes();
+        if (fork) cudaEventDestroy(fork);
         cudaFree(d_scenes);
         cudaFree(d_renders);
         cudaFree(d_ns);
@@ -202,6 +236,7 @@ struct BatchCtx {
         cudaFree(d_items);
         cudaFree(d_next);
         cudaFree(d_rays);
+        cudaFree(d_kst);
         cudaFree(d_scratch);
     }
 };
@@ -224,17 +259,19 @@ void batch_forget(const yr_scene *s) {
     }
 }
 
+// relative work of one scene (camera samples x rays per sample)
+static double scene_cost(const BatchCtx &C, uint32_t s) {
+    const Plan &P = C.plans[s];
+    return (double)P.total * (1.0 + P.ns) * (1.0 + P.npath * (double)P.depth * (1.0 + P.ns));
+}
+
 // Items for a tile cap: per scene, tiles of max(1, cap/spp) whole pixels;
 // scenes with the most work per pixel first, so the long items start early.
 static void make_items(const BatchCtx &C, int tile, std::vector<BatchItem> &items) {
     items.clear();
     std::vector<uint32_t> order(C.scenes.size());
     std::iota(order.begin(), order.end(), 0u);
-    auto cost = [&](uint32_t s) {
-        const Plan &P = C.plans[s];
-        const DevRender &R = C.scenes[s]->rdr;
-        return (double)R.spp * (1.0 + P.ns) * (1.0 + P.npath * (double)P.depth * (1.0 + P.ns));
-    };
+    auto cost = [&](uint32_t s) { return scene_cost(C, s) / std::max<double>(1.0, (double)C.plans[s].rpix); };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost(a) > cost(b); });
     for (uint32_t s : order) {
         const DevRender &R = C.scenes[s]->rdr;
@@ -263,9 +300,87 @@ static yr_status ensure(void **p, size_t &have, size_t need) {
     return YR_OK;
 }
 
+// ------------------------------------------------------------ waves schedule
+constexpr size_t kLaneBudget = 1536ull << 20;  // scratch per stream
+
+// Scenes to `n` streams, longest first onto the least loaded stream; one
+// scratch block per stream, sized for its largest wave.
+static yr_status make_lanes(BatchCtx &C, int n) {
+    if (C.lanes_n == n) return YR_OK;
+    C.drop_graph();
+    C.drop_lanes();
+    C.lanes.resize(n);
+    std::vector<uint32_t> order(C.scenes.size());
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return scene_cost(C, a) > scene_cost(C, b); });
+    std::vector<double> load(n, 0.0);
+    for (uint32_t s : order) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        C.lanes[k].scenes.push_back(s);
+        load[k] += scene_cost(C, s);
+    }
+    for (WaveLane &l : C.lanes) {
+        if (cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess)
+            return YR_ERR_CUDA;
+        size_t need = 0;
+        for (uint32_t s : l.scenes) {
+            const Plan &P = C.plans[s];
+            const uint32_t spp = C.scenes[s]->rdr.spp;
+            const uint32_t wcap = std::max(spp, wave_for_budget(P, C.scenes[s]->rdr, kLaneBudget));
+            need = std::max(need, wave_bytes(P, wcap));
+        }
+        if (need && cudaMalloc(&l.scratch, need) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
+        l.bytes = need;
+    }
+    C.lanes_n = n;
+    return YR_OK;
+}
+
+// Capture every scene's render on its stream, forked from and joined back
+// into one capture stream, as one graph.
+static yr_status capture_waves(BatchCtx &C) {
+    C.drop_graph();
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return YR_ERR_CUDA;
+    if (!C.fork && cudaEventCreateWithFlags(&C.fork, cudaEventDisableTiming) != cudaSuccess) return YR_ERR_CUDA;
+    yr_status ret = YR_OK;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return YR_ERR_CUDA;
+    }
+    cudaMemsetAsync(C.d_rays, 0, sizeof(unsigned long long) * 4 * C.scenes.size(), cs);
+    cudaEventRecord(C.fork, cs);
+    for (WaveLane &l : C.lanes) {
+        cudaStreamWaitEvent(l.stream, C.fork, 0);
+        for (uint32_t s : l.scenes) {
+            yr_scene *sc = C.scenes[s];
+            const Plan &P = C.plans[s];
+            const uint32_t wcap = std::max(sc->rdr.spp, wave_for_budget(P, sc->rdr, kLaneBudget));
+            Wave W;
+            std::memset(&W, 0, sizeof(W));
+            assign_wave(P, wcap, l.scratch, W);
+            W.rays = C.d_rays + 4 * (size_t)s;   // per-scene ray totals, outside the shared scratch
+            W.kst = C.d_kst;
+            if (ret == YR_OK) ret = enqueue_render(sc, P, wcap, W, C.outs[s], l.stream);
+        }
+        cudaEventRecord(l.done, l.stream);
+        cudaStreamWaitEvent(cs, l.done, 0);
+    }
+    const cudaError_t ee = cudaStreamEndCapture(cs, &g);
+    if (ret == YR_OK && ee != cudaSuccess) ret = YR_ERR_CUDA;
+    if (ret == YR_OK && cudaGraphInstantiate(&C.graph, g, 0) != cudaSuccess) ret = YR_ERR_CUDA;
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    return ret;
+}
+
+// ------------------------------------------------------------ tiles schedule
 // Upload items, size the scratch, launch (or replay the graph) on `st`.
-static yr_status launch_batch(BatchCtx &C, const BatchConfig &cfg, const std::vector<BatchItem> &items,
-                              cudaStream_t st, bool use_graph, float *ms_out) {
+static yr_status launch_tiles(BatchCtx &C, const BatchConfig &cfg, const std::vector<BatchItem> &items,
+                              cudaStream_t st, bool use_graph) {
     const uint32_t qmax = tile_cap(C, cfg.tile);
     const size_t cta = (wave_bytes(C.pmax, qmax) + 255) / 256 * 256;
     int sms = 148, per_sm = 1;
@@ -281,10 +396,7 @@ static yr_status launch_batch(BatchCtx &C, const BatchConfig &cfg, const std::ve
         C.d_items = nullptr;
         if (cudaMalloc(&C.d_items, sizeof(BatchItem) * items.size()) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
         C.items_cap = items.size();
-        if (C.graph) {
-            cudaGraphExecDestroy(C.graph);
-            C.graph = nullptr;
-        }
+        C.drop_graph();
     }
     if (cudaMemcpyAsync(C.d_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice, st) !=
         cudaSuccess)
@@ -308,14 +420,9 @@ static yr_status launch_batch(BatchCtx &C, const BatchConfig &cfg, const std::ve
         cudaMemsetAsync(C.d_rays, 0, sizeof(unsigned long long) * 4, s);
         kern<<<grid, cfg.block, 0, s>>>(A);
     };
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
     if (use_graph) {
         if (!C.graph || !(C.graph_cfg == cfg) || C.graph_items != A.nitems || C.graph_scratch != C.d_scratch) {
-            if (C.graph) cudaGraphExecDestroy(C.graph);
-            C.graph = nullptr;
+            C.drop_graph();
             cudaStream_t cs;
             cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
             cudaGraph_t g;
@@ -334,39 +441,93 @@ static yr_status launch_batch(BatchCtx &C, const BatchConfig &cfg, const std::ve
     } else {
         record(st);
     }
+    return cudaGetLastError() == cudaSuccess ? YR_OK : YR_ERR_CUDA;
+}
+
+// Run one configuration over all (or the given) items on `st`; device time
+// of the launch in *ms_out when not null.
+static yr_status run_config(BatchCtx &C, const BatchConfig &cfg, const std::vector<BatchItem> *items, cudaStream_t st,
+                            bool use_graph, float *ms_out) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    yr_status ret = YR_OK;
+    if (cfg.mode == YR_BATCH_WAVES) {
+        if ((ret = make_lanes(C, cfg.streams)) == YR_OK && (!C.graph || !(C.graph_cfg == cfg))) {
+            ret = capture_waves(C);
+            C.graph_cfg = cfg;
+        }
+        if (ret == YR_OK && cudaGraphLaunch(C.graph, st) != cudaSuccess) ret = YR_ERR_CUDA;
+    } else {
+        if (C.lanes_n) {  // the graph of the other schedule is stale
+            C.drop_graph();
+            C.drop_lanes();
+        }
+        ret = launch_tiles(C, cfg, items ? *items : C.items, st, use_graph);
+    }
     cudaEventRecord(e1, st);
-    if (cudaGetLastError() != cudaSuccess) return YR_ERR_CUDA;
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (ms_out) *ms_out = ms;
-    return YR_OK;
+    return ret;
 }
 
-// Time every candidate on every 8th item and keep the fastest.
-static yr_status autotune(BatchCtx &C, cudaStream_t st, BatchConfig &best) {
+// Tiles: time every (stack, tile, block) candidate on every 8th item and keep
+// the fastest, then time it on all items.  Waves: time 4 and 16 streams on
+// the whole batch.  Keep the fastest schedule.
+static yr_status autotune(BatchCtx &C, cudaStream_t st, int want_mode, BatchConfig &best) {
+    yr_status r;
     float best_ms = 3.4e38f;
-    const int blocks[2] = {128, 256}, tiles[3] = {256, 512, 1024};
-    for (int stack : kStackOptions) {
-        if (C.max_depth + 2 > stack) continue;
-        for (int tile : tiles)
-            for (int block : blocks) {
-                BatchConfig cfg{block, tile, stack};
-                std::vector<BatchItem> all, sample;
-                make_items(C, tile, all);
-                for (size_t i = 0; i < all.size(); i += 8) sample.push_back(all[i]);
-                float ms = 0.f;
-                yr_status r = launch_batch(C, cfg, sample, st, false, &ms);
-                if (r != YR_OK) return r;
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best = cfg;
+    if (want_mode != YR_BATCH_WAVES) {
+        BatchConfig bt;
+        float bt_ms = 3.4e38f;
+        const int blocks[2] = {128, 256}, tiles[3] = {256, 512, 1024};
+        for (int stack : kStackOptions) {
+            if (C.max_depth + 2 > stack) continue;
+            for (int tile : tiles)
+                for (int block : blocks) {
+                    BatchConfig cfg;
+                    cfg.mode = YR_BATCH_TILES;
+                    cfg.block = block;
+                    cfg.tile = tile;
+                    cfg.stack = stack;
+                    std::vector<BatchItem> all, sample;
+                    make_items(C, tile, all);
+                    for (size_t i = 0; i < all.size(); i += 8) sample.push_back(all[i]);
+                    float ms = 0.f;
+                    if ((r = run_config(C, cfg, &sample, st, false, &ms)) != YR_OK) return r;
+                    if (ms < bt_ms) {
+                        bt_ms = ms;
+                        bt = cfg;
+                    }
                 }
-            }
+        }
+        if (!bt.block) return YR_ERR_UNSUPPORTED;
+        make_items(C, bt.tile, C.items);
+        if ((r = run_config(C, bt, nullptr, st, false, &best_ms)) != YR_OK) return r;
+        best = bt;
     }
-    return best.block ? YR_OK : YR_ERR_UNSUPPORTED;
+    if (want_mode != YR_BATCH_TILES) {
+        const int nmax = (int)std::min<size_t>(C.scenes.size(), 16);
+        for (int n : {std::min(4, nmax), nmax}) {
+            BatchConfig cfg;
+            cfg.mode = YR_BATCH_WAVES;
+            cfg.streams = n;
+            float ms = 0.f;
+            if ((r = run_config(C, cfg, nullptr, st, true, &ms)) != YR_OK) return r;  // capture + first replay
+            if ((r = run_config(C, cfg, nullptr, st, true, &ms)) != YR_OK) return r;  // replay alone
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = cfg;
+            }
+            if (n == nmax) break;
+        }
+    }
+    return best.mode ? YR_OK : YR_ERR_UNSUPPORTED;
 }
 
 }  // namespace yr
@@ -378,6 +539,8 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
     if (!scenes || !outs || count == 0) return YR_ERR_INVALID_ARG;
     for (uint32_t i = 0; i < count; i++)
         if (!scenes[i] || !outs[i] || scenes[i]->device != scenes[0]->device) return YR_ERR_INVALID_ARG;
+    const int want_mode = params ? params->mode : YR_BATCH_AUTO;
+    if (want_mode < YR_BATCH_AUTO || want_mode > YR_BATCH_WAVES) return YR_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g_batch_mu);
     int prev = 0;
     cudaGetDevice(&prev);
@@ -417,6 +580,7 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
             C->pmax.nl = std::max(C->pmax.nl, P.nl);
             C->pmax.depth = std::max(C->pmax.depth, P.depth);
             C->max_depth = std::max(C->max_depth, scenes[i]->max_tree_depth);
+            C->primary += P.total;
             std::memcpy(&ds[i], &scenes[i]->dev, sizeof(DevScene));
             std::memcpy(&dr[i], &scenes[i]->rdr, sizeof(DevRender));
             ns[i] = P.ns;
@@ -427,7 +591,8 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
             cudaMalloc(&C->d_ns, 4 * count) != cudaSuccess || cudaMalloc(&C->d_npath, 4 * count) != cudaSuccess ||
             cudaMalloc(&C->d_outs, sizeof(float *) * count) != cudaSuccess ||
             cudaMalloc(&C->d_next, sizeof(uint32_t)) != cudaSuccess ||
-            cudaMalloc(&C->d_rays, sizeof(unsigned long long) * 4) != cudaSuccess)
+            cudaMalloc(&C->d_rays, sizeof(unsigned long long) * 4 * count) != cudaSuccess ||
+            cudaMalloc(&C->d_kst, sizeof(unsigned long long) * 3 * YR_K_COUNT) != cudaSuccess)
             return done(YR_ERR_OUT_OF_MEMORY);
         cudaMemcpy(C->d_scenes, ds.data(), sizeof(DevScene) * count, cudaMemcpyHostToDevice);
         cudaMemcpy(C->d_renders, dr.data(), sizeof(DevRender) * count, cudaMemcpyHostToDevice);
@@ -442,13 +607,13 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
     if (C.outs.size() != count || !std::equal(C.outs.begin(), C.outs.end(), outs)) {
         C.outs.assign(outs, outs + count);
         cudaMemcpy(C.d_outs, C.outs.data(), sizeof(float *) * count, cudaMemcpyHostToDevice);
+        if (C.lanes_n) C.drop_graph();  // the waves graph holds the image pointers
     }
     BatchConfig cfg;
-    const bool autotuned = !params || params->block_size == 0 || params->queue_tile == 0;
-    if (autotuned) {
-        if (!C.tuned.block && (ret = autotune(C, st, C.tuned)) != YR_OK) return done(ret);
-        cfg = C.tuned;
-    } else {
+    const bool explicit_tiles = params && params->block_size > 0 && params->queue_tile > 0 && want_mode != YR_BATCH_WAVES;
+    const bool explicit_waves = params && want_mode == YR_BATCH_WAVES && params->streams > 0;
+    if (explicit_tiles) {
+        cfg.mode = YR_BATCH_TILES;
         cfg.block = params->block_size;
         cfg.tile = params->queue_tile;
         if (cfg.block % 32 || cfg.block < 32 || cfg.block > 1024 || cfg.tile < 1) return done(YR_ERR_INVALID_ARG);
@@ -458,29 +623,45 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
                 cfg.stack = s;
                 break;
             }
+    } else if (explicit_waves) {
+        cfg.mode = YR_BATCH_WAVES;
+        cfg.streams = std::min<int>(params->streams, (int)count);
+    } else {
+        if (!C.tuned.mode || (want_mode && C.tuned.mode != want_mode)) {
+            BatchConfig t;
+            if ((ret = autotune(C, st, want_mode, t)) != YR_OK) return done(ret);
+            C.tuned = t;
+        }
+        cfg = C.tuned;
     }
-    make_items(C, cfg.tile, C.items);
+    if (cfg.mode == YR_BATCH_TILES) make_items(C, cfg.tile, C.items);
     float ms = 0.f;
-    const bool use_graph = !params || params->use_graph;
-    if ((ret = launch_batch(C, cfg, C.items, st, use_graph, &ms)) != YR_OK) return done(ret);
+    const bool use_graph = !params || params->use_graph || cfg.mode == YR_BATCH_WAVES;
+    if ((ret = run_config(C, cfg, nullptr, st, use_graph, &ms)) != YR_OK) return done(ret);
     // device status words of every scene
     for (yr_scene *sc : C.scenes)
         if ((ret = take_status(sc, st)) != YR_OK) return done(ret);
     if (stats) {
-        unsigned long long r[4] = {0, 0, 0, 0};
-        cudaMemcpy(r, C.d_rays, sizeof(r), cudaMemcpyDeviceToHost);
+        const size_t nr = cfg.mode == YR_BATCH_WAVES ? 4 * (size_t)count : 4;
+        std::vector<unsigned long long> r(nr, 0ull);
+        cudaMemcpy(r.data(), C.d_rays, sizeof(unsigned long long) * nr, cudaMemcpyDeviceToHost);
         std::memset(stats, 0, sizeof(*stats));
-        stats->rays_primary = r[0];
-        stats->rays_shadow = r[1];
-        stats->rays_bounce = r[2];
+        for (size_t i = 0; i < nr; i += 4) {
+            stats->rays_primary += r[i];
+            stats->rays_shadow += r[i + 1];
+            stats->rays_bounce += r[i + 2];
+        }
+        if (cfg.mode == YR_BATCH_WAVES) stats->rays_primary = C.primary;
         stats->ms = ms;
         stats->kernel_ms[YR_K_OTHER] = ms;
         stats->kernel_launches[YR_K_OTHER] = 1;
     }
     if (params) {  // report the configuration used
+        params->mode = cfg.mode;
         params->block_size = cfg.block;
         params->queue_tile = cfg.tile;
-        params->stack_entries = cfg.stack;
+        params->stack_entries = cfg.mode == YR_BATCH_WAVES ? kKdStackCap : cfg.stack;
+        params->streams = cfg.streams;
     }
     return done(YR_OK);
 }

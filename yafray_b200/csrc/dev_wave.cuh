@@ -823,6 +823,11 @@ __host__ __device__ inline void assign_wave(const Plan &P, uint32_t wcap, char *
     W.npath = P.npath;
 }
 
+// Enqueue every launch of one render of `scene` on `st` (no synchronization,
+// capturable): waves of `wcap` camera samples through the scratch that
+// `W` points to (render.cu).
+yr_status enqueue_render(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st);
+
 // Largest wave (whole pixels) whose scratch fits in `budget` bytes.
 inline uint32_t wave_for_budget(const Plan &P, const DevRender &R, size_t budget) {
     uint64_t lo = 0, hi = P.rpix;

@@ -41,37 +41,13 @@ static yr_status scratch(yr_scene *s, int i, size_t bytes, void **p) {
     return YR_OK;
 }
 
-// All waves of one render on `st`.  `out` is the device RGBA image.
-// With `events` false no CUDA event is created (stats->ms and the kernel
-// times stay 0).
-static yr_status run_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out,
-                           yr_render_stats *stats, cudaStream_t st, bool events) {
+// The launches of one render (all waves) on `st`, without any
+// synchronization; `timed(cls, launch)` wraps each kernel launch.
+template <class Timed>
+static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st,
+                         Timed &&timed) {
     DevRender &R = scene->rdr;
     W.out = out;
-    const bool kstats = events && stats && stats->want_kernel_stats;
-    double kms[YR_K_COUNT] = {0};
-    uint32_t klaunch[YR_K_COUNT] = {0};
-    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> kev;
-    auto timed = [&](int cls, auto &&launch) {
-        klaunch[cls]++;
-        if (!kstats) {
-            launch();
-            return;
-        }
-        cudaEvent_t a, b;
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
-        cudaEventRecord(a, st);
-        launch();
-        cudaEventRecord(b, st);
-        kev.push_back({cls, {a, b}});
-    };
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (events) {
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, st);
-    }
     cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
     cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
     // pixels outside the region are written as 0 (scene.cc:773)
@@ -116,6 +92,45 @@ static yr_status run_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &
             timed(YR_K_OTHER, [&] { k_finish<<<gf, kBlock, 0, st>>>(R, W); });
         }
     }
+}
+
+yr_status enqueue_render(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st) {
+    launch_waves(scene, P, wcap, W, out, st, [](int, auto &&launch) { launch(); });
+    return cudaGetLastError() == cudaSuccess ? YR_OK : YR_ERR_CUDA;
+}
+
+// All waves of one render on `st`.  `out` is the device RGBA image.
+// With `events` false no CUDA event is created (stats->ms and the kernel
+// times stay 0).
+static yr_status run_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out,
+                           yr_render_stats *stats, cudaStream_t st, bool events) {
+    DevRender &R = scene->rdr;
+    W.out = out;
+    const bool kstats = events && stats && stats->want_kernel_stats;
+    double kms[YR_K_COUNT] = {0};
+    uint32_t klaunch[YR_K_COUNT] = {0};
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> kev;
+    auto timed = [&](int cls, auto &&launch) {
+        klaunch[cls]++;
+        if (!kstats) {
+            launch();
+            return;
+        }
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, st);
+        launch();
+        cudaEventRecord(b, st);
+        kev.push_back({cls, {a, b}});
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (events) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, st);
+    }
+    launch_waves(scene, P, wcap, W, out, st, timed);
     if (events) cudaEventRecord(e1, st);
     if (cudaGetLastError() != cudaSuccess) return YR_ERR_CUDA;
     yr_status ret = take_status(scene, st);
