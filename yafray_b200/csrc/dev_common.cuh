@@ -94,19 +94,18 @@ struct DevObject {
     float ob[6];        // object bound (meshObject_t::getBound), the object tree's leaf box
 };
 
-struct DevObjNode {     // object tree (geomeTree_t), node 0 = root
-    float bmin[3];
-    int32_t left;       // -1 = leaf
-    float bmax[3];
-    int32_t right;      // child, or object index for a leaf
-};
 
 struct DevScene {
     const float4 *tris;         // 3 per triangle: {a, N.x}, {b, N.y}, {c, N.z}
     const uint2 *nodes;
     const uint32_t *prims;
     const DevObject *objects;
-    const DevObjNode *otree;
+    // object tree (geomeTree_t): per interior node 4 x float4 = left box
+    // (min xyz, max xyz), right box, then the children's codes (>= 0:
+    // interior node, < 0: ~object index) as int bits
+    const float4 *onodes;
+    float otb[6];               // root box
+    int oroot;                  // root code (-1 = ~0: a lone object 0; no tree when notree == 0)
     uint32_t nobjects;
     uint32_t ntris;
     uint32_t nnodes;

@@ -83,8 +83,8 @@ __device__ __forceinline__ bool box_where(const float *bmin, const float *bmax, 
 struct ObjRay {
     V3 from;
     RayR R;
-    float nf[3];   // RN(-from*y)
-    float err[3];  // per-axis error bound of t
+    float nf[3];   // RN(-from*y) with y = 1/d
+    float err[3];  // per-axis error bound of t; +inf where d = 0
     bool exact;
 };
 
@@ -94,43 +94,39 @@ __device__ __forceinline__ ObjRay make_objray(const V3 &from, const RayR &R, flo
     q.R = R;
     q.exact = exact;
     const float f[3] = {from.x, from.y, from.z}, y[3] = {R.inv.x, R.inv.y, R.inv.z};
+    const float d[3] = {R.d.x, R.d.y, R.d.z};
     for (int k = 0; k < 3; k++) {
         q.nf[k] = -f[k] * y[k];
         // |t~ - t| <= 2u|t| + u|f y| (+ rounding) with |t| <= (M + |f|)|y|:
-        // 2^-21 = 8u on (M + 2|f|)|y| leaves a factor of ~2 of headroom
-        q.err[k] = (coord_max + 2.f * fabsf(f[k])) * fabsf(y[k]) * 0x1p-21f;
+        // 2^-21 = 8u on (M + 2|f|)|y| leaves a factor of ~2 of headroom.
+        // d = 0 (y infinite): bound_t::cross skips the axis; with an infinite
+        // bound every t of that axis widens to (-inf, inf) or to NaN, which
+        // fminf / fmaxf ignore, so the axis adds no constraint.
+        q.err[k] = d[k] == 0.f ? __int_as_float(0x7f800000)
+                               : (coord_max + 2.f * fabsf(f[k])) * fabsf(y[k]) * 0x1p-21f;
     }
     return q;
 }
 
+// Conservative crossing test, branch free: the interval is the
+// intersection of the widened per-axis intervals.  bound_t::cross's
+// running form (lmin / lmax initialised to -1, early exits) accepts
+// exactly when max(t_near) <= min(t_far), min(t_far) >= 0 and
+// max(t_near) <= dist; widening every interval keeps every such box.
 __device__ __forceinline__ bool box_where_obj(const float *bmin, const float *bmax, const ObjRay &q, float dist,
                                               float &where) {
     if (q.exact) return box_where(bmin, bmax, q.from, q.R, dist, where);
-    float lmin = -1.f, lmax = -1.f;
-    const float d[3] = {q.R.d.x, q.R.d.y, q.R.d.z}, y[3] = {q.R.inv.x, q.R.inv.y, q.R.inv.z};
-    bool first = true;
+    float lo = -__int_as_float(0x7f800000), hi = __int_as_float(0x7f800000);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        if (d[k] == 0.f) continue;
-        float t1 = __fmaf_rn(bmin[k], y[k], q.nf[k]), t2 = __fmaf_rn(bmax[k], y[k], q.nf[k]);
-        if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
-        t1 -= q.err[k];
-        t2 += q.err[k];
-        if (first) {
-            lmin = t1;
-            lmax = t2;
-            first = false;
-        } else {
-            if (t1 > lmin) lmin = t1;
-            if ((t2 < lmax) || (lmax < 0.f)) lmax = t2;
-        }
-        if ((lmax < 0.f) || (lmin > dist)) return false;
+        const float y = k == 0 ? q.R.inv.x : (k == 1 ? q.R.inv.y : q.R.inv.z);
+        const float t1 = __fmaf_rn(bmin[k], y, q.nf[k]), t2 = __fmaf_rn(bmax[k], y, q.nf[k]);
+        lo = fmaxf(lo, fminf(t1, t2) - q.err[k]);
+        hi = fminf(hi, fmaxf(t1, t2) + q.err[k]);
     }
-    if ((lmin <= lmax) && (lmax >= 0.f) && (lmin <= dist)) {
-        where = (lmin > 0.f) ? lmin : 0.f;
-        return true;
-    }
-    return false;
+    const bool ok = (lo <= hi) && (hi >= 0.f) && (lo <= dist);
+    where = ok ? fmaxf(lo, 0.f) : where;  // untouched on a miss, as box_where
+    return ok;
 }
 
 struct Tri {
@@ -204,7 +200,10 @@ struct KdResult {
 constexpr uint32_t kNodeMask = 0x3fffffffu;
 
 // kdTree_t::Intersect (kdtree.cc:591-727, ANY=false) and IntersectS
-// (kdtree.cc:730-866, ANY=true).  Z is in/out (closest hit only).
+// (kdtree.cc:730-866, ANY=true).  Z is in/out (closest hit only).  Child
+// links and leaf contents were checked against the array sizes when the
+// scene was created, so the walk follows them unchecked.
+
 template <bool ANY>
 __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V3 &from, const RayR &R, float dist,
                                 float &Z, KdResult &res, const KdStack &stk) {
@@ -240,10 +239,6 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             dev_fail(S.status, kDevIterationCap);
             return false;
         }
-        if (curr >= S.nnodes) {
-            dev_fail(S.status, kDevBadTree);
-            return false;
-        }
         uint2 nd = __ldg(S.nodes + curr);
         while ((nd.y & 3u) != 3u) {
             res.nodes++;
@@ -251,10 +246,6 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             const float split = __uint_as_float(nd.x);
             const uint32_t right = nd.y >> 2;
             uint32_t far_child;
-            if (curr + 1 >= S.nnodes || right >= S.nnodes) {
-                dev_fail(S.status, kDevBadTree);
-                return false;
-            }
             if (en_pb[axis] <= split) {
                 if (ex_pb[axis] <= split) {
                     curr = curr + 1;
@@ -292,10 +283,6 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
         const uint32_t np = nd.y >> 2;
         for (uint32_t k = 0; k < np; k++) {
             const uint32_t ti = (np == 1) ? nd.x : __ldg(S.prims + nd.x + k);
-            if (ti >= S.ntris) {
-                dev_fail(S.status, kDevBadTree);
-                return false;
-            }
             res.tests++;
             const Tri tr = load_tri(S.tris, ti);
             float rt;
@@ -332,28 +319,30 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
 // geomeIterator_t (geometree.h:36-157) in its front-to-back mode: yields
 // objects whose bound the ray crosses before `maximun`, nearest entry first.
 struct ObjIter {
-    int2 st[kMaxObjStack];   // (node, bits of the entry distance)  (host checks the tree depth)
+    int2 st[kMaxObjStack];   // (node code, bits of the entry distance)  (host checks the tree depth)
     int sp;
     int current;             // object index or -1
     float maximun;
 
-    __device__ __forceinline__ void down(const DevScene &S, int node, const ObjRay &ray) {
+    __device__ __forceinline__ void down(const DevScene &S, int code, const ObjRay &ray) {
         for (;;) {
-            const DevObjNode nd = S.otree[node];
-            if (nd.left < 0) {
-                current = nd.right;
+            if (code < 0) {
+                current = ~code;
                 return;
             }
-            const DevObjNode L = S.otree[nd.left], R = S.otree[nd.right];
+            const float4 *rec = S.onodes + 4 * (size_t)code;
+            const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
+            const float lmin[3] = {q0.x, q0.y, q0.z}, lmax[3] = {q0.w, q1.x, q1.y};
+            const float rmin[3] = {q1.z, q1.w, q2.x}, rmax[3] = {q2.y, q2.z, q2.w};
             float hl = __int_as_float(0x7f800000), hr = __int_as_float(0x7f800000);
-            const bool hitl = box_where_obj(L.bmin, L.bmax, ray, maximun, hl);
-            const bool hitr = box_where_obj(R.bmin, R.bmax, ray, maximun, hr);
+            const bool hitl = box_where_obj(lmin, lmax, ray, maximun, hl);
+            const bool hitr = box_where_obj(rmin, rmax, ray, maximun, hr);
             if (!hitl && !hitr) {
                 if (sp == 0) {
                     current = -1;
                     return;
                 }
-                node = st[--sp].x;
+                code = st[--sp].x;
                 continue;
             }
             if (sp >= kMaxObjStack) {
@@ -361,12 +350,13 @@ struct ObjIter {
                 current = -1;
                 return;
             }
+            const int lc = __float_as_int(q3.x), rc = __float_as_int(q3.y);
             if (hl < hr) {
-                if (hitr) st[sp++] = make_int2(nd.right, __float_as_int(hr));
-                node = nd.left;
+                if (hitr) st[sp++] = make_int2(rc, __float_as_int(hr));
+                code = lc;
             } else {
-                if (hitl) st[sp++] = make_int2(nd.left, __float_as_int(hl));
-                node = nd.right;
+                if (hitl) st[sp++] = make_int2(lc, __float_as_int(hl));
+                code = rc;
             }
         }
     }
@@ -376,9 +366,8 @@ struct ObjIter {
         sp = 0;
         current = -1;
         if (S.notree == 0) return;
-        const DevObjNode r = S.otree[0];
         float w = 0.f;
-        if (box_where_obj(r.bmin, r.bmax, ray, maximun, w)) down(S, 0, ray);
+        if (box_where_obj(S.otb, S.otb + 3, ray, maximun, w)) down(S, S.oroot, ray);
     }
 
     __device__ __forceinline__ void next(const DevScene &S, const ObjRay &ray) {

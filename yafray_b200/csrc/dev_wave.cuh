@@ -11,6 +11,9 @@
 namespace yr {
 
 constexpr int kBlock = 128;
+#ifndef YR_TRACE_MINB
+#define YR_TRACE_MINB 10  // minimum resident blocks per SM for the traversal kernels (48 registers)
+#endif
 
 enum SlotFlag : uint8_t { kSlotNone = 0, kSlotLit = 1, kSlotShadowed = 2, kSlotPending = 3 };
 
@@ -153,7 +156,7 @@ __device__ __forceinline__ void st_primary(const DevScene &S, const DevRender &R
 }
 
 #ifdef YR_WAVE_KERNELS
-static __global__ void __launch_bounds__(kBlock) k_primary(DevScene S, DevRender R, Wave W) {
+static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_primary(DevScene S, DevRender R, Wave W) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
@@ -463,7 +466,7 @@ __device__ __forceinline__ void st_trace_shadow(const DevScene &S, const Wave &W
 }
 
 #ifdef YR_WAVE_KERNELS
-static __global__ void __launch_bounds__(kBlock) k_trace_shadow_q(DevScene S, Wave W, float self_bias) {
+static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q(DevScene S, Wave W, float self_bias) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
@@ -510,7 +513,7 @@ __device__ __forceinline__ void st_trace_bounce(const DevScene &S, const Wave &W
 }
 
 #ifdef YR_WAVE_KERNELS
-static __global__ void __launch_bounds__(kBlock) k_trace_bounce(DevScene S, Wave W) {
+static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_bounce(DevScene S, Wave W) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
     const KdStack stk{stk_nt, stk_split, kKdStackCap};

@@ -42,6 +42,24 @@ yr_status dev_upload(yr_scene *s, const T *host, size_t count, T **out) {
     return YR_OK;
 }
 
+// Child links, leaf triangles and prim-list ranges of a flattened tree.
+bool valid_tree(const std::vector<uint2> &nodes, const std::vector<uint32_t> &prims, size_t ntris) {
+    const size_t n = nodes.size();
+    for (size_t i = 0; i < n; i++) {
+        const uint32_t f = nodes[i].y, w = nodes[i].x;
+        if ((f & 3u) != 3u) {
+            if (i + 1 >= n || (f >> 2) >= n) return false;
+        } else {
+            const uint32_t np = f >> 2;
+            if (np == 1 && w >= ntris) return false;
+            if (np > 1 && ((size_t)w + np > prims.size())) return false;
+        }
+    }
+    for (uint32_t p : prims)
+        if (p >= ntris) return false;
+    return true;
+}
+
 }  // namespace
 
 void make_shader(const yr_shader_desc &d, DevShader &o) {
@@ -411,6 +429,12 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     build_object_tree(obounds, otree);
     // traversal state is sized for these limits (kd stack: depth + 2 exits)
     if (nodes.size() >= kNodeMask) return fail(YR_ERR_TOO_LARGE);
+    // every index the device walk follows stays inside its array (the walk
+    // itself only checks the stack and an iteration cap)
+    if (!valid_tree(nodes, prims, total_tris) || !valid_tree(sh_nodes, sh_prims, total_tris))
+        return fail(YR_ERR_BAD_TREE);
+    for (const DevObject &o : objects)
+        if (o.ntris && o.root >= nodes.size()) return fail(YR_ERR_BAD_TREE);
     if (s->max_tree_depth + 2 > kKdStackCap) return fail(YR_ERR_TOO_LARGE);
     {
         int depth = 0;
@@ -433,8 +457,34 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     const uint2 *d_nodes;
     const uint32_t *d_prims, *d_tri_shader;
     const DevObject *d_objects;
-    const DevObjNode *d_otree;
-    static_assert(sizeof(ObjNode) == sizeof(DevObjNode), "object node layout");
+    // object tree for the device: one 64-byte record per interior node
+    // holding both children's boxes and codes (>= 0: interior record,
+    // < 0: ~object), so that a step of the walk is one dependent load
+    std::vector<float4> onodes;
+    int oroot = -1;
+    if (!otree.empty()) {
+        std::vector<int> rec(otree.size(), -1);
+        int nrec = 0;
+        for (size_t n = 0; n < otree.size(); n++)
+            if (otree[n].left >= 0) rec[n] = nrec++;
+        auto code = [&](int n) { return otree[n].left >= 0 ? rec[n] : ~otree[n].right; };
+        onodes.resize(4 * (size_t)nrec);
+        for (size_t n = 0; n < otree.size(); n++) {
+            if (otree[n].left < 0) continue;
+            const ObjNode &L = otree[otree[n].left], &R = otree[otree[n].right];
+            float4 *o = &onodes[4 * (size_t)rec[n]];
+            o[0] = make_float4(L.bmin[0], L.bmin[1], L.bmin[2], L.bmax[0]);
+            o[1] = make_float4(L.bmax[1], L.bmax[2], R.bmin[0], R.bmin[1]);
+            o[2] = make_float4(R.bmin[2], R.bmax[0], R.bmax[1], R.bmax[2]);
+            const int lc = code(otree[n].left), rc = code(otree[n].right);
+            float lf, rf;
+            std::memcpy(&lf, &lc, 4);
+            std::memcpy(&rf, &rc, 4);
+            o[3] = make_float4(lf, rf, 0.f, 0.f);
+        }
+        oroot = code(0);
+    }
+    const float4 *d_onodes = nullptr;
     if ((st = dev_upload(s, tris.data(), tris.size(), (float4 **)&d_tris)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, nodes.data(), nodes.size(), (uint2 **)&d_nodes)) != YR_OK) return fail(st);
     if (!prims.empty() && (st = dev_upload(s, prims.data(), prims.size(), (uint32_t **)&d_prims)) != YR_OK)
@@ -443,8 +493,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     if ((st = dev_upload(s, tri_shader.data(), tri_shader.size(), (uint32_t **)&d_tri_shader)) != YR_OK)
         return fail(st);
     if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
-    if ((st = dev_upload(s, (const DevObjNode *)otree.data(), otree.size(), (DevObjNode **)&d_otree)) != YR_OK)
-        return fail(st);
+    if ((st = dev_upload(s, onodes.data(), onodes.size(), (float4 **)&d_onodes)) != YR_OK) return fail(st);
     const uint2 *d_sh_nodes = nullptr;
     const uint32_t *d_sh_prims = nullptr, *d_tri_obj = nullptr;
     if ((st = dev_upload(s, sh_nodes.data(), sh_nodes.size(), (uint2 **)&d_sh_nodes)) != YR_OK) return fail(st);
@@ -459,7 +508,12 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.nodes = d_nodes;
     D.prims = d_prims;
     D.objects = d_objects;
-    D.otree = d_otree;
+    D.onodes = d_onodes;
+    D.oroot = oroot;
+    if (!otree.empty()) {
+        std::memcpy(D.otb, otree[0].bmin, 12);
+        std::memcpy(D.otb + 3, otree[0].bmax, 12);
+    }
     D.nobjects = desc->nobjects;
     D.ntris = (uint32_t)total_tris;
     D.nnodes = (uint32_t)nodes.size();
