@@ -208,10 +208,12 @@ typedef struct yr_render_params {
  *   (scene_t::isShadowed order); the answers are identical, the walk
  *   differs.  Built at scene creation only when requested.
  * YR_RENDER_EXACT_ORDER: evaluate every object-tree slab test exactly as
- *   bound_t::cross does, so that objects are visited in the reference's
- *   order and node counts match it; by default the object tree uses a
- *   conservative reciprocal-multiply slab test (same hits except between
- *   exactly equidistant objects; faster). */
+ *   bound_t::cross does and walk the reference's object tree for shadow
+ *   rays too, so that objects are visited in the reference's order and node
+ *   counts match it; by default the object tree uses a conservative
+ *   reciprocal-multiply slab test (same hits except between exactly
+ *   equidistant objects) and shadow rays walk an SAH BVH over the shadow
+ *   casters (same answers; faster). */
 #define YR_RENDER_SHADOW_TREE 1u
 #define YR_RENDER_EXACT_ORDER 2u
 

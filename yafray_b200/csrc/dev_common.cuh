@@ -106,6 +106,12 @@ struct DevScene {
     const float4 *onodes;
     float otb[6];               // root box
     int oroot;                  // root code (-1 = ~0: a lone object 0; no tree when notree == 0)
+    // SAH BVH over the shadow-casting objects (same record format), used by
+    // shadow rays, whose answer does not depend on the visiting order
+    const float4 *sonodes;
+    float sotb[6];
+    int soroot;
+    uint32_t nsotree;
     uint32_t nobjects;
     uint32_t ntris;
     uint32_t nnodes;

@@ -323,6 +323,10 @@ struct ObjIter {
     int sp;
     int current;             // object index or -1
     float maximun;
+    const float4 *recs;      // interior records of the tree walked
+#ifdef YR_COUNT_OBJ
+    uint32_t steps = 0;      // interior records loaded (instrumented builds only)
+#endif
 
     __device__ __forceinline__ void down(const DevScene &S, int code, const ObjRay &ray) {
         for (;;) {
@@ -330,7 +334,10 @@ struct ObjIter {
                 current = ~code;
                 return;
             }
-            const float4 *rec = S.onodes + 4 * (size_t)code;
+            const float4 *rec = recs + 4 * (size_t)code;
+#ifdef YR_COUNT_OBJ
+            steps++;
+#endif
             const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
             const float lmin[3] = {q0.x, q0.y, q0.z}, lmax[3] = {q0.w, q1.x, q1.y};
             const float rmin[3] = {q1.z, q1.w, q2.x}, rmax[3] = {q2.y, q2.z, q2.w};
@@ -361,13 +368,21 @@ struct ObjIter {
         }
     }
 
-    __device__ __forceinline__ void start(const DevScene &S, const ObjRay &ray, float maxd) {
+    // walk the tree given by its records, root box and root code (n = 0: empty)
+    __device__ __forceinline__ void start_tree(const DevScene &S, const float4 *r, const float *rootbox, int root,
+                                               uint32_t n, const ObjRay &ray, float maxd) {
         maximun = maxd;
         sp = 0;
         current = -1;
-        if (S.notree == 0) return;
+        recs = r;
+        if (n == 0) return;
         float w = 0.f;
-        if (box_where_obj(S.otb, S.otb + 3, ray, maximun, w)) down(S, S.oroot, ray);
+        if (box_where_obj(rootbox, rootbox + 3, ray, maximun, w)) down(S, root, ray);
+    }
+
+    // the scene's object tree (geomeTree_t)
+    __device__ __forceinline__ void start(const DevScene &S, const ObjRay &ray, float maxd) {
+        start_tree(S, S.onodes, S.otb, S.oroot, S.notree, ray, maxd);
     }
 
     __device__ __forceinline__ void next(const DevScene &S, const ObjRay &ray) {
@@ -604,24 +619,83 @@ __device__ inline bool scene_occluded_ref(const DevScene &S, const V3 &p, int ow
             float Z = dist;
             KdResult r{kNone, 0, 0};
             const bool h = kd_trace<true>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
+#ifdef YR_COUNT_OBJ
+            tests += 1;  // objects shot
+            if (h) {
+                nodes += it.steps;
+                return true;
+            }
+#else
             nodes += r.nodes;
             tests += r.tests;
             if (h) return true;
+#endif
         }
         it.next(S, oray);
     }
+#ifdef YR_COUNT_OBJ
+    nodes += it.steps;
+#endif
     return false;
 }
 
-// isShadowed through the shadow-ray tree, or through the object tree in the
-// reference's order when the scene asks for it (yr_render_params.flags)
+// scene_t::isShadowed with the objects found through the SAH BVH over the
+// shadow casters.  The reference's answer is whether some casting object o
+// has (a) a bound that the ray from p2 crosses before dist (the object tree
+// reaches o exactly then: every enclosing box is larger, the slab
+// arithmetic is monotonic) and (b) an IntersectS hit from its origin.  The
+// BVH's conservative walk reaches every object with (a) (and possibly a
+// few more); (b) is the same kd walk; (a) is checked exactly for an
+// object with a hit before it counts.  The answer is therefore the
+// reference's, whatever the order in which objects are reached.
+__device__ inline bool scene_occluded_bvh(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
+                                          float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+    const V3 self = p + dir * self_bias;
+    const V3 p2 = p + dir * kMinRayDist;
+    const RayR ray = make_rayr(dir);
+    const ObjRay oray = make_objray(p2, ray, S.coord_max, false);
+    ObjIter it;
+    it.start_tree(S, S.sonodes, S.sotb, S.soroot, S.nsotree, oray, dist);
+    while (it.current >= 0) {
+        const int o = it.current;
+        const DevObject &obj = S.objects[o];
+        float Z = dist;
+        KdResult r{kNone, 0, 0};
+        const bool h = kd_trace<true>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
+#ifdef YR_COUNT_OBJ
+        tests += 1;  // objects shot
+#else
+        nodes += r.nodes;
+        tests += r.tests;
+#endif
+        if (h) {
+            float w;
+            if (box_where(obj.ob, obj.ob + 3, p2, ray, dist, w)) {
+#ifdef YR_COUNT_OBJ
+                nodes += it.steps;
+#endif
+                return true;
+            }
+        }
+        it.next(S, oray);
+    }
+#ifdef YR_COUNT_OBJ
+    nodes += it.steps;
+#endif
+    return false;
+}
+
+// isShadowed through the shadow-ray tree, through the object tree in the
+// reference's order when the scene asks for exact order, else through the
+// shadow casters' BVH (yr_render_params.flags)
 __device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
                                       float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     if (S.use_sh_tree) {
         if (S.sh_nnodes == 0) return false;  // nothing casts shadows
         return scene_occluded_merged(S, p, own, dir, dist, self_bias, stk, nodes, tests);
     }
-    return scene_occluded_ref(S, p, own, dir, dist, self_bias, stk, nodes, tests);
+    if (S.exact_order) return scene_occluded_ref(S, p, own, dir, dist, self_bias, stk, nodes, tests);
+    return scene_occluded_bvh(S, p, own, dir, dist, self_bias, stk, nodes, tests);
 }
 
 }  // namespace yr

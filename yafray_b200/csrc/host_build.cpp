@@ -822,4 +822,85 @@ void build_object_tree(const std::vector<Box> &object_bounds, std::vector<ObjNod
     }
 }
 
+// ------------------------------------------------------------ SAH BVH
+namespace {
+
+float half_area(const Box &b) {
+    const float dx = b.g[0] - b.a[0], dy = b.g[1] - b.a[1], dz = b.g[2] - b.a[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+void grow(Box &b, const Box &c) {
+    for (int k = 0; k < 3; k++) {
+        b.a[k] = std::min(b.a[k], c.a[k]);
+        b.g[k] = std::max(b.g[k], c.g[k]);
+    }
+}
+
+Box empty_box() {
+    Box b;
+    for (int k = 0; k < 3; k++) {
+        b.a[k] = std::numeric_limits<float>::infinity();
+        b.g[k] = -std::numeric_limits<float>::infinity();
+    }
+    return b;
+}
+
+int sah_node(const std::vector<Box> &bb, std::vector<int> &ids, int lo, int hi, std::vector<ObjNode> &out) {
+    const int me = (int)out.size();
+    out.push_back(ObjNode{});
+    Box all = empty_box();
+    for (int i = lo; i < hi; i++) grow(all, bb[ids[i]]);
+    for (int k = 0; k < 3; k++) {
+        out[me].bmin[k] = all.a[k];
+        out[me].bmax[k] = all.g[k];
+    }
+    if (hi - lo == 1) {
+        out[me].left = -1;
+        out[me].right = ids[lo];
+        return me;
+    }
+    const int n = hi - lo;
+    int best_axis = 0, best_split = lo + n / 2;
+    double best = std::numeric_limits<double>::infinity();
+    std::vector<float> right_area(n);
+    for (int axis = 0; axis < 3; axis++) {
+        auto centre = [&](int id) { return bb[id].a[axis] + bb[id].g[axis]; };
+        std::stable_sort(ids.begin() + lo, ids.begin() + hi, [&](int x, int y) { return centre(x) < centre(y); });
+        Box r = empty_box();
+        for (int i = n - 1; i >= 1; i--) {
+            grow(r, bb[ids[lo + i]]);
+            right_area[i] = half_area(r);
+        }
+        Box l = empty_box();
+        for (int i = 1; i < n; i++) {
+            grow(l, bb[ids[lo + i - 1]]);
+            const double c = (double)half_area(l) * i + (double)right_area[i] * (n - i);
+            if (c < best) {
+                best = c;
+                best_axis = axis;
+                best_split = lo + i;
+            }
+        }
+    }
+    auto centre = [&](int id) { return bb[id].a[best_axis] + bb[id].g[best_axis]; };
+    std::stable_sort(ids.begin() + lo, ids.begin() + hi, [&](int x, int y) { return centre(x) < centre(y); });
+    const int l = sah_node(bb, ids, lo, best_split, out);
+    const int r = sah_node(bb, ids, best_split, hi, out);
+    out[me].left = l;
+    out[me].right = r;
+    return me;
+}
+
+}  // namespace
+
+void build_sah_object_bvh(const std::vector<Box> &object_bounds, const std::vector<int> &ids,
+                          std::vector<ObjNode> &out) {
+    out.clear();
+    if (ids.empty()) return;
+    std::vector<int> work(ids);
+    out.reserve(2 * ids.size());
+    sah_node(object_bounds, work, 0, (int)work.size(), out);
+}
+
 }  // namespace yr

@@ -59,4 +59,12 @@ struct ObjNode {
 // Node 0 is the root.
 void build_object_tree(const std::vector<Box> &object_bounds, std::vector<ObjNode> &out);
 
+// A binary BVH over the boxes of the objects listed in `ids` (surface-area
+// heuristic, full sweep over centroids on each axis), in the same node
+// format; leaves name entries of `ids`' values.  Node 0 is the root.  Not
+// a reference structure: it serves queries whose answer does not depend
+// on the order in which objects are visited.
+void build_sah_object_bvh(const std::vector<Box> &object_bounds, const std::vector<int> &ids,
+                          std::vector<ObjNode> &out);
+
 }  // namespace yr

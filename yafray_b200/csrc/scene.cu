@@ -457,32 +457,58 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     const uint2 *d_nodes;
     const uint32_t *d_prims, *d_tri_shader;
     const DevObject *d_objects;
-    // object tree for the device: one 64-byte record per interior node
+    // object trees for the device: one 64-byte record per interior node
     // holding both children's boxes and codes (>= 0: interior record,
     // < 0: ~object), so that a step of the walk is one dependent load
-    std::vector<float4> onodes;
-    int oroot = -1;
-    if (!otree.empty()) {
-        std::vector<int> rec(otree.size(), -1);
+    auto flatten_objtree = [](const std::vector<ObjNode> &t, std::vector<float4> &recs, int &root) {
+        recs.clear();
+        root = -1;
+        if (t.empty()) return;
+        std::vector<int> rec(t.size(), -1);
         int nrec = 0;
-        for (size_t n = 0; n < otree.size(); n++)
-            if (otree[n].left >= 0) rec[n] = nrec++;
-        auto code = [&](int n) { return otree[n].left >= 0 ? rec[n] : ~otree[n].right; };
-        onodes.resize(4 * (size_t)nrec);
-        for (size_t n = 0; n < otree.size(); n++) {
-            if (otree[n].left < 0) continue;
-            const ObjNode &L = otree[otree[n].left], &R = otree[otree[n].right];
-            float4 *o = &onodes[4 * (size_t)rec[n]];
+        for (size_t n = 0; n < t.size(); n++)
+            if (t[n].left >= 0) rec[n] = nrec++;
+        auto code = [&](int n) { return t[n].left >= 0 ? rec[n] : ~t[n].right; };
+        recs.resize(4 * (size_t)nrec);
+        for (size_t n = 0; n < t.size(); n++) {
+            if (t[n].left < 0) continue;
+            const ObjNode &L = t[t[n].left], &R = t[t[n].right];
+            float4 *o = &recs[4 * (size_t)rec[n]];
             o[0] = make_float4(L.bmin[0], L.bmin[1], L.bmin[2], L.bmax[0]);
             o[1] = make_float4(L.bmax[1], L.bmax[2], R.bmin[0], R.bmin[1]);
             o[2] = make_float4(R.bmin[2], R.bmax[0], R.bmax[1], R.bmax[2]);
-            const int lc = code(otree[n].left), rc = code(otree[n].right);
+            const int lc = code(t[n].left), rc = code(t[n].right);
             float lf, rf;
             std::memcpy(&lf, &lc, 4);
             std::memcpy(&rf, &rc, 4);
             o[3] = make_float4(lf, rf, 0.f, 0.f);
         }
-        oroot = code(0);
+        root = code(0);
+    };
+    std::vector<float4> onodes, sonodes;
+    int oroot = -1, soroot = -1;
+    flatten_objtree(otree, onodes, oroot);
+    // shadow rays: an SAH BVH over the objects that cast shadows
+    std::vector<ObjNode> sotree;
+    {
+        std::vector<int> casters;
+        for (uint32_t o = 0; o < desc->nobjects; o++)
+            if (objects[o].flags & 1u) casters.push_back((int)o);
+        build_sah_object_bvh(obounds, casters, sotree);
+        int depth = 0;
+        std::vector<std::pair<int, int>> stk;
+        if (!sotree.empty()) stk.push_back({0, 0});
+        while (!stk.empty()) {
+            auto [n, d] = stk.back();
+            stk.pop_back();
+            depth = std::max(depth, d);
+            if (sotree[n].left >= 0) {
+                stk.push_back({sotree[n].left, d + 1});
+                stk.push_back({sotree[n].right, d + 1});
+            }
+        }
+        if (depth > kMaxObjStack) return fail(YR_ERR_UNSUPPORTED);
+        flatten_objtree(sotree, sonodes, soroot);
     }
     const float4 *d_onodes = nullptr;
     if ((st = dev_upload(s, tris.data(), tris.size(), (float4 **)&d_tris)) != YR_OK) return fail(st);
@@ -494,6 +520,8 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         return fail(st);
     if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, onodes.data(), onodes.size(), (float4 **)&d_onodes)) != YR_OK) return fail(st);
+    const float4 *d_sonodes = nullptr;
+    if ((st = dev_upload(s, sonodes.data(), sonodes.size(), (float4 **)&d_sonodes)) != YR_OK) return fail(st);
     const uint2 *d_sh_nodes = nullptr;
     const uint32_t *d_sh_prims = nullptr, *d_tri_obj = nullptr;
     if ((st = dev_upload(s, sh_nodes.data(), sh_nodes.size(), (uint2 **)&d_sh_nodes)) != YR_OK) return fail(st);
@@ -510,6 +538,13 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.objects = d_objects;
     D.onodes = d_onodes;
     D.oroot = oroot;
+    D.sonodes = d_sonodes;
+    D.soroot = soroot;
+    D.nsotree = (uint32_t)sotree.size();
+    if (!sotree.empty()) {
+        std::memcpy(D.sotb, sotree[0].bmin, 12);
+        std::memcpy(D.sotb + 3, sotree[0].bmax, 12);
+    }
     if (!otree.empty()) {
         std::memcpy(D.otb, otree[0].bmin, 12);
         std::memcpy(D.otb + 3, otree[0].bmax, 12);
