@@ -266,6 +266,76 @@ def run_diff(args, api, torch, local, fd_params=16):
     }))
 
 
+def run_inverse(args, api, torch, local):
+    """Batched inverse problems: `inverse_count` scenes (UV sphere of 20k-500k
+    triangles with an fBm-modulated albedo - 6 octaves, lacunarity 2, gain
+    0.5, size U(1,8) - on a plane, one area light; 256x256, 32 spp).  Target
+    images come from hidden parameters (every parameter scaled by U(0.7,1.3)).
+    Adam (lr 1e-2) runs `inverse_steps` steps per problem from the scene's
+    own parameters, once through yr_backward_batch (all problems' forward +
+    adjoint as one CUDA graph per step) and once through yr_render +
+    yr_backward per scene.  Reports the parameter error (over parameters
+    with a non-zero gradient at the start) and the wall time of both."""
+    from yafray_b200 import optim
+    scs = scenes.config_diffnoise(count=args.inverse_count)
+    t0 = time.perf_counter()
+    dss = [api.DeviceScene(sc, device=local) for sc in scs]
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(77)
+    start, hidden, targets = [], [], []
+    for d in dss:
+        th = d.params_get()
+        hd = (th * rng.uniform(0.7, 1.3, th.size)).astype(np.float32)
+        d.params_set(hd)
+        t = torch.empty((d.sc.resy, d.sc.resx, 4), dtype=torch.float32, device="cuda")
+        d.render_into(t.data_ptr())
+        targets.append(t)
+        d.params_set(th)
+        start.append(th)
+        hidden.append(hd)
+    # identifiable parameters: non-zero gradient at the start
+    ident = []
+    for d, t in zip(dss, targets):
+        img = torch.empty_like(t)
+        d.render_into(img.data_ptr())
+        g = torch.zeros(max(1, d.param_count()), dtype=torch.float32, device="cuda")
+        d.backward(img.data_ptr(), t.data_ptr(), g.data_ptr())
+        ident.append(g.cpu().numpy()[:d.param_count()] != 0)
+    rays_per_step = 0
+    for d in dss:
+        st = d.render_into(torch.empty((d.sc.resy, d.sc.resx, 4), device="cuda").data_ptr())
+        rays_per_step += 2 * (st.rays_primary + st.rays_shadow + st.rays_bounce)  # forward + adjoint recompute
+    res = {}
+    for mode in ("batched", "plain"):
+        for d, th in zip(dss, start):
+            d.params_set(th)
+        params, hist, secs = optim.fit(dss, targets, steps=args.inverse_steps, lr=1e-2, batched=(mode == "batched"))
+        errs = []
+        for x, th, hd, m in zip(params, start, hidden, ident):
+            e0 = np.linalg.norm((th - hd)[m])
+            errs.append(float(np.linalg.norm((x - hd)[m]) / e0) if e0 > 0 else 0.0)
+        res[mode] = {"seconds": secs, "ms_per_step": 1000 * secs / args.inverse_steps,
+                     "param_err_rel_median": float(np.median(errs)), "param_err_rel_max": float(np.max(errs)),
+                     "loss_ratio_median": float(np.median(hist[-1] / hist[0]))}
+    b = res["batched"]
+    value = rays_per_step * args.inverse_steps / b["seconds"] / 1e6
+    ntris = sum(int(d.info().ntriangles) for d in dss)
+    for d in dss:
+        d.close()
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.inverse_steps,
+        "warmup": 0, "ms_per_step": b["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": f"inverse: {len(dss)} problems, {ntris:,} triangles, 256x256, 32 spp, fBm albedo, "
+                               f"Adam lr 1e-2 x {args.inverse_steps} steps", "scene_setup_s": round(setup_s, 2)},
+        "batched": b, "plain_gpu": res["plain"],
+        "speedup_vs_plain": res["plain"]["seconds"] / b["seconds"],
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "wall time of the host Adam loop, parameters up and gradients down every step"},
+        "gpu_launches": args.inverse_steps,
+    }))
+
+
 def run_batch(args, api, torch, local, barrier):
     """Uneven batch: `batch_count` independent scenes (1k-200k triangles,
     1-32 objects, 64^2-512^2, 4-64 spp, 1-4 lights, GI 1-3 bounces) rendered
@@ -366,7 +436,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small", "batch", "diff"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "batch", "diff", "inverse"])
+    ap.add_argument("--inverse-count", type=int, default=32, help="problems in the inverse workload")
+    ap.add_argument("--inverse-steps", type=int, default=200, help="Adam steps per problem")
     ap.add_argument("--batch-count", type=int, default=256, help="scenes in the batch workload")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--resx", type=int, default=1920)
@@ -402,6 +474,9 @@ def main():
         return
     if args.config == "diff":
         run_diff(args, api, torch, local)
+        return
+    if args.config == "inverse":
+        run_inverse(args, api, torch, local)
         return
     sc, name = workload(args)
     if args.exact_order:
@@ -487,10 +562,16 @@ def main():
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     alg_bytes = 48.0 * agg["krays"][dom] + 16.0 * agg["knodes"][dom] + 48.0 * agg["ktests"][dom]
     achieved = alg_bytes / (kms[dom] / 1000.0) / 1e9 if kms[dom] > 0 else 0.0
-    traffic = load_traffic().get(abi.KERNEL_CLASSES[dom])
     launches = max(1.0, agg["launch"][dom])
+    # DRAM bytes per ray of this kernel class from an ncu capture of the same
+    # kernel on a smaller frame of the same scene (profiles/ncu_traffic.json),
+    # scaled to the rays of an average launch here
+    tinfo = load_traffic().get(abi.KERNEL_CLASSES[dom])
+    traffic = (float(tinfo["dram_bytes_per_ray"]) * agg["krays"][dom] / launches
+               if isinstance(tinfo, dict) and "dram_bytes_per_ray" in tinfo else None)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic, "kernel": abi.KERNEL_CLASSES[dom],
+                "traffic": traffic, "traffic_source": (tinfo or {}).get("source") if isinstance(tinfo, dict) else None,
+                "kernel": abi.KERNEL_CLASSES[dom],
                 "bytes_per_launch": alg_bytes / launches, "ms_per_launch": kms[dom] / launches,
                 "peak_source": peak_src,
                 "nodes_per_ray": agg["knodes"][dom] / max(1.0, agg["krays"][dom]),

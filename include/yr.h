@@ -426,6 +426,18 @@ YR_API yr_status yr_params_set(yr_scene *scene, const float *params);
 YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, float *dparams,
                              float *loss_out, void *stream);
 
+/* One optimisation step of `count` independent scenes (one device) as one
+ * CUDA graph: scene i is rendered into descs[i].image (device RGBA, written
+ * here), then its gradient goes to dparams[i] (device, yr_param_count
+ * floats) and its loss to losses[i] (host, may be NULL).  The scenes run
+ * as per-scene wavefronts on `streams` concurrent streams (0 = 8).  The
+ * graph is captured on the first call for a list of scenes and buffers and
+ * replayed while they stay the same; parameters changed with
+ * yr_params_set are picked up.  Results equal yr_render + yr_backward per
+ * scene.  (No counterpart in the reference.) */
+YR_API yr_status yr_backward_batch(yr_scene *const *scenes, uint32_t count, const yr_backward_desc *descs,
+                                   float *const *dparams, float *losses, int32_t streams, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

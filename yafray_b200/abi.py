@@ -164,6 +164,8 @@ SIGNATURES = {
     "yr_params_get": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "yr_params_set": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "yr_backward": (C.c_int, [_P, C.POINTER(YrBackwardDesc), _P, C.POINTER(C.c_float), _P]),
+    "yr_backward_batch": (C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(YrBackwardDesc), C.POINTER(_P),
+                                    C.POINTER(C.c_float), C.c_int32, _P]),
 }
 
 _lib = None

@@ -146,3 +146,23 @@ def render_batch(dss: List[DeviceScene], out_ptrs: List[int], block_size: int = 
     st = abi.YrRenderStats()
     abi.check(lib.yr_render_batch(hs, n, outs, C.byref(p), C.byref(st), C.c_void_p(stream)), "yr_render_batch")
     return st, p
+
+
+def backward_batch(dss: List[DeviceScene], image_ptrs: List[int], target_ptrs: List[int], grad_ptrs: List[int],
+                   loss_scale: float = 1.0, streams: int = 0, stream: int = 0) -> np.ndarray:
+    """One optimisation step of several scenes as one CUDA graph
+    (yr_backward_batch): renders scene i into image_ptrs[i], then writes its
+    gradient to grad_ptrs[i].  Returns the losses."""
+    lib = abi.load()
+    n = len(dss)
+    hs = (C.c_void_p * n)(*[d.handle.value for d in dss])
+    descs = (abi.YrBackwardDesc * n)()
+    for i in range(n):
+        descs[i].image = image_ptrs[i]
+        descs[i].target = target_ptrs[i]
+        descs[i].loss_scale = float(loss_scale)
+    gp = (C.c_void_p * n)(*grad_ptrs)
+    losses = np.zeros(n, np.float32)
+    abi.check(lib.yr_backward_batch(hs, n, descs, gp, losses.ctypes.data_as(C.POINTER(C.c_float)), int(streams),
+                                    C.c_void_p(stream)), "yr_backward_batch")
+    return losses

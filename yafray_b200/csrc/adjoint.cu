@@ -25,6 +25,10 @@
 // vector with one atomic per parameter per block.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
 #include <vector>
 
 #define YR_WAVE_KERNELS 1
@@ -348,6 +352,190 @@ static yr_status adj_scratch(yr_scene *s, size_t bytes, void **p) {
 
 int grid_for(uint32_t n, int block);
 
+constexpr size_t kAdjBudget = 1536ull << 20;
+
+// Wave size and scratch bytes of one backward pass.
+struct AdjPlan {
+    Plan P;
+    uint32_t wcap = 0;
+    size_t wave = 0;    // bytes of the wave buffers (256-aligned)
+    size_t bytes = 0;   // wave + adjoint buffers
+};
+
+static yr_status adj_plan(const yr_scene *scene, size_t budget, AdjPlan &A) {
+    const DevRender &R = scene->rdr;
+    yr_status ret = make_plan(scene, A.P);
+    if (ret != YR_OK) return ret;
+    if (R.raydepth <= 0) return YR_ERR_UNSUPPORTED;
+    const Plan &P = A.P;
+    uint64_t lo = 1, hi = P.rpix;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi + 1) / 2;
+        const uint32_t w = (uint32_t)(mid * R.spp);
+        if (wave_bytes(P, w) + adj_bytes(P, w, P.npix) <= budget) lo = mid;
+        else hi = mid - 1;
+    }
+    A.wcap = (uint32_t)(lo * R.spp);
+    A.wave = (wave_bytes(P, A.wcap) + 255) / 256 * 256;
+    A.bytes = A.wave + adj_bytes(P, A.wcap, P.npix);
+    return YR_OK;
+}
+
+// Every launch of one backward pass on `st` (capturable, no synchronization);
+// `blk` holds A.bytes of scratch; the loss is added to *d_loss.
+static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk, const yr_backward_desc *desc,
+                                  float *dparams, double *d_loss, cudaStream_t st) {
+    const DevRender &R = scene->rdr;
+    const Plan &P = AP.P;
+    const uint32_t wcap = AP.wcap;
+    Wave W;
+    std::memset(&W, 0, sizeof(W));
+    assign_wave(P, wcap, blk, W);
+    AdjWave A;
+    std::memset(&A, 0, sizeof(A));
+    assign_adj(P, wcap, P.npix, blk + AP.wave, A);
+    A.grad = dparams;
+    A.sh_pbase = scene->d_sh_pbase;
+    A.li_pidx = scene->d_li_pidx;
+    A.spec_dir = scene->d_spec_dir;
+    A.nparams = scene->nparams;
+    const size_t smem = A.nparams <= kSmemParams ? sizeof(float) * std::max<uint32_t>(A.nparams, 1u) : 0;
+
+    if (scene->nparams) cudaMemsetAsync(dparams, 0, sizeof(float) * scene->nparams, st);
+    cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
+    cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
+    k_adj_loss<<<grid_for(P.npix, kBlock), kBlock, 0, st>>>((const float4 *)desc->image,
+                                                             (const float4 *)desc->target, P.npix, desc->loss_scale,
+                                                             (float4 *)A.gpix, d_loss);
+    const DevScene &D = scene->dev;
+    const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
+    const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
+    for (uint64_t b = 0; b < P.total; b += wcap) {
+        W.base = (uint32_t)b;
+        W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
+        const int g = (int)((W.count + kBlock - 1) / kBlock);
+        cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
+        k_primary<<<g, kBlock, 0, st>>>(D, R, W);
+        k_adj_shade_camera<<<g, kBlock, 0, st>>>(D, R, W, A);
+        k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
+        k_adj_gather_camera<<<g, kBlock, smem, st>>>(R, W, A);
+        if (P.npath > 0) {
+            const size_t nc = (size_t)W.count * P.npath * P.depth;
+            k_adj_clear<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(A, nc);
+            const int gp = (int)(((size_t)W.count * P.npath + kBlock - 1) / kBlock);
+            for (int j = 0; j < R.path_depth; j++) {
+                k_trace_bounce<<<gq, kBlock, 0, st>>>(D, W);
+                cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
+                k_adj_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j, A);
+                k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
+                k_adj_gather_path<<<gp, kBlock, smem, st>>>(R, W, j, R.background, A);
+                std::swap(W.bq, W.bq2);
+                k_swap_queues<<<1, 1, 0, st>>>(W);
+            }
+            k_adj_finish<<<g, kBlock, smem, st>>>(R, W, A);
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? YR_OK : YR_ERR_CUDA;
+}
+
+// ------------------------------------------------ batched forward + backward
+// One optimisation step of many scenes as one CUDA graph: each scene's
+// forward render into its image, then its backward pass, on one of a few
+// concurrent streams (longest scenes first onto the least loaded stream);
+// scenes on one stream share one scratch block.
+struct AdjLane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<uint32_t> scenes;
+    char *scratch = nullptr;
+};
+
+struct AdjBatch {
+    int device = -1;
+    std::vector<yr_scene *> scenes;
+    std::vector<DevScene> h_scenes;
+    std::vector<DevRender> h_renders;
+    std::vector<yr_backward_desc> descs;
+    std::vector<float *> grads;
+    std::vector<AdjPlan> plans;
+    std::vector<uint32_t> fwave;   // forward wave of each scene
+    std::vector<AdjLane> lanes;
+    double *d_loss = nullptr;
+    unsigned long long *d_rays = nullptr;  // 4 per scene
+    unsigned long long *d_kst = nullptr;
+    cudaEvent_t fork = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    ~AdjBatch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (AdjLane &l : lanes) {
+            if (l.stream) cudaStreamDestroy(l.stream);
+            if (l.done) cudaEventDestroy(l.done);
+            cudaFree(l.scratch);
+        }
+        if (fork) cudaEventDestroy(fork);
+        cudaFree(d_loss);
+        cudaFree(d_rays);
+        cudaFree(d_kst);
+    }
+};
+
+static std::mutex g_adj_mu;
+static std::map<std::vector<uintptr_t>, std::unique_ptr<AdjBatch>> g_adj_batches;
+
+void adj_batch_forget(const yr_scene *s) {
+    std::lock_guard<std::mutex> lock(g_adj_mu);
+    for (auto it = g_adj_batches.begin(); it != g_adj_batches.end();) {
+        if (std::find(it->second->scenes.begin(), it->second->scenes.end(), s) != it->second->scenes.end()) {
+            int prev = 0;
+            cudaGetDevice(&prev);
+            cudaSetDevice(it->second->device);
+            it = g_adj_batches.erase(it);
+            cudaSetDevice(prev);
+        } else {
+            ++it;
+        }
+    }
+}
+
+static yr_status adj_batch_capture(AdjBatch &B) {
+    if (B.graph) cudaGraphExecDestroy(B.graph);
+    B.graph = nullptr;
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return YR_ERR_CUDA;
+    yr_status ret = YR_OK;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return YR_ERR_CUDA;
+    }
+    const size_t n = B.scenes.size();
+    cudaMemsetAsync(B.d_loss, 0, sizeof(double) * n, cs);
+    cudaEventRecord(B.fork, cs);
+    for (AdjLane &l : B.lanes) {
+        cudaStreamWaitEvent(l.stream, B.fork, 0);
+        for (uint32_t s : l.scenes) {
+            yr_scene *sc = B.scenes[s];
+            const AdjPlan &A = B.plans[s];
+            Wave W;
+            std::memset(&W, 0, sizeof(W));
+            assign_wave(A.P, B.fwave[s], l.scratch, W);
+            W.rays = B.d_rays + 4 * (size_t)s;
+            W.kst = B.d_kst;
+            if (ret == YR_OK) ret = enqueue_render(sc, A.P, B.fwave[s], W, (float *)B.descs[s].image, l.stream);
+            if (ret == YR_OK)
+                ret = enqueue_backward(sc, A, l.scratch, &B.descs[s], B.grads[s], B.d_loss + s, l.stream);
+        }
+        cudaEventRecord(l.done, l.stream);
+        cudaStreamWaitEvent(cs, l.done, 0);
+    }
+    const cudaError_t ee = cudaStreamEndCapture(cs, &g);
+    if (ret == YR_OK && ee != cudaSuccess) ret = YR_ERR_CUDA;
+    if (ret == YR_OK && cudaGraphInstantiate(&B.graph, g, 0) != cudaSuccess) ret = YR_ERR_CUDA;
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    return ret;
+}
+
 }  // namespace yr
 
 using namespace yr;
@@ -406,77 +594,14 @@ YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, floa
         return e;
     };
     cudaStream_t st = (cudaStream_t)stream;
-    const DevRender &R = scene->rdr;
-    Plan P;
-    yr_status ret = make_plan(scene, P);
+    AdjPlan A;
+    yr_status ret = adj_plan(scene, kAdjBudget, A);
     if (ret != YR_OK) return done(ret);
-    if (R.raydepth <= 0) return done(YR_ERR_UNSUPPORTED);
-    // one block: loss (double, padded), wave buffers, adjoint buffers
-    const size_t budget = 1536ull << 20;
-    uint32_t wcap = std::max<uint32_t>(R.spp, 1u);
-    {
-        uint64_t lo = 1, hi = P.rpix;
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi + 1) / 2;
-            const uint32_t w = (uint32_t)(mid * R.spp);
-            if (wave_bytes(P, w) + adj_bytes(P, w, P.npix) <= budget) lo = mid;
-            else hi = mid - 1;
-        }
-        wcap = (uint32_t)(lo * R.spp);
-    }
-    const size_t wb = (wave_bytes(P, wcap) + 255) / 256 * 256;
     void *blk = nullptr;
-    if ((ret = adj_scratch(scene, 256 + wb + adj_bytes(P, wcap, P.npix), &blk)) != YR_OK) return done(ret);
+    if ((ret = adj_scratch(scene, 256 + A.bytes, &blk)) != YR_OK) return done(ret);
     double *d_loss = (double *)blk;
-    Wave W;
-    std::memset(&W, 0, sizeof(W));
-    assign_wave(P, wcap, (char *)blk + 256, W);
-    AdjWave A;
-    std::memset(&A, 0, sizeof(A));
-    assign_adj(P, wcap, P.npix, (char *)blk + 256 + wb, A);
-    A.grad = dparams;
-    A.sh_pbase = scene->d_sh_pbase;
-    A.li_pidx = scene->d_li_pidx;
-    A.spec_dir = scene->d_spec_dir;
-    A.nparams = scene->nparams;
-    const size_t smem = A.nparams <= kSmemParams ? sizeof(float) * std::max<uint32_t>(A.nparams, 1u) : 0;
-
-    if (scene->nparams) cudaMemsetAsync(dparams, 0, sizeof(float) * scene->nparams, st);
     cudaMemsetAsync(d_loss, 0, sizeof(double), st);
-    cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
-    cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
-    k_adj_loss<<<grid_for(P.npix, kBlock), kBlock, 0, st>>>((const float4 *)desc->image,
-                                                             (const float4 *)desc->target, P.npix, desc->loss_scale,
-                                                             (float4 *)A.gpix, d_loss);
-    const DevScene &D = scene->dev;
-    const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
-    const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
-    for (uint64_t b = 0; b < P.total; b += wcap) {
-        W.base = (uint32_t)b;
-        W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
-        const int g = (int)((W.count + kBlock - 1) / kBlock);
-        cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
-        k_primary<<<g, kBlock, 0, st>>>(D, R, W);
-        k_adj_shade_camera<<<g, kBlock, 0, st>>>(D, R, W, A);
-        k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
-        k_adj_gather_camera<<<g, kBlock, smem, st>>>(R, W, A);
-        if (P.npath > 0) {
-            const size_t nc = (size_t)W.count * P.npath * P.depth;
-            k_adj_clear<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(A, nc);
-            const int gp = (int)(((size_t)W.count * P.npath + kBlock - 1) / kBlock);
-            for (int j = 0; j < R.path_depth; j++) {
-                k_trace_bounce<<<gq, kBlock, 0, st>>>(D, W);
-                cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
-                k_adj_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j, A);
-                k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
-                k_adj_gather_path<<<gp, kBlock, smem, st>>>(R, W, j, R.background, A);
-                std::swap(W.bq, W.bq2);
-                k_swap_queues<<<1, 1, 0, st>>>(W);
-            }
-            k_adj_finish<<<g, kBlock, smem, st>>>(R, W, A);
-        }
-    }
-    if (cudaGetLastError() != cudaSuccess) return done(YR_ERR_CUDA);
+    if ((ret = enqueue_backward(scene, A, (char *)blk + 256, desc, dparams, d_loss, st)) != YR_OK) return done(ret);
     if (loss_out) {
         double l = 0.0;
         if (cudaMemcpyAsync(&l, d_loss, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -485,6 +610,98 @@ YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, floa
         *loss_out = (float)l;
     }
     return done(take_status(scene, st));
+}
+
+YR_API yr_status yr_backward_batch(yr_scene *const *scenes, uint32_t count, const yr_backward_desc *descs,
+                                   float *const *dparams, float *losses, int32_t streams, void *stream) {
+    if (!scenes || !descs || !dparams || count == 0) return YR_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < count; i++)
+        if (!scenes[i] || !descs[i].image || !descs[i].target || (!dparams[i] && scenes[i]->nparams) ||
+            scenes[i]->device != scenes[0]->device)
+            return YR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g_adj_mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    const int device = scenes[0]->device;
+    cudaSetDevice(device);
+    auto done = [&](yr_status e) {
+        cudaSetDevice(prev);
+        return e;
+    };
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nl = std::max(1, std::min<int>(streams > 0 ? streams : 8, (int)count));
+    std::vector<uintptr_t> key{(uintptr_t)device, (uintptr_t)nl};
+    for (uint32_t i = 0; i < count; i++) key.push_back((uintptr_t)scenes[i]);
+    std::unique_ptr<AdjBatch> &slot = g_adj_batches[key];
+    yr_status ret;
+    if (slot)
+        for (uint32_t i = 0; i < count && slot; i++)
+            if (std::memcmp(&slot->h_scenes[i], &scenes[i]->dev, sizeof(DevScene)) ||
+                std::memcmp(&slot->h_renders[i], &scenes[i]->rdr, sizeof(DevRender)))
+                slot.reset();
+    if (!slot) {
+        std::unique_ptr<AdjBatch> B(new AdjBatch);
+        B->device = device;
+        B->scenes.assign(scenes, scenes + count);
+        B->plans.resize(count);
+        B->fwave.resize(count);
+        B->h_scenes.resize(count);
+        B->h_renders.resize(count);
+        std::vector<double> cost(count);
+        for (uint32_t i = 0; i < count; i++) {
+            if ((ret = adj_plan(scenes[i], kAdjBudget, B->plans[i])) != YR_OK) return done(ret);
+            const Plan &P = B->plans[i].P;
+            B->fwave[i] = std::max(scenes[i]->rdr.spp, wave_for_budget(P, scenes[i]->rdr, kAdjBudget));
+            std::memcpy(&B->h_scenes[i], &scenes[i]->dev, sizeof(DevScene));
+            std::memcpy(&B->h_renders[i], &scenes[i]->rdr, sizeof(DevRender));
+            cost[i] = (double)P.total * (1.0 + P.ns) * (1.0 + P.npath * (double)P.depth * (1.0 + P.ns));
+        }
+        if (cudaMalloc(&B->d_loss, sizeof(double) * count) != cudaSuccess ||
+            cudaMalloc(&B->d_rays, sizeof(unsigned long long) * 4 * count) != cudaSuccess ||
+            cudaMalloc(&B->d_kst, sizeof(unsigned long long) * 3 * YR_K_COUNT) != cudaSuccess ||
+            cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming) != cudaSuccess)
+            return done(YR_ERR_OUT_OF_MEMORY);
+        std::vector<uint32_t> order(count);
+        std::iota(order.begin(), order.end(), 0u);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+        B->lanes.resize(nl);
+        std::vector<double> load(nl, 0.0);
+        for (uint32_t s : order) {
+            const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            B->lanes[k].scenes.push_back(s);
+            load[k] += cost[s];
+        }
+        for (AdjLane &l : B->lanes) {
+            if (cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess)
+                return done(YR_ERR_CUDA);
+            size_t need = 0;
+            for (uint32_t s : l.scenes)
+                need = std::max(need, std::max(B->plans[s].bytes, wave_bytes(B->plans[s].P, B->fwave[s])));
+            if (need && cudaMalloc(&l.scratch, need) != cudaSuccess) return done(YR_ERR_OUT_OF_MEMORY);
+        }
+        slot = std::move(B);
+    }
+    AdjBatch &B = *slot;
+    bool same = B.descs.size() == count && B.grads.size() == count;
+    for (uint32_t i = 0; same && i < count; i++)
+        same = B.descs[i].image == descs[i].image && B.descs[i].target == descs[i].target &&
+               B.descs[i].loss_scale == descs[i].loss_scale && B.grads[i] == dparams[i];
+    if (!same || !B.graph) {
+        B.descs.assign(descs, descs + count);
+        B.grads.assign(dparams, dparams + count);
+        if ((ret = adj_batch_capture(B)) != YR_OK) return done(ret);
+    }
+    if (cudaGraphLaunch(B.graph, st) != cudaSuccess) return done(YR_ERR_CUDA);
+    for (yr_scene *sc : B.scenes)
+        if ((ret = take_status(sc, st)) != YR_OK) return done(ret);
+    if (losses) {
+        std::vector<double> l(count);
+        if (cudaMemcpy(l.data(), B.d_loss, sizeof(double) * count, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return done(YR_ERR_CUDA);
+        for (uint32_t i = 0; i < count; i++) losses[i] = (float)l[i];
+    }
+    return done(YR_OK);
 }
 
 }  // extern "C"

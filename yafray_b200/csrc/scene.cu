@@ -664,6 +664,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
 YR_API yr_status yr_scene_destroy(yr_scene *scene) {
     if (!scene) return YR_ERR_INVALID_ARG;
     batch_forget(scene);
+    adj_batch_forget(scene);
     destroy_scene(scene);
     return YR_OK;
 }

@@ -111,6 +111,8 @@ void make_camera(const yr_camera_desc &c, DevCamera &o);
 yr_status upload_params(yr_scene *s);
 // read and clear the device status word (synchronizes `stream`)
 yr_status take_status(yr_scene *s, cudaStream_t stream);
-// drop the cached batch state of every batch that holds `s` (batch.cu)
+// drop the cached batch state of every batch that holds `s` (batch.cu,
+// adjoint.cu)
 void batch_forget(const yr_scene *s);
+void adj_batch_forget(const yr_scene *s);
 }  // namespace yr
