@@ -335,20 +335,6 @@ static void assign_adj(const Plan &P, uint32_t wcap, uint32_t npix, char *base, 
     A.gpix = (const float4 *)ptr[6];
 }
 
-static yr_status adj_scratch(yr_scene *s, size_t bytes, void **p) {
-    constexpr int kSlot = 2;  // 0: render waves, 1: host staging
-    if ((int)s->scratch.size() <= kSlot) s->scratch.resize(kSlot + 1);
-    DevBuf &b = s->scratch[kSlot];
-    if (b.bytes < bytes) {
-        if (b.p) cudaFree(b.p);
-        b.p = nullptr;
-        b.bytes = 0;
-        if (cudaMalloc(&b.p, bytes) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
-        b.bytes = bytes;
-    }
-    *p = b.p;
-    return YR_OK;
-}
 
 int grid_for(uint32_t n, int block);
 
@@ -597,11 +583,12 @@ YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, floa
     AdjPlan A;
     yr_status ret = adj_plan(scene, kAdjBudget, A);
     if (ret != YR_OK) return done(ret);
-    void *blk = nullptr;
-    if ((ret = adj_scratch(scene, 256 + A.bytes, &blk)) != YR_OK) return done(ret);
+    PoolBlock pb(scene->device, st);  // given back (after a stream sync) when this call returns
+    if ((ret = pool_acquire(scene->device, 256 + A.bytes, pb.buf)) != YR_OK) return done(ret);
+    char *blk = (char *)pb.buf.p;
     double *d_loss = (double *)blk;
     cudaMemsetAsync(d_loss, 0, sizeof(double), st);
-    if ((ret = enqueue_backward(scene, A, (char *)blk + 256, desc, dparams, d_loss, st)) != YR_OK) return done(ret);
+    if ((ret = enqueue_backward(scene, A, blk + 256, desc, dparams, d_loss, st)) != YR_OK) return done(ret);
     if (loss_out) {
         double l = 0.0;
         if (cudaMemcpyAsync(&l, d_loss, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

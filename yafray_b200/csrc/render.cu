@@ -236,11 +236,11 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
     if (ret != YR_OK) return done(ret);
     // wave: whole pixels, scratch near 1.5 GB at most
     const uint32_t wcap = std::max(scene->rdr.spp, wave_for_budget(P, scene->rdr, 1536ull << 20));
-    void *block = nullptr;
-    if ((ret = scratch(scene, 0, wave_bytes(P, wcap), &block)) != YR_OK) return done(ret);
+    PoolBlock blk(scene->device, st);  // given back (after a stream sync) when this call returns
+    if ((ret = pool_acquire(scene->device, wave_bytes(P, wcap), blk.buf)) != YR_OK) return done(ret);
     Wave W;
     std::memset(&W, 0, sizeof(W));
-    assign_wave(P, wcap, (char *)block, W);
+    assign_wave(P, wcap, (char *)blk.buf.p, W);
     float *out = rgba;
     if (rgba_on_host) {
         void *ptr = nullptr;

@@ -1,6 +1,8 @@
 // yr_scene_create / yr_scene_destroy: host flattening and device upload.
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <chrono>
 #include <thread>
 #include <cmath>
@@ -61,6 +63,56 @@ bool valid_tree(const std::vector<uint2> &nodes, const std::vector<uint32_t> &pr
 }
 
 }  // namespace
+
+// ------------------------------------------------------------ scratch pool
+static std::mutex g_pool_mu;
+static std::map<int, std::vector<DevBuf>> g_pool_free;
+static std::map<int, int> g_live_scenes;
+
+yr_status pool_acquire(int device, size_t bytes, DevBuf &out) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    std::vector<DevBuf> &fl = g_pool_free[device];
+    int best = -1;
+    for (int i = 0; i < (int)fl.size(); i++)
+        if (fl[i].bytes >= bytes && (best < 0 || fl[i].bytes < fl[best].bytes)) best = i;
+    if (best >= 0) {
+        out = fl[best];
+        fl.erase(fl.begin() + best);
+        return YR_OK;
+    }
+    if (!fl.empty()) {  // replace the largest free block by a larger one
+        auto it = std::max_element(fl.begin(), fl.end(),
+                                   [](const DevBuf &a, const DevBuf &b) { return a.bytes < b.bytes; });
+        cudaFree(it->p);
+        fl.erase(it);
+    }
+    out.bytes = bytes ? bytes : 16;
+    if (cudaMalloc(&out.p, out.bytes) != cudaSuccess) {
+        out = DevBuf{};
+        return YR_ERR_OUT_OF_MEMORY;
+    }
+    return YR_OK;
+}
+
+void pool_release(int device, const DevBuf &b) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (g_live_scenes[device] > 0) {
+        g_pool_free[device].push_back(b);
+    } else {
+        cudaFree(b.p);
+    }
+}
+
+static void pool_scene_count(int device, int delta) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    int &n = g_live_scenes[device];
+    n += delta;
+    if (n <= 0) {
+        n = 0;
+        for (DevBuf &b : g_pool_free[device]) cudaFree(b.p);
+        g_pool_free[device].clear();
+    }
+}
 
 void make_shader(const yr_shader_desc &d, DevShader &o) {
     o.color = c3(d.color[0], d.color[1], d.color[2]);
@@ -236,6 +288,7 @@ static void destroy_scene(yr_scene *s) {
     cudaSetDevice(s->device);
     for (DevBuf &b : s->bufs) cudaFree(b.p);
     for (DevBuf &b : s->scratch) cudaFree(b.p);
+    if (s->pooled) pool_scene_count(s->device, -1);
     if (s->status) cudaFree(s->status);
     if (s->status_host) cudaFreeHost(s->status_host);
     cudaSetDevice(prev);
@@ -656,6 +709,8 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     I.device_bytes = 0;
     for (const DevBuf &b : s->bufs) I.device_bytes += b.bytes;
     I.build_seconds = std::chrono::duration<double>(t1 - t0).count();
+    pool_scene_count(s->device, +1);
+    s->pooled = true;
     cudaSetDevice(prev);
     *out = s;
     return YR_OK;

@@ -92,8 +92,9 @@ struct yr_scene {
     int *status_host = nullptr;     // pinned mirror
     yr::DevShader *d_shaders = nullptr;
     yr::DevLight *d_lights = nullptr;
-    // render scratch (grown on demand)
+    // small per-scene scratch (host staging image), grown on demand
     std::vector<yr::DevBuf> scratch;
+    bool pooled = false;            // counted among the device's live scenes
     // adjoint parameter vector: first index of each shader's and light's
     // parameters; unit specular direction of each shader
     uint32_t nparams = 0;
@@ -111,6 +112,30 @@ void make_camera(const yr_camera_desc &c, DevCamera &o);
 yr_status upload_params(yr_scene *s);
 // read and clear the device status word (synchronizes `stream`)
 yr_status take_status(yr_scene *s, cudaStream_t stream);
+// Render scratch shared by all scenes of a device: a render takes a block
+// for its duration (it synchronizes its stream before it returns) and gives
+// it back, so scenes rendered one after another share one block.  The
+// blocks are freed when the device's last scene is destroyed.
+yr_status pool_acquire(int device, size_t bytes, DevBuf &out);
+void pool_release(int device, const DevBuf &b);
+
+struct PoolBlock {
+    int device;
+    cudaStream_t stream;
+    DevBuf buf;
+    PoolBlock(int d, cudaStream_t s) : device(d), stream(s) {}
+    ~PoolBlock() {
+        if (buf.p) {
+            int cur = 0;
+            cudaGetDevice(&cur);
+            cudaSetDevice(device);
+            cudaStreamSynchronize(stream);  // nothing in flight may still use it
+            pool_release(device, buf);
+            cudaSetDevice(cur);
+        }
+    }
+};
+
 // drop the cached batch state of every batch that holds `s` (batch.cu,
 // adjoint.cu)
 void batch_forget(const yr_scene *s);

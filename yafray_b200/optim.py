@@ -38,13 +38,15 @@ class Adam:
 
 
 def fit(dss: List[api.DeviceScene], targets, steps: int = 200, lr: float = 1e-2, batched: bool = True,
-        streams: int = 0, lower: float = 0.0, loss_scale: Optional[List[float]] = None):
+        streams: int = 0, lower: float = 0.0, loss_scale: Optional[List[float]] = None, masks=None):
     """Run `steps` Adam steps on every scene (each its own problem).
-    targets: device RGBA float tensors (torch), one per scene.  Parameters
-    are kept >= `lower` (colours and powers are non-negative).  Gradients
-    are scaled per scene by 1 / (initial loss) so that one learning rate
-    suits problems of any image size.  Returns (params per scene, loss
-    history [steps, scenes], seconds of the device loop)."""
+    targets: device RGBA float tensors (torch), one per scene.  masks: per
+    scene a boolean array over the parameter vector, True = optimised (None:
+    all).  Parameters are kept >= `lower` (colours and powers are
+    non-negative).  Gradients are scaled per scene by 1 / (initial loss) so
+    that one learning rate suits problems of any image size.  Returns
+    (params per scene, loss history [steps, scenes], seconds of the device
+    loop)."""
     import torch
     n = len(dss)
     imgs = [torch.empty_like(t) for t in targets]
@@ -70,7 +72,10 @@ def fit(dss: List[api.DeviceScene], targets, steps: int = 200, lr: float = 1e-2,
         off = 0
         for i, d in enumerate(dss):
             k = d.param_count()
-            x = opts[i].step(g_host[off:off + k] * scale[i])
+            g = g_host[off:off + k] * scale[i]
+            if masks is not None:
+                g = np.where(masks[i], g, 0.0)
+            x = opts[i].step(g)
             np.maximum(x, lower, out=x)
             d.params_set(x.astype(np.float32))
             off += max(1, k)
