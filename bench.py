@@ -34,7 +34,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-from yafray_b200 import abi, scenes  # noqa: E402
+from yafray_b200 import abi, replicas, scenes  # noqa: E402
 
 METRIC = "Mrays/s"
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "yr_ref_harness")
@@ -528,13 +528,8 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    rays_all = torch.tensor([float(agg["rays"])], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        dist.all_reduce(rays_all, op=dist.ReduceOp.SUM)
-    ms_max = float(t_max.item())
-    value = float(rays_all.item()) / (ms_max / 1000.0) / 1e6
+    ms_max, rays_all = replicas.combine(ms, float(agg["rays"]), device="cuda")
+    value = rays_all / (ms_max / 1000.0) / 1e6
     gpu_launches = int(agg["launch"].sum())
 
     # end to end through the C ABI: per step the shader/light parameters go
@@ -553,12 +548,8 @@ def main():
         e2e_rays += st.rays_primary + st.rays_shadow + st.rays_bounce
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    e2e_r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(e2e_r, op=dist.ReduceOp.SUM)
-    e2e_value = float(e2e_r.item()) / float(e2e_t.item()) / 1e6
+    e2e_t, e2e_r = replicas.combine(e2e_s, float(e2e_rays), device="cuda")
+    e2e_value = e2e_r / e2e_t / 1e6
 
     # roofline of the dominant kernel class: algorithmic bytes per ray =
     # 32 (ray) + 16 (hit / occlusion record) + 16 per node visited (the
