@@ -575,6 +575,7 @@ def main():
                 "traffic": traffic, "traffic_source": (tinfo or {}).get("source") if isinstance(tinfo, dict) else None,
                 "kernel": abi.KERNEL_CLASSES[dom],
                 "bytes_per_launch": alg_bytes / launches, "ms_per_launch": kms[dom] / launches,
+                "rays_per_launch": agg["krays"][dom] / launches,
                 "peak_source": peak_src,
                 "nodes_per_ray": agg["knodes"][dom] / max(1.0, agg["krays"][dom]),
                 "tests_per_ray": agg["ktests"][dom] / max(1.0, agg["krays"][dom])}

@@ -395,7 +395,12 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
                                                              (float4 *)A.gpix, d_loss);
     const DevScene &D = scene->dev;
     const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
-    const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
+#if YR_TRACE_GRID_PERSIST
+    const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q));
+    const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce));
+#else
+    const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock), gb = gq;
+#endif
     for (uint64_t b = 0; b < P.total; b += wcap) {
         W.base = (uint32_t)b;
         W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
@@ -403,6 +408,7 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
         cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
         k_primary<<<g, kBlock, 0, st>>>(D, R, W);
         k_adj_shade_camera<<<g, kBlock, 0, st>>>(D, R, W, A);
+        cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
         k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
         k_adj_gather_camera<<<g, kBlock, smem, st>>>(R, W, A);
         if (P.npath > 0) {
@@ -410,9 +416,11 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
             k_adj_clear<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(A, nc);
             const int gp = (int)(((size_t)W.count * P.npath + kBlock - 1) / kBlock);
             for (int j = 0; j < R.path_depth; j++) {
-                k_trace_bounce<<<gq, kBlock, 0, st>>>(D, W);
+                cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
+                k_trace_bounce<<<gb, kBlock, 0, st>>>(D, W);
                 cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
                 k_adj_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j, A);
+                cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
                 k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
                 k_adj_gather_path<<<gp, kBlock, smem, st>>>(R, W, j, R.background, A);
                 std::swap(W.bq, W.bq2);

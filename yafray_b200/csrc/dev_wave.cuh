@@ -11,6 +11,12 @@
 namespace yr {
 
 constexpr int kBlock = 128;
+#ifndef YR_DYN_FETCH
+#define YR_DYN_FETCH 1  // traversal kernels take 32-ray chunks from a counter instead of a fixed stride
+#endif
+#ifndef YR_TRACE_GRID_PERSIST
+#define YR_TRACE_GRID_PERSIST 1  // traversal grids: one block per resident slot of every SM
+#endif
 #ifndef YR_TRACE_MINB
 #define YR_TRACE_MINB 10  // minimum resident blocks per SM for the traversal kernels (48 registers)
 #endif
@@ -472,10 +478,26 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
     const uint32_t n = W.counters[0];
     uint32_t rays = 0, nodes = 0, tests = 0;
+#if YR_DYN_FETCH
+    // each warp takes the next 32 queue entries until the queue is done, so
+    // warps that drew short rays take more of them (counters[6] starts at 0)
+    for (;;) {
+        uint32_t base = 0;
+        if ((threadIdx.x & 31u) == 0) base = atomicAdd(&W.counters[6], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t q = base + (threadIdx.x & 31u);
+        if (q < n) {
+            st_trace_shadow(S, W, q, self_bias, stk, nodes, tests);
+            rays++;
+        }
+    }
+#else
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         st_trace_shadow(S, W, q, self_bias, stk, nodes, tests);
         rays++;
     }
+#endif
     count_work(W, YR_K_SHADOW, rays, nodes, tests);
 }
 #endif
@@ -519,10 +541,24 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_bounce(D
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
     const uint32_t n = W.counters[1];
     uint32_t rays = 0, nodes = 0, tests = 0;
+#if YR_DYN_FETCH
+    for (;;) {  // as k_trace_shadow_q, on counters[7]
+        uint32_t base = 0;
+        if ((threadIdx.x & 31u) == 0) base = atomicAdd(&W.counters[7], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t q = base + (threadIdx.x & 31u);
+        if (q < n) {
+            st_trace_bounce(S, W, q, stk, nodes, tests);
+            rays++;
+        }
+    }
+#else
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         st_trace_bounce(S, W, q, stk, nodes, tests);
         rays++;
     }
+#endif
     count_work(W, YR_K_BOUNCE, rays, nodes, tests);
 }
 #endif
@@ -824,6 +860,23 @@ __host__ __device__ inline void assign_wave(const Plan &P, uint32_t wcap, char *
     W.kst = (unsigned long long *)ptr[k++];
     W.ns = P.ns;
     W.npath = P.npath;
+}
+
+// Blocks of kBlock threads that fill every SM once for `kernel` (queried
+// once per device and kernel), the grid of the traversal kernels.
+template <class K>
+inline int resident_grid(K kernel) {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int sms = 148, per = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBlock, 0) != cudaSuccess || per < 1) per = 1;
+        cached[dev] = sms * per;
+    }
+    return cached[dev];
 }
 
 // Enqueue every launch of one render of `scene` on `st` (no synchronization,

@@ -57,7 +57,12 @@ static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W,
         // raytrace() returns black at the ray-level cap (scene.cc:204-209)
         cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
     } else {
-        const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
+#if YR_TRACE_GRID_PERSIST
+        const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q));
+        const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce));
+#else
+        const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock), gb = gq;
+#endif
         const DevScene &D = scene->dev;
         const uint32_t npath = P.npath;
         for (uint64_t b = 0; b < P.total; b += wcap) {
@@ -68,6 +73,7 @@ static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W,
             timed(YR_K_PRIMARY, [&] { k_primary<<<g, kBlock, 0, st>>>(D, R, W); });
             timed(YR_K_SHADE_CAMERA, [&] { k_shade_camera<<<g, kBlock, 0, st>>>(D, R, W); });
             timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
+            cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
             timed(YR_K_SHADOW, [&] { k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
             timed(YR_K_GATHER, [&] { k_gather_camera<<<g, kBlock, 0, st>>>(R, W); });
             if (npath > 0) {
@@ -78,10 +84,12 @@ static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W,
                 const int gp = (int)(((size_t)W.count * npath + kBlock - 1) / kBlock);
                 for (int j = 0; j < R.path_depth; j++) {
                     timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 1); });
-                    timed(YR_K_BOUNCE, [&] { k_trace_bounce<<<gq, kBlock, 0, st>>>(D, W); });
+                    cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
+                    timed(YR_K_BOUNCE, [&] { k_trace_bounce<<<gb, kBlock, 0, st>>>(D, W); });
                     cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
                     timed(YR_K_SHADE_PATH, [&] { k_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j); });
                     timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
+                    cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
                     timed(YR_K_SHADOW, [&] { k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
                     timed(YR_K_GATHER, [&] { k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background); });
                     std::swap(W.bq, W.bq2);
