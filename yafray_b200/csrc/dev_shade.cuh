@@ -12,15 +12,8 @@ namespace yr {
 // Halton::setStart(n) followed by Halton::getNext() (mcqmc.h:24-49), i.e.
 // the radical inverse of n+1, as the shipped build evaluates it
 // (fast-math: r = (1 - 1e-10) - value, value = (hh + h) + (value - 1)).
-__device__ __forceinline__ float halton(uint32_t base, uint32_t n) {
-    const double inv = 1.0 / (double)base;
-    double value = 0.0, factor = inv;
-    uint32_t i = n;
-    while (i > 0) {
-        value += (double)(i % base) * factor;
-        i /= base;
-        factor *= inv;
-    }
+// Halton::getNext from the radical inverse `value` of n (mcqmc.h:33-49)
+__device__ __forceinline__ float halton_next(double value, double inv) {
     const double r = (1.0 - 0.0000000001) - value;
     if (inv < r) {
         value = value + inv;
@@ -33,6 +26,47 @@ __device__ __forceinline__ float halton(uint32_t base, uint32_t n) {
         value = (hh + h) + (value - 1.0);
     }
     return (float)value;
+}
+
+// Halton::setStart's radical inverse (mcqmc.h:24-31) for a base known at
+// compile time (the divisions become multiplications)
+template <uint32_t B>
+__device__ __forceinline__ float halton_b(uint32_t n) {
+    constexpr double inv = 1.0 / (double)B;
+    double value = 0.0;
+    if (B == 2) {
+        // every term is a power of two below 2^-32 apart: the sum is exact,
+        // and equals the bit-reversed index times 2^-32
+        value = (double)__brev(n) * 0x1p-32;
+    } else {
+        double factor = inv;
+        uint32_t i = n;
+        while (i > 0) {
+            value += (double)(i % B) * factor;
+            i /= B;
+            factor *= inv;
+        }
+    }
+    return halton_next(value, inv);
+}
+
+__device__ __forceinline__ float halton(uint32_t base, uint32_t n) {
+    switch (base) {
+    case 2: return halton_b<2>(n);
+    case 3: return halton_b<3>(n);
+    case 5: return halton_b<5>(n);
+    case 7: return halton_b<7>(n);
+    default: break;
+    }
+    const double inv = 1.0 / (double)base;
+    double value = 0.0, factor = inv;
+    uint32_t i = n;
+    while (i > 0) {
+        value += (double)(i % base) * factor;
+        i /= base;
+        factor *= inv;
+    }
+    return halton_next(value, inv);
 }
 
 __host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
@@ -219,35 +253,50 @@ __device__ __forceinline__ C3 modulated_color(const DevShader &sh, const V3 &P, 
     return tex * w + (1 - w) * C;
 }
 
-// genericShader_t::fromLight (basicshaders.cc:46-70) with edif = 1.
-// `lkc` is the (modulated) diffuse colour.
-__device__ __forceinline__ C3 from_light(const DevShader &sh, const C3 &lkc, const Surf &sp, const V3 &ldir,
-                                         const C3 &lcol, const V3 &eye) {
-    V3 edir = normalize(eye);
-    const V3 N = face_forward(sp.Ng, sp.N, edir);
-    const float inte = dot(N, ldir);
+// The parts of genericShader_t::fromLight (basicshaders.cc:46-70) that
+// depend only on the shading point and the eye, computed once per vertex:
+// the face-forwarded normal and the reflected eye direction.
+struct LitPre {
+    V3 N;
+    V3 refl;
+    bool spec;   // the shader has a specular colour
+};
+
+__device__ __forceinline__ LitPre lit_pre(const DevShader &sh, const Surf &sp, const V3 &eye) {
+    LitPre L;
+    const V3 edir = normalize(eye);
+    L.N = face_forward(sp.Ng, sp.N, edir);
+    L.refl = reflect(L.N, edir);
+    L.spec = sh.specular.r != 0.f || sh.specular.g != 0.f || sh.specular.b != 0.f;
+    return L;
+}
+
+// genericShader_t::fromLight with edif = 1.  `lkc` is the (modulated)
+// diffuse colour.  Without a specular colour the specular term is +0 for
+// every light direction (its factors are finite and non-negative), so only
+// that +0 is added.
+__device__ __forceinline__ C3 from_light(const DevShader &sh, const C3 &lkc, const LitPre &pre, const V3 &ldir,
+                                         const C3 &lcol) {
+    const float inte = dot(pre.N, ldir);
     if (inte < 0.f) return c3(0.f, 0.f, 0.f);
-    edir = reflect(N, edir);
-    float refle = dot(edir, ldir);
+    const C3 edif_inte = c3(1.f * inte, 1.f * inte, 1.f * inte);
+    if (!pre.spec) return ((edif_inte * lcol) * lkc) + c3(0.f, 0.f, 0.f);
+    float refle = dot(pre.refl, ldir);
     if (refle < 0.f) refle = 0.f;
     else refle = (float)pow((double)refle, (double)sh.hard);
-    const C3 edif_inte = c3(1.f * inte, 1.f * inte, 1.f * inte);
     return ((edif_inte * lcol) * lkc) + (sh.specular * refle) * lcol;
 }
 
 // from_light split into the factor of the diffuse colour (D) and of the
 // specular colour (Sp): from_light = D * lkc + specular * Sp.
-__device__ __forceinline__ void from_light_parts(const DevShader &sh, const Surf &sp, const V3 &ldir,
-                                                 const C3 &lcol, const V3 &eye, C3 &D, C3 &Sp) {
-    V3 edir = normalize(eye);
-    const V3 N = face_forward(sp.Ng, sp.N, edir);
-    const float inte = dot(N, ldir);
+__device__ __forceinline__ void from_light_parts(const DevShader &sh, const LitPre &pre, const V3 &ldir,
+                                                 const C3 &lcol, C3 &D, C3 &Sp) {
+    const float inte = dot(pre.N, ldir);
     if (inte < 0.f) {
         D = Sp = c3(0.f, 0.f, 0.f);
         return;
     }
-    edir = reflect(N, edir);
-    float refle = dot(edir, ldir);
+    float refle = dot(pre.refl, ldir);
     if (refle < 0.f) refle = 0.f;
     else refle = (float)pow((double)refle, (double)sh.hard);
     D = inte * lcol;

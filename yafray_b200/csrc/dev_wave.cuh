@@ -17,6 +17,9 @@ constexpr int kBlock = 128;
 #ifndef YR_TRACE_GRID_PERSIST
 #define YR_TRACE_GRID_PERSIST 1  // traversal grids: one block per resident slot of every SM
 #endif
+#ifndef YR_SHADE_MINB
+#define YR_SHADE_MINB 6  // minimum resident blocks per SM for the shading kernels (80 registers)
+#endif
 #ifndef YR_TRACE_MINB
 #define YR_TRACE_MINB 10  // minimum resident blocks per SM for the traversal kernels (48 registers)
 #endif
@@ -193,7 +196,11 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
         if (ADJ) *lkc_out = lkc;
     }
     V3 N = sp.N;
-    if (active) N = face_forward(sp.Ng, sp.N, normalize(eye));
+    LitPre pre;
+    if (active) {
+        pre = lit_pre(sh, sp, eye);
+        N = pre.N;  // FACE_FORWARD(Ng, N, normalize(eye)), as fromLight forms it
+    }
     uint32_t off = 0;
     for (int k = 0; k < R.nlights; k++) {
         const DevLight L = R.lights[k];
@@ -210,11 +217,11 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                 if (id2 != 0.f) id2 = 1.f / id2;
                 if (ADJ) {
                     C3 D, Sp;
-                    from_light_parts(sh, sp, dir, L.rawc * id2, eye, D, Sp);
+                    from_light_parts(sh, pre, dir, L.rawc * id2, D, Sp);
                     W.slot_c[slot] = make_float4(D.r, D.g, D.b, 0.f);
                     slot_s[slot] = make_float4(Sp.r, Sp.g, Sp.b, 0.f);
                 } else {
-                    const C3 c = from_light(sh, lkc, sp, dir, L.color * id2, eye);
+                    const C3 c = from_light(sh, lkc, pre, dir, L.color * id2);
                     W.slot_c[slot] = make_float4(c.r, c.g, c.b, 0.f);
                 }
                 if (L.cast) {
@@ -268,11 +275,11 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                             ld2 = (ld2 != 0.f) ? (1.f / ld2) : 1.f;
                             if (ADJ) {
                                 C3 D, Sp;
-                                from_light_parts(sh, sp, dir, L.color * ld2, eye, D, Sp);
+                                from_light_parts(sh, pre, dir, L.color * ld2, D, Sp);
                                 W.slot_c[slot] = make_float4(D.r, D.g, D.b, 0.f);
                                 slot_s[slot] = make_float4(Sp.r, Sp.g, Sp.b, 0.f);
                             } else {
-                                const C3 c = from_light(sh, lkc, sp, dir, (L.power * L.color) * ld2, eye);
+                                const C3 c = from_light(sh, lkc, pre, dir, (L.power * L.color) * ld2);
                                 W.slot_c[slot] = make_float4(c.r, c.g, c.b, 0.f);
                             }
                             W.slot_f[slot] = kSlotPending;
@@ -293,12 +300,12 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             V3 Nh = sp.N;
             if (active) {
                 Nh = face_forward(sp.Ng, sp.N, eye);
-                fl = from_light(sh, lkc, sp, Nh, c3(1.f, 1.f, 1.f), eye);
+                fl = from_light(sh, lkc, pre, Nh, c3(1.f, 1.f, 1.f));
                 const float mad = fmaxf(fabsf(fl.r), fmaxf(fabsf(fl.g), fabsf(fl.b)));
                 go = !(mad < 0.05f);
                 if (ADJ) {
                     C3 D, Sp;
-                    from_light_parts(sh, sp, Nh, c3(1.f, 1.f, 1.f), eye, D, Sp);
+                    from_light_parts(sh, pre, Nh, c3(1.f, 1.f, 1.f), D, Sp);
                     aux[vtx * R.nlights + k] = make_float4(D.r, Sp.r, 0.f, go ? 1.f : 0.f);
                 } else {
                     aux[vtx * R.nlights + k] = make_float4(fl.r, fl.g, fl.b, go ? 1.f : 0.f);
@@ -456,7 +463,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
 }
 
 #ifdef YR_WAVE_KERNELS
-static __global__ void __launch_bounds__(kBlock) k_shade_camera(DevScene S, DevRender R, Wave W) {
+static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_shade_camera(DevScene S, DevRender R, Wave W) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= W.count && (i & ~31u) >= W.count) return;  // whole warps past the end leave
     st_shade_camera(S, R, W, i);
@@ -625,7 +632,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
 }
 
 #ifdef YR_WAVE_KERNELS
-static __global__ void __launch_bounds__(kBlock) k_shade_path(DevScene S, DevRender R, Wave W, int j) {
+static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_shade_path(DevScene S, DevRender R, Wave W, int j) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = W.counters[1];
     if (q >= n && (q & ~31u) >= n) return;
