@@ -204,31 +204,32 @@ constexpr uint32_t kNodeMask = 0x3fffffffu;
 // links and leaf contents were checked against the array sizes when the
 // scene was created, so the walk follows them unchecked.
 
+__device__ __forceinline__ float sel3(int a, float v0, float v1, float v2) {
+    return a == 0 ? v0 : (a == 1 ? v1 : v2);
+}
+
 template <bool ANY>
 __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V3 &from, const RayR &R, float dist,
                                 float &Z, KdResult &res, const KdStack &stk) {
     float a, b;
     if (!box_enter_leave(obj.tb, obj.tb + 3, from, R, dist, a, b)) return false;
     const V3 &ray = R.d;
-    const float inv[3] = {R.inv.x, R.inv.y, R.inv.z};
-    const float fr[3] = {from.x, from.y, from.z};
-    const float rr[3] = {ray.x, ray.y, ray.z};
+    const float f0 = from.x, f1 = from.y, f2 = from.z, r0 = ray.x, r1 = ray.y, r2 = ray.z;
     bool hit = false;
     uint32_t curr = obj.root;
-    float en_t = a, en_pb[3];
+    // entry and exit points; a coordinate off the split axis is always
+    // from + t*ray, computed for every axis and replaced on the split axis
+    float en_t = a, en0, en1, en2;
     if (a >= 0.f) {
-        en_pb[0] = fr[0] + a * rr[0];
-        en_pb[1] = fr[1] + a * rr[1];
-        en_pb[2] = fr[2] + a * rr[2];
+        en0 = f0 + a * r0;
+        en1 = f1 + a * r1;
+        en2 = f2 + a * r2;
     } else {
-        en_pb[0] = fr[0];
-        en_pb[1] = fr[1];
-        en_pb[2] = fr[2];
+        en0 = f0;
+        en1 = f1;
+        en2 = f2;
     }
-    float ex_t = b, ex_pb[3];
-    ex_pb[0] = fr[0] + b * rr[0];
-    ex_pb[1] = fr[1] + b * rr[1];
-    ex_pb[2] = fr[2] + b * rr[2];
+    float ex_t = b, ex0 = f0 + b * r0, ex1 = f1 + b * r1, ex2 = f2 + b * r2;
     // stack[0] = initial exit (no node); sp = number of exits on the stack
     stk.nt[0] = make_uint2(kNodeMask | (3u << 30), __float_as_uint(b));
     int sp = 1;
@@ -246,8 +247,8 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             const float split = __uint_as_float(nd.x);
             const uint32_t right = nd.y >> 2;
             uint32_t far_child;
-            if (en_pb[axis] <= split) {
-                if (ex_pb[axis] <= split) {
+            if (sel3(axis, en0, en1, en2) <= split) {
+                if (sel3(axis, ex0, ex1, ex2) <= split) {
                     curr = curr + 1;
                     nd = __ldg(S.nodes + curr);
                     continue;
@@ -255,7 +256,7 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
                 far_child = right;
                 curr = curr + 1;
             } else {
-                if (split < ex_pb[axis]) {
+                if (split < sel3(axis, ex0, ex1, ex2)) {
                     curr = right;
                     nd = __ldg(S.nodes + curr);
                     continue;
@@ -263,7 +264,7 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
                 far_child = curr + 1;
                 curr = right;
             }
-            const float t = (split - fr[axis]) * inv[axis];
+            const float t = (split - sel3(axis, f0, f1, f2)) * sel3(axis, R.inv.x, R.inv.y, R.inv.z);
             if (sp >= stk.cap) {
                 dev_fail(S.status, kDevStackOverflow);
                 return false;
@@ -271,11 +272,10 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             stk.nt[sp] = make_uint2(far_child | ((uint32_t)axis << 30), __float_as_uint(t));
             stk.split[sp] = split;
             sp++;
-            const int na = axis == 2 ? 0 : axis + 1, pa = axis == 0 ? 2 : axis - 1;
             ex_t = t;
-            ex_pb[axis] = split;
-            ex_pb[na] = fr[na] + t * rr[na];
-            ex_pb[pa] = fr[pa] + t * rr[pa];
+            ex0 = axis == 0 ? split : f0 + t * r0;
+            ex1 = axis == 1 ? split : f1 + t * r1;
+            ex2 = axis == 2 ? split : f2 + t * r2;
             nd = __ldg(S.nodes + curr);
         }
         res.nodes++;
@@ -302,15 +302,19 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
         if (!ANY && hit && Z <= ex_t) return true;
         // the exit point becomes the entry point; descend into its far node
         en_t = ex_t;
-        en_pb[0] = ex_pb[0];
-        en_pb[1] = ex_pb[1];
-        en_pb[2] = ex_pb[2];
+        en0 = ex0;
+        en1 = ex1;
+        en2 = ex2;
         sp--;
         curr = stk.nt[sp].x & kNodeMask;
         if (curr != kNodeMask) {
             const uint2 nx = stk.nt[sp - 1];
             ex_t = __uint_as_float(nx.y);
-            exit_point(nx.x, ex_t, stk.split[sp - 1], fr, rr, ex_pb);
+            const uint32_t ax = nx.x >> 30;  // 3: the initial exit, from + ray*t on every axis
+            const float sp_split = stk.split[sp - 1];
+            ex0 = ax == 0u ? sp_split : f0 + ex_t * r0;
+            ex1 = ax == 1u ? sp_split : f1 + ex_t * r1;
+            ex2 = ax == 2u ? sp_split : f2 + ex_t * r2;
         }
     }
     return hit;
