@@ -83,3 +83,35 @@ def test_render_gi_traversal_variants(cuda, flags):
     sc.render.flags = flags
     b = api.DeviceScene(sc).render()
     assert np.array_equal(a, b)
+
+
+def _layered_spheres_scene(res=40, layers=4, n=7):
+    """Layers of small spheres between a ground plane and a point light
+    overhead: shadow rays cross the bounds of several objects on their way,
+    so the casters' BVH walk shoots many objects per ray."""
+    pv, pt = scenes.ground_plane(half=20.0, y=-1.0)
+    sc = scenes.Scene(name="layered")
+    sc.shaders = [scenes.shader((0.8, 0.8, 0.8)), scenes.shader((0.6, 0.3, 0.2), (0.2, 0.2, 0.2), hard=10.0)]
+    sc.meshes = [scenes.Mesh(pv, pt, 0)]
+    for L in range(layers):
+        for i in range(n):
+            for j in range(n):
+                c = (-1.5 + 0.5 * i + 0.13 * L, -0.4 + 0.9 * L, -1.5 + 0.5 * j - 0.07 * L)
+                v, t = scenes.uv_sphere(c, 0.24, rings=6, segments=10)
+                sc.meshes.append(scenes.Mesh(v, t, 1))
+    sc.lights = [scenes.point_light((0.3, 9.0, 0.2), 60.0)]
+    sc.camera = scenes.camera((0, 2.5, 6), (0, 0, 0), (0, 3.5, 6), res, res)
+    sc.render = scenes.render_params(spp=2, seed=3)
+    return sc
+
+
+def test_render_many_shadow_candidates(cuda):
+    sc = _layered_spheres_scene()
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    ref, stats = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref)
+    assert ds.last_stats.rays_shadow == stats[1]
+    sc.render.flags = 2  # exact order: the nested walk, same image
+    assert np.array_equal(api.DeviceScene(sc).render(), img)
