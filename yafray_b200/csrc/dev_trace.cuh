@@ -246,11 +246,14 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             const int axis = (int)(nd.y & 3u);
             const float split = __uint_as_float(nd.x);
             const uint32_t right = nd.y >> 2;
+            // both children are fetched before the side is decided, so the
+            // next level's load overlaps this level's arithmetic
+            const uint2 nl = __ldg(S.nodes + curr + 1), nr = __ldg(S.nodes + right);
             uint32_t far_child;
             if (sel3(axis, en0, en1, en2) <= split) {
                 if (sel3(axis, ex0, ex1, ex2) <= split) {
                     curr = curr + 1;
-                    nd = __ldg(S.nodes + curr);
+                    nd = nl;
                     continue;
                 }
                 far_child = right;
@@ -258,7 +261,7 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             } else {
                 if (split < sel3(axis, ex0, ex1, ex2)) {
                     curr = right;
-                    nd = __ldg(S.nodes + curr);
+                    nd = nr;
                     continue;
                 }
                 far_child = curr + 1;
@@ -276,7 +279,7 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
             ex0 = axis == 0 ? split : f0 + t * r0;
             ex1 = axis == 1 ? split : f1 + t * r1;
             ex2 = axis == 2 ? split : f2 + t * r2;
-            nd = __ldg(S.nodes + curr);
+            nd = curr == right ? nr : nl;
         }
         res.nodes++;
         // leaf
