@@ -338,7 +338,7 @@ static void assign_adj(const Plan &P, uint32_t wcap, uint32_t npix, char *base, 
 
 int grid_for(uint32_t n, int block);
 
-constexpr size_t kAdjBudget = 1536ull << 20;
+
 
 // Wave size and scratch bytes of one backward pass.
 struct AdjPlan {
@@ -589,7 +589,7 @@ YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, floa
     };
     cudaStream_t st = (cudaStream_t)stream;
     AdjPlan A;
-    yr_status ret = adj_plan(scene, kAdjBudget, A);
+    yr_status ret = adj_plan(scene, render_budget(1), A);
     if (ret != YR_OK) return done(ret);
     PoolBlock pb(scene->device, st);  // given back (after a stream sync) when this call returns
     if ((ret = pool_acquire(scene->device, 256 + A.bytes, pb.buf)) != YR_OK) return done(ret);
@@ -628,6 +628,7 @@ YR_API yr_status yr_backward_batch(yr_scene *const *scenes, uint32_t count, cons
     std::vector<uintptr_t> key{(uintptr_t)device, (uintptr_t)nl};
     for (uint32_t i = 0; i < count; i++) key.push_back((uintptr_t)scenes[i]);
     std::unique_ptr<AdjBatch> &slot = g_adj_batches[key];
+    const size_t lane_budget = render_budget(nl);
     yr_status ret;
     if (slot)
         for (uint32_t i = 0; i < count && slot; i++)
@@ -644,9 +645,9 @@ YR_API yr_status yr_backward_batch(yr_scene *const *scenes, uint32_t count, cons
         B->h_renders.resize(count);
         std::vector<double> cost(count);
         for (uint32_t i = 0; i < count; i++) {
-            if ((ret = adj_plan(scenes[i], kAdjBudget, B->plans[i])) != YR_OK) return done(ret);
+            if ((ret = adj_plan(scenes[i], lane_budget, B->plans[i])) != YR_OK) return done(ret);
             const Plan &P = B->plans[i].P;
-            B->fwave[i] = std::max(scenes[i]->rdr.spp, wave_for_budget(P, scenes[i]->rdr, kAdjBudget));
+            B->fwave[i] = std::max(scenes[i]->rdr.spp, wave_for_budget(P, scenes[i]->rdr, lane_budget));
             std::memcpy(&B->h_scenes[i], &scenes[i]->dev, sizeof(DevScene));
             std::memcpy(&B->h_renders[i], &scenes[i]->rdr, sizeof(DevRender));
             cost[i] = (double)P.total * (1.0 + P.ns) * (1.0 + P.npath * (double)P.depth * (1.0 + P.ns));

@@ -209,6 +209,7 @@ struct BatchCtx {
     std::vector<BatchItem> items;
     std::vector<WaveLane> lanes;
     int lanes_n = 0;
+    size_t lane_budget = 1536ull << 20;
     cudaEvent_t fork = nullptr;
 
     void drop_graph() {
@@ -301,12 +302,13 @@ static yr_status ensure(void **p, size_t &have, size_t need) {
 }
 
 // ------------------------------------------------------------ waves schedule
-constexpr size_t kLaneBudget = 1536ull << 20;  // scratch per stream
+
 
 // Scenes to `n` streams, longest first onto the least loaded stream; one
 // scratch block per stream, sized for its largest wave.
 static yr_status make_lanes(BatchCtx &C, int n) {
     if (C.lanes_n == n) return YR_OK;
+    C.lane_budget = render_budget(n);  // scratch per stream
     C.drop_graph();
     C.drop_lanes();
     C.lanes.resize(n);
@@ -328,7 +330,7 @@ static yr_status make_lanes(BatchCtx &C, int n) {
         for (uint32_t s : l.scenes) {
             const Plan &P = C.plans[s];
             const uint32_t spp = C.scenes[s]->rdr.spp;
-            const uint32_t wcap = std::max(spp, wave_for_budget(P, C.scenes[s]->rdr, kLaneBudget));
+            const uint32_t wcap = std::max(spp, wave_for_budget(P, C.scenes[s]->rdr, C.lane_budget));
             need = std::max(need, wave_bytes(P, wcap));
         }
         if (need && cudaMalloc(&l.scratch, need) != cudaSuccess) return YR_ERR_OUT_OF_MEMORY;
@@ -358,7 +360,7 @@ static yr_status capture_waves(BatchCtx &C) {
         for (uint32_t s : l.scenes) {
             yr_scene *sc = C.scenes[s];
             const Plan &P = C.plans[s];
-            const uint32_t wcap = std::max(sc->rdr.spp, wave_for_budget(P, sc->rdr, kLaneBudget));
+            const uint32_t wcap = std::max(sc->rdr.spp, wave_for_budget(P, sc->rdr, C.lane_budget));
             Wave W;
             std::memset(&W, 0, sizeof(W));
             assign_wave(P, wcap, l.scratch, W);

@@ -243,7 +243,7 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
     yr_status ret = make_plan(scene, P);
     if (ret != YR_OK) return done(ret);
     // wave: whole pixels, scratch near 1.5 GB at most
-    const uint32_t wcap = std::max(scene->rdr.spp, wave_for_budget(P, scene->rdr, 1536ull << 20));
+    const uint32_t wcap = std::max(scene->rdr.spp, wave_for_budget(P, scene->rdr, render_budget(1)));
     PoolBlock blk(scene->device, st);  // given back (after a stream sync) when this call returns
     if ((ret = pool_acquire(scene->device, wave_bytes(P, wcap), blk.buf)) != YR_OK) return done(ret);
     Wave W;
