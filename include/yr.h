@@ -229,6 +229,11 @@ typedef struct yr_object_desc {
                                 YR_PER_TRIANGLE, else ignored                 */
     const yr_kdtree *tree;   /* optional prebuilt tree (e.g. flattened from
                                 YafRay's own kdTree_t); NULL = build here     */
+    float smooth_angle;      /* meshObject_t::autoSmooth angle in degrees
+                                (mesh.cc:201-279): < 1 flat shading, >= 180
+                                one normal per vertex, else per corner over
+                                the faces within the angle                    */
+    uint32_t reserved;
 } yr_object_desc;
 
 #define YR_PER_TRIANGLE 0xffffffffu

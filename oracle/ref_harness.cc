@@ -109,6 +109,7 @@ struct SceneFile {
     std::vector<yr_light_desc> lights;
     struct Obj {
         uint32_t nv, nt, shader, cast;
+        float smooth;
         std::vector<float> v;
         std::vector<uint32_t> t;
         std::vector<uint32_t> tri_shader;  // when shader == YR_PER_TRIANGLE
@@ -139,6 +140,8 @@ static void load_scene(const char *path, SceneFile &s) {
         uint32_t oh[4];
         rd(f, oh, 16);
         SceneFile::Obj &o = s.objs[i];
+        o.smooth = 0.f;
+        if (hdr[3] >= 1) rd(f, &o.smooth, 4);  // record version 1: smoothing angle
         o.nv = oh[0];
         o.nt = oh[1];
         o.shader = oh[2];
@@ -241,6 +244,7 @@ static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true) 
         meshObject_t *m = meshObject_t::factory(ver, nor, ts, fuv, fvcol);
         m->setShader(r.shaders.at(o.shader == YR_PER_TRIANGLE ? o.tri_shader[0] : o.shader));
         m->castShadows(o.cast != 0);
+        if (o.smooth >= 1.f) m->autoSmooth(o.smooth);  // as the loader does (render.cc:764)
         r.meshes.push_back(m);
         r.objindex[m] = (int)i;
         r.scene->addObject(m);

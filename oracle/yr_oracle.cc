@@ -131,6 +131,8 @@ bool cross_w(const Box &b, const V &from, const V &ray, float dist, float &where
 
 struct Obj {
     std::vector<V> tri_a, tri_b, tri_c, tri_n;
+    std::vector<V> tri_na, tri_nb, tri_nc;  // corner normals when smoothed
+    bool smooth = false;
     std::vector<uint32_t> tri_shader;
     std::vector<yr_kd_node> nodes;
     std::vector<uint32_t> prims;
@@ -543,6 +545,27 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from, const 
     s.P = from + Z * ray;
     const Obj &o = S.objs[obj];
     s.N = s.Ng = o.tri_n[tri];
+    if (o.smooth) {
+        // triangle_t::getSurface + getInterpolation (triangle.cc:74-155), in
+        // the shipped build's evaluation order (fast-math): the reciprocal
+        // of the denominator, fa from the sum of the numerators, and
+        // na*fa + (nb*fb + nc*fc)
+        const V &a = o.tri_a[tri], &b = o.tri_b[tri], &c = o.tri_c[tri], &h = s.P, &N = s.Ng;
+        float uu0, vv0, uu1, vv1, uu2, vv2;
+        const float nx = fabsf(N.x), ny = fabsf(N.y), nz = fabsf(N.z);
+        if (nx >= ny && nx >= nz) {
+            uu0 = h.y - a.y; vv0 = h.z - a.z; uu1 = b.y - a.y; vv1 = b.z - a.z; uu2 = c.y - a.y; vv2 = c.z - a.z;
+        } else if (ny >= nx && ny >= nz) {
+            uu0 = h.x - a.x; vv0 = h.z - a.z; uu1 = b.x - a.x; vv1 = b.z - a.z; uu2 = c.x - a.x; vv2 = c.z - a.z;
+        } else {
+            uu0 = h.x - a.x; vv0 = h.y - a.y; uu1 = b.x - a.x; vv1 = b.y - a.y; uu2 = c.x - a.x; vv2 = c.y - a.y;
+        }
+        const float an = uu0 * vv2 - vv0 * uu2, bn = uu1 * vv0 - vv1 * uu0, den = uu1 * vv2 - vv1 * uu2;
+        const float rc = 1.f / den, fb = an * rc, fc = bn * rc, fa = 1.f - (an + bn) * rc;
+        const V &na = o.tri_na[tri], &nb = o.tri_nb[tri], &nc = o.tri_nc[tri];
+        s.N = normalize(V(na.x * fa + (nb.x * fb + nc.x * fc), na.y * fa + (nb.y * fb + nc.y * fc),
+                          na.z * fa + (nb.z * fb + nc.z * fc)));
+    }
     createCS(s.N, s.NU, s.NV);
     s.obj = obj;
     s.shader = (int)o.tri_shader[tri];
@@ -813,6 +836,52 @@ struct orc_scene {
     Scene s;
 };
 
+// meshObject_t::autoSmooth (mesh.cc:201-279) in the shipped build's order:
+// vertex normals (angle >= 180) are normalized with the length summed as
+// y*y + (x*x + z*z); the per-corner test uses the dot y*y' + (z*z' + x*x').
+void auto_smooth(Obj &ob, const std::vector<uint32_t> &t, uint32_t nv, float angle) {
+    const size_t nt = ob.tri_n.size();
+    ob.smooth = true;
+    ob.tri_na.resize(nt);
+    ob.tri_nb.resize(nt);
+    ob.tri_nc.resize(nt);
+    std::vector<V> *corner[3] = {&ob.tri_na, &ob.tri_nb, &ob.tri_nc};
+    if (angle >= 180.f) {
+        std::vector<V> vn(nv);
+        for (size_t k = 0; k < nt; k++)
+            for (int j = 0; j < 3; j++) vn[t[3 * k + j]] = vn[t[3 * k + j]] + ob.tri_n[k];
+        for (size_t i = 0; i < vn.size(); i++) {
+            V &a = vn[i];
+            const float l = a.y * a.y + (a.x * a.x + a.z * a.z);
+            if (l != 0) {
+                const float q = (float)(1.0 / sqrt((double)l));
+                a.x *= q;
+                a.y *= q;
+                a.z *= q;
+            }
+        }
+        for (size_t k = 0; k < nt; k++)
+            for (int j = 0; j < 3; j++) (*corner[j])[k] = vn[t[3 * k + j]];
+        return;
+    }
+    const float cosa = (float)cos((double)angle * M_PI / 180.0);
+    std::vector<std::vector<size_t> > cnx(nv);
+    for (size_t k = 0; k < nt; k++)
+        for (int j = 0; j < 3; j++) cnx[t[3 * k + j]].push_back(k);
+    for (size_t k = 0; k < nt; k++) {
+        const V &N = ob.tri_n[k];
+        for (int j = 0; j < 3; j++) {
+            V sn(0, 0, 0);
+            const std::vector<size_t> &around = cnx[t[3 * k + j]];
+            for (size_t m = 0; m < around.size(); m++) {
+                const V &M = ob.tri_n[around[m]];
+                if (cosa < M.y * N.y + (M.z * N.z + M.x * N.x)) sn = sn + M;
+            }
+            (*corner[j])[k] = normalize(sn);
+        }
+    }
+}
+
 // Load a YRS1 file.  Trees are added with orc_set_tree / orc_set_object_tree.
 orc_scene *orc_load(const char *path) {
     FILE *f = fopen(path, "rb");
@@ -830,7 +899,8 @@ orc_scene *orc_load(const char *path) {
     S.objs.resize(hdr[0]);
     for (uint32_t i = 0; ok && i < hdr[0]; i++) {
         uint32_t oh[4];
-        ok = rdv(f, oh, 4);
+        float smooth_angle = 0.f;
+        ok = rdv(f, oh, 4) && (hdr[3] < 1 || rdv(f, &smooth_angle, 1));
         if (!ok) break;
         std::vector<float> v(3 * (size_t)oh[0]);
         std::vector<uint32_t> t(3 * (size_t)oh[1]), ts;
@@ -849,6 +919,7 @@ orc_scene *orc_load(const char *path) {
             ob.tri_n.push_back(normalize((b - a) ^ (c - a)));  // triangle.cc:30-43
             ob.tri_shader.push_back(oh[2] == YR_PER_TRIANGLE ? ts[k] : oh[2]);
         }
+        if (ok && smooth_angle >= 1.f) auto_smooth(ob, t, oh[0], smooth_angle);
     }
     fclose(f);
     if (!ok) {

@@ -77,6 +77,26 @@ def camera_and_render():
     np.savez_compressed(os.path.join(HERE, "render_small_160x120.npz"), camera=cam, image=img)
 
 
+def smooth_scene():
+    """A coarse sphere smoothed at 180 degrees (one normal per vertex), a
+    torus smoothed at 40 degrees (per-corner normals) and a flat plane;
+    point light, a specular shader so that the normal shows."""
+    sc = scenes.config_small(96, 72)
+    sv, st = scenes.uv_sphere((-0.6, 0.0, 0.0), 0.8, rings=10, segments=20)
+    tv, tt = scenes.torus((1.2, -0.3, 0.5), 0.6, 0.25, nu=24, nv=12)
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    sc.shaders = [scenes.shader((0.8, 0.7, 0.6), (0.4, 0.4, 0.4), hard=25.0), scenes.shader((0.8, 0.8, 0.8))]
+    sc.meshes = [scenes.Mesh(sv, st, 0, smooth_angle=180.0), scenes.Mesh(tv, tt, 0, smooth_angle=40.0),
+                 scenes.Mesh(pv, pt, 1)]
+    return sc
+
+
+def smooth_render():
+    sc = smooth_scene()
+    img, _ = T.harness_render(sc)
+    np.savez_compressed(os.path.join(HERE, "render_smooth_96x72.npz"), image=img)
+
+
 def halton_noise():
     with tempfile.TemporaryDirectory() as d:
         hp = os.path.join(d, "h.bin")
@@ -100,6 +120,7 @@ if __name__ == "__main__":
     trees()
     rays()
     camera_and_render()
+    smooth_render()
     halton_noise()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,6 +1,7 @@
 """The CPU oracle and the host-side builders against golden vectors produced
 by the unmodified reference (tests/golden/make_golden.py)."""
 import os
+import sys
 
 import numpy as np
 import pytest
@@ -89,6 +90,19 @@ def test_oracle_camera_and_render_match_reference():
     rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
     assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
     assert stats[0] == 160 * 120
+
+
+def test_oracle_smooth_render_matches_reference():
+    """meshObject_t::autoSmooth at 180 and 40 degrees and the interpolated
+    normals of triangle_t::getSurface, against the reference's render."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    g = load("render_smooth_96x72.npz")
+    img, stats = T.OracleScene(make_golden.smooth_scene()).render()
+    ref = g["image"]
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
 
 
 def test_oracle_halton_and_ri_match_reference():

@@ -115,3 +115,22 @@ def test_render_many_shadow_candidates(cuda):
     assert ds.last_stats.rays_shadow == stats[1]
     sc.render.flags = 2  # exact order: the nested walk, same image
     assert np.array_equal(api.DeviceScene(sc).render(), img)
+
+
+@pytest.mark.parametrize("gi", [False, True])
+def test_render_smoothed_meshes(cuda, gi):
+    """Interpolated shading normals of smoothed meshes (autoSmooth at 180 and
+    40 degrees), with a point light, and with area light + path GI."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.smooth_scene()
+    if gi:
+        sc.lights = [scenes.quad_light_down(0.5, 5.0, 0.5, 2.0, 2.0, 30.0, 4),
+                     scenes.path_light(samples=1, depth=2, power=1.0)]
+        sc.render.spp = 3
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    ref, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref, frac=0.995 if gi else 1.0)

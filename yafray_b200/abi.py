@@ -86,7 +86,8 @@ class YrObjectDesc(C.Structure):
     _fields_ = [("verts", C.POINTER(C.c_float)), ("nverts", C.c_uint32),
                 ("tris", C.POINTER(C.c_uint32)), ("ntris", C.c_uint32),
                 ("shader", C.c_uint32), ("cast_shadows", C.c_uint32),
-                ("tri_shaders", C.POINTER(C.c_uint32)), ("tree", C.POINTER(YrKdTree))]
+                ("tri_shaders", C.POINTER(C.c_uint32)), ("tree", C.POINTER(YrKdTree)),
+                ("smooth_angle", C.c_float), ("reserved", C.c_uint32)]
 
 
 class YrSceneDesc(C.Structure):

@@ -35,6 +35,7 @@ class DeviceScene:
             objs[i].ntris = t.shape[0]
             objs[i].shader = m.shader & 0xFFFFFFFF
             objs[i].cast_shadows = 1 if m.cast_shadows else 0
+            objs[i].smooth_angle = float(m.smooth_angle)
             if m.shader == abi.YR_PER_TRIANGLE:
                 ts = np.ascontiguousarray(m.tri_shaders, np.uint32)
                 self._keep.append(ts)

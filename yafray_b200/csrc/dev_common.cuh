@@ -90,7 +90,7 @@ struct DevObject {
     uint32_t root;      // global index of the root kd node
     uint32_t tri_base;  // first global triangle index
     uint32_t ntris;
-    uint32_t flags;     // bit0: casts shadows
+    uint32_t flags;     // bit0: casts shadows, bit1: smoothed (corner normals in DevScene::tri_nrm)
     float ob[6];        // object bound (meshObject_t::getBound), the object tree's leaf box
 };
 
@@ -100,6 +100,7 @@ struct DevScene {
     const uint2 *nodes;
     const uint32_t *prims;
     const DevObject *objects;
+    const float *tri_nrm;       // corner normals, 9 per triangle, of smoothed objects
     // object tree (geomeTree_t): per interior node 4 x float4 = left box
     // (min xyz, max xyz), right box, then the children's codes (>= 0:
     // interior node, < 0: ~object index) as int bits

@@ -211,16 +211,42 @@ __device__ __forceinline__ V3 reflect(const V3 &n, const V3 &v) {
     return (2 * vn) * n - v;
 }
 
-// meshObject_t::shoot + triangle_t::getSurface for a flat triangle
-// (mesh.cc:570-576, triangle.cc:138-141): P = from + Z*ray, N = Ng.
+// meshObject_t::shoot + triangle_t::getSurface (mesh.cc:570-576,
+// triangle.cc:138-207): P = from + Z*ray; N = Ng for a flat triangle, else
+// the corner normals interpolated at P (getInterpolation's dominant-axis
+// barycentrics) and normalized.  The shipped build evaluates the
+// interpolation as r = 1/denum, fb = alpha r, fc = beta r,
+// fa = 1 - (alpha + beta) r, and the sum as na fa + (nb fb + nc fc).
 __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender &R, int object, uint32_t tri,
                                              float Z, const V3 &from, const V3 &ray) {
     Surf s;
     s.P = from + Z * ray;
     const float4 p = __ldg(S.tris + 3 * (size_t)tri), q = __ldg(S.tris + 3 * (size_t)tri + 1),
                  r = __ldg(S.tris + 3 * (size_t)tri + 2);
-    s.N = v3(p.w, q.w, r.w);
-    s.Ng = s.N;
+    s.Ng = v3(p.w, q.w, r.w);
+    s.N = s.Ng;
+    if (S.objects[object].flags & 2u) {
+        const V3 a = v3(p.x, p.y, p.z), b = v3(q.x, q.y, q.z), c = v3(r.x, r.y, r.z), &h = s.P;
+        const float nx = fabsf(s.Ng.x), ny = fabsf(s.Ng.y), nz = fabsf(s.Ng.z);
+        float uu0, vv0, uu1, vv1, uu2, vv2;
+        if (nx >= ny && nx >= nz) {
+            uu0 = h.y - a.y; vv0 = h.z - a.z; uu1 = b.y - a.y; vv1 = b.z - a.z; uu2 = c.y - a.y; vv2 = c.z - a.z;
+        } else if (ny >= nx && ny >= nz) {
+            uu0 = h.x - a.x; vv0 = h.z - a.z; uu1 = b.x - a.x; vv1 = b.z - a.z; uu2 = c.x - a.x; vv2 = c.z - a.z;
+        } else {
+            uu0 = h.x - a.x; vv0 = h.y - a.y; uu1 = b.x - a.x; vv1 = b.y - a.y; uu2 = c.x - a.x; vv2 = c.y - a.y;
+        }
+        const float alpha = uu0 * vv2 - vv0 * uu2;
+        const float beta = uu1 * vv0 - vv1 * uu0;
+        const float denum = uu1 * vv2 - vv1 * uu2;
+        const float rd = 1.f / denum;
+        const float fb = alpha * rd, fc = beta * rd, fa = 1.f - (alpha + beta) * rd;
+        const float *cn = S.tri_nrm + 9 * (size_t)tri;
+        const V3 nn = v3(__ldg(cn + 0) * fa + (__ldg(cn + 3) * fb + __ldg(cn + 6) * fc),
+                         __ldg(cn + 1) * fa + (__ldg(cn + 4) * fb + __ldg(cn + 7) * fc),
+                         __ldg(cn + 2) * fa + (__ldg(cn + 5) * fb + __ldg(cn + 8) * fc));
+        s.N = normalize(nn);
+    }
     create_cs(s.N, s.NU, s.NV);
     s.object = object;
     s.shader = (int)__ldg(R.tri_shader + tri);

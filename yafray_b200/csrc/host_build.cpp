@@ -903,4 +903,94 @@ void build_sah_object_bvh(const std::vector<Box> &object_bounds, const std::vect
     sah_node(object_bounds, work, 0, (int)work.size(), out);
 }
 
+// ------------------------------------------------------------ smoothing
+namespace {
+
+struct N3 {
+    float x, y, z;
+};
+
+// vector3d_t::normalize with its length summed as the caller's build sums it
+N3 norm_sum_xyz(N3 a) {  // (x*x + y*y) + z*z
+    const float l = a.x * a.x + a.y * a.y + a.z * a.z;
+    if (l != 0.f) {
+        const float k = (float)(1.0 / std::sqrt((double)l));
+        a.x *= k;
+        a.y *= k;
+        a.z *= k;
+    }
+    return a;
+}
+
+N3 norm_sum_yxz(N3 a) {  // y*y + (x*x + z*z): the vertex-normal pass (fast-math)
+    const float l = a.y * a.y + (a.x * a.x + a.z * a.z);
+    if (l != 0.f) {
+        const float k = (float)(1.0 / std::sqrt((double)l));
+        a.x *= k;
+        a.y *= k;
+        a.z *= k;
+    }
+    return a;
+}
+
+}  // namespace
+
+void smooth_normals(const float *verts, const uint32_t *tris, uint32_t nverts, uint32_t ntris, float angle,
+                    std::vector<float> &corner) {
+    corner.assign(9 * (size_t)ntris, 0.f);
+    if (!(angle >= 1.f)) return;
+    // face normals as triangle_t::setVertices forms them: (b-a)^(c-a), normalized
+    std::vector<N3> fn(ntris);
+    for (uint32_t t = 0; t < ntris; t++) {
+        const float *a = verts + 3 * tris[3 * t], *b = verts + 3 * tris[3 * t + 1], *c = verts + 3 * tris[3 * t + 2];
+        const N3 u{b[0] - a[0], b[1] - a[1], b[2] - a[2]}, v{c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        fn[t] = norm_sum_xyz(N3{u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x});
+    }
+    if (angle >= 180.f) {  // one normal per vertex: the sum of its faces' normals
+        std::vector<N3> vn(nverts, N3{0.f, 0.f, 0.f});
+        for (uint32_t t = 0; t < ntris; t++)
+            for (int k = 0; k < 3; k++) {
+                N3 &n = vn[tris[3 * t + k]];
+                n.x += fn[t].x;
+                n.y += fn[t].y;
+                n.z += fn[t].z;
+            }
+        for (N3 &n : vn) n = norm_sum_yxz(n);
+        for (uint32_t t = 0; t < ntris; t++)
+            for (int k = 0; k < 3; k++) {
+                const N3 &n = vn[tris[3 * t + k]];
+                float *o = &corner[9 * (size_t)t + 3 * k];
+                o[0] = n.x;
+                o[1] = n.y;
+                o[2] = n.z;
+            }
+        return;
+    }
+    // per corner: the faces around the vertex whose normal is within the angle
+    const float cosa = (float)std::cos((double)angle * M_PI / 180.0);
+    std::vector<std::vector<uint32_t>> cnx(nverts);
+    for (uint32_t t = 0; t < ntris; t++)
+        for (int k = 0; k < 3; k++) cnx[tris[3 * t + k]].push_back(t);
+    for (uint32_t t = 0; t < ntris; t++) {
+        const N3 &N = fn[t];
+        for (int k = 0; k < 3; k++) {
+            N3 sn{0.f, 0.f, 0.f};
+            for (uint32_t o : cnx[tris[3 * t + k]]) {
+                const N3 &m = fn[o];
+                const float d = m.y * N.y + (m.z * N.z + m.x * N.x);  // fast-math order of the dot
+                if (cosa < d) {
+                    sn.x += m.x;
+                    sn.y += m.y;
+                    sn.z += m.z;
+                }
+            }
+            sn = norm_sum_xyz(sn);
+            float *o = &corner[9 * (size_t)t + 3 * k];
+            o[0] = sn.x;
+            o[1] = sn.y;
+            o[2] = sn.z;
+        }
+    }
+}
+
 }  // namespace yr

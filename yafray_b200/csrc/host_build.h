@@ -46,6 +46,12 @@ yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris
 // vertices grown by BOX_MIN.
 Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris);
 
+// meshObject_t::autoSmooth (mesh.cc:201-279) as the shipped build
+// evaluates it: the shading normal of every triangle corner (9 floats per
+// triangle: a, b, c) for a smoothing angle >= 1 degree.
+void smooth_normals(const float *verts, const uint32_t *tris, uint32_t nverts, uint32_t ntris, float angle,
+                    std::vector<float> &corner);
+
 // Flattened object tree node (geomeTree_t, geometree.h:8-32).
 struct ObjNode {
     float bmin[3];

@@ -326,6 +326,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     std::vector<float4> tris;
     std::vector<uint2> nodes;
     std::vector<uint32_t> prims, tri_shader;
+    std::vector<float> tri_nrm;  // 9 per triangle (corner normals) up to the last smoothed object
     std::vector<DevObject> objects;
     std::vector<Box> obounds;
     size_t total_tris = 0;
@@ -400,6 +401,14 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
             if (sh >= desc->nshaders) return fail(YR_ERR_INVALID_ARG);
             tri_shader.push_back(sh);
         }
+        // smoothed objects: the corner normals of meshObject_t::autoSmooth
+        const bool smooth = od.smooth_angle >= 1.f;
+        if (smooth) {
+            std::vector<float> cn;
+            smooth_normals(od.verts, od.tris, od.nverts, od.ntris, od.smooth_angle, cn);
+            if (tri_nrm.size() < 9 * (size_t)tri_base) tri_nrm.resize(9 * (size_t)tri_base, 0.f);
+            tri_nrm.insert(tri_nrm.end(), cn.begin(), cn.end());
+        }
         for (const yr_kd_node &nd : tree.nodes) {
             uint2 g;
             g.y = nd.flags;
@@ -430,7 +439,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         dob.root = node_base;
         dob.tri_base = tri_base;
         dob.ntris = od.ntris;
-        dob.flags = od.cast_shadows ? 1u : 0u;
+        dob.flags = (od.cast_shadows ? 1u : 0u) | (smooth ? 2u : 0u);
         const Box obb = mesh_bound(od.verts, od.tris, od.ntris);
         std::memcpy(dob.ob, obb.a, 12);
         std::memcpy(dob.ob + 3, obb.g, 12);
@@ -571,6 +580,8 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     if (prims.empty()) d_prims = nullptr;
     if ((st = dev_upload(s, tri_shader.data(), tri_shader.size(), (uint32_t **)&d_tri_shader)) != YR_OK)
         return fail(st);
+    const float *d_tri_nrm = nullptr;
+    if ((st = dev_upload(s, tri_nrm.data(), tri_nrm.size(), (float **)&d_tri_nrm)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, onodes.data(), onodes.size(), (float4 **)&d_onodes)) != YR_OK) return fail(st);
     const float4 *d_sonodes = nullptr;
@@ -589,6 +600,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.nodes = d_nodes;
     D.prims = d_prims;
     D.objects = d_objects;
+    D.tri_nrm = d_tri_nrm;
     D.onodes = d_onodes;
     D.oroot = oroot;
     D.sonodes = d_sonodes;

@@ -98,6 +98,7 @@ class Mesh:
     shader: int = 0
     tri_shaders: Optional[np.ndarray] = None
     cast_shadows: bool = True
+    smooth_angle: float = 0.0   # meshObject_t::autoSmooth angle (degrees); < 1 = flat
 
 
 @dataclass
@@ -367,7 +368,8 @@ def config_diffnoise(seed=5, count=32, **kw) -> List[Scene]:
 def write_yrs(sc: Scene, path: str) -> None:
     with open(path, "wb") as f:
         f.write(b"YRS1")
-        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 0))
+        # last header word: record version; 1 = object records carry the smoothing angle
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 1))
         f.write(bytes(sc.camera))
         f.write(bytes(sc.render))
         for s in sc.shaders:
@@ -377,7 +379,8 @@ def write_yrs(sc: Scene, path: str) -> None:
         for m in sc.meshes:
             v = np.ascontiguousarray(m.verts, dtype=np.float32)
             t = np.ascontiguousarray(m.tris, dtype=np.uint32)
-            f.write(struct.pack("<4I", v.shape[0], t.shape[0], m.shader & 0xFFFFFFFF, 1 if m.cast_shadows else 0))
+            f.write(struct.pack("<4If", v.shape[0], t.shape[0], m.shader & 0xFFFFFFFF, 1 if m.cast_shadows else 0,
+                                float(m.smooth_angle)))
             f.write(v.tobytes())
             f.write(t.tobytes())
             if m.shader == abi.YR_PER_TRIANGLE:
@@ -387,7 +390,7 @@ def write_yrs(sc: Scene, path: str) -> None:
 def read_yrs(path: str) -> Scene:
     data = open(path, "rb").read()
     assert data[:4] == b"YRS1", "bad magic"
-    nobj, nsh, nl, _ = struct.unpack_from("<4I", data, 4)
+    nobj, nsh, nl, version = struct.unpack_from("<4I", data, 4)
     off = 20
     sc = Scene()
     sc.camera = abi.YrCameraDesc.from_buffer_copy(data, off)
@@ -403,6 +406,10 @@ def read_yrs(path: str) -> Scene:
     for _ in range(nobj):
         nv, nt, shid, cast = struct.unpack_from("<4I", data, off)
         off += 16
+        smooth = 0.0
+        if version >= 1:
+            (smooth,) = struct.unpack_from("<f", data, off)
+            off += 4
         v = np.frombuffer(data, np.float32, 3 * nv, off).reshape(nv, 3).copy()
         off += 12 * nv
         t = np.frombuffer(data, np.uint32, 3 * nt, off).reshape(nt, 3).copy()
@@ -411,7 +418,7 @@ def read_yrs(path: str) -> Scene:
         if shid == abi.YR_PER_TRIANGLE:
             ts = np.frombuffer(data, np.uint32, nt, off).copy()
             off += 4 * nt
-        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast)))
+        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast), float(smooth)))
     return sc
 
 
