@@ -20,7 +20,10 @@ from . import abi, scenes
 class DeviceScene:
     """A scene uploaded to one GPU (yr_scene_create)."""
 
-    def __init__(self, sc: scenes.Scene, device: int = 0):
+    def __init__(self, sc: scenes.Scene, device: int = 0, trees=None):
+        """trees: optional list (one entry per mesh, None = build here) of
+        prebuilt kd-trees (pointers to abi.YrKdTree), e.g. from yr_kdtree_build
+        or flattened from YafRay's own kdTree_t."""
         self.lib = abi.load()
         self.sc = sc
         self._keep = []
@@ -36,6 +39,8 @@ class DeviceScene:
             objs[i].shader = m.shader & 0xFFFFFFFF
             objs[i].cast_shadows = 1 if m.cast_shadows else 0
             objs[i].smooth_angle = float(m.smooth_angle)
+            if trees is not None and trees[i] is not None:
+                objs[i].tree = trees[i]
             if m.shader == abi.YR_PER_TRIANGLE:
                 ts = np.ascontiguousarray(m.tri_shaders, np.uint32)
                 self._keep.append(ts)
