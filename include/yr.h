@@ -162,8 +162,19 @@ typedef struct yr_shader_desc {
     uint32_t tex_noise;      /* YR_NOISE_*                                     */
     int32_t tex_depth;       /* clouds: turbulence octaves                     */
     uint32_t tex_hard;       /* clouds: hard noise                             */
-    uint32_t reserved[1];
+    uint32_t tex_map;        /* modulator "texco" and "proj_x/y/z"
+                                (modulator_t::doMapping, texture.cc:122-320,
+                                procedural path): bits 0-7 YR_TEXCO_*, bits
+                                8-15 / 16-23 / 24-31 the source axis of x / y
+                                / z as YR_PROJ_*; 0 = global texco, x y z     */
 } yr_shader_desc;
+
+/* yr_shader_desc.tex_map.  TEXCO_ORCO reads the hit point as orco does for
+ * a mesh without orco coordinates and without a transform
+ * (meshObject_t::toObjectOrco, mesh.cc:510-514); TEXCO_NORMAL reads the
+ * shading normal. */
+enum { YR_TEXCO_GLOBAL = 0, YR_TEXCO_ORCO = 1, YR_TEXCO_NORMAL = 2 };
+enum { YR_PROJ_DEFAULT = 0, YR_PROJ_X = 1, YR_PROJ_Y = 2, YR_PROJ_Z = 3, YR_PROJ_NONE = 4 };
 
 enum { YR_LIGHT_POINT = 0, YR_LIGHT_AREA = 1, YR_LIGHT_HEMI = 2, YR_LIGHT_PATH = 3 };
 

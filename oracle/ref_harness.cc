@@ -201,9 +201,15 @@ static shader_t *make_shader(const yr_shader_desc &d, std::vector<texture_t *> &
         modu.reflection(0);
         modu.displace(0);
         modu.string2maptype("flat");
-        modu.string2texcotype("global");
+        static const char *texco[3] = {"global", "orco", "normal"};
+        modu.string2texcotype(texco[(d.tex_map & 0xffu) < 3 ? (d.tex_map & 0xffu) : 0]);
         modu.string2cliptype("extend");
-        modu.string2texprojection("x", "y", "z");
+        std::string proj[3];
+        for (int k = 0; k < 3; k++) {
+            const uint32_t pc = (d.tex_map >> (8 * (k + 1))) & 0xffu;
+            proj[k] = pc == YR_PROJ_DEFAULT ? std::string(1, "xyz"[k]) : std::string(1, "nxyzn"[pc < 5 ? pc : 4]);
+        }
+        modu.string2texprojection(proj[0], proj[1], proj[2]);
         sh->addModulator(modu);
     }
     return sh;

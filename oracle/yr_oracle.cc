@@ -466,31 +466,115 @@ const unsigned char kPerm[256] = {
     175, 83,  7,   224, 41,  166, 197, 227, 245, 247, 74,  65,  38,  106, 22,  94,  82,  45,  33,  173, 240, 145,
     255, 234, 84,  250, 102, 26,  69,  57,  207, 117, 164, 136, 251, 93};
 int hsh(int i) { return kPerm[i & 255]; }
-float fade(float t) { return t * t * t * (t * (t * 6 - 15) + 10); }
-float lerp(float t, float a, float b) { return a + t * (b - a); }
-float grad(int hash, float x, float y, float z) {
+// the two signed terms of newPerlin_t::grad (noise.h:33-39)
+void grad_parts(int hash, float x, float y, float z, float &U, float &Vv) {
     int h = hash & 15;
     float u = h < 8 ? x : y, v = h < 4 ? y : h == 12 || h == 14 ? x : z;
-    return ((h & 1) == 0 ? u : -u) + ((h & 2) == 0 ? v : -v);
+    U = (h & 1) == 0 ? u : -u;
+    Vv = (h & 2) == 0 ? v : -v;
 }
-// newPerlin_t::operator() (noise.cc:161-183), source order
+// newPerlin_t::operator() (noise.cc:161-183) as the shipped build
+// (-O3 -ffast-math) evaluates it: g++ splits every grad() into its two
+// signed terms (U = +-u, V = +-v of each cube corner) and regroups the
+// three lerps into the sum below; this is its order of operations, read
+// from the compiler's optimized tree of noise.cc, term for term.
 float perlin(const V &pt) {
-    float x = pt.x, y = pt.y, z = pt.z;
-    float u = floorf(x), v = floorf(y), w = floorf(z);
-    int X = ((int)u) & 255, Y = ((int)v) & 255, Z = ((int)w) & 255;
-    x -= u;
-    y -= v;
-    z -= w;
-    u = fade(x);
-    v = fade(y);
-    w = fade(z);
-    int A = hsh(X) + Y, AA = hsh(A) + Z, AB = hsh(A + 1) + Z, B = hsh(X + 1) + Y, BA = hsh(B) + Z, BB = hsh(B + 1) + Z;
-    float nv = lerp(w,
-                    lerp(v, lerp(u, grad(hsh(AA), x, y, z), grad(hsh(BA), x - 1, y, z)),
-                         lerp(u, grad(hsh(AB), x, y - 1, z), grad(hsh(BB), x - 1, y - 1, z))),
-                    lerp(v, lerp(u, grad(hsh(AA + 1), x, y, z - 1), grad(hsh(BA + 1), x - 1, y, z - 1)),
-                         lerp(u, grad(hsh(AB + 1), x, y - 1, z - 1), grad(hsh(BB + 1), x - 1, y - 1, z - 1))));
-    return (float)(0.5 + 0.5 * (double)nv);
+    const float px = pt.x, py = pt.y, pz = pt.z;
+    const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+    const int X = ((int)fx) & 255, Y = ((int)fy) & 255, Z = ((int)fz) & 255;
+    const float x = px - fx, y = py - fy, z = pz - fz;
+    const float x1 = x - 1.f, y1 = y - 1.f, z1 = z - 1.f;
+    const int A = hsh(X) + Y, AA = hsh(A) + Z, AB = hsh(A + 1) + Z, B = hsh(X + 1) + Y, BA = hsh(B) + Z,
+              BB = hsh(B + 1) + Z;
+    float U_aa, V_aa, U_ba, V_ba, U_ab, V_ab, U_bb, V_bb, U_aa1, V_aa1, U_ba1, V_ba1, U_ab1, V_ab1, U_bb1, V_bb1;
+    grad_parts(hsh(AA), x, y, z, U_aa, V_aa);
+    grad_parts(hsh(BA), x1, y, z, U_ba, V_ba);
+    grad_parts(hsh(AB), x, y1, z, U_ab, V_ab);
+    grad_parts(hsh(BB), x1, y1, z, U_bb, V_bb);
+    grad_parts(hsh(AA + 1), x, y, z1, U_aa1, V_aa1);
+    grad_parts(hsh(BA + 1), x1, y, z1, U_ba1, V_ba1);
+    grad_parts(hsh(AB + 1), x, y1, z1, U_ab1, V_ab1);
+    grad_parts(hsh(BB + 1), x1, y1, z1, U_bb1, V_bb1);
+    const float t283 = x * x;
+    const float t293 = y * y;
+    const float t348 = x * 6.f;
+    const float t349 = t348 - 15.f;
+    const float t350 = x * t349;
+    const float t351 = t350 + 10.f;
+    const float t282 = x * t351;
+    const float t352 = t282 * t283;
+    const float t341 = y * 6.f;
+    const float t342 = t341 - 15.f;
+    const float t343 = y * t342;
+    const float t344 = t343 + 10.f;
+    const float t292 = y * t344;
+    const float t345 = t292 * t293;
+    const float t334 = z * 6.f;
+    const float t335 = t334 - 15.f;
+    const float t336 = z * t335;
+    const float t337 = t336 + 10.f;
+    const float t485 = U_aa + V_aa;
+    const float t528 = U_ba - U_aa;
+    const float t527 = V_ba + t528;
+    const float t25 = t527 - V_aa;
+    const float t26 = t25 * t352;
+    const float t390 = U_ab + t528;
+    const float t310 = U_bb + V_bb;
+    const float t304 = V_aa - V_ab;
+    const float t512 = U_aa - U_ba;
+    const float t311 = t512 - U_ab;
+    const float t303 = t310 + t311;
+    const float t294 = t304 - V_ba;
+    const float t504 = t294 + t303;
+    const float t505 = t352 * t504;
+    const float t321 = V_ab + t505;
+    const float t322 = U_ab - U_aa;
+    const float t312 = t321 + t322;
+    const float t40 = t312 - V_aa;
+    const float t41 = t40 * t345;
+    const float t483 = t26 + t41;
+    const float t477 = t483 + t485;
+    const float t452 = U_ba1 + V_ba1;
+    const float t458 = t512 - U_aa1;
+    const float t440 = t452 + t458;
+    const float t386 = U_bb1 + V_bb1;
+    const float t381 = V_aa1 - V_ab1;
+    const float t281 = U_ab1 + U_ba1;
+    const float t383 = t386 - t281;
+    const float t411 = U_ab1 - U_aa1;
+    const float t410 = V_ab1 - V_aa1;
+    const float t407 = V_aa + t410;
+    const float t380 = V_ba - V_ba1;
+    const float t346 = t380 + t381;
+    const float t340 = V_ab - V_aa;
+    const float t389 = U_aa1 - U_bb;
+    const float t384 = t389 + t390;
+    const float t347 = t383 + t384;
+    const float t339 = t346 + t347;
+    const float t323 = t340 - V_bb;
+    const float t416 = t323 + t339;
+    const float t414 = t352 * t416;
+    const float t413 = U_aa - U_ab;
+    const float t408 = t411 + t413;
+    const float t404 = t407 + t408;
+    const float t405 = t414 - V_ab;
+    const float t425 = t404 + t405;
+    const float t426 = t345 * t425;
+    const float t466 = V_aa1 + t426;
+    const float t442 = V_aa - V_aa1;
+    const float t434 = t442 - V_ba;
+    const float t427 = t434 + t440;
+    const float t428 = t352 * t427;
+    const float t468 = U_aa1 - U_aa;
+    const float t464 = t466 + t468;
+    const float t460 = t428 - V_aa;
+    const float t83 = t460 + t464;
+    const float tpowmult276 = z * z;
+    const float tpowmult284 = z * tpowmult276;
+    const float t489 = tpowmult284 * t337;
+    const float t84 = t83 * t489;
+    const float tnv123 = t84 + t477;
+    return (float)(((double)tnv123 + 1.0) * 0.5);
 }
 // fBm_t::operator() (noise.cc:638-650)
 float fbm(V tp, float H, float lac, float oct) {
@@ -579,8 +663,17 @@ C diffuse(const Scene &S, const SP &sp) {
     const yr_shader_desc &d = S.shaders[sp.shader];
     C c = col3(d.color);
     if (d.tex_type == YR_TEX_NONE || !(d.mod_color > 0)) return c;
-    V tp(d.mod_size[0] * (sp.P.x + d.mod_ofs[0]), d.mod_size[1] * (sp.P.y + d.mod_ofs[1]),
-         d.mod_size[2] * (sp.P.z + d.mod_ofs[2]));
+    // modulator_t::doMapping, procedural path (texture.cc:122-320): texco
+    // "global" / "orco" (an untransformed mesh without orco data: P) or
+    // "normal", then projections size*(src[axis] + ofs) / size*ofs
+    const V src = (d.tex_map & 0xffu) == YR_TEXCO_NORMAL ? sp.N : sp.P;
+    float t[3];
+    for (int k = 0; k < 3; k++) {
+        const uint32_t pc = (d.tex_map >> (8 * (k + 1))) & 0xffu;
+        const int a = pc == YR_PROJ_DEFAULT ? k : (pc >= YR_PROJ_X && pc <= YR_PROJ_Z ? (int)pc - 1 : -1);
+        t[k] = a < 0 ? d.mod_size[k] * d.mod_ofs[k] : d.mod_size[k] * (src[a] + d.mod_ofs[k]);
+    }
+    V tp(t[0], t[1], t[2]);
     float f;
     if (d.tex_type == YR_TEX_MUSGRAVE_FBM)
         f = d.tex_intensity * fbm(V(tp.x * d.tex_size, tp.y * d.tex_size, tp.z * d.tex_size), d.tex_H,

@@ -91,10 +91,25 @@ def smooth_scene():
     return sc
 
 
+def texco_scene():
+    """fBm textures addressed by the shading normal and by swapped / switched
+    off projection axes, on smoothed and flat meshes."""
+    sc = smooth_scene()
+    sc.shaders = [scenes.fbm_shader((0.6, 0.5, 0.4), (0.7, 0.3, 0.2), (1.0, 1.0, 1.0), 0.8, 2.5, mod_color=0.8,
+                                    texco="normal", proj=("y", "x", "z")),
+                  scenes.fbm_shader((0.8, 0.8, 0.8), (0.2, 0.5, 0.7), (1.0, 1.0, 1.0), 0.6, 1.5, mod_color=0.9,
+                                    texco="orco", proj=("z", "n", "x"))]
+    sc.shaders[1].mod_size[:] = [1.0, 2.0, 0.5]
+    sc.shaders[1].mod_ofs[:] = [0.3, -0.2, 0.1]
+    return sc
+
+
 def smooth_render():
     sc = smooth_scene()
     img, _ = T.harness_render(sc)
     np.savez_compressed(os.path.join(HERE, "render_smooth_96x72.npz"), image=img)
+    img, _ = T.harness_render(texco_scene())
+    np.savez_compressed(os.path.join(HERE, "render_texco_96x72.npz"), image=img)
 
 
 def halton_noise():

@@ -134,3 +134,16 @@ def test_render_smoothed_meshes(cuda, gi):
     ref, _ = T.OracleScene(sc).render()
     assert np.array_equal(img[..., 3], ref[..., 3])
     _cmp(img, ref, frac=0.995 if gi else 1.0)
+
+
+def test_render_texture_coordinates(cuda):
+    """fBm modulators addressed by the shading normal, by orco, and through
+    swapped / switched-off projection axes."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.texco_scene()
+    img = api.DeviceScene(sc).render()
+    ref, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref)

@@ -25,6 +25,8 @@ STATUS_NAMES = {
 YR_TEX_NONE, YR_TEX_MUSGRAVE_FBM, YR_TEX_CLOUDS = 0, 1, 2
 YR_LIGHT_POINT, YR_LIGHT_AREA, YR_LIGHT_HEMI, YR_LIGHT_PATH = 0, 1, 2, 3
 YR_BATCH_AUTO, YR_BATCH_TILES, YR_BATCH_WAVES = 0, 1, 2
+YR_TEXCO_GLOBAL, YR_TEXCO_ORCO, YR_TEXCO_NORMAL = 0, 1, 2
+YR_PROJ_DEFAULT, YR_PROJ_X, YR_PROJ_Y, YR_PROJ_Z, YR_PROJ_NONE = 0, 1, 2, 3, 4
 YR_PER_TRIANGLE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
 
@@ -64,7 +66,7 @@ class YrShaderDesc(C.Structure):
         ("tex_color1", f3), ("tex_color2", f3), ("tex_H", C.c_float), ("tex_lacunarity", C.c_float),
         ("tex_octaves", C.c_float), ("tex_size", C.c_float), ("tex_intensity", C.c_float),
         ("mod_color", C.c_float), ("mod_size", f3), ("mod_ofs", f3), ("tex_noise", C.c_uint32),
-        ("tex_depth", C.c_int32), ("tex_hard", C.c_uint32), ("reserved", C.c_uint32 * 1),
+        ("tex_depth", C.c_int32), ("tex_hard", C.c_uint32), ("tex_map", C.c_uint32),
     ]
 
 

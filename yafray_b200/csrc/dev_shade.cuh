@@ -122,34 +122,116 @@ __device__ const uint8_t kPerm[256] = {
 
 __device__ __forceinline__ int perm(int i) { return (int)__ldg(&kPerm[i & 255]); }
 
-__device__ __forceinline__ float nfade(float t) { return t * t * t * (t * (t * 6 - 15) + 10); }
-__device__ __forceinline__ float nlerp(float t, float a, float b) { return a + t * (b - a); }
-__device__ __forceinline__ float ngrad(int hash, float x, float y, float z) {
+// the two signed terms of newPerlin_t::grad (noise.h:33-39)
+__device__ __forceinline__ void grad_parts(int hash, float x, float y, float z, float &U, float &V) {
     const int h = hash & 15;
     const float u = h < 8 ? x : y, v = h < 4 ? y : (h == 12 || h == 14 ? x : z);
-    return ((h & 1) == 0 ? u : -u) + ((h & 2) == 0 ? v : -v);
+    U = (h & 1) == 0 ? u : -u;
+    V = (h & 2) == 0 ? v : -v;
 }
 
-// newPerlin_t::operator() (noise.cc:161-183): improved Perlin noise in [0,1]
+// newPerlin_t::operator() (noise.cc:161-183): improved Perlin noise in
+// [0,1], as the shipped build (-O3 -ffast-math) evaluates it: every grad()
+// split into its two signed terms per cube corner and the three lerps
+// regrouped into the sum below, in the order of operations of the
+// compiler's optimized tree of noise.cc (bit-identical to the reference).
 __device__ __forceinline__ float perlin(const V3 &pt) {
-    float x = pt.x, y = pt.y, z = pt.z;
-    float u = floorf(x), v = floorf(y), w = floorf(z);
-    const int X = ((int)u) & 255, Y = ((int)v) & 255, Z = ((int)w) & 255;
-    x -= u;
-    y -= v;
-    z -= w;
-    u = nfade(x);
-    v = nfade(y);
-    w = nfade(z);
+    const float px = pt.x, py = pt.y, pz = pt.z;
+    const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+    const int X = ((int)fx) & 255, Y = ((int)fy) & 255, Z = ((int)fz) & 255;
+    const float x = px - fx, y = py - fy, z = pz - fz;
+    const float x1 = x - 1.f, y1 = y - 1.f, z1 = z - 1.f;
     const int A = perm(X) + Y, AA = perm(A) + Z, AB = perm(A + 1) + Z;
     const int B = perm(X + 1) + Y, BA = perm(B) + Z, BB = perm(B + 1) + Z;
-    const float nv =
-        nlerp(w,
-              nlerp(v, nlerp(u, ngrad(perm(AA), x, y, z), ngrad(perm(BA), x - 1, y, z)),
-                    nlerp(u, ngrad(perm(AB), x, y - 1, z), ngrad(perm(BB), x - 1, y - 1, z))),
-              nlerp(v, nlerp(u, ngrad(perm(AA + 1), x, y, z - 1), ngrad(perm(BA + 1), x - 1, y, z - 1)),
-                    nlerp(u, ngrad(perm(AB + 1), x, y - 1, z - 1), ngrad(perm(BB + 1), x - 1, y - 1, z - 1))));
-    return (float)(0.5 + 0.5 * (double)nv);
+    float U_aa, V_aa, U_ba, V_ba, U_ab, V_ab, U_bb, V_bb, U_aa1, V_aa1, U_ba1, V_ba1, U_ab1, V_ab1, U_bb1, V_bb1;
+    grad_parts(perm(AA), x, y, z, U_aa, V_aa);
+    grad_parts(perm(BA), x1, y, z, U_ba, V_ba);
+    grad_parts(perm(AB), x, y1, z, U_ab, V_ab);
+    grad_parts(perm(BB), x1, y1, z, U_bb, V_bb);
+    grad_parts(perm(AA + 1), x, y, z1, U_aa1, V_aa1);
+    grad_parts(perm(BA + 1), x1, y, z1, U_ba1, V_ba1);
+    grad_parts(perm(AB + 1), x, y1, z1, U_ab1, V_ab1);
+    grad_parts(perm(BB + 1), x1, y1, z1, U_bb1, V_bb1);
+    const float t283 = x * x;
+    const float t293 = y * y;
+    const float t348 = x * 6.f;
+    const float t349 = t348 - 15.f;
+    const float t350 = x * t349;
+    const float t351 = t350 + 10.f;
+    const float t282 = x * t351;
+    const float t352 = t282 * t283;
+    const float t341 = y * 6.f;
+    const float t342 = t341 - 15.f;
+    const float t343 = y * t342;
+    const float t344 = t343 + 10.f;
+    const float t292 = y * t344;
+    const float t345 = t292 * t293;
+    const float t334 = z * 6.f;
+    const float t335 = t334 - 15.f;
+    const float t336 = z * t335;
+    const float t337 = t336 + 10.f;
+    const float t485 = U_aa + V_aa;
+    const float t528 = U_ba - U_aa;
+    const float t527 = V_ba + t528;
+    const float t25 = t527 - V_aa;
+    const float t26 = t25 * t352;
+    const float t390 = U_ab + t528;
+    const float t310 = U_bb + V_bb;
+    const float t304 = V_aa - V_ab;
+    const float t512 = U_aa - U_ba;
+    const float t311 = t512 - U_ab;
+    const float t303 = t310 + t311;
+    const float t294 = t304 - V_ba;
+    const float t504 = t294 + t303;
+    const float t505 = t352 * t504;
+    const float t321 = V_ab + t505;
+    const float t322 = U_ab - U_aa;
+    const float t312 = t321 + t322;
+    const float t40 = t312 - V_aa;
+    const float t41 = t40 * t345;
+    const float t483 = t26 + t41;
+    const float t477 = t483 + t485;
+    const float t452 = U_ba1 + V_ba1;
+    const float t458 = t512 - U_aa1;
+    const float t440 = t452 + t458;
+    const float t386 = U_bb1 + V_bb1;
+    const float t381 = V_aa1 - V_ab1;
+    const float t281 = U_ab1 + U_ba1;
+    const float t383 = t386 - t281;
+    const float t411 = U_ab1 - U_aa1;
+    const float t410 = V_ab1 - V_aa1;
+    const float t407 = V_aa + t410;
+    const float t380 = V_ba - V_ba1;
+    const float t346 = t380 + t381;
+    const float t340 = V_ab - V_aa;
+    const float t389 = U_aa1 - U_bb;
+    const float t384 = t389 + t390;
+    const float t347 = t383 + t384;
+    const float t339 = t346 + t347;
+    const float t323 = t340 - V_bb;
+    const float t416 = t323 + t339;
+    const float t414 = t352 * t416;
+    const float t413 = U_aa - U_ab;
+    const float t408 = t411 + t413;
+    const float t404 = t407 + t408;
+    const float t405 = t414 - V_ab;
+    const float t425 = t404 + t405;
+    const float t426 = t345 * t425;
+    const float t466 = V_aa1 + t426;
+    const float t442 = V_aa - V_aa1;
+    const float t434 = t442 - V_ba;
+    const float t427 = t434 + t440;
+    const float t428 = t352 * t427;
+    const float t468 = U_aa1 - U_aa;
+    const float t464 = t466 + t468;
+    const float t460 = t428 - V_aa;
+    const float t83 = t460 + t464;
+    const float tpowmult276 = z * z;
+    const float tpowmult284 = z * tpowmult276;
+    const float t489 = tpowmult284 * t337;
+    const float t84 = t83 * t489;
+    const float tnv123 = t84 + t477;
+    return (float)(((double)tnv123 + 1.0) * 0.5);
 }
 
 // fBm_t::operator() (noise.cc:638-650) over newPerlin with getSignedNoise
@@ -259,10 +341,25 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
 // diffuse colour only.
 // `m_out` (optional) receives the noise value before the intensity scale
 // (the fBm sum, or the clouds turbulence), which the adjoint needs.
-__device__ __forceinline__ C3 modulated_color(const DevShader &sh, const V3 &P, float *m_out = nullptr) {
+// Texture point of the procedural path of modulator_t::doMapping
+// (texture.cc:122-320): the texco source (hit point, or the shading
+// normal), then per axis size*(source[proj] + ofs), or size*ofs when the
+// axis is switched off.
+__device__ __forceinline__ V3 tex_point(const DevShader &sh, const V3 &P, const V3 &N) {
+    const V3 &src = sh.texco == YR_TEXCO_NORMAL ? N : P;
+    float t[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int a = sh.proj[k];
+        t[k] = a < 0 ? sh.msize[k] * sh.mofs[k] : sh.msize[k] * (comp(src, a) + sh.mofs[k]);
+    }
+    return v3(t[0], t[1], t[2]);
+}
+
+__device__ __forceinline__ C3 modulated_color(const DevShader &sh, const V3 &P, const V3 &N, float *m_out = nullptr) {
     C3 C = sh.color;
     if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f)) return C;
-    const V3 tp = v3(sh.msize[0] * (P.x + sh.mofs[0]), sh.msize[1] * (P.y + sh.mofs[1]), sh.msize[2] * (P.z + sh.mofs[2]));
+    const V3 tp = tex_point(sh, P, N);
     float f;
     if (sh.tex_type == YR_TEX_MUSGRAVE_FBM) {  // textureMusgrave_t::getFloat (basictex.cc:677-680)
         const float m = fbm(V3{tp.x * sh.tsize, tp.y * sh.tsize, tp.z * sh.tsize}, sh.H, sh.lacunarity, sh.octaves);

@@ -192,7 +192,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
     C3 lkc = c3(0.f, 0.f, 0.f);
     if (active) {
         sh = R.shaders[sp.shader];
-        lkc = modulated_color(sh, sp.P, ADJ ? m_out : nullptr);
+        lkc = modulated_color(sh, sp.P, sp.N, ADJ ? m_out : nullptr);
         if (ADJ) *lkc_out = lkc;
     }
     V3 N = sp.N;
@@ -435,7 +435,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
     bool paths = false;
     if (active) {
         const DevShader sh = R.shaders[sp.shader];
-        const C3 dif = modulated_color(sh, sp.P);
+        const C3 dif = modulated_color(sh, sp.P, sp.N);
         paths = !(energy(dif) < 0.05f);
         const DevLight PL = R.lights[R.path_light];
         W.diff0[i] = make_float4(dif.r, dif.g, dif.b, paths ? PL.power : 0.f);
@@ -613,7 +613,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
         shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux);
     }
     if (active) {
-        if (!ADJ) dif = modulated_color(R.shaders[sp.shader], sp.P);
+        if (!ADJ) dif = modulated_color(R.shaders[sp.shader], sp.P, sp.N);
         const float4 col = W.p_col[p];
         const C3 nc = c3(col.x, col.y, col.z) * dif;
         W.p_next[p] = make_float4(nc.r, nc.g, nc.b, 0.f);

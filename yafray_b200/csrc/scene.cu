@@ -133,6 +133,11 @@ void make_shader(const yr_shader_desc &d, DevShader &o) {
     }
     o.tdepth = d.tex_depth;
     o.thard = (int)d.tex_hard;
+    o.texco = (int)(d.tex_map & 0xffu);
+    for (int k = 0; k < 3; k++) {
+        const uint32_t p = (d.tex_map >> (8 * (k + 1))) & 0xffu;
+        o.proj[k] = p == YR_PROJ_DEFAULT ? k : (p >= YR_PROJ_X && p <= YR_PROJ_Z ? (int)p - 1 : -1);
+    }
 }
 
 // areaLight_t::fillQuad (arealight.cc:31-73): sample grid and jitter axes.

@@ -21,6 +21,8 @@ struct DevShader {
     float mod_color;
     float msize[3], mofs[3];
     int tdepth, thard;
+    int texco;           // YR_TEXCO_*
+    int proj[3];         // source axis (0..2) of texture x / y / z, -1 = none
 };
 
 struct DevLight {

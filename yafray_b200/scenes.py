@@ -133,8 +133,16 @@ def shader(color, specular=(0.0, 0.0, 0.0), hard=1.0) -> abi.YrShaderDesc:
     return s
 
 
+def tex_map(texco="global", proj=("x", "y", "z")) -> int:
+    """yr_shader_desc.tex_map from the modulator's "texco" and "proj_x/y/z"
+    parameters ("global" / "orco" / "normal"; axes "x" "y" "z" or "n")."""
+    tc = {"global": abi.YR_TEXCO_GLOBAL, "orco": abi.YR_TEXCO_ORCO, "normal": abi.YR_TEXCO_NORMAL}[texco]
+    pc = {"x": abi.YR_PROJ_X, "y": abi.YR_PROJ_Y, "z": abi.YR_PROJ_Z, "n": abi.YR_PROJ_NONE}
+    return tc | (pc[proj[0]] << 8) | (pc[proj[1]] << 16) | (pc[proj[2]] << 24)
+
+
 def fbm_shader(color, color1, color2, intensity, size, octaves=6.0, lacunarity=2.0, H=1.0,
-               mod_color=1.0) -> abi.YrShaderDesc:
+               mod_color=1.0, texco="global", proj=("x", "y", "z")) -> abi.YrShaderDesc:
     """genericShader_t whose albedo is mixed with a musgrave fBm texture."""
     s = shader(color)
     s.tex_type = abi.YR_TEX_MUSGRAVE_FBM
@@ -147,6 +155,7 @@ def fbm_shader(color, color1, color2, intensity, size, octaves=6.0, lacunarity=2
     s.tex_intensity = float(intensity)
     s.mod_color = float(mod_color)
     s.tex_noise = 0
+    s.tex_map = tex_map(texco, proj)
     return s
 
 
