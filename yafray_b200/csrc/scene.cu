@@ -596,8 +596,9 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     if ((st = dev_upload(s, sh_nodes.data(), sh_nodes.size(), (uint2 **)&d_sh_nodes)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, sh_prims.data(), sh_prims.size(), (uint32_t **)&d_sh_prims)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, tri_obj.data(), tri_obj.size(), (uint32_t **)&d_tri_obj)) != YR_OK) return fail(st);
-    if (cudaMalloc(&s->status, sizeof(int)) != cudaSuccess) return fail(YR_ERR_OUT_OF_MEMORY);
-    if (cudaMemset(s->status, 0, sizeof(int)) != cudaSuccess) return fail(YR_ERR_CUDA);
+    // [0] status word, [1] work counter of the ray-query kernels
+    if (cudaMalloc(&s->status, 2 * sizeof(int)) != cudaSuccess) return fail(YR_ERR_OUT_OF_MEMORY);
+    if (cudaMemset(s->status, 0, 2 * sizeof(int)) != cudaSuccess) return fail(YR_ERR_CUDA);
     if (cudaMallocHost(&s->status_host, sizeof(int)) != cudaSuccess) return fail(YR_ERR_OUT_OF_MEMORY);
 
     DevScene &D = s->dev;

@@ -90,7 +90,7 @@ struct yr_scene {
     yr_render_params render{};
     yr_scene_info info{};
     int max_tree_depth = 0;
-    int *status = nullptr;          // device status word
+    int *status = nullptr;          // device status word, then the ray-query work counter
     int *status_host = nullptr;     // pinned mirror
     yr::DevShader *d_shaders = nullptr;
     yr::DevLight *d_lights = nullptr;
