@@ -11,6 +11,8 @@
 //   yr_ref_harness render  SCENE OUT THREADS [x0 x1 y0 y1 [REPEATS]]
 //                                              stock scene_t::render, float sink,
 //                                              ray counts, one JSON line per render
+//   yr_ref_harness illum   SCENE QUERIES OUT   one light's illuminate() with the
+//                                              sample stream set from outside
 //   yr_ref_harness noise   POINTS OUT          newPerlin / fBm / turbulence
 //   yr_ref_harness halton  OUT                 Halton setStart+getNext values
 //
@@ -505,6 +507,100 @@ static void cmd_render(const SceneFile &s, const char *out, int threads, const i
     fclose(f);
 }
 
+// ------------------------------------------------------------- illuminate
+// One light's illuminate() at the first hit of a ray, with the light's
+// sample stream set from outside, so that the oracle can be given the same
+// samples:
+//   hemi (hemilight.cc:57-115): HSEQ[0], HSEQ[1] setStart(m0 * samples);
+//   path (pathlight.cc:223-403, pathtools.cc:8-43): every level's Halton
+//        stream of the state's sampler setStart(m0 * samples); `synced` says
+//        whether each level 0..depth-1 was then advanced exactly `samples`
+//        times (true when no path stops early);
+//   area (arealight.cc:93-174): the global LCG (vector3d.h:262-285) seeded
+//        with `lcg`; the values it hands out are returned in vals[].
+// Query: u32 light, u32 m0, i32 lcg, f32 eye[3], f32 from[3], f32 dir[3]
+// Output: u32 hit, u32 synced, f32 rgb[3], u32 nvals, f32 vals[64]
+struct IllumRec {
+    uint32_t light, m0;
+    int32_t lcg;
+    float eye[3], from[3], dir[3];
+};
+
+static void cmd_illum(const SceneFile &s, const char *q_path, const char *out) {
+    RefScene r;
+    build_ref(s, r, true);
+    r.scene->BTree = buildObjectTree(r.scene->obj_list);
+    r.scene->setupLights();  // as scene_t::render does (scene.cc:555)
+    FILE *fi = fopen(q_path, "rb");
+    if (!fi) die("cannot open queries");
+    uint32_t n;
+    rd(fi, &n, 4);
+    std::vector<IllumRec> qs(n);
+    if (n) rd(fi, &qs[0], sizeof(IllumRec) * n);
+    fclose(fi);
+    FILE *f = fopen(out, "wb");
+    if (!f) die("cannot open output");
+    for (uint32_t i = 0; i < n; i++) {
+        const IllumRec &q = qs[i];
+        uint32_t head[2] = {0, 1};
+        float rgb[3] = {0, 0, 0};
+        uint32_t nvals = 0;
+        float vals[64];
+        memset(vals, 0, sizeof(vals));
+        renderState_t state;
+        surfacePoint_t sp;
+        if (q.light >= r.lights.size()) die("bad light index");
+        if (r.scene->firstHit(state, sp, P3(q.from), vector3d_t(q.dir[0], q.dir[1], q.dir[2]), false)) {
+            head[0] = 1;
+            light_t *l = r.lights[q.light];
+            const vector3d_t eye = P3(q.eye) - sp.P();
+            haltonSampler_t *hs = NULL;
+            pathLight_t *pl = NULL;
+            switch (s.lights[q.light].type) {
+            case YR_LIGHT_HEMI: {
+                hemiLight_t *hl = (hemiLight_t *)l;
+                hl->HSEQ[0].setStart(q.m0 * (unsigned)hl->samples);
+                hl->HSEQ[1].setStart(q.m0 * (unsigned)hl->samples);
+                break;
+            }
+            case YR_LIGHT_PATH: {
+                pl = (pathLight_t *)l;
+                hs = (haltonSampler_t *)pl->getSampler(state, *r.scene);
+                for (int k = 0; k < 2 * (pl->maxdepth + 1); k++) hs->HSEQ[k].setStart(q.m0 * (unsigned)pl->samples);
+                break;
+            }
+            case YR_LIGHT_AREA: {
+                areaLight_t *al = (areaLight_t *)l;
+                nvals = 2u * (uint32_t)al->samples;
+                if (nvals > 64) die("area light with more than 32 samples");
+                myseed = q.lcg;
+                for (uint32_t k = 0; k < nvals; k++) vals[k] = ourRandom();
+                myseed = q.lcg;
+                break;
+            }
+            }
+            const color_t c = l->illuminate(state, *r.scene, sp, eye);
+            rgb[0] = c.getR();
+            rgb[1] = c.getG();
+            rgb[2] = c.getB();
+            if (hs) {
+                for (int lev = 0; lev < pl->maxdepth; lev++)
+                    for (int k = 2 * lev; k < 2 * lev + 2; k++) {
+                        Halton ref(hs->HSEQ[k]._base);
+                        ref.setStart(q.m0 * (unsigned)pl->samples);
+                        for (int m = 0; m < pl->samples; m++) ref.getNext();
+                        if (ref.value != hs->HSEQ[k].value) head[1] = 0;
+                    }
+            }
+        }
+        wr(f, head, 8);
+        wr(f, rgb, 12);
+        wr(f, &nvals, 4);
+        wr(f, vals, sizeof(vals));
+    }
+    fclose(f);
+}
+
 // ------------------------------------------------------------------- noise
 static void cmd_noise(const char *pts_path, const char *out) {
     FILE *fi = fopen(pts_path, "rb");
@@ -568,6 +664,9 @@ int main(int argc, char **argv) {
     } else if (cmd == "rays") {
         if (argc < 5) die("rays SCENE RAYS OUT");
         cmd_rays(s, argv[3], argv[4]);
+    } else if (cmd == "illum") {
+        if (argc < 5) die("illum SCENE QUERIES OUT");
+        cmd_illum(s, argv[3], argv[4]);
     } else if (cmd == "camera") {
         cmd_camera(s, argv[3]);
     } else if (cmd == "render") {

@@ -168,6 +168,10 @@ struct Scene {
     Cam cam;
     yr_render_params rp;
     Stats st;
+    // orc_illum only: Cranley-Patterson rotation off, and the area lights'
+    // random values given from outside (2 per sample) instead of Halton
+    bool no_rot = false;
+    const float *area_vals = nullptr;
 };
 
 // ------------------------------------------------------------- triangles
@@ -439,6 +443,7 @@ float cp_add(float v, float r) {
     if (u >= 1.0f) u -= 1.0f;
     return u;
 }
+float rot(const Scene &S, uint32_t pixel, uint32_t dim) { return S.no_rot ? 0.f : cp_rot(S.rp.seed, pixel, dim); }
 const unsigned kPrimes[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
 uint32_t light_dim(int k, int v) { return 64u + 16u * (uint32_t)k + 2u * (uint32_t)v; }
 
@@ -724,11 +729,20 @@ C illum_area(Scene &S, int k, const Light &L, const SP &sp, const V &eye, int v,
     float plane_at = (sp.P - L.from) * L.direction;
     if (plane_at <= 0) return C();
     const uint32_t d = light_dim(k, v);
-    const float r0 = cp_rot(S.rp.seed, cx.pixel, d), r1 = cp_rot(S.rp.seed, cx.pixel, d + 1);
+    const float r0 = rot(S, cx.pixel, d), r1 = rot(S, cx.pixel, d + 1);
     C resul;
     for (int i = 0; i < L.samples; i++) {
         const uint32_t m = m0 * (uint32_t)L.samples + (uint32_t)i;
-        const float h2 = cp_add(halton(2, m), r0), h3 = cp_add(halton(3, m), r1);
+        float h2, h3;
+        if (S.area_vals) {
+            // the shipped build draws toY's value first in the one-sample
+            // expression corner + toX*ourRandom() + toY*ourRandom()
+            h2 = S.area_vals[L.samples == 1 ? 1 : 2 * i];
+            h3 = S.area_vals[L.samples == 1 ? 0 : 2 * i + 1];
+        } else {
+            h2 = cp_add(halton(2, m), r0);
+            h3 = cp_add(halton(3, m), r1);
+        }
         V sampleP;
         if (L.samples == 1) sampleP = (L.corner + L.tox * h2) + L.toy * h3;
         else sampleP = (L.pts[i] + L.jit1[i] * (h2 - 0.5f)) + L.jit2[i] * (h3 - 0.5f);
@@ -758,7 +772,7 @@ C illum_hemi(Scene &S, int k, const Light &L, const SP &sp, const V &eye, int v,
     if (fabsf(fl.b) > mad) mad = fabsf(fl.b);
     if (mad < 0.05f) return C();
     const uint32_t d = light_dim(k, v);
-    const float r0 = cp_rot(S.rp.seed, cx.pixel, d), r1 = cp_rot(S.rp.seed, cx.pixel, d + 1);
+    const float r0 = rot(S, cx.pixel, d), r1 = rot(S, cx.pixel, d + 1);
     C total;
     for (int sm = 0; sm < L.samples; sm++) {
         const uint32_t m = m0 * (uint32_t)L.samples + (uint32_t)sm;
@@ -793,8 +807,8 @@ C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx
     C total;
     for (int i = 0; i < P; i++) {
         const uint32_t n = cx.s * (uint32_t)P + (uint32_t)i;
-        V ray = cosHemi(N, sp.NU, sp.NV, cp_add(halton(kPrimes[0], n), cp_rot(S.rp.seed, cx.pixel, 0)),
-                        cp_add(halton(kPrimes[1], n), cp_rot(S.rp.seed, cx.pixel, 1)));
+        V ray = cosHemi(N, sp.NU, sp.NV, cp_add(halton(kPrimes[0], n), rot(S, cx.pixel, 0)),
+                        cp_add(halton(kPrimes[1], n), rot(S, cx.pixel, 1)));
         const V startray = ray;
         V where = sp.P;
         C raycolor(1, 1, 1);
@@ -819,8 +833,8 @@ C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx
             if (j + 1 < depth) {
                 const int lev = j + 1;
                 ray = cosHemi(HN, t.NU, t.NV,
-                              cp_add(halton(kPrimes[2 * lev], n), cp_rot(S.rp.seed, cx.pixel, 2 * lev)),
-                              cp_add(halton(kPrimes[2 * lev + 1], n), cp_rot(S.rp.seed, cx.pixel, 2 * lev + 1)));
+                              cp_add(halton(kPrimes[2 * lev], n), rot(S, cx.pixel, 2 * lev)),
+                              cp_add(halton(kPrimes[2 * lev + 1], n), rot(S, cx.pixel, 2 * lev + 1)));
             }
             where = t.P;
         }
@@ -1180,6 +1194,44 @@ void orc_render(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint6
         stats[6] = S.st.roots;
     }
     g_stats = NULL;
+}
+
+// One light's illuminate at the first hit of (from, dir) (scene_t::firstHit,
+// scene.cc:688-720), eye point `eye`, QMC sample index m0 at vertex level 0,
+// rotation off; an area light takes its 2 values per sample from `vals`.
+// Returns whether the ray hit; rgb = the light's contribution.
+int orc_illum(orc_scene *o, uint32_t light, const float *eye, const float *from, const float *dir, uint32_t m0,
+              const float *vals, float *rgb) {
+    Scene &S = o->s;
+    rgb[0] = rgb[1] = rgb[2] = 0.f;
+    if (light >= S.lights.size()) return -1;
+    const V d(dir[0], dir[1], dir[2]);
+    const V f = V(from[0], from[1], from[2]) + d * kMinRay;
+    Hit h = closest(S, f, d, false, false);
+    if (h.obj < 0) return 0;
+    SP sp = surface(S, h.obj, h.tri, h.Z, f, d);
+    Ctx cx;
+    cx.pixel = 0;
+    cx.s = m0;
+    cx.pi = 0;
+    cx.npath = 0;
+    const V eyev = V(eye[0], eye[1], eye[2]) - sp.P;
+    const Light &L = S.lights[light];
+    S.no_rot = true;
+    S.area_vals = L.d.type == YR_LIGHT_AREA ? vals : nullptr;
+    C c;
+    switch (L.d.type) {
+    case YR_LIGHT_POINT: c = illum_point(S, L, sp, eyev); break;
+    case YR_LIGHT_AREA: c = illum_area(S, (int)light, L, sp, eyev, 0, m0, cx); break;
+    case YR_LIGHT_HEMI: c = illum_hemi(S, (int)light, L, sp, eyev, 0, m0, cx); break;
+    case YR_LIGHT_PATH: c = illum_path(S, L, sp, eyev, cx); break;
+    }
+    S.no_rot = false;
+    S.area_vals = nullptr;
+    rgb[0] = c.r;
+    rgb[1] = c.g;
+    rgb[2] = c.b;
+    return 1;
 }
 
 // primary ray directions of pixel centres (camera_t::shootRay)

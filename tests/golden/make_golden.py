@@ -112,6 +112,76 @@ def smooth_render():
     np.savez_compressed(os.path.join(HERE, "render_texco_96x72.npz"), image=img)
 
 
+def illum_scene():
+    """Smoothed sphere, torus and plane (textured and specular shaders) lit
+    by a 16-sample and a 1-sample area light, two hemi lights (unbounded and
+    at maxdist 2.5) and a point light."""
+    sc = texco_scene()
+    sc.shaders.append(scenes.shader((0.7, 0.6, 0.5), (0.5, 0.5, 0.5), hard=12.0))
+    sc.meshes[2].shader = 2
+    sc.lights = [scenes.quad_light_down(0.5, 3.0, 0.5, 2.0, 1.5, 3.0, samples=16, color=(1.0, 0.9, 0.8)),
+                 scenes.area_light((-2.0, 2.5, -1.0), (-1.0, 2.5, -1.0), (-1.0, 2.5, 0.0), (-2.0, 2.5, 0.0), 2.0,
+                                   samples=1),
+                 scenes.hemi_light(samples=9, power=0.8, color=(0.9, 0.95, 1.0)),
+                 scenes.hemi_light(samples=4, power=1.2, maxdist=2.5),
+                 scenes.point_light((2.0, 3.0, 2.0), 4.0)]
+    return sc
+
+
+def box_mesh(lo, hi, shader):
+    """Closed axis-aligned box, 12 triangles."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], np.float32)
+    t = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4],
+                  [3, 6, 2], [3, 7, 6], [0, 4, 7], [0, 7, 3], [1, 2, 6], [1, 6, 5]], np.uint32)
+    return scenes.Mesh(v, t, shader)
+
+
+def path_scene():
+    """A closed room (no path reaches the background) with a smoothed sphere
+    and a torus, bright albedos (no path ends early), a point light for the
+    direct light at the bounce vertices and a 4-sample, 3-bounce path light."""
+    sc = smooth_scene()
+    sc.shaders = [scenes.shader((0.9, 0.8, 0.7), (0.3, 0.3, 0.3), hard=20.0),
+                  scenes.fbm_shader((0.85, 0.85, 0.8), (0.7, 0.8, 0.9), (0.95, 0.85, 0.7), 0.7, 1.5, mod_color=0.8),
+                  scenes.shader((0.8, 0.85, 0.9))]
+    sc.meshes = [sc.meshes[0], sc.meshes[1], box_mesh((-4.0, -1.0, -4.0), (4.0, 4.0, 6.0), 2)]
+    sc.meshes[1].shader = 1
+    sc.lights = [scenes.point_light((0.5, 3.0, 1.0), 6.0), scenes.path_light(samples=4, depth=3, power=1.0)]
+    return sc
+
+
+def illum_queries(sc, n, seed):
+    """Rays from the camera towards random points of the image, each for one
+    light (in turn), with a random QMC sample index and LCG seed."""
+    rng = np.random.default_rng(seed)
+    q = np.zeros(n, T.ILLUM_REC)
+    cam = sc.camera
+    pos = np.array(cam.pos[:], np.float32)
+    look = np.array(cam.look[:], np.float32)
+    tgt = look + rng.uniform(-2.5, 2.5, (n, 3)).astype(np.float32) * np.float32([1.0, 0.6, 1.0])
+    d = tgt - pos
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    q["light"] = np.arange(n) % len(sc.lights)
+    q["m0"] = rng.integers(0, 4096, n)
+    q["lcg"] = rng.integers(1, 2 ** 31 - 2, n)
+    q["eye"] = pos
+    q["frm"] = pos
+    q["dir"] = d.astype(np.float32)
+    return q
+
+
+def illum():
+    out = {}
+    for name, sc, n, seed in (("gi", illum_scene(), 600, 11), ("path", path_scene(), 200, 12)):
+        q = illum_queries(sc, n, seed)
+        out[name + "_q"] = q
+        out[name + "_o"] = T.harness_illum(sc, q)
+    np.savez_compressed(os.path.join(HERE, "illum.npz"), **out)
+
+
 def halton_noise():
     with tempfile.TemporaryDirectory() as d:
         hp = os.path.join(d, "h.bin")
@@ -136,6 +206,7 @@ if __name__ == "__main__":
     rays()
     camera_and_render()
     smooth_render()
+    illum()
     halton_noise()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

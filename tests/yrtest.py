@@ -43,6 +43,7 @@ def oracle() -> C.CDLL:
             "orc_kd": (None, [P, U, P, P, F, C.c_int, P]),
             "orc_render": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
             "orc_camera_rays": (None, [P, P]),
+            "orc_illum": (C.c_int, [P, U, P, P, P, U, P, P]),
             "orc_halton": (F, [U, U]),
             "orc_ri_lp": (F, [U]),
             "orc_cp_rot": (F, [U, U, U]),
@@ -177,6 +178,23 @@ class OracleScene:
         self.lib.orc_camera_rays(self.h, ptr(d))
         return d
 
+    def illum(self, q: np.ndarray, vals: np.ndarray):
+        """One light's contribution at the first hit of each ILLUM_REC query,
+        rotation off, area lights fed `vals` (n, 64).  Returns (hit, rgb)."""
+        n = q.shape[0]
+        hit = np.zeros(n, np.int32)
+        rgb = np.zeros((n, 3), np.float32)
+        for i in range(n):
+            e = np.ascontiguousarray(q["eye"][i], np.float32)
+            f = np.ascontiguousarray(q["frm"][i], np.float32)
+            d = np.ascontiguousarray(q["dir"][i], np.float32)
+            v = np.ascontiguousarray(vals[i], np.float32)
+            out = np.zeros(3, np.float32)
+            hit[i] = self.lib.orc_illum(self.h, int(q["light"][i]), ptr(e), ptr(f), ptr(d), int(q["m0"][i]), ptr(v),
+                                        ptr(out))
+            rgb[i] = out
+        return hit, rgb
+
 
 # ----------------------------------------------------------------- harness
 def run_harness(*args, timeout=600):
@@ -246,6 +264,24 @@ def harness_render(sc: scenes.Scene, threads=1, crop=None):
         img = np.fromfile(op, np.float32).reshape(sc.resy, sc.resx, 4)
     import json
     return img, json.loads(out.strip().splitlines()[-1])
+
+
+ILLUM_REC = np.dtype([("light", "<u4"), ("m0", "<u4"), ("lcg", "<i4"), ("eye", "<f4", 3), ("frm", "<f4", 3),
+                      ("dir", "<f4", 3)])
+ILLUM_OUT = np.dtype([("hit", "<u4"), ("synced", "<u4"), ("rgb", "<f4", 3), ("nvals", "<u4"), ("vals", "<f4", 64)])
+
+
+def harness_illum(sc: scenes.Scene, q: np.ndarray) -> np.ndarray:
+    """One light's illuminate() per ILLUM_REC query in the reference, with
+    the light's sample stream set from the query; returns ILLUM_OUT records."""
+    with tempfile.TemporaryDirectory() as d:
+        sp, qp, op = os.path.join(d, "s.yrs"), os.path.join(d, "q.bin"), os.path.join(d, "o.bin")
+        scenes.write_yrs(sc, sp)
+        with open(qp, "wb") as f:
+            f.write(struct.pack("<I", q.shape[0]))
+            f.write(np.ascontiguousarray(q, ILLUM_REC).tobytes())
+        run_harness("illum", sp, qp, op)
+        return np.fromfile(op, ILLUM_OUT)
 
 
 def harness_camera(sc: scenes.Scene) -> np.ndarray:
