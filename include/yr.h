@@ -137,13 +137,54 @@ typedef struct yr_camera_desc {
     float focal;             /* "focal": width-1 image plane at this distance  */
 } yr_camera_desc;
 
-enum { YR_TEX_NONE = 0, YR_TEX_MUSGRAVE_FBM = 1, YR_TEX_CLOUDS = 2 };
-enum { YR_NOISE_NEWPERLIN = 0 };
+/* Procedural textures (basictex.cc).  Musgrave types share
+ * textureMusgrave_t (basictex.cc:656-709) with the generator of its "type". */
+enum {
+    YR_TEX_NONE = 0,
+    YR_TEX_MUSGRAVE_FBM = 1,             /* musgrave, type "fBm"           */
+    YR_TEX_CLOUDS = 2,                   /* clouds (basictex.cc:64-104)     */
+    YR_TEX_MARBLE = 3,                   /* marble (basictex.cc:110-175)    */
+    YR_TEX_WOOD = 4,                     /* wood (basictex.cc:181-249)      */
+    YR_TEX_VORONOI = 5,                  /* voronoi (basictex.cc:560-650)   */
+    YR_TEX_MUSGRAVE_MULTIFRACTAL = 6,    /* musgrave, type "multifractal"   */
+    YR_TEX_MUSGRAVE_HETEROTERRAIN = 7,   /* musgrave, type "heteroterrain"  */
+    YR_TEX_MUSGRAVE_HYBRIDMF = 8,        /* musgrave, type "hybridmf"       */
+    YR_TEX_MUSGRAVE_RIDGEDMF = 9,        /* musgrave, type "ridgedmf"       */
+    YR_TEX_DISTORTED_NOISE = 10,         /* distorted_noise (basictex.cc:711-746) */
+    YR_TEX_GRADIENT = 11                 /* gradient (basictex.cc:752-815)  */
+};
+/* Noise bases by the "noise_type" names of newNoise (basictex.cc:34-60). */
+enum {
+    YR_NOISE_NEWPERLIN = 0,       /* "newperlin" (the default)        */
+    YR_NOISE_STDPERLIN = 1,       /* "stdperlin"                      */
+    YR_NOISE_BLENDER = 2,         /* "blender"                        */
+    YR_NOISE_VORONOI_F1 = 3,      /* "voronoi_f1" (distance: real)    */
+    YR_NOISE_VORONOI_F2 = 4,      /* "voronoi_f2"                     */
+    YR_NOISE_VORONOI_F3 = 5,      /* "voronoi_f3"                     */
+    YR_NOISE_VORONOI_F4 = 6,      /* "voronoi_f4"                     */
+    YR_NOISE_VORONOI_F2F1 = 7,    /* "voronoi_f2f1"                   */
+    YR_NOISE_VORONOI_CRACKLE = 8, /* "voronoi_crackle"                */
+    YR_NOISE_CELLNOISE = 9        /* "cellnoise"                      */
+};
+/* marble / wood "shape" */
+enum { YR_WAVE_SIN = 0, YR_WAVE_SAW = 1, YR_WAVE_TRI = 2 };
+/* voronoi texture "distance_metric" (voronoi_t::dMetricType) */
+enum {
+    YR_DIST_REAL = 0, YR_DIST_SQUARED = 1, YR_DIST_MANHATTAN = 2, YR_DIST_CHEBYCHEV = 3,
+    YR_DIST_MINKOVSKY_HALF = 4, YR_DIST_MINKOVSKY_FOUR = 5, YR_DIST_MINKOVSKY = 6
+};
+/* gradient "gradient_type" */
+enum {
+    YR_GRAD_LINEAR = 0, YR_GRAD_QUADRATIC = 1, YR_GRAD_CUBIC = 2, YR_GRAD_DIAGONAL = 3,
+    YR_GRAD_SPHERE = 4, YR_GRAD_HALO = 5
+};
+/* modulator "mode" (texture.cc:499-534) applied to the diffuse colour */
+enum { YR_MOD_MIX = 0, YR_MOD_MUL = 1, YR_MOD_ADD = 2, YR_MOD_SUB = 3 };
 
 /* genericShader_t (basicshaders.h:37-152) with at most one modulator
- * (texture.cc:499-534, mode "mix", texco global/orco of an untransformed
- * mesh, i.e. the hit position) driving a musgrave fBm texture
- * (basictex.cc:656-709).  64 bytes of colour params + texture block. */
+ * (texture.cc:499-534) on the diffuse colour, driving one procedural
+ * texture.  The texture's parameters keep the names of its factory; each
+ * texture reads the fields its factory reads and ignores the others. */
 typedef struct yr_shader_desc {
     float color[3];          /* "color": diffuse albedo (scolor)               */
     float specular[3];       /* "specular": Phong colour (ks)                  */
@@ -154,19 +195,39 @@ typedef struct yr_shader_desc {
     float tex_H;             /* "H"                                            */
     float tex_lacunarity;    /* "lacunarity"                                   */
     float tex_octaves;       /* "octaves"                                      */
-    float tex_size;          /* texture "size" (p*size inside getFloat)        */
-    float tex_intensity;     /* "intensity" (iscale)                           */
+    float tex_size;          /* texture "size" (musgrave, clouds, marble, wood,
+                                voronoi, distorted_noise)                     */
+    float tex_intensity;     /* musgrave / voronoi "intensity" (iscale)        */
     float mod_color;         /* modulator "color": mix weight into C           */
     float mod_size[3];       /* modulator sizex/y/z                            */
     float mod_ofs[3];        /* modulator ofsx/y/z                             */
     uint32_t tex_noise;      /* YR_NOISE_*                                     */
-    int32_t tex_depth;       /* clouds: turbulence octaves                     */
-    uint32_t tex_hard;       /* clouds: hard noise                             */
+    int32_t tex_depth;       /* clouds / marble / wood "depth": turbulence
+                                octaves                                       */
+    uint32_t tex_hard;       /* clouds / marble / wood "hard"                  */
     uint32_t tex_map;        /* modulator "texco" and "proj_x/y/z"
                                 (modulator_t::doMapping, texture.cc:122-320,
                                 procedural path): bits 0-7 YR_TEXCO_*, bits
                                 8-15 / 16-23 / 24-31 the source axis of x / y
                                 / z as YR_PROJ_*; 0 = global texco, x y z     */
+    /* record version 2 */
+    uint32_t mod_mode;       /* modulator "mode": YR_MOD_*                     */
+    uint32_t tex_shape;      /* marble / wood "shape" YR_WAVE_*; gradient
+                                "gradient_type" YR_GRAD_*; voronoi
+                                "color_type" 0 int, 1-3 col1-col3             */
+    uint32_t tex_variant;    /* wood "wood_type": 1 rings, 0 bands; clouds
+                                "bias": 0 none, 1 positive, 2 negative;
+                                gradient "flip_xy"                            */
+    float tex_turbulence;    /* marble / wood "turbulence"                     */
+    float tex_sharpness;     /* marble "sharpness"                             */
+    float tex_offset;        /* musgrave "offset"                              */
+    float tex_gain;          /* musgrave "gain"                                */
+    float tex_distort;       /* distorted_noise "distort"                      */
+    uint32_t tex_noise2;     /* distorted_noise "noise_type2" (tex_noise is
+                                "noise_type1")                                */
+    float tex_weights[4];    /* voronoi "weight1".."weight4"                   */
+    float tex_mk_exponent;   /* voronoi "mk_exponent"                          */
+    uint32_t tex_metric;     /* voronoi "distance_metric" YR_DIST_*            */
 } yr_shader_desc;
 
 /* yr_shader_desc.tex_map.  TEXCO_ORCO reads the hit point as orco does for
@@ -422,7 +483,9 @@ YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t count, float 
  * Adjoint.  Gradient of  L = sum_pixels w * |img - target|^2  ... see
  * yr_backward_desc.  Parameter vector layout, per scene:
  *   for each shader s: color[3], specular weight (the scalar that scales
- *   "specular"), tex amplitude (tex_intensity), tex base colour (tex_color1[3])
+ *   "specular"), tex amplitude (tex_intensity: musgrave and voronoi
+ *   textures; its gradient is 0 for the others), tex base colour
+ *   (tex_color1[3]; gradient 0 for voronoi, whose colour does not use it)
  *   for each light l: power
  * ------------------------------------------------------------------------ */
 typedef struct yr_backward_desc {

@@ -15,6 +15,10 @@
 //                                              sample stream set from outside
 //   yr_ref_harness noise   POINTS OUT          newPerlin / fBm / turbulence
 //   yr_ref_harness halton  OUT                 Halton setStart+getNext values
+//   yr_ref_harness noisegen POINTS OUT         every noise basis, turbulence,
+//                                              voronoi distances per metric
+//   yr_ref_harness texeval SCENE POINTS OUT    each shader's texture getColor /
+//                                              getFloat
 //
 // Private members (kdTree_t::nodes, meshObject_t::triangles, scene_t::BTree)
 // are read by compiling the reference headers with private/protected
@@ -39,6 +43,7 @@
 #undef private
 #undef protected
 
+#include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -59,6 +64,7 @@ namespace yafray {
 // image textures are not on the path.
 cBuffer_t *load_jpeg(const char *name) { return NULL; }
 geomeTree_t<object3d_t> *buildObjectTree(std::list<object3d_t *> &obj_list);
+noiseGenerator_t *newNoise(const std::string &ntype);
 }
 
 // Ray counters: the reference has none (mesh.cc:409-412 are unused), so
@@ -134,7 +140,10 @@ static void load_scene(const char *path, SceneFile &s) {
     rd(f, &s.cam, sizeof(s.cam));
     rd(f, &s.rp, sizeof(s.rp));
     s.shaders.resize(hdr[1]);
-    if (hdr[1]) rd(f, &s.shaders[0], sizeof(yr_shader_desc) * hdr[1]);
+    memset(s.shaders.data(), 0, sizeof(yr_shader_desc) * hdr[1]);
+    // shader records before version 2 end at mod_mode
+    const size_t shsize = hdr[3] >= 2 ? sizeof(yr_shader_desc) : offsetof(yr_shader_desc, mod_mode);
+    for (uint32_t i = 0; i < hdr[1]; i++) rd(f, &s.shaders[i], shsize);
     s.lights.resize(hdr[2]);
     if (hdr[2]) rd(f, &s.lights[0], sizeof(yr_light_desc) * hdr[2]);
     s.objs.resize(hdr[0]);
@@ -174,19 +183,63 @@ struct RefScene {
 static point3d_t P3(const float *p) { return point3d_t(p[0], p[1], p[2]); }
 static color_t C3(const float *p) { return color_t(p[0], p[1], p[2]); }
 
+static const char *noise_name(uint32_t t) {
+    static const char *n[10] = {"newperlin",  "stdperlin",  "blender",    "voronoi_f1",      "voronoi_f2",
+                                "voronoi_f3", "voronoi_f4", "voronoi_f2f1", "voronoi_crackle", "cellnoise"};
+    return t < 10 ? n[t] : "newperlin";
+}
+
+// the texture of a shader record, through the plugin's own constructors
+static texture_t *make_texture(const yr_shader_desc &d) {
+    const color_t c1 = C3(d.tex_color1), c2 = C3(d.tex_color2);
+    static const char *shapes[3] = {"sin", "saw", "tri"};
+    const char *shape = shapes[d.tex_shape < 3 ? d.tex_shape : 0];
+    switch (d.tex_type) {
+    case YR_TEX_MUSGRAVE_FBM:
+    case YR_TEX_MUSGRAVE_MULTIFRACTAL:
+    case YR_TEX_MUSGRAVE_HETEROTERRAIN:
+    case YR_TEX_MUSGRAVE_HYBRIDMF:
+    case YR_TEX_MUSGRAVE_RIDGEDMF: {
+        static const char *mt[5] = {"fBm", "multifractal", "heteroterrain", "hybridmf", "ridgedmf"};
+        const int k = d.tex_type == YR_TEX_MUSGRAVE_FBM ? 0 : (int)d.tex_type - YR_TEX_MUSGRAVE_MULTIFRACTAL + 1;
+        return new textureMusgrave_t(c1, c2, d.tex_H, d.tex_lacunarity, d.tex_octaves, d.tex_offset, d.tex_gain,
+                                     d.tex_size, d.tex_intensity, noise_name(d.tex_noise), mt[k]);
+    }
+    case YR_TEX_CLOUDS:
+        return new textureClouds_t(d.tex_depth, d.tex_size, d.tex_hard != 0, c1, c2, noise_name(d.tex_noise),
+                                   d.tex_variant == 1 ? "positive" : (d.tex_variant == 2 ? "negative" : ""));
+    case YR_TEX_MARBLE:
+        return new textureMarble_t(d.tex_depth, d.tex_size, c1, c2, d.tex_turbulence, d.tex_sharpness,
+                                   d.tex_hard != 0, noise_name(d.tex_noise), shape);
+    case YR_TEX_WOOD:
+        return new textureWood_t(d.tex_depth, d.tex_size, c1, c2, d.tex_turbulence, d.tex_hard != 0,
+                                 noise_name(d.tex_noise), d.tex_variant ? "rings" : "bands", shape);
+    case YR_TEX_VORONOI: {
+        static const char *dm[7] = {"real",           "squared",        "manhattan", "chebychev",
+                                    "minkovsky_half", "minkovsky_four", "minkovsky"};
+        return new textureVoronoi_t(c1, c2, (int)d.tex_shape, d.tex_weights[0], d.tex_weights[1], d.tex_weights[2],
+                                    d.tex_weights[3], d.tex_mk_exponent, d.tex_size, d.tex_intensity,
+                                    dm[d.tex_metric < 7 ? d.tex_metric : 0]);
+    }
+    case YR_TEX_DISTORTED_NOISE:
+        return new textureDistortedNoise_t(c1, c2, d.tex_distort, d.tex_size, noise_name(d.tex_noise),
+                                           noise_name(d.tex_noise2));
+    case YR_TEX_GRADIENT: {
+        static const char *gt[6] = {"linear", "quadratic", "cubic", "diagonal", "sphere", "halo"};
+        return new textureGradient_t(c1, c2, gt[d.tex_shape < 6 ? d.tex_shape : 0], d.tex_variant != 0);
+    }
+    }
+    die("bad texture type");
+    return NULL;
+}
+
 static shader_t *make_shader(const yr_shader_desc &d, std::vector<texture_t *> &textures) {
     // genericShader_t::factory defaults (basicshaders.cc:217-262)
     genericShader_t *sh = new genericShader_t(C3(d.color), d.hard, (CFLOAT)1.0, color_t(0.0), color_t(0.0),
                                               C3(d.specular), color_t(0.0), color_t(0.0), NULL, 0.0, (CFLOAT)1.0,
                                               1.0, false, false, 0, 0, false, color_t(0.0));
     if (d.tex_type != YR_TEX_NONE) {
-        texture_t *tex;
-        if (d.tex_type == YR_TEX_MUSGRAVE_FBM)
-            tex = new textureMusgrave_t(C3(d.tex_color1), C3(d.tex_color2), d.tex_H, d.tex_lacunarity,
-                                        d.tex_octaves, 1.0, 1.0, d.tex_size, d.tex_intensity, "newperlin", "fBm");
-        else
-            tex = new textureClouds_t(d.tex_depth, d.tex_size, d.tex_hard != 0, C3(d.tex_color1),
-                                      C3(d.tex_color2), "newperlin", "");
+        texture_t *tex = make_texture(d);
         textures.push_back(tex);
         modulator_t modu(tex);
         modu.sizeX(d.mod_size[0]);
@@ -195,7 +248,8 @@ static shader_t *make_shader(const yr_shader_desc &d, std::vector<texture_t *> &
         modu.ofsX(d.mod_ofs[0]);
         modu.ofsY(d.mod_ofs[1]);
         modu.ofsZ(d.mod_ofs[2]);
-        modu.string2modetype("mix");
+        static const char *modes[4] = {"mix", "mul", "add", "sub"};
+        modu.string2modetype(modes[d.mod_mode < 4 ? d.mod_mode : 0]);
         modu.color(d.mod_color);
         modu.specular(0);
         modu.hard(0);
@@ -623,6 +677,71 @@ static void cmd_noise(const char *pts_path, const char *out) {
     fclose(f);
 }
 
+// ---------------------------------------------------------- noise bases
+// Every noise basis of newNoise (basictex.cc:34-60) and turbulence
+// (noise.cc:808-819) over it, plus the voronoi texture's own metrics.
+// Output per point: 10 bases, then turbulence(basis, p, 3, 1.5, hard) for
+// hard = 0 / 1 per basis (20 values), then voronoi_t::getFeatures distances
+// da[0..3] for the 7 metrics (mk_exponent 2.5): 58 floats.
+static void cmd_noisegen(const char *pts_path, const char *out) {
+    FILE *fi = fopen(pts_path, "rb");
+    if (!fi) die("cannot open points");
+    uint32_t n;
+    rd(fi, &n, 4);
+    std::vector<float> pts(3 * (size_t)n);
+    if (n) rd(fi, &pts[0], 12 * (size_t)n);
+    fclose(fi);
+    noiseGenerator_t *gens[10];
+    for (int k = 0; k < 10; k++) gens[k] = newNoise(noise_name(k));
+    voronoi_t vor[7];
+    for (int k = 0; k < 7; k++) {
+        vor[k].setDistM((voronoi_t::dMetricType)k);
+        vor[k].setMinkovskyExponent(2.5);
+    }
+    FILE *f = fopen(out, "wb");
+    for (uint32_t i = 0; i < n; i++) {
+        const point3d_t p(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+        float v[58];
+        for (int k = 0; k < 10; k++) {
+            v[k] = (*gens[k])(p);
+            v[10 + 2 * k] = turbulence(gens[k], p, 3, 1.5, false);
+            v[11 + 2 * k] = turbulence(gens[k], p, 3, 1.5, true);
+        }
+        for (int k = 0; k < 7; k++) {
+            vor[k].getFeatures(p);
+            for (int j = 0; j < 4; j++) v[30 + 4 * k + j] = vor[k].getDistance(j);
+        }
+        wr(f, v, sizeof(v));
+    }
+    fclose(f);
+}
+
+// -------------------------------------------------------------- textures
+// Each textured shader's texture_t::getColor (rgb) and getFloat at the
+// given texture-space points: per shader, per point, 4 floats.
+static void cmd_texeval(const SceneFile &s, const char *pts_path, const char *out) {
+    FILE *fi = fopen(pts_path, "rb");
+    if (!fi) die("cannot open points");
+    uint32_t n;
+    rd(fi, &n, 4);
+    std::vector<float> pts(3 * (size_t)n);
+    if (n) rd(fi, &pts[0], 12 * (size_t)n);
+    fclose(fi);
+    FILE *f = fopen(out, "wb");
+    for (size_t k = 0; k < s.shaders.size(); k++) {
+        if (s.shaders[k].tex_type == YR_TEX_NONE) continue;
+        texture_t *tex = make_texture(s.shaders[k]);
+        for (uint32_t i = 0; i < n; i++) {
+            const point3d_t p(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+            const colorA_t c = tex->getColor(p);
+            const float v[4] = {c.getR(), c.getG(), c.getB(), tex->getFloat(p)};
+            wr(f, v, 16);
+        }
+        delete tex;
+    }
+    fclose(f);
+}
+
 // ------------------------------------------------------------------ halton
 static void cmd_halton(const char *out) {
     FILE *f = fopen(out, "wb");
@@ -657,6 +776,11 @@ int main(int argc, char **argv) {
         cmd_halton(argv[2]);
         return 0;
     }
+    if (cmd == "noisegen") {
+        if (argc < 4) die("noisegen POINTS OUT");
+        cmd_noisegen(argv[2], argv[3]);
+        return 0;
+    }
     SceneFile s;
     load_scene(argv[2], s);
     if (cmd == "tree") {
@@ -664,6 +788,9 @@ int main(int argc, char **argv) {
     } else if (cmd == "rays") {
         if (argc < 5) die("rays SCENE RAYS OUT");
         cmd_rays(s, argv[3], argv[4]);
+    } else if (cmd == "texeval") {
+        if (argc < 5) die("texeval SCENE POINTS OUT");
+        cmd_texeval(s, argv[3], argv[4]);
     } else if (cmd == "illum") {
         if (argc < 5) die("illum SCENE QUERIES OUT");
         cmd_illum(s, argv[3], argv[4]);

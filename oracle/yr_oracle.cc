@@ -17,6 +17,7 @@
 // kd-trees and object tree (yr_kdtree layout), so the traversal can be run
 // on the reference's own trees.
 #include <math.h>
+#include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -26,6 +27,7 @@
 #include <vector>
 
 #include "../include/yr.h"
+#include "../yafray_b200/csrc/noise_tables.h"
 
 namespace {
 
@@ -605,6 +607,410 @@ float turbulence(const V &pt, int oct, float size, bool hard) {
     return sum * ((float)(1 << oct) / (float)((1 << (oct + 1)) - 1));
 }
 
+// ---------------------------------------------------------- noise bases
+// Blender's feature-point and gradient tables (noise.cc:7-116, 129-187)
+const float kHashPnt[768] = YR_HASHPNT_INIT;
+const float kHashVect[768] = YR_HASHVECT_INIT;
+
+// stdPerlin_t::operator() (noise.cc:374-434) in the shipped build's
+// (-O3 -ffast-math) evaluation: t = x + 1e4 in float, each corner value
+// u = (q0*rx + q1*ry) + q2*rz and each lerp toward v formed as
+// ((v0 + v1) + (v2 - u)) * s + u; stdp_p / stdp_g repeat the permutation
+// and hashvectf with period 256
+float std_perlin(const V &pt) {
+    const float vec[3] = {pt.x, pt.y, pt.z};
+    int b0[3], b1[3];
+    float r0[3], r1[3], sv[3];
+    for (int k = 0; k < 3; k++) {
+        const float t = vec[k] + 10000.0f;
+        const int ti = (int)t;
+        b0[k] = ti & 255;
+        b1[k] = (b0[k] + 1) & 255;
+        r0[k] = t - (float)ti;
+        r1[k] = r0[k] - 1.0f;
+        sv[k] = (float)((double)(r0[k] * r0[k]) * (3.0 - (double)r0[k] * 2.0));
+    }
+    const int i = hsh(b0[0]), j = hsh(b1[0]);
+    const int b00 = hsh(i + b0[1]), b10 = hsh(j + b0[1]), b01 = hsh(i + b1[1]), b11 = hsh(j + b1[1]);
+    auto at = [](int g, float rx, float ry, float rz) {
+        const float *q = kHashVect + 3 * (g & 255);
+        return (q[0] * rx + q[1] * ry) + q[2] * rz;
+    };
+    auto lerp_to = [](int g, float rx, float ry, float rz, float u, float s) {
+        const float *q = kHashVect + 3 * (g & 255);
+        return ((q[0] * rx + q[1] * ry) + (q[2] * rz - u)) * s + u;
+    };
+    const float sx = sv[0], sy = sv[1], sz = sv[2];
+    float u = at(b00 + b0[2], r0[0], r0[1], r0[2]);
+    const float a0 = lerp_to(b10 + b0[2], r1[0], r0[1], r0[2], u, sx);
+    u = at(b01 + b0[2], r0[0], r1[1], r0[2]);
+    const float bb0 = lerp_to(b11 + b0[2], r1[0], r1[1], r0[2], u, sx);
+    const float c = (bb0 - a0) * sy + a0;
+    u = at(b00 + b1[2], r0[0], r0[1], r1[2]);
+    const float a1 = lerp_to(b10 + b1[2], r1[0], r0[1], r1[2], u, sx);
+    u = at(b01 + b1[2], r0[0], r1[1], r1[2]);
+    const float bb1 = lerp_to(b11 + b1[2], r1[0], r1[1], r1[2], u, sx);
+    const float d = (bb1 - a1) * sy + a1;
+    return (float)((double)((d - c) * sz + c) * 0.75 + 0.5);
+}
+
+// blenderNoise_t::operator() (noise.cc:439-510) in the shipped build's
+// evaluation: the corner weights cn in double as x*x*(2x - 3) + 1 and
+// 1 - x*x*(2x + 3), the four corners of each z layer summed as a vector
+// reduction ((v0 + v2) + (v1 + v3)) and scaled once by that layer's z
+// weight: n = cn6*R1 + (cn3*R0 + 0.5)
+float blender_noise(const V &pt) {
+    const float x = pt.x, y = pt.y, z = pt.z;
+    const int ix = (int)floorf(x), iy = (int)floorf(y), iz = (int)floorf(z);
+    const float ox = x - (float)ix, oy = y - (float)iy, oz = z - (float)iz;
+    const float jx = ox - 1.0f, jy = oy - 1.0f, jz = oz - 1.0f;
+    auto cn_o = [](float o) { return (float)((double)(o * o) * ((double)o * 2.0 - 3.0) + 1.0); };
+    auto cn_j = [](float j) { return (float)(1.0 - (double)(j * j) * ((double)j * 2.0 + 3.0)); };
+    const float cn1 = cn_o(ox), cn2 = cn_o(oy), cn3 = cn_o(oz), cn4 = cn_j(jx), cn5 = cn_j(jy), cn6 = cn_j(jz);
+    const int b00 = hsh(hsh(ix & 255) + (iy & 255)), b10 = hsh(hsh((ix + 1) & 255) + (iy & 255)),
+              b01 = hsh(hsh(ix & 255) + ((iy + 1) & 255)), b11 = hsh(hsh((ix + 1) & 255) + ((iy + 1) & 255));
+    const int b20 = iz & 255, b21 = (iz + 1) & 255;
+    auto g = [](int k, float a, float b, float c) {
+        const float *h = kHashVect + 3 * hsh(k);
+        return (h[0] * a + h[1] * b) + h[2] * c;
+    };
+    const float w0 = cn4 * cn5, w1 = cn2 * cn4, w2 = cn1 * cn5, w3 = cn1 * cn2;
+    const float R0 = (w0 * g(b20 + b11, jx, jy, oz) + w2 * g(b20 + b01, ox, jy, oz)) +
+                     (w1 * g(b20 + b10, jx, oy, oz) + w3 * g(b20 + b00, ox, oy, oz));
+    const float R1 = (w0 * g(b21 + b11, jx, jy, jz) + w2 * g(b21 + b01, ox, jy, jz)) +
+                     (w1 * g(b21 + b10, jx, oy, jz) + w3 * g(b21 + b00, ox, oy, jz));
+    float n = cn6 * R1 + (cn3 * R0 + 0.5f);
+    if (n > 1.0f) n = 1.0f;
+    if (n < 0.0f) n = 0.0f;
+    return n;
+}
+
+// the distance metrics of voronoi_t (noise.h:69-129), e = mk_exponent, as
+// the shipped build evaluates them (sums grouped x + (y + z); manhattan,
+// minkovsky 1/2, 4 and general in double)
+float vor_dist(int metric, float x, float y, float z, float e) {
+    switch (metric) {
+    case YR_DIST_SQUARED: return x * x + (y * y + z * z);
+    case YR_DIST_MANHATTAN: return (float)((double)fabsf(x) + ((double)fabsf(y) + (double)fabsf(z)));
+    case YR_DIST_CHEBYCHEV: {
+        x = fabsf(x);
+        y = fabsf(y);
+        z = fabsf(z);
+        const float t = (y > z) ? y : z;
+        return (x > t) ? x : t;
+    }
+    case YR_DIST_MINKOVSKY_HALF: {
+        const float d = (float)((sqrt((double)fabsf(x)) + sqrt((double)fabsf(y))) + sqrt((double)fabsf(z)));
+        return d * d;
+    }
+    case YR_DIST_MINKOVSKY_FOUR: {
+        const float x2 = x * x, y2 = y * y, z2 = z * z;
+        return (float)sqrt(sqrt((double)(x2 * x2 + (y2 * y2 + z2 * z2))));
+    }
+    case YR_DIST_MINKOVSKY: {
+        const double ed = (double)e;
+        return (float)pow((pow((double)fabsf(x), ed) + pow((double)fabsf(y), ed)) + pow((double)fabsf(z), ed),
+                          (double)(1.0f / e));
+    }
+    default: return sqrtf(x * x + (y * y + z * z));
+    }
+}
+
+const float *hashpnt(int x, int y, int z) {  // HASHPNT (noise.cc:6)
+    return kHashPnt + 3 * kPerm[(kPerm[(kPerm[z & 255] + y) & 255] + x) & 255];
+}
+
+// voronoi_t::getFeatures (noise.cc:550-589): the 4 nearest feature points
+struct Features {
+    float da[4];
+    V pa[4];
+};
+void vor_features(const V &pt, int metric, float mex, Features &F) {
+    const float x = pt.x, y = pt.y, z = pt.z;
+    const int xi = (int)floorf(x), yi = (int)floorf(y), zi = (int)floorf(z);
+    F.da[0] = F.da[1] = F.da[2] = F.da[3] = 1e10f;
+    for (int xx = xi - 1; xx <= xi + 1; xx++)
+        for (int yy = yi - 1; yy <= yi + 1; yy++)
+            for (int zz = zi - 1; zz <= zi + 1; zz++) {
+                const float *p = hashpnt(xx, yy, zz);
+                // (x - xx) - p[0]: the shipped build's grouping of x - (p[0] + xx)
+                const float xd = (x - (float)xx) - p[0], yd = (y - (float)yy) - p[1], zd = (z - (float)zz) - p[2];
+                const float d = vor_dist(metric, xd, yd, zd, mex);
+                const V fp(p[0] + (float)xx, p[1] + (float)yy, p[2] + (float)zz);
+                int k = 4;
+                while (k > 0 && d < F.da[k - 1]) k--;
+                if (k < 4) {
+                    for (int m = 3; m > k; m--) {
+                        F.da[m] = F.da[m - 1];
+                        F.pa[m] = F.pa[m - 1];
+                    }
+                    F.da[k] = d;
+                    F.pa[k] = fp;
+                }
+            }
+}
+
+// cellNoise_t::operator() (noise.cc:614-622)
+float cell_noise(const V &pt) {
+    const int xi = (int)floorf(pt.x), yi = (int)floorf(pt.y), zi = (int)floorf(pt.z);
+    unsigned int n = (unsigned)xi + (unsigned)yi * 1301u + (unsigned)zi * 314159u;
+    n ^= (n << 13);
+    return (float)((double)(float)(n * (n * n * 15731u + 789221u) + 1376312589u) / 4294967296.0);
+}
+
+// the basis of newNoise (basictex.cc:34-60)
+float noise_gen(uint32_t type, const V &p) {
+    switch (type) {
+    case YR_NOISE_STDPERLIN: return std_perlin(p);
+    case YR_NOISE_BLENDER: return blender_noise(p);
+    case YR_NOISE_VORONOI_F1:
+    case YR_NOISE_VORONOI_F2:
+    case YR_NOISE_VORONOI_F3:
+    case YR_NOISE_VORONOI_F4:
+    case YR_NOISE_VORONOI_F2F1:
+    case YR_NOISE_VORONOI_CRACKLE: {  // voronoi_t::operator() (noise.cc:591-611), real distance
+        Features F;
+        vor_features(p, YR_DIST_REAL, 2.5f, F);
+        switch (type) {
+        case YR_NOISE_VORONOI_F2: return F.da[1];
+        case YR_NOISE_VORONOI_F3: return F.da[2];
+        case YR_NOISE_VORONOI_F4: return F.da[3];
+        case YR_NOISE_VORONOI_F2F1: return F.da[1] - F.da[0];
+        case YR_NOISE_VORONOI_CRACKLE: {
+            const float t = (F.da[1] - F.da[0]) * 10.0f;
+            return (t > 1.0f) ? 1.0f : t;
+        }
+        default: return F.da[0];
+        }
+    }
+    case YR_NOISE_CELLNOISE: return cell_noise(p);
+    default: return perlin(p);
+    }
+}
+float signed_noise(uint32_t type, const V &p) { return (float)2.0 * noise_gen(type, p) - (float)1.0; }
+
+// turbulence (noise.cc:808-819) over any basis; only the blender basis
+// offsets the point (noiseGenerator_t::offset, noise.h:16-17, 55-63)
+float turbulence_gen(uint32_t type, const V &pt, int oct, float size, bool hard) {
+    float amp = 1, sum = 0;
+    const V q = type == YR_NOISE_BLENDER ? V(pt.x + 1.0f, pt.y + 1.0f, pt.z + 1.0f) : pt;
+    V tp(q.x * size, q.y * size, q.z * size);
+    for (int i = 0; i <= oct; i++, amp *= 0.5f, tp = V(tp.x * 2.0f, tp.y * 2.0f, tp.z * 2.0f)) {
+        float val = noise_gen(type, tp);
+        if (hard) val = (float)fabs(2.0 * (double)val - 1.0);
+        sum += amp * val;
+    }
+    return sum * ((float)(1 << oct) / (float)((1 << (oct + 1)) - 1));
+}
+
+// the musgrave generators (noise.cc:638-800) over basis `nt`, in the
+// shipped build's groupings: sn + offset as (offset - 1) + 2n, heteroterrain
+// value *= (sn + offset)*pwr + 1, hybrid weight = (gain*w)*signal, the
+// fractional octaves' products reordered as noted per case
+float musgrave(uint32_t kind, uint32_t nt, V tp, float H, float lac, float oct, float offset, float gain) {
+    const float pwHL = (float)pow((double)lac, (double)-H);
+    auto scale = [&](V &p) { p = V(p.x * lac, p.y * lac, p.z * lac); };
+    const float rmd = oct - floorf(oct);
+    switch (kind) {
+    case YR_TEX_MUSGRAVE_MULTIFRACTAL: {
+        float value = 1, pwr = 1;
+        for (int i = 0; i < (int)oct; i++) {
+            value *= (pwr * signed_noise(nt, tp) + (float)1.0);
+            pwr *= pwHL;
+            scale(tp);
+        }
+        if (rmd != (float)0.0) value *= ((rmd * pwr) * signed_noise(nt, tp) + (float)1.0);
+        return value;
+    }
+    case YR_TEX_MUSGRAVE_HETEROTERRAIN: {
+        auto sno = [&](const V &q) { return (offset - 1.0f) + noise_gen(nt, q) * 2.0f; };
+        float pwr = pwHL;
+        float value = noise_gen(nt, tp) * 2.0f + (offset - 1.0f);
+        scale(tp);
+        for (int i = 1; i < (int)oct; i++) {
+            value = (sno(tp) * pwr + 1.0f) * value;
+            pwr *= pwHL;
+            scale(tp);
+        }
+        if (rmd != (float)0.0) value = (pwr * value) * (sno(tp) * rmd) + value;
+        return value;
+    }
+    case YR_TEX_MUSGRAVE_HYBRIDMF: {
+        auto sno = [&](const V &q) { return (offset - 1.0f) + noise_gen(nt, q) * 2.0f; };
+        float pwr = pwHL;
+        float result = sno(tp);
+        float weight = gain * result;
+        scale(tp);
+        for (int i = 1; (weight > (float)0.001) && (i < (int)oct); i++) {
+            const float w = weight > 1.0f ? 1.0f : weight;
+            const float signal = sno(tp) * pwr;
+            pwr *= pwHL;
+            result = signal * w + result;
+            weight = (gain * w) * signal;
+            scale(tp);
+        }
+        if (rmd != (float)0.0) result = sno(tp) * (rmd * pwr) + result;
+        return result;
+    }
+    case YR_TEX_MUSGRAVE_RIDGEDMF: {
+        float pwr = pwHL;
+        float signal = offset - fabsf(signed_noise(nt, tp));
+        signal *= signal;
+        float result = signal;
+        for (int i = 1; i < (int)oct; i++) {
+            scale(tp);
+            float weight = gain * signal;
+            weight = weight > 0.0f ? weight : 0.0f;
+            weight = weight < 1.0f ? weight : 1.0f;
+            const float q = offset - fabsf(signed_noise(nt, tp));
+            signal = weight * (q * q);
+            result = signal * pwr + result;
+            pwr = pwHL * pwr;
+        }
+        return result;
+    }
+    default: {  // fBm
+        float value = 0, pwr = 1;
+        for (int i = 0; i < (int)oct; i++) {
+            value += signed_noise(nt, tp) * pwr;
+            pwr *= pwHL;
+            scale(tp);
+        }
+        if (rmd != 0.f) value += rmd * signed_noise(nt, tp) * pwr;
+        return value;
+    }
+    }
+}
+
+C col3(const float *p) { return C(p[0], p[1], p[2]); }
+
+// marble / wood wave shapes (basictex.cc:124-140, 199-214)
+float wave(uint32_t shape, float w) {
+    if (shape == YR_WAVE_SAW) {
+        w *= (float)(0.5 * M_1_PI);
+        w -= floorf(w);
+    } else if (shape == YR_WAVE_TRI) {
+        w *= (float)(0.5 * M_1_PI);
+        w = fabsf((float)2.0 * (w - floorf(w)) - (float)1.0);
+    } else {
+        w = (sinf(w) + 1.0f) * 0.5f;  // the shipped build's form of 0.5 + 0.5*sin(w)
+    }
+    return w;
+}
+
+// A texture's value: getFloat, and getColor (rgb) at texture point p.
+struct TexVal {
+    float f;
+    C col;
+};
+TexVal texture_eval(const yr_shader_desc &d, const V &p) {
+    TexVal r;
+    const C c1 = col3(d.tex_color1), c2 = col3(d.tex_color2);
+    const V ps(p.x * d.tex_size, p.y * d.tex_size, p.z * d.tex_size);
+    switch (d.tex_type) {
+    case YR_TEX_CLOUDS: {  // textureClouds_t::getFloat (basictex.cc:76-85)
+        float v = turbulence_gen(d.tex_noise, p, d.tex_depth, d.tex_size, d.tex_hard != 0);
+        if (d.tex_variant == 1 || d.tex_variant == 2) {
+            v *= v;
+            if (d.tex_variant == 1) v = -v;
+        }
+        r.f = v;
+        break;
+    }
+    case YR_TEX_MARBLE: {  // textureMarble_t::getFloat (basictex.cc:122-146)
+        const float sharp = d.tex_sharpness > 1 ? (float)(1.0 / (double)d.tex_sharpness) : 1.0f;
+        const double tu = d.tex_turbulence == 0.0f
+                              ? 0.0
+                              : (double)(d.tex_turbulence *
+                                         turbulence_gen(d.tex_noise, p, d.tex_depth, d.tex_size, d.tex_hard != 0));
+        const float w = (float)((double)(p.x + p.y + p.z) * 5.0 + tu);
+        r.f = powf(wave(d.tex_shape, w), sharp);
+        break;
+    }
+    case YR_TEX_WOOD: {  // textureWood_t::getFloat (basictex.cc:192-216)
+        float w = d.tex_variant ? sqrtf(p.x * p.x + p.y * p.y + p.z * p.z) * 20.0f : (p.x + p.y + p.z) * 10.0f;
+        const double tu = d.tex_turbulence == 0.0f
+                              ? 0.0
+                              : (double)(d.tex_turbulence *
+                                         turbulence_gen(d.tex_noise, p, d.tex_depth, d.tex_size, d.tex_hard != 0));
+        w = (float)((double)w + tu);
+        r.f = wave(d.tex_shape, w);
+        break;
+    }
+    case YR_TEX_VORONOI: {  // textureVoronoi_t (basictex.cc:560-617)
+        const float aw[4] = {fabsf(d.tex_weights[0]), fabsf(d.tex_weights[1]), fabsf(d.tex_weights[2]),
+                             fabsf(d.tex_weights[3])};
+        float iscale = aw[0] + aw[1] + aw[2] + aw[3];
+        if (iscale != 0) iscale = d.tex_intensity / iscale;
+        Features F;
+        vor_features(ps, (int)d.tex_metric, d.tex_mk_exponent, F);
+        // the weighted sum as the shipped build's vector reduction
+        const float inte = iscale * fabsf((d.tex_weights[0] * F.da[0] + d.tex_weights[2] * F.da[2]) +
+                                          (d.tex_weights[1] * F.da[1] + d.tex_weights[3] * F.da[3]));
+        r.f = inte;
+        if (d.tex_shape == 0) {
+            r.col = C(inte, inte, inte);
+        } else {
+            C col;
+            for (int k = 0; k < 4; k++) {  // cellNoiseColor (noise.cc:795-803)
+                const float *cl = hashpnt((int)floorf(F.pa[k].x), (int)floorf(F.pa[k].y), (int)floorf(F.pa[k].z));
+                col = col + C(aw[k] * cl[0], aw[k] * cl[1], aw[k] * cl[2]);
+            }
+            if (d.tex_shape >= 2) {
+                const float dd = F.da[1] - F.da[0];
+                float t1 = dd > 0.1f ? 1.0f : dd * 10.0f;  // the shipped build's form
+                if (d.tex_shape == 3) t1 *= inte;
+                else t1 *= iscale;
+                col = col * t1;
+            } else {
+                col = col * iscale;
+            }
+            r.col = col;
+        }
+        return r;
+    }
+    case YR_TEX_DISTORTED_NOISE: {  // textureDistortedNoise_t::getFloat (basictex.cc:721-727)
+        const V rv(signed_noise(d.tex_noise, V(ps.x + 13.5f, ps.y + 13.5f, ps.z + 13.5f)),
+                   signed_noise(d.tex_noise, ps), signed_noise(d.tex_noise, V(ps.x - 13.5f, ps.y - 13.5f, ps.z - 13.5f)));
+        r.f = signed_noise(d.tex_noise2, V(ps.x + rv.x * d.tex_distort, ps.y + rv.y * d.tex_distort,
+                                           ps.z + rv.z * d.tex_distort));
+        break;
+    }
+    case YR_TEX_GRADIENT: {  // textureGradient_t::getFloat (basictex.cc:772-800)
+        const float x = d.tex_variant ? p.y : p.x, y = d.tex_variant ? p.x : p.y;
+        float gr;
+        switch (d.tex_shape) {
+        case YR_GRAD_QUADRATIC:
+            gr = (float)((1.0 + (double)x) * 0.5);
+            r.f = gr < 0 ? 0.f : gr * gr;
+            break;
+        case YR_GRAD_CUBIC:
+            gr = (float)((1.0 + (double)x) * 0.5);
+            if (gr > 1) {  // getColor folds color1 + 1*(color2 - color1) to color2 in the shipped build
+                r.f = 1.f;
+                r.col = c2;
+                return r;
+            }
+            r.f = gr < 0 ? 0.f : (float)((double)(gr * gr) * (3.0 - 2.0 * (double)gr));
+            break;
+        case YR_GRAD_DIAGONAL: r.f = (float)(((double)x + (double)y + 2.0) * 0.25); break;
+        case YR_GRAD_SPHERE:
+        case YR_GRAD_HALO:
+            gr = (float)(1.0 - (double)sqrtf(x * x + y * y + p.z * p.z));
+            r.f = gr < 0 ? 0.f : (d.tex_shape == YR_GRAD_HALO ? gr * gr : gr);
+            break;
+        default: r.f = (float)((1.0 + (double)x) * 0.5);
+        }
+        break;
+    }
+    default:  // musgrave: iscale * generator(p * size) (basictex.cc:677-680)
+        r.f = d.tex_intensity *
+              musgrave(d.tex_type, d.tex_noise, ps, d.tex_H, d.tex_lacunarity, d.tex_octaves, d.tex_offset, d.tex_gain);
+    }
+    r.col = c1 + r.f * (c2 - c1);
+    return r;
+}
+
 // --------------------------------------------------------------- shading
 struct SP {
     V P, N, Ng, NU, NV;
@@ -661,16 +1067,12 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from, const 
     return s;
 }
 
-C col3(const float *p) { return C(p[0], p[1], p[2]); }
 
-// modulator "mix" of a musgrave/clouds texture into the diffuse colour
-C diffuse(const Scene &S, const SP &sp) {
-    const yr_shader_desc &d = S.shaders[sp.shader];
-    C c = col3(d.color);
-    if (d.tex_type == YR_TEX_NONE || !(d.mod_color > 0)) return c;
-    // modulator_t::doMapping, procedural path (texture.cc:122-320): texco
-    // "global" / "orco" (an untransformed mesh without orco data: P) or
-    // "normal", then projections size*(src[axis] + ofs) / size*ofs
+// the modulator's texture point (modulator_t::doMapping, texture.cc:122-320,
+// procedural path): texco "global" / "orco" (an untransformed mesh without
+// orco data: P) or "normal", then projections size*(src[axis] + ofs) /
+// size*ofs
+V tex_point(const yr_shader_desc &d, const SP &sp) {
     const V src = (d.tex_map & 0xffu) == YR_TEXCO_NORMAL ? sp.N : sp.P;
     float t[3];
     for (int k = 0; k < 3; k++) {
@@ -678,17 +1080,30 @@ C diffuse(const Scene &S, const SP &sp) {
         const int a = pc == YR_PROJ_DEFAULT ? k : (pc >= YR_PROJ_X && pc <= YR_PROJ_Z ? (int)pc - 1 : -1);
         t[k] = a < 0 ? d.mod_size[k] * d.mod_ofs[k] : d.mod_size[k] * (src[a] + d.mod_ofs[k]);
     }
-    V tp(t[0], t[1], t[2]);
-    float f;
-    if (d.tex_type == YR_TEX_MUSGRAVE_FBM)
-        f = d.tex_intensity * fbm(V(tp.x * d.tex_size, tp.y * d.tex_size, tp.z * d.tex_size), d.tex_H,
-                                  d.tex_lacunarity, d.tex_octaves);
-    else
-        f = turbulence(tp, d.tex_depth, d.tex_size, d.tex_hard != 0);
-    C tex = col3(d.tex_color1) + f * (col3(d.tex_color2) - col3(d.tex_color1));
-    float w = d.mod_color;
-    if (w > 1.0f) return tex;
-    return tex * w + (1 - w) * c;
+    return V(t[0], t[1], t[2]);
+}
+
+// mix(a, b, point) (color.cc:103-109)
+C mixc(const C &a, const C &b, float w) {
+    if (w < 0.0) return b;
+    if (w > 1.0) return a;
+    return a * w + (1 - w) * b;
+}
+
+// the diffuse colour after the modulator (modulator_t::modulate,
+// texture.cc:499-534, colour channel; modes mix / mul / add / sub)
+C diffuse(const Scene &S, const SP &sp) {
+    const yr_shader_desc &d = S.shaders[sp.shader];
+    C c = col3(d.color);
+    if (d.tex_type == YR_TEX_NONE || !(d.mod_color > 0)) return c;
+    const C tex = texture_eval(d, tex_point(d, sp)).col;
+    const float w = d.mod_color;
+    switch (d.mod_mode) {
+    case YR_MOD_MUL: return mixc(tex, C(1, 1, 1), w) * c;
+    case YR_MOD_ADD: return (tex * w) + c;
+    case YR_MOD_SUB: return (tex * -w) + c;
+    default: return mixc(tex, c, w);
+    }
 }
 
 // genericShader_t::fromLight (basicshaders.cc:46-70)
@@ -872,13 +1287,16 @@ void make_camera(const yr_camera_desc &c, Cam &o) {
     float vl = vto * vto;
     if (vl != 0) {
         vl = sqrtf(vl);
-        const float d = (float)(1.0 / vl);
+        const float d = 1.0f / vl;  // the shipped build divides in float
         vto = V(vto.x * d, vto.y * d, vto.z * d);
     }
-    vup = vup * (c.aspect * (float)c.resy / (float)c.resx);
+    // the shipped build (-ffast-math) multiplies by the reciprocals of
+    // resx and resy: vup *= (resy*aspect) * (1/resx), vup *= 1/resy, vright *= 1/resx
+    const float rx = 1.0f / (float)c.resx, ry = 1.0f / (float)c.resy;
+    vup = vup * (((float)c.resy * c.aspect) * rx);
     vto = (vto * c.focal) - 0.5f * (vup + vright);
-    vup = vup / (float)c.resy;
-    vright = vright / (float)c.resx;
+    vup = vup * ry;
+    vright = vright * rx;
     o.pos = pos;
     o.vright = vright;
     o.vup = vup;
@@ -1000,9 +1418,12 @@ orc_scene *orc_load(const char *path) {
     yr_camera_desc cam;
     bool ok = rdv(f, magic, 4) && memcmp(magic, "YRS1", 4) == 0 && rdv(f, hdr, 4) && rdv(f, &cam, 1) &&
               rdv(f, &S.rp, 1);
-    S.shaders.resize(hdr[1]);
+    S.shaders.assign(hdr[1], yr_shader_desc());
     std::vector<yr_light_desc> ld(hdr[2]);
-    ok = ok && rdv(f, S.shaders.data(), hdr[1]) && rdv(f, ld.data(), hdr[2]);
+    // shader records before version 2 end at mod_mode
+    const size_t shsize = hdr[3] >= 2 ? sizeof(yr_shader_desc) : offsetof(yr_shader_desc, mod_mode);
+    for (uint32_t i = 0; ok && i < hdr[1]; i++) ok = fread(&S.shaders[i], 1, shsize, f) == shsize;
+    ok = ok && rdv(f, ld.data(), hdr[2]);
     S.objs.resize(hdr[0]);
     for (uint32_t i = 0; ok && i < hdr[0]; i++) {
         uint32_t oh[4];
@@ -1251,6 +1672,24 @@ float orc_halton(uint32_t base, uint32_t n) { return halton(base, n); }
 float orc_ri_lp(uint32_t i) { return ri_lp(i); }
 float orc_cp_rot(uint32_t seed, uint32_t pixel, uint32_t dim) { return cp_rot(seed, pixel, dim); }
 float orc_perlin(float x, float y, float z) { return perlin(V(x, y, z)); }
+float orc_noise_gen(uint32_t type, float x, float y, float z) { return noise_gen(type, V(x, y, z)); }
+float orc_turbulence_gen(uint32_t type, float x, float y, float z, int oct, float size, int hard) {
+    return turbulence_gen(type, V(x, y, z), oct, size, hard != 0);
+}
+// voronoi_t::getFeatures distances da[0..3] under `metric`
+void orc_vor_features(int metric, float mex, float x, float y, float z, float *da) {
+    Features F;
+    vor_features(V(x, y, z), metric, mex, F);
+    for (int k = 0; k < 4; k++) da[k] = F.da[k];
+}
+// a shader record's texture at texture point (x, y, z): getColor rgb, getFloat
+void orc_texture(const yr_shader_desc *d, float x, float y, float z, float *out) {
+    const TexVal t = texture_eval(*d, V(x, y, z));
+    out[0] = t.col.r;
+    out[1] = t.col.g;
+    out[2] = t.col.b;
+    out[3] = t.f;
+}
 float orc_fbm(float x, float y, float z, float H, float lac, float oct) { return fbm(V(x, y, z), H, lac, oct); }
 float orc_turbulence(float x, float y, float z, int oct, float size, int hard) {
     return turbulence(V(x, y, z), oct, size, hard != 0);

@@ -20,7 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 import yrtest as T  # noqa: E402
-from yafray_b200 import scenes  # noqa: E402
+from yafray_b200 import abi, scenes  # noqa: E402
 
 
 def small_sphere_scene():
@@ -182,6 +182,138 @@ def illum():
     np.savez_compressed(os.path.join(HERE, "illum.npz"), **out)
 
 
+def texture_shaders():
+    """One shader per texture configuration: every noise basis under clouds,
+    the marble / wood shapes and variants, voronoi under every metric and
+    colour type, the musgrave types over three bases and fractional
+    octaves, distorted noise and the gradient types."""
+    ts, c1, c2 = scenes.texture_shader, (0.1, 0.3, 0.8), (0.9, 0.6, 0.2)
+    out = []
+    for nt in abi.NOISE_TYPES:
+        out.append(ts((0.5,) * 3, "clouds", c1, c2, noise_type=nt, depth=3, size=1.3))
+    out += [ts((0.5,) * 3, "clouds", c1, c2, hard=True, bias="positive", depth=2),
+            ts((0.5,) * 3, "clouds", c1, c2, bias="negative", noise_type="blender")]
+    for sh in ("sin", "saw", "tri"):
+        out.append(ts((0.5,) * 3, "marble", c1, c2, shape=sh, turbulence=2.5, sharpness=3.0, depth=3, size=0.7))
+        out.append(ts((0.5,) * 3, "wood", c1, c2, shape=sh, wood_type="rings", turbulence=1.5,
+                      noise_type="stdperlin"))
+        out.append(ts((0.5,) * 3, "wood", c1, c2, shape=sh, hard=True, turbulence=0.5))
+    out.append(ts((0.5,) * 3, "marble", c1, c2, turbulence=0.0))
+    for m in abi.DIST_METRICS:
+        for ct in ("int", "col1", "col2", "col3"):
+            out.append(ts((0.5,) * 3, "voronoi", c1, c2, color_type=ct, distance_metric=m, weight1=1.0, weight2=-0.5,
+                          weight3=0.3, weight4=0.2, intensity=1.7, size=2.0, mk_exponent=1.7))
+    for mt in ("fBm", "multifractal", "heteroterrain", "hybridmf", "ridgedmf"):
+        for nt in ("newperlin", "blender", "voronoi_f2f1"):
+            for oc in (3.0, 4.5):
+                out.append(ts((0.5,) * 3, "musgrave", c1, c2, type=mt, noise_type=nt, octaves=oc, H=0.8,
+                              lacunarity=2.2, offset=0.9, gain=1.7, size=1.4, intensity=0.6))
+    for n1, n2 in (("newperlin", "stdperlin"), ("voronoi_crackle", "blender"), ("cellnoise", "newperlin")):
+        out.append(ts((0.5,) * 3, "distorted_noise", c1, c2, noise_type1=n1, noise_type2=n2, distort=2.2, size=1.1))
+    for gt in abi.GRADIENT_TYPES:
+        for fl in (False, True):
+            out.append(ts((0.5,) * 3, "gradient", c1, c2, gradient_type=gt, flip_xy=fl))
+    return out
+
+
+def texture_points():
+    rng = np.random.default_rng(3)
+    return np.concatenate([rng.uniform(-1.5, 1.5, (96, 3)), rng.uniform(-40, 40, (32, 3))]).astype(np.float32)
+
+
+def textures():
+    """noise bases (newNoise, turbulence, voronoi metrics) and every texture
+    configuration's getColor / getFloat, from the reference."""
+    pts = texture_points()
+    sc = scenes.config_small(8, 8)
+    sc.shaders = texture_shaders()
+    with tempfile.TemporaryDirectory() as d:
+        sp, pp, op, np_ = (os.path.join(d, n) for n in ("s.yrs", "p.bin", "t.bin", "n.bin"))
+        scenes.write_yrs(sc, sp)
+        with open(pp, "wb") as f:
+            f.write(struct.pack("<I", len(pts)))
+            f.write(pts.tobytes())
+        T.run_harness("texeval", sp, pp, op)
+        tex = np.fromfile(op, np.float32).reshape(len(sc.shaders), len(pts), 4)
+        T.run_harness("noisegen", pp, np_)
+        gen = np.fromfile(np_, np.float32).reshape(len(pts), 58)
+    np.savez_compressed(os.path.join(HERE, "textures.npz"), pts=pts, tex=tex, noisegen=gen)
+
+
+def texture_scene():
+    """A 4 x 3 grid of small spheres, each with another texture, noise basis
+    and modulator mode, on a plane with a voronoi colour texture; two point
+    lights."""
+    sc = scenes.config_small(128, 96)
+    ts = scenes.texture_shader
+    sc.shaders = [
+        ts((0.6, 0.6, 0.6), "marble", (0.9, 0.9, 0.85), (0.2, 0.2, 0.3), mod_color=0.9, shape="sin", turbulence=3.0,
+           sharpness=2.0, depth=3, size=2.0),
+        ts((0.7, 0.5, 0.3), "wood", (0.5, 0.3, 0.1), (0.8, 0.6, 0.3), mode="mul", mod_color=0.8, wood_type="rings",
+           shape="tri", noise_type="stdperlin", turbulence=0.8),
+        ts((0.3, 0.3, 0.3), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mode="add", mod_color=0.5, color_type="col2",
+           distance_metric="manhattan", weight1=1.0, weight2=-0.6, size=4.0),
+        ts((0.5, 0.5, 0.6), "musgrave", (0.2, 0.4, 0.1), (0.9, 0.9, 0.7), type="ridgedmf", noise_type="blender",
+           octaves=4.0, H=1.0, offset=1.0, gain=2.0, size=2.5, intensity=0.5),
+        ts((0.5, 0.5, 0.5), "musgrave", (0.3, 0.2, 0.1), (0.8, 0.7, 0.9), type="hybridmf", noise_type="voronoi_f1",
+           octaves=3.5, H=0.25, offset=0.7, gain=1.0, size=1.5, intensity=0.8, mod_color=0.7),
+        ts((0.8, 0.8, 0.8), "musgrave", (0.1, 0.1, 0.1), (0.6, 0.5, 0.4), mode="sub", mod_color=0.4,
+           type="heteroterrain", noise_type="cellnoise", octaves=3.0, offset=0.5, size=3.0, intensity=0.4),
+        ts((0.4, 0.6, 0.5), "musgrave", (0.9, 0.2, 0.2), (0.2, 0.2, 0.9), type="multifractal", noise_type="stdperlin",
+           octaves=5.0, H=0.7, size=2.0, intensity=0.5, texco="normal"),
+        ts((0.5, 0.5, 0.5), "distorted_noise", (0.1, 0.5, 0.2), (0.9, 0.8, 0.1), noise_type1="voronoi_crackle",
+           noise_type2="newperlin", distort=1.5, size=2.0, mod_color=0.9),
+        ts((0.5, 0.4, 0.3), "gradient", (0.0, 0.0, 0.2), (1.0, 0.9, 0.6), gradient_type="halo", texco="normal",
+           mode="mul", mod_color=1.0),
+        ts((0.6, 0.6, 0.6), "clouds", (0.2, 0.3, 0.6), (0.9, 0.9, 0.9), noise_type="blender", bias="negative",
+           depth=4, size=0.8, hard=True, mod_color=0.8),
+        ts((0.5, 0.5, 0.5), "gradient", (0.2, 0.2, 0.2), (0.9, 0.8, 0.3), gradient_type="cubic", flip_xy=True,
+           proj=("y", "n", "x"), mod_color=0.95),
+        ts((0.5, 0.6, 0.4), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mode="mix", mod_color=0.6,
+           color_type="int", distance_metric="minkovsky", mk_exponent=3.5, weight1=0.5, weight2=0.5, size=3.0,
+           intensity=1.2),
+        ts((0.7, 0.7, 0.7), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mod_color=0.7, color_type="col3",
+           distance_metric="minkovsky_half", weight1=1.0, weight2=-1.0, size=1.0, intensity=2.0),
+    ]
+    meshes = []
+    for k in range(12):
+        v, t = scenes.uv_sphere((-1.8 + 1.2 * (k % 4), -0.5, -1.0 + 1.1 * (k // 4)), 0.5, rings=12, segments=24)
+        meshes.append(scenes.Mesh(v, t, k))
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    meshes.append(scenes.Mesh(pv, pt, 12))
+    sc.meshes = meshes
+    sc.lights = [scenes.point_light((2.0, 4.0, 3.0), 14.0), scenes.point_light((-3.0, 3.0, -1.0), 6.0,
+                                                                               color=(0.8, 0.9, 1.0))]
+    sc.camera = scenes.camera((0.0, 3.0, 4.5), (0.0, -0.5, 0.0), (0.0, 4.0, 4.5), 128, 96)
+    return sc
+
+
+def texture_board():
+    """Every texture configuration of texture_shaders() on its own quad of a
+    10 x 10 board (per-triangle materials), seen from above, point light."""
+    shs = texture_shaders()
+    n = len(shs)
+    verts, tris, tsh = [], [], []
+    for k in range(n):
+        x0, z0 = -5.0 + (k % 10), -5.0 + (k // 10)
+        b = len(verts)
+        verts += [(x0, 0.0, z0), (x0 + 1.0, 0.0, z0), (x0 + 1.0, 0.0, z0 + 1.0), (x0, 0.0, z0 + 1.0)]
+        tris += [(b, b + 2, b + 1), (b, b + 3, b + 2)]
+        tsh += [k, k]
+    sc = scenes.config_small(160, 160)
+    sc.shaders = shs
+    sc.meshes = [scenes.Mesh(np.array(verts, np.float32), np.array(tris, np.uint32), abi.YR_PER_TRIANGLE,
+                             np.array(tsh, np.uint32))]
+    sc.lights = [scenes.point_light((0.5, 6.0, 1.0), 40.0)]
+    sc.camera = scenes.camera((0.0, 9.0, 0.01), (0.0, 0.0, 0.0), (0.0, 10.0, 0.01), 160, 160, fov_deg=65.0)
+    return sc
+
+
+def texture_render():
+    img, _ = T.harness_render(texture_scene())
+    np.savez_compressed(os.path.join(HERE, "render_textures_128x96.npz"), image=img)
+
+
 def halton_noise():
     with tempfile.TemporaryDirectory() as d:
         hp = os.path.join(d, "h.bin")
@@ -206,6 +338,8 @@ if __name__ == "__main__":
     rays()
     camera_and_render()
     smooth_render()
+    textures()
+    texture_render()
     illum()
     halton_noise()
     for f in sorted(os.listdir(HERE)):

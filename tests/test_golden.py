@@ -1,5 +1,6 @@
 """The CPU oracle and the host-side builders against golden vectors produced
 by the unmodified reference (tests/golden/make_golden.py)."""
+import ctypes as C
 import os
 import sys
 
@@ -143,6 +144,62 @@ def test_oracle_light_estimators_match_reference(name):
     assert (np.abs(rgb - ref) <= tol).all(), np.abs(rgb - ref).max()
     for k in range(len(sc.lights)):  # every light contributes somewhere
         assert (ref[q["light"] == k].sum(1) > 0).any()
+
+
+def test_oracle_noise_bases_match_reference():
+    """Every noise basis of newNoise (stdperlin, blender, voronoi F1-F4 /
+    F2-F1 / crackle, cellnoise, newperlin), turbulence over each (soft and
+    hard, with the blender offset) and voronoi_t::getFeatures under all
+    seven distance metrics: bit-identical to the reference."""
+    g = load("textures.npz")
+    pts, ref = g["pts"], g["noisegen"]
+    lib = T.oracle()
+    out = np.zeros_like(ref)
+    da = np.zeros(4, np.float32)
+    for i, (x, y, z) in enumerate(pts.astype(np.float64)):
+        for k in range(10):
+            out[i, k] = lib.orc_noise_gen(k, x, y, z)
+            out[i, 10 + 2 * k] = lib.orc_turbulence_gen(k, x, y, z, 3, 1.5, 0)
+            out[i, 11 + 2 * k] = lib.orc_turbulence_gen(k, x, y, z, 3, 1.5, 1)
+        for m in range(7):
+            lib.orc_vor_features(m, 2.5, x, y, z, T.ptr(da))
+            out[i, 30 + 4 * m:34 + 4 * m] = da
+    assert np.array_equal(out, ref)
+
+
+def test_oracle_textures_match_reference():
+    """getColor / getFloat of every texture configuration (clouds over each
+    basis and bias, marble / wood shapes, voronoi metrics x colour types,
+    the five musgrave types over three bases with fractional octaves,
+    distorted noise, the six gradient types): bit-identical."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    g = load("textures.npz")
+    pts, ref = g["pts"], g["tex"]
+    shaders = make_golden.texture_shaders()
+    assert ref.shape[0] == len(shaders)
+    lib = T.oracle()
+    o = np.zeros(4, np.float32)
+    for k, sh in enumerate(shaders):
+        out = np.zeros((len(pts), 4), np.float32)
+        for i, (x, y, z) in enumerate(pts.astype(np.float64)):
+            lib.orc_texture(C.addressof(sh), x, y, z, T.ptr(o))
+            out[i] = o
+        assert np.array_equal(out, ref[k]), k
+
+
+def test_oracle_texture_render_matches_reference():
+    """Twelve textures with the mix / mul / add / sub modulator modes,
+    normal texco and switched projections, rendered by the reference and by
+    the oracle (the camera of this view is also where the reciprocal forms
+    of camera_t's divisions show)."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    ref = load("render_textures_128x96.npz")["image"]
+    img, _ = T.OracleScene(make_golden.texture_scene()).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
 
 
 def test_oracle_halton_and_ri_match_reference():

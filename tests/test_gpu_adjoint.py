@@ -186,3 +186,29 @@ def test_inverse_fit_recovers_parameters(cuda):
     params, hist, secs = optim.fit(dss, targets, steps=60, lr=2e-2, batched=True, streams=2)
     for i in range(len(dss)):
         assert hist[-1, i] < 0.2 * hist[0, i]
+
+
+def test_grad_procedural_textures_and_modes(cuda):
+    """Texture amplitude and base colour through ridged musgrave (mix),
+    voronoi cell colours (add), marble (mul) and clouds (sub), point and area
+    light."""
+    import torch
+    ts = scenes.texture_shader
+    sc = scenes.config_small(48, 36)
+    sc.shaders = [ts((0.6, 0.5, 0.4), "musgrave", (0.2, 0.4, 0.1), (0.9, 0.9, 0.7), mod_color=0.7, type="ridgedmf",
+                     noise_type="blender", octaves=3.0, offset=1.0, gain=2.0, size=2.0, intensity=0.6),
+                  ts((0.3, 0.3, 0.3), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mode="add", mod_color=0.5,
+                     color_type="col2", weight1=1.0, weight2=-0.6, size=3.0, intensity=0.8)]
+    sv, st = scenes.uv_sphere((1.3, 0.0, 0.0), 0.6, rings=16, segments=32)
+    tv, tt = scenes.uv_sphere((-1.3, 0.0, 0.0), 0.6, rings=16, segments=32)
+    sc.shaders += [ts((0.7, 0.6, 0.5), "marble", (0.9, 0.9, 0.8), (0.3, 0.2, 0.2), mode="mul", mod_color=0.8,
+                      turbulence=2.0, depth=2, size=1.5),
+                   ts((0.8, 0.8, 0.8), "clouds", (0.1, 0.2, 0.3), (0.5, 0.4, 0.3), mode="sub", mod_color=0.4,
+                      noise_type="stdperlin", depth=3, size=1.2)]
+    sc.meshes[0].shader = 0
+    sc.meshes[1].shader = 1
+    sc.meshes += [scenes.Mesh(sv, st, 2), scenes.Mesh(tv, tt, 3)]
+    sc.lights = [scenes.point_light((3.0, 5.0, 2.0), 20.0), scenes.quad_light_down(0.0, 4.0, 1.0, 2.0, 2.0, 20.0, 4)]
+    sc.render.spp = 2
+    ds, g, fd = _check(torch, sc, _hidden(5), nsample=20, rtol=1e-3, seed=1)
+    assert ds.param_count() == 4 * 8 + 2

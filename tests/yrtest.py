@@ -44,6 +44,10 @@ def oracle() -> C.CDLL:
             "orc_render": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
             "orc_camera_rays": (None, [P, P]),
             "orc_illum": (C.c_int, [P, U, P, P, P, U, P, P]),
+            "orc_noise_gen": (F, [U, F, F, F]),
+            "orc_turbulence_gen": (F, [U, F, F, F, C.c_int, F, C.c_int]),
+            "orc_vor_features": (None, [C.c_int, F, F, F, F, P]),
+            "orc_texture": (None, [P, F, F, F, P]),
             "orc_halton": (F, [U, U]),
             "orc_ri_lp": (F, [U]),
             "orc_cp_rot": (F, [U, U, U]),

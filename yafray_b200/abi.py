@@ -22,7 +22,18 @@ STATUS_NAMES = {
     10: "YR_ERR_NO_DEVICE", 11: "YR_ERR_TOO_LARGE",
 }
 
-YR_TEX_NONE, YR_TEX_MUSGRAVE_FBM, YR_TEX_CLOUDS = 0, 1, 2
+YR_TEX_NONE, YR_TEX_MUSGRAVE_FBM, YR_TEX_CLOUDS, YR_TEX_MARBLE, YR_TEX_WOOD, YR_TEX_VORONOI = 0, 1, 2, 3, 4, 5
+(YR_TEX_MUSGRAVE_MULTIFRACTAL, YR_TEX_MUSGRAVE_HETEROTERRAIN, YR_TEX_MUSGRAVE_HYBRIDMF,
+ YR_TEX_MUSGRAVE_RIDGEDMF) = 6, 7, 8, 9
+YR_TEX_DISTORTED_NOISE, YR_TEX_GRADIENT = 10, 11
+# noise_type names in newNoise order (basictex.cc:34-60) -> YR_NOISE_*
+NOISE_TYPES = {"newperlin": 0, "stdperlin": 1, "blender": 2, "voronoi_f1": 3, "voronoi_f2": 4, "voronoi_f3": 5,
+               "voronoi_f4": 6, "voronoi_f2f1": 7, "voronoi_crackle": 8, "cellnoise": 9}
+WAVE_SHAPES = {"sin": 0, "saw": 1, "tri": 2}
+DIST_METRICS = {"real": 0, "squared": 1, "manhattan": 2, "chebychev": 3, "minkovsky_half": 4,
+                "minkovsky_four": 5, "minkovsky": 6}
+GRADIENT_TYPES = {"linear": 0, "quadratic": 1, "cubic": 2, "diagonal": 3, "sphere": 4, "halo": 5}
+MOD_MODES = {"mix": 0, "mul": 1, "add": 2, "sub": 3}
 YR_LIGHT_POINT, YR_LIGHT_AREA, YR_LIGHT_HEMI, YR_LIGHT_PATH = 0, 1, 2, 3
 YR_BATCH_AUTO, YR_BATCH_TILES, YR_BATCH_WAVES = 0, 1, 2
 YR_TEXCO_GLOBAL, YR_TEXCO_ORCO, YR_TEXCO_NORMAL = 0, 1, 2
@@ -67,6 +78,11 @@ class YrShaderDesc(C.Structure):
         ("tex_octaves", C.c_float), ("tex_size", C.c_float), ("tex_intensity", C.c_float),
         ("mod_color", C.c_float), ("mod_size", f3), ("mod_ofs", f3), ("tex_noise", C.c_uint32),
         ("tex_depth", C.c_int32), ("tex_hard", C.c_uint32), ("tex_map", C.c_uint32),
+        # record version 2
+        ("mod_mode", C.c_uint32), ("tex_shape", C.c_uint32), ("tex_variant", C.c_uint32),
+        ("tex_turbulence", C.c_float), ("tex_sharpness", C.c_float), ("tex_offset", C.c_float),
+        ("tex_gain", C.c_float), ("tex_distort", C.c_float), ("tex_noise2", C.c_uint32),
+        ("tex_weights", C.c_float * 4), ("tex_mk_exponent", C.c_float), ("tex_metric", C.c_uint32),
     ]
 
 

@@ -64,19 +64,32 @@ __device__ __forceinline__ void grad_end(const AdjWave &A, const GradAcc &g) {
 
 __device__ __forceinline__ float dot3(const C3 &a, const C3 &b) { return a.r * b.r + a.g * b.g + a.b * b.b; }
 
-// dL/dC and dL/dS at a vertex of shader `sid` -> the shader's parameters
+// dL/dC and dL/dS at a vertex of shader `sid` -> the shader's parameters.
+// C is the modulated diffuse colour; md[0] = (d tex / d intensity, d tex /
+// d color1), md[1] = (tex, 0) at the vertex (modulated_color's TexDeriv).
 __device__ __forceinline__ void chain_shader(const DevRender &R, const AdjWave &A, const GradAcc &acc, int sid,
-                                             float m, const C3 &dC, const C3 &dS) {
+                                             const float4 *md, const C3 &dC, const C3 &dS) {
     const DevShader &sh = R.shaders[sid];
     const int b = A.sh_pbase[sid];
     C3 dCb = dC;
     if (sh.tex_type != YR_TEX_NONE && sh.mod_color > 0.f) {
+        const float4 m0 = md[0], m1 = md[1];
+        const C3 tex = c3(m1.x, m1.y, m1.z);
         const float w = sh.mod_color;
-        const C3 dtex = w > 1.f ? dC : dC * w;
-        dCb = w > 1.f ? c3(0.f, 0.f, 0.f) : dC * (1.f - w);
-        const float f = sh.tex_type == YR_TEX_MUSGRAVE_FBM ? sh.intensity * m : m;
-        const C3 dtc1 = dtex * (1.f - f);
-        if (sh.tex_type == YR_TEX_MUSGRAVE_FBM) acc.add(b + 4, m * dot3(dtex, sh.tc2 - sh.tc1));
+        C3 dtex;
+        switch (sh.mod_mode) {
+        case YR_MOD_MUL:  // C' = mix(tex, 1, w) * C
+            dtex = w > 1.f ? dC * sh.color : (dC * sh.color) * w;
+            dCb = dC * (w > 1.f ? tex : tex * w + (1 - w) * c3(1.f, 1.f, 1.f));
+            break;
+        case YR_MOD_ADD: dtex = dC * w; break;
+        case YR_MOD_SUB: dtex = dC * -w; break;
+        default:  // mix(tex, C, w)
+            dtex = w > 1.f ? dC : dC * w;
+            dCb = w > 1.f ? c3(0.f, 0.f, 0.f) : dC * (1.f - w);
+        }
+        acc.add(b + 4, dot3(dtex, c3(m0.x, m0.y, m0.z)));
+        const C3 dtc1 = dtex * m0.w;
         acc.add(b + 5, dtc1.r);
         acc.add(b + 6, dtc1.g);
         acc.add(b + 7, dtc1.b);
@@ -93,7 +106,7 @@ __device__ __forceinline__ void chain_shader(const DevRender &R, const AdjWave &
 // and returns the direct light sum G.
 __device__ __forceinline__ C3 adj_vertex_direct(const DevRender &R, const Wave &W, const AdjWave &A,
                                                 const GradAcc &acc, uint32_t vtx, const float4 *aux, const C3 &lkc,
-                                                int sid, float m, const C3 &Wv) {
+                                                int sid, const float4 *md, const C3 &Wv) {
     const C3 spec = R.shaders[sid].specular;
     C3 Dt = c3(0.f, 0.f, 0.f), St = c3(0.f, 0.f, 0.f);
     uint32_t off = 0;
@@ -144,7 +157,7 @@ __device__ __forceinline__ C3 adj_vertex_direct(const DevRender &R, const Wave &
         }
         off += light_slots(L);
     }
-    chain_shader(R, A, acc, sid, m, Wv * Dt, Wv * St);
+    chain_shader(R, A, acc, sid, md, Wv * Dt, Wv * St);
     return lkc * Dt + spec * St;
 }
 
@@ -185,7 +198,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather_camera(DevRender R, Wave 
         const float4 h = W.hit0[i];
         if (__float_as_int(h.y) >= 0) {
             const float4 v = A.v0[i];
-            adj_vertex_direct(R, W, A, acc, i, W.aux, c3(v.x, v.y, v.z), __float_as_int(v.w), A.v0m[i],
+            adj_vertex_direct(R, W, A, acc, i, W.aux, c3(v.x, v.y, v.z), __float_as_int(v.w), A.v0m + 2 * (size_t)i,
                               sample_weight(R, A, W.base + i));
         }
     }
@@ -233,7 +246,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather_path(DevRender R, Wave W,
                 const C3 Wv = ((g * c3(d0.x, d0.y, d0.z)) * (d0.w * mult * startN)) * c3(col.x, col.y, col.z);
                 const float4 v = A.pv[ci];
                 const C3 G = adj_vertex_direct(R, W, A, acc, p, W.p_aux, c3(v.x, v.y, v.z), __float_as_int(v.w),
-                                               A.pm[ci], Wv);
+                                               A.pm + 2 * ci, Wv);
                 A.pG[ci] = make_float4(G.r, G.g, G.b, 1.f);
                 const float4 nc = W.p_next[p];
                 const C3 ncol = c3(nc.x, nc.y, nc.z);
@@ -282,7 +295,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_finish(DevRender R, Wave W, AdjW
                     const int sid = __float_as_int(v.w);
                     if (sid >= 0) {
                         if (U.r != 0.f || U.g != 0.f || U.b != 0.f)
-                            chain_shader(R, A, acc, sid, A.pm[c0 + jj], (Acol * startN) * (rc[jj] * U),
+                            chain_shader(R, A, acc, sid, A.pm + 2 * (c0 + jj), (Acol * startN) * (rc[jj] * U),
                                          c3(0.f, 0.f, 0.f));
                         U = c3(G.x, G.y, G.z) + c3(v.x, v.y, v.z) * U;
                     } else {
@@ -292,7 +305,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_finish(DevRender R, Wave W, AdjW
                 Tsum = Tsum + startN * U;
             }
             const float4 v = A.v0[i];
-            chain_shader(R, A, acc, __float_as_int(v.w), A.v0m[i], g * (Tsum * (d0.w * mult)), c3(0.f, 0.f, 0.f));
+            chain_shader(R, A, acc, __float_as_int(v.w), A.v0m + 2 * (size_t)i, g * (Tsum * (d0.w * mult)),
+                         c3(0.f, 0.f, 0.f));
             acc.add(A.li_pidx[R.path_light], dot3(g, dif0 * (Tsum * mult)));
         }
     }
@@ -306,7 +320,7 @@ static void adj_sizes(const Plan &P, uint32_t wcap, uint32_t npix, size_t *b) {
     const size_t w = wcap, pc = (size_t)wcap * (P.npath > 1u ? P.npath : 1u), vc = w > pc ? w : pc;
     const size_t slots = vc * (P.ns > 1u ? P.ns : 1u), pd = pc * (size_t)P.depth;
     const size_t f4 = sizeof(float4);
-    const size_t sizes[kNumAdjBufs] = {f4 * slots, f4 * w, 4 * w, f4 * pd, 4 * pd, f4 * pd, f4 * (size_t)npix};
+    const size_t sizes[kNumAdjBufs] = {f4 * slots, f4 * w, 2 * f4 * w, f4 * pd, 2 * f4 * pd, f4 * pd, f4 * (size_t)npix};
     for (int i = 0; i < kNumAdjBufs; i++) b[i] = sizes[i];
 }
 
@@ -328,9 +342,9 @@ static void assign_adj(const Plan &P, uint32_t wcap, uint32_t npix, char *base, 
     }
     A.slot_s = (float4 *)ptr[0];
     A.v0 = (float4 *)ptr[1];
-    A.v0m = (float *)ptr[2];
+    A.v0m = (float4 *)ptr[2];
     A.pv = (float4 *)ptr[3];
-    A.pm = (float *)ptr[4];
+    A.pm = (float4 *)ptr[4];
     A.pG = (float4 *)ptr[5];
     A.gpix = (const float4 *)ptr[6];
 }

@@ -261,6 +261,12 @@ __device__ __forceinline__ float turbulence(const V3 &pt, int oct, float size, b
     return sum * ((float)(1 << oct) / (float)((1 << (oct + 1)) - 1));
 }
 
+}  // namespace yr
+
+#include "dev_tex.cuh"
+
+namespace yr {
+
 // --------------------------------------------------------------- shading
 struct Surf {
     V3 P, N, Ng, NU, NV;
@@ -336,11 +342,6 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
     return s;
 }
 
-// modulator_t::modulate (texture.cc:499-534) in "mix" mode with procedural
-// texture coordinates size*(P + ofs) (texture.cc:307-312), applied to the
-// diffuse colour only.
-// `m_out` (optional) receives the noise value before the intensity scale
-// (the fBm sum, or the clouds turbulence), which the adjoint needs.
 // Texture point of the procedural path of modulator_t::doMapping
 // (texture.cc:122-320): the texco source (hit point, or the shading
 // normal), then per axis size*(source[proj] + ofs), or size*ofs when the
@@ -356,24 +357,42 @@ __device__ __forceinline__ V3 tex_point(const DevShader &sh, const V3 &P, const 
     return v3(t[0], t[1], t[2]);
 }
 
-__device__ __forceinline__ C3 modulated_color(const DevShader &sh, const V3 &P, const V3 &N, float *m_out = nullptr) {
-    C3 C = sh.color;
+// What the adjoint keeps of a vertex's texture: its colour and the
+// colour's derivatives by the texture intensity and by color1.
+struct TexDeriv {
+    C3 tex;
+    C3 dint;
+    float dc1;
+};
+
+// modulator_t::modulate (texture.cc:499-534), colour channel: the texture
+// colour at the modulator's texture point, mixed into the diffuse colour
+// by the modulator's mode - mix: mix(tex, C, w); mul: mix(tex, 1, w) * C;
+// add: tex*w + C; sub: tex*(-w) + C, where mix (color.cc:103-109) is
+// a*w + (1-w)*b and returns a for w > 1.  `td` (optional) receives what
+// the adjoint needs.
+// `shp` points at the shader record in device memory.
+__device__ __forceinline__ C3 modulated_color(const DevShader *shp, const V3 &P, const V3 &N,
+                                              TexDeriv *td = nullptr) {
+    const DevShader &sh = *shp;
+    const C3 C = sh.color;
     if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f)) return C;
-    const V3 tp = tex_point(sh, P, N);
-    float f;
-    if (sh.tex_type == YR_TEX_MUSGRAVE_FBM) {  // textureMusgrave_t::getFloat (basictex.cc:677-680)
-        const float m = fbm(V3{tp.x * sh.tsize, tp.y * sh.tsize, tp.z * sh.tsize}, sh.H, sh.lacunarity, sh.octaves);
-        if (m_out) *m_out = m;
-        f = sh.intensity * m;
-    } else {  // textureClouds_t::getFloat (basictex.cc:83-91), no bias
-        f = turbulence(tp, sh.tdepth, sh.tsize, sh.thard != 0);
-        if (m_out) *m_out = f;
+    const TexEval te = texture_eval(shp, tex_point(sh, P, N));
+    if (td) {
+        td->tex = te.col;
+        td->dint = te.dint;
+        td->dc1 = te.dc1;
     }
-    const C3 tex = sh.tc1 + f * (sh.tc2 - sh.tc1);
-    // mix(texcolor, C, w) (color.cc:103-109)
+    const C3 tex = te.col;
     const float w = sh.mod_color;
-    if (w > 1.0f) return tex;
-    return tex * w + (1 - w) * C;
+    switch (sh.mod_mode) {
+    case YR_MOD_MUL: return (w > 1.0f ? tex : tex * w + (1 - w) * c3(1.f, 1.f, 1.f)) * C;
+    case YR_MOD_ADD: return (tex * w) + C;
+    case YR_MOD_SUB: return (tex * -w) + C;
+    default:
+        if (w > 1.0f) return tex;
+        return tex * w + (1 - w) * C;
+    }
 }
 
 // The parts of genericShader_t::fromLight (basicshaders.cc:46-70) that

@@ -64,9 +64,9 @@ struct Wave {
 struct AdjWave {
     float4 *slot_s;        // [slots] specular factor per light sample (slot_c: diffuse factor)
     float4 *v0;            // [count] camera vertex: diffuse colour, shader (bits)
-    float *v0m;            // [count] noise value at the camera vertex
+    float4 *v0m;           // [2*count] camera vertex texture: (d colour / d intensity, d colour / d color1), (colour, 0)
     float4 *pv;            // [count*npath*depth] path vertex: diffuse colour, shader (bits); w = -1: none
-    float *pm;             // [count*npath*depth] noise value at the path vertex
+    float4 *pm;            // [2*count*npath*depth] path vertex texture, as v0m
     float4 *pG;            // [count*npath*depth] direct light (or background) at the vertex; w = 1: present
     const float4 *gpix;    // per image pixel: dL/d(pixel rgb)
     float *grad;           // parameter gradient (global)
@@ -187,12 +187,12 @@ template <bool ADJ = false>
 __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender &R, const Wave &W, bool active,
                                              const Surf &sp, const V3 &eye, uint32_t vtx, int v, uint32_t m0,
                                              uint32_t pixel, float4 *aux, float4 *slot_s = nullptr,
-                                             C3 *lkc_out = nullptr, float *m_out = nullptr) {
+                                             C3 *lkc_out = nullptr, TexDeriv *td_out = nullptr) {
     DevShader sh;
     C3 lkc = c3(0.f, 0.f, 0.f);
     if (active) {
         sh = R.shaders[sp.shader];
-        lkc = modulated_color(sh, sp.P, sp.N, ADJ ? m_out : nullptr);
+        lkc = modulated_color(R.shaders + sp.shader, sp.P, sp.N, ADJ ? td_out : nullptr);
         if (ADJ) *lkc_out = lkc;
     }
     V3 N = sp.N;
@@ -420,11 +420,12 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
     }
     if (ADJ) {
         C3 lkc = c3(0.f, 0.f, 0.f);
-        float m = 0.f;
-        shade_lights<true>(S, R, W, active, sp, eye, inb ? i : 0, 0, s, pixel, W.aux, A->slot_s, &lkc, &m);
+        TexDeriv td{};
+        shade_lights<true>(S, R, W, active, sp, eye, inb ? i : 0, 0, s, pixel, W.aux, A->slot_s, &lkc, &td);
         if (active) {
             A->v0[i] = make_float4(lkc.r, lkc.g, lkc.b, __int_as_float(sp.shader));
-            A->v0m[i] = m;
+            A->v0m[2 * (size_t)i] = make_float4(td.dint.r, td.dint.g, td.dint.b, td.dc1);
+            A->v0m[2 * (size_t)i + 1] = make_float4(td.tex.r, td.tex.g, td.tex.b, 0.f);
         }
     } else {
         shade_lights(S, R, W, active, sp, eye, inb ? i : 0, 0, s, pixel, W.aux);
@@ -435,7 +436,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
     bool paths = false;
     if (active) {
         const DevShader sh = R.shaders[sp.shader];
-        const C3 dif = modulated_color(sh, sp.P, sp.N);
+        const C3 dif = modulated_color(R.shaders + sp.shader, sp.P, sp.N);
         paths = !(energy(dif) < 0.05f);
         const DevLight PL = R.lights[R.path_light];
         W.diff0[i] = make_float4(dif.r, dif.g, dif.b, paths ? PL.power : 0.f);
@@ -601,19 +602,20 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
     }
     C3 dif = c3(0.f, 0.f, 0.f);
     if (ADJ) {
-        float m = 0.f;
+        TexDeriv td{};
         shade_lights<true>(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux, A->slot_s, &dif,
-                           &m);
+                           &td);
         if (active) {
             const size_t ci = (size_t)p * R.path_depth + j;
             A->pv[ci] = make_float4(dif.r, dif.g, dif.b, __int_as_float(sp.shader));
-            A->pm[ci] = m;
+            A->pm[2 * ci] = make_float4(td.dint.r, td.dint.g, td.dint.b, td.dc1);
+            A->pm[2 * ci + 1] = make_float4(td.tex.r, td.tex.g, td.tex.b, 0.f);
         }
     } else {
         shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux);
     }
     if (active) {
-        if (!ADJ) dif = modulated_color(R.shaders[sp.shader], sp.P, sp.N);
+        if (!ADJ) dif = modulated_color(R.shaders + sp.shader, sp.P, sp.N);
         const float4 col = W.p_col[p];
         const C3 nc = c3(col.x, col.y, col.z) * dif;
         W.p_next[p] = make_float4(nc.r, nc.g, nc.b, 0.f);

@@ -138,6 +138,44 @@ void make_shader(const yr_shader_desc &d, DevShader &o) {
         const uint32_t p = (d.tex_map >> (8 * (k + 1))) & 0xffu;
         o.proj[k] = p == YR_PROJ_DEFAULT ? k : (p >= YR_PROJ_X && p <= YR_PROJ_Z ? (int)p - 1 : -1);
     }
+    o.mod_mode = (int)d.mod_mode;
+    o.noise = (int)d.tex_noise;
+    o.noise2 = (int)d.tex_noise2;
+    o.tshape = (int)d.tex_shape;
+    o.tvariant = (int)d.tex_variant;
+    o.turb = d.tex_turbulence;
+    // textureMarble_t ctor (basictex.cc:113-115)
+    o.sharp = d.tex_sharpness > 1 ? (float)(1.0 / (double)d.tex_sharpness) : 1.0f;
+    o.offset = d.tex_offset;
+    o.gain = d.tex_gain;
+    o.distort = d.tex_distort;
+    for (int k = 0; k < 4; k++) o.weights[k] = d.tex_weights[k];
+    o.mk_exp = d.tex_mk_exponent;
+    o.metric = (int)d.tex_metric;
+    // textureVoronoi_t ctor (basictex.cc:585-589): iscale = intensity / sum |w|
+    const float sw = ((std::fabs(d.tex_weights[0]) + std::fabs(d.tex_weights[1])) + std::fabs(d.tex_weights[2])) +
+                     std::fabs(d.tex_weights[3]);
+    o.viscale = sw != 0.f ? d.tex_intensity / sw : 0.f;
+    o.vinvw = sw != 0.f ? 1.0f / sw : 0.f;
+}
+
+// Enumerations of a shader record in range (texture type, noise bases,
+// modulator mode, shape / type / metric fields of the texture used).
+bool valid_shader(const yr_shader_desc &d) {
+    if (d.tex_type > YR_TEX_GRADIENT || d.mod_mode > YR_MOD_SUB) return false;
+    if ((d.tex_map & 0xffu) > YR_TEXCO_NORMAL) return false;
+    for (int k = 1; k < 4; k++)
+        if (((d.tex_map >> (8 * k)) & 0xffu) > YR_PROJ_NONE) return false;
+    if (d.tex_type == YR_TEX_NONE) return true;
+    if (d.tex_noise > YR_NOISE_CELLNOISE || d.tex_noise2 > YR_NOISE_CELLNOISE) return false;
+    switch (d.tex_type) {
+    case YR_TEX_MARBLE:
+    case YR_TEX_WOOD: return d.tex_shape <= YR_WAVE_TRI && d.tex_depth >= 0 && d.tex_depth < 30;
+    case YR_TEX_CLOUDS: return d.tex_variant <= 2 && d.tex_depth >= 0 && d.tex_depth < 30;
+    case YR_TEX_VORONOI: return d.tex_shape <= 3 && d.tex_metric <= YR_DIST_MINKOVSKY;
+    case YR_TEX_GRADIENT: return d.tex_shape <= YR_GRAD_HALO;
+    default: return true;
+    }
 }
 
 // areaLight_t::fillQuad (arealight.cc:31-73): sample grid and jitter axes.
@@ -225,6 +263,10 @@ yr_status make_lights(const std::vector<yr_light_desc> &in, std::vector<DevLight
 }
 
 // camera_t ctor for CM_PERSPECTIVE (camera.cc:27-87)
+// camera_t ctor (camera.cc:27-87), perspective, in the shipped build's
+// (-O3 -ffast-math) evaluation: vto.normLen() as a float division 1/|vto|,
+// and the divisions by resx and resy as products with their reciprocals
+// (vup scaled by (resy*aspect) * (1/resx), then by 1/resy; vright by 1/resx).
 void make_camera(const yr_camera_desc &c, DevCamera &o) {
     const V3 pos = hv(c.pos);
     V3 vup = hv(c.up) - pos;
@@ -239,16 +281,17 @@ void make_camera(const yr_camera_desc &c, DevCamera &o) {
         float vl = vto.x * vto.x + vto.y * vto.y + vto.z * vto.z;
         if (vl != 0.f) {
             vl = std::sqrt(vl);
-            const float dv = (float)(1.0 / vl);
+            const float dv = 1.0f / vl;
             vto.x *= dv;
             vto.y *= dv;
             vto.z *= dv;
         }
     }
-    vup = vup * (c.aspect * (float)c.resy / (float)c.resx);
+    const float rx = 1.0f / (float)c.resx, ry = 1.0f / (float)c.resy;
+    vup = vup * (((float)c.resy * c.aspect) * rx);
     vto = (vto * c.focal) - 0.5f * (vup + vright);
-    vup = h_div(vup, (float)c.resy);
-    vright = h_div(vright, (float)c.resx);
+    vup = vup * ry;
+    vright = vright * rx;
     o.pos = pos;
     o.vright = vright;
     o.vup = vup;
@@ -643,7 +686,10 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     s->shader_desc.assign(desc->shaders, desc->shaders + desc->nshaders);
     s->light_desc.assign(desc->lights, desc->lights + desc->nlights);
     s->shaders.resize(desc->nshaders);
-    for (uint32_t i = 0; i < desc->nshaders; i++) make_shader(desc->shaders[i], s->shaders[i]);
+    for (uint32_t i = 0; i < desc->nshaders; i++) {
+        if (!valid_shader(desc->shaders[i])) return fail(YR_ERR_INVALID_ARG);
+        make_shader(desc->shaders[i], s->shaders[i]);
+    }
     if ((st = make_lights(s->light_desc, s->lights, s->area_pts)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, s->shaders.data(), s->shaders.size(), &s->d_shaders)) != YR_OK) return fail(st);
     if (!s->lights.empty() && (st = dev_upload(s, s->lights.data(), s->lights.size(), &s->d_lights)) != YR_OK)
@@ -754,6 +800,11 @@ YR_API yr_status yr_scene_set_params(yr_scene *scene, const yr_shader_desc *shad
     cudaGetDevice(&prev);
     cudaSetDevice(scene->device);
     if (shaders) {
+        for (size_t i = 0; i < scene->shader_desc.size(); i++)
+            if (!valid_shader(shaders[i])) {
+                cudaSetDevice(prev);
+                return YR_ERR_INVALID_ARG;
+            }
         scene->shader_desc.assign(shaders, shaders + scene->shader_desc.size());
         for (size_t i = 0; i < scene->shaders.size(); i++) make_shader(shaders[i], scene->shaders[i]);
     }

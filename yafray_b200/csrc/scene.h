@@ -23,6 +23,19 @@ struct DevShader {
     int tdepth, thard;
     int texco;           // YR_TEXCO_*
     int proj[3];         // source axis (0..2) of texture x / y / z, -1 = none
+    int mod_mode;        // YR_MOD_*
+    int noise, noise2;   // YR_NOISE_* (noise_type / noise_type1, noise_type2)
+    int tshape;          // marble / wood shape, gradient type, voronoi colour type
+    int tvariant;        // wood rings, clouds bias, gradient flip_xy
+    float turb;          // marble / wood turbulence
+    float sharp;         // marble: 1/sharpness when sharpness > 1, else 1
+    float offset, gain;  // musgrave
+    float distort;       // distorted noise
+    float weights[4];    // voronoi weight1..4
+    float mk_exp;        // voronoi minkovsky exponent
+    int metric;          // voronoi YR_DIST_*
+    float viscale;       // voronoi intensity / sum |weight| (0 when the sum is 0)
+    float vinvw;         // voronoi 1 / sum |weight| (0 when the sum is 0)
 };
 
 struct DevLight {
@@ -109,6 +122,7 @@ struct yr_scene {
 namespace yr {
 // derived device records from the ABI descriptors (scene.cu)
 void make_shader(const yr_shader_desc &d, DevShader &o);
+bool valid_shader(const yr_shader_desc &d);
 yr_status make_lights(const std::vector<yr_light_desc> &in, std::vector<DevLight> &out, std::vector<float> &pts);
 void make_camera(const yr_camera_desc &c, DevCamera &o);
 yr_status upload_params(yr_scene *s);

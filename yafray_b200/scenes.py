@@ -159,6 +159,87 @@ def fbm_shader(color, color1, color2, intensity, size, octaves=6.0, lacunarity=2
     return s
 
 
+# Procedural textures: the parameters of each factory with its defaults
+# (basictex.cc: clouds :94-104, marble :155-175, wood :222-249, voronoi
+# :619-650, musgrave :683-709, distorted_noise :731-746, gradient :805-815).
+_TEX_DEFAULTS = {
+    "clouds": dict(depth=2, size=1.0, hard=False, bias="", noise_type="newperlin"),
+    "marble": dict(depth=2, turbulence=1.0, sharpness=1.0, size=1.0, hard=False, shape="sin",
+                   noise_type="newperlin"),
+    "wood": dict(depth=2, turbulence=1.0, size=1.0, hard=False, wood_type="bands", shape="sin",
+                 noise_type="newperlin"),
+    "voronoi": dict(color_type="int", weight1=1.0, weight2=0.0, weight3=0.0, weight4=0.0, mk_exponent=2.5,
+                    intensity=1.0, size=1.0, distance_metric="real"),
+    "musgrave": dict(type="fBm", noise_type="newperlin", H=1.0, lacunarity=2.0, octaves=2.0, offset=1.0,
+                     gain=1.0, size=1.0, intensity=1.0),
+    "distorted_noise": dict(noise_type1="newperlin", noise_type2="newperlin", distort=1.0, size=1.0),
+    "gradient": dict(gradient_type="linear", flip_xy=False),
+}
+_MUSGRAVE_TYPES = {"fBm": abi.YR_TEX_MUSGRAVE_FBM, "multifractal": abi.YR_TEX_MUSGRAVE_MULTIFRACTAL,
+                   "heteroterrain": abi.YR_TEX_MUSGRAVE_HETEROTERRAIN, "hybridmf": abi.YR_TEX_MUSGRAVE_HYBRIDMF,
+                   "ridgedmf": abi.YR_TEX_MUSGRAVE_RIDGEDMF}
+
+
+def texture_shader(color, kind, color1=(0.0, 0.0, 0.0), color2=(1.0, 1.0, 1.0), mod_color=1.0, mode="mix",
+                   texco="global", proj=("x", "y", "z"), **params) -> abi.YrShaderDesc:
+    """genericShader_t whose diffuse colour is modulated by one procedural
+    texture `kind` ("clouds", "marble", "wood", "voronoi", "musgrave",
+    "distorted_noise", "gradient") with the factory's parameter names and
+    defaults; unknown parameter names raise."""
+    p = dict(_TEX_DEFAULTS[kind])
+    for k in params:
+        if k not in p:
+            raise KeyError(f"{kind} has no parameter {k!r}")
+    p.update(params)
+    s = shader(color)
+    s.tex_color1[:] = [float(c) for c in color1]
+    s.tex_color2[:] = [float(c) for c in color2]
+    s.mod_color = float(mod_color)
+    s.mod_mode = abi.MOD_MODES[mode]
+    s.tex_map = tex_map(texco, proj)
+    nt = lambda name: abi.NOISE_TYPES.get(name, 0)  # newNoise: unknown names give newperlin
+    if kind == "clouds":
+        s.tex_type = abi.YR_TEX_CLOUDS
+        s.tex_depth, s.tex_size, s.tex_hard = int(p["depth"]), float(p["size"]), int(bool(p["hard"]))
+        s.tex_variant = {"positive": 1, "negative": 2}.get(p["bias"], 0)
+        s.tex_noise = nt(p["noise_type"])
+    elif kind in ("marble", "wood"):
+        s.tex_type = abi.YR_TEX_MARBLE if kind == "marble" else abi.YR_TEX_WOOD
+        s.tex_depth, s.tex_size, s.tex_hard = int(p["depth"]), float(p["size"]), int(bool(p["hard"]))
+        s.tex_turbulence = float(p["turbulence"])
+        s.tex_shape = abi.WAVE_SHAPES.get(p["shape"], 0)
+        s.tex_noise = nt(p["noise_type"])
+        if kind == "marble":
+            s.tex_sharpness = float(p["sharpness"])
+        else:
+            s.tex_variant = 1 if p["wood_type"] == "rings" else 0
+    elif kind == "voronoi":
+        s.tex_type = abi.YR_TEX_VORONOI
+        s.tex_shape = {"col1": 1, "col2": 2, "col3": 3}.get(p["color_type"], 0)
+        s.tex_weights[:] = [float(p[f"weight{i}"]) for i in range(1, 5)]
+        s.tex_mk_exponent = float(p["mk_exponent"])
+        s.tex_intensity = float(p["intensity"])
+        s.tex_size = float(p["size"])
+        s.tex_metric = abi.DIST_METRICS.get(p["distance_metric"], 0)
+    elif kind == "musgrave":
+        s.tex_type = _MUSGRAVE_TYPES.get(p["type"], abi.YR_TEX_MUSGRAVE_FBM)
+        s.tex_noise = nt(p["noise_type"])
+        s.tex_H, s.tex_lacunarity, s.tex_octaves = float(p["H"]), float(p["lacunarity"]), float(p["octaves"])
+        s.tex_offset, s.tex_gain = float(p["offset"]), float(p["gain"])
+        s.tex_size, s.tex_intensity = float(p["size"]), float(p["intensity"])
+    elif kind == "distorted_noise":
+        s.tex_type = abi.YR_TEX_DISTORTED_NOISE
+        s.tex_noise, s.tex_noise2 = nt(p["noise_type1"]), nt(p["noise_type2"])
+        s.tex_distort, s.tex_size = float(p["distort"]), float(p["size"])
+    elif kind == "gradient":
+        s.tex_type = abi.YR_TEX_GRADIENT
+        s.tex_shape = abi.GRADIENT_TYPES.get(p["gradient_type"], 0)
+        s.tex_variant = int(bool(p["flip_xy"]))
+    else:
+        raise KeyError(kind)
+    return s
+
+
 def point_light(pos, power=1.0, color=(1.0, 1.0, 1.0), cast_shadows=True) -> abi.YrLightDesc:
     l = abi.YrLightDesc()
     l.type = abi.YR_LIGHT_POINT
@@ -377,8 +458,9 @@ def config_diffnoise(seed=5, count=32, **kw) -> List[Scene]:
 def write_yrs(sc: Scene, path: str) -> None:
     with open(path, "wb") as f:
         f.write(b"YRS1")
-        # last header word: record version; 1 = object records carry the smoothing angle
-        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 1))
+        # last header word: record version; 1 = object records carry the
+        # smoothing angle; 2 = shader records carry the version-2 texture fields
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 2))
         f.write(bytes(sc.camera))
         f.write(bytes(sc.render))
         for s in sc.shaders:
@@ -406,9 +488,13 @@ def read_yrs(path: str) -> Scene:
     off += C_sizeof(abi.YrCameraDesc)
     sc.render = abi.YrRenderParams.from_buffer_copy(data, off)
     off += C_sizeof(abi.YrRenderParams)
+    # shader records before version 2 end at mod_mode
+    shsize = C_sizeof(abi.YrShaderDesc) if version >= 2 else abi.YrShaderDesc.mod_mode.offset
     for _ in range(nsh):
-        sc.shaders.append(abi.YrShaderDesc.from_buffer_copy(data, off))
-        off += C_sizeof(abi.YrShaderDesc)
+        s = abi.YrShaderDesc()
+        C_memmove(s, data[off:off + shsize])
+        sc.shaders.append(s)
+        off += shsize
     for _ in range(nl):
         sc.lights.append(abi.YrLightDesc.from_buffer_copy(data, off))
         off += C_sizeof(abi.YrLightDesc)
@@ -434,3 +520,8 @@ def read_yrs(path: str) -> Scene:
 def C_sizeof(t) -> int:
     import ctypes
     return ctypes.sizeof(t)
+
+
+def C_memmove(dst, raw: bytes) -> None:
+    import ctypes
+    ctypes.memmove(ctypes.addressof(dst), raw, len(raw))
