@@ -272,6 +272,10 @@ typedef struct yr_render_params {
     int32_t region[4];       /* x0, x1, y0, y1: render only these pixels
                                 (scene_t::setRegion / the loader's -r option);
                                 all zero = the whole image                    */
+    /* record version 3 */
+    float exposure;          /* render "exposure" (scene_t::setExposure; 0 =
+                                off); applied with YR_RENDER_TONEMAP          */
+    float gamma;             /* render "gamma" (scene_t::setGamma; 1 = off)   */
 } yr_render_params;
 
 /* yr_render_params.flags:
@@ -288,6 +292,17 @@ typedef struct yr_render_params {
  *   casters (same answers; faster). */
 #define YR_RENDER_SHADOW_TREE 1u
 #define YR_RENDER_EXACT_ORDER 2u
+/* YR_RENDER_TONEMAP: every camera sample passes through
+ *   color_t::expgam_Adjust(exposure, gamma, clamp_rgb) before the pixel
+ *   average (scene.cc:763, 807), as scene_t::render does when the loader
+ *   writes a TGA (tonemap(true); HDR / EXR output turns it off).
+ * YR_RENDER_CLAMP_RGB: render "clamp_rgb": with TONEMAP, exposure 0 and
+ *   gamma 1, each sample is clamped to [0, 1].
+ * YR_RENDER_ALPHA_PREMULTIPLY: render "alpha_premultiply": the pixel's RGB
+ *   times its alpha (scene.cc:818-822). */
+#define YR_RENDER_TONEMAP 4u
+#define YR_RENDER_CLAMP_RGB 8u
+#define YR_RENDER_ALPHA_PREMULTIPLY 16u
 
 typedef struct yr_object_desc {
     const float *verts;      /* 3*nverts                                       */
@@ -516,6 +531,28 @@ YR_API yr_status yr_backward(yr_scene *scene, const yr_backward_desc *desc, floa
  * scene.  (No counterpart in the reference.) */
 YR_API yr_status yr_backward_batch(yr_scene *const *scenes, uint32_t count, const yr_backward_desc *descs,
                                    float *const *dparams, float *losses, int32_t streams, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Image outputs (host).  A rendered RGBA float image (row-major, top row
+ * first, as yr_render writes it) encoded byte for byte as YafRay's
+ * colorOutput_t writers encode the same pixels:
+ *   YR_IMAGE_TGA: outTga_t (targaIO.cc:37-130), 24-bit BGR, or 32-bit BGRA
+ *     with YR_IMAGE_ALPHA (the loader's save_alpha);
+ *   YR_IMAGE_HDR: outHDR_t (HDR_io.cc:34-160), Radiance RGBE with
+ *     run-length scanlines; alpha is not stored.
+ * The loader renders a TGA with the per-sample tone map on
+ * (YR_RENDER_TONEMAP) and an HDR with it off.
+ * ------------------------------------------------------------------------ */
+enum { YR_IMAGE_TGA = 0, YR_IMAGE_HDR = 1 };
+#define YR_IMAGE_ALPHA 1u
+
+/* Encode into `out` (host, `capacity` bytes); `size` receives the encoded
+ * size.  With out == NULL only the size is returned. */
+YR_API yr_status yr_image_encode(int32_t format, const float *rgba, int32_t width, int32_t height, int32_t flags,
+                                 uint8_t *out, size_t capacity, size_t *size);
+/* Encode and write to the file `path`. */
+YR_API yr_status yr_image_write(const char *path, int32_t format, const float *rgba, int32_t width, int32_t height,
+                                int32_t flags);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,8 @@
 //                                              sample stream set from outside
 //   yr_ref_harness noise   POINTS OUT          newPerlin / fBm / turbulence
 //   yr_ref_harness halton  OUT                 Halton setStart+getNext values
+//   yr_ref_harness imgout  KIND IN OUT         float RGBA image through outTga_t /
+//                                              outHDR_t (KIND tga, tga_alpha, hdr)
 //   yr_ref_harness noisegen POINTS OUT         every noise basis, turbulence,
 //                                              voronoi distances per metric
 //   yr_ref_harness texeval SCENE POINTS OUT    each shader's texture getColor /
@@ -40,6 +42,8 @@
 #include "pathlight.h"
 #include "basicshaders.h"
 #include "basictex.h"
+#include "targaIO.h"
+#include "HDR_io.h"
 #undef private
 #undef protected
 
@@ -138,7 +142,10 @@ static void load_scene(const char *path, SceneFile &s) {
     uint32_t hdr[4];
     rd(f, hdr, 16);
     rd(f, &s.cam, sizeof(s.cam));
-    rd(f, &s.rp, sizeof(s.rp));
+    // render parameters before record version 3 end at exposure (gamma then 1)
+    memset(&s.rp, 0, sizeof(s.rp));
+    s.rp.gamma = 1.f;
+    rd(f, &s.rp, hdr[3] >= 3 ? sizeof(s.rp) : offsetof(yr_render_params, exposure));
     s.shaders.resize(hdr[1]);
     memset(s.shaders.data(), 0, sizeof(yr_shader_desc) * hdr[1]);
     // shader records before version 2 end at mod_mode
@@ -288,6 +295,17 @@ static light_t *make_light(const yr_light_desc &d) {
     return NULL;
 }
 
+// the "constant" background plugin (constBackground_t, sunsky.h:12-21): a
+// fixed colour for every direction
+class constBg_t : public background_t {
+  public:
+    constBg_t(const color_t &c) : color(c) {}
+    virtual color_t operator()(const vector3d_t &dir, renderState_t &state, bool filtered = false) const {
+        return color;
+    }
+    color_t color;
+};
+
 static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true) {
     r.scene = scene_t::factory();
     for (size_t i = 0; i < s.shaders.size(); i++) r.shaders.push_back(make_shader(s.shaders[i], r.textures));
@@ -317,9 +335,13 @@ static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true) 
     r.scene->setCamera(r.camera);
     r.scene->setBias(s.rp.self_bias);
     r.scene->setMaxRayDepth(s.rp.raydepth);
-    r.scene->tonemap(false);
-    r.scene->clampRGB(false);
-    r.scene->alphaPremultiply(false);
+    r.scene->tonemap((s.rp.flags & YR_RENDER_TONEMAP) != 0);
+    r.scene->clampRGB((s.rp.flags & YR_RENDER_CLAMP_RGB) != 0);
+    r.scene->alphaPremultiply((s.rp.flags & YR_RENDER_ALPHA_PREMULTIPLY) != 0);
+    r.scene->setExposure(s.rp.exposure);
+    r.scene->setGamma(s.rp.gamma);
+    if (s.rp.background[0] != 0.f || s.rp.background[1] != 0.f || s.rp.background[2] != 0.f)
+        r.scene->setBackground(new constBg_t(C3(s.rp.background)));
     r.scene->alphaMaskBackground(false);
     r.scene->setFog(0, color_t(0.0));
     if (with_lights)
@@ -526,9 +548,12 @@ static void cmd_render(const SceneFile &s, const char *out, int threads, const i
         tsc->setCamera(r.camera);
         tsc->setBias(s.rp.self_bias);
         tsc->setMaxRayDepth(s.rp.raydepth);
-        tsc->tonemap(false);
-        tsc->clampRGB(false);
-        tsc->alphaPremultiply(false);
+        tsc->tonemap((s.rp.flags & YR_RENDER_TONEMAP) != 0);
+        tsc->clampRGB((s.rp.flags & YR_RENDER_CLAMP_RGB) != 0);
+        tsc->alphaPremultiply((s.rp.flags & YR_RENDER_ALPHA_PREMULTIPLY) != 0);
+        tsc->setExposure(s.rp.exposure);
+        tsc->setGamma(s.rp.gamma);
+        tsc->setBackground(r.scene->background);
         tsc->alphaMaskBackground(false);
         tsc->setFog(0, color_t(0.0));
         sc = tsc;
@@ -742,6 +767,33 @@ static void cmd_texeval(const SceneFile &s, const char *pts_path, const char *ou
     fclose(f);
 }
 
+// ------------------------------------------------------------ image outputs
+// A float RGBA image (u32 w, u32 h, then w*h*4 floats, top row first)
+// written by the reference's own outTga_t (with or without alpha) or
+// outHDR_t, pixel by pixel through putPixel as renderArea_t::out does
+// (renderblock.cc:8-20).
+static void cmd_imgout(const char *kind, const char *in, const char *out) {
+    FILE *fi = fopen(in, "rb");
+    if (!fi) die("cannot open image");
+    uint32_t wh[2];
+    rd(fi, wh, 8);
+    std::vector<float> px(4 * (size_t)wh[0] * wh[1]);
+    if (!px.empty()) rd(fi, &px[0], 4 * px.size());
+    fclose(fi);
+    const std::string k = kind;
+    colorOutput_t *o;
+    if (k == "hdr") o = new outHDR_t(wh[0], wh[1], out);
+    else if (k == "tga" || k == "tga_alpha") o = new outTga_t(wh[0], wh[1], out, k == "tga_alpha");
+    else die("image kind: tga, tga_alpha or hdr");
+    for (uint32_t y = 0; y < wh[1]; y++)
+        for (uint32_t x = 0; x < wh[0]; x++) {
+            const float *p = &px[4 * ((size_t)y * wh[0] + x)];
+            o->putPixel(x, y, color_t(p[0], p[1], p[2]), p[3], 0);
+        }
+    o->flush();
+    delete o;
+}
+
 // ------------------------------------------------------------------ halton
 static void cmd_halton(const char *out) {
     FILE *f = fopen(out, "wb");
@@ -774,6 +826,11 @@ int main(int argc, char **argv) {
     }
     if (cmd == "halton") {
         cmd_halton(argv[2]);
+        return 0;
+    }
+    if (cmd == "imgout") {
+        if (argc < 5) die("imgout KIND IN OUT");
+        cmd_imgout(argv[2], argv[3], argv[4]);
         return 0;
     }
     if (cmd == "noisegen") {

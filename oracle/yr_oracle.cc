@@ -1306,6 +1306,29 @@ void make_camera(const yr_camera_desc &c, Cam &o) {
 }
 V shoot(const Cam &c, float px, float py) { return normalize(c.vto + (c.vright * px + c.vup * py)); }
 
+// color_t::expgam_Adjust (color.h:175-195) as the shipped build evaluates
+// it: x = 1 - exp(e*max(x,0)) with the product in float and exp in double;
+// x = pow(max(x,0), gamma_R) in double; clamp to [0,1] only when neither
+void expgam_adjust(float *c, float e, float g, bool clamp_rgb) {
+    if (e == 0.f && g == 1.f) {
+        if (clamp_rgb)
+            for (int k = 0; k < 3; k++) c[k] = fmaxf(fminf(c[k], 1.f), 0.f);
+        return;
+    }
+    if (e != 0.f)
+        for (int k = 0; k < 3; k++) c[k] = (float)(1.0 - exp((double)(e * fmaxf(c[k], 0.f))));
+    if (g != 1.f)
+        for (int k = 0; k < 3; k++) c[k] = (float)pow((double)fmaxf(c[k], 0.f), (double)g);
+}
+
+// the scene's per-sample tone mapping (scene.cc:763, 807), when on
+void tonemap_sample(const Scene &S, float *rgba) {
+    if (!(S.rp.flags & YR_RENDER_TONEMAP)) return;
+    // scene_t::setExposure / setGamma (scene.h:162-163)
+    const float e = -S.rp.exposure, g = S.rp.gamma != 0.f ? (float)(1.0 / (double)S.rp.gamma) : 0.f;
+    expgam_adjust(rgba, e, g, (S.rp.flags & YR_RENDER_CLAMP_RGB) != 0);
+}
+
 // one camera sample: scene_t::raytrace (scene.cc:200-258)
 void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
     const uint32_t spp = S.rp.spp ? S.rp.spp : 1;
@@ -1321,6 +1344,7 @@ void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
     S.st.primary++;
     if (S.rp.raydepth <= 0) {
         rgba[0] = rgba[1] = rgba[2] = rgba[3] = 0.f;
+        tonemap_sample(S, rgba);
         return;
     }
     const V f = S.cam.pos + ray * kMinRay;
@@ -1330,6 +1354,7 @@ void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
         rgba[1] = S.rp.background[1];
         rgba[2] = S.rp.background[2];
         rgba[3] = 0.f;
+        tonemap_sample(S, rgba);
         return;
     }
     SP sp = surface(S, h.obj, h.tri, h.Z, f, ray);
@@ -1342,6 +1367,7 @@ void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
     rgba[1] = c.g;
     rgba[2] = c.b;
     rgba[3] = 1.f;
+    tonemap_sample(S, rgba);
 }
 
 // ----------------------------------------------------------- scene load
@@ -1416,8 +1442,12 @@ orc_scene *orc_load(const char *path) {
     orc_scene *o = new orc_scene;
     Scene &S = o->s;
     yr_camera_desc cam;
-    bool ok = rdv(f, magic, 4) && memcmp(magic, "YRS1", 4) == 0 && rdv(f, hdr, 4) && rdv(f, &cam, 1) &&
-              rdv(f, &S.rp, 1);
+    bool ok = rdv(f, magic, 4) && memcmp(magic, "YRS1", 4) == 0 && rdv(f, hdr, 4) && rdv(f, &cam, 1);
+    // render parameters before record version 3 end at exposure (gamma then 1)
+    memset(&S.rp, 0, sizeof(S.rp));
+    S.rp.gamma = 1.f;
+    const size_t rpsize = hdr[3] >= 3 ? sizeof(yr_render_params) : offsetof(yr_render_params, exposure);
+    ok = ok && fread(&S.rp, 1, rpsize, f) == rpsize;
     S.shaders.assign(hdr[1], yr_shader_desc());
     std::vector<yr_light_desc> ld(hdr[2]);
     // shader records before version 2 end at mod_mode
@@ -1604,6 +1634,8 @@ void orc_render(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint6
             } else {
                 memcpy(px, first, 16);
             }
+            if (S.rp.flags & YR_RENDER_ALPHA_PREMULTIPLY)  // colorA_t::alphaPremultiply
+                for (int k = 0; k < 3; k++) px[k] *= px[3];
         }
     if (stats) {
         stats[0] = S.st.primary;

@@ -314,6 +314,55 @@ def texture_render():
     np.savez_compressed(os.path.join(HERE, "render_textures_128x96.npz"), image=img)
 
 
+def tonemap_configs():
+    """The render block's tone mapping variants: clamp_rgb, exposure, gamma,
+    both, and gamma with alpha premultiply, on a constant background."""
+    return [dict(tonemap=True, clamp_rgb=True), dict(tonemap=True, exposure=1.5), dict(tonemap=True, gamma=2.2),
+            dict(tonemap=True, exposure=0.7, gamma=1.8), dict(tonemap=True, gamma=2.0, alpha_premultiply=True)]
+
+
+def tonemap_scene(cfg):
+    sc = smooth_scene()
+    sc.render = scenes.render_params(spp=3, background=(0.2, 0.3, 0.9), **cfg)
+    sc.camera = scenes.camera((0, 1.5, 4.5), (0, -0.3, 0), (0, 2.5, 4.5), 48, 36, fov_deg=70)
+    return sc
+
+
+def tonemap_renders():
+    imgs = [T.harness_render(tonemap_scene(c))[0] for c in tonemap_configs()]
+    np.savez_compressed(os.path.join(HERE, "render_tonemap_48x36.npz"), images=np.stack(imgs))
+
+
+def sample_images():
+    rng = np.random.default_rng(2)
+    a = rng.uniform(-0.2, 1.3, (17, 23, 4)).astype(np.float32)
+    b = np.zeros((6, 300, 4), np.float32)
+    b[:, 40:200] = (0.5, 0.25, 2.0, 1.0)
+    b[2:4] = rng.uniform(0, 100, (2, 300, 4))
+    c = rng.uniform(0, 5, (9, 5, 4)).astype(np.float32)
+    d = np.exp(rng.normal(0, 4, (8, 64, 4))).astype(np.float32)
+    return [a, b, c, d]
+
+
+def image_outputs():
+    """The reference's outTga_t (with and without alpha) and outHDR_t bytes
+    for a few float images (out-of-range values, runs, a row too narrow to
+    run-length encode, a wide dynamic range)."""
+    out = {}
+    with tempfile.TemporaryDirectory() as dd:
+        for i, im in enumerate(sample_images()):
+            ip = os.path.join(dd, "i.bin")
+            with open(ip, "wb") as f:
+                f.write(struct.pack("<2I", im.shape[1], im.shape[0]))
+                f.write(np.ascontiguousarray(im).tobytes())
+            out[f"img{i}"] = im
+            for kind in ("tga", "tga_alpha", "hdr"):
+                op = os.path.join(dd, "o.bin")
+                T.run_harness("imgout", kind, ip, op)
+                out[f"img{i}_{kind}"] = np.frombuffer(open(op, "rb").read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "image_outputs.npz"), **out)
+
+
 def halton_noise():
     with tempfile.TemporaryDirectory() as d:
         hp = os.path.join(d, "h.bin")
@@ -340,6 +389,8 @@ if __name__ == "__main__":
     smooth_render()
     textures()
     texture_render()
+    tonemap_renders()
+    image_outputs()
     illum()
     halton_noise()
     for f in sorted(os.listdir(HERE)):

@@ -202,6 +202,31 @@ def test_oracle_texture_render_matches_reference():
     assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
 
 
+@pytest.mark.parametrize("k", range(5))
+def test_oracle_tonemap_matches_reference(k):
+    """Per-sample expgam_Adjust (clamp_rgb, exposure, gamma, both) and alpha
+    premultiply on a constant background, against the reference's render."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    ref = load("render_tonemap_48x36.npz")["images"][k]
+    img, _ = T.OracleScene(make_golden.tonemap_scene(make_golden.tonemap_configs()[k])).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
+
+
+def test_image_outputs_match_reference():
+    """yr_image_encode (host code of the library) against the reference's
+    outTga_t / outHDR_t bytes for the same float images."""
+    from yafray_b200 import api
+    g = load("image_outputs.npz")
+    for i in range(4):
+        im = g[f"img{i}"]
+        assert api.encode_image(im, "tga") == g[f"img{i}_tga"].tobytes()
+        assert api.encode_image(im, "tga", alpha=True) == g[f"img{i}_tga_alpha"].tobytes()
+        assert api.encode_image(im, "hdr") == g[f"img{i}_hdr"].tobytes()
+
+
 def test_oracle_halton_and_ri_match_reference():
     g = load("qmc_noise.npz")
     lib = T.oracle()

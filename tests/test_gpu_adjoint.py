@@ -212,3 +212,25 @@ def test_grad_procedural_textures_and_modes(cuda):
     sc.render.spp = 2
     ds, g, fd = _check(torch, sc, _hidden(5), nsample=20, rtol=1e-3, seed=1)
     assert ds.param_count() == 4 * 8 + 2
+
+
+def test_grad_alpha_premultiply(cuda):
+    """With alpha premultiply the image is the sample average times its
+    alpha coverage; gradients follow through the coverage."""
+    import torch
+    sc = scenes.config_small(40, 30)
+    sc.render = scenes.render_params(spp=2, alpha_premultiply=True, background=(0.1, 0.2, 0.4))
+    _check(torch, sc, _hidden(6), nsample=5)
+
+
+def test_backward_refuses_tone_mapping(cuda):
+    """Per-sample exposure / gamma is not differentiated: refused."""
+    import torch
+    from yafray_b200 import abi
+    sc = scenes.config_small(16, 12)
+    sc.render = scenes.render_params(tonemap=True, gamma=2.2)
+    ds = api.DeviceScene(sc)
+    img = _render(torch, ds)
+    grad = torch.zeros(ds.param_count(), dtype=torch.float32, device="cuda")
+    with pytest.raises(abi.YrError):
+        ds.backward(img.data_ptr(), img.data_ptr(), grad.data_ptr())

@@ -191,3 +191,24 @@ def test_invalid_texture_records_rejected(cuda):
         sc.shaders = [s]
         with pytest.raises(RuntimeError):
             api.DeviceScene(sc)
+
+
+@pytest.mark.parametrize("k", range(5))
+def test_render_tone_mapping(cuda, k):
+    """Per-sample exposure / gamma / clamp (the loader's TGA path) and alpha
+    premultiply on a constant background, against the oracle."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.tonemap_scene(make_golden.tonemap_configs()[k])
+    img = api.DeviceScene(sc).render()
+    ref, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref)
+
+
+def test_tone_mapping_gamma_zero_refused(cuda):
+    sc = scenes.config_small(16, 12)
+    sc.render = scenes.render_params(tonemap=True, gamma=0.0)
+    with pytest.raises(RuntimeError):
+        api.DeviceScene(sc)

@@ -38,6 +38,9 @@ YR_LIGHT_POINT, YR_LIGHT_AREA, YR_LIGHT_HEMI, YR_LIGHT_PATH = 0, 1, 2, 3
 YR_BATCH_AUTO, YR_BATCH_TILES, YR_BATCH_WAVES = 0, 1, 2
 YR_TEXCO_GLOBAL, YR_TEXCO_ORCO, YR_TEXCO_NORMAL = 0, 1, 2
 YR_PROJ_DEFAULT, YR_PROJ_X, YR_PROJ_Y, YR_PROJ_Z, YR_PROJ_NONE = 0, 1, 2, 3, 4
+YR_RENDER_SHADOW_TREE, YR_RENDER_EXACT_ORDER, YR_RENDER_TONEMAP = 1, 2, 4
+YR_RENDER_CLAMP_RGB, YR_RENDER_ALPHA_PREMULTIPLY = 8, 16
+YR_IMAGE_TGA, YR_IMAGE_HDR, YR_IMAGE_ALPHA = 0, 1, 1
 YR_PER_TRIANGLE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
 
@@ -97,7 +100,9 @@ class YrLightDesc(C.Structure):
 class YrRenderParams(C.Structure):
     _fields_ = [("self_bias", C.c_float), ("raydepth", C.c_int32), ("spp", C.c_uint32),
                 ("aa_pixelwidth", C.c_float), ("seed", C.c_uint32), ("background", f3),
-                ("flags", C.c_uint32), ("region", C.c_int32 * 4)]
+                ("flags", C.c_uint32), ("region", C.c_int32 * 4),
+                # record version 3
+                ("exposure", C.c_float), ("gamma", C.c_float)]
 
 
 class YrObjectDesc(C.Structure):
@@ -185,6 +190,9 @@ SIGNATURES = {
     "yr_backward": (C.c_int, [_P, C.POINTER(YrBackwardDesc), _P, C.POINTER(C.c_float), _P]),
     "yr_backward_batch": (C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(YrBackwardDesc), C.POINTER(_P),
                                     C.POINTER(C.c_float), C.c_int32, _P]),
+    "yr_image_encode": (C.c_int, [C.c_int32, C.POINTER(C.c_float), C.c_int32, C.c_int32, C.c_int32, _P, C.c_size_t,
+                                  C.POINTER(C.c_size_t)]),
+    "yr_image_write": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_float), C.c_int32, C.c_int32, C.c_int32]),
 }
 
 _lib = None

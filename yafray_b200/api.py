@@ -172,3 +172,25 @@ def backward_batch(dss: List[DeviceScene], image_ptrs: List[int], target_ptrs: L
     abi.check(lib.yr_backward_batch(hs, n, descs, gp, losses.ctypes.data_as(C.POINTER(C.c_float)), int(streams),
                                     C.c_void_p(stream)), "yr_backward_batch")
     return losses
+
+
+def encode_image(rgba: np.ndarray, fmt: str = "tga", alpha: bool = False) -> bytes:
+    """The bytes YafRay's TGA (outTga_t) or Radiance HDR (outHDR_t) writer
+    produces for this float RGBA image (rows top first)."""
+    img = np.ascontiguousarray(rgba, np.float32)
+    h, w = img.shape[:2]
+    lib = abi.load()
+    f = {"tga": abi.YR_IMAGE_TGA, "hdr": abi.YR_IMAGE_HDR}[fmt]
+    flags = abi.YR_IMAGE_ALPHA if alpha else 0
+    fp = img.ctypes.data_as(C.POINTER(C.c_float))
+    n = C.c_size_t(0)
+    abi.check(lib.yr_image_encode(f, fp, w, h, flags, None, 0, C.byref(n)), "yr_image_encode")
+    out = (C.c_uint8 * n.value)()
+    abi.check(lib.yr_image_encode(f, fp, w, h, flags, out, n.value, C.byref(n)), "yr_image_encode")
+    return bytes(out)
+
+
+def write_image(path: str, rgba: np.ndarray, fmt: str = "tga", alpha: bool = False) -> None:
+    """Write a render as YafRay's loader would (TGA or HDR)."""
+    with open(path, "wb") as f:
+        f.write(encode_image(rgba, fmt, alpha))

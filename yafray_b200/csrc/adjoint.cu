@@ -170,15 +170,18 @@ __device__ __forceinline__ C3 sample_weight(const DevRender &R, const AdjWave &A
 }
 
 // --------------------------------------------------------------- kernels
-// dL/dpixel = 2 * scale * (img - target) over RGB; loss in double
+// dL/dpixel = 2 * scale * (img - target) over RGB; loss in double.  With
+// alpha premultiply the image is the average times its alpha, so the
+// gradient of the average is alpha times that.
 __global__ void __launch_bounds__(kBlock) k_adj_loss(const float4 *img, const float4 *target, uint32_t npix,
-                                                      float scale, float4 *gpix, double *loss) {
+                                                      float scale, int premultiply, float4 *gpix, double *loss) {
     double part = 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
         const float4 a = img[i], b = target[i];
         const float r = a.x - b.x, g = a.y - b.y, bl = a.z - b.z;
         part += (double)scale * ((double)r * r + (double)g * g + (double)bl * bl);
-        gpix[i] = make_float4(2.f * scale * r, 2.f * scale * g, 2.f * scale * bl, 0.f);
+        const float s2 = premultiply ? 2.f * scale * a.w : 2.f * scale;
+        gpix[i] = make_float4(s2 * r, s2 * g, s2 * bl, 0.f);
     }
     for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
     if ((threadIdx.x & 31) == 0 && part != 0.0) atomicAdd(loss, part);
@@ -367,6 +370,8 @@ static yr_status adj_plan(const yr_scene *scene, size_t budget, AdjPlan &A) {
     yr_status ret = make_plan(scene, A.P);
     if (ret != YR_OK) return ret;
     if (R.raydepth <= 0) return YR_ERR_UNSUPPORTED;
+    // per-sample exposure / gamma is not differentiated
+    if (R.tonemap && !(R.exposure == 0.f && R.gamma_r == 1.f && !R.clamp_rgb)) return YR_ERR_UNSUPPORTED;
     const Plan &P = A.P;
     uint64_t lo = 1, hi = P.rpix;
     while (lo < hi) {
@@ -406,7 +411,7 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
     cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
     k_adj_loss<<<grid_for(P.npix, kBlock), kBlock, 0, st>>>((const float4 *)desc->image,
                                                              (const float4 *)desc->target, P.npix, desc->loss_scale,
-                                                             (float4 *)A.gpix, d_loss);
+                                                             scene->rdr.premultiply, (float4 *)A.gpix, d_loss);
     const DevScene &D = scene->dev;
     const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
 #if YR_TRACE_GRID_PERSIST

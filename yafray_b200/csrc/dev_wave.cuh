@@ -691,6 +691,27 @@ static __global__ void __launch_bounds__(kBlock) k_gather_path(DevRender R, Wave
 }
 #endif
 
+// color_t::expgam_Adjust (color.h:175-195) in the shipped build's form:
+// with exposure e != 0, x = 1 - exp(e*max(x,0)) (the product in float, exp in
+// double); with gamma_R != 1, x = pow(max(x,0), gamma_R) in double; with
+// neither, clamp to [0,1] when clamp_rgb.
+__device__ __forceinline__ C3 expgam_adjust(const C3 &c, float e, float g, bool clamp_rgb) {
+    float v[3] = {c.r, c.g, c.b};
+    if (e == 0.0f && g == 1.0f) {
+        if (clamp_rgb)
+#pragma unroll
+            for (int k = 0; k < 3; k++) v[k] = fmaxf(fminf(v[k], 1.0f), 0.0f);
+        return c3(v[0], v[1], v[2]);
+    }
+    if (e != 0.0f)
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = (float)(1.0 - exp((double)(e * fmaxf(v[k], 0.0f))));
+    if (g != 1.0f)
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = (float)pow((double)fmaxf(v[k], 0.0f), (double)g);
+    return c3(v[0], v[1], v[2]);
+}
+
 // one pixel of the wave: AA average of its camera samples
 __device__ __forceinline__ void st_finish(const DevRender &R, const Wave &W, uint32_t px) {
     float4 first = make_float4(0.f, 0.f, 0.f, 0.f), tot = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -729,6 +750,7 @@ __device__ __forceinline__ void st_finish(const DevRender &R, const Wave &W, uin
         } else {
             col = R.background;
         }
+        if (R.tonemap) col = expgam_adjust(col, R.exposure, R.gamma_r, R.clamp_rgb != 0);
         const float4 c4 = make_float4(col.r, col.g, col.b, hit ? 1.f : 0.f);
         if (s == 0) {
             first = c4;
@@ -745,6 +767,7 @@ __device__ __forceinline__ void st_finish(const DevRender &R, const Wave &W, uin
         const float d = (float)(1 + (R.spp - 1));
         o = make_float4((first.x + tot.x) / d, (first.y + tot.y) / d, (first.z + tot.z) / d, (first.w + tot.w) / d);
     }
+    if (R.premultiply) o = make_float4(o.x * o.w, o.y * o.w, o.z * o.w, o.w);  // colorA_t::alphaPremultiply
     int x, y;
     const uint32_t pixel = cs_pixel(R, W.base + px * R.spp, x, y);
     reinterpret_cast<float4 *>(W.out)[pixel] = o;

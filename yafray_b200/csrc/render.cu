@@ -54,7 +54,9 @@ static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W,
     if (P.rpix != P.npix) cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
     const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
     if (R.raydepth <= 0) {
-        // raytrace() returns black at the ray-level cap (scene.cc:204-209)
+        // raytrace() returns black at the ray-level cap (scene.cc:204-209);
+        // a tone map keeps black black except pow(0, 0) = 1 for gamma 0,
+        // which is refused when the scene is created
         cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
     } else {
 #if YR_TRACE_GRID_PERSIST

@@ -712,6 +712,15 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     R.totsamdiv = R.spp > 1 ? (float)(1.0 / (float)(R.spp - 1)) : 0.f;
     R.seed = desc->render.seed;
     R.self_bias = desc->render.self_bias;
+    // scene_t::setExposure / setGamma (scene.h:162-163), tonemap, clampRGB,
+    // alphaPremultiply
+    R.tonemap = (desc->render.flags & YR_RENDER_TONEMAP) ? 1 : 0;
+    R.clamp_rgb = (desc->render.flags & YR_RENDER_CLAMP_RGB) ? 1 : 0;
+    R.premultiply = (desc->render.flags & YR_RENDER_ALPHA_PREMULTIPLY) ? 1 : 0;
+    R.exposure = -desc->render.exposure;
+    // gamma 0 makes every sample pow(x, 0) = 1 (white); not supported
+    if (R.tonemap && desc->render.gamma == 0.0f) return fail(YR_ERR_UNSUPPORTED);
+    R.gamma_r = desc->render.gamma != 0.0f ? (float)(1.0 / (double)desc->render.gamma) : 0.0f;
     R.raydepth = desc->render.raydepth;
     R.background = c3(desc->render.background[0], desc->render.background[1], desc->render.background[2]);
     {

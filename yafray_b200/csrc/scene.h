@@ -79,6 +79,11 @@ struct DevRender {
     int path_light;             // index of the path light or -1
     int path_samples;
     int path_depth;
+    int tonemap;                // YR_RENDER_TONEMAP
+    int clamp_rgb;              // YR_RENDER_CLAMP_RGB
+    int premultiply;            // YR_RENDER_ALPHA_PREMULTIPLY
+    float exposure;             // scene_t::exposure = -"exposure"
+    float gamma_r;              // scene_t::gamma_R = 1/"gamma" (0 for gamma 0)
 };
 
 // Device allocation tracked by the scene (freed in yr_scene_destroy).

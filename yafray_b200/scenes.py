@@ -304,7 +304,11 @@ def camera(pos, look, up, resx, resy, fov_deg=45.0, aspect=1.0) -> abi.YrCameraD
     return c
 
 
-def render_params(spp=1, seed=0, bias=0.1, raydepth=3, pixelwidth=1.0, background=(0.0, 0.0, 0.0)):
+def render_params(spp=1, seed=0, bias=0.1, raydepth=3, pixelwidth=1.0, background=(0.0, 0.0, 0.0),
+                  exposure=0.0, gamma=1.0, tonemap=False, clamp_rgb=False, alpha_premultiply=False):
+    """The render block's parameters (loader/render.cc:1025-1225); `tonemap`
+    is what the loader sets for TGA output (exposure / gamma / clamp_rgb per
+    camera sample), off for HDR / EXR."""
     r = abi.YrRenderParams()
     r.self_bias = float(bias)
     r.raydepth = int(raydepth)
@@ -312,7 +316,10 @@ def render_params(spp=1, seed=0, bias=0.1, raydepth=3, pixelwidth=1.0, backgroun
     r.aa_pixelwidth = float(pixelwidth)
     r.seed = int(seed) & 0xFFFFFFFF
     r.background[:] = [float(x) for x in background]
-    r.flags = 0
+    r.flags = ((abi.YR_RENDER_TONEMAP if tonemap else 0) | (abi.YR_RENDER_CLAMP_RGB if clamp_rgb else 0) |
+               (abi.YR_RENDER_ALPHA_PREMULTIPLY if alpha_premultiply else 0))
+    r.exposure = float(exposure)
+    r.gamma = float(gamma)
     return r
 
 
@@ -459,8 +466,9 @@ def write_yrs(sc: Scene, path: str) -> None:
     with open(path, "wb") as f:
         f.write(b"YRS1")
         # last header word: record version; 1 = object records carry the
-        # smoothing angle; 2 = shader records carry the version-2 texture fields
-        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 2))
+        # smoothing angle; 2 = shader records carry the version-2 texture
+        # fields; 3 = render parameters carry exposure and gamma
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 3))
         f.write(bytes(sc.camera))
         f.write(bytes(sc.render))
         for s in sc.shaders:
@@ -486,8 +494,13 @@ def read_yrs(path: str) -> Scene:
     sc = Scene()
     sc.camera = abi.YrCameraDesc.from_buffer_copy(data, off)
     off += C_sizeof(abi.YrCameraDesc)
-    sc.render = abi.YrRenderParams.from_buffer_copy(data, off)
-    off += C_sizeof(abi.YrRenderParams)
+    # render parameters before version 3 end at exposure (gamma then 1)
+    rpsize = C_sizeof(abi.YrRenderParams) if version >= 3 else abi.YrRenderParams.exposure.offset
+    sc.render = abi.YrRenderParams()
+    C_memmove(sc.render, data[off:off + rpsize])
+    if version < 3:
+        sc.render.gamma = 1.0
+    off += rpsize
     # shader records before version 2 end at mod_mode
     shsize = C_sizeof(abi.YrShaderDesc) if version >= 2 else abi.YrShaderDesc.mod_mode.offset
     for _ in range(nsh):
