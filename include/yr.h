@@ -117,6 +117,11 @@ typedef struct yr_object_node {
     int32_t right;
 } yr_object_node;
 
+/* referenceObject_t::getBound (reference.cc:135-165): the box of the eight
+ * corners of `bound` (min xyz, max xyz) placed by the row-major 4x4 matrix
+ * M, as the object tree sees an instance. */
+YR_API yr_status yr_instance_bound(const float *bound, const float *matrix, float *out);
+
 /* buildObjectTree (object3d.cc:30-53): greedy nearest-pair clustering of
  * the objects' bounds (6 floats each: min xyz, max xyz) with the
  * bound_distance metric, in object-list order.  `out` must hold 2n-1 nodes. */
@@ -321,6 +326,27 @@ typedef struct yr_object_desc {
                                 one normal per vertex, else per corner over
                                 the faces within the angle                    */
     uint32_t reserved;
+    const float *instance_matrix; /* non-NULL: this object is a reference to
+                                object `instance_of` (referenceObject_t,
+                                reference.cc:9-171): that mesh placed by the
+                                row-major 4x4 matrix M (16 floats).  Rays are
+                                taken into the mesh's space by M's inverse
+                                and hits brought back by M (points) and the
+                                row-normalised rotation part of M (normals);
+                                the geometry fields above are ignored and the
+                                shader and shadow flag are the original's.
+                                An instance of an instance is refused.      */
+    const float *instance_inverse; /* optional M^-1 (16 floats, row-major);
+                                NULL = computed here by Gauss-Jordan with
+                                exact divisions.  The reference computes it
+                                with the shipped build's vectorised division
+                                (an approximate reciprocal refined once, whose
+                                last bit depends on the CPU: 1/1 gives
+                                0.99999994 on x86), so a caller that wants the
+                                reference's rays bit for bit passes
+                                referenceObject_t::back here.                */
+    uint32_t instance_of;
+    uint32_t reserved2;
 } yr_object_desc;
 
 #define YR_PER_TRIANGLE 0xffffffffu

@@ -8,6 +8,7 @@
 //   yr_ref_harness tree    SCENE OUT           kd-trees + object tree
 //   yr_ref_harness rays    SCENE RAYS OUT      kd / scene ray queries
 //   yr_ref_harness camera  SCENE OUT           primary ray directions
+//   yr_ref_harness instmat SCENE OUT           each reference's M^-1 (back)
 //   yr_ref_harness render  SCENE OUT THREADS [x0 x1 y0 y1 [REPEATS]]
 //                                              stock scene_t::render, float sink,
 //                                              ray counts, one JSON line per render
@@ -30,6 +31,7 @@
 #include "scene.h"
 #include "threadedscene.h"
 #include "mesh.h"
+#include "reference.h"
 #include "kdtree.h"
 #include "camera.h"
 #include "noise.h"
@@ -122,6 +124,8 @@ struct SceneFile {
     struct Obj {
         uint32_t nv, nt, shader, cast;
         float smooth;
+        int32_t inst;  // >= 0: a reference to that object, placed by M
+        float M[16];
         std::vector<float> v;
         std::vector<uint32_t> t;
         std::vector<uint32_t> tri_shader;  // when shader == YR_PER_TRIANGLE
@@ -160,6 +164,19 @@ static void load_scene(const char *path, SceneFile &s) {
         SceneFile::Obj &o = s.objs[i];
         o.smooth = 0.f;
         if (hdr[3] >= 1) rd(f, &o.smooth, 4);  // record version 1: smoothing angle
+        o.inst = -1;
+        if (hdr[3] >= 4) rd(f, &o.inst, 4);    // record version 4: reference index (+ matrix)
+        if (o.inst >= 0) {
+            rd(f, o.M, 64);
+            int32_t has_inv = 0;
+            float inv[16];
+            rd(f, &has_inv, 4);  // a given M^-1 is the library's input; the reference computes its own
+            if (has_inv) rd(f, inv, 64);
+            o.nv = o.nt = 0;
+            o.shader = oh[2];
+            o.cast = oh[3];
+            continue;
+        }
         o.nv = oh[0];
         o.nt = oh[1];
         o.shader = oh[2];
@@ -180,7 +197,8 @@ static void load_scene(const char *path, SceneFile &s) {
 struct RefScene {
     scene_t *scene;
     camera_t *camera;
-    std::vector<meshObject_t *> meshes;
+    std::vector<meshObject_t *> meshes;   // per object; NULL for references
+    std::vector<object3d_t *> objs;       // per object
     std::vector<shader_t *> shaders;
     std::vector<texture_t *> textures;
     std::vector<light_t *> lights;
@@ -311,6 +329,11 @@ static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true) 
     for (size_t i = 0; i < s.shaders.size(); i++) r.shaders.push_back(make_shader(s.shaders[i], r.textures));
     for (size_t i = 0; i < s.objs.size(); i++) {
         const SceneFile::Obj &o = s.objs[i];
+        if (o.inst >= 0) {  // made below, once the meshes exist
+            r.meshes.push_back(NULL);
+            r.objs.push_back(NULL);
+            continue;
+        }
         std::vector<point3d_t> ver(o.nv);
         for (uint32_t k = 0; k < o.nv; k++) ver[k] = P3(&o.v[3 * k]);
         std::vector<triangle_t> ts(o.nt);
@@ -326,9 +349,22 @@ static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true) 
         m->castShadows(o.cast != 0);
         if (o.smooth >= 1.f) m->autoSmooth(o.smooth);  // as the loader does (render.cc:764)
         r.meshes.push_back(m);
+        r.objs.push_back(m);
         r.objindex[m] = (int)i;
-        r.scene->addObject(m);
     }
+    // references (the loader's objects with an "original", render.cc:672-680)
+    for (size_t i = 0; i < s.objs.size(); i++) {
+        const SceneFile::Obj &o = s.objs[i];
+        if (o.inst < 0) continue;
+        if ((size_t)o.inst >= r.meshes.size() || !r.meshes[o.inst]) die("reference to a missing mesh");
+        matrix4x4_t M(1);
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) M[a][b] = o.M[4 * a + b];
+        referenceObject_t *ro = referenceObject_t::factory(M, r.meshes[o.inst]);
+        r.objs[i] = ro;
+        r.objindex[ro] = (int)i;
+    }
+    for (size_t i = 0; i < r.objs.size(); i++) r.scene->addObject(r.objs[i]);
     const yr_camera_desc &c = s.cam;
     r.camera = new camera_t(P3(c.pos), P3(c.look), P3(c.up), c.resx, c.resy, c.aspect, c.focal, 0, 0, false,
                             camera_t::CM_PERSPECTIVE, camera_t::BK_DISK1, camera_t::BB_NONE, 0);
@@ -362,10 +398,12 @@ static void cmd_tree(const SceneFile &s, const char *out) {
     build_ref(s, r, false);
     FILE *f = fopen(out, "wb");
     if (!f) die("cannot open output");
-    uint32_t n = (uint32_t)r.meshes.size();
+    uint32_t n = 0;  // trees of the meshes (references share their original's)
+    for (size_t i = 0; i < r.meshes.size(); i++) n += r.meshes[i] ? 1 : 0;
     wr(f, &n, 4);
     for (size_t i = 0; i < r.meshes.size(); i++) {
         meshObject_t *m = r.meshes[i];
+        if (!m) continue;
         kdTree_t *t = m->n_tree;
         const triangle_t *base = &m->triangles[0];
         std::vector<uint32_t> nodes, prims;
@@ -488,16 +526,43 @@ static void cmd_rays(const SceneFile &s, const char *rays_path, const char *out)
             if (h) {
                 o[1] = r.objindex[sp.getObject()];
                 meshObject_t *m = r.meshes.at(o[1]);
+                if (!m) m = r.meshes.at(s.objs[o[1]].inst);  // a reference: the original's triangle
                 o[2] = (uint32_t)((const triangle_t *)sp.getOrigin() - &m->triangles[0]);
                 float zf = sp.Z();
                 memcpy(&o[3], &zf, 4);
             }
         } else if (q.mode == 3) {
-            surfacePoint_t sp(r.meshes.at(q.object), from, from, vector3d_t(0, 0, 1), vector3d_t(0, 0, 1), 0, 0,
+            surfacePoint_t sp(r.objs.at(q.object), from, from, vector3d_t(0, 0, 1), vector3d_t(0, 0, 1), 0, 0,
                               color_t(0.0), 0);
             o[0] = r.scene->isShadowed(state, sp, P3(q.l));
         }
         wr(f, o, 16);
+    }
+    fclose(f);
+}
+
+// -------------------------------------------------------------- references
+// Each reference's M^-1 as referenceObject_t computes it (back,
+// reference.cc:13-14): u32 count, then per reference u32 object index and
+// 16 floats.
+static void cmd_instmat(const SceneFile &s, const char *out) {
+    RefScene r;
+    build_ref(s, r, false);
+    std::vector<uint32_t> idx;
+    for (size_t i = 0; i < r.objs.size(); i++)
+        if (!r.meshes[i]) idx.push_back((uint32_t)i);
+    FILE *f = fopen(out, "wb");
+    if (!f) die("cannot open output");
+    uint32_t n = (uint32_t)idx.size();
+    wr(f, &n, 4);
+    for (size_t k = 0; k < idx.size(); k++) {
+        const referenceObject_t *ro = (const referenceObject_t *)r.objs[idx[k]];
+        wr(f, &idx[k], 4);
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) {
+                const float v = ro->back[a][b];
+                wr(f, &v, 4);
+            }
     }
     fclose(f);
 }
@@ -543,7 +608,7 @@ static void cmd_render(const SceneFile &s, const char *out, int threads, const i
         // threadedscene_t holds its own copy of the scene state; rebuild through it
         tsc = (threadedscene_t *)threadedscene_t::factory();
         tsc->setCPUs(threads);
-        for (size_t i = 0; i < r.meshes.size(); i++) tsc->addObject(r.meshes[i]);
+        for (size_t i = 0; i < r.objs.size(); i++) tsc->addObject(r.objs[i]);
         for (size_t i = 0; i < r.lights.size(); i++) tsc->addLight(r.lights[i]);
         tsc->setCamera(r.camera);
         tsc->setBias(s.rp.self_bias);
@@ -845,6 +910,8 @@ int main(int argc, char **argv) {
     } else if (cmd == "rays") {
         if (argc < 5) die("rays SCENE RAYS OUT");
         cmd_rays(s, argv[3], argv[4]);
+    } else if (cmd == "instmat") {
+        cmd_instmat(s, argv[3]);
     } else if (cmd == "texeval") {
         if (argc < 5) die("texeval SCENE POINTS OUT");
         cmd_texeval(s, argv[3], argv[4]);

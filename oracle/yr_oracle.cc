@@ -140,7 +140,76 @@ struct Obj {
     std::vector<uint32_t> prims;
     Box tb, ob;
     bool cast;
+    // a reference (referenceObject_t): the original object, the first three
+    // rows of M and of its inverse, and M's rows normalised (reference.cc:9-46)
+    int inst = -1;
+    float m[12], back[12], rot[9];
 };
+
+// matrix4x4_t * point3d_t as the shipped build groups it
+V xf_point(const float *m, const V &p) {
+    return V((m[0] * p.x + m[1] * p.y) + (m[2] * p.z + m[3]), (m[4] * p.x + m[5] * p.y) + (m[6] * p.z + m[7]),
+             (m[8] * p.x + m[9] * p.y) + (m[10] * p.z + m[11]));
+}
+// matrix4x4_t * vector3d_t
+V xf_vec(const float *m, const V &v) {
+    return V((m[0] * v.x + m[1] * v.y) + m[2] * v.z, (m[4] * v.x + m[5] * v.y) + m[6] * v.z,
+             (m[8] * v.x + m[9] * v.y) + m[10] * v.z);
+}
+V rot_vec(const float *r, const V &v) {
+    return V((r[0] * v.x + r[1] * v.y) + r[2] * v.z, (r[3] * v.x + r[4] * v.y) + r[5] * v.z,
+             (r[6] * v.x + r[7] * v.y) + r[8] * v.z);
+}
+
+// referenceObject_t ctor: back = M.inverse() (matrix4x4_t::inverse,
+// matrix4.cc:68-117: Gauss-Jordan, pivot on the largest |m[k][i]|, rows
+// divided by the pivot then reduced), MRot = M's rows normalised
+bool make_instance(Obj &o, const float *M) {
+    float a[4][4], id[4][4];
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            a[i][j] = M[4 * i + j];
+            id[i][j] = i == j ? 1.f : 0.f;
+        }
+    for (int i = 0; i < 4; i++) {
+        float mx = 0;
+        int ci = 0;
+        for (int k = i; k < 4; k++)
+            if (fabsf(a[k][i]) > mx) {
+                mx = fabsf(a[k][i]);
+                ci = k;
+            }
+        if (mx == 0) return false;
+        for (int j = 0; j < 4; j++) {
+            float t = a[i][j];
+            a[i][j] = a[ci][j];
+            a[ci][j] = t;
+            t = id[i][j];
+            id[i][j] = id[ci][j];
+            id[ci][j] = t;
+        }
+        float f = a[i][i];
+        for (int j = 0; j < 4; j++) a[i][j] /= f;
+        for (int j = 0; j < 4; j++) id[i][j] /= f;
+        for (int k = 0; k < 4; k++) {
+            if (k == i) continue;
+            f = a[k][i];
+            for (int j = 0; j < 4; j++) a[k][j] -= a[i][j] * f;
+            for (int j = 0; j < 4; j++) id[k][j] -= id[i][j] * f;
+        }
+    }
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 4; j++) {
+            o.m[4 * i + j] = M[4 * i + j];
+            o.back[4 * i + j] = id[i][j];
+        }
+        const V r = normalize(V(M[4 * i], M[4 * i + 1], M[4 * i + 2]));
+        o.rot[3 * i] = r.x;
+        o.rot[3 * i + 1] = r.y;
+        o.rot[3 * i + 2] = r.z;
+    }
+    return true;
+}
 
 struct ONode {
     Box b;
@@ -345,6 +414,15 @@ struct Hit {
 };
 
 // closest hit: raytrace (limit passed to shoot) or firstHit (scene.cc:200-258, 688-721)
+// object3d_t::shoot: a mesh walks its own tree; a reference walks its
+// original's with origin and direction taken there by M's inverse
+// (referenceObject_t::shoot, reference.cc:95-114; not renormalised)
+bool shoot(Scene &S, int oi, const V &from, const V &ray, float dist, uint32_t &tr, float &Z, bool any) {
+    const Obj &o = S.objs[oi];
+    if (o.inst < 0) return kd_intersect(S, o, from, ray, dist, tr, Z, any);
+    return kd_intersect(S, S.objs[o.inst], xf_point(o.back, from), xf_vec(o.back, ray), dist, tr, Z, any);
+}
+
 Hit closest(Scene &S, const V &f, const V &ray, bool pass_limit, bool shadow_only) {
     Hit best = {-1, 0, 0};
     float limit = kInf;
@@ -355,7 +433,7 @@ Hit closest(Scene &S, const V &f, const V &ray, bool pass_limit, bool shadow_onl
             float dis = pass_limit ? limit : kInf;
             float Z = dis;
             uint32_t tr = 0;
-            if (kd_intersect(S, o, f, ray, dis, tr, Z, false) && Z > 0) {
+            if (shoot(S, it.current, f, ray, dis, tr, Z, false) && Z > 0) {
                 if (pass_limit) limit = Z;
                 it.limit(Z);
                 if (best.obj < 0 || Z < best.Z) {
@@ -380,7 +458,7 @@ bool shadowed(Scene &S, const V &p, int own, const V &ray, float dist) {
         if (o.cast) {
             float Z = dist;
             uint32_t tr;
-            if (kd_intersect(S, o, it.current == own ? self : p2, ray, dist, tr, Z, true)) return true;
+            if (shoot(S, it.current, it.current == own ? self : p2, ray, dist, tr, Z, true)) return true;
         }
         it.next();
     }
@@ -1014,6 +1092,7 @@ TexVal texture_eval(const yr_shader_desc &d, const V &p) {
 // --------------------------------------------------------------- shading
 struct SP {
     V P, N, Ng, NU, NV;
+    V orco;  // toObjectOrco(P): P, or M^-1 P on a reference
     int obj;
     int shader;
 };
@@ -1035,10 +1114,16 @@ V reflectv(const V &n, const V &v) {
     return (2 * vn) * n - v;
 }
 
-SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from, const V &ray) {
+SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from_w, const V &ray_w) {
     SP s;
+    // a reference's hit is formed in its original's space (the ray taken
+    // there by M's inverse), then N, Ng, NU, NV go back by MRot and P by M
+    // (referenceObject_t::shoot, reference.cc:95-114)
+    const Obj &ow = S.objs[obj];
+    const bool ref = ow.inst >= 0;
+    const V from = ref ? xf_point(ow.back, from_w) : from_w, ray = ref ? xf_vec(ow.back, ray_w) : ray_w;
     s.P = from + Z * ray;
-    const Obj &o = S.objs[obj];
+    const Obj &o = ref ? S.objs[ow.inst] : ow;
     s.N = s.Ng = o.tri_n[tri];
     if (o.smooth) {
         // triangle_t::getSurface + getInterpolation (triangle.cc:74-155), in
@@ -1062,6 +1147,15 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from, const 
                           na.z * fa + (nb.z * fb + nc.z * fc)));
     }
     createCS(s.N, s.NU, s.NV);
+    s.orco = s.P;
+    if (ref) {
+        s.N = rot_vec(ow.rot, s.N);
+        s.Ng = rot_vec(ow.rot, s.Ng);
+        s.P = xf_point(ow.m, s.P);
+        s.NU = rot_vec(ow.rot, s.NU);
+        s.NV = rot_vec(ow.rot, s.NV);
+        s.orco = xf_point(ow.back, s.P);  // referenceObject_t::toObjectOrco
+    }
     s.obj = obj;
     s.shader = (int)o.tri_shader[tri];
     return s;
@@ -1073,7 +1167,8 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from, const 
 // orco data: P) or "normal", then projections size*(src[axis] + ofs) /
 // size*ofs
 V tex_point(const yr_shader_desc &d, const SP &sp) {
-    const V src = (d.tex_map & 0xffu) == YR_TEXCO_NORMAL ? sp.N : sp.P;
+    const uint32_t tc = d.tex_map & 0xffu;
+    const V src = tc == YR_TEXCO_NORMAL ? sp.N : (tc == YR_TEXCO_ORCO ? sp.orco : sp.P);
     float t[3];
     for (int k = 0; k < 3; k++) {
         const uint32_t pc = (d.tex_map >> (8 * (k + 1))) & 0xffu;
@@ -1458,8 +1553,20 @@ orc_scene *orc_load(const char *path) {
     for (uint32_t i = 0; ok && i < hdr[0]; i++) {
         uint32_t oh[4];
         float smooth_angle = 0.f;
-        ok = rdv(f, oh, 4) && (hdr[3] < 1 || rdv(f, &smooth_angle, 1));
+        int32_t inst = -1;
+        ok = rdv(f, oh, 4) && (hdr[3] < 1 || rdv(f, &smooth_angle, 1)) && (hdr[3] < 4 || rdv(f, &inst, 1));
         if (!ok) break;
+        if (inst >= 0) {  // record version 4: a reference, its matrix, and M^-1 when given
+            float M[16], inv[16];
+            int32_t has_inv = 0;
+            ok = rdv(f, M, 16) && rdv(f, &has_inv, 1) && (!has_inv || rdv(f, inv, 16)) && (uint32_t)inst < hdr[0] &&
+                 make_instance(S.objs[i], M);
+            if (ok && has_inv)
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 4; b++) S.objs[i].back[4 * a + b] = inv[4 * a + b];
+            S.objs[i].inst = inst;
+            continue;
+        }
         std::vector<float> v(3 * (size_t)oh[0]);
         std::vector<uint32_t> t(3 * (size_t)oh[1]), ts;
         ok = rdv(f, v.data(), v.size()) && rdv(f, t.data(), t.size());
@@ -1480,6 +1587,12 @@ orc_scene *orc_load(const char *path) {
         if (ok && smooth_angle >= 1.f) auto_smooth(ob, t, oh[0], smooth_angle);
     }
     fclose(f);
+    // references take the shadow flag of their original (reference.cc:41)
+    for (size_t i = 0; ok && i < S.objs.size(); i++)
+        if (S.objs[i].inst >= 0) {
+            if (S.objs[S.objs[i].inst].inst >= 0) ok = false;  // no reference to a reference
+            else S.objs[i].cast = S.objs[S.objs[i].inst].cast;
+        }
     if (!ok) {
         delete o;
         return NULL;

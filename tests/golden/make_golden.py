@@ -363,6 +363,60 @@ def image_outputs():
     np.savez_compressed(os.path.join(HERE, "image_outputs.npz"), **out)
 
 
+def instance_scene():
+    """References (referenceObject_t): a smoothed torus and a smoothed,
+    orco-textured sphere, each placed twice by rotation, non-uniform scale and
+    translation (the originals moved off to the side), over a plane."""
+    sc = scenes.config_small(96, 72)
+    tv, tt = scenes.torus((0.0, 0.0, 0.0), 0.6, 0.25, nu=24, nv=12)
+    sv, st = scenes.uv_sphere((0.0, 0.0, 0.0), 0.5, rings=10, segments=20)
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    sc.shaders = [scenes.shader((0.8, 0.6, 0.5), (0.4, 0.4, 0.4), hard=20.0),
+                  scenes.texture_shader((0.5, 0.5, 0.5), "marble", (0.9, 0.9, 0.8), (0.2, 0.3, 0.5), texco="orco",
+                                        turbulence=2.0, size=2.0, mod_color=0.9),
+                  scenes.shader((0.8, 0.8, 0.8))]
+    sc.meshes = [scenes.Mesh(tv + np.float32([5.0, 0.0, 0.0]), tt, 0, smooth_angle=40.0),
+                 scenes.Mesh(sv, st, 1, smooth_angle=180.0), scenes.Mesh(pv, pt, 2),
+                 scenes.instance(0, scenes.transform((-6.4, -0.4, 0.3), (30, 0, 10), (1.0, 1.0, 1.0))),
+                 scenes.instance(0, scenes.transform((-3.7, 0.1, -0.5), (70, 20, 0), (1.2, 0.7, 1.0))),
+                 scenes.instance(1, scenes.transform((0.2, 0.8, -1.2), (0, 45, 0), (1.5, 0.6, 1.5))),
+                 scenes.instance(1, scenes.transform((-0.3, -0.6, 1.2), (10, 0, 0), (0.5, 0.5, 0.5)))]
+    sc.lights = [scenes.point_light((2.0, 4.0, 3.0), 14.0)]
+    sc.camera = scenes.camera((0.0, 1.5, 4.5), (0.0, -0.2, 0.0), (0.0, 2.5, 4.5), 96, 72, fov_deg=60)
+    return sc
+
+
+def instance_rays(n=2000, seed=4):
+    rng = np.random.default_rng(seed)
+    frm = rng.uniform(-2.5, 2.5, (n, 3)).astype(np.float32)
+    frm[:, 1] = rng.uniform(-0.9, 2.0, n)
+    tgt = rng.uniform(-2, 2, (n, 3)).astype(np.float32)
+    tgt[:, 1] = rng.uniform(-1.2, 1.2, n)
+    d = tgt - frm
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    own = rng.integers(0, 7, n)
+    return frm, d.astype(np.float32), tgt, own
+
+
+def instances():
+    """The reference's M^-1 of each reference, its object tree (the placed
+    boxes), closest and shadow answers through the references, and a render."""
+    sc = instance_scene()
+    inv = T.harness_instance_inverses(sc)
+    _, ot = T.harness_trees(sc)
+    frm, d, tgt, own = instance_rays()
+    recs = np.zeros(len(frm), T.RAY_REC)
+    recs["mode"], recs["frm"], recs["dir"], recs["dist"] = 2, frm, d, -1
+    closest = T.harness_rays(sc, recs)
+    recs3 = np.zeros(len(frm), T.RAY_REC)
+    recs3["mode"], recs3["frm"], recs3["object"], recs3["l"] = 3, frm, own, tgt
+    shadow = T.harness_rays(sc, recs3)[:, 0]
+    img, _ = T.harness_render(sc)
+    np.savez_compressed(os.path.join(HERE, "instances.npz"), inv_idx=np.array(sorted(inv)),
+                        inv=np.stack([inv[i] for i in sorted(inv)]), otree=ot, closest=closest, shadow=shadow,
+                        image=img)
+
+
 def halton_noise():
     with tempfile.TemporaryDirectory() as d:
         hp = os.path.join(d, "h.bin")
@@ -391,6 +445,7 @@ if __name__ == "__main__":
     texture_render()
     tonemap_renders()
     image_outputs()
+    instances()
     illum()
     halton_noise()
     for f in sorted(os.listdir(HERE)):

@@ -212,3 +212,26 @@ def test_tone_mapping_gamma_zero_refused(cuda):
     sc.render = scenes.render_params(tonemap=True, gamma=0.0)
     with pytest.raises(RuntimeError):
         api.DeviceScene(sc)
+
+
+@pytest.mark.parametrize("gi", [False, True])
+@pytest.mark.parametrize("reference_inverses", [False, True])
+def test_render_instances(cuda, gi, reference_inverses):
+    """References (instanced meshes) shaded through MRot / M, orco at M^-1 P,
+    smoothed originals; point light, and area light + path GI."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.instance_scene()
+    if reference_inverses:
+        g = np.load(os.path.join(T.GOLDEN, "instances.npz"))
+        for i, inv in zip(g["inv_idx"], g["inv"]):
+            sc.meshes[int(i)].inverse = inv
+    if gi:
+        sc.lights = [scenes.quad_light_down(0.0, 4.0, 0.5, 2.0, 2.0, 30.0, 4),
+                     scenes.path_light(samples=1, depth=2, power=1.0)]
+        sc.render.spp = 2
+    img = api.DeviceScene(sc).render()
+    ref, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref, frac=0.995 if gi else 0.999)

@@ -108,3 +108,54 @@ def test_empty_query(cuda):
     sc = scenes.config_small(32, 24)
     ds = api.DeviceScene(sc)
     assert _run_closest(cuda, ds, np.zeros((0, 8), np.float32)).shape == (0, 4)
+
+
+def _instance_scene(reference_inverses):
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.instance_scene()
+    if reference_inverses:
+        g = np.load(os.path.join(T.GOLDEN, "instances.npz"))
+        for i, inv in zip(g["inv_idx"], g["inv"]):
+            sc.meshes[int(i)].inverse = inv
+    return make_golden, sc
+
+
+@pytest.mark.parametrize("reference_inverses", [False, True])
+@pytest.mark.parametrize("exact", [False, True])
+def test_instances_closest_and_shadow(cuda, reference_inverses, exact):
+    """Rays through references (referenceObject_t): the original's tree with
+    the ray taken there by M^-1; hits and shadow answers bit for bit."""
+    mg, sc = _instance_scene(reference_inverses)
+    if exact:
+        sc.render.flags = EXACT
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    frm, d, tgt, own = mg.instance_rays(20000, 9)
+    rays = np.zeros((len(frm), 8), np.float32)
+    rays[:, :3], rays[:, 3], rays[:, 4:7] = frm, np.inf, d
+    got, ref = _run_closest(cuda, ds, rays), O.trace_closest(rays)
+    assert np.array_equal(got[:, :3], ref[:, :3])
+    assert np.isin(ref[:, 1], [3, 4, 5, 6]).sum() > 1000
+    s = np.zeros((len(frm), 8), np.float32)
+    s[:, :3], s[:, 3], s[:, 4:7] = frm, own.astype(np.uint32).view(np.float32), tgt
+    assert np.array_equal(_run_shadow(cuda, ds, s), O.trace_shadow(s))
+
+
+def test_instance_records_checked(cuda):
+    """A reference to a reference, a singular matrix and references with
+    the shadow-ray tree are refused."""
+    from yafray_b200 import abi
+    _, sc = _instance_scene(False)
+    sc.meshes.append(scenes.instance(3, np.eye(4)))
+    with pytest.raises(abi.YrError):
+        api.DeviceScene(sc)
+    _, sc = _instance_scene(False)
+    sc.meshes.append(scenes.instance(0, np.diag([1.0, 0.0, 1.0, 1.0])))
+    with pytest.raises(abi.YrError):
+        api.DeviceScene(sc)
+    _, sc = _instance_scene(False)
+    sc.render.flags = SHADOW_TREE
+    with pytest.raises(abi.YrError):
+        api.DeviceScene(sc)

@@ -98,10 +98,25 @@ def mesh_bound(mesh: scenes.Mesh) -> np.ndarray:
     return np.concatenate([lo, hi]).astype(np.float32)
 
 
+def object_bound(sc: scenes.Scene, i: int) -> np.ndarray:
+    """object3d_t::getBound of object i: the mesh bound, or for a reference
+    the placed box of its original's (yr_instance_bound)."""
+    m = sc.meshes[i]
+    if not m.is_instance:
+        return mesh_bound(m)
+    b = np.ascontiguousarray(mesh_bound(sc.meshes[m.instance_of]), np.float32)
+    mat = np.ascontiguousarray(m.matrix, np.float32).reshape(16)
+    out = np.zeros(6, np.float32)
+    fp = C.POINTER(C.c_float)
+    abi.check(abi.load().yr_instance_bound(b.ctypes.data_as(fp), mat.ctypes.data_as(fp), out.ctypes.data_as(fp)),
+              "yr_instance_bound")
+    return out
+
+
 def product_object_tree(sc: scenes.Scene) -> np.ndarray:
     """(n, 8) float32 records bmin[3], left(int bits), bmax[3], right(int bits)."""
     lib = abi.load()
-    b = np.ascontiguousarray(np.stack([mesh_bound(m) for m in sc.meshes]), np.float32)
+    b = np.ascontiguousarray(np.stack([object_bound(sc, i) for i in range(len(sc.meshes))]), np.float32)
     n = len(sc.meshes)
     out = (abi.YrObjectNode * (2 * n - 1))()
     nout = C.c_uint32()
@@ -122,9 +137,11 @@ class OracleScene:
         self.lib = oracle()
         self.h = self.lib.orc_load(self.path.encode())
         assert self.h, "oracle could not load the scene"
-        trees = trees if trees is not None else [product_tree(m) for m in sc.meshes]
+        trees = trees if trees is not None else [None if m.is_instance else product_tree(m) for m in sc.meshes]
         self._keep = []
         for i, (m, t) in enumerate(zip(sc.meshes, trees)):
+            if m.is_instance:  # shares its original's tree
+                continue
             nodes = np.ascontiguousarray(t["nodes"], np.uint32)
             prims = np.ascontiguousarray(t["prims"], np.uint32) if len(t["prims"]) else np.zeros(1, np.uint32)
             tb = np.ascontiguousarray(t["tb"], np.float32)
@@ -286,6 +303,23 @@ def harness_illum(sc: scenes.Scene, q: np.ndarray) -> np.ndarray:
             f.write(np.ascontiguousarray(q, ILLUM_REC).tobytes())
         run_harness("illum", sp, qp, op)
         return np.fromfile(op, ILLUM_OUT)
+
+
+def harness_instance_inverses(sc: scenes.Scene) -> dict:
+    """{object index: 4x4 M^-1} of every reference, as referenceObject_t
+    computes it."""
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "o.bin")
+        scenes.write_yrs(sc, sp)
+        run_harness("instmat", sp, op)
+        data = open(op, "rb").read()
+    n, = struct.unpack_from("<I", data, 0)
+    out, off = {}, 4
+    for _ in range(n):
+        i, = struct.unpack_from("<I", data, off)
+        out[i] = np.frombuffer(data, np.float32, 16, off + 4).reshape(4, 4).copy()
+        off += 68
+    return out
 
 
 def harness_camera(sc: scenes.Scene) -> np.ndarray:

@@ -110,7 +110,9 @@ class YrObjectDesc(C.Structure):
                 ("tris", C.POINTER(C.c_uint32)), ("ntris", C.c_uint32),
                 ("shader", C.c_uint32), ("cast_shadows", C.c_uint32),
                 ("tri_shaders", C.POINTER(C.c_uint32)), ("tree", C.POINTER(YrKdTree)),
-                ("smooth_angle", C.c_float), ("reserved", C.c_uint32)]
+                ("smooth_angle", C.c_float), ("reserved", C.c_uint32),
+                ("instance_matrix", C.POINTER(C.c_float)), ("instance_inverse", C.POINTER(C.c_float)),
+                ("instance_of", C.c_uint32), ("reserved2", C.c_uint32)]
 
 
 class YrSceneDesc(C.Structure):
@@ -174,6 +176,7 @@ SIGNATURES = {
                                      C.POINTER(YrKdTreeParams), C.c_int, C.POINTER(C.POINTER(YrKdTree))]),
     "yr_object_tree_build": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(YrObjectNode),
                                        C.POINTER(C.c_uint32)]),
+    "yr_instance_bound": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "yr_scene_create": (C.c_int, [C.POINTER(YrSceneDesc), C.c_int, C.POINTER(_P)]),
     "yr_scene_destroy": (C.c_int, [_P]),
     "yr_scene_info_get": (C.c_int, [_P, C.POINTER(YrSceneInfo)]),

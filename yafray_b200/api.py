@@ -29,6 +29,16 @@ class DeviceScene:
         self._keep = []
         objs = (abi.YrObjectDesc * len(sc.meshes))()
         for i, m in enumerate(sc.meshes):
+            if m.is_instance:
+                mat = np.ascontiguousarray(m.matrix, np.float32).reshape(16)
+                self._keep.append(mat)
+                objs[i].instance_matrix = mat.ctypes.data_as(C.POINTER(C.c_float))
+                if m.inverse is not None:
+                    inv = np.ascontiguousarray(m.inverse, np.float32).reshape(16)
+                    self._keep.append(inv)
+                    objs[i].instance_inverse = inv.ctypes.data_as(C.POINTER(C.c_float))
+                objs[i].instance_of = m.instance_of
+                continue
             v = np.ascontiguousarray(m.verts, np.float32)
             t = np.ascontiguousarray(m.tris, np.uint32)
             self._keep += [v, t]

@@ -415,20 +415,24 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
     const DevScene &D = scene->dev;
     const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
 #if YR_TRACE_GRID_PERSIST
-    const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q));
-    const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce));
+    const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false>));
+    const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce<false>));
 #else
     const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock), gb = gq;
 #endif
+    const bool inst = D.insts != nullptr;
+    auto k_prim = inst ? k_primary<true> : k_primary<false>;
+    auto k_shadow = inst ? k_trace_shadow_q<true> : k_trace_shadow_q<false>;
+    auto k_bounce = inst ? k_trace_bounce<true> : k_trace_bounce<false>;
     for (uint64_t b = 0; b < P.total; b += wcap) {
         W.base = (uint32_t)b;
         W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
         const int g = (int)((W.count + kBlock - 1) / kBlock);
         cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
-        k_primary<<<g, kBlock, 0, st>>>(D, R, W);
+        k_prim<<<g, kBlock, 0, st>>>(D, R, W);
         k_adj_shade_camera<<<g, kBlock, 0, st>>>(D, R, W, A);
         cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
-        k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
+        k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
         k_adj_gather_camera<<<g, kBlock, smem, st>>>(R, W, A);
         if (P.npath > 0) {
             const size_t nc = (size_t)W.count * P.npath * P.depth;
@@ -436,11 +440,11 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
             const int gp = (int)(((size_t)W.count * P.npath + kBlock - 1) / kBlock);
             for (int j = 0; j < R.path_depth; j++) {
                 cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
-                k_trace_bounce<<<gb, kBlock, 0, st>>>(D, W);
+                k_bounce<<<gb, kBlock, 0, st>>>(D, W);
                 cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
                 k_adj_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j, A);
                 cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
-                k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
+                k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias);
                 k_adj_gather_path<<<gp, kBlock, smem, st>>>(R, W, j, R.background, A);
                 std::swap(W.bq, W.bq2);
                 k_swap_queues<<<1, 1, 0, st>>>(W);

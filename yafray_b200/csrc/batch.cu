@@ -47,7 +47,7 @@ struct BatchArgs {
     unsigned long long *rays; // primary, shadow, bounce
 };
 
-template <int STACK>
+template <int STACK, bool INST>
 __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
     __shared__ DevScene S;
     __shared__ DevRender R;
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
         __syncthreads();
         const uint32_t count = W.count;
         for (uint32_t i = tid; i < count; i += nthr) {
-            st_primary(S, R, W, i, stk, nodes, tests);
+            st_primary<INST>(S, R, W, i, stk, nodes, tests);
             n_prim++;
         }
         __syncthreads();
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
         {
             const uint32_t n = cnt[0];
             for (uint32_t q = tid; q < n; q += nthr) {
-                st_trace_shadow(S, W, q, R.self_bias, stk, nodes, tests);
+                st_trace_shadow<INST>(S, W, q, R.self_bias, stk, nodes, tests);
                 n_sh++;
             }
         }
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
             for (int j = 0; j < R.path_depth; j++) {
                 const uint32_t nb = cnt[1];
                 for (uint32_t q = tid; q < nb; q += nthr) {
-                    st_trace_bounce(S, W, q, stk, nodes, tests);
+                    st_trace_bounce<INST>(S, W, q, stk, nodes, tests);
                     n_b++;
                 }
                 __syncthreads();
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
                 {
                     const uint32_t n = cnt[0];
                     for (uint32_t q = tid; q < n; q += nthr) {
-                        st_trace_shadow(S, W, q, R.self_bias, stk, nodes, tests);
+                        st_trace_shadow<INST>(S, W, q, R.self_bias, stk, nodes, tests);
                         n_sh++;
                     }
                 }
@@ -151,10 +151,16 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
 
 using BatchKernel = void (*)(BatchArgs);
 static const int kStackOptions[3] = {32, 48, kKdStackCap};
-static BatchKernel batch_kernel(int stack) {
-    if (stack == 32) return k_batch<32>;
-    if (stack == 48) return k_batch<48>;
-    return k_batch<kKdStackCap>;
+// inst: some scene of the batch has references (instanced objects)
+static BatchKernel batch_kernel(int stack, bool inst) {
+    if (inst) {
+        if (stack == 32) return k_batch<32, true>;
+        if (stack == 48) return k_batch<48, true>;
+        return k_batch<kKdStackCap, true>;
+    }
+    if (stack == 32) return k_batch<32, false>;
+    if (stack == 48) return k_batch<48, false>;
+    return k_batch<kKdStackCap, false>;
 }
 
 struct BatchConfig {
@@ -387,7 +393,9 @@ static yr_status launch_tiles(BatchCtx &C, const BatchConfig &cfg, const std::ve
     const size_t cta = (wave_bytes(C.pmax, qmax) + 255) / 256 * 256;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, C.device);
-    BatchKernel kern = batch_kernel(cfg.stack);
+    bool inst = false;
+    for (const yr_scene *sc : C.scenes) inst = inst || sc->dev.insts != nullptr;
+    BatchKernel kern = batch_kernel(cfg.stack, inst);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.block, 0) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     const int grid = std::max(1, std::min<int>(sms * per_sm, (int)items.size()));

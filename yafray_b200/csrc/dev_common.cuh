@@ -92,7 +92,36 @@ struct DevObject {
     uint32_t ntris;
     uint32_t flags;     // bit0: casts shadows, bit1: smoothed (corner normals in DevScene::tri_nrm)
     float ob[6];        // object bound (meshObject_t::getBound), the object tree's leaf box
+    int inst;           // instance record (DevScene::insts) or -1; the tree
+                        // and triangle fields above are then the original's
+    int pad[3];
 };
+
+// referenceObject_t's matrices: rows 0-2 of M and of its inverse, and the
+// row-normalised rotation part of M
+struct DevInst {
+    float m[12];
+    float back[12];
+    float rot[9];
+    float pad[3];
+};
+
+// matrix4x4_t * point3d_t as the shipped build groups it:
+// (m0*x + m1*y) + (m2*z + m3) per row
+__host__ __device__ __forceinline__ V3 xf_point(const float *m, const V3 &p) {
+    return v3((m[0] * p.x + m[1] * p.y) + (m[2] * p.z + m[3]), (m[4] * p.x + m[5] * p.y) + (m[6] * p.z + m[7]),
+              (m[8] * p.x + m[9] * p.y) + (m[10] * p.z + m[11]));
+}
+// matrix4x4_t * vector3d_t (no translation), sums left to right
+__host__ __device__ __forceinline__ V3 xf_vec(const float *m, const V3 &v) {
+    return v3((m[0] * v.x + m[1] * v.y) + m[2] * v.z, (m[4] * v.x + m[5] * v.y) + m[6] * v.z,
+              (m[8] * v.x + m[9] * v.y) + m[10] * v.z);
+}
+// a 3x3 row-major rotation times a vector
+__host__ __device__ __forceinline__ V3 rot_vec(const float *r, const V3 &v) {
+    return v3((r[0] * v.x + r[1] * v.y) + r[2] * v.z, (r[3] * v.x + r[4] * v.y) + r[5] * v.z,
+              (r[6] * v.x + r[7] * v.y) + r[8] * v.z);
+}
 
 
 struct DevScene {
@@ -100,6 +129,7 @@ struct DevScene {
     const uint2 *nodes;
     const uint32_t *prims;
     const DevObject *objects;
+    const DevInst *insts;       // instance matrices (referenceObject_t)
     const float *tri_nrm;       // corner normals, 9 per triangle, of smoothed objects
     // object tree (geomeTree_t): per interior node 4 x float4 = left box
     // (min xyz, max xyz), right box, then the children's codes (>= 0:

@@ -270,6 +270,7 @@ namespace yr {
 // --------------------------------------------------------------- shading
 struct Surf {
     V3 P, N, Ng, NU, NV;
+    V3 orco;  // the texture's "orco" point: P, or M^-1 P on a reference
     int object;
     int shader;
     float Z;
@@ -306,8 +307,14 @@ __device__ __forceinline__ V3 reflect(const V3 &n, const V3 &v) {
 // interpolation as r = 1/denum, fb = alpha r, fc = beta r,
 // fa = 1 - (alpha + beta) r, and the sum as na fa + (nb fb + nc fc).
 __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender &R, int object, uint32_t tri,
-                                             float Z, const V3 &from, const V3 &ray) {
+                                             float Z, const V3 &from_w, const V3 &ray_w) {
     Surf s;
+    // a reference's hit is formed in its original's space (the ray taken
+    // there by M's inverse) and brought back below (reference.cc:100-112)
+    const int inst = S.objects[object].inst;
+    const DevInst *I = inst >= 0 ? S.insts + inst : nullptr;
+    const V3 from = I ? xf_point(I->back, from_w) : from_w;
+    const V3 ray = I ? xf_vec(I->back, ray_w) : ray_w;
     s.P = from + Z * ray;
     const float4 p = __ldg(S.tris + 3 * (size_t)tri), q = __ldg(S.tris + 3 * (size_t)tri + 1),
                  r = __ldg(S.tris + 3 * (size_t)tri + 2);
@@ -336,6 +343,15 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
         s.N = normalize(nn);
     }
     create_cs(s.N, s.NU, s.NV);
+    s.orco = s.P;
+    if (I) {  // N, Ng, NU, NV by MRot; P by M; orco = M^-1 P (toObjectOrco)
+        s.N = rot_vec(I->rot, s.N);
+        s.Ng = rot_vec(I->rot, s.Ng);
+        s.P = xf_point(I->m, s.P);
+        s.NU = rot_vec(I->rot, s.NU);
+        s.NV = rot_vec(I->rot, s.NV);
+        s.orco = xf_point(I->back, s.P);
+    }
     s.object = object;
     s.shader = (int)__ldg(R.tri_shader + tri);
     s.Z = Z;
@@ -346,8 +362,8 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
 // (texture.cc:122-320): the texco source (hit point, or the shading
 // normal), then per axis size*(source[proj] + ofs), or size*ofs when the
 // axis is switched off.
-__device__ __forceinline__ V3 tex_point(const DevShader &sh, const V3 &P, const V3 &N) {
-    const V3 &src = sh.texco == YR_TEXCO_NORMAL ? N : P;
+__device__ __forceinline__ V3 tex_point(const DevShader &sh, const Surf &sp) {
+    const V3 &src = sh.texco == YR_TEXCO_NORMAL ? sp.N : (sh.texco == YR_TEXCO_ORCO ? sp.orco : sp.P);
     float t[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -372,12 +388,11 @@ struct TexDeriv {
 // a*w + (1-w)*b and returns a for w > 1.  `td` (optional) receives what
 // the adjoint needs.
 // `shp` points at the shader record in device memory.
-__device__ __forceinline__ C3 modulated_color(const DevShader *shp, const V3 &P, const V3 &N,
-                                              TexDeriv *td = nullptr) {
+__device__ __forceinline__ C3 modulated_color(const DevShader *shp, const Surf &sp, TexDeriv *td = nullptr) {
     const DevShader &sh = *shp;
     const C3 C = sh.color;
     if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f)) return C;
-    const TexEval te = texture_eval(shp, tex_point(sh, P, N));
+    const TexEval te = texture_eval(shp, tex_point(sh, sp));
     if (td) {
         td->tex = te.col;
         td->dint = te.dint;

@@ -565,13 +565,32 @@ struct SceneHit {
     uint32_t tests;
 };
 
+// object3d_t::shoot with shadow = true: the any-hit walk of the object's
+// tree; a reference (referenceObject_t::shoot, reference.cc:95-114) walks its
+// original's tree with origin and direction taken into the original's space
+// by M's inverse (not renormalised, so the distances stay the world's)
+template <bool INST>
+__device__ __forceinline__ bool shoot_any(const DevScene &S, const DevObject &obj, const V3 &from, const RayR &ray,
+                                          float dist, float &Z, KdResult &r, const KdStack &stk) {
+    if (!INST) return kd_trace<true>(S, obj, from, ray, dist, Z, r, stk);
+    V3 f = from;
+    RayR rr = ray;
+    if (obj.inst >= 0) {
+        const DevInst &I = S.insts[obj.inst];
+        f = xf_point(I.back, from);
+        rr = make_rayr(xf_vec(I.back, ray.d));
+    }
+    return kd_trace<true>(S, obj, f, rr, dist, Z, r, stk);
+}
+
 // Closest hit over all objects.  `f` is the already offset origin.
 //   pass_limit = true : scene_t::raytrace (scene.cc:210-233) - each object
 //                       is shot with the current closest distance
 //   pass_limit = false: scene_t::firstHit (scene.cc:688-707)
 //   shadow_only: skip objects that do not cast shadows (firstHit's shadow arg)
-__device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V3 &dir, bool pass_limit,
-                                         bool shadow_only, const KdStack &stk) {
+template <bool INST>
+__device__ inline SceneHit scene_closest_t(const DevScene &S, const V3 &f, const V3 &dir, bool pass_limit,
+                                           bool shadow_only, const KdStack &stk) {
     const RayR ray = make_rayr(dir);
     const ObjRay oray = make_objray(f, ray, S.coord_max, S.exact_order != 0);
     SceneHit best;
@@ -591,7 +610,19 @@ __device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V
             const float dis = pass_limit ? limit : inf;
             float Z = dis;
             KdResult r{kNone, 0, 0};
-            const bool h = kd_trace<false>(S, obj, f, ray, dis, Z, r, stk);
+            bool h;
+            if (!INST) {
+                h = kd_trace<false>(S, obj, f, ray, dis, Z, r, stk);
+            } else {
+                V3 fo = f;
+                RayR ro = ray;
+                if (obj.inst >= 0) {  // referenceObject_t::shoot: the ray in the original's space
+                    const DevInst &I = S.insts[obj.inst];
+                    fo = xf_point(I.back, f);
+                    ro = make_rayr(xf_vec(I.back, dir));
+                }
+                h = kd_trace<false>(S, obj, fo, ro, dis, Z, r, stk);
+            }
             best.nodes += r.nodes;
             best.tests += r.tests;
             if (h && Z > 0.f) {
@@ -609,8 +640,15 @@ __device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V
     return best;
 }
 
+__device__ inline SceneHit scene_closest(const DevScene &S, const V3 &f, const V3 &dir, bool pass_limit,
+                                         bool shadow_only, const KdStack &stk) {
+    if (S.insts) return scene_closest_t<true>(S, f, dir, pass_limit, shadow_only, stk);
+    return scene_closest_t<false>(S, f, dir, pass_limit, shadow_only, stk);
+}
+
 // scene_t::isShadowed (scene.cc:107-185).  p: shading point, own: its
 // object, ray: unit direction, dist: |l - p| (or infinity).
+template <bool INST>
 __device__ inline bool scene_occluded_ref(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
                                           float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     const V3 self = p + dir * self_bias;
@@ -625,7 +663,7 @@ __device__ inline bool scene_occluded_ref(const DevScene &S, const V3 &p, int ow
         if (obj.flags & 1u) {
             float Z = dist;
             KdResult r{kNone, 0, 0};
-            const bool h = kd_trace<true>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
+            const bool h = shoot_any<INST>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
 #ifdef YR_COUNT_OBJ
             tests += 1;  // objects shot
             if (h) {
@@ -655,6 +693,7 @@ __device__ inline bool scene_occluded_ref(const DevScene &S, const V3 &p, int ow
 // few more); (b) is the same kd walk; (a) is checked exactly for an
 // object with a hit before it counts.  The answer is therefore the
 // reference's, whatever the order in which objects are reached.
+template <bool INST>
 __device__ inline bool scene_occluded_bvh(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
                                           float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     const V3 self = p + dir * self_bias;
@@ -668,7 +707,7 @@ __device__ inline bool scene_occluded_bvh(const DevScene &S, const V3 &p, int ow
         const DevObject &obj = S.objects[o];
         float Z = dist;
         KdResult r{kNone, 0, 0};
-        const bool h = kd_trace<true>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
+        const bool h = shoot_any<INST>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
 #ifdef YR_COUNT_OBJ
         tests += 1;  // objects shot
 #else
@@ -695,14 +734,23 @@ __device__ inline bool scene_occluded_bvh(const DevScene &S, const V3 &p, int ow
 // isShadowed through the shadow-ray tree, through the object tree in the
 // reference's order when the scene asks for exact order, else through the
 // shadow casters' BVH (yr_render_params.flags)
-__device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
-                                      float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+template <bool INST>
+__device__ inline bool scene_occluded_t(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
+                                        float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     if (S.use_sh_tree) {
         if (S.sh_nnodes == 0) return false;  // nothing casts shadows
         return scene_occluded_merged(S, p, own, dir, dist, self_bias, stk, nodes, tests);
     }
-    if (S.exact_order) return scene_occluded_ref(S, p, own, dir, dist, self_bias, stk, nodes, tests);
-    return scene_occluded_bvh(S, p, own, dir, dist, self_bias, stk, nodes, tests);
+    if (S.exact_order) return scene_occluded_ref<INST>(S, p, own, dir, dist, self_bias, stk, nodes, tests);
+    return scene_occluded_bvh<INST>(S, p, own, dir, dist, self_bias, stk, nodes, tests);
+}
+
+// the same, choosing the loops with or without references at run time
+// (kernels on the render path are instantiated for each instead)
+__device__ inline bool scene_occluded(const DevScene &S, const V3 &p, int own, const V3 &dir, float dist,
+                                      float self_bias, const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+    if (S.insts) return scene_occluded_t<true>(S, p, own, dir, dist, self_bias, stk, nodes, tests);
+    return scene_occluded_t<false>(S, p, own, dir, dist, self_bias, stk, nodes, tests);
 }
 
 }  // namespace yr

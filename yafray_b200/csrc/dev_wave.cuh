@@ -147,6 +147,9 @@ __device__ __forceinline__ void emit_shadow(const Wave &W, bool pred, const V3 &
 // Stage bodies.  Each wavefront kernel runs one stage over the whole wave;
 // the batched persistent kernel runs the same stages over one tile inside
 // a block.  Stages marked "whole warp" must be called by all 32 lanes.
+// INST: the scene has references (instanced objects); the traversal loops
+// that transform rays are compiled only into those instantiations.
+template <bool INST>
 __device__ __forceinline__ void st_primary(const DevScene &S, const DevRender &R, const Wave &W, uint32_t i,
                                            const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     {
@@ -157,7 +160,7 @@ __device__ __forceinline__ void st_primary(const DevScene &S, const DevRender &R
         sample_pos(R, pixel, s, fx, fy);
         const V3 ray = camera_ray(R.cam, (float)x + fx, (float)y + fy);
         const V3 f = R.cam.pos + ray * kMinRayDist;  // scene.cc:211
-        const SceneHit h = scene_closest(S, f, ray, true, false, stk);
+        const SceneHit h = scene_closest_t<INST>(S, f, ray, true, false, stk);
         W.hit0[i] = make_float4(h.t, __int_as_float(h.object), __uint_as_float(h.tri), 0.f);
         nodes += h.nodes;
         tests += h.tests;
@@ -165,13 +168,14 @@ __device__ __forceinline__ void st_primary(const DevScene &S, const DevRender &R
 }
 
 #ifdef YR_WAVE_KERNELS
+template <bool INST>
 static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_primary(DevScene S, DevRender R, Wave W) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
     const KdStack stk{stk_nt, stk_split, kKdStackCap};
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t nodes = 0, tests = 0;
-    if (i < W.count) st_primary(S, R, W, i, stk, nodes, tests);
+    if (i < W.count) st_primary<INST>(S, R, W, i, stk, nodes, tests);
     count_work(W, YR_K_PRIMARY, i < W.count ? 1u : 0u, nodes, tests);
 }
 #endif
@@ -192,7 +196,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
     C3 lkc = c3(0.f, 0.f, 0.f);
     if (active) {
         sh = R.shaders[sp.shader];
-        lkc = modulated_color(R.shaders + sp.shader, sp.P, sp.N, ADJ ? td_out : nullptr);
+        lkc = modulated_color(R.shaders + sp.shader, sp, ADJ ? td_out : nullptr);
         if (ADJ) *lkc_out = lkc;
     }
     V3 N = sp.N;
@@ -436,7 +440,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
     bool paths = false;
     if (active) {
         const DevShader sh = R.shaders[sp.shader];
-        const C3 dif = modulated_color(R.shaders + sp.shader, sp.P, sp.N);
+        const C3 dif = modulated_color(R.shaders + sp.shader, sp);
         paths = !(energy(dif) < 0.05f);
         const DevLight PL = R.lights[R.path_light];
         W.diff0[i] = make_float4(dif.r, dif.g, dif.b, paths ? PL.power : 0.f);
@@ -471,15 +475,17 @@ static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_shade_camera(D
 }
 #endif
 
+template <bool INST>
 __device__ __forceinline__ void st_trace_shadow(const DevScene &S, const Wave &W, uint32_t q, float self_bias,
                                                 const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     const float4 a = W.shq0[q], b = W.shq1[q];
-    const bool occ = scene_occluded(S, v3(a.x, a.y, a.z), __float_as_int(a.w), v3(b.x, b.y, b.z), b.w, self_bias,
+    const bool occ = scene_occluded_t<INST>(S, v3(a.x, a.y, a.z), __float_as_int(a.w), v3(b.x, b.y, b.z), b.w, self_bias,
                                     stk, nodes, tests);
     W.slot_f[W.shq_slot[q]] = occ ? kSlotShadowed : kSlotLit;
 }
 
 #ifdef YR_WAVE_KERNELS
+template <bool INST>
 static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q(DevScene S, Wave W, float self_bias) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
@@ -496,13 +502,13 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q
         if (base >= n) break;
         const uint32_t q = base + (threadIdx.x & 31u);
         if (q < n) {
-            st_trace_shadow(S, W, q, self_bias, stk, nodes, tests);
+            st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests);
             rays++;
         }
     }
 #else
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        st_trace_shadow(S, W, q, self_bias, stk, nodes, tests);
+        st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests);
         rays++;
     }
 #endif
@@ -530,19 +536,21 @@ static __global__ void __launch_bounds__(kBlock) k_gather_camera(DevRender R, Wa
 }
 #endif
 
+template <bool INST>
 __device__ __forceinline__ void st_trace_bounce(const DevScene &S, const Wave &W, uint32_t q, const KdStack &stk,
                                                 uint32_t &nodes, uint32_t &tests) {
     const uint32_t p = W.bq[q];
     const float4 wh = W.p_where[p], rr = W.p_ray[p];
     const V3 ray = v3(rr.x, rr.y, rr.z);
     const V3 f = v3(wh.x, wh.y, wh.z) + ray * kMinRayDist;  // scene.cc:693
-    const SceneHit h = scene_closest(S, f, ray, false, true, stk);
+    const SceneHit h = scene_closest_t<INST>(S, f, ray, false, true, stk);
     W.p_hit[p] = make_float4(h.t, __int_as_float(h.object), __uint_as_float(h.tri), 0.f);
     nodes += h.nodes;
     tests += h.tests;
 }
 
 #ifdef YR_WAVE_KERNELS
+template <bool INST>
 static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_bounce(DevScene S, Wave W) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
@@ -557,13 +565,13 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_bounce(D
         if (base >= n) break;
         const uint32_t q = base + (threadIdx.x & 31u);
         if (q < n) {
-            st_trace_bounce(S, W, q, stk, nodes, tests);
+            st_trace_bounce<INST>(S, W, q, stk, nodes, tests);
             rays++;
         }
     }
 #else
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        st_trace_bounce(S, W, q, stk, nodes, tests);
+        st_trace_bounce<INST>(S, W, q, stk, nodes, tests);
         rays++;
     }
 #endif
@@ -615,7 +623,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
         shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux);
     }
     if (active) {
-        if (!ADJ) dif = modulated_color(R.shaders + sp.shader, sp.P, sp.N);
+        if (!ADJ) dif = modulated_color(R.shaders + sp.shader, sp);
         const float4 col = W.p_col[p];
         const C3 nc = c3(col.x, col.y, col.z) * dif;
         W.p_next[p] = make_float4(nc.r, nc.g, nc.b, 0.f);

@@ -994,3 +994,93 @@ void smooth_normals(const float *verts, const uint32_t *tris, uint32_t nverts, u
 }
 
 }  // namespace yr
+
+// ------------------------------------------------------------ instances
+namespace yr {
+
+bool instance_xf(const float *M16, InstanceXf &out) {
+    // matrix4x4_t::inverse: Gauss-Jordan with partial pivoting on the
+    // largest |m[k][i]|, rows divided by the pivot, then reduced
+    float m[4][4], id[4][4];
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            m[i][j] = M16[4 * i + j];
+            id[i][j] = i == j ? 1.0f : 0.0f;
+        }
+    for (int i = 0; i < 4; i++) {
+        float mx = 0;
+        int ci = 0;
+        for (int k = i; k < 4; k++)
+            if (std::fabs(m[k][i]) > mx) {
+                mx = std::fabs(m[k][i]);
+                ci = k;
+            }
+        if (mx == 0) return false;
+        for (int j = 0; j < 4; j++) {
+            std::swap(m[i][j], m[ci][j]);
+            std::swap(id[i][j], id[ci][j]);
+        }
+        float f = m[i][i];
+        for (int j = 0; j < 4; j++) m[i][j] /= f;
+        for (int j = 0; j < 4; j++) id[i][j] /= f;
+        for (int k = 0; k < 4; k++) {
+            if (k == i) continue;
+            f = m[k][i];
+            for (int j = 0; j < 4; j++) m[k][j] -= m[i][j] * f;
+            for (int j = 0; j < 4; j++) id[k][j] -= id[i][j] * f;
+        }
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 4; j++) {
+            out.m[4 * i + j] = M16[4 * i + j];
+            out.back[4 * i + j] = id[i][j];
+        }
+    // MRot: each row of M's 3x3 part normalised (vector3d_t::normalize)
+    for (int i = 0; i < 3; i++) {
+        const float x = M16[4 * i], y = M16[4 * i + 1], z = M16[4 * i + 2];
+        float l = x * x + y * y + z * z;
+        float k = 1.f;
+        if (l != 0.f) k = (float)(1.0 / std::sqrt((double)l));
+        out.rot[3 * i] = l != 0.f ? x * k : x;
+        out.rot[3 * i + 1] = l != 0.f ? y * k : y;
+        out.rot[3 * i + 2] = l != 0.f ? z * k : z;
+    }
+    return true;
+}
+
+Box instance_bound(const Box &b, const float *M) {
+    // the eight corners: x and y take a or g (the shipped build folds
+    // a + (g - a) to g), z takes a.z or a.z + (g.z - a.z); each placed by
+    // M with its sums grouped (m0*x + m1*y) + (m2*z + m3)
+    const float toz = b.g[2] - b.a[2];
+    const float zs[2] = {b.a[2], b.a[2] + toz};
+    Box o;
+    bool first = true;
+    for (int iz = 0; iz < 2; iz++)
+        for (int iy = 0; iy < 2; iy++)
+            for (int ix = 0; ix < 2; ix++) {
+                const float x = ix ? b.g[0] : b.a[0], y = iy ? b.g[1] : b.a[1], z = zs[iz];
+                float p[3];
+                for (int r = 0; r < 3; r++)
+                    p[r] = (M[4 * r] * x + M[4 * r + 1] * y) + (M[4 * r + 2] * z + M[4 * r + 3]);
+                for (int r = 0; r < 3; r++) {
+                    if (first || p[r] < o.a[r]) o.a[r] = p[r];
+                    if (first || p[r] > o.g[r]) o.g[r] = p[r];
+                }
+                first = false;
+            }
+    return o;
+}
+
+}  // namespace yr
+
+YR_API yr_status yr_instance_bound(const float *bound, const float *matrix, float *out) {
+    if (!bound || !matrix || !out) return YR_ERR_INVALID_ARG;
+    yr::Box b;
+    std::memcpy(b.a, bound, 12);
+    std::memcpy(b.g, bound + 3, 12);
+    const yr::Box o = yr::instance_bound(b, matrix);
+    std::memcpy(out, o.a, 12);
+    std::memcpy(out + 3, o.g, 12);
+    return YR_OK;
+}

@@ -46,6 +46,20 @@ yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris
 // vertices grown by BOX_MIN.
 Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris);
 
+// referenceObject_t's matrices (reference.cc:9-46): the first three rows of
+// M and of its inverse (matrix4x4_t::inverse, matrix4.cc:68-117), and M's
+// rows normalised (the rotation used for normals).  Returns false when M
+// is singular (the reference stops there).
+struct InstanceXf {
+    float m[12];
+    float back[12];
+    float rot[9];
+};
+bool instance_xf(const float *M16, InstanceXf &out);
+// referenceObject_t::getBound (reference.cc:135-165) in the shipped build's
+// evaluation
+Box instance_bound(const Box &b, const float *M16);
+
 // meshObject_t::autoSmooth (mesh.cc:201-279) as the shipped build
 // evaluates it: the shading normal of every triangle corner (9 floats per
 // triangle: a, b, c) for a smoothing angle >= 1 degree.

@@ -60,23 +60,29 @@ static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W,
         cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
     } else {
 #if YR_TRACE_GRID_PERSIST
-        const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q));
-        const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce));
+        const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false>));
+        const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce<false>));
 #else
         const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock), gb = gq;
 #endif
         const DevScene &D = scene->dev;
         const uint32_t npath = P.npath;
+        // the traversal kernels with the reference-transforming loops only
+        // for scenes that have references
+        const bool inst = D.insts != nullptr;
+        auto k_prim = inst ? k_primary<true> : k_primary<false>;
+        auto k_shadow = inst ? k_trace_shadow_q<true> : k_trace_shadow_q<false>;
+        auto k_bounce = inst ? k_trace_bounce<true> : k_trace_bounce<false>;
         for (uint64_t b = 0; b < P.total; b += wcap) {
             W.base = (uint32_t)b;
             W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
             const int g = (int)((W.count + kBlock - 1) / kBlock);
             cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
-            timed(YR_K_PRIMARY, [&] { k_primary<<<g, kBlock, 0, st>>>(D, R, W); });
+            timed(YR_K_PRIMARY, [&] { k_prim<<<g, kBlock, 0, st>>>(D, R, W); });
             timed(YR_K_SHADE_CAMERA, [&] { k_shade_camera<<<g, kBlock, 0, st>>>(D, R, W); });
             timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
             cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
-            timed(YR_K_SHADOW, [&] { k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+            timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
             timed(YR_K_GATHER, [&] { k_gather_camera<<<g, kBlock, 0, st>>>(R, W); });
             if (npath > 0) {
                 const size_t nc = (size_t)W.count * npath * P.depth;
@@ -87,12 +93,12 @@ static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W,
                 for (int j = 0; j < R.path_depth; j++) {
                     timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 1); });
                     cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
-                    timed(YR_K_BOUNCE, [&] { k_trace_bounce<<<gb, kBlock, 0, st>>>(D, W); });
+                    timed(YR_K_BOUNCE, [&] { k_bounce<<<gb, kBlock, 0, st>>>(D, W); });
                     cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
                     timed(YR_K_SHADE_PATH, [&] { k_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j); });
                     timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
                     cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
-                    timed(YR_K_SHADOW, [&] { k_trace_shadow_q<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+                    timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
                     timed(YR_K_GATHER, [&] { k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background); });
                     std::swap(W.bq, W.bq2);
                     timed(YR_K_OTHER, [&] { k_swap_queues<<<1, 1, 0, st>>>(W); });

@@ -378,13 +378,23 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     std::vector<DevObject> objects;
     std::vector<Box> obounds;
     size_t total_tris = 0;
-    for (uint32_t o = 0; o < desc->nobjects; o++) total_tris += desc->objects[o].ntris;
+    std::vector<DevInst> insts;
+    auto is_inst = [&](uint32_t o) { return desc->objects[o].instance_matrix != nullptr; };
+    for (uint32_t o = 0; o < desc->nobjects; o++)
+        if (!is_inst(o)) total_tris += desc->objects[o].ntris;
     if (total_tris == 0) return fail(YR_ERR_EMPTY_SCENE);
     if (total_tris >= (1u << 30)) return fail(YR_ERR_TOO_LARGE);
     tris.reserve(3 * total_tris);
     tri_shader.reserve(total_tris);
     for (uint32_t o = 0; o < desc->nobjects; o++) {
         const yr_object_desc &od = desc->objects[o];
+        if (is_inst(o)) {  // a reference to a mesh (not to another reference)
+            if (od.instance_of >= desc->nobjects || is_inst(od.instance_of)) return fail(YR_ERR_INVALID_ARG);
+            for (int k = 0; k < 16; k++)
+                if (!std::isfinite(od.instance_matrix[k])) return fail(YR_ERR_INVALID_ARG);
+            if (desc->render.flags & YR_RENDER_SHADOW_TREE) return fail(YR_ERR_UNSUPPORTED);
+            continue;
+        }
         if (od.ntris == 0 || !od.verts || !od.tris) return fail(YR_ERR_EMPTY_SCENE);
         if (od.shader != YR_PER_TRIANGLE && od.shader >= desc->nshaders) return fail(YR_ERR_INVALID_ARG);
         if (od.shader == YR_PER_TRIANGLE && !od.tri_shaders) return fail(YR_ERR_INVALID_ARG);
@@ -399,6 +409,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
             for (;;) {
                 const uint32_t o = next.fetch_add(1);
                 if (o >= desc->nobjects) return;
+                if (is_inst(o)) continue;  // shares its original's tree
                 const yr_object_desc &od = desc->objects[o];
                 KdTree &tree = trees[o];
                 try {
@@ -425,6 +436,11 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     }
     for (uint32_t o = 0; o < desc->nobjects; o++) {
         const yr_object_desc &od = desc->objects[o];
+        if (is_inst(o)) {  // filled in below, once every mesh is placed
+            objects.push_back(DevObject{});
+            obounds.push_back(Box{});
+            continue;
+        }
         if (tree_st[o] != YR_OK) return fail(tree_st[o]);
         KdTree tree = std::move(trees[o]);
         if (tree.max_depth > s->max_tree_depth) s->max_tree_depth = tree.max_depth;
@@ -491,8 +507,33 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         const Box obb = mesh_bound(od.verts, od.tris, od.ntris);
         std::memcpy(dob.ob, obb.a, 12);
         std::memcpy(dob.ob + 3, obb.g, 12);
+        dob.inst = -1;
         objects.push_back(dob);
         obounds.push_back(obb);
+    }
+    // references (referenceObject_t): the original's tree, triangles,
+    // shading flags and shadow flag (reference.cc:38-44), its own matrices
+    // and the placed box of the original's bound
+    for (uint32_t o = 0; o < desc->nobjects; o++) {
+        if (!is_inst(o)) continue;
+        const yr_object_desc &od = desc->objects[o];
+        InstanceXf xf;
+        if (!instance_xf(od.instance_matrix, xf)) return fail(YR_ERR_INVALID_ARG);  // singular matrix
+        if (od.instance_inverse)  // the caller's M^-1 (e.g. referenceObject_t::back)
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 4; j++) xf.back[4 * i + j] = od.instance_inverse[4 * i + j];
+        DevInst di{};
+        std::memcpy(di.m, xf.m, sizeof(xf.m));
+        std::memcpy(di.back, xf.back, sizeof(xf.back));
+        std::memcpy(di.rot, xf.rot, sizeof(xf.rot));
+        DevObject dob = objects[od.instance_of];
+        const Box ob = instance_bound(obounds[od.instance_of], od.instance_matrix);
+        std::memcpy(dob.ob, ob.a, 12);
+        std::memcpy(dob.ob + 3, ob.g, 12);
+        dob.inst = (int)insts.size();
+        insts.push_back(di);
+        objects[o] = dob;
+        obounds[o] = ob;
     }
     // shadow-ray tree over the triangles of every shadow-casting object
     std::vector<uint2> sh_nodes;
@@ -502,6 +543,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         std::vector<float> mv;
         std::vector<uint32_t> mt, remap;
         for (uint32_t o = 0; o < desc->nobjects; o++) {
+            if (is_inst(o)) continue;  // (no shadow-ray tree with references)
             const yr_object_desc &od = desc->objects[o];
             for (uint32_t t = 0; t < od.ntris; t++) tri_obj[objects[o].tri_base + t] = o;
             if (!od.cast_shadows) continue;
@@ -631,6 +673,9 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     const float *d_tri_nrm = nullptr;
     if ((st = dev_upload(s, tri_nrm.data(), tri_nrm.size(), (float **)&d_tri_nrm)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
+    const DevInst *d_insts = nullptr;
+    if (!insts.empty() && (st = dev_upload(s, insts.data(), insts.size(), (DevInst **)&d_insts)) != YR_OK)
+        return fail(st);
     if ((st = dev_upload(s, onodes.data(), onodes.size(), (float4 **)&d_onodes)) != YR_OK) return fail(st);
     const float4 *d_sonodes = nullptr;
     if ((st = dev_upload(s, sonodes.data(), sonodes.size(), (float4 **)&d_sonodes)) != YR_OK) return fail(st);
@@ -649,6 +694,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.nodes = d_nodes;
     D.prims = d_prims;
     D.objects = d_objects;
+    D.insts = d_insts;
     D.tri_nrm = d_tri_nrm;
     D.onodes = d_onodes;
     D.oroot = oroot;

@@ -99,6 +99,36 @@ class Mesh:
     tri_shaders: Optional[np.ndarray] = None
     cast_shadows: bool = True
     smooth_angle: float = 0.0   # meshObject_t::autoSmooth angle (degrees); < 1 = flat
+    instance_of: int = -1       # >= 0: a referenceObject_t of that mesh, placed by `matrix`
+    matrix: Optional[np.ndarray] = None   # 4x4 row-major (instances only)
+    inverse: Optional[np.ndarray] = None  # optional M^-1 (else computed by the library)
+
+    @property
+    def is_instance(self) -> bool:
+        return self.instance_of >= 0
+
+
+def instance(original: int, matrix, inverse=None) -> "Mesh":
+    """A reference to mesh `original` placed by the 4x4 row-major `matrix`
+    (the loader's object with an "original" attribute, render.cc:650-680);
+    `inverse`: optional M^-1 as the caller computed it."""
+    m = np.ascontiguousarray(np.asarray(matrix, np.float32).reshape(4, 4))
+    inv = None if inverse is None else np.ascontiguousarray(np.asarray(inverse, np.float32).reshape(4, 4))
+    return Mesh(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32), 0, instance_of=int(original), matrix=m,
+                inverse=inv)
+
+
+def transform(translate=(0.0, 0.0, 0.0), rotate_deg=(0.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0)) -> np.ndarray:
+    """A 4x4 row-major matrix: scale, then rotations about x, y and z, then
+    the translation."""
+    s = np.diag([*scale, 1.0])
+    rx, ry, rz = (np.radians(a) for a in rotate_deg)
+    Rx = np.array([[1, 0, 0, 0], [0, np.cos(rx), -np.sin(rx), 0], [0, np.sin(rx), np.cos(rx), 0], [0, 0, 0, 1]])
+    Ry = np.array([[np.cos(ry), 0, np.sin(ry), 0], [0, 1, 0, 0], [-np.sin(ry), 0, np.cos(ry), 0], [0, 0, 0, 1]])
+    Rz = np.array([[np.cos(rz), -np.sin(rz), 0, 0], [np.sin(rz), np.cos(rz), 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]])
+    t = np.eye(4)
+    t[:3, 3] = translate
+    return (t @ Rz @ Ry @ Rx @ s).astype(np.float32)
 
 
 @dataclass
@@ -467,8 +497,10 @@ def write_yrs(sc: Scene, path: str) -> None:
         f.write(b"YRS1")
         # last header word: record version; 1 = object records carry the
         # smoothing angle; 2 = shader records carry the version-2 texture
-        # fields; 3 = render parameters carry exposure and gamma
-        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 3))
+        # fields; 3 = render parameters carry exposure and gamma; 4 = object
+        # records carry the instance index (-1: a mesh) and, for instances,
+        # the 4x4 matrix
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 4))
         f.write(bytes(sc.camera))
         f.write(bytes(sc.render))
         for s in sc.shaders:
@@ -478,8 +510,13 @@ def write_yrs(sc: Scene, path: str) -> None:
         for m in sc.meshes:
             v = np.ascontiguousarray(m.verts, dtype=np.float32)
             t = np.ascontiguousarray(m.tris, dtype=np.uint32)
-            f.write(struct.pack("<4If", v.shape[0], t.shape[0], m.shader & 0xFFFFFFFF, 1 if m.cast_shadows else 0,
-                                float(m.smooth_angle)))
+            f.write(struct.pack("<4Ifi", v.shape[0], t.shape[0], m.shader & 0xFFFFFFFF, 1 if m.cast_shadows else 0,
+                                float(m.smooth_angle), int(m.instance_of)))
+            if m.is_instance:  # M, then a flag and M^-1 when given
+                f.write(np.ascontiguousarray(m.matrix, np.float32).reshape(16).tobytes())
+                f.write(struct.pack("<i", 0 if m.inverse is None else 1))
+                if m.inverse is not None:
+                    f.write(np.ascontiguousarray(m.inverse, np.float32).reshape(16).tobytes())
             f.write(v.tobytes())
             f.write(t.tobytes())
             if m.shader == abi.YR_PER_TRIANGLE:
@@ -518,6 +555,18 @@ def read_yrs(path: str) -> Scene:
         if version >= 1:
             (smooth,) = struct.unpack_from("<f", data, off)
             off += 4
+        inst, mat, inv = -1, None, None
+        if version >= 4:
+            (inst,) = struct.unpack_from("<i", data, off)
+            off += 4
+            if inst >= 0:
+                mat = np.frombuffer(data, np.float32, 16, off).reshape(4, 4).copy()
+                off += 64
+                (has_inv,) = struct.unpack_from("<i", data, off)
+                off += 4
+                if has_inv:
+                    inv = np.frombuffer(data, np.float32, 16, off).reshape(4, 4).copy()
+                    off += 64
         v = np.frombuffer(data, np.float32, 3 * nv, off).reshape(nv, 3).copy()
         off += 12 * nv
         t = np.frombuffer(data, np.uint32, 3 * nt, off).reshape(nt, 3).copy()
@@ -526,7 +575,7 @@ def read_yrs(path: str) -> Scene:
         if shid == abi.YR_PER_TRIANGLE:
             ts = np.frombuffer(data, np.uint32, nt, off).copy()
             off += 4 * nt
-        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast), float(smooth)))
+        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast), float(smooth), inst, mat, inv))
     return sc
 
 
