@@ -41,6 +41,60 @@ def random_mesh_scene(n, seed):
     return sc
 
 
+def box_soup(rng, n):
+    """n axis-aligned boxes (12 triangles each) on an integer grid, some
+    stacked: many coplanar, flat and coincident triangle bounds."""
+    faces = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    vs, ts = [], []
+    for k in range(n):
+        x, z = rng.integers(0, 24, 2)
+        y = rng.integers(0, 3)
+        w = rng.integers(1, 3)
+        c = np.array([[x + (i & 1) * w, y + ((i >> 1) & 1), z + ((i >> 2) & 1) * w] for i in range(8)], np.float32)
+        b = 8 * k
+        for a0, a1, a2, a3 in faces:
+            ts += [(b + a0, b + a1, b + a2), (b + a0, b + a2, b + a3)]
+        vs.append(c)
+    return np.concatenate(vs), np.array(ts, np.uint32)
+
+
+def terrace(nx, nz, seed):
+    """A height field on an nx x nz grid with heights quantised to 4 levels."""
+    rng = np.random.default_rng(seed)
+    h = rng.integers(0, 4, (nz + 1, nx + 1)).astype(np.float32) * 0.5
+    xs, zs = np.meshgrid(np.arange(nx + 1, dtype=np.float32), np.arange(nz + 1, dtype=np.float32))
+    v = np.stack([xs, h, zs], -1).reshape(-1, 3)
+    t = []
+    for j in range(nz):
+        for i in range(nx):
+            a = j * (nx + 1) + i
+            t += [(a, a + 1, a + nx + 2), (a, a + nx + 2, a + nx + 1)]
+    return v, np.array(t, np.uint32)
+
+
+def tie_scene():
+    """Meshes whose kd builds are decided by ties: equal split candidates
+    (shared vertices, coplanar faces) and flat bounds, above and below the
+    128-triangle switch between the binned and the sorted sweeps."""
+    rng = np.random.default_rng(21)
+    sc = scenes.config_small(80, 60)
+    bv, bt = box_soup(rng, 400)
+    tv, tt = terrace(40, 30, 22)
+    sv, st = scenes.uv_sphere((0.0, 0.0, 0.0), 1.0, rings=48, segments=96)
+    gv, gt = terrace(6, 5, 23)
+    sc.meshes = [scenes.Mesh(bv, bt, 0), scenes.Mesh(tv, tt, 0), scenes.Mesh(sv, st, 0), scenes.Mesh(gv, gt, 0)]
+    return sc
+
+
+def tie_trees():
+    out = {}
+    tr, _ = T.harness_trees(tie_scene())
+    for i, t in enumerate(tr):
+        for k in ("nodes", "prims", "tb"):
+            out[f"ties_{i}_{k}"] = t[k]
+    np.savez_compressed(os.path.join(HERE, "trees_ties.npz"), **out)
+
+
 def trees():
     out = {}
     for name, sc in (("sphere16", small_sphere_scene()), ("random3000", random_mesh_scene(3000, 11))):
@@ -438,6 +492,7 @@ def halton_noise():
 if __name__ == "__main__":
     assert T.has_harness(), "build the reference first: make -C oracle"
     trees()
+    tie_trees()
     rays()
     camera_and_render()
     smooth_render()

@@ -40,6 +40,26 @@ def test_kdtree_build_matches_reference(name):
         assert np.array_equal(T.mesh_bound(m).view(np.uint32), g[f"{name}_{i}_ob"].view(np.uint32))
 
 
+def _tie_scene():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mg", os.path.join(G, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.tie_scene()
+
+
+def test_kdtree_build_matches_reference_on_ties():
+    """Box soups, terraces and a dense sphere: trees decided by equal split
+    candidates and flat bounds (the order std::sort leaves equal edges in,
+    the binned sweep's flat-bound bookkeeping) still match node for node."""
+    g = load("trees_ties.npz")
+    for i, m in enumerate(_tie_scene().meshes):
+        t = T.product_tree(m)
+        assert np.array_equal(t["nodes"], g[f"ties_{i}_nodes"]), i
+        assert np.array_equal(t["prims"], g[f"ties_{i}_prims"]), i
+        assert np.array_equal(t["tb"].view(np.uint32), g[f"ties_{i}_tb"].view(np.uint32)), i
+
+
 def test_object_tree_matches_reference():
     g = load("trees.npz")
     sc = _scenes()["sphere16"]

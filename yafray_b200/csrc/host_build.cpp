@@ -19,6 +19,7 @@
 //   raw - (0.1 + l/d)*eb*raw         -> raw * (1 - (l/d + 0.1)*eb)
 //   lo - 0.021*h - 1e-5*s            -> lo - (0.021*h + 1e-5*s)   (and hi + ...)
 #include "host_build.h"
+#include "kd_sort.h"
 
 #include <algorithm>
 #include <cmath>
@@ -47,15 +48,7 @@ struct Bin {
 
 enum EdgeEnd { kLower = 0, kBoth = 1, kUpper = 2 };  // kdtree.cc:10-12
 
-struct Edge {
-    float pos;
-    int prim;
-    int end;
-    bool operator<(const Edge &e) const {  // boundEdge::operator< (kdtree.h:71-75)
-        if (pos == e.pos) return end < e.end;
-        return pos < e.pos;
-    }
-};
+using Edge = KdEdge;  // boundEdge (kdtree.h:64-76)
 
 struct Split {
     int axis = -1;
@@ -425,7 +418,7 @@ class Builder {
                     ed.push_back({bb.g[axis], pn, kUpper});
                 }
             }
-            std::sort(ed.begin(), ed.end());
+            kd_sort(ed.data(), (int)ed.size());  // std::sort's permutation (kd_sort.h)
             const int ne = (int)ed.size();
             const float cap_area = d[(axis + 1) % 3] * d[(axis + 2) % 3];
             const float cap_perim = d[(axis + 1) % 3] + d[(axis + 2) % 3];
