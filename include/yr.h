@@ -107,6 +107,25 @@ typedef struct yr_kdtree_params {
 YR_API yr_status yr_kdtree_build_ex(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris,
                                     const yr_kdtree_params *params, int nthreads, yr_kdtree **out);
 
+/* The same trees as yr_kdtree_build_ex, node for node and leaf list for
+ * leaf list, for several meshes at once, built on GPU `device`: the binned
+ * sweep of nodes above 128 triangles (kdTree_t::pigeonMinCost,
+ * kdtree.cc:167-304) level by level over all meshes, then one thread per
+ * node of at most 128 triangles running kdTree_t::buildTree's recursion
+ * (kdtree.cc:416-582, with triBoxClip, triclip.cc:50-240, and the exact
+ * sweep kdTree_t::minimalCost, kdtree.cc:311-406).  Inputs and outputs are
+ * host memory; out[i] (freed by yr_kdtree_free) is mesh i's tree.
+ * Coordinates must be finite (YR_ERR_INVALID_ARG otherwise). */
+typedef struct yr_kdtree_mesh {
+    const float *verts;      /* 3*nverts floats                                */
+    uint32_t nverts;
+    const uint32_t *tris;    /* 3*ntris vertex indices                         */
+    uint32_t ntris;
+} yr_kdtree_mesh;
+
+YR_API yr_status yr_kdtree_build_gpu(const yr_kdtree_mesh *meshes, uint32_t nmeshes,
+                                     const yr_kdtree_params *params, int32_t device, yr_kdtree **out);
+
 /* Object tree node (geomeTree_t, geometree.h:8-32): left < 0 marks a leaf
  * whose `right` is the object index; node 0 is the root, children follow
  * in depth-first order (left subtree first). */
@@ -308,6 +327,9 @@ typedef struct yr_render_params {
 #define YR_RENDER_TONEMAP 4u
 #define YR_RENDER_CLAMP_RGB 8u
 #define YR_RENDER_ALPHA_PREMULTIPLY 16u
+/* Build the meshes' kd-trees on the scene's GPU at yr_scene_create
+ * (yr_kdtree_build_gpu; the trees are the host build's). */
+#define YR_RENDER_GPU_KD_BUILD 32u
 
 typedef struct yr_object_desc {
     const float *verts;      /* 3*nverts                                       */

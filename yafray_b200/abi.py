@@ -40,6 +40,7 @@ YR_TEXCO_GLOBAL, YR_TEXCO_ORCO, YR_TEXCO_NORMAL = 0, 1, 2
 YR_PROJ_DEFAULT, YR_PROJ_X, YR_PROJ_Y, YR_PROJ_Z, YR_PROJ_NONE = 0, 1, 2, 3, 4
 YR_RENDER_SHADOW_TREE, YR_RENDER_EXACT_ORDER, YR_RENDER_TONEMAP = 1, 2, 4
 YR_RENDER_CLAMP_RGB, YR_RENDER_ALPHA_PREMULTIPLY = 8, 16
+YR_RENDER_GPU_KD_BUILD = 32
 YR_IMAGE_TGA, YR_IMAGE_HDR, YR_IMAGE_ALPHA = 0, 1, 1
 YR_PER_TRIANGLE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
@@ -67,6 +68,11 @@ class YrObjectNode(C.Structure):
 class YrKdTreeParams(C.Structure):
     _fields_ = [("max_depth", C.c_int32), ("max_leaf_size", C.c_int32), ("cost_ratio", C.c_float),
                 ("empty_bonus", C.c_float), ("large_scene_penalty", C.c_int32), ("reserved", C.c_int32)]
+
+
+class YrKdTreeMesh(C.Structure):
+    _fields_ = [("verts", C.POINTER(C.c_float)), ("nverts", C.c_uint32),
+                ("tris", C.POINTER(C.c_uint32)), ("ntris", C.c_uint32)]
 
 
 class YrCameraDesc(C.Structure):
@@ -174,6 +180,8 @@ SIGNATURES = {
     "yr_kdtree_free": (None, [C.POINTER(YrKdTree)]),
     "yr_kdtree_build_ex": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32,
                                      C.POINTER(YrKdTreeParams), C.c_int, C.POINTER(C.POINTER(YrKdTree))]),
+    "yr_kdtree_build_gpu": (C.c_int, [C.POINTER(YrKdTreeMesh), C.c_uint32, C.POINTER(YrKdTreeParams), C.c_int32,
+                                      C.POINTER(C.POINTER(YrKdTree))]),
     "yr_object_tree_build": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(YrObjectNode),
                                        C.POINTER(C.c_uint32)]),
     "yr_instance_bound": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),

@@ -5,6 +5,32 @@
 
 #include "host_build.h"
 
+namespace yr {
+yr_status export_tree(const KdTree &t, yr_kdtree **out) {
+    yr_kdtree *r = new (std::nothrow) yr_kdtree;
+    if (!r) return YR_ERR_OUT_OF_MEMORY;
+    std::memset(r, 0, sizeof(*r));
+    r->nnodes = (uint32_t)t.nodes.size();
+    r->nprims = (uint32_t)t.prims.size();
+    r->nodes = new (std::nothrow) yr_kd_node[r->nnodes ? r->nnodes : 1];
+    r->prims = new (std::nothrow) uint32_t[r->nprims ? r->nprims : 1];
+    if (!r->nodes || !r->prims) {
+        yr_kdtree_free(r);
+        return YR_ERR_OUT_OF_MEMORY;
+    }
+    if (r->nnodes) std::memcpy(r->nodes, t.nodes.data(), sizeof(yr_kd_node) * r->nnodes);
+    if (r->nprims) std::memcpy(r->prims, t.prims.data(), 4 * (size_t)r->nprims);
+    std::memcpy(r->bound, t.bound.a, 12);
+    std::memcpy(r->bound + 3, t.bound.g, 12);
+    r->max_depth = t.max_depth;
+    r->max_leaf_size = t.max_leaf_size;
+    r->cost_ratio = t.cost_ratio;
+    r->empty_bonus = t.empty_bonus;
+    *out = r;
+    return YR_OK;
+}
+}  // namespace yr
+
 extern "C" {
 
 YR_API const char *yr_status_string(yr_status s) {
@@ -26,6 +52,7 @@ YR_API const char *yr_status_string(yr_status s) {
 }
 
 YR_API const char *yr_version(void) { return "yafray_b200 0.1 (YafRay 0.0.9 hot path, sm_100a)"; }
+
 
 YR_API yr_status yr_kdtree_build(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris,
                                  yr_kdtree **out) {
@@ -52,27 +79,7 @@ YR_API yr_status yr_kdtree_build_ex(const float *verts, uint32_t nverts, const u
         return YR_ERR_OUT_OF_MEMORY;
     }
     if (st != YR_OK) return st;
-    yr_kdtree *r = new (std::nothrow) yr_kdtree;
-    if (!r) return YR_ERR_OUT_OF_MEMORY;
-    std::memset(r, 0, sizeof(*r));
-    r->nnodes = (uint32_t)t.nodes.size();
-    r->nprims = (uint32_t)t.prims.size();
-    r->nodes = new (std::nothrow) yr_kd_node[r->nnodes ? r->nnodes : 1];
-    r->prims = new (std::nothrow) uint32_t[r->nprims ? r->nprims : 1];
-    if (!r->nodes || !r->prims) {
-        yr_kdtree_free(r);
-        return YR_ERR_OUT_OF_MEMORY;
-    }
-    if (r->nnodes) std::memcpy(r->nodes, t.nodes.data(), sizeof(yr_kd_node) * r->nnodes);
-    if (r->nprims) std::memcpy(r->prims, t.prims.data(), 4 * (size_t)r->nprims);
-    std::memcpy(r->bound, t.bound.a, 12);
-    std::memcpy(r->bound + 3, t.bound.g, 12);
-    r->max_depth = t.max_depth;
-    r->max_leaf_size = t.max_leaf_size;
-    r->cost_ratio = t.cost_ratio;
-    r->empty_bonus = t.empty_bonus;
-    *out = r;
-    return YR_OK;
+    return yr::export_tree(t, out);
 }
 
 YR_API yr_status yr_object_tree_build(const float *bounds, uint32_t n, yr_object_node *out, uint32_t *nout) {

@@ -19,6 +19,7 @@
 //   raw - (0.1 + l/d)*eb*raw         -> raw * (1 - (l/d + 0.1)*eb)
 //   lo - 0.021*h - 1e-5*s            -> lo - (0.021*h + 1e-5*s)   (and hi + ...)
 #include "host_build.h"
+#include "kd_clip.h"
 #include "kd_sort.h"
 
 #include <algorithm>
@@ -60,82 +61,10 @@ struct Split {
     int n_edge = 0;
 };
 
-// Sutherland-Hodgman clip of a triangle against an axis-aligned box, in
-// double (triClip.cc:50-240).  Returns 0 = clipped bound in `box`,
-// 1 = nothing left, 2 = polygon overflow (caller keeps the full bound).
+// Sutherland-Hodgman clip (kd_clip.h).  Returns 0 = clipped bound in
+// `box`, 1 = nothing left, 2 = polygon overflow (caller keeps the full bound).
 int clip_triangle(const double bmin[3], const double bmax[3], const double v[3][3], Box &box) {
-    double buf1[11][3], buf2[11][3];
-    double(*poly)[3] = buf1;
-    double(*cpoly)[3] = buf2;
-    for (int q = 0; q < 3; q++) {
-        poly[q][0] = v[q][0];
-        poly[q][1] = v[q][1];
-        poly[q][2] = v[q][2];
-        poly[3][q] = v[0][q];
-    }
-    int n = 3;
-    for (int axis = 0; axis < 3; axis++) {
-        const int na = (axis + 1) % 3, pa = (axis + 2) % 3;
-        for (int side = 0; side < 2; side++) {
-            // side 0 clips against the lower plane, side 1 against the upper one
-            const double plane = side == 0 ? bmin[axis] : bmax[axis];
-            auto inside = [&](double x) { return side == 0 ? (x >= plane) : (x <= plane); };
-            auto strictly_in = [&](double x) { return side == 0 ? (x > plane) : (x < plane); };
-            int nc = 0;
-            bool p1_in = inside(poly[0][axis]);
-            for (int i = 0; i < n; i++) {
-                const double *p1 = poly[i], *p2 = poly[i + 1];
-                if (p1_in) {
-                    if (inside(p2[axis])) {
-                        std::memcpy(cpoly[nc], p2, sizeof(double) * 3);
-                        nc++;
-                        p1_in = true;
-                    } else {
-                        double t = (plane - p1[axis]) / (p2[axis] - p1[axis]);
-                        cpoly[nc][axis] = plane;
-                        cpoly[nc][na] = p1[na] + t * (p2[na] - p1[na]);
-                        cpoly[nc][pa] = p1[pa] + t * (p2[pa] - p1[pa]);
-                        nc++;
-                        p1_in = false;
-                    }
-                } else {
-                    if (strictly_in(p2[axis])) {
-                        double t = (plane - p2[axis]) / (p1[axis] - p2[axis]);
-                        cpoly[nc][axis] = plane;
-                        cpoly[nc][na] = p2[na] + t * (p1[na] - p2[na]);
-                        cpoly[nc][pa] = p2[pa] + t * (p1[pa] - p2[pa]);
-                        nc++;
-                        std::memcpy(cpoly[nc], p2, sizeof(double) * 3);
-                        nc++;
-                        p1_in = true;
-                    } else if (p2[axis] == plane) {
-                        std::memcpy(cpoly[nc], p2, sizeof(double) * 3);
-                        nc++;
-                        p1_in = true;
-                    } else {
-                        p1_in = false;
-                    }
-                }
-            }
-            if (nc > 9) return 2;
-            std::memcpy(cpoly[nc], cpoly[0], sizeof(double) * 3);
-            n = nc;
-            std::swap(poly, cpoly);
-        }
-    }
-    if (n < 2) return 1;
-    double a[3], g[3];
-    for (int k = 0; k < 3; k++) a[k] = g[k] = poly[0][k];
-    for (int i = 1; i < n; i++)
-        for (int k = 0; k < 3; k++) {
-            a[k] = std::min(a[k], poly[i][k]);
-            g[k] = std::max(g[k], poly[i][k]);
-        }
-    for (int k = 0; k < 3; k++) {
-        box.a[k] = (float)a[k];
-        box.g[k] = (float)g[k];
-    }
-    return 0;
+    return kd_clip_triangle(bmin, bmax, v, box.a, box.g);
 }
 
 class Builder {
@@ -159,19 +88,8 @@ class Builder {
 
     yr_status run(const KdParams &kp, int nthreads) {
         // kdTree_t ctor parameter defaults (kdtree.cc:57-80)
-        cost_ratio_ = kp.cost_ratio;
         ebonus_ = kp.empty_bonus;
-        max_depth_ = kp.max_depth;
-        max_leaf_ = kp.max_leaf;
-        if (max_depth_ <= 0) max_depth_ = int(6.0f + 1.66f * std::log(float(n_)));
-        const double log_leaves = 1.442695f * std::log(double(n_));
-        if (max_leaf_ <= 0) {
-            max_leaf_ = int(log_leaves - 16.0);
-            if (max_leaf_ <= 0) max_leaf_ = 1;
-        }
-        if (max_depth_ > 64) max_depth_ = 64;
-        if (kp.large_scene_penalty && log_leaves > 16.0)
-            cost_ratio_ = (float)(cost_ratio_ + 0.25 * (log_leaves - 16.0));
+        kd_limits(n_, kp, max_depth_, max_leaf_, cost_ratio_);
         if (nthreads > 1 && n_ > 4096) {
             defer_depth_ = 0;
             while ((1 << defer_depth_) < 4 * nthreads && defer_depth_ < 12) defer_depth_++;
@@ -195,13 +113,7 @@ class Builder {
                 }
             }
         }
-        // grow by 1e-4 of the diagonal (kdtree.cc:83-89)
-        float dx = tree_.g[0] - tree_.a[0], dy = tree_.g[1] - tree_.a[1], dz = tree_.g[2] - tree_.a[2];
-        float diag = (float)(std::sqrt(dx * dx + dy * dy + dz * dz) * 0.0001);
-        for (int k = 0; k < 3; k++) {
-            tree_.a[k] -= diag;
-            tree_.g[k] += diag;
-        }
+        tree_ = kd_grow_bound(tree_);
         std::vector<uint32_t> all(n_);
         for (uint32_t i = 0; i < n_; i++) all[i] = i;
         out_.nodes.clear();
@@ -739,6 +651,31 @@ class Clusterer {
 };
 
 }  // namespace
+
+void kd_limits(uint32_t n, const KdParams &kp, int &max_depth, int &max_leaf, float &cost_ratio) {
+    cost_ratio = kp.cost_ratio;
+    max_depth = kp.max_depth;
+    max_leaf = kp.max_leaf;
+    if (max_depth <= 0) max_depth = int(6.0f + 1.66f * std::log(float(n)));
+    const double log_leaves = 1.442695f * std::log(double(n));
+    if (max_leaf <= 0) {
+        max_leaf = int(log_leaves - 16.0);
+        if (max_leaf <= 0) max_leaf = 1;
+    }
+    if (max_depth > 64) max_depth = 64;
+    if (kp.large_scene_penalty && log_leaves > 16.0) cost_ratio = (float)(cost_ratio + 0.25 * (log_leaves - 16.0));
+}
+
+Box kd_grow_bound(const Box &b) {
+    Box t = b;
+    const float dx = t.g[0] - t.a[0], dy = t.g[1] - t.a[1], dz = t.g[2] - t.a[2];
+    const float diag = (float)(std::sqrt(dx * dx + dy * dy + dz * dz) * 0.0001);
+    for (int k = 0; k < 3; k++) {
+        t.a[k] -= diag;
+        t.g[k] += diag;
+    }
+    return t;
+}
 
 yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris, uint32_t ntris, KdTree &out,
                        const KdParams &params, int nthreads) {

@@ -42,6 +42,27 @@ yr_status build_kdtree(const float *verts, uint32_t nverts, const uint32_t *tris
                        uint32_t ntris, KdTree &out, const KdParams &params = KdParams(),
                        int nthreads = 1);
 
+// kdTree_t's constructor defaults for n triangles (kdtree.cc:57-80): the
+// depth and leaf-size limits and the cost ratio with the large-scene penalty.
+void kd_limits(uint32_t n, const KdParams &kp, int &max_depth, int &max_leaf, float &cost_ratio);
+// The tree bound: the triangles' bound grown by 1e-4 of its diagonal on
+// every side (kdtree.cc:83-89).
+Box kd_grow_bound(const Box &b);
+
+// The same trees as build_kdtree for several meshes at once, built on the
+// GPU `device` (kd_gpu.cu).
+struct KdMesh {
+    const float *verts;
+    uint32_t nverts;
+    const uint32_t *tris;
+    uint32_t ntris;
+};
+yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &params, int device,
+                            std::vector<KdTree> &out);
+
+// A KdTree as a yr_kdtree allocated for the caller (freed by yr_kdtree_free).
+yr_status export_tree(const KdTree &t, yr_kdtree **out);
+
 // meshObject_t::recalcBound (mesh.cc:343-379): bound of the triangles'
 // vertices grown by BOX_MIN.
 Box mesh_bound(const float *verts, const uint32_t *tris, uint32_t ntris);

@@ -33,21 +33,45 @@ struct KdEdge {
     int end;  // 0 lower, 1 both (flat), 2 upper (kdtree.cc:10-12)
 };
 
+// The same edge in 8 bytes: triangle index << 2 | end.
+struct KdEdge8 {
+    float pos;
+    uint32_t pe;
+};
+
 YR_HD bool kd_edge_less(const KdEdge &a, const KdEdge &b) {
     if (a.pos == b.pos) return a.end < b.end;
     return a.pos < b.pos;
 }
 
-YR_HD void kd_swap(KdEdge &a, KdEdge &b) {
-    KdEdge t = a;
-    a = b;
-    b = t;
+YR_HD bool kd_edge_less(const KdEdge8 &a, const KdEdge8 &b) {
+    if (a.pos == b.pos) return (a.pe & 3u) < (b.pe & 3u);
+    return a.pos < b.pos;
+}
+
+// An array whose elements lie `s` apart (one thread's column of an
+// interleaved shared-memory block).
+template <class T>
+struct KdStrided {
+    T *p;
+    int s;
+    YR_HD T &operator[](int i) const { return p[(size_t)i * s]; }
+    YR_HD KdStrided operator+(int k) const { return KdStrided{p + (size_t)k * s, s}; }
+};
+
+// The functions below take any array-like `E` (a pointer or KdStrided).
+template <class E>
+YR_HD void kd_swap_at(E e, int i, int j) {
+    auto t = e[i];
+    e[i] = e[j];
+    e[j] = t;
 }
 
 // Sift `v` down from `hole` in the max-heap e[0, len), then back up towards
 // the starting index (the two-phase heap adjustment of the SGI heap
 // algorithms).
-YR_HD void kd_heap_adjust(KdEdge *e, int hole, int len, KdEdge v) {
+template <class E, class T>
+YR_HD void kd_heap_adjust(E e, int hole, int len, T v) {
     const int top = hole;
     int child = hole;
     while (child < (len - 1) / 2) {
@@ -72,51 +96,56 @@ YR_HD void kd_heap_adjust(KdEdge *e, int hole, int len, KdEdge v) {
 
 // Heapsort of e[0, n): build the heap bottom-up, then move the maximum to
 // the back one element at a time.
-YR_HD void kd_heapsort(KdEdge *e, int n) {
+template <class E>
+YR_HD void kd_heapsort(E e, int n) {
     if (n < 2) return;
     for (int parent = (n - 2) / 2;; parent--) {
-        kd_heap_adjust(e, parent, n, e[parent]);
+        auto v = e[parent];
+        kd_heap_adjust(e, parent, n, v);
         if (parent == 0) break;
     }
     for (int last = n - 1; last > 0; last--) {
-        const KdEdge v = e[last];
+        auto v = e[last];
         e[last] = e[0];
         kd_heap_adjust(e, 0, last, v);
     }
 }
 
 // Move the median of e[a], e[b], e[c] into e[r].
-YR_HD void kd_median_to(KdEdge *e, int r, int a, int b, int c) {
+template <class E>
+YR_HD void kd_median_to(E e, int r, int a, int b, int c) {
     if (kd_edge_less(e[a], e[b])) {
-        if (kd_edge_less(e[b], e[c])) kd_swap(e[r], e[b]);
-        else if (kd_edge_less(e[a], e[c])) kd_swap(e[r], e[c]);
-        else kd_swap(e[r], e[a]);
+        if (kd_edge_less(e[b], e[c])) kd_swap_at(e, r, b);
+        else if (kd_edge_less(e[a], e[c])) kd_swap_at(e, r, c);
+        else kd_swap_at(e, r, a);
     } else if (kd_edge_less(e[a], e[c])) {
-        kd_swap(e[r], e[a]);
+        kd_swap_at(e, r, a);
     } else if (kd_edge_less(e[b], e[c])) {
-        kd_swap(e[r], e[c]);
+        kd_swap_at(e, r, c);
     } else {
-        kd_swap(e[r], e[b]);
+        kd_swap_at(e, r, b);
     }
 }
 
 // Hoare partition of e[lo, hi) around the pivot at e[p] (p < lo), without
 // bounds checks: the median-of-three guarantees both scans stop.
-YR_HD int kd_partition(KdEdge *e, int lo, int hi, int p) {
+template <class E>
+YR_HD int kd_partition(E e, int lo, int hi, int p) {
     for (;;) {
         while (kd_edge_less(e[lo], e[p])) ++lo;
         --hi;
         while (kd_edge_less(e[p], e[hi])) --hi;
         if (!(lo < hi)) return lo;
-        kd_swap(e[lo], e[hi]);
+        kd_swap_at(e, lo, hi);
         ++lo;
     }
 }
 
 // Insert e[i] into the sorted run to its left, knowing a smaller-or-equal
 // element stops the scan.
-YR_HD void kd_insert_unguarded(KdEdge *e, int i) {
-    const KdEdge v = e[i];
+template <class E>
+YR_HD void kd_insert_unguarded(E e, int i) {
+    const auto v = e[i];
     int j = i - 1;
     while (kd_edge_less(v, e[j])) {
         e[i] = e[j];
@@ -126,11 +155,12 @@ YR_HD void kd_insert_unguarded(KdEdge *e, int i) {
     e[i] = v;
 }
 
-YR_HD void kd_insertion_sort(KdEdge *e, int lo, int hi) {
+template <class E>
+YR_HD void kd_insertion_sort(E e, int lo, int hi) {
     if (lo == hi) return;
     for (int i = lo + 1; i != hi; ++i) {
         if (kd_edge_less(e[i], e[lo])) {
-            const KdEdge v = e[i];
+            const auto v = e[i];
             for (int j = i; j > lo; --j) e[j] = e[j - 1];
             e[lo] = v;
         } else {
@@ -142,11 +172,13 @@ YR_HD void kd_insertion_sort(KdEdge *e, int lo, int hi) {
 constexpr int kKdSortThreshold = 16;
 
 // The quicksort phase on e[lo, hi): the right part of each partition is
-// sorted before the left one, whose bounds wait on an explicit stack (the
-// depth limit 2*log2 n keeps it below 64 entries for every 32-bit size).
+// sorted before the left one, whose bounds wait on an explicit stack.  Each
+// entry uses up one level of the depth limit 2*floor(log2 n), so kCap
+// entries serve every n below 2^(kCap/2 + 1) (16 entries: n <= 511).
 // The parts are disjoint, so the order only matters for readability.
-YR_HD void kd_introsort_loop(KdEdge *e, int lo, int hi, int depth) {
-    int st_lo[64], st_hi[64], st_depth[64];
+template <int kCap, class E>
+YR_HD void kd_introsort_loop(E e, int lo, int hi, int depth) {
+    int st_lo[kCap], st_hi[kCap], st_depth[kCap];
     int sp = 0;
     for (;;) {
         while (hi - lo > kKdSortThreshold) {
@@ -181,9 +213,10 @@ YR_HD int kd_floor_log2(int n) {
     return k;
 }
 
-YR_HD void kd_sort(KdEdge *e, int n) {
+template <int kCap = 64, class E>
+YR_HD void kd_sort(E e, int n) {
     if (n <= 0) return;
-    kd_introsort_loop(e, 0, n, 2 * kd_floor_log2(n));
+    kd_introsort_loop<kCap>(e, 0, n, 2 * kd_floor_log2(n));
     if (n > kKdSortThreshold) {
         kd_insertion_sort(e, 0, kKdSortThreshold);
         for (int i = kKdSortThreshold; i < n; ++i) kd_insert_unguarded(e, i);

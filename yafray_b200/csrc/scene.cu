@@ -403,6 +403,31 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     // cores (each tree is the same as a sequential build)
     std::vector<KdTree> trees(desc->nobjects);
     std::vector<yr_status> tree_st(desc->nobjects, YR_OK);
+    std::vector<char> built(desc->nobjects, 0);
+    if (desc->render.flags & YR_RENDER_GPU_KD_BUILD) {  // all meshes' trees in one GPU build
+        std::vector<KdMesh> ms;
+        std::vector<uint32_t> which;
+        for (uint32_t o = 0; o < desc->nobjects; o++) {
+            const yr_object_desc &od = desc->objects[o];
+            if (is_inst(o) || od.tree) continue;
+            ms.push_back(KdMesh{od.verts, od.nverts, od.tris, od.ntris});
+            which.push_back(o);
+        }
+        if (!ms.empty()) {
+            std::vector<KdTree> gt;
+            yr_status gs;
+            try {
+                gs = build_kdtrees_gpu(ms, KdParams(), device, gt);
+            } catch (const std::bad_alloc &) {
+                gs = YR_ERR_OUT_OF_MEMORY;
+            }
+            if (gs != YR_OK) return fail(gs);
+            for (size_t i = 0; i < which.size(); i++) {
+                trees[which[i]] = std::move(gt[i]);
+                built[which[i]] = 1;
+            }
+        }
+    }
     {
         std::atomic<uint32_t> next{0};
         auto worker = [&] {
@@ -410,6 +435,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
                 const uint32_t o = next.fetch_add(1);
                 if (o >= desc->nobjects) return;
                 if (is_inst(o)) continue;  // shares its original's tree
+                if (built[o]) continue;
                 const yr_object_desc &od = desc->objects[o];
                 KdTree &tree = trees[o];
                 try {
