@@ -449,13 +449,71 @@ def run_batch(args, api, torch, local, barrier):
     print(json.dumps(line))
 
 
+def run_kdbuild(args, api, local):
+    """kd-trees of every mesh of the large scene (kdTree_t, kdtree.cc:57-582):
+    yr_kdtree_build_gpu (host meshes in, host trees out, one call) against
+    the host build on all host cores (yr_kdtree_build_ex per mesh, meshes
+    spread over threads, as scene creation does); trees compared node for
+    node."""
+    import concurrent.futures as cf
+    import ctypes as C
+    import numpy as np
+    from yafray_b200 import abi, scenes
+    sc = scenes.config_large(seed=args.seed, resx=64, resy=64, spp=1, grid=args.grid)
+    meshes = [m for m in sc.meshes if not m.is_instance]
+    ntris = sum(int(m.tris.shape[0]) for m in meshes)
+    for _ in range(args.warmup):
+        api.kdtrees_gpu(meshes, device=local)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        g = api.kdtrees_gpu(meshes, device=local)
+        times.append(time.perf_counter() - t0)
+    lib = abi.load()
+
+    def host(m):
+        v = np.ascontiguousarray(m.verts, np.float32)
+        t = np.ascontiguousarray(m.tris, np.uint32)
+        p = C.POINTER(abi.YrKdTree)()
+        abi.check(lib.yr_kdtree_build_ex(v.ctypes.data_as(C.POINTER(C.c_float)), v.shape[0],
+                                         t.ctypes.data_as(C.POINTER(C.c_uint32)), t.shape[0], None, 1,
+                                         C.byref(p)), "yr_kdtree_build_ex")
+        tr = p.contents
+        nodes = np.ctypeslib.as_array(C.cast(tr.nodes, C.POINTER(C.c_uint32)), (2 * tr.nnodes,)).copy()
+        prims = np.ctypeslib.as_array(tr.prims, (max(tr.nprims, 1),))[:tr.nprims].copy()
+        lib.yr_kdtree_free(p)
+        return nodes, prims
+
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(cores) as ex:
+        h = list(ex.map(host, meshes))
+    host_s = time.perf_counter() - t0
+    same = all(np.array_equal(a["nodes"].reshape(-1), b[0]) and np.array_equal(a["prims"], b[1])
+               for a, b in zip(g, h))
+    best = min(times)
+    line = {
+        "metric": "kd-tree build Mtriangles/s", "value": ntris / best / 1e6, "unit": "Mtriangles/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * best,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+        "data": "synthetic (seeded scene generator)",
+        "config": {"workload": f"kd build of the large scene's {len(meshes)} meshes ({ntris} triangles), "
+                               "host meshes in, host trees out (yr_kdtree_build_gpu)",
+                   "timing": "wall clock around the call (host copies, device build, trees back)"},
+        "host_build": {"value": ntris / host_s / 1e6, "unit": "Mtriangles/s", "seconds": host_s, "cores": cores},
+        "trees_identical": bool(same),
+        "gpu_seconds": [round(t, 4) for t in times],
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small", "batch", "diff", "inverse"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "batch", "diff", "inverse", "kdbuild"])
     ap.add_argument("--inverse-count", type=int, default=32, help="problems in the inverse workload")
     ap.add_argument("--inverse-steps", type=int, default=200, help="Adam steps per problem")
     ap.add_argument("--batch-count", type=int, default=256, help="scenes in the batch workload")
@@ -488,6 +546,10 @@ def main():
         if world > 1:
             dist.barrier()
 
+    if args.config == "kdbuild":
+        if rank == 0:
+            run_kdbuild(args, api, local)
+        return
     if args.config == "batch":
         run_batch(args, api, torch, local, barrier)
         return
@@ -508,6 +570,13 @@ def main():
     ds = api.DeviceScene(sc, device=local)
     info = ds.info()
     build_s = time.perf_counter() - t0
+    # the same kd-trees built on the GPU (yr_kdtree_build_gpu), timed once
+    meshes = [m for m in sc.meshes if not m.is_instance]
+    t0 = time.perf_counter()
+    gtrees = api.kdtrees_gpu(meshes, device=local)
+    gpu_kd_s = time.perf_counter() - t0
+    gpu_kd_nodes = int(sum(t["nodes"].shape[0] for t in gtrees))
+    del gtrees
     out = torch.empty((sc.resy, sc.resx, 4), dtype=torch.float32, device="cuda")
     for _ in range(args.warmup):
         ds.render_into(out.data_ptr())
@@ -596,6 +665,7 @@ def main():
                    "kd_nodes": int(info.nnodes), "l2": "inputs larger than L2 (scene arrays "
                    f"{info.device_bytes / 1e6:.0f} MB on the device)",
                    "host_build_s": round(info.build_seconds, 3), "scene_setup_s": round(build_s, 3),
+                   "gpu_kd_build_s": round(gpu_kd_s, 3), "gpu_kd_nodes_equal": gpu_kd_nodes == int(info.nnodes),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": gpu_launches,

@@ -93,29 +93,8 @@ def product_tree(mesh: scenes.Mesh, params=None, nthreads=1) -> dict:
 def gpu_trees(meshes, params=None, device=0) -> list:
     """yr_kdtree_build_gpu over several meshes: one dict per mesh, as
     product_tree returns."""
-    lib = abi.load()
-    keep = []
-    arr = (abi.YrKdTreeMesh * len(meshes))()
-    for i, m in enumerate(meshes):
-        v = np.ascontiguousarray(m.verts, np.float32)
-        t = np.ascontiguousarray(m.tris, np.uint32)
-        keep += [v, t]
-        arr[i].verts = v.ctypes.data_as(C.POINTER(C.c_float))
-        arr[i].nverts = v.shape[0]
-        arr[i].tris = t.ctypes.data_as(C.POINTER(C.c_uint32))
-        arr[i].ntris = t.shape[0]
-    outs = (C.POINTER(abi.YrKdTree) * len(meshes))()
-    abi.check(lib.yr_kdtree_build_gpu(arr, len(meshes), C.byref(params) if params is not None else None, device,
-                                      outs), "yr_kdtree_build_gpu")
-    res = []
-    for p in outs:
-        tr = p.contents
-        nodes = np.ctypeslib.as_array(C.cast(tr.nodes, C.POINTER(C.c_uint32)), (2 * tr.nnodes,)).reshape(-1, 2).copy()
-        prims = np.ctypeslib.as_array(tr.prims, (max(tr.nprims, 1),))[:tr.nprims].copy()
-        res.append(dict(nodes=nodes, prims=prims, tb=np.array(tr.bound[:], np.float32), max_depth=tr.max_depth,
-                        max_leaf=tr.max_leaf_size, cost_ratio=np.float32(tr.cost_ratio)))
-        lib.yr_kdtree_free(p)
-    return res
+    from yafray_b200 import api
+    return api.kdtrees_gpu(meshes, params, device)
 
 
 def mesh_bound(mesh: scenes.Mesh) -> np.ndarray:

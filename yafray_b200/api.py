@@ -184,6 +184,35 @@ def backward_batch(dss: List[DeviceScene], image_ptrs: List[int], target_ptrs: L
     return losses
 
 
+def kdtrees_gpu(meshes, params: Optional[abi.YrKdTreeParams] = None, device: int = 0) -> List[dict]:
+    """kd-trees of several meshes built on one GPU (yr_kdtree_build_gpu):
+    per mesh a dict of nodes ((n, 2) uint32: word, flags), prims, tb (tree
+    bound), max_depth, max_leaf, cost_ratio -- the host build's trees."""
+    lib = abi.load()
+    keep = []
+    arr = (abi.YrKdTreeMesh * len(meshes))()
+    for i, m in enumerate(meshes):
+        v = np.ascontiguousarray(m.verts, np.float32)
+        t = np.ascontiguousarray(m.tris, np.uint32)
+        keep += [v, t]
+        arr[i].verts = v.ctypes.data_as(C.POINTER(C.c_float))
+        arr[i].nverts = v.shape[0]
+        arr[i].tris = t.ctypes.data_as(C.POINTER(C.c_uint32))
+        arr[i].ntris = t.shape[0]
+    outs = (C.POINTER(abi.YrKdTree) * len(meshes))()
+    abi.check(lib.yr_kdtree_build_gpu(arr, len(meshes), C.byref(params) if params is not None else None, device,
+                                      outs), "yr_kdtree_build_gpu")
+    res = []
+    for p in outs:
+        tr = p.contents
+        nodes = np.ctypeslib.as_array(C.cast(tr.nodes, C.POINTER(C.c_uint32)), (2 * tr.nnodes,)).reshape(-1, 2).copy()
+        prims = np.ctypeslib.as_array(tr.prims, (max(tr.nprims, 1),))[:tr.nprims].copy()
+        res.append(dict(nodes=nodes, prims=prims, tb=np.array(tr.bound[:], np.float32), max_depth=tr.max_depth,
+                        max_leaf=tr.max_leaf_size, cost_ratio=np.float32(tr.cost_ratio)))
+        lib.yr_kdtree_free(p)
+    return res
+
+
 def encode_image(rgba: np.ndarray, fmt: str = "tga", alpha: bool = False) -> bytes:
     """The bytes YafRay's TGA (outTga_t) or Radiance HDR (outHDR_t) writer
     produces for this float RGBA image (rows top first)."""

@@ -50,7 +50,9 @@ void kd_limits(uint32_t n, const KdParams &kp, int &max_depth, int &max_leaf, fl
 Box kd_grow_bound(const Box &b);
 
 // The same trees as build_kdtree for several meshes at once, built on the
-// GPU `device` (kd_gpu.cu).
+// GPU `device` (kd_gpu.cu).  With `abi_out` (one slot per mesh) the trees
+// go to yr_kdtree records allocated there instead of `out`; on failure the
+// slots filled so far are left for the caller to free.
 struct KdMesh {
     const float *verts;
     uint32_t nverts;
@@ -58,7 +60,7 @@ struct KdMesh {
     uint32_t ntris;
 };
 yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &params, int device,
-                            std::vector<KdTree> &out);
+                            std::vector<KdTree> &out, yr_kdtree **abi_out = nullptr);
 
 // A KdTree as a yr_kdtree allocated for the caller (freed by yr_kdtree_free).
 yr_status export_tree(const KdTree &t, yr_kdtree **out);

@@ -31,10 +31,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <chrono>
 #include <cmath>
-#include <cstdio>
 #include <cstring>
+#include <new>
+#include <thread>
 #include <vector>
 
 #include "host_build.h"
@@ -805,29 +805,52 @@ inline unsigned blocks(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t
 
 }  // namespace
 
+namespace {
+
+// Run f(o) for every mesh o on all host cores.
+template <class F>
+void for_meshes(uint32_t n, F f) {
+    unsigned nth = std::thread::hardware_concurrency();
+    nth = std::max(1u, std::min(nth ? nth : 1u, n));
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nth; t++)
+        pool.emplace_back([&, t] {
+            for (uint32_t o = t; o < n; o += nth) f(o);
+        });
+    for (uint32_t o = 0; o < n; o += nth) f(o);
+    for (std::thread &th : pool) th.join();
+}
+
+}  // namespace
+
 yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &kp, int device,
-                            std::vector<KdTree> &out) {
+                            std::vector<KdTree> &out, yr_kdtree **abi_out) {
     const uint32_t nobj = (uint32_t)meshes.size();
     if (nobj == 0) return YR_ERR_INVALID_ARG;
-#ifdef YR_KD_TIMING  // phase times on stderr (timing builds only)
-    const auto t_start = std::chrono::steady_clock::now();
-    auto mark = [&](const char *what) {
-        fprintf(stderr, "kd_gpu %-10s %8.2f ms\n", what,
-                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
-    };
-#else
-    auto mark = [](const char *) {};
-#endif
     size_t nt = 0, nv = 0;
     for (const KdMesh &m : meshes) {
         if (!m.verts || !m.tris || m.ntris == 0) return YR_ERR_EMPTY_SCENE;
-        for (size_t i = 0; i < 3 * (size_t)m.ntris; i++)
-            if (m.tris[i] >= m.nverts) return YR_ERR_INVALID_ARG;
-        // the sweeps need ordered positions: no NaN or infinite coordinate
-        for (size_t i = 0; i < 3 * (size_t)m.nverts; i++)
-            if (!std::isfinite(m.verts[i])) return YR_ERR_INVALID_ARG;
         nt += m.ntris;
         nv += m.nverts;
+    }
+    {
+        std::vector<yr_status> chk(nobj, YR_OK);
+        for_meshes(nobj, [&](uint32_t o) {
+            const KdMesh &m = meshes[o];
+            for (size_t i = 0; i < 3 * (size_t)m.ntris; i++)
+                if (m.tris[i] >= m.nverts) {
+                    chk[o] = YR_ERR_INVALID_ARG;
+                    return;
+                }
+            // the sweeps need ordered positions: no NaN or infinite coordinate
+            for (size_t i = 0; i < 3 * (size_t)m.nverts; i++)
+                if (!std::isfinite(m.verts[i])) {
+                    chk[o] = YR_ERR_INVALID_ARG;
+                    return;
+                }
+        });
+        for (yr_status c : chk)
+            if (c != YR_OK) return c;
     }
     // candidates pack index << 2; list offsets carry two flag bits
     if (nt >= (1u << 28) || nv >= 0xffffffffu / 3) return YR_ERR_TOO_LARGE;
@@ -849,22 +872,27 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     std::vector<uint32_t> ht(3 * nt);
     std::vector<ObjP> hop(nobj);
     {
+        std::vector<size_t> vbase(nobj), tbase(nobj);
         size_t vb = 0, tb = 0;
         for (uint32_t o = 0; o < nobj; o++) {
+            vbase[o] = vb;
+            tbase[o] = tb;
+            vb += meshes[o].nverts;
+            tb += meshes[o].ntris;
+        }
+        for_meshes(nobj, [&](uint32_t o) {
             const KdMesh &m = meshes[o];
-            std::memcpy(hv.data() + 3 * vb, m.verts, 12 * (size_t)m.nverts);
-            for (size_t i = 0; i < 3 * (size_t)m.ntris; i++) ht[3 * tb + i] = (uint32_t)(m.tris[i] + vb);
+            std::memcpy(hv.data() + 3 * vbase[o], m.verts, 12 * (size_t)m.nverts);
+            for (size_t i = 0; i < 3 * (size_t)m.ntris; i++)
+                ht[3 * tbase[o] + i] = (uint32_t)(m.tris[i] + vbase[o]);
             ObjP &P = hop[o];
             std::memset(&P, 0, sizeof(P));
-            P.tri_base = (uint32_t)tb;
+            P.tri_base = (uint32_t)tbase[o];
             P.ntris = m.ntris;
             P.ebonus = kp.empty_bonus;
             kd_limits(m.ntris, kp, P.max_depth, P.max_leaf, P.cost_ratio);
-            vb += m.nverts;
-            tb += m.ntris;
-        }
+        });
     }
-    mark("inputs");
     DBuf d_verts, d_tris, d_bnd, d_op, d_obnd, d_err, d_tot;
     if (!d_verts.ensure(hv.size() * 4, 0, st) || !d_tris.ensure(ht.size() * 4, 0, st) || !d_bnd.ensure(24 * nt, 0, st) ||
         !d_op.ensure(sizeof(ObjP) * nobj, 0, st) || !d_obnd.ensure(24 * (size_t)nobj, 0, st) ||
@@ -910,7 +938,6 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         std::memcpy(hop[o].tb + 3, g.g, 12);
     }
 
-    mark("bounds");
     // depth 0: the roots, above or below the 128-triangle switch
     std::vector<BigNode> hbig, hsmall;
     std::vector<uint32_t> hrefs, hsrefs;
@@ -955,7 +982,6 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     T.nids = nobj;
     std::vector<uint32_t> level_lo{0}, level_hi{nobj};
 
-    mark("setup");
     // one depth per step, over all meshes
     while (nbig + nsmall > 0) {
         const size_t nodes_now = (size_t)nbig + nsmall, refs_now = big_refs + small_refs;
@@ -1013,7 +1039,6 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         small_refs = T.small_refs;
     }
 
-    mark("depths");
     // node order: sizes bottom-up, places top-down, then every node written
     const uint32_t nids = T.nids;
     DBuf d_size, d_place, d_onodes, d_oprims;
@@ -1048,25 +1073,51 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     }
     k_write<<<blocks(nids, 256), 256, 0, st>>>(d_rec.as<NodeRec>(), nids, d_place.as<uint2>(), d_op.as<ObjP>(),
                                                d_pool.as<uint32_t>(), d_onodes.as<uint2>(), d_oprims.as<uint32_t>());
-    std::vector<yr_kd_node> hn(tot_nodes);
-    std::vector<uint32_t> hp(tot_prims);
-    if (tot_nodes) cudaMemcpyAsync(hn.data(), d_onodes.p, 8 * tot_nodes, cudaMemcpyDeviceToHost, st);
-    if (tot_prims) cudaMemcpyAsync(hp.data(), d_oprims.p, 4 * tot_prims, cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return YR_ERR_CUDA;
-    mark("order+d2h");
-    out.assign(nobj, KdTree());
-    for (uint32_t o = 0; o < nobj; o++) {
-        KdTree &t = out[o];
-        t.nodes.assign(hn.begin() + hop[o].nbase, hn.begin() + hop[o].nbase + rs[o].x);
-        t.prims.assign(hp.begin() + hop[o].pbase, hp.begin() + hop[o].pbase + rs[o].y);
-        std::memcpy(t.bound.a, hop[o].tb, 12);
-        std::memcpy(t.bound.g, hop[o].tb + 3, 12);
-        t.max_depth = hop[o].max_depth;
-        t.max_leaf_size = hop[o].max_leaf;
-        t.cost_ratio = hop[o].cost_ratio;
-        t.empty_bonus = hop[o].ebonus;
+    // each tree straight into its destination: yr_kdtree records for the
+    // caller, or the KdTree vectors
+    if (abi_out) {
+        for (uint32_t o = 0; o < nobj; o++) abi_out[o] = nullptr;
+        for (uint32_t o = 0; o < nobj; o++) {
+            yr_kdtree *r = new (std::nothrow) yr_kdtree;
+            if (!r) return YR_ERR_OUT_OF_MEMORY;
+            std::memset(r, 0, sizeof(*r));
+            abi_out[o] = r;
+            r->nnodes = rs[o].x;
+            r->nprims = rs[o].y;
+            r->nodes = new (std::nothrow) yr_kd_node[r->nnodes ? r->nnodes : 1];
+            r->prims = new (std::nothrow) uint32_t[r->nprims ? r->nprims : 1];
+            if (!r->nodes || !r->prims) return YR_ERR_OUT_OF_MEMORY;
+            std::memcpy(r->bound, hop[o].tb, 24);
+            r->max_depth = hop[o].max_depth;
+            r->max_leaf_size = hop[o].max_leaf;
+            r->cost_ratio = hop[o].cost_ratio;
+            r->empty_bonus = hop[o].ebonus;
+            cudaMemcpyAsync(r->nodes, d_onodes.as<uint2>() + hop[o].nbase, 8 * (size_t)rs[o].x, cudaMemcpyDeviceToHost,
+                            st);
+            if (rs[o].y)
+                cudaMemcpyAsync(r->prims, d_oprims.as<uint32_t>() + hop[o].pbase, 4 * (size_t)rs[o].y,
+                                cudaMemcpyDeviceToHost, st);
+        }
+    } else {
+        out.assign(nobj, KdTree());
+        for (uint32_t o = 0; o < nobj; o++) {
+            KdTree &t = out[o];
+            t.nodes.resize(rs[o].x);
+            t.prims.resize(rs[o].y);
+            cudaMemcpyAsync(t.nodes.data(), d_onodes.as<uint2>() + hop[o].nbase, 8 * (size_t)rs[o].x,
+                            cudaMemcpyDeviceToHost, st);
+            if (rs[o].y)
+                cudaMemcpyAsync(t.prims.data(), d_oprims.as<uint32_t>() + hop[o].pbase, 4 * (size_t)rs[o].y,
+                                cudaMemcpyDeviceToHost, st);
+            std::memcpy(t.bound.a, hop[o].tb, 12);
+            std::memcpy(t.bound.g, hop[o].tb + 3, 12);
+            t.max_depth = hop[o].max_depth;
+            t.max_leaf_size = hop[o].max_leaf;
+            t.cost_ratio = hop[o].cost_ratio;
+            t.empty_bonus = hop[o].ebonus;
+        }
     }
-    mark("trees");
+    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return YR_ERR_CUDA;
     return YR_OK;
 }
 
@@ -1086,23 +1137,19 @@ YR_API yr_status yr_kdtree_build_gpu(const yr_kdtree_mesh *meshes, uint32_t nmes
     }
     std::vector<yr::KdMesh> ms(nmeshes);
     for (uint32_t i = 0; i < nmeshes; i++) ms[i] = yr::KdMesh{meshes[i].verts, meshes[i].nverts, meshes[i].tris, meshes[i].ntris};
-    std::vector<yr::KdTree> trees;
+    std::vector<yr::KdTree> unused;
     yr_status st;
     try {
-        st = yr::build_kdtrees_gpu(ms, kp, device, trees);
+        st = yr::build_kdtrees_gpu(ms, kp, device, unused, out);
     } catch (const std::bad_alloc &) {
-        return YR_ERR_OUT_OF_MEMORY;
+        st = YR_ERR_OUT_OF_MEMORY;
     }
-    if (st != YR_OK) return st;
-    for (uint32_t i = 0; i < nmeshes; i++) {
-        st = yr::export_tree(trees[i], &out[i]);
-        if (st != YR_OK) {
-            for (uint32_t j = 0; j < nmeshes; j++) {
-                yr_kdtree_free(out[j]);
-                out[j] = nullptr;
-            }
-            return st;
+    if (st != YR_OK) {
+        for (uint32_t j = 0; j < nmeshes; j++) {
+            yr_kdtree_free(out[j]);
+            out[j] = nullptr;
         }
+        return st;
     }
     return YR_OK;
 }
