@@ -556,12 +556,13 @@ __global__ void __launch_bounds__(kSmallThreads) k_small(const BigNode *__restri
                                                          const ObjP *__restrict__ op, KdEdge8 *__restrict__ edge_scratch,
                                                          float *__restrict__ clip_scratch, BigNode *__restrict__ small_next,
                                                          uint32_t *__restrict__ small_next_refs, uint32_t *__restrict__ pool,
-                                                         NodeRec *__restrict__ rec, Totals *__restrict__ tot) {
+                                                         NodeRec *__restrict__ rec, Totals *__restrict__ tot,
+                                                         const uint32_t *__restrict__ order) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
     const KdStrided<KdEdge8> ed{edge_scratch + g, (int)T};
     const KdStrided<float> clipb{clip_scratch + g, (int)T};
     for (uint32_t k = g; k < n; k += T) {
-        const BigNode nd = nodes[k];
+        const BigNode nd = nodes[order[k]];
         const ObjP P = op[nd.obj];
         uint32_t *L = refs + nd.beg;
         uint32_t np = nd.cnt;
@@ -705,6 +706,40 @@ __global__ void __launch_bounds__(kSmallThreads) k_small(const BigNode *__restri
         c.id = id0 + 1;
         small_next[slot + 1] = c;
     }
+}
+
+// Order of the small nodes for k_small: largest lists first, so that the
+// threads of a warp get nodes of similar size (their sorts then run for
+// similar lengths) and the longest nodes start first.  Counting sort over
+// the list sizes 0..128; the order inside a size is free.
+// Lanes of a warp holding the same size share one atomic.
+__device__ __forceinline__ uint32_t size_slot(uint32_t *hist, uint32_t c) {
+    const unsigned m = __match_any_sync(__activemask(), c);
+    const int lane = (int)(threadIdx.x & 31u), leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&hist[c], (uint32_t)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+__global__ void k_size_hist(const BigNode *__restrict__ nodes, uint32_t n, uint32_t *__restrict__ hist) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) size_slot(hist, nodes[i].cnt);
+}
+
+__global__ void k_size_scan(uint32_t *__restrict__ hist) {  // one thread
+    uint32_t run = 0;
+    for (int c = (int)kPigeonThresh; c >= 0; c--) {
+        const uint32_t h = hist[c];
+        hist[c] = run;
+        run += h;
+    }
+}
+
+__global__ void k_size_scatter(const BigNode *__restrict__ nodes, uint32_t n, uint32_t *__restrict__ hist,
+                               uint32_t *__restrict__ perm) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) perm[size_slot(hist, nodes[i].cnt)] = i;
 }
 
 // ------------------------------------------------------------ node order
@@ -958,8 +993,9 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
     const size_t small_threads = (size_t)dev_sms * kSmallCtasPerSm * kSmallThreads;
     DBuf d_cur, d_next, d_refs, d_nrefs, d_small, d_small_next, d_srefs, d_srefs_next, d_pool, d_rec, d_best, d_dec,
-        d_edges, d_clip;
+        d_edges, d_clip, d_hist, d_order;
     if (!d_edges.ensure(sizeof(KdEdge8) * kEdgeCap * small_threads, 0, st) ||
+        !d_hist.ensure(4 * (kPigeonThresh + 1), 0, st) ||
         !d_clip.ensure(4 * 6 * kClipThresh * small_threads, 0, st))
         return YR_ERR_OUT_OF_MEMORY;
     uint32_t nbig = (uint32_t)hbig.size(), nsmall = (uint32_t)hsmall.size();
@@ -1012,12 +1048,18 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
                                                      d_srefs_next.as<uint32_t>(), d_pool.as<uint32_t>());
         }
         if (nsmall) {
+            if (!d_order.ensure(4 * (size_t)nsmall, 0, st)) return YR_ERR_OUT_OF_MEMORY;
+            cudaMemsetAsync(d_hist.p, 0, 4 * (kPigeonThresh + 1), st);
+            k_size_hist<<<blocks(nsmall, 256), 256, 0, st>>>(d_small.as<BigNode>(), nsmall, d_hist.as<uint32_t>());
+            k_size_scan<<<1, 1, 0, st>>>(d_hist.as<uint32_t>());
+            k_size_scatter<<<blocks(nsmall, 256), 256, 0, st>>>(d_small.as<BigNode>(), nsmall, d_hist.as<uint32_t>(),
+                                                                d_order.as<uint32_t>());
             const unsigned sb = std::min(blocks(nsmall, kSmallThreads), (unsigned)(dev_sms * kSmallCtasPerSm));
             k_small<<<sb, kSmallThreads, 0, st>>>(
                 d_small.as<BigNode>(), nsmall, d_srefs.as<uint32_t>(), d_bnd.as<float>(), d_verts.as<float>(),
                 d_tris.as<uint32_t>(), d_op.as<ObjP>(), d_edges.as<KdEdge8>(), d_clip.as<float>(),
                 d_small_next.as<BigNode>(), d_srefs_next.as<uint32_t>(), d_pool.as<uint32_t>(), d_rec.as<NodeRec>(),
-                d_tot.as<Totals>());
+                d_tot.as<Totals>(), d_order.as<uint32_t>());
         }
         const uint32_t nids_before = T.nids;
         int herr = 0;
