@@ -901,6 +901,24 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
             cudaStreamDestroy(s);
         }
     } sg{st};
+    // nodes of at most 128 triangles run on a second stream, beside the
+    // binned sweep of the larger ones
+    cudaStream_t st2;
+    if (cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking) != cudaSuccess) return YR_ERR_CUDA;
+    StreamGuard sg2{st2};
+    cudaEvent_t ev_go, ev_done;
+    if (cudaEventCreateWithFlags(&ev_go, cudaEventDisableTiming) != cudaSuccess) return YR_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventDestroy(ev_go);
+        return YR_ERR_CUDA;
+    }
+    struct EventGuard {
+        cudaEvent_t a, b;
+        ~EventGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } eg{ev_go, ev_done};
 
     // inputs: all meshes concatenated, vertex indices made global
     std::vector<float> hv(3 * nv);
@@ -1028,8 +1046,11 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
             !d_small_next.ensure(sizeof(BigNode) * 2 * nodes_now, 0, st) ||
             !d_srefs_next.ensure(4 * 2 * refs_now, 0, st))
             return YR_ERR_OUT_OF_MEMORY;
+        if (nsmall && !d_order.ensure(4 * (size_t)nsmall, 0, st)) return YR_ERR_OUT_OF_MEMORY;
         T.nnext = T.next_refs = T.nsmall = T.small_refs = 0;
         cudaMemcpyAsync(d_tot.p, &T, sizeof(T), cudaMemcpyHostToDevice, st);
+        cudaEventRecord(ev_go, st);
+        cudaStreamWaitEvent(st2, ev_go, 0);
         if (nbig) {
             if (!d_best.ensure(sizeof(AxisBest) * 3 * (size_t)nbig, 0, st) ||
                 !d_dec.ensure(sizeof(Decision) * (size_t)nbig, 0, st) ||
@@ -1048,19 +1069,20 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
                                                      d_srefs_next.as<uint32_t>(), d_pool.as<uint32_t>());
         }
         if (nsmall) {
-            if (!d_order.ensure(4 * (size_t)nsmall, 0, st)) return YR_ERR_OUT_OF_MEMORY;
-            cudaMemsetAsync(d_hist.p, 0, 4 * (kPigeonThresh + 1), st);
-            k_size_hist<<<blocks(nsmall, 256), 256, 0, st>>>(d_small.as<BigNode>(), nsmall, d_hist.as<uint32_t>());
-            k_size_scan<<<1, 1, 0, st>>>(d_hist.as<uint32_t>());
-            k_size_scatter<<<blocks(nsmall, 256), 256, 0, st>>>(d_small.as<BigNode>(), nsmall, d_hist.as<uint32_t>(),
-                                                                d_order.as<uint32_t>());
+            cudaMemsetAsync(d_hist.p, 0, 4 * (kPigeonThresh + 1), st2);
+            k_size_hist<<<blocks(nsmall, 256), 256, 0, st2>>>(d_small.as<BigNode>(), nsmall, d_hist.as<uint32_t>());
+            k_size_scan<<<1, 1, 0, st2>>>(d_hist.as<uint32_t>());
+            k_size_scatter<<<blocks(nsmall, 256), 256, 0, st2>>>(d_small.as<BigNode>(), nsmall, d_hist.as<uint32_t>(),
+                                                                 d_order.as<uint32_t>());
             const unsigned sb = std::min(blocks(nsmall, kSmallThreads), (unsigned)(dev_sms * kSmallCtasPerSm));
-            k_small<<<sb, kSmallThreads, 0, st>>>(
+            k_small<<<sb, kSmallThreads, 0, st2>>>(
                 d_small.as<BigNode>(), nsmall, d_srefs.as<uint32_t>(), d_bnd.as<float>(), d_verts.as<float>(),
                 d_tris.as<uint32_t>(), d_op.as<ObjP>(), d_edges.as<KdEdge8>(), d_clip.as<float>(),
                 d_small_next.as<BigNode>(), d_srefs_next.as<uint32_t>(), d_pool.as<uint32_t>(), d_rec.as<NodeRec>(),
                 d_tot.as<Totals>(), d_order.as<uint32_t>());
         }
+        cudaEventRecord(ev_done, st2);
+        cudaStreamWaitEvent(st, ev_done, 0);
         const uint32_t nids_before = T.nids;
         int herr = 0;
         cudaMemcpyAsync(&T, d_tot.p, sizeof(T), cudaMemcpyDeviceToHost, st);
