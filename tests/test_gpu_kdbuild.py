@@ -146,3 +146,22 @@ def test_gpu_kdtree_rejects_non_finite():
     arr[0].ntris = 1
     outs = (C.POINTER(abi.YrKdTree) * 1)()
     assert lib.yr_kdtree_build_gpu(arr, 1, None, 0, outs) == 1
+
+
+def test_scene_gpu_kd_build_with_instances_and_many_objects():
+    """Instances share their original's GPU-built tree; a scene of many
+    meshes of every size class renders as with host-built trees."""
+    rng = np.random.default_rng(12)
+    sc = scenes.config_small(96, 72)
+    sv, st = scenes.uv_sphere((0.0, 0.0, 0.0), 0.6, rings=24, segments=48)
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    sc.meshes = [scenes.Mesh(sv, st, 0), scenes.Mesh(pv, pt, 0),
+                 scenes.instance(0, scenes.transform(translate=(1.2, 0.1, 0.3), rotate_deg=(0, 30, 0)))]
+    for n in (1, 7, 40, 129, 600):
+        m = _soup(rng, n, 1.5, 0.2)
+        m.verts = (m.verts + np.array([0.0, 0.5, -2.0], np.float32)).astype(np.float32)
+        sc.meshes.append(m)
+    img0 = api.DeviceScene(sc).render()
+    sc.render.flags |= abi.YR_RENDER_GPU_KD_BUILD
+    img1 = api.DeviceScene(sc).render()
+    assert np.array_equal(img0.view(np.uint32), img1.view(np.uint32))

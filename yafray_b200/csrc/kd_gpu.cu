@@ -17,7 +17,7 @@
 //
 // Exactness.  The bin bookkeeping of the binned sweep depends on the order
 // in which a bin sees its edges (a flat triangle above the bin's current
-// split value moves it without flushing the counters), so each round of
+// split value moves it without flushing the counters), so each batch of
 // 512 triangles sorts its 1024 edge events by (bin, event index) and the
 // first thread of each bin's run applies them in list order.  Costs are
 // the host build's float expressions (the shipped build's -ffast-math
@@ -48,7 +48,7 @@ constexpr int kBins = 1024;             // KD_BINS (kdtree.cc:17)
 constexpr uint32_t kClipThresh = 32;    // TRI_CLIP_THRESH (kdtree.cc:16)
 constexpr uint32_t kPigeonThresh = 128;
 constexpr int kBinThreads = 512;        // one CTA per (node, axis)
-constexpr int kChunk = 512;             // triangles per binning round
+constexpr int kChunk = 512;             // triangles per binning batch
 constexpr int kEvents = 2 * kChunk;     // lower and upper edge of each
 constexpr int kPartThreads = 1024;
 constexpr int kScanThreads = 1024;
