@@ -197,116 +197,55 @@ __global__ void k_obj_bounds(const float *__restrict__ bnd, const ObjP *__restri
     }
 }
 
-// ------------------------------------------------ phase A: binned sweep
-// One CTA per (node, axis): the bins of kdTree_t::pigeonMinCost filled in
-// list order, then the sweep over the 1025 bins.
-__global__ void __launch_bounds__(kBinThreads) k_bin(const BigNode *__restrict__ nodes, const uint32_t *__restrict__ refs,
-                                                     const float *__restrict__ bnd, const ObjP *__restrict__ op,
-                                                     AxisBest *__restrict__ best, int *__restrict__ err) {
-    __shared__ float bt[kBins + 1];
-    __shared__ int bn[kBins + 1], bcl[kBins + 1], bcr[kBins + 1], bcb[kBins + 1], bcbl[kBins + 1];
-    __shared__ uint32_t key[kEvents];
-    __shared__ float epos[kEvents];
-    __shared__ uint8_t eflat[kChunk];
-    __shared__ uint32_t scan_smem[2 * 32];
-    __shared__ float red_c[kBinThreads / 32];
-    __shared__ int red_i[kBinThreads / 32];
+// One edge event of kdTree_t::pigeonMinCost's bin bookkeeping
+// (kdtree.cc:191-240) on bin b; kind 0 lower edge, 1 flat triangle, 2 upper
+// edge.  The result depends on the order of a bin's events.
+__device__ __forceinline__ void bin_apply(uint32_t b, float x, int kind, float *bt, int *bn, int *bcl, int *bcr,
+                                          int *bcb, int *bcbl) {
+    if (kind == 1) {
+        if (bn[b] == 0 || x >= bt[b]) {
+            bt[b] = x;
+            bcb[b]++;
+        } else {
+            bcl[b]++;
+            bcr[b]++;
+        }
+        bn[b] += 2;
+    } else if (kind == 0) {
+        if (bn[b] == 0 || x > bt[b]) {
+            bt[b] = x;
+            bcl[b] += bcb[b] + bcbl[b];
+            bcr[b] += bcb[b];
+            bcb[b] = bcbl[b] = 0;
+            bcbl[b]++;
+        } else if (x == bt[b]) {
+            bcbl[b]++;
+        } else {
+            bcl[b]++;
+        }
+        bn[b]++;
+    } else {
+        bcr[b]++;
+        if (bn[b] == 0 || x > bt[b]) {
+            bt[b] = x;
+            bcl[b] += bcb[b] + bcbl[b];
+            bcr[b] += bcb[b];
+            bcb[b] = bcbl[b] = 0;
+        }
+        bn[b]++;
+    }
+}
 
-    const uint32_t node = blockIdx.x / 3;
-    const int axis = blockIdx.x % 3;
-    const BigNode nd = nodes[node];
-    const ObjP P = op[nd.obj];
-    AxisBest *outp = best + blockIdx.x;
-    if (nd.cnt <= (uint32_t)P.max_leaf || (int)nd.depth >= P.max_depth) {
-        if (threadIdx.x == 0) *outp = AxisBest{0.f, 0.f, 0, 0};
-        return;
-    }
+// The sweep over the 1025 bins of kdTree_t::pigeonMinCost (kdtree.cc:
+// 243-300) by a CTA of kBinThreads: thread t owns bins [3t, 3t+3); the
+// earliest bin of the lowest cost goes to *outp.
+__device__ void bin_sweep(const BigNode &nd, const ObjP &P, int axis, const float *bt, const int *bn, const int *bcl,
+                          const int *bcr, const int *bcb, const int *bcbl, uint32_t *scan_smem, float *red_c,
+                          int *red_i, AxisBest *outp, int *err) {
     const int tid = threadIdx.x;
-    for (int b = tid; b <= kBins; b += kBinThreads) {
-        bt[b] = 0.f;
-        bn[b] = bcl[b] = bcr[b] = bcb[b] = bcbl[b] = 0;
-    }
-    const float d[3] = {nd.nb[3] - nd.nb[0], nd.nb[4] - nd.nb[1], nd.nb[5] - nd.nb[2]};
-    const float s = kBins / d[axis];
-    const float lo = nd.nb[axis], hi = nd.nb[3 + axis];
     const uint32_t np = nd.cnt;
-    __syncthreads();
-    for (uint32_t c0 = 0; c0 < np; c0 += kChunk) {
-        uint32_t k0 = kNone, k1 = kNone;
-        if (c0 + tid < np) {
-            const uint32_t p = refs[nd.beg + c0 + tid];
-            const float tl = bnd[6 * (size_t)p + axis], tu = bnd[6 * (size_t)p + 3 + axis];
-            int bl = (int)((tl - lo) * s), br = (int)((tu - lo) * s);
-            bl = bl < 0 ? 0 : (bl > kBins ? kBins : bl);
-            br = br < 0 ? 0 : (br > kBins ? kBins : br);
-            epos[2 * tid] = tl;
-            epos[2 * tid + 1] = tu;
-            const bool flat = tl == tu;
-            eflat[tid] = flat;
-            k0 = ((uint32_t)bl << 11) | (uint32_t)(2 * tid);
-            if (!flat) k1 = ((uint32_t)br << 11) | (uint32_t)(2 * tid + 1);
-        }
-        key[2 * tid] = k0;
-        key[2 * tid + 1] = k1;
-        __syncthreads();
-        // bitonic sort of the 1024 keys (unique: the event index is part of the key)
-        for (int k = 2; k <= kEvents; k <<= 1)
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                const int i = 2 * tid - (tid & (j - 1));
-                const int l = i + j;
-                const uint32_t a = key[i], b = key[l];
-                if ((a > b) == ((i & k) == 0)) {
-                    key[i] = b;
-                    key[l] = a;
-                }
-                __syncthreads();
-            }
-        // the first event of each bin's run applies the run in list order
-        for (int q = tid; q < kEvents; q += kBinThreads) {
-            const uint32_t kq = key[q];
-            if (kq == kNone) continue;
-            const uint32_t b = kq >> 11;
-            if (q > 0 && (key[q - 1] >> 11) == b) continue;
-            for (int m = q; m < kEvents && key[m] != kNone && (key[m] >> 11) == b; m++) {
-                const uint32_t ev = key[m] & 2047u;
-                const float x = epos[ev];
-                if (eflat[ev >> 1]) {
-                    if (bn[b] == 0 || x >= bt[b]) {
-                        bt[b] = x;
-                        bcb[b]++;
-                    } else {
-                        bcl[b]++;
-                        bcr[b]++;
-                    }
-                    bn[b] += 2;
-                } else if ((ev & 1u) == 0) {  // lower edge
-                    if (bn[b] == 0 || x > bt[b]) {
-                        bt[b] = x;
-                        bcl[b] += bcb[b] + bcbl[b];
-                        bcr[b] += bcb[b];
-                        bcb[b] = bcbl[b] = 0;
-                        bcbl[b]++;
-                    } else if (x == bt[b]) {
-                        bcbl[b]++;
-                    } else {
-                        bcl[b]++;
-                    }
-                    bn[b]++;
-                } else {  // upper edge
-                    bcr[b]++;
-                    if (bn[b] == 0 || x > bt[b]) {
-                        bt[b] = x;
-                        bcl[b] += bcb[b] + bcbl[b];
-                        bcr[b] += bcb[b];
-                        bcb[b] = bcbl[b] = 0;
-                    }
-                    bn[b]++;
-                }
-            }
-        }
-        __syncthreads();
-    }
-    // sweep: thread t owns bins [3t, 3t+3)
+    const float d[3] = {nd.nb[3] - nd.nb[0], nd.nb[4] - nd.nb[1], nd.nb[5] - nd.nb[2]};
+    const float lo = nd.nb[axis], hi = nd.nb[3 + axis];
     const int b0 = 3 * tid, b1 = min(b0 + 3, kBins + 1);
     uint32_t v[2] = {0u, 0u}, tot[2];
     for (int b = b0; b < b1; b++) {
@@ -369,6 +308,247 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(const BigNode *__restrict__
         const bool found = bi <= kBins && bc < __int_as_float(0x7f800000);
         *outp = AxisBest{bc, found ? bt[bi] : 0.f, found ? 1 : 0, 0};
     }
+}
+
+// ------------------------------------------------ phase A: binned sweep
+// One CTA per (node, axis): the bins of kdTree_t::pigeonMinCost filled in
+// list order, then the sweep over the 1025 bins.
+__global__ void __launch_bounds__(kBinThreads) k_bin(const BigNode *__restrict__ nodes, const uint32_t *__restrict__ refs,
+                                                     const float *__restrict__ bnd, const ObjP *__restrict__ op,
+                                                     AxisBest *__restrict__ best, int *__restrict__ err) {
+    __shared__ float bt[kBins + 1];
+    __shared__ int bn[kBins + 1], bcl[kBins + 1], bcr[kBins + 1], bcb[kBins + 1], bcbl[kBins + 1];
+    __shared__ uint32_t key[kEvents];
+    __shared__ float epos[kEvents];
+    __shared__ uint8_t eflat[kChunk];
+    __shared__ uint32_t scan_smem[2 * 32];
+    __shared__ float red_c[kBinThreads / 32];
+    __shared__ int red_i[kBinThreads / 32];
+
+    const uint32_t node = blockIdx.x / 3;
+    const int axis = blockIdx.x % 3;
+    const BigNode nd = nodes[node];
+    const ObjP P = op[nd.obj];
+    AxisBest *outp = best + blockIdx.x;
+    if (nd.cnt <= (uint32_t)P.max_leaf || (int)nd.depth >= P.max_depth) {
+        if (threadIdx.x == 0) *outp = AxisBest{0.f, 0.f, 0, 0};
+        return;
+    }
+    const int tid = threadIdx.x;
+    for (int b = tid; b <= kBins; b += kBinThreads) {
+        bt[b] = 0.f;
+        bn[b] = bcl[b] = bcr[b] = bcb[b] = bcbl[b] = 0;
+    }
+    const float d[3] = {nd.nb[3] - nd.nb[0], nd.nb[4] - nd.nb[1], nd.nb[5] - nd.nb[2]};
+    const float s = kBins / d[axis];
+    const float lo = nd.nb[axis];
+    const uint32_t np = nd.cnt;
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < np; c0 += kChunk) {
+        uint32_t k0 = kNone, k1 = kNone;
+        if (c0 + tid < np) {
+            const uint32_t p = refs[nd.beg + c0 + tid];
+            const float tl = bnd[6 * (size_t)p + axis], tu = bnd[6 * (size_t)p + 3 + axis];
+            int bl = (int)((tl - lo) * s), br = (int)((tu - lo) * s);
+            bl = bl < 0 ? 0 : (bl > kBins ? kBins : bl);
+            br = br < 0 ? 0 : (br > kBins ? kBins : br);
+            epos[2 * tid] = tl;
+            epos[2 * tid + 1] = tu;
+            const bool flat = tl == tu;
+            eflat[tid] = flat;
+            k0 = ((uint32_t)bl << 11) | (uint32_t)(2 * tid);
+            if (!flat) k1 = ((uint32_t)br << 11) | (uint32_t)(2 * tid + 1);
+        }
+        key[2 * tid] = k0;
+        key[2 * tid + 1] = k1;
+        __syncthreads();
+        // bitonic sort of the 1024 keys (unique: the event index is part of the key)
+        for (int k = 2; k <= kEvents; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const int i = 2 * tid - (tid & (j - 1));
+                const int l = i + j;
+                const uint32_t a = key[i], b = key[l];
+                if ((a > b) == ((i & k) == 0)) {
+                    key[i] = b;
+                    key[l] = a;
+                }
+                __syncthreads();
+            }
+        // the first event of each bin's run applies the run in list order
+        for (int q = tid; q < kEvents; q += kBinThreads) {
+            const uint32_t kq = key[q];
+            if (kq == kNone) continue;
+            const uint32_t b = kq >> 11;
+            if (q > 0 && (key[q - 1] >> 11) == b) continue;
+            for (int m = q; m < kEvents && key[m] != kNone && (key[m] >> 11) == b; m++) {
+                const uint32_t ev = key[m] & 2047u;
+                bin_apply(b, epos[ev], eflat[ev >> 1] ? 1 : (int)(ev & 1u) * 2, bt, bn, bcl, bcr, bcb, bcbl);
+            }
+        }
+        __syncthreads();
+    }
+    bin_sweep(nd, P, axis, bt, bn, bcl, bcr, bcb, bcbl, scan_smem, red_c, red_i, outp, err);
+}
+
+// The same binned sweep for a depth with few large nodes, spread over all
+// SMs: every 512-triangle batch of every (node, axis) sorts its events by
+// (bin, event index) in its own CTA (k_wide_sort), the per-batch bin counts
+// give every event its place in bin-major, list order (k_wide_offsets,
+// k_wide_scatter), and one thread per bin applies its events in that order
+// (k_wide_apply) before the usual sweep.
+struct WideBatch {
+    uint32_t node, axis, c0;  // node, axis, first list position of the batch
+    uint32_t row;             // this batch's row in the count / offset tables
+};
+
+struct WideSet {  // one (node, axis)
+    uint32_t row0, nrows;     // its batches' rows
+    uint32_t ev0;             // first of its events in the event array
+    uint32_t pad;
+};
+
+__global__ void __launch_bounds__(kBinThreads) k_wide_sort(const WideBatch *__restrict__ batches,
+                                                           const BigNode *__restrict__ nodes,
+                                                           const uint32_t *__restrict__ refs, const float *__restrict__ bnd,
+                                                           uint32_t *__restrict__ hist, uint2 *__restrict__ sorted) {
+    __shared__ uint32_t key[kEvents];
+    __shared__ float epos[kEvents];
+    const WideBatch W = batches[blockIdx.x];
+    const BigNode nd = nodes[W.node];
+    const int axis = (int)W.axis, tid = threadIdx.x;
+    const float d = nd.nb[3 + axis] - nd.nb[axis];
+    const float s = kBins / d, lo = nd.nb[axis];
+    uint32_t k0 = kNone, k1 = kNone;
+    if (W.c0 + tid < nd.cnt) {  // as k_bin
+        const uint32_t p = refs[nd.beg + W.c0 + tid];
+        const float tl = bnd[6 * (size_t)p + axis], tu = bnd[6 * (size_t)p + 3 + axis];
+        int bl = (int)((tl - lo) * s), br = (int)((tu - lo) * s);
+        bl = bl < 0 ? 0 : (bl > kBins ? kBins : bl);
+        br = br < 0 ? 0 : (br > kBins ? kBins : br);
+        epos[2 * tid] = tl;
+        epos[2 * tid + 1] = tu;
+        const bool flat = tl == tu;
+        k0 = ((uint32_t)bl << 11) | (uint32_t)(2 * tid) | (flat ? 0x80000000u : 0u);
+        if (!flat) k1 = ((uint32_t)br << 11) | (uint32_t)(2 * tid + 1);
+    }
+    key[2 * tid] = k0;
+    key[2 * tid + 1] = k1;
+    __syncthreads();
+    for (int k = 2; k <= kEvents; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int i = 2 * tid - (tid & (j - 1));
+            const int l = i + j;
+            const uint32_t a = key[i], b = key[l];
+            // the flat flag (bit 31) does not take part in the order
+            if (((a & 0x7fffffffu) > (b & 0x7fffffffu) || (a == kNone && b != kNone)) == ((i & k) == 0)) {
+                key[i] = b;
+                key[l] = a;
+            }
+            __syncthreads();
+        }
+    for (int q = tid; q < kEvents; q += kBinThreads) {
+        const uint32_t kq = key[q];
+        sorted[(size_t)W.row * kEvents + q] = make_uint2(kq, kq == kNone ? 0u : __float_as_uint(epos[kq & 2047u]));
+        if (kq == kNone) continue;
+        const uint32_t b = (kq & 0x7fffffffu) >> 11;
+        if (q > 0 && key[q - 1] != kNone && ((key[q - 1] & 0x7fffffffu) >> 11) == b) continue;
+        int m = q;
+        while (m < kEvents && key[m] != kNone && ((key[m] & 0x7fffffffu) >> 11) == b) m++;
+        hist[(size_t)W.row * (kBins + 1) + b] = (uint32_t)(m - q);
+    }
+}
+
+// Per (node, axis): where each bin's events start (bin-major) and each
+// batch's place inside each bin (offsets, same layout as the counts).
+__global__ void __launch_bounds__(1024) k_wide_offsets(const WideSet *__restrict__ sets, const uint32_t *__restrict__ hist,
+                                                       uint32_t *__restrict__ offs, uint32_t *__restrict__ bin_start) {
+    __shared__ uint32_t smem[32];
+    const WideSet S = sets[blockIdx.x];
+    const int t = threadIdx.x;
+    uint32_t tot1024 = 0;
+    uint32_t v[1] = {0u}, sum[1];
+    for (uint32_t r = 0; r < S.nrows; r++) {
+        v[0] += hist[(size_t)(S.row0 + r) * (kBins + 1) + t];
+        if (t == 0) tot1024 += hist[(size_t)(S.row0 + r) * (kBins + 1) + kBins];
+    }
+    block_scan<1024, 1>(v, sum, smem);
+    uint32_t run = v[0];  // bins 0..1023 in order, bin 1024 last
+    uint32_t run1024 = sum[0];
+    for (uint32_t r = 0; r < S.nrows; r++) {
+        const size_t at = (size_t)(S.row0 + r) * (kBins + 1);
+        offs[at + t] = run;
+        run += hist[at + t];
+        if (t == 0) {
+            offs[at + kBins] = run1024;
+            run1024 += hist[at + kBins];
+        }
+    }
+    bin_start[(size_t)blockIdx.x * (kBins + 2) + t] = v[0];
+    if (t == 0) {
+        bin_start[(size_t)blockIdx.x * (kBins + 2) + kBins] = sum[0];
+        bin_start[(size_t)blockIdx.x * (kBins + 2) + kBins + 1] = sum[0] + tot1024;
+    }
+}
+
+__global__ void __launch_bounds__(kBinThreads) k_wide_scatter(const WideBatch *__restrict__ batches,
+                                                              const WideSet *__restrict__ sets,
+                                                              const uint2 *__restrict__ sorted,
+                                                              const uint32_t *__restrict__ offs, uint2 *__restrict__ events) {
+    __shared__ uint32_t key[kEvents];
+    __shared__ int run_start[kBins + 1];
+    const WideBatch W = batches[blockIdx.x];
+    const WideSet S = sets[3 * W.node + W.axis];
+    const int tid = threadIdx.x;
+    for (int q = tid; q < kEvents; q += kBinThreads) key[q] = sorted[(size_t)W.row * kEvents + q].x;
+    __syncthreads();
+    for (int q = tid; q < kEvents; q += kBinThreads) {
+        const uint32_t kq = key[q];
+        if (kq == kNone) continue;
+        const uint32_t b = (kq & 0x7fffffffu) >> 11;
+        if (q == 0 || key[q - 1] == kNone || ((key[q - 1] & 0x7fffffffu) >> 11) != b) run_start[b] = q;
+    }
+    __syncthreads();
+    for (int q = tid; q < kEvents; q += kBinThreads) {
+        const uint2 e = sorted[(size_t)W.row * kEvents + q];
+        if (e.x == kNone) continue;
+        const uint32_t b = (e.x & 0x7fffffffu) >> 11;
+        const uint32_t ev = e.x & 2047u;
+        const uint32_t kind = (e.x & 0x80000000u) ? 1u : (ev & 1u) * 2u;
+        const uint32_t dst = offs[(size_t)W.row * (kBins + 1) + b] + (uint32_t)(q - run_start[b]);
+        events[S.ev0 + dst] = make_uint2(e.y, (b << 2) | kind);
+    }
+}
+
+__global__ void __launch_bounds__(kBinThreads) k_wide_apply(const BigNode *__restrict__ nodes, const WideSet *__restrict__ sets,
+                                                            const uint32_t *__restrict__ bin_start,
+                                                            const uint2 *__restrict__ events, const ObjP *__restrict__ op,
+                                                            AxisBest *__restrict__ best, int *__restrict__ err) {
+    __shared__ float bt[kBins + 1];
+    __shared__ int bn[kBins + 1], bcl[kBins + 1], bcr[kBins + 1], bcb[kBins + 1], bcbl[kBins + 1];
+    __shared__ uint32_t scan_smem[2 * 32];
+    __shared__ float red_c[kBinThreads / 32];
+    __shared__ int red_i[kBinThreads / 32];
+    const uint32_t node = blockIdx.x / 3;
+    const int axis = blockIdx.x % 3;
+    const BigNode nd = nodes[node];
+    const ObjP P = op[nd.obj];
+    AxisBest *outp = best + blockIdx.x;
+    if (nd.cnt <= (uint32_t)P.max_leaf || (int)nd.depth >= P.max_depth) {
+        if (threadIdx.x == 0) *outp = AxisBest{0.f, 0.f, 0, 0};
+        return;
+    }
+    const WideSet S = sets[blockIdx.x];
+    const uint32_t *bs = bin_start + (size_t)blockIdx.x * (kBins + 2);
+    for (int b = threadIdx.x; b <= kBins; b += kBinThreads) {
+        bt[b] = 0.f;
+        bn[b] = bcl[b] = bcr[b] = bcb[b] = bcbl[b] = 0;
+        for (uint32_t i = bs[b]; i < bs[b + 1]; i++) {
+            const uint2 e = events[S.ev0 + i];
+            bin_apply((uint32_t)b, __uint_as_float(e.x), (int)(e.y & 3u), bt, bn, bcl, bcr, bcb, bcbl);
+        }
+    }
+    __syncthreads();
+    bin_sweep(nd, P, axis, bt, bn, bcl, bcr, bcb, bcbl, scan_smem, red_c, red_i, outp, err);
 }
 
 // Split or leaf per node (kdTree_t::buildTree, kdtree.cc:416-520): the best
@@ -1011,7 +1191,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
     const size_t small_threads = (size_t)dev_sms * kSmallCtasPerSm * kSmallThreads;
     DBuf d_cur, d_next, d_refs, d_nrefs, d_small, d_small_next, d_srefs, d_srefs_next, d_pool, d_rec, d_best, d_dec,
-        d_edges, d_clip, d_hist, d_order;
+        d_edges, d_clip, d_hist, d_order, d_wbatch, d_wset, d_whist, d_woffs, d_wsorted, d_wstart, d_wevents;
     if (!d_edges.ensure(sizeof(KdEdge8) * kEdgeCap * small_threads, 0, st) ||
         !d_hist.ensure(4 * (kPigeonThresh + 1), 0, st) ||
         !d_clip.ensure(4 * 6 * kClipThresh * small_threads, 0, st))
@@ -1056,8 +1236,51 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
                 !d_dec.ensure(sizeof(Decision) * (size_t)nbig, 0, st) ||
                 !d_next.ensure(sizeof(BigNode) * 2 * (size_t)nbig, 0, st) || !d_nrefs.ensure(4 * 2 * big_refs, 0, st))
                 return YR_ERR_OUT_OF_MEMORY;
-            k_bin<<<3 * nbig, kBinThreads, 0, st>>>(d_cur.as<BigNode>(), d_refs.as<uint32_t>(), d_bnd.as<float>(),
-                                                   d_op.as<ObjP>(), d_best.as<AxisBest>(), d_err.as<int>());
+            if (big_refs > (size_t)nbig * 8 * kChunk) {
+                // large nodes (above 8 batches on average): spread each
+                // node's binning over many CTAs
+                std::vector<BigNode> hb(nbig);
+                cudaMemcpyAsync(hb.data(), d_cur.p, sizeof(BigNode) * nbig, cudaMemcpyDeviceToHost, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess) return YR_ERR_CUDA;
+                std::vector<WideBatch> wb;
+                std::vector<WideSet> ws(3 * (size_t)nbig);
+                uint32_t rows = 0, evs = 0;
+                for (uint32_t j = 0; j < nbig; j++)
+                    for (uint32_t a = 0; a < 3; a++) {
+                        WideSet &S = ws[3 * j + a];
+                        S.row0 = rows;
+                        S.nrows = (hb[j].cnt + kChunk - 1) / kChunk;
+                        S.ev0 = evs;
+                        S.pad = 0;
+                        for (uint32_t r = 0; r < S.nrows; r++) wb.push_back(WideBatch{j, a, r * (uint32_t)kChunk, rows + r});
+                        rows += S.nrows;
+                        evs += 2 * hb[j].cnt;
+                    }
+                if (!d_wbatch.ensure(sizeof(WideBatch) * wb.size(), 0, st) ||
+                    !d_wset.ensure(sizeof(WideSet) * ws.size(), 0, st) ||
+                    !d_whist.ensure(4 * (size_t)rows * (kBins + 1), 0, st) ||
+                    !d_woffs.ensure(4 * (size_t)rows * (kBins + 1), 0, st) ||
+                    !d_wsorted.ensure(8 * (size_t)rows * kEvents, 0, st) ||
+                    !d_wstart.ensure(4 * ws.size() * (kBins + 2), 0, st) || !d_wevents.ensure(8 * (size_t)evs, 0, st))
+                    return YR_ERR_OUT_OF_MEMORY;
+                cudaMemcpyAsync(d_wbatch.p, wb.data(), sizeof(WideBatch) * wb.size(), cudaMemcpyHostToDevice, st);
+                cudaMemcpyAsync(d_wset.p, ws.data(), sizeof(WideSet) * ws.size(), cudaMemcpyHostToDevice, st);
+                cudaMemsetAsync(d_whist.p, 0, 4 * (size_t)rows * (kBins + 1), st);
+                k_wide_sort<<<rows, kBinThreads, 0, st>>>(d_wbatch.as<WideBatch>(), d_cur.as<BigNode>(),
+                                                          d_refs.as<uint32_t>(), d_bnd.as<float>(), d_whist.as<uint32_t>(),
+                                                          d_wsorted.as<uint2>());
+                k_wide_offsets<<<3 * nbig, 1024, 0, st>>>(d_wset.as<WideSet>(), d_whist.as<uint32_t>(),
+                                                          d_woffs.as<uint32_t>(), d_wstart.as<uint32_t>());
+                k_wide_scatter<<<rows, kBinThreads, 0, st>>>(d_wbatch.as<WideBatch>(), d_wset.as<WideSet>(),
+                                                             d_wsorted.as<uint2>(), d_woffs.as<uint32_t>(),
+                                                             d_wevents.as<uint2>());
+                k_wide_apply<<<3 * nbig, kBinThreads, 0, st>>>(d_cur.as<BigNode>(), d_wset.as<WideSet>(),
+                                                               d_wstart.as<uint32_t>(), d_wevents.as<uint2>(),
+                                                               d_op.as<ObjP>(), d_best.as<AxisBest>(), d_err.as<int>());
+            } else {
+                k_bin<<<3 * nbig, kBinThreads, 0, st>>>(d_cur.as<BigNode>(), d_refs.as<uint32_t>(), d_bnd.as<float>(),
+                                                       d_op.as<ObjP>(), d_best.as<AxisBest>(), d_err.as<int>());
+            }
             k_decide<<<blocks(nbig, 128), 128, 0, st>>>(d_cur.as<BigNode>(), nbig, d_best.as<AxisBest>(),
                                                         d_op.as<ObjP>(), d_dec.as<Decision>());
             k_count<<<nbig, kPartThreads, 0, st>>>(d_cur.as<BigNode>(), d_refs.as<uint32_t>(), d_bnd.as<float>(),
