@@ -1212,6 +1212,12 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         cudaMemcpyAsync(d_srefs.p, hsrefs.data(), 4 * small_refs, cudaMemcpyHostToDevice, st);
     }
     cudaMemcpyAsync(d_op.p, hop.data(), sizeof(ObjP) * nobj, cudaMemcpyHostToDevice, st);
+    // node records and leaf lists grow with every depth; reserve for a
+    // typical tree (about 2 nodes and 2.5 leaf entries per triangle) so
+    // that they rarely move
+    if (!d_rec.ensure(sizeof(NodeRec) * (2 * nt + 2 * (size_t)nobj + 16), 0, st) ||
+        !d_pool.ensure(4 * (3 * nt + 16), 0, st))
+        return YR_ERR_OUT_OF_MEMORY;
     Totals T{};
     T.nids = nobj;
     std::vector<uint32_t> level_lo{0}, level_hi{nobj};
@@ -1256,12 +1262,15 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
                         rows += S.nrows;
                         evs += 2 * hb[j].cnt;
                     }
-                if (!d_wbatch.ensure(sizeof(WideBatch) * wb.size(), 0, st) ||
-                    !d_wset.ensure(sizeof(WideSet) * ws.size(), 0, st) ||
-                    !d_whist.ensure(4 * (size_t)rows * (kBins + 1), 0, st) ||
-                    !d_woffs.ensure(4 * (size_t)rows * (kBins + 1), 0, st) ||
-                    !d_wsorted.ensure(8 * (size_t)rows * kEvents, 0, st) ||
-                    !d_wstart.ensure(4 * ws.size() * (kBins + 2), 0, st) || !d_wevents.ensure(8 * (size_t)evs, 0, st))
+                // twice the need: the next depths' lists are longer (straddling
+                // triangles), and each regrowth is a free and a new allocation
+                if (!d_wbatch.ensure(2 * sizeof(WideBatch) * wb.size(), 0, st) ||
+                    !d_wset.ensure(2 * sizeof(WideSet) * ws.size(), 0, st) ||
+                    !d_whist.ensure(2 * 4 * (size_t)rows * (kBins + 1), 0, st) ||
+                    !d_woffs.ensure(2 * 4 * (size_t)rows * (kBins + 1), 0, st) ||
+                    !d_wsorted.ensure(2 * 8 * (size_t)rows * kEvents, 0, st) ||
+                    !d_wstart.ensure(2 * 4 * ws.size() * (kBins + 2), 0, st) ||
+                    !d_wevents.ensure(2 * 8 * (size_t)evs, 0, st))
                     return YR_ERR_OUT_OF_MEMORY;
                 cudaMemcpyAsync(d_wbatch.p, wb.data(), sizeof(WideBatch) * wb.size(), cudaMemcpyHostToDevice, st);
                 cudaMemcpyAsync(d_wset.p, ws.data(), sizeof(WideSet) * ws.size(), cudaMemcpyHostToDevice, st);
