@@ -1212,12 +1212,6 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         cudaMemcpyAsync(d_srefs.p, hsrefs.data(), 4 * small_refs, cudaMemcpyHostToDevice, st);
     }
     cudaMemcpyAsync(d_op.p, hop.data(), sizeof(ObjP) * nobj, cudaMemcpyHostToDevice, st);
-    // node records and leaf lists grow with every depth; reserve for a
-    // typical tree (about 2 nodes and 2.5 leaf entries per triangle) so
-    // that they rarely move
-    if (!d_rec.ensure(sizeof(NodeRec) * (2 * nt + 2 * (size_t)nobj + 16), 0, st) ||
-        !d_pool.ensure(4 * (3 * nt + 16), 0, st))
-        return YR_ERR_OUT_OF_MEMORY;
     Totals T{};
     T.nids = nobj;
     std::vector<uint32_t> level_lo{0}, level_hi{nobj};
