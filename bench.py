@@ -103,41 +103,68 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- CPU legs
-def reference_render(sc, threads, rows, reps, timeout=900):
-    """Run the unmodified reference (oracle/_ref) on full-width rows [0, rows)
-    of the frame; returns per-render dicts (render_s, primary, shadow, bounce)."""
+BLOCK = 64  # threadedscene_t's block size (blockSpliter_t(resx, resy, 64))
+
+
+def sample_blocks(sc, cores, target_s=15.0):
+    """A stratified sample of the frame's 64x64 blocks for the CPU timing:
+    the first distinct blocks of the R2 low-discrepancy sequence over the
+    block grid (spread over the whole frame), about `target_s` seconds of
+    work for `cores` threads (~0.9 Mrays/s per core, ~74 rays per camera
+    sample on the large frame), at least one block per thread."""
+    bw, bh = (sc.resx + BLOCK - 1) // BLOCK, (sc.resy + BLOCK - 1) // BLOCK
+    spp = max(1, sc.render.spp)
+    rays_per_block = BLOCK * BLOCK * spp * 74.0
+    n = int(target_s * cores * 0.9e6 / rays_per_block)
+    n = max(min(cores, bw * bh), min(n, bw * bh))
+    a1, a2 = 0.7548776662466927, 0.5698402909980532   # R2 sequence (plastic number)
+    seen, out, k = set(), [], 0
+    while len(out) < n:
+        bx = int(((0.5 + k * a1) % 1.0) * bw)
+        by = int(((0.5 + k * a2) % 1.0) * bh)
+        k += 1
+        if (bx, by) not in seen:
+            seen.add((bx, by))
+            out.append((bx, by))
+    return out
+
+
+def reference_blocks(sc, threads, blocks, reps, timeout=1800):
+    """Run the unmodified reference (oracle/_ref) on the listed 64x64 blocks
+    with `threads` workers (threadedscene_t's worker loop over the block
+    list); returns per-render dicts (render_s, primary, shadow, bounce)."""
     with tempfile.TemporaryDirectory() as d:
         sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "o.bin")
         scenes.write_yrs(sc, sp)
-        cmd = [HARNESS, "render", sp, op, str(threads), "0", str(sc.resx), "0", str(rows), str(reps)]
+        spec = ",".join(f"{bx}.{by}" for bx, by in blocks)
+        cmd = [HARNESS, "render_blocks", sp, op, str(threads), spec, str(reps)]
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(r.stderr[-2000:])
         return [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
 
 
-def cpu_sample_rows(sc, threads):
-    """Full-width band sized for ~10 s of wall time on `threads` cores
-    (~1000 px/s per core at 16 spp); at least one 64-pixel block row."""
-    spp = max(1, sc.render.spp)
-    px = 10.0 * 1000.0 * threads * 16.0 / spp
-    rows = int(min(sc.resy, max(64, px / sc.resx)))
-    return rows
+def sample_text(sc, blocks, thr, res):
+    nb = ((sc.resx + BLOCK - 1) // BLOCK) * ((sc.resy + BLOCK - 1) // BLOCK)
+    rps = (res["shadow"] + res["bounce"] + res["primary"]) / max(1, res["primary"])
+    return (f"unmodified reference, {thr} worker threads running threadedscene_t's per-block render "
+            f"(scene_t::render(renderArea_t&)) over {len(blocks)} of the frame's {nb} 64x64 blocks "
+            f"({100.0 * len(blocks) / nb:.1f}% of the frame, stratified by the R2 sequence over the block grid, "
+            f"{sc.render.spp} spp, {rps:.1f} rays per camera sample); rays counted at "
+            f"scene_t::isShadowed/firstHit + camera rays in per-thread counters; render phase timed, kd build "
+            f"excluded")
 
 
 def cpu_baseline(sc):
     threads = host_cores()
     if os.path.exists(HARNESS):
-        # threadedscene_t aborts when threads exceed the 64x64 blocks that hold work
-        rows = cpu_sample_rows(sc, threads)
-        blocks = ((sc.resx + 63) // 64) * ((rows + 63) // 64)
-        thr = max(1, min(threads, blocks))
-        res = reference_render(sc, thr, rows, 1)[-1]
+        blocks = sample_blocks(sc, threads)
+        res = reference_blocks(sc, threads, blocks, 1)[-1]
         rays = res["primary"] + res["shadow"] + res["bounce"]
-        return {"value": rays / res["render_s"] / 1e6, "unit": METRIC, "cores": thr, "kind": "reference",
-                "sample": f"unmodified reference (threadedscene_t, {thr} threads) on rows 0-{rows} of the frame "
-                          f"({sc.resx}x{rows} px x {sc.render.spp} spp, {rays:,} rays counted at "
-                          f"scene_t::isShadowed/firstHit + camera rays), render phase only; kd build excluded"}
+        return {"value": rays / res["render_s"] / 1e6, "unit": METRIC, "cores": threads, "kind": "reference",
+                "sample": sample_text(sc, blocks, threads, res),
+                "blocks": [list(b) for b in blocks],
+                "rays_per_sample": rays / max(1, res["primary"])}
     import yrtest as T
     O = T.OracleScene(sc)
     t0 = time.perf_counter()
@@ -157,23 +184,19 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/yr_ref_harness was not built"}))
         return
     threads = host_cores()
-    rows = cpu_sample_rows(sc, threads)
-    blocks = ((sc.resx + 63) // 64) * ((rows + 63) // 64)
-    thr = max(1, min(threads, blocks))
-    res = reference_render(sc, thr, rows, args.warmup + args.steps, timeout=1800)
+    blocks = sample_blocks(sc, threads, target_s=10.0)
+    res = reference_blocks(sc, threads, blocks, args.warmup + args.steps)
     timed = res[args.warmup:]
     rays = sum(r["primary"] + r["shadow"] + r["bounce"] for r in timed)
     secs = sum(r["render_s"] for r in timed)
     value = rays / secs / 1e6
-    sample = (f"unmodified reference (threadedscene_t, {thr} threads) rendering rows 0-{rows} of the frame "
-              f"per step ({sc.resx}x{rows} px x {sc.render.spp} spp); rays counted at scene_t::isShadowed/firstHit "
-              f"+ camera rays; render phase timed, kd build excluded")
+    sample = sample_text(sc, blocks, threads, timed[-1])
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * secs / max(1, len(timed)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": name, "sample_rows": rows},
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": thr, "kind": "reference", "sample": sample},
+        "config": {"workload": name, "sample_blocks": len(blocks)},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

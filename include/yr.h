@@ -403,6 +403,18 @@ YR_API yr_status yr_scene_info_get(const yr_scene *scene, yr_scene_info *info);
  * (used by the inverse-rendering loop). */
 YR_API yr_status yr_scene_set_params(yr_scene *scene, const yr_shader_desc *shaders,
                                      const yr_light_desc *lights);
+/* Set the camera from a constructed camera_t's own vectors instead of its
+ * constructor arguments (a host that holds a camera_t, as a scene_t
+ * subclass does with render_camera, has no look / up points to give):
+ * position, vto, vup, vright as camera_t's constructor leaves them
+ * (camera.cc:27-87, CM_PERSPECTIVE); camera rays are then
+ * normalize(vto + vright*px + vup*py) from pos (camera_t::shootRay,
+ * camera.cc:184-188).  The resolution stays yr_camera_desc's.  Replaces
+ * the camera yr_scene_create derived from yr_camera_desc; call it before
+ * rendering (batched renders captured earlier keep the old camera, so they
+ * are re-captured). */
+YR_API yr_status yr_scene_set_camera_vectors(yr_scene *scene, const float *pos, const float *vto,
+                                             const float *vup, const float *vright);
 
 /* ------------------------------------------------------------------------
  * Ray queries (device pointers, asynchronous on `stream`).
@@ -494,11 +506,13 @@ YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
                            yr_render_stats *stats, void *stream);
 
 /* yr_render for callers that cannot allocate GPU memory at render time -
- * for example a host that runs inside a memory pool it does not own, or a
- * plugin that may not call cudaMalloc while the application holds a
- * capture or a custom allocator.  It renders the same image as yr_render
- * but draws its scratch from one fixed 64 MiB block that every GPU loading
- * this library holds until the process exits, instead of allocating.
+ * for example a renderer plugin loaded into an application that owns all
+ * of the GPU's memory through its own allocator and forbids its plugins to
+ * call cudaMalloc / cudaFree, or a host that has reserved every byte of the
+ * device for itself before the render starts.  It renders the same image
+ * as yr_render but draws its scratch from one fixed 64 MiB block that every
+ * GPU loading this library holds until the process exits, instead of
+ * allocating.
  * (No counterpart in the reference: YafRay renders on the CPU.)
  *   - `rgba` is a device pointer (resx*resy*4 floats); nothing is staged.
  *   - The render runs in as many passes as the block needs; a render whose
@@ -511,7 +525,9 @@ YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
  *     calls that overlap on the GPU (different streams or threads) race and
  *     must be serialized by the caller.
  *   - No CUDA events are created: stats->ms and the kernel times stay 0;
- *     the ray counts are filled in. */
+ *     the ray counts are filled in.
+ *   - Like yr_render, the call waits for `stream` before it returns (it
+ *     reads the render's device status word back). */
 YR_API yr_status yr_render_noalloc(yr_scene *scene, float *rgba, yr_render_stats *stats, void *stream);
 
 /* Render `count` independent scenes (one device) as one launch.  Two

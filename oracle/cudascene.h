@@ -1,0 +1,47 @@
+// cudascene_t: a YafRay 0.0.9 scene class whose render(colorOutput_t&)
+// renders through the B200 library (include/yr.h) instead of the CPU
+// block loop.  This is the class a YafRay maintainer adds to yafraycore
+// (yafraycore/cudascene.{h,cc}) to make the library a drop-in: the loader
+// picks it where it picks threadedscene_t (loader/render.cc:1131-1153,
+// interface_impl.cc:562,755), everything that fills the scene (objects,
+// lights, shaders, camera, render settings) stays as it is.
+//
+// Built here against the reference's headers as they are (no access
+// changes) and linked with the reference's objects and libyafray_b200.so,
+// as test infrastructure: oracle/Makefile's yr_ref_cudascene renders a
+// scene built from the reference's own objects through this class.
+#ifndef YR_CUDASCENE_H
+#define YR_CUDASCENE_H
+
+#include "scene.h"
+
+extern "C" {
+#include "../include/yr.h"
+}
+
+__BEGIN_YAFRAY
+
+class cudascene_t : public scene_t {
+  public:
+    explicit cudascene_t(int device = 0) : handle(0), dev(device), status(YR_OK) {}
+    virtual ~cudascene_t();
+    // scene_t::render(colorOutput_t&) (scene.h:136): the frame through
+    // yr_render, pixels handed to the output with colorOutput_t::putPixel
+    // (output.h:36-38) as renderArea_t::out does (renderblock.cc:8-20).
+    // A scene the library cannot take, or a device error, leaves the output
+    // untouched and is reported by lastStatus(); nothing falls back to the
+    // CPU renderer.
+    virtual void render(colorOutput_t &out);
+    yr_status lastStatus() const { return status; }
+    static scene_t *factory(int device = 0) { return new cudascene_t(device); }
+
+  private:
+    yr_status capture();  // the scene's objects, lights and camera -> yr_scene
+    yr_scene *handle;
+    int dev;
+    yr_status status;
+};
+
+__END_YAFRAY
+
+#endif

@@ -9,6 +9,13 @@
 //   yr_ref_harness rays    SCENE RAYS OUT      kd / scene ray queries
 //   yr_ref_harness camera  SCENE OUT           primary ray directions
 //   yr_ref_harness instmat SCENE OUT           each reference's M^-1 (back)
+//   yr_ref_cudascene cudarender SCENE OUT [x0 x1 y0 y1]
+//                                              the scene through cudascene_t (the
+//                                              library), a build of this file
+//                                              with YR_HARNESS_CUDASCENE
+//   yr_ref_harness render_blocks SCENE OUT THREADS BLOCKS [REPEATS]
+//                                              listed 64x64 blocks of the frame,
+//                                              threadedscene_t's worker loop
 //   yr_ref_harness render  SCENE OUT THREADS [x0 x1 y0 y1 [REPEATS]]
 //                                              stock scene_t::render, float sink,
 //                                              ray counts, one JSON line per render
@@ -46,16 +53,22 @@
 #include "basictex.h"
 #include "targaIO.h"
 #include "HDR_io.h"
+#ifdef YR_HARNESS_CUDASCENE
+#include "cudascene.h"
+#endif
 #undef private
 #undef protected
 
+#include <pthread.h>
 #include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <sys/time.h>
+#include <algorithm>
 #include <map>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -76,13 +89,49 @@ noiseGenerator_t *newNoise(const std::string &ntype);
 // Ray counters: the reference has none (mesh.cc:409-412 are unused), so
 // the calls that plugins make into scene_t::isShadowed / firstHit are
 // counted through link-time wrappers (-Wl,--wrap in oracle/Makefile).
-static volatile long g_shadow_rays = 0, g_bounce_rays = 0;
+// Each thread counts in its own counter record (registered on its first
+// count, one cache line each), so the timed render shares no counter cache
+// line between threads; a render's totals are the sum over the records
+// once its threads are done.
+struct RayCounter {
+    long shadow, bounce;
+    char pad[64 - 2 * sizeof(long)];
+} __attribute__((aligned(64)));
+static __thread RayCounter *t_ctr = NULL;
+static std::vector<RayCounter *> g_ctrs;
+static pthread_mutex_t g_ctr_mu = PTHREAD_MUTEX_INITIALIZER;
+static RayCounter *my_counter() {
+    if (!t_ctr) {
+        void *mem = NULL;
+        if (posix_memalign(&mem, 64, sizeof(RayCounter)) != 0) abort();
+        t_ctr = new (mem) RayCounter();
+        t_ctr->shadow = t_ctr->bounce = 0;
+        pthread_mutex_lock(&g_ctr_mu);
+        g_ctrs.push_back(t_ctr);
+        pthread_mutex_unlock(&g_ctr_mu);
+    }
+    return t_ctr;
+}
+static void counts_reset() {
+    pthread_mutex_lock(&g_ctr_mu);
+    for (size_t i = 0; i < g_ctrs.size(); i++) g_ctrs[i]->shadow = g_ctrs[i]->bounce = 0;
+    pthread_mutex_unlock(&g_ctr_mu);
+}
+static void counts_sum(long &shadow, long &bounce) {
+    shadow = bounce = 0;
+    pthread_mutex_lock(&g_ctr_mu);
+    for (size_t i = 0; i < g_ctrs.size(); i++) {
+        shadow += g_ctrs[i]->shadow;
+        bounce += g_ctrs[i]->bounce;
+    }
+    pthread_mutex_unlock(&g_ctr_mu);
+}
 extern "C" {
 bool __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_9point3d_tE(
     const scene_t *, renderState_t &, const surfacePoint_t &, const point3d_t &);
 bool __wrap__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_9point3d_tE(
     const scene_t *s, renderState_t &st, const surfacePoint_t &sp, const point3d_t &l) {
-    __sync_fetch_and_add(&g_shadow_rays, 1);
+    ++my_counter()->shadow;
     return __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_9point3d_tE(s, st, sp,
                                                                                                            l);
 }
@@ -90,7 +139,7 @@ bool __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePo
     const scene_t *, renderState_t &, const surfacePoint_t &, const vector3d_t &);
 bool __wrap__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_10vector3d_tE(
     const scene_t *s, renderState_t &st, const surfacePoint_t &sp, const vector3d_t &d) {
-    __sync_fetch_and_add(&g_shadow_rays, 1);
+    ++my_counter()->shadow;
     return __real__ZNK6yafray7scene_t10isShadowedERNS_13renderState_tERKNS_14surfacePoint_tERKNS_10vector3d_tE(s, st,
                                                                                                             sp, d);
 }
@@ -98,7 +147,7 @@ bool __real__ZNK6yafray7scene_t8firstHitERNS_13renderState_tERNS_14surfacePoint_
     const scene_t *, renderState_t &, surfacePoint_t &, const point3d_t &, const vector3d_t &, bool);
 bool __wrap__ZNK6yafray7scene_t8firstHitERNS_13renderState_tERNS_14surfacePoint_tERKNS_9point3d_tERKNS_10vector3d_tEb(
     const scene_t *s, renderState_t &st, surfacePoint_t &sp, const point3d_t &p, const vector3d_t &r, bool sh) {
-    __sync_fetch_and_add(&g_bounce_rays, 1);
+    ++my_counter()->bounce;
     return __real__ZNK6yafray7scene_t8firstHitERNS_13renderState_tERNS_14surfacePoint_tERKNS_9point3d_tERKNS_10vector3d_tEb(
         s, st, sp, p, r, sh);
 }
@@ -324,8 +373,10 @@ class constBg_t : public background_t {
     color_t color;
 };
 
-static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true) {
-    r.scene = scene_t::factory();
+// `scene`: the scene object to fill (a derived scene class); NULL = a new
+// plain scene_t
+static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true, scene_t *scene = NULL) {
+    r.scene = scene ? scene : scene_t::factory();
     for (size_t i = 0; i < s.shaders.size(); i++) r.shaders.push_back(make_shader(s.shaders[i], r.textures));
     for (size_t i = 0; i < s.objs.size(); i++) {
         const SceneFile::Obj &o = s.objs[i];
@@ -638,18 +689,148 @@ static void cmd_render(const SceneFile &s, const char *out, int threads, const i
     floatSink_t sink(s.cam.resx, s.cam.resy);
     // repeated renders share one scene (and one kd-tree build); each prints a line
     for (int rep = 0; rep < reps; rep++) {
-        g_shadow_rays = g_bounce_rays = 0;
+        counts_reset();
         double t0 = now_s();
         sc->render(sink);
         double t1 = now_s();
+        long nsh = 0, nbo = 0;
+        counts_sum(nsh, nbo);
         printf("{\"render_s\": %.6f, \"threads\": %d, \"primary\": %ld, \"shadow\": %ld, \"bounce\": %ld}\n",
-               t1 - t0, threads, region_px * (long)spp, (long)g_shadow_rays, (long)g_bounce_rays);
+               t1 - t0, threads, region_px * (long)spp, nsh, nbo);
         fflush(stdout);
     }
     FILE *f = fopen(out, "wb");
     wr(f, &sink.img[0], 4 * sink.img.size());
     fclose(f);
 }
+
+// ---------------------------------------------------------- render blocks
+// CPU timing on a stratified sample of the frame.  threadedscene_t renders
+// a frame as 64x64 blocks (blockSpliter_t, renderblock.cc:71-101: each
+// block's area carries a one-pixel border on its inner sides) that worker
+// threads take one at a time and pass to the scene's own per-area render,
+// scene_t::render(renderArea_t&) (threadedscene.cc:77-95).  This command
+// runs that worker loop over a chosen list of those blocks instead of all of
+// them, so that a sample spread over the whole frame can be timed on every
+// host core (threadedscene_t refuses more threads than blocks of its region).
+class blockScene_t : public scene_t {
+  public:
+    blockScene_t() {}
+    // what scene_t::render(colorOutput_t&) and threadedscene_t::render do
+    // before the first block (scene.cc:555; threadedscene.cc:110-116)
+    void prepare() {
+        BTree = buildObjectTree(obj_list);
+        setupLights();
+    }
+    void release() {
+        delete BTree;
+        BTree = NULL;
+    }
+};
+
+struct BlockRun {
+    const blockScene_t *scene;
+    std::vector<renderArea_t> *areas;
+    colorOutput_t *out;
+    long next;
+};
+
+static void *block_worker(void *arg) {
+    BlockRun *R = (BlockRun *)arg;
+    for (;;) {
+        const long k = __sync_fetch_and_add(&R->next, 1L);
+        if (k >= (long)R->areas->size()) break;
+        renderArea_t &a = (*R->areas)[k];
+        R->scene->render(a);
+        a.out(*R->out);  // blocks write disjoint real regions
+    }
+    return NULL;
+}
+
+// blocks: "bx.by,bx.by,..." in 64-pixel block units
+static void cmd_render_blocks(const SceneFile &s, const char *out, int threads, const char *blocks, int reps) {
+    RefScene r;
+    blockScene_t *bs = new blockScene_t();
+    build_ref(s, r, true, bs);
+    const uint32_t spp = s.rp.spp ? s.rp.spp : 1;
+    bs->setAASamples(spp > 1 ? 1 : 0, spp > 1 ? (int)spp - 1 : 1, s.rp.aa_pixelwidth, 0.0, false);
+    const int W = s.cam.resx, H = s.cam.resy, B = 64;
+    std::vector<renderArea_t> areas;
+    long traced_px = 0;
+    for (const char *q = blocks; *q;) {
+        int bx = 0, by = 0, used = 0;
+        if (sscanf(q, "%d.%d%n", &bx, &by, &used) != 2) die("bad block list");
+        q += used;
+        if (*q == ',') q++;
+        const int rx = bx * B, ry = by * B;
+        if (rx < 0 || ry < 0 || rx >= W || ry >= H) die("block outside the frame");
+        // blockSpliter_t's area of this block (renderblock.cc:84-97)
+        int x = rx, y = ry, w = std::min(B, W - rx), h = std::min(B, H - ry);
+        const int rw = w, rh = h;
+        if (x > 0) { x--; w++; }
+        if (y > 0) { y--; h++; }
+        if (x + w < W - 1) w++;
+        if (y + h < H - 1) h++;
+        renderArea_t a;
+        a.set(x, y, w, h);
+        a.setReal(rx, ry, rw, rh);
+        areas.push_back(a);
+        traced_px += (long)w * h;
+    }
+    if (threads < 1) threads = 1;
+    floatSink_t sink(W, H);
+    bs->prepare();
+    for (int rep = 0; rep < reps; rep++) {
+        counts_reset();
+        BlockRun R = {bs, &areas, &sink, 0};
+        std::vector<pthread_t> th(threads);
+        double t0 = now_s();
+        for (int i = 0; i < threads; i++) pthread_create(&th[i], NULL, block_worker, &R);
+        for (int i = 0; i < threads; i++) pthread_join(th[i], NULL);
+        double t1 = now_s();
+        long nsh = 0, nbo = 0;
+        counts_sum(nsh, nbo);
+        printf("{\"render_s\": %.6f, \"threads\": %d, \"blocks\": %d, \"primary\": %ld, \"shadow\": %ld, "
+               "\"bounce\": %ld}\n",
+               t1 - t0, threads, (int)areas.size(), traced_px * (long)spp, nsh, nbo);
+        fflush(stdout);
+    }
+    bs->release();
+    FILE *f = fopen(out, "wb");
+    wr(f, &sink.img[0], 4 * sink.img.size());
+    fclose(f);
+}
+
+#ifdef YR_HARNESS_CUDASCENE
+// ------------------------------------------------------------ cudarender
+// The drop-in: the same scene built from the reference's own objects
+// (meshObject_t, genericShader_t, pointLight_t, camera_t) into a
+// cudascene_t, rendered by cudascene_t::render - the library, through
+// yr_render - into the float sink.  One JSON line: the library's status
+// and the render time.
+static void cmd_cudarender(const SceneFile &s, const char *out, const int *crop) {
+    RefScene r;
+    cudascene_t *cs = new cudascene_t(0);
+    build_ref(s, r, true, cs);
+    const uint32_t spp = s.rp.spp ? s.rp.spp : 1;
+    cs->setAASamples(spp > 1 ? 1 : 0, spp > 1 ? (int)spp - 1 : 1, s.rp.aa_pixelwidth, 0.0, false);
+    if (crop) {
+        PFLOAT rx = (PFLOAT)s.cam.resx, ry = (PFLOAT)s.cam.resy;
+        cs->setRegion(2.0 * crop[0] / rx - 1.0, 2.0 * crop[1] / rx - 1.0, 1.0 - 2.0 * crop[3] / ry,
+                      1.0 - 2.0 * crop[2] / ry);
+    }
+    floatSink_t sink(s.cam.resx, s.cam.resy);
+    double t0 = now_s();
+    cs->render(sink);
+    double t1 = now_s();
+    printf("{\"status\": %d, \"render_s\": %.6f}\n", (int)cs->lastStatus(), t1 - t0);
+    fflush(stdout);
+    FILE *f = fopen(out, "wb");
+    wr(f, &sink.img[0], 4 * sink.img.size());
+    fclose(f);
+    delete cs;
+}
+#endif
 
 // ------------------------------------------------------------- illuminate
 // One light's illuminate() at the first hit of a ray, with the light's
@@ -928,6 +1109,19 @@ int main(int argc, char **argv) {
             for (int k = 0; k < 4; k++) crop[k] = atoi(argv[5 + k]);
         const int reps = argc >= 10 ? atoi(argv[9]) : 1;
         cmd_render(s, argv[3], atoi(argv[4]), has_crop ? crop : NULL, reps < 1 ? 1 : reps);
+#ifdef YR_HARNESS_CUDASCENE
+    } else if (cmd == "cudarender") {
+        if (argc < 4) die("cudarender SCENE OUT [x0 x1 y0 y1]");
+        int crop[4];
+        const bool has_crop = argc >= 8;
+        if (has_crop)
+            for (int k = 0; k < 4; k++) crop[k] = atoi(argv[4 + k]);
+        cmd_cudarender(s, argv[3], has_crop ? crop : NULL);
+#endif
+    } else if (cmd == "render_blocks") {
+        if (argc < 6) die("render_blocks SCENE OUT THREADS BLOCKS [REPEATS]");
+        const int reps = argc >= 7 ? atoi(argv[6]) : 1;
+        cmd_render_blocks(s, argv[3], atoi(argv[4]), argv[5], reps < 1 ? 1 : reps);
     } else {
         die("unknown command");
     }

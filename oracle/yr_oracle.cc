@@ -86,6 +86,24 @@ C operator*(float f, const C &a) { return C(f * a.r, f * a.g, f * a.b); }
 C operator/(const C &a, float f) { return C(a.r / f, a.g / f, a.b / f); }
 float energy(const C &c) { return (c.r + c.g + c.b) * 0.333333f; }  // color.h:67
 
+// The estimators' energy cut-offs: a path stops when its colour's energy
+// falls below 0.05 (pathlight.cc:315), a shading point whose diffuse
+// colour's energy is below 0.05 gets no path light (pathlight.cc:398), and
+// a hemi light skips a point whose fromLight(N, 1) has every channel below
+// 0.05 (hemilight.cc:67).  A few ulps of difference in the value decide
+// these branches when it lies at the threshold.  For the tests, a render
+// can record, per pixel, the smallest relative distance of any such value
+// from the threshold, and can take the other branch of every decision whose
+// value lies within a relative band of it (orc_render_ex).
+thread_local float t_flip_band = 0.f;   // 0: every decision as computed
+thread_local float t_min_margin = 1e30f;
+bool below_cut(float e) {
+    const float m = fabsf(e - 0.05f) / 0.05f;
+    if (m < t_min_margin) t_min_margin = m;
+    const bool b = e < 0.05f;
+    return (t_flip_band > 0.f && m <= t_flip_band) ? !b : b;
+}
+
 struct Box {
     float a[3], g[3];
 };
@@ -93,7 +111,11 @@ struct Box {
 struct Stats {
     uint64_t primary, shadow, bounce, nodes, tests, boxes, roots;
 };
-Stats *g_stats = NULL;  // the scene being traced (for the slab-test counter)
+// Counters of the calling thread: several threads may trace or render
+// disjoint pixel sets of one loaded scene at once (the scene is read-only
+// while tracing); each entry point reports its own thread's counts.
+thread_local Stats t_st;
+thread_local Stats *g_stats = NULL;  // the counters the slab test adds to (NULL: not counting)
 
 // bound_t::cross(from, ray, enter, leave, dist), shipped (fast-math) form (bound.cc:389-436)
 bool cross_el(const Box &b, const V &from, const V &ray, float dist, float &enter, float &leave) {
@@ -238,7 +260,6 @@ struct Scene {
     std::vector<Light> lights;
     Cam cam;
     yr_render_params rp;
-    Stats st;
     // orc_illum only: Cranley-Patterson rotation off, and the area lights'
     // random values given from outside (2 per sample) instead of Halton
     bool no_rot = false;
@@ -269,7 +290,7 @@ struct KdStackE {
 // kdTree_t::Intersect (kdtree.cc:591-727) if !any, IntersectS (kdtree.cc:730-866) if any
 bool kd_intersect(Scene &S, const Obj &o, const V &from, const V &ray, float dist, uint32_t &tr, float &Z, bool any) {
     float a, b, t;
-    S.st.roots++;
+    t_st.roots++;
     if (!cross_el(o.tb, from, ray, dist, a, b)) return false;
     const V invDir(1.f / ray.x, 1.f / ray.y, 1.f / ray.z);
     bool hit = false;
@@ -287,7 +308,7 @@ bool kd_intersect(Scene &S, const Obj &o, const V &from, const V &ray, float dis
     while (curr != kNull) {
         if (dist < stack[enPt].t) break;
         while ((o.nodes[curr].flags & 3u) != 3u) {
-            S.st.nodes++;
+            t_st.nodes++;
             const int axis = (int)(o.nodes[curr].flags & 3u);
             float split;
             memcpy(&split, &o.nodes[curr].word, 4);
@@ -328,11 +349,11 @@ bool kd_intersect(Scene &S, const Obj &o, const V &from, const V &ray, float dis
             stack[exPt].pb[nextAxis] = from[nextAxis] + t * ray[nextAxis];
             stack[exPt].pb[prevAxis] = from[prevAxis] + t * ray[prevAxis];
         }
-        S.st.nodes++;
+        t_st.nodes++;
         const uint32_t np = o.nodes[curr].flags >> 2;
         for (uint32_t k = 0; k < np; k++) {
             const uint32_t ti = (np == 1) ? o.nodes[curr].word : o.prims[o.nodes[curr].word + k];
-            S.st.tests++;
+            t_st.tests++;
             float rt;
             if (tri_hit(o, ti, from, ray, rt)) {
                 if (any) {
@@ -466,7 +487,7 @@ bool shadowed(Scene &S, const V &p, int own, const V &ray, float dist) {
 }
 
 bool shadowed_point(Scene &S, const V &p, int own, const V &l) {
-    S.st.shadow++;
+    t_st.shadow++;
     V ray = l - p;
     float dist = length(ray);
     ray = normalize(ray);
@@ -474,7 +495,7 @@ bool shadowed_point(Scene &S, const V &p, int own, const V &l) {
 }
 
 bool shadowed_dir(Scene &S, const V &p, int own, const V &dir) {
-    S.st.shadow++;
+    t_st.shadow++;
     return shadowed(S, p, own, normalize(dir), kInf);
 }
 
@@ -1280,7 +1301,7 @@ C illum_hemi(Scene &S, int k, const Light &L, const SP &sp, const V &eye, int v,
     float mad = fabsf(fl.r);
     if (fabsf(fl.g) > mad) mad = fabsf(fl.g);
     if (fabsf(fl.b) > mad) mad = fabsf(fl.b);
-    if (mad < 0.05f) return C();
+    if (below_cut(mad)) return C();
     const uint32_t d = light_dim(k, v);
     const float r0 = rot(S, cx.pixel, d), r1 = rot(S, cx.pixel, d + 1);
     C total;
@@ -1312,7 +1333,7 @@ C light_sum(Scene &S, const SP &sp, const V &eye, bool indirect, int v, uint32_t
 C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx) {
     V N = faceForward(sp.Ng, sp.N, eye);
     C dif = diffuse(S, sp);
-    if (energy(dif) < 0.05f) return C();
+    if (below_cut(energy(dif))) return C();
     const int P = L.d.samples, depth = L.d.depth;
     C total;
     for (int i = 0; i < P; i++) {
@@ -1324,8 +1345,8 @@ C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx
         C raycolor(1, 1, 1);
         const float startN = startray * N;
         for (int j = 0; j < depth; ++j) {
-            if (energy(raycolor) < 0.05f) break;
-            S.st.bounce++;
+            if (below_cut(energy(raycolor))) break;
+            t_st.bounce++;
             const V f = where + ray * kMinRay;
             Hit h = closest(S, f, ray, false, true);
             if (h.obj < 0) {
@@ -1436,7 +1457,7 @@ void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
         fy = (float)(0.5 + (double)S.rp.aa_pixelwidth * ((double)((float)c * tsd) - 0.5));
     }
     const V ray = shoot(S.cam, (float)x + fx, (float)y + fy);
-    S.st.primary++;
+    t_st.primary++;
     if (S.rp.raydepth <= 0) {
         rgba[0] = rgba[1] = rgba[2] = rgba[3] = 0.f;
         tonemap_sample(S, rgba);
@@ -1647,7 +1668,7 @@ orc_scene *orc_load(const char *path) {
         }
         S.lights.push_back(L);
     }
-    memset(&S.st, 0, sizeof(S.st));
+    memset(&t_st, 0, sizeof(t_st));
     return o;
 }
 
@@ -1685,13 +1706,13 @@ void orc_trace_closest(orc_scene *o, const float *rays, uint32_t n, uint32_t *hi
     for (uint32_t i = 0; i < n; i++) {
         const float *r = rays + 8 * (size_t)i;
         const V org(r[0], r[1], r[2]), dir(r[4], r[5], r[6]);
-        const uint64_t n0 = o->s.st.nodes;
+        const uint64_t n0 = t_st.nodes;
         Hit h = closest(o->s, org + dir * kMinRay, dir, false, shadow_only != 0);
         float t = h.obj >= 0 ? h.Z : 0.f;
         memcpy(&hits[4 * i], &t, 4);
         hits[4 * i + 1] = h.obj >= 0 ? (uint32_t)h.obj : 0xffffffffu;
         hits[4 * i + 2] = h.obj >= 0 ? h.tri : 0xffffffffu;
-        hits[4 * i + 3] = (uint32_t)(o->s.st.nodes - n0);
+        hits[4 * i + 3] = (uint32_t)(t_st.nodes - n0);
     }
 }
 
@@ -1711,7 +1732,7 @@ void orc_trace_shadow(orc_scene *o, const float *rays, uint32_t n, uint8_t *occ)
 // Kd traversal of one object only (kdTree_t::Intersect / IntersectS):
 // out: hit, tri, Z bits, nodes visited
 void orc_kd(orc_scene *o, uint32_t obj, const float *from, const float *dir, float dist, int any, uint32_t *out) {
-    const uint64_t n0 = o->s.st.nodes;
+    const uint64_t n0 = t_st.nodes;
     uint32_t tr = 0;
     float Z = dist < 0 ? kInf : dist;
     bool h = kd_intersect(o->s, o->s.objs[obj], V(from[0], from[1], from[2]), V(dir[0], dir[1], dir[2]),
@@ -1720,19 +1741,34 @@ void orc_kd(orc_scene *o, uint32_t obj, const float *from, const float *dir, flo
     out[1] = h ? tr : 0xffffffffu;
     float z = (h && !any) ? Z : 0.f;
     memcpy(&out[2], &z, 4);
-    out[3] = (uint32_t)(o->s.st.nodes - n0);
+    out[3] = (uint32_t)(t_st.nodes - n0);
 }
 
 // Render pixels [x0,x1) x [y0,y1) into rgba (full image layout, resx*resy*4).
 // stats: primary, shadow, bounce, nodes, tests, slab tests, kd roots tried
+// orc_render_ex: the same, taking the other branch of every energy cut-off
+// whose value lies within `flip_band` (relative) of the threshold (0: none),
+// and writing per pixel the smallest relative distance of any cut-off value
+// from the threshold into margin (full image layout, resx*resy; may be NULL).
+// Threads may render disjoint regions of one scene at once.
+void orc_render_ex(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint64_t *stats, float flip_band,
+                   float *margin);
+
 void orc_render(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint64_t *stats) {
+    orc_render_ex(o, rgba, x0, x1, y0, y1, stats, 0.f, NULL);
+}
+
+void orc_render_ex(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint64_t *stats, float flip_band,
+                   float *margin) {
     Scene &S = o->s;
     const uint32_t spp = S.rp.spp ? S.rp.spp : 1;
-    memset(&S.st, 0, sizeof(S.st));
-    g_stats = &S.st;
+    memset(&t_st, 0, sizeof(t_st));
+    g_stats = &t_st;
+    t_flip_band = flip_band;
     for (int y = y0; y < y1; y++)
         for (int x = x0; x < x1; x++) {
             const uint32_t pixel = (uint32_t)(y * S.cam.resx + x);
+            t_min_margin = 1e30f;
             float first[4], tot[4] = {0, 0, 0, 0}, c[4];
             for (uint32_t s = 0; s < spp; s++) {
                 camera_sample(S, pixel, s, c);
@@ -1749,15 +1785,17 @@ void orc_render(orc_scene *o, float *rgba, int x0, int x1, int y0, int y1, uint6
             }
             if (S.rp.flags & YR_RENDER_ALPHA_PREMULTIPLY)  // colorA_t::alphaPremultiply
                 for (int k = 0; k < 3; k++) px[k] *= px[3];
+            if (margin) margin[pixel] = t_min_margin;
         }
+    t_flip_band = 0.f;
     if (stats) {
-        stats[0] = S.st.primary;
-        stats[1] = S.st.shadow;
-        stats[2] = S.st.bounce;
-        stats[3] = S.st.nodes;
-        stats[4] = S.st.tests;
-        stats[5] = S.st.boxes;
-        stats[6] = S.st.roots;
+        stats[0] = t_st.primary;
+        stats[1] = t_st.shadow;
+        stats[2] = t_st.bounce;
+        stats[3] = t_st.nodes;
+        stats[4] = t_st.tests;
+        stats[5] = t_st.boxes;
+        stats[6] = t_st.roots;
     }
     g_stats = NULL;
 }

@@ -42,6 +42,7 @@ def oracle() -> C.CDLL:
             "orc_trace_shadow": (None, [P, P, U, P]),
             "orc_kd": (None, [P, U, P, P, F, C.c_int, P]),
             "orc_render": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P]),
+            "orc_render_ex": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P, F, P]),
             "orc_camera_rays": (None, [P, P]),
             "orc_illum": (C.c_int, [P, U, P, P, P, U, P, P]),
             "orc_noise_gen": (F, [U, F, F, F]),
@@ -200,6 +201,41 @@ class OracleScene:
         stats = np.zeros(7, np.uint64)
         self.lib.orc_render(self.h, ptr(img), x0, x1, y0, y1, ptr(stats))
         return img, stats
+
+    def render_ex(self, x0, x1, y0, y1, img=None, flip_band=0.0):
+        """Render pixels [x0,x1) x [y0,y1) into `img` (full image layout;
+        a new one when None), taking the other branch of every energy
+        cut-off within `flip_band` (relative) of its threshold.  Returns
+        (img, stats, margin): margin[y, x] = the smallest relative distance
+        of any cut-off value of the pixel from its threshold."""
+        sc = self.sc
+        if img is None:
+            img = np.zeros((sc.resy, sc.resx, 4), np.float32)
+        margin = np.full((sc.resy, sc.resx), np.inf, np.float32)
+        stats = np.zeros(7, np.uint64)
+        self.lib.orc_render_ex(self.h, ptr(img), x0, x1, y0, y1, ptr(stats), float(flip_band), ptr(margin))
+        return img, stats, margin
+
+    def render_regions(self, regions, threads=None):
+        """Render several disjoint pixel regions (x0, x1, y0, y1) on host
+        threads; returns (img, stats summed, margin)."""
+        import concurrent.futures as cf
+        sc = self.sc
+        img = np.zeros((sc.resy, sc.resx, 4), np.float32)
+        margin = np.full((sc.resy, sc.resx), np.inf, np.float32)
+        stats = np.zeros(7, np.uint64)
+
+        def one(r):
+            m = np.full((sc.resy, sc.resx), np.inf, np.float32)
+            st = np.zeros(7, np.uint64)
+            self.lib.orc_render_ex(self.h, ptr(img), r[0], r[1], r[2], r[3], ptr(st), 0.0, ptr(m))
+            return r, st, m
+
+        with cf.ThreadPoolExecutor(threads or min(len(regions), os.cpu_count() or 1)) as ex:
+            for r, st, m in ex.map(one, regions):
+                stats += st
+                margin[r[2]:r[3], r[0]:r[1]] = m[r[2]:r[3], r[0]:r[1]]
+        return img, stats, margin
 
     def camera_rays(self):
         d = np.zeros((self.sc.resy, self.sc.resx, 3), np.float32)

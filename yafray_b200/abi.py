@@ -189,6 +189,8 @@ SIGNATURES = {
     "yr_scene_destroy": (C.c_int, [_P]),
     "yr_scene_info_get": (C.c_int, [_P, C.POINTER(YrSceneInfo)]),
     "yr_scene_set_params": (C.c_int, [_P, C.POINTER(YrShaderDesc), C.POINTER(YrLightDesc)]),
+    "yr_scene_set_camera_vectors": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                              C.POINTER(C.c_float)]),
     "yr_trace_closest": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_int, _P]),
     "yr_trace_shadow": (C.c_int, [_P, _P, C.c_uint32, _P, _P]),
     "yr_render": (C.c_int, [_P, _P, C.c_int, C.POINTER(YrRenderStats), _P]),

@@ -3,6 +3,7 @@
 #pragma once
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "dev_shade.cuh"
 #include "dev_trace.cuh"
@@ -904,12 +905,20 @@ __host__ __device__ inline void assign_wave(const Plan &P, uint32_t wcap, char *
 
 // Blocks of kBlock threads that fill every SM once for `kernel` (queried
 // once per device and kernel), the grid of the traversal kernels.
+// The per-device caches below are filled under one lock: the first renders
+// on a device may come from several host threads at once.
+inline std::mutex &device_cache_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+
 template <class K>
 inline int resident_grid(K kernel) {
     static int cached[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
+    std::lock_guard<std::mutex> lock(device_cache_mutex());
     if (!cached[dev]) {
         int sms = 148, per = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -935,6 +944,7 @@ inline size_t render_budget(int sharers) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
+    std::lock_guard<std::mutex> lock(device_cache_mutex());
     if (!free_at_start[dev]) {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b == 0) free_b = 1;

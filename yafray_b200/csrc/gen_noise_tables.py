@@ -1,5 +1,10 @@
 """Write noise_tables.h from the reference's noise.cc (run where the
-reference sources are present; the header is committed).
+reference sources are present; the header is committed):
+
+    python gen_noise_tables.py <reference>/src/yafraycore/noise.cc
+
+(or with the reference's root directory in the YR_REFERENCE environment
+variable and no argument).
 
 Blender's noise tables, as yafray 0.0.9 keeps them in noise.cc:
   hashpntf[768]  feature point offsets of the voronoi / cell bases
@@ -18,7 +23,6 @@ import os
 import re
 import sys
 
-SRC = "/root/reference/src/yafraycore/noise.cc"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "noise_tables.h")
 
 
@@ -28,7 +32,12 @@ def table(src, name):
     return [t.strip() for t in body.split(",") if t.strip()]
 
 
-def main(src_path=SRC):
+def main(src_path=None):
+    if src_path is None:
+        root = os.environ.get("YR_REFERENCE")
+        if not root:
+            sys.exit("usage: gen_noise_tables.py <path of the reference's noise.cc> (or set YR_REFERENCE)")
+        src_path = os.path.join(root, "src", "yafraycore", "noise.cc")
     src = open(src_path).read()
     hp, h, hv = table(src, "hashpntf"), table(src, "hash"), table(src, "hashvectf")
     sp, sg = table(src, "stdp_p"), table(src, "stdp_g")

@@ -460,7 +460,11 @@ __global__ void __launch_bounds__(kBinThreads) k_wide_sort(const WideBatch *__re
 
 // Per (node, axis): where each bin's events start (bin-major) and each
 // batch's place inside each bin (offsets, same layout as the counts).
-__global__ void __launch_bounds__(1024) k_wide_offsets(const WideSet *__restrict__ sets, const uint32_t *__restrict__ hist,
+// One thread per bin 0..kBins-1 (bin kBins is summed beside the scan), so
+// the block is exactly kBins threads.
+constexpr int kWideOffsetThreads = 1024;
+static_assert(kBins == kWideOffsetThreads, "k_wide_offsets runs one thread per bin");
+__global__ void __launch_bounds__(kWideOffsetThreads) k_wide_offsets(const WideSet *__restrict__ sets, const uint32_t *__restrict__ hist,
                                                        uint32_t *__restrict__ offs, uint32_t *__restrict__ bin_start) {
     __shared__ uint32_t smem[32];
     const WideSet S = sets[blockIdx.x];
@@ -1272,7 +1276,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
                 k_wide_sort<<<rows, kBinThreads, 0, st>>>(d_wbatch.as<WideBatch>(), d_cur.as<BigNode>(),
                                                           d_refs.as<uint32_t>(), d_bnd.as<float>(), d_whist.as<uint32_t>(),
                                                           d_wsorted.as<uint2>());
-                k_wide_offsets<<<3 * nbig, 1024, 0, st>>>(d_wset.as<WideSet>(), d_whist.as<uint32_t>(),
+                k_wide_offsets<<<3 * nbig, kWideOffsetThreads, 0, st>>>(d_wset.as<WideSet>(), d_whist.as<uint32_t>(),
                                                           d_woffs.as<uint32_t>(), d_wstart.as<uint32_t>());
                 k_wide_scatter<<<rows, kBinThreads, 0, st>>>(d_wbatch.as<WideBatch>(), d_wset.as<WideSet>(),
                                                              d_wsorted.as<uint2>(), d_woffs.as<uint32_t>(),

@@ -241,7 +241,7 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
     if (!scene || !rgba) return YR_ERR_INVALID_ARG;
     int prev = 0;
     cudaGetDevice(&prev);
-    cudaSetDevice(scene->device);
+    if (cudaSetDevice(scene->device) != cudaSuccess) return YR_ERR_CUDA;
     cudaStream_t st = (cudaStream_t)stream;
     auto done = [&](yr_status e) {
         cudaSetDevice(prev);

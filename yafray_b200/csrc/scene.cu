@@ -875,6 +875,24 @@ YR_API yr_status yr_scene_info_get(const yr_scene *scene, yr_scene_info *info) {
     return YR_OK;
 }
 
+YR_API yr_status yr_scene_set_camera_vectors(yr_scene *scene, const float *pos, const float *vto, const float *vup,
+                                             const float *vright) {
+    if (!scene || !pos || !vto || !vup || !vright) return YR_ERR_INVALID_ARG;
+    for (int k = 0; k < 3; k++)
+        if (!std::isfinite(pos[k]) || !std::isfinite(vto[k]) || !std::isfinite(vup[k]) || !std::isfinite(vright[k]))
+            return YR_ERR_INVALID_ARG;
+    DevCamera &c = scene->rdr.cam;
+    c.pos = v3(pos[0], pos[1], pos[2]);
+    c.vto = v3(vto[0], vto[1], vto[2]);
+    c.vup = v3(vup[0], vup[1], vup[2]);
+    c.vright = v3(vright[0], vright[1], vright[2]);
+    // batched renders and adjoint steps captured before keep kernel
+    // arguments with the old camera: drop them so they are captured again
+    batch_forget(scene);
+    adj_batch_forget(scene);
+    return YR_OK;
+}
+
 YR_API yr_status yr_scene_set_params(yr_scene *scene, const yr_shader_desc *shaders, const yr_light_desc *lights) {
     if (!scene) return YR_ERR_INVALID_ARG;
     int prev = 0;
