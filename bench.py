@@ -212,15 +212,15 @@ def load_traffic():
     return {}
 
 
-def run_diff(args, api, torch, local, fd_params=16):
+def run_diff(args, api, torch, local, fd_params=16, steps=None, warmup=None):
     """Adjoint workload: the small scene at 512x512, 64 spp, 64 material
     groups (diffuse RGB + specular weight) and 8 area lights = 264
     parameters; target rendered from hidden parameters.  One step = one
     forward render + one yr_backward.  Reports the adjoint / forward time
     ratio and a check of the gradient against FP64-accumulated central
     differences (step 1e-3) on `fd_params` sampled parameters."""
-    sc = scenes.config_diff()
-    hid = scenes.config_diff(hidden=True)
+    sc = scenes.config_diff(res=args.diff_res, spp=args.diff_spp)
+    hid = scenes.config_diff(res=args.diff_res, spp=args.diff_spp, hidden=True)
     ds = api.DeviceScene(sc, device=local)
     n = ds.param_count()
     theta = ds.params_get()
@@ -230,7 +230,9 @@ def run_diff(args, api, torch, local, fd_params=16):
     dh.close()
     img = torch.empty_like(target)
     grad = torch.empty(n, dtype=torch.float32, device="cuda")
-    for _ in range(args.warmup):
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    for _ in range(warmup):
         ds.render_into(img.data_ptr())
         ds.backward(img.data_ptr(), target.data_ptr(), grad.data_ptr())
     torch.cuda.synchronize()
@@ -239,7 +241,7 @@ def run_diff(args, api, torch, local, fd_params=16):
     rays = 0
     clocks = ClockSampler(local)
     clocks.start()
-    for _ in range(args.steps):
+    for _ in range(steps):
         ev[0].record()
         st = ds.render_into(img.data_ptr())
         ev[1].record()
@@ -281,20 +283,20 @@ def run_diff(args, api, torch, local, fd_params=16):
     ds.params_set(theta)
     ds.close()
     value = rays / ((fwd_ms + bwd_ms) / 1000.0) / 1e6 if fwd_ms + bwd_ms > 0 else 0.0
-    print(json.dumps({
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": (fwd_ms + bwd_ms) / args.steps, "higher_is_better": True,
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "ms_per_step": (fwd_ms + bwd_ms) / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-        "config": {"workload": f"adjoint: small scene 512x512, 64 spp, 64 material groups, 8 area lights, "
-                               f"{n} parameters", "parameters": n},
-        "forward_ms": fwd_ms / args.steps, "adjoint_ms": bwd_ms / args.steps,
+        "config": {"workload": f"adjoint: small scene {args.diff_res}x{args.diff_res}, {args.diff_spp} spp, 64 "
+                               f"material groups, 8 area lights, {n} parameters", "parameters": n},
+        "forward_ms": fwd_ms / steps, "adjoint_ms": bwd_ms / steps,
         "adjoint_over_forward": bwd_ms / fwd_ms if fwd_ms else None, "loss": loss,
         "fd_check": {"params": [int(k) for k in idx], "max_rel_err": float(max(big)),
                      "median_rel_err": float(np.median(big)), "params_with_zero_gradient": len(rel) - len(big),
                      "max_abs_err_zero_gradient": float(tiny_abs), "max_abs_gradient": float(fmax),
                      "step": 1e-3, "accumulation": "fp64"},
         "gpu_launches": None, "clocks": clk,
-    }))
+    }
 
 
 def run_inverse(args, api, torch, local):
@@ -378,13 +380,15 @@ def run_inverse(args, api, torch, local):
     }))
 
 
-def run_batch(args, api, torch, local, barrier):
+def run_batch(args, api, torch, local, barrier, steps=None, warmup=None, count=None):
     """Uneven batch: `batch_count` independent scenes (1k-200k triangles,
     1-32 objects, 64^2-512^2, 4-64 spp, 1-4 lights, GI 1-3 bounces) rendered
     as one launch (yr_render_batch: autotuned schedule, CUDA graph), with
     the plain one-scene-per-call path (yr_render per scene) timed beside it
     on the same scenes; images of both paths are compared bit for bit."""
-    scs = scenes.config_batch(count=args.batch_count)
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    scs = scenes.config_batch(count=args.batch_count if count is None else count)
     t0 = time.perf_counter()
     dss = [api.DeviceScene(sc, device=local) for sc in scs]
     setup_s = time.perf_counter() - t0
@@ -395,7 +399,7 @@ def run_batch(args, api, torch, local, barrier):
     t0 = time.perf_counter()
     st, prm = api.render_batch(dss, ptrs)   # first call autotunes and captures the graph
     tune_s = time.perf_counter() - t0
-    for _ in range(max(0, args.warmup - 1)):
+    for _ in range(max(0, warmup - 1)):
         api.render_batch(dss, ptrs)
         for d, o in zip(dss, plain):
             d.render_into(o.data_ptr())
@@ -407,7 +411,7 @@ def run_batch(args, api, torch, local, barrier):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         rays = 0
-        for _ in range(args.steps):
+        for _ in range(steps):
             rays += fn()
         e1.record()
         torch.cuda.synchronize()
@@ -441,7 +445,7 @@ def run_batch(args, api, torch, local, barrier):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_rays = 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         for d in dss:
             d.set_params(d.sc.shaders, d.sc.lights)
         e2e_rays += batched()
@@ -450,26 +454,26 @@ def run_batch(args, api, torch, local, barrier):
         torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     line = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms_b / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
         "config": {"workload": f"batch: {len(dss)} scenes, {ntris:,} triangles, one graph launch",
                    "schedule": {1: "tiles", 2: "waves"}.get(prm.mode, prm.mode), "streams": prm.streams,
                    "block_size": prm.block_size, "queue_tile": prm.queue_tile,
                    "stack_entries": prm.stack_entries, "autotune_s": round(tune_s, 3),
                    "scene_setup_s": round(setup_s, 3), "l2": "scene arrays and images larger than L2"},
-        "plain_gpu": {"value": plain_value, "unit": METRIC, "ms_per_step": ms_p / args.steps,
+        "plain_gpu": {"value": plain_value, "unit": METRIC, "ms_per_step": ms_p / steps,
                       "launch": "yr_render per scene"},
         "speedup_vs_plain": value / plain_value if plain_value else None,
         "identical_images": identical,
         "e2e": {"value": e2e_rays / e2e_s / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps,
+        "gpu_launches": steps,
         "clocks": clk,
     }
     for d in dss:
         d.close()
-    print(json.dumps(line))
+    return line
 
 
 def run_kdbuild(args, api, local):
@@ -540,12 +544,16 @@ def main():
     ap.add_argument("--inverse-count", type=int, default=32, help="problems in the inverse workload")
     ap.add_argument("--inverse-steps", type=int, default=200, help="Adam steps per problem")
     ap.add_argument("--batch-count", type=int, default=256, help="scenes in the batch workload")
+    ap.add_argument("--diff-res", type=int, default=512, help="image size of the adjoint workload")
+    ap.add_argument("--diff-spp", type=int, default=64, help="samples per pixel of the adjoint workload")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--resx", type=int, default=1920)
     ap.add_argument("--resy", type=int, default=1080)
     ap.add_argument("--spp", type=int, default=16)
     ap.add_argument("--grid", type=int, default=16)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batch and adjoint ratios that the default line carries")
     ap.add_argument("--exact-order", action="store_true",
                     help="exact slab tests in the object tree (reference visiting order)")
     ap.add_argument("--shadow-tree", action="store_true", help="answer shadow rays with the shadow-ray tree")
@@ -574,10 +582,10 @@ def main():
             run_kdbuild(args, api, local)
         return
     if args.config == "batch":
-        run_batch(args, api, torch, local, barrier)
+        print(json.dumps(run_batch(args, api, torch, local, barrier)))
         return
     if args.config == "diff":
-        run_diff(args, api, torch, local)
+        print(json.dumps(run_diff(args, api, torch, local)))
         return
     if args.config == "inverse":
         run_inverse(args, api, torch, local)
@@ -593,11 +601,15 @@ def main():
     ds = api.DeviceScene(sc, device=local)
     info = ds.info()
     build_s = time.perf_counter() - t0
-    # the same kd-trees built on the GPU (yr_kdtree_build_gpu), timed once
+    # the same kd-trees built on the GPU (yr_kdtree_build_gpu): the process's
+    # first build (cold: module load, first device allocations) and a second
+    # one (warm)
     meshes = [m for m in sc.meshes if not m.is_instance]
-    t0 = time.perf_counter()
-    gtrees = api.kdtrees_gpu(meshes, device=local)
-    gpu_kd_s = time.perf_counter() - t0
+    kd_s = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        gtrees = api.kdtrees_gpu(meshes, device=local)
+        kd_s.append(time.perf_counter() - t0)
     gpu_kd_nodes = int(sum(t["nodes"].shape[0] for t in gtrees))
     del gtrees
     out = torch.empty((sc.resy, sc.resx, 4), dtype=torch.float32, device="cuda")
@@ -688,7 +700,8 @@ def main():
                    "kd_nodes": int(info.nnodes), "l2": "inputs larger than L2 (scene arrays "
                    f"{info.device_bytes / 1e6:.0f} MB on the device)",
                    "host_build_s": round(info.build_seconds, 3), "scene_setup_s": round(build_s, 3),
-                   "gpu_kd_build_s": round(gpu_kd_s, 3), "gpu_kd_nodes_equal": gpu_kd_nodes == int(info.nnodes),
+                   "gpu_kd_build_cold_s": round(kd_s[0], 3), "gpu_kd_build_warm_s": round(kd_s[1], 3),
+                   "gpu_kd_nodes_equal": gpu_kd_nodes == int(info.nnodes),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": gpu_launches,
@@ -699,9 +712,23 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline(sc)
+            line["cpu_baseline"]["frame_rays_per_sample"] = rays_all / (world * args.steps * sc.resx * sc.resy *
+                                                                         sc.render.spp)
         except Exception as ex:  # the GPU number stands without it
             line["cpu_baseline"] = {"value": None, "error": str(ex)[:300]}
     ds.close()
+    if world == 1 and not args.no_extras:
+        # the metric's other two ratios, on their own workloads
+        b = run_batch(args, api, torch, local, barrier, steps=2, warmup=2)
+        line["batch"] = {"workload": b["config"]["workload"], "schedule": b["config"]["schedule"],
+                         "streams": b["config"]["streams"], "value": b["value"], "unit": METRIC,
+                         "plain_gpu_value": b["plain_gpu"]["value"], "ratio": b["speedup_vs_plain"],
+                         "identical_images": b["identical_images"], "ms_per_step": b["ms_per_step"],
+                         "plain_ms_per_step": b["plain_gpu"]["ms_per_step"], "steps": b["steps"]}
+        d = run_diff(args, api, torch, local, steps=3, warmup=2)
+        line["adjoint"] = {"workload": d["config"]["workload"], "forward_ms": d["forward_ms"],
+                           "adjoint_ms": d["adjoint_ms"], "ratio": d["adjoint_over_forward"],
+                           "fd_check": d["fd_check"], "steps": d["steps"]}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -252,6 +252,15 @@ typedef struct yr_shader_desc {
     float tex_weights[4];    /* voronoi "weight1".."weight4"                   */
     float tex_mk_exponent;   /* voronoi "mk_exponent"                          */
     uint32_t tex_metric;     /* voronoi "distance_metric" YR_DIST_*            */
+    /* record version 3 */
+    float mod_specular;      /* modulator "specular": weight of the texture
+                                colour in the specular colour ks, by the same
+                                mode as "color" (modulator_t::modulate,
+                                texture.cc:499-534); 0 = not modulated        */
+    float mod_hard;          /* modulator "hard": weight of the texture value
+                                (getFloat) in the Phong exponent; 0 = not
+                                modulated.  The adjoint refuses shaders with
+                                either weight above 0                          */
 } yr_shader_desc;
 
 /* yr_shader_desc.tex_map.  TEXCO_ORCO reads the hit point as orco does for

@@ -201,8 +201,10 @@ static void load_scene(const char *path, SceneFile &s) {
     rd(f, &s.rp, hdr[3] >= 3 ? sizeof(s.rp) : offsetof(yr_render_params, exposure));
     s.shaders.resize(hdr[1]);
     memset(s.shaders.data(), 0, sizeof(yr_shader_desc) * hdr[1]);
-    // shader records before version 2 end at mod_mode
-    const size_t shsize = hdr[3] >= 2 ? sizeof(yr_shader_desc) : offsetof(yr_shader_desc, mod_mode);
+    // shader records before version 2 end at mod_mode, before version 5 at mod_specular
+    const size_t shsize = hdr[3] >= 5   ? sizeof(yr_shader_desc)
+                          : hdr[3] >= 2 ? offsetof(yr_shader_desc, mod_specular)
+                                        : offsetof(yr_shader_desc, mod_mode);
     for (uint32_t i = 0; i < hdr[1]; i++) rd(f, &s.shaders[i], shsize);
     s.lights.resize(hdr[2]);
     if (hdr[2]) rd(f, &s.lights[0], sizeof(yr_light_desc) * hdr[2]);
@@ -325,8 +327,8 @@ static shader_t *make_shader(const yr_shader_desc &d, std::vector<texture_t *> &
         static const char *modes[4] = {"mix", "mul", "add", "sub"};
         modu.string2modetype(modes[d.mod_mode < 4 ? d.mod_mode : 0]);
         modu.color(d.mod_color);
-        modu.specular(0);
-        modu.hard(0);
+        modu.specular(d.mod_specular);
+        modu.hard(d.mod_hard);
         modu.transmision(0);
         modu.reflection(0);
         modu.displace(0);

@@ -1206,35 +1206,65 @@ C mixc(const C &a, const C &b, float w) {
     return a * w + (1 - w) * b;
 }
 
-// the diffuse colour after the modulator (modulator_t::modulate,
-// texture.cc:499-534, colour channel; modes mix / mul / add / sub)
-C diffuse(const Scene &S, const SP &sp) {
+// modulator_t::modulate (texture.cc:499-534): the diffuse colour C, the
+// specular colour S and the Phong exponent H after the modulator, each
+// channel by its own weight ("color", "specular", "hard"; a channel whose
+// weight is not above 0 is left as it is), modes mix / mul / add / sub
+struct Mod {
+    C c, s;
+    float h;
+};
+Mod modulated(const Scene &S, const SP &sp) {
     const yr_shader_desc &d = S.shaders[sp.shader];
-    C c = col3(d.color);
-    if (d.tex_type == YR_TEX_NONE || !(d.mod_color > 0)) return c;
-    const C tex = texture_eval(d, tex_point(d, sp)).col;
-    const float w = d.mod_color;
+    Mod m;
+    m.c = col3(d.color);
+    m.s = col3(d.specular);
+    m.h = d.hard;
+    if (d.tex_type == YR_TEX_NONE || !(d.mod_color > 0 || d.mod_specular > 0 || d.mod_hard > 0)) return m;
+    const TexVal tv = texture_eval(d, tex_point(d, sp));
+    const C &tex = tv.col;
+    const float tf = tv.f, wc = d.mod_color, ws = d.mod_specular, wh = d.mod_hard;
     switch (d.mod_mode) {
-    case YR_MOD_MUL: return mixc(tex, C(1, 1, 1), w) * c;
-    case YR_MOD_ADD: return (tex * w) + c;
-    case YR_MOD_SUB: return (tex * -w) + c;
-    default: return mixc(tex, c, w);
+    case YR_MOD_MUL:
+        if (wc > 0) m.c = mixc(tex, C(1, 1, 1), wc) * m.c;
+        if (ws > 0) m.s = mixc(tex, C(1, 1, 1), ws) * m.s;
+        if (wh > 0) m.h = (tf * wh + (1 - wh)) * m.h;
+        break;
+    case YR_MOD_ADD:
+        if (wc > 0) m.c = (tex * wc) + m.c;
+        if (ws > 0) m.s = (tex * ws) + m.s;
+        if (wh > 0) m.h = tf * wh + m.h;
+        break;
+    case YR_MOD_SUB:
+        if (wc > 0) m.c = (tex * -wc) + m.c;
+        if (ws > 0) m.s = (tex * -ws) + m.s;
+        if (wh > 0) m.h = (tf * -wh) + m.h;
+        break;
+    default:
+        if (wc > 0) m.c = mixc(tex, m.c, wc);
+        if (ws > 0) m.s = mixc(tex, m.s, ws);
+        if (wh > 0) m.h = tf * wh + m.h * (1 - wh);
+        break;
     }
+    return m;
 }
+
+// the diffuse colour after the modulator (genericShader_t::getDiffuse,
+// basicshaders.cc:191-204)
+C diffuse(const Scene &S, const SP &sp) { return modulated(S, sp).c; }
 
 // genericShader_t::fromLight (basicshaders.cc:46-70)
 C fromLight(const Scene &S, const SP &sp, const V &ldir, const C &lcol, const V &eye) {
-    const yr_shader_desc &d = S.shaders[sp.shader];
     V edir = normalize(eye);
     V N = faceForward(sp.Ng, sp.N, edir);
     float inte = N * ldir;
     if (inte < 0) return C();
-    C lkc = diffuse(S, sp), lks = col3(d.specular);
+    const Mod m = modulated(S, sp);
     edir = reflectv(N, edir);
     float refle = edir * ldir;
     if (refle < 0) refle = 0;
-    else refle = (float)pow((double)refle, (double)d.hard);
-    return ((C(1.f * inte, 1.f * inte, 1.f * inte) * lcol) * lkc) + (lks * refle) * lcol;
+    else refle = (float)pow((double)refle, (double)m.h);
+    return ((C(1.f * inte, 1.f * inte, 1.f * inte) * lcol) * m.c) + (m.s * refle) * lcol;
 }
 
 // --------------------------------------------------------------- lights
@@ -1566,8 +1596,10 @@ orc_scene *orc_load(const char *path) {
     ok = ok && fread(&S.rp, 1, rpsize, f) == rpsize;
     S.shaders.assign(hdr[1], yr_shader_desc());
     std::vector<yr_light_desc> ld(hdr[2]);
-    // shader records before version 2 end at mod_mode
-    const size_t shsize = hdr[3] >= 2 ? sizeof(yr_shader_desc) : offsetof(yr_shader_desc, mod_mode);
+    // shader records before version 2 end at mod_mode, before version 5 at mod_specular
+    const size_t shsize = hdr[3] >= 5   ? sizeof(yr_shader_desc)
+                          : hdr[3] >= 2 ? offsetof(yr_shader_desc, mod_specular)
+                                        : offsetof(yr_shader_desc, mod_mode);
     for (uint32_t i = 0; ok && i < hdr[1]; i++) ok = fread(&S.shaders[i], 1, shsize, f) == shsize;
     ok = ok && rdv(f, ld.data(), hdr[2]);
     S.objs.resize(hdr[0]);

@@ -368,6 +368,51 @@ def texture_render():
     np.savez_compressed(os.path.join(HERE, "render_textures_128x96.npz"), image=img)
 
 
+def specmod_scene():
+    """Six spheres and the plane whose modulators also drive the specular
+    colour and the Phong exponent (the modulator's "specular" and "hard"
+    weights) in every mode - some with the colour channel off - over a
+    specular base colour; two point lights."""
+    sc = scenes.config_small(96, 72)
+    ts = scenes.texture_shader
+    base = dict(mod_specular=0.7, mod_hard=0.5)
+    sc.shaders = [
+        ts((0.6, 0.6, 0.6), "marble", (0.9, 0.9, 0.85), (0.2, 0.2, 0.3), mod_color=0.6, turbulence=2.0, size=2.0,
+           **base),
+        ts((0.7, 0.5, 0.3), "musgrave", (0.5, 0.3, 0.1), (0.8, 0.6, 0.3), mode="mul", mod_color=0.8, size=2.5,
+           intensity=0.6, mod_specular=0.9, mod_hard=0.3),
+        ts((0.3, 0.3, 0.3), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mode="add", mod_color=0.5,
+           color_type="col2", weight1=1.0, weight2=-0.6, size=4.0, mod_specular=0.4, mod_hard=0.25),
+        ts((0.8, 0.8, 0.8), "clouds", (0.1, 0.1, 0.1), (0.6, 0.5, 0.4), mode="sub", mod_color=0.4, depth=3,
+           size=1.5, mod_specular=0.2, mod_hard=0.2),
+        ts((0.5, 0.5, 0.6), "wood", (0.5, 0.3, 0.1), (0.8, 0.6, 0.3), mod_color=0.0, turbulence=0.8,
+           mod_specular=1.0, mod_hard=0.0),
+        ts((0.4, 0.6, 0.5), "gradient", (0.0, 0.0, 0.2), (1.0, 0.9, 0.6), gradient_type="sphere", texco="normal",
+           mode="mul", mod_color=0.0, mod_specular=0.0, mod_hard=0.8),
+        ts((0.7, 0.7, 0.7), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mod_color=0.3, color_type="int",
+           size=1.0, intensity=1.0, **base),
+    ]
+    for s in sc.shaders:
+        s.specular[:] = [0.35, 0.3, 0.25]
+        s.hard = 18.0
+    meshes = []
+    for k in range(6):
+        v, t = scenes.uv_sphere((-1.5 + 1.5 * (k % 3), -0.45, -0.6 + 1.3 * (k // 3)), 0.55, rings=16, segments=32)
+        meshes.append(scenes.Mesh(v, t, k))
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    meshes.append(scenes.Mesh(pv, pt, 6))
+    sc.meshes = meshes
+    sc.lights = [scenes.point_light((2.0, 4.0, 3.0), 14.0), scenes.point_light((-3.0, 3.0, 1.0), 6.0,
+                                                                               color=(0.8, 0.9, 1.0))]
+    sc.camera = scenes.camera((0.0, 3.0, 4.5), (0.0, -0.5, 0.0), (0.0, 4.0, 4.5), 96, 72)
+    return sc
+
+
+def specmod_render():
+    img, _ = T.harness_render(specmod_scene())
+    np.savez_compressed(os.path.join(HERE, "render_specmod_96x72.npz"), image=img)
+
+
 def tonemap_configs():
     """The render block's tone mapping variants: clamp_rgb, exposure, gamma,
     both, and gamma with alpha premultiply, on a constant background."""
@@ -498,6 +543,7 @@ if __name__ == "__main__":
     smooth_render()
     textures()
     texture_render()
+    specmod_render()
     tonemap_renders()
     image_outputs()
     instances()

@@ -222,6 +222,25 @@ def test_oracle_texture_render_matches_reference():
     assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
 
 
+def test_oracle_specular_hardness_modulation_matches_reference():
+    """Modulators that also drive the specular colour and the Phong
+    exponent (the modulator's "specular" / "hard" weights, every mode,
+    some with the colour channel off), against the reference's render."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    ref = load("render_specmod_96x72.npz")["image"]
+    sc = make_golden.specmod_scene()
+    img, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
+    # the weights matter: without them the image differs
+    for s in sc.shaders:
+        s.mod_specular = s.mod_hard = 0.0
+    plain, _ = T.OracleScene(sc).render()
+    assert np.abs(plain - ref).max() > 1e-2
+
+
 @pytest.mark.parametrize("k", range(5))
 def test_oracle_tonemap_matches_reference(k):
     """Per-sample expgam_Adjust (clamp_rgb, exposure, gamma, both) and alpha

@@ -122,6 +122,94 @@ def test_grad_hemi_light(cuda):
     _check(torch, sc, _hidden(4), nsample=5, rtol=1e-2)
 
 
+def _scene_with_params(sc, theta):
+    """A copy of the scene description with the parameter vector written
+    into its shader and light records the way yr_params_set maps it (per
+    shader: colour, the specular weight along the specular colour's
+    direction, and for textured shaders the texture amplitude and base
+    colour; per light: power), in float32 as the library does."""
+    import copy
+    from yafray_b200 import abi
+    s2 = copy.copy(sc)
+    s2.shaders, s2.lights = [], []
+    f32 = np.float32
+    n = 0
+    for d in sc.shaders:
+        e = abi.YrShaderDesc.from_buffer_copy(d)
+        ks = [f32(x) for x in d.specular]
+        w = max(ks)
+        sdir = [k / w if w > 0 else f32(1.0) for k in ks]
+        e.color[:] = [float(theta[n + c]) for c in range(3)]
+        e.specular[:] = [float(f32(theta[n + 3]) * sdir[c]) for c in range(3)]
+        n += 4
+        if d.tex_type != abi.YR_TEX_NONE:
+            e.tex_intensity = float(theta[n])
+            e.tex_color1[:] = [float(theta[n + 1 + c]) for c in range(3)]
+            n += 4
+        s2.shaders.append(e)
+    for l in sc.lights:
+        e = abi.YrLightDesc.from_buffer_copy(l)
+        e.power = float(theta[n])
+        n += 1
+        s2.lights.append(e)
+    assert n == len(theta)
+    return s2
+
+
+@pytest.mark.parametrize("gi", [False, True])
+def test_grad_against_oracle_finite_differences(cuda, gi):
+    """The adjoint against central differences of the ORACLE's forward
+    render (the CPU restatement of the reference's estimators, FP64 loss
+    accumulation, step 1e-3) on a config-4-shaped scene at small size: 8
+    material groups (diffuse RGB + specular weight) and 2 area lights, 48x48,
+    4 spp; with `gi` also a 2-bounce path light.  The oracle's renders
+    are checked to keep every energy cut-off decision at least 20% away from
+    its threshold, so a step of 1e-3 cannot flip one."""
+    import torch
+    import yrtest as T
+    sc = scenes.config_diff(res=48, spp=4, groups=8, nlights=2)
+    if gi:
+        sc.lights.append(scenes.path_light(samples=1, depth=2, power=1.0))
+    ds = api.DeviceScene(sc)
+    theta = ds.params_get().astype(np.float32)
+    n = theta.size
+    assert n == 8 * 4 + len(sc.lights)
+    ds.params_set(_hidden(7)(theta))
+    target = _render(torch, ds)
+    ds.params_set(theta)
+    img = _render(torch, ds)
+    grad = torch.zeros(n, dtype=torch.float32, device="cuda")
+    ds.backward(img.data_ptr(), target.data_ptr(), grad.data_ptr(), 1.0)
+    g = grad.cpu().numpy().astype(np.float64)
+    tgt = target.cpu().numpy()
+    trees = [T.product_tree(m) for m in sc.meshes]
+
+    def oracle_loss(th):
+        O = T.OracleScene(_scene_with_params(sc, th), trees=trees)
+        im, _, margin = O.render_ex(0, sc.resx, 0, sc.resy)
+        O.close()
+        return _loss(im, tgt), float(margin.min())
+
+    l0, m0 = oracle_loss(theta)
+    assert m0 > 0.2, f"an energy cut-off value lies within {m0:.3g} (relative) of its threshold"
+    assert l0 == pytest.approx(_loss(img.cpu().numpy(), tgt), rel=1e-4)  # oracle and device forwards agree
+    rng = np.random.default_rng(11)
+    idx = rng.choice(n, size=16, replace=False)
+    fd = np.zeros(idx.size)
+    for q, k in enumerate(idx):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] = np.float32(theta[k] + 1e-3)
+        tm[k] = np.float32(theta[k] - 1e-3)
+        (lp, mp), (lm, mm) = oracle_loss(tp), oracle_loss(tm)
+        assert min(mp, mm) > 0.2
+        fd[q] = (lp - lm) / (float(tp[k]) - float(tm[k]))
+    big = np.abs(fd) > 1e-3 * np.abs(fd).max()
+    rel = np.abs(g[idx] - fd) / np.maximum(np.abs(fd), 1e-30)
+    assert big.sum() >= 12
+    assert (rel[big] <= 1e-3).all(), f"params {idx[big][rel[big] > 1e-3]}: rel {rel[big][rel[big] > 1e-3]}"
+    assert (np.abs(g[idx] - fd)[~big] <= 1e-4 * np.abs(fd).max()).all()
+
+
 def test_backward_rejects_bad_args(cuda):
     import torch
     from yafray_b200 import abi

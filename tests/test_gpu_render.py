@@ -1,7 +1,12 @@
 """yr_render against the oracle on the same scenes and QMC indices.
 
 Tolerances (from the specification of this path): radiance within 1e-4
-relative; pixel coverage (alpha) identical."""
+relative for every pixel; pixel coverage (alpha) identical.  A pixel beyond
+1e-4 is accepted only when an energy cut-off of the estimators explains it
+(a path stopping below 0.05, pathlight.cc:315 / 398; a hemi point skipped,
+hemilight.cc:67): the oracle re-renders that pixel taking the other branch
+of every cut-off within 1e-5 (relative) of its threshold, and that render
+must agree with the device's."""
 import numpy as np
 import pytest
 
@@ -13,12 +18,26 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-4
 
 
-def _cmp(img, ref, frac=1.0):
+FLIP_BAND = 1e-5
+
+
+def _cmp(img, ref, O=None):
+    """Every pixel within RTOL, or explained by an energy cut-off flip
+    (needs the oracle scene `O` that rendered `ref`)."""
     assert img.shape == ref.shape
     assert np.isfinite(img).all()
     rel = np.abs(img[..., :3] - ref[..., :3]) / np.maximum(np.abs(ref[..., :3]), 1e-3)
-    ok = (rel <= RTOL).all(-1)
-    assert ok.mean() >= frac, f"{(~ok).sum()} pixels beyond {RTOL}; worst {rel.max()}"
+    bad = np.argwhere((rel > RTOL).any(-1))
+    unexplained = []
+    for y, x in bad:
+        if O is not None:
+            fl, _, margin = O.render_ex(int(x), int(x) + 1, int(y), int(y) + 1, flip_band=FLIP_BAND)
+            r2 = np.abs(img[y, x, :3] - fl[y, x, :3]) / np.maximum(np.abs(fl[y, x, :3]), 1e-3)
+            if margin[y, x] <= FLIP_BAND and (r2 <= RTOL).all():
+                continue
+        unexplained.append((int(x), int(y), float(rel[y, x].max())))
+    assert not unexplained, (f"{len(unexplained)} of {len(bad)} pixels beyond {RTOL} without a cut-off flip: "
+                             f"{unexplained[:6]}")
     return rel
 
 
@@ -27,9 +46,10 @@ def test_render_small_point_light(cuda):
     sc = scenes.config_small()
     ds = api.DeviceScene(sc)
     img = ds.render()
-    ref, stats = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, stats = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref)
+    _cmp(img, ref, O)
     st = ds.last_stats
     assert st.rays_primary == stats[0] and st.rays_shadow == stats[1]
 
@@ -39,8 +59,9 @@ def test_render_small_aa(cuda):
     sc.render.spp = 5
     ds = api.DeviceScene(sc)
     img = ds.render()
-    ref, _ = T.OracleScene(sc).render()
-    _cmp(img, ref)
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
+    _cmp(img, ref, O)
 
 
 def test_render_gi_area_lights(cuda):
@@ -48,8 +69,9 @@ def test_render_gi_area_lights(cuda):
     sc = scenes.config_large(seed=2, resx=64, resy=40, spp=4, grid=2)
     ds = api.DeviceScene(sc)
     img = ds.render()
-    ref, stats = T.OracleScene(sc).render()
-    _cmp(img, ref, frac=0.995)
+    O = T.OracleScene(sc)
+    ref, stats = O.render()
+    _cmp(img, ref, O)
     st = ds.last_stats
     assert st.rays_primary == stats[0]
     assert abs(int(st.rays_shadow) - int(stats[1])) <= 0.001 * stats[1] + 4
@@ -63,16 +85,18 @@ def test_render_hemi_and_texture(cuda):
     sc.render.spp = 2
     ds = api.DeviceScene(sc)
     img = ds.render()
-    ref, _ = T.OracleScene(sc).render()
-    _cmp(img, ref, frac=0.995)
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
+    _cmp(img, ref, O)
 
 
 def test_render_per_triangle_materials(cuda):
     sc = scenes.config_diff(res=48, spp=2, groups=8, nlights=2)
     ds = api.DeviceScene(sc)
     img = ds.render()
-    ref, _ = T.OracleScene(sc).render()
-    _cmp(img, ref, frac=0.995)
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
+    _cmp(img, ref, O)
 
 
 @pytest.mark.parametrize("flags", [1, 2, 3])
@@ -109,9 +133,10 @@ def test_render_many_shadow_candidates(cuda):
     sc = _layered_spheres_scene()
     ds = api.DeviceScene(sc)
     img = ds.render()
-    ref, stats = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, stats = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref)
+    _cmp(img, ref, O)
     assert ds.last_stats.rays_shadow == stats[1]
     sc.render.flags = 2  # exact order: the nested walk, same image
     assert np.array_equal(api.DeviceScene(sc).render(), img)
@@ -131,9 +156,10 @@ def test_render_smoothed_meshes(cuda, gi):
         sc.render.spp = 3
     ds = api.DeviceScene(sc)
     img = ds.render()
-    ref, _ = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref, frac=0.995 if gi else 1.0)
+    _cmp(img, ref, O)
 
 
 def test_render_texture_coordinates(cuda):
@@ -144,9 +170,10 @@ def test_render_texture_coordinates(cuda):
     import make_golden
     sc = make_golden.texco_scene()
     img = api.DeviceScene(sc).render()
-    ref, _ = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref)
+    _cmp(img, ref, O)
 
 
 @pytest.mark.parametrize("gi", [False, True])
@@ -164,9 +191,24 @@ def test_render_procedural_textures(cuda, gi):
                      scenes.path_light(samples=1, depth=2, power=1.0)]
         sc.render.spp = 2
     img = api.DeviceScene(sc).render()
-    ref, _ = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref, frac=0.995 if gi else 0.999)
+    _cmp(img, ref, O)
+
+
+def test_render_specular_hardness_modulation(cuda):
+    """The modulator's "specular" and "hard" weights: the texture also
+    drives the specular colour and the Phong exponent, every mode."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.specmod_scene()
+    img = api.DeviceScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref, O)
 
 
 def test_render_texture_board(cuda):
@@ -177,9 +219,10 @@ def test_render_texture_board(cuda):
     import make_golden
     sc = make_golden.texture_board()
     img = api.DeviceScene(sc).render()
-    ref, _ = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref, frac=0.999)
+    _cmp(img, ref, O)
 
 
 def test_invalid_texture_records_rejected(cuda):
@@ -202,9 +245,10 @@ def test_render_tone_mapping(cuda, k):
     import make_golden
     sc = make_golden.tonemap_scene(make_golden.tonemap_configs()[k])
     img = api.DeviceScene(sc).render()
-    ref, _ = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref)
+    _cmp(img, ref, O)
 
 
 def test_tone_mapping_gamma_zero_refused(cuda):
@@ -232,6 +276,7 @@ def test_render_instances(cuda, gi, reference_inverses):
                      scenes.path_light(samples=1, depth=2, power=1.0)]
         sc.render.spp = 2
     img = api.DeviceScene(sc).render()
-    ref, _ = T.OracleScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
     assert np.array_equal(img[..., 3], ref[..., 3])
-    _cmp(img, ref, frac=0.995 if gi else 0.999)
+    _cmp(img, ref, O)

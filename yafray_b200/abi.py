@@ -92,6 +92,8 @@ class YrShaderDesc(C.Structure):
         ("tex_turbulence", C.c_float), ("tex_sharpness", C.c_float), ("tex_offset", C.c_float),
         ("tex_gain", C.c_float), ("tex_distort", C.c_float), ("tex_noise2", C.c_uint32),
         ("tex_weights", C.c_float * 4), ("tex_mk_exponent", C.c_float), ("tex_metric", C.c_uint32),
+        # record version 3
+        ("mod_specular", C.c_float), ("mod_hard", C.c_float),
     ]
 
 

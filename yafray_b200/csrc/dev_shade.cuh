@@ -381,6 +381,47 @@ struct TexDeriv {
     float dc1;
 };
 
+// modulator_t::modulate (texture.cc:499-534), all three channels: the
+// diffuse colour C, the specular colour S and the Phong exponent H, each
+// by its own weight (a channel whose weight is not above 0 keeps its
+// value), in the modulator's mode - mix: C = mix(tex, C, wc), S =
+// mix(tex, S, ws), H = f*wh + H*(1-wh); mul: mix(tex, 1, w) * C (S alike),
+// H = (f*wh + (1-wh)) * H; add: tex*w + C, f*wh + H; sub: tex*(-w) + C,
+// f*(-wh) + H - with tex the texture's colour and f its value (getFloat).
+__device__ __forceinline__ void modulated_all(const DevShader *shp, const Surf &sp, C3 &C, C3 &S, float &H) {
+    const DevShader &sh = *shp;
+    C = sh.color;
+    S = sh.specular;
+    H = sh.hard;
+    if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f || sh.mod_spec > 0.f || sh.mod_hard > 0.f)) return;
+    const TexEval te = texture_eval(shp, tex_point(sh, sp));
+    const C3 tex = te.col;
+    const float f = te.f, wc = sh.mod_color, ws = sh.mod_spec, wh = sh.mod_hard;
+    const C3 one = c3(1.f, 1.f, 1.f);
+    switch (sh.mod_mode) {
+    case YR_MOD_MUL:
+        if (wc > 0.f) C = (wc > 1.0f ? tex : tex * wc + (1 - wc) * one) * C;
+        if (ws > 0.f) S = (ws > 1.0f ? tex : tex * ws + (1 - ws) * one) * S;
+        if (wh > 0.f) H = (f * wh + (1 - wh)) * H;
+        break;
+    case YR_MOD_ADD:
+        if (wc > 0.f) C = (tex * wc) + C;
+        if (ws > 0.f) S = (tex * ws) + S;
+        if (wh > 0.f) H = f * wh + H;
+        break;
+    case YR_MOD_SUB:
+        if (wc > 0.f) C = (tex * -wc) + C;
+        if (ws > 0.f) S = (tex * -ws) + S;
+        if (wh > 0.f) H = (f * -wh) + H;
+        break;
+    default:
+        if (wc > 0.f) C = wc > 1.0f ? tex : tex * wc + (1 - wc) * C;
+        if (ws > 0.f) S = ws > 1.0f ? tex : tex * ws + (1 - ws) * S;
+        if (wh > 0.f) H = f * wh + H * (1 - wh);
+        break;
+    }
+}
+
 // modulator_t::modulate (texture.cc:499-534), colour channel: the texture
 // colour at the modulator's texture point, mixed into the diffuse colour
 // by the modulator's mode - mix: mix(tex, C, w); mul: mix(tex, 1, w) * C;
@@ -392,6 +433,12 @@ __device__ __forceinline__ C3 modulated_color(const DevShader *shp, const Surf &
     const DevShader &sh = *shp;
     const C3 C = sh.color;
     if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f)) return C;
+    if (sh.mod_spec > 0.f || sh.mod_hard > 0.f) {  // one texture evaluation for all three channels
+        C3 c, s;
+        float h;
+        modulated_all(shp, sp, c, s, h);
+        return c;
+    }
     const TexEval te = texture_eval(shp, tex_point(sh, sp));
     if (td) {
         td->tex = te.col;

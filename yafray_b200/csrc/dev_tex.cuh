@@ -328,6 +328,7 @@ struct TexEval {
     C3 col;
     C3 dint;
     float dc1;
+    float f;   // getFloat (the hardness modulator's value)
 };
 
 static __device__ __noinline__ TexEval texture_eval(const DevShader *__restrict__ shp, const V3 &p) {
@@ -369,6 +370,7 @@ static __device__ __noinline__ TexEval texture_eval(const DevShader *__restrict_
                               (sh.weights[1] * F.da[1] + sh.weights[3] * F.da[3]));
         const float inte = sh.viscale * S;
         r.dc1 = 0.f;
+        r.f = inte;
         if (sh.tshape == 0) {
             r.col = c3(inte, inte, inte);
             const float d = sh.vinvw * S;
@@ -417,6 +419,7 @@ static __device__ __noinline__ TexEval texture_eval(const DevShader *__restrict_
             if (gr > 1) {  // getColor folds color1 + 1*(color2 - color1) to color2 in the shipped build
                 r.col = sh.tc2;
                 r.dc1 = 0.f;
+                r.f = 1.f;
                 return r;
             }
             f = gr < 0 ? 0.f : (float)((double)(gr * gr) * (3.0 - 2.0 * (double)gr));
@@ -439,6 +442,7 @@ static __device__ __noinline__ TexEval texture_eval(const DevShader *__restrict_
     }
     r.col = sh.tc1 + f * (sh.tc2 - sh.tc1);
     r.dc1 = 1.f - f;
+    r.f = f;
     return r;
 }
 

@@ -197,7 +197,13 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
     C3 lkc = c3(0.f, 0.f, 0.f);
     if (active) {
         sh = R.shaders[sp.shader];
-        lkc = modulated_color(R.shaders + sp.shader, sp, ADJ ? td_out : nullptr);
+        if (!ADJ && (sh.mod_spec > 0.f || sh.mod_hard > 0.f)) {
+            // the modulator also sets this point's specular colour and
+            // Phong exponent (fromLight, basicshaders.cc:55-62)
+            modulated_all(R.shaders + sp.shader, sp, lkc, sh.specular, sh.hard);
+        } else {
+            lkc = modulated_color(R.shaders + sp.shader, sp, ADJ ? td_out : nullptr);
+        }
         if (ADJ) *lkc_out = lkc;
     }
     V3 N = sp.N;

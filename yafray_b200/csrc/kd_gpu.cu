@@ -31,7 +31,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <thread>
@@ -974,6 +976,26 @@ __global__ void k_write(const NodeRec *__restrict__ rec, uint32_t nids, const ui
 }
 
 // ------------------------------------------------------------ host side
+// Phase timings of a build on stderr, for variant builds only
+// (-DYR_KD_PHASE_TIMES): wall time of each phase since the previous mark,
+// and the time spent growing device buffers.
+#ifdef YR_KD_PHASE_TIMES
+static double kd_now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+static double g_kd_mark = 0.0, g_kd_alloc = 0.0;
+static int g_kd_allocs = 0;
+static void kd_phase(const char *name) {
+    const double t = kd_now();
+    if (name) fprintf(stderr, "kd phase %-14s %8.2f ms (buffer growth so far %d, %.2f ms)\n", name,
+                      1e3 * (t - g_kd_mark), g_kd_allocs, 1e3 * g_kd_alloc);
+    g_kd_mark = t;
+}
+#define KD_PHASE(name) kd_phase(name)
+#else
+#define KD_PHASE(name) ((void)0)
+#endif
+
 struct DBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -986,6 +1008,16 @@ struct DBuf {
     // grow to at least n bytes, keeping the first `keep` bytes
     bool ensure(size_t n, size_t keep, cudaStream_t s) {
         if (n <= bytes) return true;
+#ifdef YR_KD_PHASE_TIMES
+        const double t0 = kd_now();
+        struct Acc {
+            double t0;
+            ~Acc() {
+                g_kd_alloc += kd_now() - t0;
+                g_kd_allocs++;
+            }
+        } acc{t0};
+#endif
         const size_t nb = std::max(n, bytes + bytes / 2);
         void *q = nullptr;
         if (cudaMalloc(&q, nb) != cudaSuccess) return false;
@@ -1046,6 +1078,11 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
                             std::vector<KdTree> &out, yr_kdtree **abi_out) {
     const uint32_t nobj = (uint32_t)meshes.size();
     if (nobj == 0) return YR_ERR_INVALID_ARG;
+#ifdef YR_KD_PHASE_TIMES
+    g_kd_alloc = 0.0;
+    g_kd_allocs = 0;
+#endif
+    KD_PHASE(nullptr);
     size_t nt = 0, nv = 0;
     for (const KdMesh &m : meshes) {
         if (!m.verts || !m.tris || m.ntris == 0) return YR_ERR_EMPTY_SCENE;
@@ -1071,6 +1108,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         for (yr_status c : chk)
             if (c != YR_OK) return c;
     }
+    KD_PHASE("input checks");
     // candidates pack index << 2; list offsets carry two flag bits
     if (nt >= (1u << 28) || nv >= 0xffffffffu / 3) return YR_ERR_TOO_LARGE;
     int ndev = 0;
@@ -1104,6 +1142,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         }
     } eg{ev_go, ev_done};
 
+    KD_PHASE("streams");
     // inputs: all meshes concatenated, vertex indices made global
     std::vector<float> hv(3 * nv);
     std::vector<uint32_t> ht(3 * nt);
@@ -1145,6 +1184,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     std::vector<float> ob(6 * (size_t)nobj);
     cudaMemcpyAsync(ob.data(), d_obnd.p, 24 * (size_t)nobj, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return YR_ERR_CUDA;
+    KD_PHASE("pack+upload");
     for (uint32_t o = 0; o < nobj; o++) {
         Box raw;
         std::memcpy(raw.a, &ob[6 * o], 12);
@@ -1220,6 +1260,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     T.nids = nobj;
     std::vector<uint32_t> level_lo{0}, level_hi{nobj};
 
+    KD_PHASE("roots+buffers");
     // one depth per step, over all meshes
     while (nbig + nsmall > 0) {
         const size_t nodes_now = (size_t)nbig + nsmall, refs_now = big_refs + small_refs;
@@ -1333,6 +1374,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         small_refs = T.small_refs;
     }
 
+    KD_PHASE("depths");
     // node order: sizes bottom-up, places top-down, then every node written
     const uint32_t nids = T.nids;
     DBuf d_size, d_place, d_onodes, d_oprims;
@@ -1367,6 +1409,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
     }
     k_write<<<blocks(nids, 256), 256, 0, st>>>(d_rec.as<NodeRec>(), nids, d_place.as<uint2>(), d_op.as<ObjP>(),
                                                d_pool.as<uint32_t>(), d_onodes.as<uint2>(), d_oprims.as<uint32_t>());
+    KD_PHASE("layout");
     // each tree straight into its destination: yr_kdtree records for the
     // caller, or the KdTree vectors
     if (abi_out) {
@@ -1412,6 +1455,7 @@ yr_status build_kdtrees_gpu(const std::vector<KdMesh> &meshes, const KdParams &k
         }
     }
     if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return YR_ERR_CUDA;
+    KD_PHASE("trees out");
     return YR_OK;
 }
 

@@ -127,6 +127,8 @@ void make_shader(const yr_shader_desc &d, DevShader &o) {
     o.tsize = d.tex_size;
     o.intensity = d.tex_intensity;
     o.mod_color = d.mod_color;
+    o.mod_spec = d.mod_specular;
+    o.mod_hard = d.mod_hard;
     for (int k = 0; k < 3; k++) {
         o.msize[k] = d.mod_size[k];
         o.mofs[k] = d.mod_ofs[k];

@@ -19,6 +19,7 @@ struct DevShader {
     C3 tc1, tc2;     // texture color1 / color2
     float H, lacunarity, octaves, tsize, intensity;
     float mod_color;
+    float mod_spec, mod_hard;  // modulator "specular" / "hard" weights
     float msize[3], mofs[3];
     int tdepth, thard;
     int texco;           // YR_TEXCO_*

@@ -211,11 +211,14 @@ _MUSGRAVE_TYPES = {"fBm": abi.YR_TEX_MUSGRAVE_FBM, "multifractal": abi.YR_TEX_MU
 
 
 def texture_shader(color, kind, color1=(0.0, 0.0, 0.0), color2=(1.0, 1.0, 1.0), mod_color=1.0, mode="mix",
-                   texco="global", proj=("x", "y", "z"), **params) -> abi.YrShaderDesc:
+                   texco="global", proj=("x", "y", "z"), mod_specular=0.0, mod_hard=0.0,
+                   **params) -> abi.YrShaderDesc:
     """genericShader_t whose diffuse colour is modulated by one procedural
     texture `kind` ("clouds", "marble", "wood", "voronoi", "musgrave",
     "distorted_noise", "gradient") with the factory's parameter names and
-    defaults; unknown parameter names raise."""
+    defaults; unknown parameter names raise.  mod_specular / mod_hard: the
+    modulator's "specular" and "hard" weights (the texture also modulates
+    the specular colour and the Phong exponent)."""
     p = dict(_TEX_DEFAULTS[kind])
     for k in params:
         if k not in p:
@@ -225,6 +228,8 @@ def texture_shader(color, kind, color1=(0.0, 0.0, 0.0), color2=(1.0, 1.0, 1.0), 
     s.tex_color1[:] = [float(c) for c in color1]
     s.tex_color2[:] = [float(c) for c in color2]
     s.mod_color = float(mod_color)
+    s.mod_specular = float(mod_specular)
+    s.mod_hard = float(mod_hard)
     s.mod_mode = abi.MOD_MODES[mode]
     s.tex_map = tex_map(texco, proj)
     nt = lambda name: abi.NOISE_TYPES.get(name, 0)  # newNoise: unknown names give newperlin
@@ -499,8 +504,9 @@ def write_yrs(sc: Scene, path: str) -> None:
         # smoothing angle; 2 = shader records carry the version-2 texture
         # fields; 3 = render parameters carry exposure and gamma; 4 = object
         # records carry the instance index (-1: a mesh) and, for instances,
-        # the 4x4 matrix
-        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 4))
+        # the 4x4 matrix; 5 = shader records carry the specular / hardness
+        # modulation weights
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 5))
         f.write(bytes(sc.camera))
         f.write(bytes(sc.render))
         for s in sc.shaders:
@@ -538,8 +544,10 @@ def read_yrs(path: str) -> Scene:
     if version < 3:
         sc.render.gamma = 1.0
     off += rpsize
-    # shader records before version 2 end at mod_mode
-    shsize = C_sizeof(abi.YrShaderDesc) if version >= 2 else abi.YrShaderDesc.mod_mode.offset
+    # shader records before version 2 end at mod_mode, before version 5 at
+    # mod_specular
+    shsize = (C_sizeof(abi.YrShaderDesc) if version >= 5 else
+              abi.YrShaderDesc.mod_specular.offset if version >= 2 else abi.YrShaderDesc.mod_mode.offset)
     for _ in range(nsh):
         s = abi.YrShaderDesc()
         C_memmove(s, data[off:off + shsize])
