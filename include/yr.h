@@ -539,6 +539,25 @@ YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_host,
  *     reads the render's device status word back). */
 YR_API yr_status yr_render_noalloc(yr_scene *scene, float *rgba, yr_render_stats *stats, void *stream);
 
+/* Progressive render with cancellation - the output side of YafRay's
+ * block loop, where each finished block goes through colorOutput_t::putPixel
+ * and a putPixel that returns false stops the render (renderblock.cc:8-20,
+ * threadedscene.cc:186-197).  The frame is rendered wave by wave (waves of
+ * at most `wave_pixels` pixels, 0 = as large as the scratch budget allows);
+ * after each wave its pixels are in the HOST image `rgba` (resx*resy*4
+ * floats) and `on_pixels(user, first, count)` is called with them: region
+ * pixels first .. first+count-1 in row-major order of the render region
+ * (region pixel k is (x0 + k % w, y0 + k / w); the whole image when no
+ * region is set).  Returning 0 from on_pixels stops the render after that
+ * wave and the call returns YR_ERR_CANCELLED; pixels not delivered keep the
+ * buffer's previous content (pixels outside the region are 0).  The image
+ * of a render that runs to the end is yr_render's; stats carry the rays of
+ * the waves rendered (no event timing).  The call returns when the last
+ * wave is delivered. */
+typedef int (*yr_pixels_fn)(void *user, uint32_t first, uint32_t count);
+YR_API yr_status yr_render_progressive(yr_scene *scene, float *rgba, uint32_t wave_pixels, yr_pixels_fn on_pixels,
+                                       void *user, yr_render_stats *stats, void *stream);
+
 /* Render `count` independent scenes (one device) as one launch.  Two
  * schedules, both giving each scene exactly yr_render's image:
  *   YR_BATCH_TILES: one persistent kernel; work items are tiles of whole

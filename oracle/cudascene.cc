@@ -213,6 +213,10 @@ yr_status cudascene_t::capture() {
         }
     }
     if (x1 <= x0 || y1 <= y0) return YR_ERR_INVALID_ARG;
+    rx0 = x0;
+    ry0 = y0;
+    rw = x1 - x0;
+    rh = y1 - y0;
     if (!(x0 == 0 && x1 == W && y0 == 0 && y1 == H)) {
         r.region[0] = x0;
         r.region[1] = x1;
@@ -233,6 +237,22 @@ yr_status cudascene_t::capture() {
     return yr_scene_set_camera_vectors(handle, pos, vto, vup, vright);
 }
 
+// yr_render_progressive's callback: one wave's region pixels to putPixel
+struct putPixels_t {
+    colorOutput_t *out;
+    const float *rgba;
+    int W, x0, y0, rw;
+};
+static int put_pixels(void *user, uint32_t first, uint32_t count) {
+    const putPixels_t &p = *(const putPixels_t *)user;
+    for (uint32_t k = first; k < first + count; k++) {
+        const int x = p.x0 + (int)(k % (uint32_t)p.rw), y = p.y0 + (int)(k / (uint32_t)p.rw);
+        const float *c = &p.rgba[4 * ((size_t)y * p.W + x)];
+        if (!p.out->putPixel(x, y, color_t(c[0], c[1], c[2]), c[3], 0)) return 0;  // the output asked to stop
+    }
+    return 1;
+}
+
 void cudascene_t::render(colorOutput_t &out) {
     if (!handle) {
         status = capture();
@@ -247,15 +267,18 @@ void cudascene_t::render(colorOutput_t &out) {
     std::vector<float> rgba((size_t)W * H * 4);
     yr_render_stats st;
     memset(&st, 0, sizeof(st));
-    status = yr_render(handle, &rgba[0], 1 /* host image */, &st, 0 /* default stream */);
+    putPixels_t pp = {&out, &rgba[0], W, rx0, ry0, rw};
+    // waves of about 64 rows, so the output sees the frame as it is made
+    status = yr_render_progressive(handle, &rgba[0], (uint32_t)(64 * rw), put_pixels, &pp, &st, 0);
     if (status != YR_OK) {
-        std::cerr << "cudascene_t: " << yr_status_string(status) << std::endl;
+        if (status != YR_ERR_CANCELLED) std::cerr << "cudascene_t: " << yr_status_string(status) << std::endl;
         return;
     }
+    // pixels outside the region are rendered as 0 by scene_t::render too
     for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x) {
-            const float *p = &rgba[4 * ((size_t)y * W + x)];
-            if (!out.putPixel(x, y, color_t(p[0], p[1], p[2]), p[3], 0)) return;  // output asked to stop
+            if (x >= rx0 && x < rx0 + rw && y >= ry0 && y < ry0 + rh) continue;
+            if (!out.putPixel(x, y, color_t(0.0), 0, 0)) return;
         }
 }
 

@@ -23,14 +23,16 @@ __BEGIN_YAFRAY
 
 class cudascene_t : public scene_t {
   public:
-    explicit cudascene_t(int device = 0) : handle(0), dev(device), status(YR_OK) {}
+    explicit cudascene_t(int device = 0) : handle(0), dev(device), status(YR_OK), rx0(0), ry0(0), rw(0), rh(0) {}
     virtual ~cudascene_t();
     // scene_t::render(colorOutput_t&) (scene.h:136): the frame through
-    // yr_render, pixels handed to the output with colorOutput_t::putPixel
-    // (output.h:36-38) as renderArea_t::out does (renderblock.cc:8-20).
-    // A scene the library cannot take, or a device error, leaves the output
-    // untouched and is reported by lastStatus(); nothing falls back to the
-    // CPU renderer.
+    // yr_render_progressive, each finished wave's pixels handed to the
+    // output with colorOutput_t::putPixel (output.h:36-38) as
+    // renderArea_t::out does (renderblock.cc:8-20); a putPixel that returns
+    // false stops the render (lastStatus() YR_ERR_CANCELLED).  A scene the
+    // library cannot take, or a device error, leaves the output untouched
+    // and is reported by lastStatus(); nothing falls back to the CPU
+    // renderer.
     virtual void render(colorOutput_t &out);
     yr_status lastStatus() const { return status; }
     static scene_t *factory(int device = 0) { return new cudascene_t(device); }
@@ -40,6 +42,7 @@ class cudascene_t : public scene_t {
     yr_scene *handle;
     int dev;
     yr_status status;
+    int rx0, ry0, rw, rh;  // the render region in pixels
 };
 
 __END_YAFRAY

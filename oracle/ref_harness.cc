@@ -9,7 +9,7 @@
 //   yr_ref_harness rays    SCENE RAYS OUT      kd / scene ray queries
 //   yr_ref_harness camera  SCENE OUT           primary ray directions
 //   yr_ref_harness instmat SCENE OUT           each reference's M^-1 (back)
-//   yr_ref_cudascene cudarender SCENE OUT [x0 x1 y0 y1]
+//   yr_ref_cudascene cudarender SCENE OUT [x0 x1 y0 y1 [STOP_AFTER]]
 //                                              the scene through cudascene_t (the
 //                                              library), a build of this file
 //                                              with YR_HARNESS_CUDASCENE
@@ -810,7 +810,19 @@ static void cmd_render_blocks(const SceneFile &s, const char *out, int threads, 
 // cudascene_t, rendered by cudascene_t::render - the library, through
 // yr_render - into the float sink.  One JSON line: the library's status
 // and the render time.
-static void cmd_cudarender(const SceneFile &s, const char *out, const int *crop) {
+// a float sink that asks the render to stop after `limit` pixels
+class stoppingSink_t : public floatSink_t {
+  public:
+    stoppingSink_t(int w, int h, long lim) : floatSink_t(w, h), limit(lim), taken(0) {}
+    virtual bool putPixel(int x, int y, const color_t &c, CFLOAT alpha, PFLOAT depth) {
+        if (limit >= 0 && taken >= limit) return false;
+        taken++;
+        return floatSink_t::putPixel(x, y, c, alpha, depth);
+    }
+    long limit, taken;
+};
+
+static void cmd_cudarender(const SceneFile &s, const char *out, const int *crop, long stop_after) {
     RefScene r;
     cudascene_t *cs = new cudascene_t(0);
     build_ref(s, r, true, cs);
@@ -821,11 +833,12 @@ static void cmd_cudarender(const SceneFile &s, const char *out, const int *crop)
         cs->setRegion(2.0 * crop[0] / rx - 1.0, 2.0 * crop[1] / rx - 1.0, 1.0 - 2.0 * crop[3] / ry,
                       1.0 - 2.0 * crop[2] / ry);
     }
-    floatSink_t sink(s.cam.resx, s.cam.resy);
+    stoppingSink_t sink(s.cam.resx, s.cam.resy, stop_after);
     double t0 = now_s();
     cs->render(sink);
     double t1 = now_s();
-    printf("{\"status\": %d, \"render_s\": %.6f}\n", (int)cs->lastStatus(), t1 - t0);
+    printf("{\"status\": %d, \"render_s\": %.6f, \"pixels\": %ld}\n", (int)cs->lastStatus(), t1 - t0,
+           sink.taken);
     fflush(stdout);
     FILE *f = fopen(out, "wb");
     wr(f, &sink.img[0], 4 * sink.img.size());
@@ -1113,12 +1126,12 @@ int main(int argc, char **argv) {
         cmd_render(s, argv[3], atoi(argv[4]), has_crop ? crop : NULL, reps < 1 ? 1 : reps);
 #ifdef YR_HARNESS_CUDASCENE
     } else if (cmd == "cudarender") {
-        if (argc < 4) die("cudarender SCENE OUT [x0 x1 y0 y1]");
+        if (argc < 4) die("cudarender SCENE OUT [x0 x1 y0 y1 [STOP_AFTER]]");
         int crop[4];
         const bool has_crop = argc >= 8;
         if (has_crop)
             for (int k = 0; k < 4; k++) crop[k] = atoi(argv[4 + k]);
-        cmd_cudarender(s, argv[3], has_crop ? crop : NULL);
+        cmd_cudarender(s, argv[3], has_crop ? crop : NULL, argc >= 9 ? atol(argv[8]) : -1L);
 #endif
     } else if (cmd == "render_blocks") {
         if (argc < 6) die("render_blocks SCENE OUT THREADS BLOCKS [REPEATS]");

@@ -80,3 +80,17 @@ def test_cudascene_refuses_what_it_cannot_take(cuda):
     dev, st = _run([CUDASCENE, "cudarender"], sc)
     assert st["status"] == 8  # YR_ERR_UNSUPPORTED
     assert not dev.any()
+
+
+def test_cudascene_output_can_stop_the_render(cuda):
+    """An output whose putPixel returns false after 5000 pixels stops the
+    render, as it stops scene_t::render: YR_ERR_CANCELLED, the pixels it
+    took are the full render's, no more are written."""
+    _need()
+    sc = scenes.config_small(160, 120)
+    full, _ = _run([CUDASCENE, "cudarender"], sc)
+    part, st = _run([CUDASCENE, "cudarender"], sc, 0, 160, 0, 120, 5000)
+    assert st["status"] == 7 and st["pixels"] == 5000  # YR_ERR_CANCELLED
+    flat, ref = part.reshape(-1, 4), full.reshape(-1, 4)
+    assert np.array_equal(flat[:5000], ref[:5000])
+    assert not flat[5000:].any()

@@ -174,6 +174,9 @@ class YrBackwardDesc(C.Structure):
 
 # Every symbol include/yr.h declares, with its ctypes signature.
 _P = C.c_void_p
+# yr_pixels_fn: int (*)(void *user, uint32_t first, uint32_t count)
+PIXELS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.c_uint32)
+
 SIGNATURES = {
     "yr_status_string": (C.c_char_p, [C.c_int]),
     "yr_version": (C.c_char_p, []),
@@ -196,6 +199,7 @@ SIGNATURES = {
     "yr_trace_closest": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_int, _P]),
     "yr_trace_shadow": (C.c_int, [_P, _P, C.c_uint32, _P, _P]),
     "yr_render": (C.c_int, [_P, _P, C.c_int, C.POINTER(YrRenderStats), _P]),
+    "yr_render_progressive": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.POINTER(YrRenderStats), _P]),
     "yr_render_noalloc": (C.c_int, [_P, _P, C.POINTER(YrRenderStats), _P]),
     "yr_render_batch": (C.c_int, [C.POINTER(_P), C.c_uint32, C.POINTER(_P), C.POINTER(YrBatchParams),
                                   C.POINTER(YrRenderStats), _P]),

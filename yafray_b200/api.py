@@ -101,6 +101,35 @@ class DeviceScene:
         self.last_stats = self.render_into(img.ctypes.data, on_host=True)
         return img
 
+    def render_progressive(self, on_pixels, wave_pixels: int = 0, img: np.ndarray = None):
+        """Render wave by wave into a host RGBA image (yr_render_progressive):
+        on_pixels(first, count) is called after each wave with the region
+        pixels it finished (row-major in the render region); returning False
+        stops the render.  Returns (image, status): status 0, or
+        YR_ERR_CANCELLED when the callback stopped it."""
+        if img is None:
+            img = np.zeros((self.sc.resy, self.sc.resx, 4), np.float32)
+        assert img.dtype == np.float32 and img.flags["C_CONTIGUOUS"] and img.shape == (self.sc.resy, self.sc.resx, 4)
+        errors = []
+
+        def cb(user, first, count):
+            try:
+                return 1 if on_pixels(int(first), int(count)) is not False else 0
+            except Exception as ex:  # stop the render, raise after the call
+                errors.append(ex)
+                return 0
+
+        fn = abi.PIXELS_FN(cb)
+        st = abi.YrRenderStats()
+        rc = self.lib.yr_render_progressive(self.handle, C.c_void_p(img.ctypes.data), int(wave_pixels), fn, None,
+                                            C.byref(st), None)
+        if errors:
+            raise errors[0]
+        if rc not in (0, 7):  # YR_OK, YR_ERR_CANCELLED
+            abi.check(rc, "yr_render_progressive")
+        self.last_stats = st
+        return img, rc
+
     # ------------------------------------------------------------- adjoint
     def param_count(self) -> int:
         return int(self.lib.yr_param_count(self.handle))

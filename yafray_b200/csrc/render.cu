@@ -41,73 +41,93 @@ static yr_status scratch(yr_scene *s, int i, size_t bytes, void **p) {
     return YR_OK;
 }
 
-// The launches of one render (all waves) on `st`, without any
-// synchronization; `timed(cls, launch)` wraps each kernel launch.
-template <class Timed>
-static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st,
-                         Timed &&timed) {
+// The launches of one render on `st`, without any synchronization;
+// `timed(cls, launch)` wraps each kernel launch.  waves_begin() clears the
+// render's counters and the image outside the region; wave_launch() runs
+// the wave of camera samples [b, b + wcap); launch_waves() is all of it.
+struct WaveGrids {
+    int gq, gb;
+};
+
+static WaveGrids waves_begin(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st) {
     DevRender &R = scene->rdr;
     W.out = out;
     cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
     cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
     // pixels outside the region are written as 0 (scene.cc:773)
     if (P.rpix != P.npix) cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
-    const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
+    WaveGrids G{0, 0};
     if (R.raydepth <= 0) {
         // raytrace() returns black at the ray-level cap (scene.cc:204-209);
         // a tone map keeps black black except pow(0, 0) = 1 for gamma 0,
         // which is refused when the scene is created
         cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
-    } else {
+        return G;
+    }
+    const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
 #if YR_TRACE_GRID_PERSIST
-        const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false>));
-        const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce<false>));
+    G.gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false>));
+    G.gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce<false>));
 #else
-        const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock), gb = gq;
+    G.gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
+    G.gb = G.gq;
 #endif
-        const DevScene &D = scene->dev;
-        const uint32_t npath = P.npath;
-        // the traversal kernels with the reference-transforming loops only
-        // for scenes that have references
-        const bool inst = D.insts != nullptr;
-        auto k_prim = inst ? k_primary<true> : k_primary<false>;
-        auto k_shadow = inst ? k_trace_shadow_q<true> : k_trace_shadow_q<false>;
-        auto k_bounce = inst ? k_trace_bounce<true> : k_trace_bounce<false>;
-        for (uint64_t b = 0; b < P.total; b += wcap) {
-            W.base = (uint32_t)b;
-            W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
-            const int g = (int)((W.count + kBlock - 1) / kBlock);
-            cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
-            timed(YR_K_PRIMARY, [&] { k_prim<<<g, kBlock, 0, st>>>(D, R, W); });
-            timed(YR_K_SHADE_CAMERA, [&] { k_shade_camera<<<g, kBlock, 0, st>>>(D, R, W); });
+    return G;
+}
+
+template <class Timed>
+static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, const WaveGrids &G, uint64_t b,
+                        cudaStream_t st, Timed &&timed) {
+    DevRender &R = scene->rdr;
+    const DevScene &D = scene->dev;
+    const uint32_t npath = P.npath;
+    const int gq = G.gq, gb = G.gb;
+    // the traversal kernels with the reference-transforming loops only
+    // for scenes that have references
+    const bool inst = D.insts != nullptr;
+    auto k_prim = inst ? k_primary<true> : k_primary<false>;
+    auto k_shadow = inst ? k_trace_shadow_q<true> : k_trace_shadow_q<false>;
+    auto k_bounce = inst ? k_trace_bounce<true> : k_trace_bounce<false>;
+    W.base = (uint32_t)b;
+    W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
+    const int g = (int)((W.count + kBlock - 1) / kBlock);
+    cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
+    timed(YR_K_PRIMARY, [&] { k_prim<<<g, kBlock, 0, st>>>(D, R, W); });
+    timed(YR_K_SHADE_CAMERA, [&] { k_shade_camera<<<g, kBlock, 0, st>>>(D, R, W); });
+    timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
+    cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
+    timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+    timed(YR_K_GATHER, [&] { k_gather_camera<<<g, kBlock, 0, st>>>(R, W); });
+    if (npath > 0) {
+        const size_t nc = (size_t)W.count * npath * P.depth;
+        timed(YR_K_OTHER, [&] {
+            k_clear_contri<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(W, nc);
+        });
+        const int gp = (int)(((size_t)W.count * npath + kBlock - 1) / kBlock);
+        for (int j = 0; j < R.path_depth; j++) {
+            timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 1); });
+            cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
+            timed(YR_K_BOUNCE, [&] { k_bounce<<<gb, kBlock, 0, st>>>(D, W); });
+            cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
+            timed(YR_K_SHADE_PATH, [&] { k_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j); });
             timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
             cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
             timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
-            timed(YR_K_GATHER, [&] { k_gather_camera<<<g, kBlock, 0, st>>>(R, W); });
-            if (npath > 0) {
-                const size_t nc = (size_t)W.count * npath * P.depth;
-                timed(YR_K_OTHER, [&] {
-                    k_clear_contri<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(W, nc);
-                });
-                const int gp = (int)(((size_t)W.count * npath + kBlock - 1) / kBlock);
-                for (int j = 0; j < R.path_depth; j++) {
-                    timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 1); });
-                    cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
-                    timed(YR_K_BOUNCE, [&] { k_bounce<<<gb, kBlock, 0, st>>>(D, W); });
-                    cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
-                    timed(YR_K_SHADE_PATH, [&] { k_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j); });
-                    timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
-                    cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
-                    timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
-                    timed(YR_K_GATHER, [&] { k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background); });
-                    std::swap(W.bq, W.bq2);
-                    timed(YR_K_OTHER, [&] { k_swap_queues<<<1, 1, 0, st>>>(W); });
-                }
-            }
-            const int gf = (int)((W.count / R.spp + kBlock - 1) / kBlock);
-            timed(YR_K_OTHER, [&] { k_finish<<<gf, kBlock, 0, st>>>(R, W); });
+            timed(YR_K_GATHER, [&] { k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background); });
+            std::swap(W.bq, W.bq2);
+            timed(YR_K_OTHER, [&] { k_swap_queues<<<1, 1, 0, st>>>(W); });
         }
     }
+    const int gf = (int)((W.count / R.spp + kBlock - 1) / kBlock);
+    timed(YR_K_OTHER, [&] { k_finish<<<gf, kBlock, 0, st>>>(R, W); });
+}
+
+template <class Timed>
+static void launch_waves(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st,
+                         Timed &&timed) {
+    const WaveGrids G = waves_begin(scene, P, wcap, W, out, st);
+    if (scene->rdr.raydepth <= 0) return;
+    for (uint64_t b = 0; b < P.total; b += wcap) wave_launch(scene, P, wcap, W, G, b, st, timed);
 }
 
 yr_status enqueue_render(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st) {
@@ -271,4 +291,71 @@ extern "C" YR_API yr_status yr_render(yr_scene *scene, float *rgba, int rgba_on_
         if (cudaStreamSynchronize(st) != cudaSuccess) return done(YR_ERR_CUDA);
     }
     return done(YR_OK);
+}
+
+extern "C" YR_API yr_status yr_render_progressive(yr_scene *scene, float *rgba, uint32_t wave_pixels,
+                                                  yr_pixels_fn on_pixels, void *user, yr_render_stats *stats,
+                                                  void *stream) {
+    if (!scene || !rgba || !on_pixels) return YR_ERR_INVALID_ARG;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(scene->device) != cudaSuccess) return YR_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    auto done = [&](yr_status e) {
+        cudaSetDevice(prev);
+        return e;
+    };
+    Plan P;
+    yr_status ret = make_plan(scene, P);
+    if (ret != YR_OK) return done(ret);
+    const DevRender &R = scene->rdr;
+    uint32_t wcap = std::max(R.spp, wave_for_budget(P, R, render_budget(1)));
+    if (wave_pixels) wcap = std::min(wcap, std::max(1u, wave_pixels) * R.spp);
+    PoolBlock blk(scene->device, st);
+    if ((ret = pool_acquire(scene->device, wave_bytes(P, wcap), blk.buf)) != YR_OK) return done(ret);
+    Wave W;
+    std::memset(&W, 0, sizeof(W));
+    assign_wave(P, wcap, (char *)blk.buf.p, W);
+    void *img = nullptr;
+    if ((ret = scratch(scene, 1, sizeof(float) * 4 * (size_t)P.npix, &img)) != YR_OK) return done(ret);
+    float *out = (float *)img;
+    const WaveGrids G = waves_begin(scene, P, wcap, W, out, st);
+    const size_t row = sizeof(float) * 4 * (size_t)R.cam.resx;
+    auto no_timing = [](int, auto &&launch) { launch(); };
+    uint64_t next = 0;  // first camera sample not yet delivered
+    bool stop = false;
+    if (R.raydepth <= 0 || P.rpix != P.npix) {
+        // every pixel outside the region (or all, at ray depth 0) is 0 now
+        if (cudaMemcpyAsync(rgba, out, row * R.cam.resy, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return done(YR_ERR_CUDA);
+    }
+    for (uint64_t b = 0; b < P.total && R.raydepth > 0 && !stop; b += wcap) {
+        wave_launch(scene, P, wcap, W, G, b, st, no_timing);
+        if (cudaGetLastError() != cudaSuccess) return done(YR_ERR_CUDA);
+        // the wave's pixels, region pixels [b/spp, (b+count)/spp): copy the
+        // image rows they lie on, then hand them to the caller
+        const uint32_t p0 = (uint32_t)(b / R.spp);
+        const uint32_t p1 = (uint32_t)(std::min<uint64_t>(P.total, b + wcap) / R.spp);
+        const int y0 = R.ry0 + (int)(p0 / (uint32_t)R.rw), y1 = R.ry0 + (int)((p1 - 1) / (uint32_t)R.rw);
+        if (cudaMemcpyAsync((char *)rgba + row * y0, (char *)out + row * y0, row * (size_t)(y1 - y0 + 1),
+                            cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return done(YR_ERR_CUDA);
+        if ((ret = take_status(scene, st)) != YR_OK) return done(ret);  // waits for the copy too
+        next = (uint64_t)p1 * R.spp;
+        stop = on_pixels(user, p0, p1 - p0) == 0;
+    }
+    if (R.raydepth <= 0 || P.rpix != P.npix) {
+        if (cudaStreamSynchronize(st) != cudaSuccess) return done(YR_ERR_CUDA);
+        if (R.raydepth <= 0) stop = on_pixels(user, 0, P.rpix) == 0;
+    }
+    if (stats) {
+        unsigned long long r[4] = {0, 0, 0, 0};
+        cudaMemcpyAsync(r, W.rays, sizeof(r), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return done(YR_ERR_CUDA);
+        stats->ms = 0.f;
+        stats->rays_primary = (R.raydepth > 0) ? next : 0;
+        stats->rays_shadow = r[1];
+        stats->rays_bounce = r[2];
+    }
+    return done(stop && next < P.total ? YR_ERR_CANCELLED : YR_OK);
 }
