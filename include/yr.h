@@ -274,7 +274,8 @@ enum { YR_LIGHT_POINT = 0, YR_LIGHT_AREA = 1, YR_LIGHT_HEMI = 2, YR_LIGHT_PATH =
 
 /* One record for every light plugin on the path:
  *   point: pointlight.cc:70-90   (p[0] = "from")
- *   area:  arealight.cc:235-254  (p[0..3] = "a","b","c","d", samples)
+ *   area:  arealight.cc:235-254  (p[0..3] = "a","b","c","d", samples,
+ *          psamples)
  *   hemi:  hemilight.cc:117+     (samples, maxdist, use_QMC always)
  *   path:  pathlight.cc:753-807  (samples, depth; use_QMC, cache off,
  *          no photon maps, adaptive repetitions off) */
@@ -287,7 +288,15 @@ typedef struct yr_light_desc {
     int32_t depth;
     float maxdist;
     uint32_t cast_shadows;   /* point light "cast_shadows" (default 1)        */
-    uint32_t reserved[3];
+    int32_t psamples;        /* area light "psamples" (0..64): probes of the
+                                penumbra guess (areaLight_t::guessLight,
+                                arealight.cc:176-198) before the samples; 0 =
+                                every point samples the light.  Probe j of a
+                                point with QMC sample index m looks at grid
+                                point floor(samples * u), u = halton(5,
+                                m*psamples + j) rotated like the light's first
+                                dimension (see yr_render)                    */
+    uint32_t reserved[2];
 } yr_light_desc;
 
 /* Render parameters.  The pixel loop follows scene_t::render(renderArea_t&)

@@ -352,8 +352,8 @@ static light_t *make_light(const yr_light_desc &d) {
     case YR_LIGHT_POINT:
         return new pointLight_t(P3(d.p[0]), C3(d.color), d.power, d.cast_shadows != 0);
     case YR_LIGHT_AREA:
-        return new areaLight_t(P3(d.p[0]), P3(d.p[1]), P3(d.p[2]), P3(d.p[3]), d.samples, C3(d.color), d.power, 0,
-                               false);
+        return new areaLight_t(P3(d.p[0]), P3(d.p[1]), P3(d.p[2]), P3(d.p[3]), d.samples, C3(d.color), d.power,
+                               d.psamples, false);
     case YR_LIGHT_HEMI:
         return new hemiLight_t(d.samples, C3(d.color), d.power, d.maxdist, false, true);
     case YR_LIGHT_PATH:
@@ -856,8 +856,10 @@ static void cmd_cudarender(const SceneFile &s, const char *out, const int *crop,
 //        stream of the state's sampler setStart(m0 * samples); `synced` says
 //        whether each level 0..depth-1 was then advanced exactly `samples`
 //        times (true when no path stops early);
-//   area (arealight.cc:93-174): the global LCG (vector3d.h:262-285) seeded
-//        with `lcg`; the values it hands out are returned in vals[].
+//   area (arealight.cc:93-198): the global LCG (vector3d.h:262-285) seeded
+//        with `lcg`; the values it hands out are returned in vals[], then
+//        the grid points of the penumbra guess's probes (rand() seeded with
+//        `lcg`, arealight.cc:186).
 // Query: u32 light, u32 m0, i32 lcg, f32 eye[3], f32 from[3], f32 dir[3]
 // Output: u32 hit, u32 synced, f32 rgb[3], u32 nvals, f32 vals[64]
 struct IllumRec {
@@ -912,10 +914,16 @@ static void cmd_illum(const SceneFile &s, const char *q_path, const char *out) {
             case YR_LIGHT_AREA: {
                 areaLight_t *al = (areaLight_t *)l;
                 nvals = 2u * (uint32_t)al->samples;
-                if (nvals > 64) die("area light with more than 32 samples");
+                if (nvals + (uint32_t)al->fsamples > 64) die("area light with more than 64 values");
                 myseed = q.lcg;
                 for (uint32_t k = 0; k < nvals; k++) vals[k] = ourRandom();
                 myseed = q.lcg;
+                // the penumbra guess draws its grid points with rand()
+                // (arealight.cc:186): the same seed, the same draws
+                srand((unsigned)q.lcg);
+                for (int k = 0; k < al->fsamples; k++) vals[nvals + k] = (float)(rand() % al->samples);
+                srand((unsigned)q.lcg);
+                nvals += (uint32_t)al->fsamples;
                 break;
             }
             }

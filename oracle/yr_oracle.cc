@@ -1284,6 +1284,37 @@ C illum_point(Scene &S, const Light &L, const SP &sp, const V &eye) {
     return col;
 }
 
+// areaLight_t::guessLight (arealight.cc:176-198): `psamples` probes of
+// unjittered grid points, in order; a probe sees shadow when the point is
+// behind the surface or occluded, light otherwise; the guess stops at the
+// first probe once both were seen.  Probe j of QMC sample index m0 looks at
+// grid point floor(samples * u), u = halton(5, m0*psamples + j) rotated by
+// the light's first dimension (the reference draws rand() % samples); in
+// the pinning queries the grid points come from the reference's draws.
+enum { kGuessShadow = 0, kGuessPenumbra = 1, kGuessLight = 2 };
+int guess_light(Scene &S, const Light &L, const SP &sp, const V &N, uint32_t m0, float r0) {
+    const int F = L.d.psamples;
+    if (F <= 0) return kGuessPenumbra;
+    bool luz = false, sombra = false;
+    for (int j = 0; j < F; j++) {
+        if (luz && sombra) return kGuessPenumbra;
+        int rs;
+        if (S.area_vals) {
+            rs = (int)S.area_vals[2 * L.samples + j];
+        } else {
+            const float u = cp_add(halton(5, m0 * (uint32_t)F + (uint32_t)j), r0);
+            rs = (int)(u * (float)L.samples);
+            if (rs >= L.samples) rs = L.samples - 1;
+        }
+        const V Lv = L.pts[rs] - sp.P;
+        if ((Lv * N) < 0) sombra = true;
+        else if (shadowed_point(S, sp.P, sp.obj, L.pts[rs])) sombra = true;
+        else luz = true;
+    }
+    if (luz && sombra) return kGuessPenumbra;
+    return luz ? kGuessLight : kGuessShadow;
+}
+
 C illum_area(Scene &S, int k, const Light &L, const SP &sp, const V &eye, int v, uint32_t m0, const Ctx &cx) {
     V edir = normalize(eye);
     V N = faceForward(sp.Ng, sp.N, edir);
@@ -1292,6 +1323,20 @@ C illum_area(Scene &S, int k, const Light &L, const SP &sp, const V &eye, int v,
     const uint32_t d = light_dim(k, v);
     const float r0 = rot(S, cx.pixel, d), r1 = rot(S, cx.pixel, d + 1);
     C resul;
+    if (L.samples > 1) {
+        const int g = guess_light(S, L, sp, N, m0, r0);
+        if (g == kGuessShadow) return C();  // fromLight of zero energy
+        if (g == kGuessLight) {
+            // every grid point, unjittered, without a shadow test (arealight.cc:156-166)
+            for (int i = 0; i < L.samples; i++) {
+                V dir = L.pts[i] - sp.P;
+                float ld2 = normLenSqr(dir);
+                ld2 = (ld2 != 0) ? (1.f / ld2) : 1.f;
+                resul = resul + fromLight(S, sp, dir, (L.d.power * L.color) * ld2, eye);
+            }
+            return (plane_at * resul) / (float)L.samples;
+        }
+    }
     for (int i = 0; i < L.samples; i++) {
         const uint32_t m = m0 * (uint32_t)L.samples + (uint32_t)i;
         float h2, h3;

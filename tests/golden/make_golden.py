@@ -236,6 +236,24 @@ def illum():
     np.savez_compressed(os.path.join(HERE, "illum.npz"), **out)
 
 
+def guess_scene():
+    """The illumination scene lit by area lights with the penumbra guess
+    (psamples 4 over a 12-point grid, 6 over 9, 3 over 2): the objects put
+    points in full light, in full shadow and in penumbra."""
+    sc = illum_scene()
+    sc.lights = [scenes.quad_light_down(0.5, 3.0, 0.5, 2.0, 1.5, 3.0, samples=16, color=(1.0, 0.9, 0.8),
+                                        psamples=4),
+                 scenes.quad_light_down(-1.0, 2.5, -0.5, 1.2, 1.2, 2.0, samples=9, psamples=6),
+                 scenes.quad_light_down(1.5, 2.0, -1.0, 0.8, 0.6, 1.5, samples=4, psamples=3)]
+    return sc
+
+
+def illum_guess():
+    sc = guess_scene()
+    q = illum_queries(sc, 900, 21)
+    np.savez_compressed(os.path.join(HERE, "illum_guess.npz"), q=q, o=T.harness_illum(sc, q))
+
+
 def texture_shaders():
     """One shader per texture configuration: every noise basis under clouds,
     the marble / wood shapes and variants, voronoi under every metric and
@@ -548,6 +566,7 @@ if __name__ == "__main__":
     image_outputs()
     instances()
     illum()
+    illum_guess()
     halton_noise()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

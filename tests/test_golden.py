@@ -166,6 +166,35 @@ def test_oracle_light_estimators_match_reference(name):
         assert (ref[q["light"] == k].sum(1) > 0).any()
 
 
+def test_oracle_penumbra_guess_matches_reference():
+    """Area lights with the penumbra guess (psamples > 0): each query's
+    areaLight_t::illuminate in the reference, its guessLight probes drawn
+    by rand() from a seed and its penumbra jitter by the LCG from the same
+    seed, against the oracle given those grid points and jitter values.
+    The queries hold points the guess calls lit, shadowed and penumbra."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    g = load("illum_guess.npz")
+    q, o = g["q"], g["o"]
+    sc = make_golden.guess_scene()
+    hit, rgb = T.OracleScene(sc).illum(q, o["vals"])
+    assert np.array_equal(hit, o["hit"].astype(np.int32))
+    ref = o["rgb"]
+    # within 2e-6 of the query's largest channel: the lit guess sums every
+    # grid point's fromLight, with terms of both signs under a subtracting
+    # modulator, in the shipped build's fast-math order
+    tol = 2e-6 * np.maximum(np.abs(ref).max(1, keepdims=True), 1e-3)
+    assert (np.abs(rgb - ref) <= tol).all(), np.abs(rgb - ref).max()
+    # all three outcomes of the guess occur among the lit-side queries
+    lit = ref.sum(1) > 0
+    assert lit.sum() > 100 and (hit.astype(bool) & ~lit).sum() > 20
+    # the guess matters: without it the same queries differ
+    for l in sc.lights:
+        l.psamples = 0
+    _, plain = T.OracleScene(sc).illum(q, o["vals"])
+    assert np.abs(plain - ref).max() > 1e-3
+
+
 def test_oracle_noise_bases_match_reference():
     """Every noise basis of newNoise (stdperlin, blender, voronoi F1-F4 /
     F2-F1 / crackle, cellnoise, newperlin), turbulence over each (soft and

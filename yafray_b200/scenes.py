@@ -285,7 +285,9 @@ def point_light(pos, power=1.0, color=(1.0, 1.0, 1.0), cast_shadows=True) -> abi
     return l
 
 
-def area_light(a, b, c, d, power=1.0, samples=16, color=(1.0, 1.0, 1.0)) -> abi.YrLightDesc:
+def area_light(a, b, c, d, power=1.0, samples=16, color=(1.0, 1.0, 1.0), psamples=0) -> abi.YrLightDesc:
+    """areaLight_t: corners a, b, c, d; `psamples` probes of the penumbra
+    guess (0 = off, the factory's default)."""
     l = abi.YrLightDesc()
     l.type = abi.YR_LIGHT_AREA
     l.color[:] = [float(x) for x in color]
@@ -294,16 +296,17 @@ def area_light(a, b, c, d, power=1.0, samples=16, color=(1.0, 1.0, 1.0)) -> abi.
         l.p[i][:] = [float(x) for x in p]
     l.samples = int(samples)
     l.cast_shadows = 1
+    l.psamples = int(psamples)
     return l
 
 
-def quad_light_down(cx, y, cz, w, h, power, samples=16, color=(1.0, 1.0, 1.0)) -> abi.YrLightDesc:
+def quad_light_down(cx, y, cz, w, h, power, samples=16, color=(1.0, 1.0, 1.0), psamples=0) -> abi.YrLightDesc:
     """Horizontal quad at height y facing down ((b-a)x(d-a) points to -y)."""
     a = (cx - w / 2, y, cz - h / 2)
     b = (cx + w / 2, y, cz - h / 2)
     c = (cx + w / 2, y, cz + h / 2)
     d = (cx - w / 2, y, cz + h / 2)
-    return area_light(a, b, c, d, power, samples, color)
+    return area_light(a, b, c, d, power, samples, color, psamples)
 
 
 def hemi_light(samples=16, power=1.0, color=(1.0, 1.0, 1.0), maxdist=-1.0) -> abi.YrLightDesc:
