@@ -211,6 +211,48 @@ def test_render_specular_hardness_modulation(cuda):
     _cmp(img, ref, O)
 
 
+@pytest.mark.parametrize("gi", [False, True])
+def test_render_penumbra_guess(cuda, gi):
+    """Area lights that guess the penumbra first (psamples 4, 6 and 3):
+    the probes, the decision (lit: every grid point without a shadow ray;
+    shadow: nothing; penumbra: the jittered samples) at the camera hit and,
+    with a 2-bounce path light, at every path vertex."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.guess_scene()
+    sc.render.spp = 2
+    if gi:
+        sc.lights.append(scenes.path_light(samples=1, depth=2, power=1.0))
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref, O)
+    # the guess changes the image
+    for l in sc.lights:
+        l.psamples = 0
+    assert np.abs(api.DeviceScene(sc).render() - img).max() > 1e-3
+
+
+def test_render_penumbra_guess_batch(cuda):
+    """The batched renderer on scenes with the penumbra guess (waves
+    schedule): each image equals yr_render's."""
+    import torch
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    scs = [make_golden.guess_scene(), scenes.config_small(64, 48)]
+    scs[0].render.spp = 2
+    dss = [api.DeviceScene(sc) for sc in scs]
+    outs = [torch.zeros((sc.resy, sc.resx, 4), dtype=torch.float32, device="cuda") for sc in scs]
+    api.render_batch(dss, [o.data_ptr() for o in outs])
+    torch.cuda.synchronize()
+    for d, o in zip(dss, outs):
+        assert np.array_equal(o.cpu().numpy().view(np.uint32), d.render().view(np.uint32))
+
+
 def test_render_texture_board(cuda):
     """All 95 texture configurations of the golden texture set, one quad
     each (per-triangle materials)."""

@@ -619,8 +619,15 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
         cudaMemcpy(C.d_outs, C.outs.data(), sizeof(float *) * count, cudaMemcpyHostToDevice);
         if (C.lanes_n) C.drop_graph();  // the waves graph holds the image pointers
     }
+    // the tiles kernel runs each vertex's light sampling in one stage: a
+    // scene whose area lights guess the penumbra first takes the waves
+    bool guess = false;
+    for (uint32_t i = 0; i < count; i++) guess = guess || scenes[i]->rdr.has_guess;
+    if (guess && want_mode == YR_BATCH_TILES) return done(YR_ERR_UNSUPPORTED);
+    const int mode_wanted = guess ? YR_BATCH_WAVES : want_mode;
     BatchConfig cfg;
-    const bool explicit_tiles = params && params->block_size > 0 && params->queue_tile > 0 && want_mode != YR_BATCH_WAVES;
+    const bool explicit_tiles = !guess && params && params->block_size > 0 && params->queue_tile > 0 &&
+                                want_mode != YR_BATCH_WAVES;
     const bool explicit_waves = params && want_mode == YR_BATCH_WAVES && params->streams > 0;
     if (explicit_tiles) {
         cfg.mode = YR_BATCH_TILES;
@@ -637,9 +644,9 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
         cfg.mode = YR_BATCH_WAVES;
         cfg.streams = std::min<int>(params->streams, (int)count);
     } else {
-        if (!C.tuned.mode || (want_mode && C.tuned.mode != want_mode)) {
+        if (!C.tuned.mode || (mode_wanted && C.tuned.mode != mode_wanted)) {
             BatchConfig t;
-            if ((ret = autotune(C, st, want_mode, t)) != YR_OK) return done(ret);
+            if ((ret = autotune(C, st, mode_wanted, t)) != YR_OK) return done(ret);
             C.tuned = t;
         }
         cfg = C.tuned;

@@ -184,9 +184,34 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_primary(DevSce
 }
 #endif
 
+// sample slots of a light at one vertex (a point light's one, an area or
+// hemi light's samples); the penumbra guess's probe slots come after all
+__device__ __forceinline__ uint32_t light_slots(const DevLight &L) {
+    if (L.type == YR_LIGHT_POINT) return 1;
+    if (L.type == YR_LIGHT_AREA || L.type == YR_LIGHT_HEMI) return (uint32_t)L.samples;
+    return 0;
+}
+
+// Grid point of probe j of the penumbra guess (areaLight_t::guessLight,
+// arealight.cc:176-198, which draws rand() % samples): floor(samples * u),
+// u = halton(5, m0*psamples + j) rotated like the light's first dimension.
+__device__ __forceinline__ int guess_point(const DevLight &L, uint32_t m0, int j, float r0) {
+    const float u = cp_add(halton(5, m0 * (uint32_t)L.psamples + (uint32_t)j), r0);
+    const int rs = (int)(u * (float)L.samples);
+    return rs < L.samples ? rs : L.samples - 1;
+}
+
+enum GuessStatus { kGuessShadow = 0, kGuessPenumbra = 1, kGuessLight = 2 };
+
 // per-light sampling at one shading vertex; writes slots, aux and queue
 // entries.  vtx = vertex index for slots/aux, v = QMC vertex level,
 // m0 = QMC sample index of this vertex.
+// Area lights with a penumbra guess (psamples > 0) take two stages:
+// stage 0 queues the guess's probe rays (and does every other light);
+// stage 1, once the probes are answered, decides each guess light
+// (guessLight's order, with its early stop once light and shadow were
+// both seen) and queues the light's sample rays in penumbra, or counts every
+// grid point lit without a shadow ray, or none in shadow.
 // ADJ (adjoint recompute): slot_c / slot_s receive the diffuse and specular
 // factors per unit light power instead of the light sample's colour, hemi
 // aux holds (diffuse factor, specular factor, 0, go), and the vertex's
@@ -195,7 +220,7 @@ template <bool ADJ = false>
 __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender &R, const Wave &W, bool active,
                                              const Surf &sp, const V3 &eye, uint32_t vtx, int v, uint32_t m0,
                                              uint32_t pixel, float4 *aux, float4 *slot_s = nullptr,
-                                             C3 *lkc_out = nullptr, TexDeriv *td_out = nullptr) {
+                                             C3 *lkc_out = nullptr, TexDeriv *td_out = nullptr, int stage = 0) {
     DevShader sh;
     C3 lkc = c3(0.f, 0.f, 0.f);
     if (active) {
@@ -218,6 +243,11 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
     uint32_t off = 0;
     for (int k = 0; k < R.nlights; k++) {
         const DevLight L = R.lights[k];
+        const bool guess = !ADJ && L.type == YR_LIGHT_AREA && L.psamples > 0;
+        if (stage == 1 && !guess) {  // the second stage handles the guessing lights only
+            off += light_slots(L);
+            continue;
+        }
         if (L.type == YR_LIGHT_POINT) {
             const uint32_t slot = vtx * W.ns + off;
             bool emit = false;
@@ -252,25 +282,80 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             emit_shadow(W, emit, sp.P, sp.object, rdir, dist, slot);
             off += 1;
         } else if (L.type == YR_LIGHT_AREA) {
-            // areaLight_t::illuminate (arealight.cc:93-174), penumbra branch
-            // (psamples = 0) with explicit QMC jitter
+            // areaLight_t::illuminate (arealight.cc:93-174): the penumbra
+            // branch with explicit QMC jitter; with psamples > 0 the guess
+            // (arealight.cc:176-198) decides it first
             float plane_at = 0.f;
             bool lit_side = false;
             if (active) {
                 plane_at = dot(sp.P - L.from, L.direction);
                 lit_side = plane_at > 0.f;
-                aux[vtx * R.nlights + k] = make_float4(plane_at, lit_side ? 1.f : 0.f, 0.f, 0.f);
+                if (stage == 0) aux[vtx * R.nlights + k] = make_float4(plane_at, lit_side ? 1.f : 0.f, 0.f, 0.f);
             }
             const uint32_t d = light_dim(k, v);
             const float r0 = cp_rot(R.seed, pixel, d), r1 = cp_rot(R.seed, pixel, d + 1);
+            if (guess && stage == 0) {
+                // the guess's probes: unjittered grid points; a point behind
+                // the surface counts as shadow without a ray
+                for (int j = 0; j < L.psamples; j++) {
+                    const uint32_t slot = vtx * W.ns + (uint32_t)L.probe_off + (uint32_t)j;
+                    bool emit = false;
+                    V3 rdir;
+                    float dist = 0.f;
+                    if (active) {
+                        W.slot_f[slot] = kSlotNone;
+                        if (lit_side) {
+                            const float *pt = R.area_pts + 9 * (size_t)(L.pt_base + guess_point(L, m0, j, r0));
+                            const V3 gp = v3(pt[0], pt[1], pt[2]);
+                            if (dot(gp - sp.P, N) < 0.f) {
+                                W.slot_f[slot] = kSlotShadowed;
+                            } else {
+                                rdir = gp - sp.P;
+                                dist = length(rdir);
+                                rdir = normalize(rdir);
+                                emit = true;
+                                W.slot_f[slot] = kSlotPending;
+                            }
+                        }
+                    }
+                    emit_shadow(W, emit, sp.P, sp.object, rdir, dist, slot);
+                }
+                if (active)
+                    for (int jj = 0; jj < L.samples; jj++) W.slot_f[vtx * W.ns + off + (uint32_t)jj] = kSlotNone;
+                off += (uint32_t)L.samples;
+                continue;
+            }
+            int status = kGuessPenumbra;
+            if (guess && active && lit_side) {
+                bool luz = false, sombra = false;
+                int decided = -1;
+                for (int j = 0; j < L.psamples; j++) {
+                    if (luz && sombra) {
+                        decided = kGuessPenumbra;
+                        break;
+                    }
+                    if (W.slot_f[vtx * W.ns + (uint32_t)L.probe_off + (uint32_t)j] == kSlotLit) luz = true;
+                    else sombra = true;
+                }
+                status = decided >= 0 ? decided : ((luz && sombra) ? kGuessPenumbra : (luz ? kGuessLight : kGuessShadow));
+            }
             for (int jj = 0; jj < L.samples; jj++) {
                 const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
                 bool emit = false;
                 V3 rdir;
                 float dist = 0.f;
-                if (active) {
+                if (active && status == kGuessLight) {
+                    // every grid point, unjittered, no shadow test (arealight.cc:156-166)
+                    const float *pt = R.area_pts + 9 * (size_t)(L.pt_base + jj);
+                    V3 dir = v3(pt[0], pt[1], pt[2]) - sp.P;
+                    float ld2 = norm_len_sqr(dir);
+                    ld2 = (ld2 != 0.f) ? (1.f / ld2) : 1.f;
+                    const C3 c = from_light(sh, lkc, pre, dir, (L.power * L.color) * ld2);
+                    W.slot_c[slot] = make_float4(c.r, c.g, c.b, 0.f);
+                    W.slot_f[slot] = kSlotLit;
+                } else if (active) {
                     W.slot_f[slot] = kSlotNone;
-                    if (lit_side) {
+                    if (lit_side && status == kGuessPenumbra) {
                         const uint32_t m = m0 * (uint32_t)L.samples + (uint32_t)jj;
                         const float h2 = cp_add(halton(2, m), r0), h3 = cp_add(halton(3, m), r1);
                         V3 sampleP;
@@ -400,12 +485,6 @@ __device__ __forceinline__ C3 gather_term(const DevRender &R, const Wave &W, con
         return (L.sampdiv * total) * c3(a.x, a.y, a.z);
     }
     return c3(0.f, 0.f, 0.f);
-}
-
-__device__ __forceinline__ uint32_t light_slots(const DevLight &L) {
-    if (L.type == YR_LIGHT_POINT) return 1;
-    if (L.type == YR_LIGHT_AREA || L.type == YR_LIGHT_HEMI) return (uint32_t)L.samples;
-    return 0;
 }
 
 // whole warp
@@ -837,11 +916,84 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
             const V3 nr = cos_hemi_dir(HN, sp.NU, sp.NV, z1, z2);
             W.p_nray[p] = make_float4(nr.x, nr.y, nr.z, 0.f);
         }
-        W.p_where[p] = make_float4(sp.P.x, sp.P.y, sp.P.z, W.p_where[p].w);
+        // with a penumbra guess the guess stage needs the bounce origin
+        // still: it moves the path there itself
+        if (!R.has_guess) W.p_where[p] = make_float4(sp.P.x, sp.P.y, sp.P.z, W.p_where[p].w);
     }
 }
 
+// The penumbra guess's second stage at the camera vertex of sample i (whole
+// warp): the vertex is set up again as st_shade_camera does, and the
+// guessing area lights are decided from their answered probes.
+__device__ __forceinline__ void st_guess_camera(const DevScene &S, const DevRender &R, const Wave &W, uint32_t i) {
+    const bool inb = i < W.count;
+    const uint32_t cs = W.base + (inb ? i : 0);
+    int x, y;
+    const uint32_t pixel = cs_pixel(R, cs, x, y), s = cs % R.spp;
+    bool active = false;
+    Surf sp;
+    V3 eye = v3(0.f, 0.f, 0.f);
+    if (inb) {
+        const float4 h = W.hit0[i];
+        const int obj = __float_as_int(h.y);
+        if (obj >= 0) {
+            float fx, fy;
+            sample_pos(R, pixel, s, fx, fy);
+            const V3 ray = camera_ray(R.cam, (float)x + fx, (float)y + fy);
+            const V3 f = R.cam.pos + ray * kMinRayDist;
+            sp = make_surface(S, R, obj, __float_as_uint(h.z), h.x, f, ray);
+            eye = R.cam.pos - sp.P;
+            active = true;
+        }
+    }
+    shade_lights(S, R, W, active, sp, eye, inb ? i : 0, 0, s, pixel, W.aux, nullptr, nullptr, nullptr, 1);
+}
+
+// The same at path vertex j (bounce queue entry q, whole warp); it then
+// moves the path to the vertex, as st_shade_path does without a guess.
+__device__ __forceinline__ void st_guess_path(const DevScene &S, const DevRender &R, const Wave &W, int j, uint32_t q,
+                                              uint32_t n) {
+    const bool inq = q < n;
+    const uint32_t p = inq ? W.bq[q] : 0;
+    const uint32_t i = p / W.npath, pi = p % W.npath;
+    const uint32_t cs = W.base + i;
+    int px_x, px_y;
+    const uint32_t pixel = cs_pixel(R, cs, px_x, px_y), s = cs % R.spp;
+    bool active = false;
+    Surf sp;
+    V3 eye = v3(0.f, 0.f, 0.f);
+    float4 wh = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (inq) {
+        const float4 h = W.p_hit[p];
+        const int obj = __float_as_int(h.y);
+        wh = W.p_where[p];
+        const float4 rr = W.p_ray[p];
+        const V3 ray = v3(rr.x, rr.y, rr.z);
+        if (obj >= 0) {
+            const V3 f = v3(wh.x, wh.y, wh.z) + ray * kMinRayDist;
+            sp = make_surface(S, R, obj, __float_as_uint(h.z), h.x, f, ray);
+            eye = (sp.P + (-ray)) - sp.P;
+            active = true;
+        }
+    }
+    shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux, nullptr, nullptr, nullptr, 1);
+    if (active) W.p_where[p] = make_float4(sp.P.x, sp.P.y, sp.P.z, wh.w);
+}
+
 #ifdef YR_WAVE_KERNELS
+static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_guess_camera(DevScene S, DevRender R, Wave W) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W.count && (i & ~31u) >= W.count) return;  // whole warps past the end leave
+    st_guess_camera(S, R, W, i);
+}
+
+static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_guess_path(DevScene S, DevRender R, Wave W, int j) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = W.counters[1];
+    if (q >= n && (q & ~31u) >= n) return;
+    st_guess_path(S, R, W, j, q, n);
+}
+
 static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_shade_path(DevScene S, DevRender R, Wave W, int j) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = W.counters[1];
@@ -1035,6 +1187,7 @@ inline yr_status make_plan(const yr_scene *scene, Plan &P) {
     for (const DevLight &L : scene->lights) {
         if (L.type == YR_LIGHT_POINT) P.ns += 1;
         else if (L.type == YR_LIGHT_AREA || L.type == YR_LIGHT_HEMI) P.ns += (uint32_t)L.samples;
+        P.ns += (uint32_t)L.psamples;  // the penumbra guess's probe slots, after the sample slots
     }
     P.npath = R.path_light >= 0 ? (uint32_t)R.path_samples : 0;
     P.nl = (uint32_t)std::max(1, R.nlights);

@@ -107,6 +107,15 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
     timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
     cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
     timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+    if (R.has_guess) {
+        // the penumbra guess decided from its probes, then the sample rays
+        // of the points in penumbra
+        cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
+        timed(YR_K_SHADE_CAMERA, [&] { k_guess_camera<<<g, kBlock, 0, st>>>(D, R, W); });
+        timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
+        cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
+        timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+    }
     timed(YR_K_GATHER, [&] { k_gather_camera<<<g, kBlock, 0, st>>>(R, W); });
     if (npath > 0) {
         const size_t nc = (size_t)W.count * npath * P.depth;
@@ -123,6 +132,13 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
             timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
             cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
             timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+            if (R.has_guess) {
+                cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
+                timed(YR_K_SHADE_PATH, [&] { k_guess_path<<<gp, kBlock, 0, st>>>(D, R, W, j); });
+                timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
+                cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);
+                timed(YR_K_SHADOW, [&] { k_shadow<<<gq, kBlock, 0, st>>>(D, W, R.self_bias); });
+            }
             timed(YR_K_GATHER, [&] { k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background); });
             std::swap(W.bq, W.bq2);
             timed(YR_K_OTHER, [&] { k_swap_queues<<<1, 1, 0, st>>>(W); });

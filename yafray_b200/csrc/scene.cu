@@ -241,6 +241,9 @@ yr_status make_lights(const std::vector<yr_light_desc> &in, std::vector<DevLight
         case YR_LIGHT_AREA: {
             yr_status st = fill_quad(d, L, pts);
             if (st != YR_OK) return st;
+            if (d.psamples < 0 || d.psamples > 64) return YR_ERR_INVALID_ARG;
+            // the guess runs only with more than one sample (arealight.cc:115-134)
+            L.psamples = L.samples > 1 ? d.psamples : 0;
             const V3 a = hv(d.p[0]), b = hv(d.p[1]), c = hv(d.p[2]), dd = hv(d.p[3]);
             L.direction = h_normalize(cross(b - a, dd - a));
             L.from = (((a + b) + c) + dd) * 0.25f;
@@ -261,6 +264,15 @@ yr_status make_lights(const std::vector<yr_light_desc> &in, std::vector<DevLight
         }
         out.push_back(L);
     }
+    // probe slots of a vertex follow its sample slots
+    int ns = 0;
+    for (const DevLight &L : out)
+        ns += L.type == YR_LIGHT_POINT ? 1 : (L.type == YR_LIGHT_AREA || L.type == YR_LIGHT_HEMI ? L.samples : 0);
+    for (DevLight &L : out)
+        if (L.psamples > 0) {
+            L.probe_off = ns;
+            ns += L.psamples;
+        }
     return YR_OK;
 }
 
@@ -781,6 +793,9 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     R.tri_shader = d_tri_shader;
     R.nlights = (int)s->lights.size();
     R.nshaders = (int)s->shaders.size();
+    R.has_guess = 0;
+    for (const DevLight &L : s->lights)
+        if (L.psamples > 0) R.has_guess = 1;
     R.spp = desc->render.spp ? desc->render.spp : 1;
     R.pw = desc->render.aa_pixelwidth;
     R.totsamdiv = R.spp > 1 ? (float)(1.0 / (float)(R.spp - 1)) : 0.f;

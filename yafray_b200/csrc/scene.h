@@ -52,8 +52,9 @@ struct DevLight {
     float maxdist;       // hemi
     float sampdiv;       // hemi: power/samples
     int pt_base;         // area: first entry in DevRender::area_pts
-    int pad;
+    int psamples;        // area: probes of the penumbra guess (0: none)
     C3 rawc;             // the light's "color" parameter (before any power scale)
+    int probe_off;       // area with psamples: first probe slot of a vertex
 };
 
 struct DevCamera {
@@ -85,6 +86,7 @@ struct DevRender {
     int premultiply;            // YR_RENDER_ALPHA_PREMULTIPLY
     float exposure;             // scene_t::exposure = -"exposure"
     float gamma_r;              // scene_t::gamma_R = 1/"gamma" (0 for gamma 0)
+    int has_guess;              // some area light guesses the penumbra first (psamples > 0)
 };
 
 // Device allocation tracked by the scene (freed in yr_scene_destroy).
