@@ -358,14 +358,28 @@ extern "C" YR_API yr_status yr_render_progressive(yr_scene *scene, float *rgba, 
     for (uint64_t b = 0; b < P.total && R.raydepth > 0 && !stop; b += wcap) {
         wave_launch(scene, P, wcap, W, G, b, st, no_timing);
         if (cudaGetLastError() != cudaSuccess) return done(YR_ERR_CUDA);
-        // the wave's pixels, region pixels [b/spp, (b+count)/spp): copy the
-        // image rows they lie on, then hand them to the caller
+        // the wave's pixels, region pixels [b/spp, (b+count)/spp): copy
+        // exactly those (row segments of the region), then hand them over
         const uint32_t p0 = (uint32_t)(b / R.spp);
         const uint32_t p1 = (uint32_t)(std::min<uint64_t>(P.total, b + wcap) / R.spp);
-        const int y0 = R.ry0 + (int)(p0 / (uint32_t)R.rw), y1 = R.ry0 + (int)((p1 - 1) / (uint32_t)R.rw);
-        if (cudaMemcpyAsync((char *)rgba + row * y0, (char *)out + row * y0, row * (size_t)(y1 - y0 + 1),
-                            cudaMemcpyDeviceToHost, st) != cudaSuccess)
-            return done(YR_ERR_CUDA);
+        for (uint32_t p = p0; p < p1;) {
+            const uint32_t ry = p / (uint32_t)R.rw, rx = p % (uint32_t)R.rw;
+            const uint32_t n = std::min<uint32_t>(p1 - p, (uint32_t)R.rw - rx);
+            const size_t at = sizeof(float) * 4 * ((size_t)(R.ry0 + ry) * R.cam.resx + R.rx0 + rx);
+            if (rx == 0 && n == (uint32_t)R.rw && p1 - p >= 2 * (uint32_t)R.rw) {
+                // whole region rows: one strided copy
+                const uint32_t rows = (p1 - p) / (uint32_t)R.rw;
+                if (cudaMemcpy2DAsync((char *)rgba + at, row, (char *)out + at, row, sizeof(float) * 4 * R.rw, rows,
+                                      cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                    return done(YR_ERR_CUDA);
+                p += rows * (uint32_t)R.rw;
+                continue;
+            }
+            if (cudaMemcpyAsync((char *)rgba + at, (char *)out + at, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost,
+                                st) != cudaSuccess)
+                return done(YR_ERR_CUDA);
+            p += n;
+        }
         if ((ret = take_status(scene, st)) != YR_OK) return done(ret);  // waits for the copy too
         next = (uint64_t)p1 * R.spp;
         stop = on_pixels(user, p0, p1 - p0) == 0;
