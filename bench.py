@@ -706,6 +706,20 @@ def main():
                 "peak_source": peak_src,
                 "nodes_per_ray": agg["knodes"][dom] / max(1.0, agg["krays"][dom]),
                 "tests_per_ray": agg["ktests"][dom] / max(1.0, agg["krays"][dom])}
+    # the traversal is bound by instruction issue, not by HBM: the same
+    # kernel against the SMs' issue rate (one warp instruction per clock per
+    # sub-partition, 4 per SM), with warp instructions per ray and lanes per
+    # warp instruction from the ncu capture of the kernel (profiles/)
+    if isinstance(tinfo, dict) and "warp_inst_per_ray" in tinfo:
+        props = __import__("torch").cuda.get_device_properties(local)
+        mhz = clk.get("sm_mhz") or 1965.0
+        issue_peak = props.multi_processor_count * 4 * mhz * 1e6 / 1e9   # G warp instructions/s
+        rays_s = agg["krays"][dom] / (kms[dom] / 1000.0) if kms[dom] > 0 else 0.0
+        achieved_issue = float(tinfo["warp_inst_per_ray"]) * rays_s / 1e9
+        roofline["issue"] = {"achieved": achieved_issue, "peak": issue_peak, "unit": "G warp inst/s",
+                             "frac": achieved_issue / issue_peak, "warp_inst_per_ray": tinfo["warp_inst_per_ray"],
+                             "threads_per_warp_inst": tinfo.get("threads_per_warp_inst"),
+                             "source": tinfo.get("issue_source")}
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,

@@ -21,6 +21,9 @@ constexpr int kBlock = 128;
 #ifndef YR_SHADE_MINB
 #define YR_SHADE_MINB 6  // minimum resident blocks per SM for the shading kernels (80 registers)
 #endif
+#ifndef YR_SHADOW_REFILL
+#define YR_SHADOW_REFILL 1  // shadow queues on the casters' BVH use the refilling walk (k_trace_shadow_refill)
+#endif
 #ifndef YR_SHADOW_TREE_REFILL
 #define YR_SHADOW_TREE_REFILL 1  // shadow queues on the shadow-ray tree use the refilling walk (k_trace_shadow_tree)
 #endif
@@ -601,6 +604,90 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q
         rays++;
     }
 #endif
+    count_work(W, YR_K_SHADOW, rays, nodes, tests);
+}
+#endif
+
+#ifdef YR_WAVE_KERNELS
+// The shadow queue on the shadow casters' BVH (scene_occluded_bvh's walk),
+// with lanes that never wait for the others' rays: each loop step takes
+// every lane through one candidate object (its kd walk, IntersectS from the
+// object's origin, the exact bound check on a hit, then the BVH walk on to
+// the next candidate), and a lane whose ray is answered takes the next
+// queue entry at the next step (one atomic per warp for all lanes that
+// need one).  The answers are scene_occluded_bvh's.
+template <bool INST>
+static __global__ void __launch_bounds__(kBlock, 8) k_trace_shadow_refill(DevScene S, Wave W, float self_bias) {
+    uint2 stk_nt[kKdStackCap];
+    float stk_split[kKdStackCap];
+    const KdStack stk{stk_nt, stk_split, kKdStackCap};
+    const uint32_t n = W.counters[0];
+    const unsigned lane = threadIdx.x & 31u;
+    bool live = false, drained = false;
+    uint32_t q = 0;
+    int own = -1;
+    float dist = 0.f;
+    V3 self = v3(0.f, 0.f, 0.f), p2 = self;
+    RayR ray;
+    ray.d = self;
+    ray.inv = self;
+    ObjRay oray;
+    ObjIter it;
+    it.current = -1;
+    it.sp = 0;
+    uint32_t rays = 0, nodes = 0, tests = 0;
+    for (;;) {
+        if (!drained) {
+            const unsigned need = __ballot_sync(0xffffffffu, !live);
+            if (need) {
+                const int leader = __ffs(need) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(&W.counters[6], (uint32_t)__popc(need));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (uint32_t)__popc(need) >= n) drained = true;  // the same on every lane
+                if (!live) {
+                    q = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                    if (q < n) {
+                        const float4 a = W.shq0[q], b = W.shq1[q];
+                        const V3 p = v3(a.x, a.y, a.z);
+                        own = __float_as_int(a.w);
+                        ray = make_rayr(v3(b.x, b.y, b.z));
+                        dist = b.w;
+                        rays++;
+                        self = p + ray.d * self_bias;
+                        p2 = p + ray.d * kMinRayDist;
+                        oray = make_objray(p2, ray, S.coord_max, false);
+                        it.start_tree(S, S.sonodes, S.sotb, S.soroot, S.nsotree, oray, dist);
+                        if (it.current >= 0) live = true;
+                        else W.slot_f[W.shq_slot[q]] = kSlotLit;  // no casting object on its way
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, live)) {
+            if (drained) break;
+            continue;
+        }
+        if (!live) continue;
+        // one candidate object of this lane's ray
+        const int o = it.current;
+        const DevObject &obj = S.objects[o];
+        float Z = dist;
+        KdResult r{kNone, 0, 0};
+        const bool h = shoot_any<INST>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
+        nodes += r.nodes;
+        tests += r.tests;
+        bool occluded = false;
+        if (h) {
+            float w;
+            occluded = box_where(obj.ob, obj.ob + 3, p2, ray, dist, w);
+        }
+        if (!occluded) it.next(S, oray);
+        if (occluded || it.current < 0) {
+            W.slot_f[W.shq_slot[q]] = occluded ? kSlotShadowed : kSlotLit;
+            live = false;
+        }
+    }
     count_work(W, YR_K_SHADOW, rays, nodes, tests);
 }
 #endif
