@@ -21,12 +21,6 @@ constexpr int kBlock = 128;
 #ifndef YR_SHADE_MINB
 #define YR_SHADE_MINB 6  // minimum resident blocks per SM for the shading kernels (80 registers)
 #endif
-#ifndef YR_SHADOW_REFILL
-#define YR_SHADOW_REFILL 1  // shadow queues on the casters' BVH use the refilling walk (k_trace_shadow_refill)
-#endif
-#ifndef YR_SHADOW_TREE_REFILL
-#define YR_SHADOW_TREE_REFILL 1  // shadow queues on the shadow-ray tree use the refilling walk (k_trace_shadow_tree)
-#endif
 #ifndef YR_TRACE_MINB
 #define YR_TRACE_MINB 10  // minimum resident blocks per SM for the traversal kernels (48 registers)
 #endif
@@ -604,280 +598,6 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q
         rays++;
     }
 #endif
-    count_work(W, YR_K_SHADOW, rays, nodes, tests);
-}
-#endif
-
-#ifdef YR_WAVE_KERNELS
-// The shadow queue on the shadow casters' BVH (scene_occluded_bvh's walk),
-// with lanes that never wait for the others' rays: each loop step takes
-// every lane through one candidate object (its kd walk, IntersectS from the
-// object's origin, the exact bound check on a hit, then the BVH walk on to
-// the next candidate), and a lane whose ray is answered takes the next
-// queue entry at the next step (one atomic per warp for all lanes that
-// need one).  The answers are scene_occluded_bvh's.
-template <bool INST>
-static __global__ void __launch_bounds__(kBlock, 8) k_trace_shadow_refill(DevScene S, Wave W, float self_bias) {
-    uint2 stk_nt[kKdStackCap];
-    float stk_split[kKdStackCap];
-    const KdStack stk{stk_nt, stk_split, kKdStackCap};
-    const uint32_t n = W.counters[0];
-    const unsigned lane = threadIdx.x & 31u;
-    bool live = false, drained = false;
-    uint32_t q = 0;
-    int own = -1;
-    float dist = 0.f;
-    V3 self = v3(0.f, 0.f, 0.f), p2 = self;
-    RayR ray;
-    ray.d = self;
-    ray.inv = self;
-    ObjRay oray;
-    ObjIter it;
-    it.current = -1;
-    it.sp = 0;
-    uint32_t rays = 0, nodes = 0, tests = 0;
-    for (;;) {
-        if (!drained) {
-            const unsigned need = __ballot_sync(0xffffffffu, !live);
-            if (need) {
-                const int leader = __ffs(need) - 1;
-                uint32_t base = 0;
-                if ((int)lane == leader) base = atomicAdd(&W.counters[6], (uint32_t)__popc(need));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (base + (uint32_t)__popc(need) >= n) drained = true;  // the same on every lane
-                if (!live) {
-                    q = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                    if (q < n) {
-                        const float4 a = W.shq0[q], b = W.shq1[q];
-                        const V3 p = v3(a.x, a.y, a.z);
-                        own = __float_as_int(a.w);
-                        ray = make_rayr(v3(b.x, b.y, b.z));
-                        dist = b.w;
-                        rays++;
-                        self = p + ray.d * self_bias;
-                        p2 = p + ray.d * kMinRayDist;
-                        oray = make_objray(p2, ray, S.coord_max, false);
-                        it.start_tree(S, S.sonodes, S.sotb, S.soroot, S.nsotree, oray, dist);
-                        if (it.current >= 0) live = true;
-                        else W.slot_f[W.shq_slot[q]] = kSlotLit;  // no casting object on its way
-                    }
-                }
-            }
-        }
-        if (!__any_sync(0xffffffffu, live)) {
-            if (drained) break;
-            continue;
-        }
-        if (!live) continue;
-        // one candidate object of this lane's ray
-        const int o = it.current;
-        const DevObject &obj = S.objects[o];
-        float Z = dist;
-        KdResult r{kNone, 0, 0};
-        const bool h = shoot_any<INST>(S, obj, (o == own) ? self : p2, ray, dist, Z, r, stk);
-        nodes += r.nodes;
-        tests += r.tests;
-        bool occluded = false;
-        if (h) {
-            float w;
-            occluded = box_where(obj.ob, obj.ob + 3, p2, ray, dist, w);
-        }
-        if (!occluded) it.next(S, oray);
-        if (occluded || it.current < 0) {
-            W.slot_f[W.shq_slot[q]] = occluded ? kSlotShadowed : kSlotLit;
-            live = false;
-        }
-    }
-    count_work(W, YR_K_SHADOW, rays, nodes, tests);
-}
-#endif
-
-#ifdef YR_WAVE_KERNELS
-// The shadow queue answered with the shadow-ray tree (scene_occluded_merged's
-// walk), restructured so that no lane waits for the others' rays: each loop
-// step takes every lane one leaf further (descend to the next leaf, test its
-// triangles, pop), and a lane whose ray is answered takes the next queue
-// entry at the next step (one atomic per warp for all lanes that need one).
-// The answers are scene_occluded_merged's: the same walk per ray, only
-// interleaved differently across the lanes.
-static __global__ void __launch_bounds__(kBlock, 8) k_trace_shadow_tree(DevScene S, Wave W, float self_bias) {
-    uint2 stk_nt[kKdStackCap];
-    float stk_split[kKdStackCap];
-    const uint32_t n = W.counters[0];
-    const unsigned lane = threadIdx.x & 31u;
-    const bool self_first = self_bias < kMinRayDist;
-    bool live = false, drained = false;
-    uint32_t q = 0, curr = 0, leaves = 0;
-    int own = -1, sp = 0;
-    float dist = 0.f, tdist = 0.f, en_t = 0.f, ex_t = 0.f;
-    V3 self = v3(0.f, 0.f, 0.f), p2 = self, ray = self;
-    float fr[3] = {0.f, 0.f, 0.f}, rr[3] = {0.f, 0.f, 0.f}, inv[3] = {0.f, 0.f, 0.f};
-    float en_pb[3] = {0.f, 0.f, 0.f}, ex_pb[3] = {0.f, 0.f, 0.f};
-    uint32_t rays = 0, nodes = 0, tests = 0;
-    for (;;) {
-        if (!drained) {
-            // lanes without a ray take the next queue entries
-            const unsigned need = __ballot_sync(0xffffffffu, !live);
-            if (need) {
-                const int leader = __ffs(need) - 1;
-                uint32_t base = 0;
-                if ((int)lane == leader) base = atomicAdd(&W.counters[6], (uint32_t)__popc(need));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (base + (uint32_t)__popc(need) >= n) drained = true;  // the same on every lane
-                if (!live) {
-                    q = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                    if (q < n) {
-                        const float4 a = W.shq0[q], b = W.shq1[q];
-                        const V3 p = v3(a.x, a.y, a.z);
-                        own = __float_as_int(a.w);
-                        ray = v3(b.x, b.y, b.z);
-                        dist = b.w;
-                        rays++;
-                        self = p + ray * self_bias;
-                        p2 = p + ray * kMinRayDist;
-                        const V3 o = self_first ? self : p2;
-                        tdist = (dist + fabsf(self_bias - kMinRayDist)) * 1.000001f + 1e-6f;
-                        const RayR R = make_rayr(ray);
-                        float ta, tb;
-                        if (S.sh_nnodes != 0 && box_enter_leave(S.sh_tb, S.sh_tb + 3, o, R, tdist, ta, tb)) {
-                            fr[0] = o.x;
-                            fr[1] = o.y;
-                            fr[2] = o.z;
-                            rr[0] = ray.x;
-                            rr[1] = ray.y;
-                            rr[2] = ray.z;
-                            inv[0] = R.inv.x;
-                            inv[1] = R.inv.y;
-                            inv[2] = R.inv.z;
-                            en_t = ta;
-#pragma unroll
-                            for (int k = 0; k < 3; k++) {
-                                en_pb[k] = ta >= 0.f ? fr[k] + ta * rr[k] : fr[k];
-                                ex_pb[k] = fr[k] + tb * rr[k];
-                            }
-                            ex_t = tb;
-                            stk_nt[0] = make_uint2(kNodeMask | (3u << 30), __float_as_uint(tb));
-                            sp = 1;
-                            curr = 0;
-                            leaves = 0;
-                            live = true;
-                        } else {
-                            W.slot_f[W.shq_slot[q]] = kSlotLit;  // nothing that casts shadows on its way
-                        }
-                    }
-                }
-            }
-        }
-        if (!__any_sync(0xffffffffu, live)) {
-            if (drained) break;
-            continue;
-        }
-        if (!live) continue;
-        // one leaf of this lane's walk
-        bool occluded = false, finished = false;
-        if (tdist < en_t) {
-            finished = true;
-        } else if (++leaves > kMaxLeafVisits) {
-            dev_fail(S.status, kDevIterationCap);
-            finished = true;
-        } else {
-            uint2 nd = __ldg(S.sh_nodes + curr);
-            bool bad = false;
-            while ((nd.y & 3u) != 3u) {
-                nodes++;
-                const int axis = (int)(nd.y & 3u);
-                const float split = __uint_as_float(nd.x);
-                const uint32_t right = nd.y >> 2;
-                if (curr + 1 >= S.sh_nnodes || right >= S.sh_nnodes) {
-                    bad = true;
-                    break;
-                }
-                const float enp = axis == 0 ? en_pb[0] : (axis == 1 ? en_pb[1] : en_pb[2]);
-                const float exq = axis == 0 ? ex_pb[0] : (axis == 1 ? ex_pb[1] : ex_pb[2]);
-                uint32_t far_child;
-                if (enp <= split) {
-                    if (exq <= split) {
-                        curr = curr + 1;
-                        nd = __ldg(S.sh_nodes + curr);
-                        continue;
-                    }
-                    far_child = right;
-                    curr = curr + 1;
-                } else {
-                    if (split < exq) {
-                        curr = right;
-                        nd = __ldg(S.sh_nodes + curr);
-                        continue;
-                    }
-                    far_child = curr + 1;
-                    curr = right;
-                }
-                const float fa = axis == 0 ? fr[0] : (axis == 1 ? fr[1] : fr[2]);
-                const float ia = axis == 0 ? inv[0] : (axis == 1 ? inv[1] : inv[2]);
-                const float t = (split - fa) * ia;
-                if (sp >= kKdStackCap) {
-                    bad = true;
-                    break;
-                }
-                stk_nt[sp] = make_uint2(far_child | ((uint32_t)axis << 30), __float_as_uint(t));
-                stk_split[sp] = split;
-                sp++;
-                ex_t = t;
-                ex_pb[0] = axis == 0 ? split : fr[0] + t * rr[0];
-                ex_pb[1] = axis == 1 ? split : fr[1] + t * rr[1];
-                ex_pb[2] = axis == 2 ? split : fr[2] + t * rr[2];
-                nd = __ldg(S.sh_nodes + curr);
-            }
-            if (bad) {
-                dev_fail(S.status, sp >= kKdStackCap ? kDevStackOverflow : kDevBadTree);
-                finished = true;
-            } else {
-                nodes++;
-                const uint32_t np = nd.y >> 2;
-                for (uint32_t k = 0; k < np; k++) {
-                    const uint32_t ti = (np == 1) ? nd.x : __ldg(S.sh_prims + nd.x + k);
-                    if (ti >= S.ntris) {
-                        dev_fail(S.status, kDevBadTree);
-                        finished = true;
-                        break;
-                    }
-                    tests++;
-                    const Tri tr = load_tri(S.tris, ti);
-                    const int obj = (int)__ldg(S.tri_obj + ti);
-                    float rt;
-                    if (tri_hit(tr, obj == own ? self : p2, ray, rt) && rt < dist && rt > 0.f) {
-                        // only objects whose bound the ray from p2 crosses before dist count
-                        const DevObject &ob = S.objects[obj];
-                        float w;
-                        if (box_where(ob.ob, ob.ob + 3, p2, make_rayr(ray), dist, w)) {
-                            occluded = true;
-                            break;
-                        }
-                    }
-                }
-                if (!occluded && !finished) {
-                    // the exit point becomes the entry point; go to the far node on the stack
-                    en_t = ex_t;
-                    en_pb[0] = ex_pb[0];
-                    en_pb[1] = ex_pb[1];
-                    en_pb[2] = ex_pb[2];
-                    sp--;
-                    curr = stk_nt[sp].x & kNodeMask;
-                    if (curr == kNodeMask) {
-                        finished = true;
-                    } else {
-                        const uint2 nx = stk_nt[sp - 1];
-                        ex_t = __uint_as_float(nx.y);
-                        exit_point(nx.x, ex_t, stk_split[sp - 1], fr, rr, ex_pb);
-                    }
-                }
-            }
-        }
-        if (occluded || finished) {
-            W.slot_f[W.shq_slot[q]] = occluded ? kSlotShadowed : kSlotLit;
-            live = false;
-        }
-    }
     count_work(W, YR_K_SHADOW, rays, nodes, tests);
 }
 #endif

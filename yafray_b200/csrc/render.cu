@@ -46,7 +46,7 @@ static yr_status scratch(yr_scene *s, int i, size_t bytes, void **p) {
 // render's counters and the image outside the region; wave_launch() runs
 // the wave of camera samples [b, b + wcap); launch_waves() is all of it.
 struct WaveGrids {
-    int gq, gb, gt, gr;  // shadow queue (plain, shadow-ray tree, refilling BVH walk), bounce queue
+    int gq, gb;  // shadow queue, bounce queue
 };
 
 static WaveGrids waves_begin(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st) {
@@ -56,7 +56,7 @@ static WaveGrids waves_begin(yr_scene *scene, const Plan &P, uint32_t wcap, Wave
     cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
     // pixels outside the region are written as 0 (scene.cc:773)
     if (P.rpix != P.npix) cudaMemsetAsync(out, 0, sizeof(float) * 4 * (size_t)P.npix, st);
-    WaveGrids G{0, 0, 0, 0};
+    WaveGrids G{0, 0};
     if (R.raydepth <= 0) {
         // raytrace() returns black at the ray-level cap (scene.cc:204-209);
         // a tone map keeps black black except pow(0, 0) = 1 for gamma 0,
@@ -68,13 +68,9 @@ static WaveGrids waves_begin(yr_scene *scene, const Plan &P, uint32_t wcap, Wave
 #if YR_TRACE_GRID_PERSIST
     G.gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false>));
     G.gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce<false>));
-    G.gt = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_tree));
-    G.gr = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_refill<false>));
 #else
     G.gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
     G.gb = G.gq;
-    G.gt = G.gq;
-    G.gr = G.gq;
 #endif
     return G;
 }
@@ -85,28 +81,13 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
     DevRender &R = scene->rdr;
     const DevScene &D = scene->dev;
     const uint32_t npath = P.npath;
-    int gq = G.gq;
-    const int gb = G.gb;
+    const int gq = G.gq, gb = G.gb;
     // the traversal kernels with the reference-transforming loops only
     // for scenes that have references
     const bool inst = D.insts != nullptr;
     auto k_prim = inst ? k_primary<true> : k_primary<false>;
     auto k_shadow = inst ? k_trace_shadow_q<true> : k_trace_shadow_q<false>;
     auto k_bounce = inst ? k_trace_bounce<true> : k_trace_bounce<false>;
-#if YR_SHADOW_REFILL
-    // the casters' BVH (the default shadow walk): the refilling walk
-    if (!D.use_sh_tree && !D.exact_order) {
-        k_shadow = inst ? k_trace_shadow_refill<true> : k_trace_shadow_refill<false>;
-        gq = G.gr;
-    }
-#endif
-#if YR_SHADOW_TREE_REFILL
-    // the shadow-ray tree (never with references): the refilling walk
-    if (D.use_sh_tree && !inst) {
-        k_shadow = k_trace_shadow_tree;
-        gq = G.gt;
-    }
-#endif
     W.base = (uint32_t)b;
     W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
     const int g = (int)((W.count + kBlock - 1) / kBlock);
