@@ -277,8 +277,8 @@ enum { YR_LIGHT_POINT = 0, YR_LIGHT_AREA = 1, YR_LIGHT_HEMI = 2, YR_LIGHT_PATH =
  *   area:  arealight.cc:235-254  (p[0..3] = "a","b","c","d", samples,
  *          psamples)
  *   hemi:  hemilight.cc:117+     (samples, maxdist, use_QMC always)
- *   path:  pathlight.cc:753-807  (samples, depth; use_QMC, cache off,
- *          no photon maps, adaptive repetitions off) */
+ *   path:  pathlight.cc:753-807  (samples, depth, threshold; use_QMC,
+ *          cache off, no photon maps) */
 typedef struct yr_light_desc {
     uint32_t type;
     float color[3];
@@ -296,7 +296,14 @@ typedef struct yr_light_desc {
                                 point floor(samples * u), u = halton(5,
                                 m*psamples + j) rotated like the light's first
                                 dimension (see yr_render)                    */
-    uint32_t reserved[2];
+    float threshold;         /* path light "threshold" (the factory's default
+                                0.1): after the first round of paths, up to 3
+                                more rounds where the rounds' four partial
+                                sums disagree (pathLight_t::takeSample,
+                                pathlight.cc:349-374); <= 0 = one round only.
+                                Round r of camera sample s takes the QMC
+                                index (r*spp + s)*samples + i for path i     */
+    uint32_t reserved;
 } yr_light_desc;
 
 /* Render parameters.  The pixel loop follows scene_t::render(renderArea_t&)

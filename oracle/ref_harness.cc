@@ -357,8 +357,9 @@ static light_t *make_light(const yr_light_desc &d) {
     case YR_LIGHT_HEMI:
         return new hemiLight_t(d.samples, C3(d.color), d.power, d.maxdist, false, true);
     case YR_LIGHT_PATH:
-        // use_QMC, no cache, adaptive repetitions off (threshold 1e9)
-        return new pathLight_t(d.samples, d.power, d.depth, 0, true, false, 1.0, 1e9f);
+        // use_QMC, no cache; adaptive repetitions at the record's threshold
+        // (off, as a huge threshold, when it is not above 0)
+        return new pathLight_t(d.samples, d.power, d.depth, 0, true, false, 1.0, d.threshold > 0 ? d.threshold : 1e9f);
     }
     die("bad light type");
     return NULL;
@@ -932,13 +933,23 @@ static void cmd_illum(const SceneFile &s, const char *q_path, const char *out) {
             rgb[1] = c.getG();
             rgb[2] = c.getB();
             if (hs) {
+                // how many rounds of paths ran: every level's stream must
+                // have advanced the same whole number of rounds of `samples`
+                // values (true when no path stops early); head[1] = rounds
+                int rounds = -1;
                 for (int lev = 0; lev < pl->maxdepth; lev++)
                     for (int k = 2 * lev; k < 2 * lev + 2; k++) {
                         Halton ref(hs->HSEQ[k]._base);
                         ref.setStart(q.m0 * (unsigned)pl->samples);
-                        for (int m = 0; m < pl->samples; m++) ref.getNext();
-                        if (ref.value != hs->HSEQ[k].value) head[1] = 0;
+                        int found = 0;
+                        for (int rr = 1; rr <= 4 && !found; rr++) {
+                            for (int m = 0; m < pl->samples; m++) ref.getNext();
+                            if (ref.value == hs->HSEQ[k].value) found = rr;
+                        }
+                        if (!found || (rounds >= 0 && rounds != found)) rounds = 0;
+                        else if (rounds < 0) rounds = found;
                     }
+                head[1] = rounds > 0 ? (uint32_t)rounds : 0;
             }
         }
         wr(f, head, 8);

@@ -1271,6 +1271,7 @@ C fromLight(const Scene &S, const SP &sp, const V &ldir, const C &lcol, const V 
 struct Ctx {
     uint32_t pixel, s, pi;  // pixel, camera sample, path index
     int npath;
+    uint32_t stride = 1;    // camera samples per pixel: round r of the path light uses index (r*stride + s)*P + i
 };
 
 C illum_point(Scene &S, const Light &L, const SP &sp, const V &eye) {
@@ -1404,15 +1405,56 @@ V cosHemi(const V &N, const V &Ru, const V &Rv, float z1, float z2) {  // pathto
 // with it (camera vertex); v = QMC vertex level, m0 = QMC sample index.
 C light_sum(Scene &S, const SP &sp, const V &eye, bool indirect, int v, uint32_t m0, const Ctx &cx);
 
+void expgam_adjust(float *c, float e, float g, bool clamp_rgb);
+
+// the scene's color_t::expgam_Adjust (scene_t::adjustColor, scene.h:164):
+// applied whether or not the render tone-maps its samples
+C adjust_color(const Scene &S, const C &c) {
+    float v[3] = {c.r, c.g, c.b};
+    const float e = -S.rp.exposure, g = S.rp.gamma != 0.f ? (float)(1.0 / (double)S.rp.gamma) : 0.f;
+    expgam_adjust(v, e, g, (S.rp.flags & YR_RENDER_CLAMP_RGB) != 0);
+    return C(v[0], v[1], v[2]);
+}
+
+// The adaptive extra rounds of pathLight_t::takeSample (pathlight.cc:349-374):
+// from the first round's four partial sums (path i adds to sum i % 4),
+// each times multiplier() = 1/P, the per-channel minimum and maximum after
+// the scene's tone adjustment; extra = int(diff^2) - 1 in [0, 3] with
+// diff = maxAbsDiff(max, min) / (max(ene, 1) * 4) / threshold and
+// ene = maxAbsDiff(min, 0).
+int extra_rounds(const Scene &S, const C *sub, int P, float threshold) {
+    float mn[3] = {1000, 1000, 1000}, mx[3] = {0, 0, 0};
+    const float mult = (float)(1.0 / (double)(float)P);
+    for (int k = 0; k < 4; k++) {
+        const C c = sub[k] * mult;
+        const float v[3] = {c.r, c.g, c.b};
+        for (int ch = 0; ch < 3; ch++) {
+            if (v[ch] > mx[ch]) mx[ch] = v[ch];
+            if (v[ch] < mn[ch]) mn[ch] = v[ch];
+        }
+    }
+    const C lo = adjust_color(S, C(mn[0], mn[1], mn[2])), hi = adjust_color(S, C(mx[0], mx[1], mx[2]));
+    const float ene = fmaxf(fabsf(lo.r), fmaxf(fabsf(lo.g), fabsf(lo.b)));
+    const float mad = fmaxf(fabsf(hi.r - lo.r), fmaxf(fabsf(hi.g - lo.g), fabsf(hi.b - lo.b)));
+    float diff = (float)((double)mad / (((ene < 1.0) ? 1.0 : (double)ene) * 2.0 * 2.0));
+    diff /= threshold;
+    int extra = (int)(diff * diff) - 1;
+    if (extra > 3) extra = 3;
+    if (extra < 0) extra = 0;
+    return extra;
+}
+
 // pathLight_t::normalSample + takeSample (pathlight.cc:223-403), explicit indices
 C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx) {
     V N = faceForward(sp.Ng, sp.N, eye);
     C dif = diffuse(S, sp);
     if (below_cut(energy(dif))) return C();
     const int P = L.d.samples, depth = L.d.depth;
-    C total;
+    C total, sub[4];
+    int rounds = 1;
+    for (int r = 0; r < rounds; r++) {
     for (int i = 0; i < P; i++) {
-        const uint32_t n = cx.s * (uint32_t)P + (uint32_t)i;
+        const uint32_t n = ((uint32_t)r * cx.stride + cx.s) * (uint32_t)P + (uint32_t)i;
         V ray = cosHemi(N, sp.NU, sp.NV, cp_add(halton(kPrimes[0], n), rot(S, cx.pixel, 0)),
                         cp_add(halton(kPrimes[1], n), rot(S, cx.pixel, 1)));
         const V startray = ray;
@@ -1425,7 +1467,9 @@ C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx
             const V f = where + ray * kMinRay;
             Hit h = closest(S, f, ray, false, true);
             if (h.obj < 0) {
-                total = total + (startN * raycolor) * col3(S.rp.background);
+                const C contri = (startN * raycolor) * col3(S.rp.background);
+                total = total + contri;
+                if (r == 0) sub[i % 4] = sub[i % 4] + contri;
                 break;
             }
             SP t = surface(S, h.obj, h.tri, h.Z, f, ray);
@@ -1433,7 +1477,9 @@ C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx
             c2.pi = (uint32_t)i;
             const V eye2 = (t.P + (-ray)) - t.P;
             C light = light_sum(S, t, eye2, true, j + 1, n, c2);
-            total = total + (startN * raycolor) * light;
+            const C contri = (startN * raycolor) * light;
+            total = total + contri;
+            if (r == 0) sub[i % 4] = sub[i % 4] + contri;
             const V HN = faceForward(t.Ng, t.N, -ray);
             raycolor = raycolor * diffuse(S, t);
             if (j + 1 < depth) {
@@ -1445,7 +1491,9 @@ C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx
             where = t.P;
         }
     }
-    total = total * ((float)(1.0 / (double)(float)P) / 1.0f);
+        if (r == 0 && L.d.threshold > 0.f) rounds += extra_rounds(S, sub, P, L.d.threshold);
+    }
+    total = total * ((float)(1.0 / (double)(float)P) / (float)rounds);
     return (dif * total) * L.d.power;
 }
 
@@ -1553,6 +1601,7 @@ void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
     cx.pixel = pixel;
     cx.s = s;
     cx.pi = 0;
+    cx.stride = spp;
     C c = light_sum(S, sp, S.cam.pos - sp.P, false, 0, s, cx);
     rgba[0] = c.r;
     rgba[1] = c.g;

@@ -248,6 +248,24 @@ def guess_scene():
     return sc
 
 
+def rounds_scene(threshold):
+    """The path scene with the path light's adaptive rounds on."""
+    sc = path_scene()
+    sc.lights[1] = scenes.path_light(samples=4, depth=3, power=1.0, threshold=threshold)
+    return sc
+
+
+def illum_rounds():
+    out = {}
+    for name, thr, seed in (("t10", 0.1, 31), ("t005", 0.005, 32), ("t001", 0.001, 33)):
+        sc = rounds_scene(thr)
+        q = illum_queries(sc, 200, seed)
+        q["light"] = 1
+        out[name + "_q"] = q
+        out[name + "_o"] = T.harness_illum(sc, q)
+    np.savez_compressed(os.path.join(HERE, "illum_rounds.npz"), **out)
+
+
 def illum_guess():
     sc = guess_scene()
     q = illum_queries(sc, 900, 21)
@@ -567,6 +585,7 @@ if __name__ == "__main__":
     instances()
     illum()
     illum_guess()
+    illum_rounds()
     halton_noise()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -166,6 +166,28 @@ def test_oracle_light_estimators_match_reference(name):
         assert (ref[q["light"] == k].sum(1) > 0).any()
 
 
+@pytest.mark.parametrize("name", ["t10", "t005", "t001"])
+def test_oracle_path_rounds_match_reference(name):
+    """The path light's adaptive extra rounds (threshold 0.1, 0.005,
+    0.001): the reference's takeSample with each level's Halton stream
+    started at the query's index, and the rounds it ran read back from the
+    streams, against the oracle's estimator on the same samples.  The
+    queries hold one to four rounds."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    g = load("illum_rounds.npz")
+    q, o = g[name + "_q"], g[name + "_o"]
+    sc = make_golden.rounds_scene({"t10": 0.1, "t005": 0.005, "t001": 0.001}[name])
+    assert (o["synced"] > 0).all()            # every path reached every level in every round
+    hit, rgb = T.OracleScene(sc).illum(q, o["vals"])
+    assert np.array_equal(hit, o["hit"].astype(np.int32))
+    ref = o["rgb"]
+    tol = 1e-6 * np.maximum(np.abs(ref), 1e-3)
+    assert (np.abs(rgb - ref) <= tol).all(), np.abs(rgb - ref).max()
+    if name == "t10":
+        assert len(np.unique(o["synced"])) >= 3   # one round and several extra ones both occur
+
+
 def test_oracle_penumbra_guess_matches_reference():
     """Area lights with the penumbra guess (psamples > 0): each query's
     areaLight_t::illuminate in the reference, its guessLight probes drawn

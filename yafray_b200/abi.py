@@ -101,7 +101,8 @@ class YrLightDesc(C.Structure):
     _fields_ = [
         ("type", C.c_uint32), ("color", f3), ("power", C.c_float), ("p", (C.c_float * 3) * 4),
         ("samples", C.c_int32), ("depth", C.c_int32), ("maxdist", C.c_float),
-        ("cast_shadows", C.c_uint32), ("psamples", C.c_int32), ("reserved", C.c_uint32 * 2),
+        ("cast_shadows", C.c_uint32), ("psamples", C.c_int32), ("threshold", C.c_float),
+        ("reserved", C.c_uint32),
     ]
 
 

@@ -319,13 +319,16 @@ def hemi_light(samples=16, power=1.0, color=(1.0, 1.0, 1.0), maxdist=-1.0) -> ab
     return l
 
 
-def path_light(samples=1, depth=2, power=1.0) -> abi.YrLightDesc:
+def path_light(samples=1, depth=2, power=1.0, threshold=0.0) -> abi.YrLightDesc:
+    """pathLight_t with use_QMC; `threshold` > 0 turns the adaptive extra
+    rounds of paths on (the factory's default is 0.1), 0 = one round."""
     l = abi.YrLightDesc()
     l.type = abi.YR_LIGHT_PATH
     l.color[:] = [1.0, 1.0, 1.0]
     l.power = float(power)
     l.samples = int(samples)
     l.depth = int(depth)
+    l.threshold = float(threshold)
     return l
 
 
