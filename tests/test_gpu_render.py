@@ -237,20 +237,62 @@ def test_render_penumbra_guess(cuda, gi):
 
 
 def test_render_penumbra_guess_batch(cuda):
-    """The batched renderer on scenes with the penumbra guess (waves
-    schedule): each image equals yr_render's."""
+    """The batched renderer on scenes with the penumbra guess and with the
+    path light's adaptive rounds (waves schedule): each image equals
+    yr_render's."""
     import torch
     import sys, os
     sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
     import make_golden
-    scs = [make_golden.guess_scene(), scenes.config_small(64, 48)]
+    scs = [make_golden.guess_scene(), scenes.config_small(64, 48), make_golden.rounds_scene(0.005)]
     scs[0].render.spp = 2
+    scs[2].camera.resx, scs[2].camera.resy = 40, 30
     dss = [api.DeviceScene(sc) for sc in scs]
     outs = [torch.zeros((sc.resy, sc.resx, 4), dtype=torch.float32, device="cuda") for sc in scs]
     api.render_batch(dss, [o.data_ptr() for o in outs])
     torch.cuda.synchronize()
     for d, o in zip(dss, outs):
         assert np.array_equal(o.cpu().numpy().view(np.uint32), d.render().view(np.uint32))
+
+
+@pytest.mark.parametrize("threshold", [0.1, 0.005])
+def test_render_path_adaptive_rounds(cuda, threshold):
+    """The path light's adaptive extra rounds (threshold 0.1, the factory's
+    default, and 0.005): round 0's partial sums decide up to three more
+    rounds of paths per camera sample, with their own QMC indices."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    sc = make_golden.rounds_scene(threshold)
+    sc.camera.resx, sc.camera.resy = 48, 36
+    sc.render.spp = 2
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    O = T.OracleScene(sc)
+    ref, stats = O.render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref, O)
+    st = ds.last_stats
+    assert abs(int(st.rays_bounce) - int(stats[2])) <= 0.001 * stats[2] + 4
+    # extra rounds were taken, and they change the image
+    sc.lights[1].threshold = 0.0
+    d1 = api.DeviceScene(sc)
+    one = d1.render()
+    assert d1.last_stats.rays_bounce < st.rays_bounce
+    assert np.abs(one - img).max() > 1e-4
+
+
+def test_render_path_rounds_large_config(cuda):
+    """The benchmark's GI scene (2x2 grid) with the path light at its
+    factory default threshold 0.1."""
+    sc = scenes.config_large(seed=2, resx=48, resy=32, spp=2, grid=2)
+    sc.lights[-1].threshold = 0.1
+    ds = api.DeviceScene(sc)
+    img = ds.render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref, O)
 
 
 def test_render_texture_board(cuda):

@@ -372,9 +372,10 @@ static yr_status adj_plan(const yr_scene *scene, size_t budget, AdjPlan &A) {
     if (R.raydepth <= 0) return YR_ERR_UNSUPPORTED;
     // per-sample exposure / gamma is not differentiated
     if (R.tonemap && !(R.exposure == 0.f && R.gamma_r == 1.f && !R.clamp_rgb)) return YR_ERR_UNSUPPORTED;
-    // nor the penumbra guess's decisions, nor a texture's modulation of
+    // nor the penumbra guess's decisions or the path light's adaptive
+    // rounds, nor a texture's modulation of
     // the specular colour or exponent
-    if (R.has_guess) return YR_ERR_UNSUPPORTED;
+    if (R.has_guess || R.path_threshold > 0.f) return YR_ERR_UNSUPPORTED;
     for (const yr_shader_desc &d : scene->shader_desc)
         if (d.tex_type != YR_TEX_NONE && (d.mod_specular > 0.f || d.mod_hard > 0.f)) return YR_ERR_UNSUPPORTED;
     const Plan &P = A.P;

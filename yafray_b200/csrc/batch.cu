@@ -619,10 +619,12 @@ extern "C" YR_API yr_status yr_render_batch(yr_scene *const *scenes, uint32_t co
         cudaMemcpy(C.d_outs, C.outs.data(), sizeof(float *) * count, cudaMemcpyHostToDevice);
         if (C.lanes_n) C.drop_graph();  // the waves graph holds the image pointers
     }
-    // the tiles kernel runs each vertex's light sampling in one stage: a
-    // scene whose area lights guess the penumbra first takes the waves
+    // the tiles kernel runs each vertex's light sampling in one stage and
+    // one round of paths: a scene whose area lights guess the penumbra
+    // first, or whose path light takes adaptive rounds, takes the waves
     bool guess = false;
-    for (uint32_t i = 0; i < count; i++) guess = guess || scenes[i]->rdr.has_guess;
+    for (uint32_t i = 0; i < count; i++)
+        guess = guess || scenes[i]->rdr.has_guess || scenes[i]->rdr.path_threshold > 0.f;
     if (guess && want_mode == YR_BATCH_TILES) return done(YR_ERR_UNSUPPORTED);
     const int mode_wanted = guess ? YR_BATCH_WAVES : want_mode;
     BatchConfig cfg;

@@ -54,6 +54,9 @@ struct Wave {
     uint32_t *shq_slot;
     uint32_t *bq;        // bounce queue (path indices)
     uint32_t *bq2;
+    float4 *ptot;        // [count] path light: the rounds' sum of path contributions (adaptive rounds)
+    uint32_t *nrep;      // [count] path light: extra rounds of the camera sample
+    uint32_t rep;        // the round of paths being traced (0 = the first)
     uint32_t *counters;  // [0] shadow queue, [1] bounce queue, [2] next bounce queue,
                          // [3..5] ray totals (primary, shadow, bounce) as 2x u32 lo/hi pairs
     unsigned long long *rays;  // [3] primary, shadow, bounce
@@ -95,6 +98,12 @@ __device__ __forceinline__ uint32_t cs_pixel(const DevRender &R, uint32_t cs, in
     x = R.rx0 + (int)(lp % (uint32_t)R.rw);
     y = R.ry0 + (int)(lp / (uint32_t)R.rw);
     return (uint32_t)y * (uint32_t)R.cam.resx + (uint32_t)x;
+}
+
+// QMC index of path pi of camera sample s (s = sample within its pixel) in
+// the current round of paths: (round * spp + s) * P + pi
+__device__ __forceinline__ uint32_t path_index(const DevRender &R, const Wave &W, uint32_t s, uint32_t pi) {
+    return (W.rep * R.spp + s) * W.npath + pi;
 }
 
 // ---------------------------------------------------------------- camera
@@ -534,7 +543,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
             const V3 N0 = face_forward(sp.Ng, sp.N, eye);
             const float r0 = cp_rot(R.seed, pixel, 0), r1 = cp_rot(R.seed, pixel, 1);
             for (uint32_t pi = 0; pi < W.npath; pi++) {
-                const uint32_t n = s * W.npath + pi;
+                const uint32_t n = path_index(R, W, s, pi);
                 const float z1 = cp_add(halton(kPrimes[0], n), r0), z2 = cp_add(halton(kPrimes[1], n), r1);
                 const V3 ray = cos_hemi_dir(N0, sp.NU, sp.NV, z1, z2);
                 const uint32_t p = i * W.npath + pi;
@@ -697,7 +706,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
     C3 dif = c3(0.f, 0.f, 0.f);
     if (ADJ) {
         TexDeriv td{};
-        shade_lights<true>(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux, A->slot_s, &dif,
+        shade_lights<true>(S, R, W, active, sp, eye, p, j + 1, path_index(R, W, s, pi), pixel, W.p_aux, A->slot_s, &dif,
                            &td);
         if (active) {
             const size_t ci = (size_t)p * R.path_depth + j;
@@ -706,7 +715,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
             A->pm[2 * ci + 1] = make_float4(td.tex.r, td.tex.g, td.tex.b, 0.f);
         }
     } else {
-        shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux);
+        shade_lights(S, R, W, active, sp, eye, p, j + 1, path_index(R, W, s, pi), pixel, W.p_aux);
     }
     if (active) {
         if (!ADJ) dif = modulated_color(R.shaders + sp.shader, sp);
@@ -717,7 +726,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
         const int lev = j + 1;
         if (j + 1 < R.path_depth) {
             const float r0 = cp_rot(R.seed, pixel, 2 * lev), r1 = cp_rot(R.seed, pixel, 2 * lev + 1);
-            const uint32_t nidx = s * W.npath + pi;
+            const uint32_t nidx = path_index(R, W, s, pi);
             const float z1 = cp_add(halton(kPrimes[2 * lev], nidx), r0);
             const float z2 = cp_add(halton(kPrimes[2 * lev + 1], nidx), r1);
             const V3 nr = cos_hemi_dir(HN, sp.NU, sp.NV, z1, z2);
@@ -783,7 +792,8 @@ __device__ __forceinline__ void st_guess_path(const DevScene &S, const DevRender
             active = true;
         }
     }
-    shade_lights(S, R, W, active, sp, eye, p, j + 1, s * W.npath + pi, pixel, W.p_aux, nullptr, nullptr, nullptr, 1);
+    shade_lights(S, R, W, active, sp, eye, p, j + 1, path_index(R, W, s, pi), pixel, W.p_aux, nullptr, nullptr, nullptr,
+                 1);
     if (active) W.p_where[p] = make_float4(sp.P.x, sp.P.y, sp.P.z, wh.w);
 }
 
@@ -896,15 +906,22 @@ __device__ __forceinline__ void st_finish(const DevRender &R, const Wave &W, uin
                     C3 pt = c3(0.f, 0.f, 0.f);
                     if (d0.w != 0.f) {
                         C3 total = c3(0.f, 0.f, 0.f);
-                        for (uint32_t pi = 0; pi < W.npath; pi++)
-                            for (int j = 0; j < R.path_depth; j++) {
-                                const float4 c = W.p_contri[((size_t)(i * W.npath + pi)) * R.path_depth + j];
-                                if (c.w == 0.f) break;
-                                total = total + c3(c.x, c.y, c.z);
-                            }
-                        // multiplier() = 1/(taken+1), divided by one repetition
+                        float rounds = 1.0f;
+                        if (R.path_threshold > 0.f) {  // the rounds' sum, formed round by round
+                            const float4 t = W.ptot[i];
+                            total = c3(t.x, t.y, t.z);
+                            rounds = (float)(1u + W.nrep[i]);
+                        } else {
+                            for (uint32_t pi = 0; pi < W.npath; pi++)
+                                for (int j = 0; j < R.path_depth; j++) {
+                                    const float4 c = W.p_contri[((size_t)(i * W.npath + pi)) * R.path_depth + j];
+                                    if (c.w == 0.f) break;
+                                    total = total + c3(c.x, c.y, c.z);
+                                }
+                        }
+                        // multiplier() = 1/(taken+1), divided by the rounds taken
                         const float mult = (float)(1.0 / (double)(float)W.npath);
-                        total = total * (mult / 1.0f);
+                        total = total * (mult / rounds);
                         pt = (c3(d0.x, d0.y, d0.z) * total) * d0.w;
                     }
                     fl = fl + pt;
@@ -939,6 +956,103 @@ __device__ __forceinline__ void st_finish(const DevRender &R, const Wave &W, uin
     const uint32_t pixel = cs_pixel(R, W.base + px * R.spp, x, y);
     reinterpret_cast<float4 *>(W.out)[pixel] = o;
 }
+
+// The path light's adaptive rounds (pathLight_t::takeSample,
+// pathlight.cc:349-374), per camera sample i once round W.rep of its paths
+// is gathered.  Round 0: the contributions summed in the reference's order
+// (path by path, vertex by vertex) and, per partial sum i % 4, the extra
+// rounds: the sums times multiplier() = 1/P, their per-channel minimum and
+// maximum after the scene's tone adjustment (scene_t::adjustColor),
+// diff = maxAbsDiff(max, min) / (max(ene, 1) * 4) / threshold with
+// ene = maxAbsDiff(min, 0), extra = int(diff^2) - 1 in [0, 3].  Later
+// rounds: their contributions added in the same order.
+__device__ __forceinline__ void st_path_round(const DevRender &R, const Wave &W, uint32_t i) {
+    if (W.diff0[i].w == 0.f) return;  // no paths from this point
+    if (W.rep > 0 && W.nrep[i] < W.rep) return;
+    C3 total = c3(0.f, 0.f, 0.f), sub[4];
+    for (int k = 0; k < 4; k++) sub[k] = c3(0.f, 0.f, 0.f);
+    if (W.rep > 0) {
+        const float4 t = W.ptot[i];
+        total = c3(t.x, t.y, t.z);
+    }
+    for (uint32_t pi = 0; pi < W.npath; pi++)
+        for (int j = 0; j < R.path_depth; j++) {
+            const float4 c = W.p_contri[((size_t)(i * W.npath + pi)) * R.path_depth + j];
+            if (c.w == 0.f) break;
+            total = total + c3(c.x, c.y, c.z);
+            sub[pi & 3u] = sub[pi & 3u] + c3(c.x, c.y, c.z);
+        }
+    W.ptot[i] = make_float4(total.r, total.g, total.b, 0.f);
+    if (W.rep > 0) return;
+    const float mult = (float)(1.0 / (double)(float)W.npath);
+    float mn[3] = {1000.f, 1000.f, 1000.f}, mx[3] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < 4; k++) {
+        const C3 c = sub[k] * mult;
+        const float v[3] = {c.r, c.g, c.b};
+        for (int ch = 0; ch < 3; ch++) {
+            if (v[ch] > mx[ch]) mx[ch] = v[ch];
+            if (v[ch] < mn[ch]) mn[ch] = v[ch];
+        }
+    }
+    const C3 lo = expgam_adjust(c3(mn[0], mn[1], mn[2]), R.exposure, R.gamma_r, R.clamp_rgb != 0);
+    const C3 hi = expgam_adjust(c3(mx[0], mx[1], mx[2]), R.exposure, R.gamma_r, R.clamp_rgb != 0);
+    const float ene = fmaxf(fabsf(lo.r), fmaxf(fabsf(lo.g), fabsf(lo.b)));
+    const float mad = fmaxf(fabsf(hi.r - lo.r), fmaxf(fabsf(hi.g - lo.g), fabsf(hi.b - lo.b)));
+    float diff = (float)((double)mad / (((ene < 1.0f) ? 1.0 : (double)ene) * 2.0 * 2.0));
+    diff /= R.path_threshold;
+    int extra = (int)(diff * diff) - 1;
+    extra = extra > 3 ? 3 : (extra < 0 ? 0 : extra);
+    W.nrep[i] = (uint32_t)extra;
+}
+
+// The first directions of round W.rep (> 0) for the camera samples that
+// take it: the camera vertex set up again as st_shade_camera does, then
+// its paths queued (whole warp).
+__device__ __forceinline__ void st_path_restart(const DevScene &S, const DevRender &R, const Wave &W, uint32_t i) {
+    const bool inb = i < W.count;
+    bool paths = false;
+    if (inb && W.diff0[i].w != 0.f && W.nrep[i] >= W.rep) {
+        const uint32_t cs = W.base + i;
+        int x, y;
+        const uint32_t pixel = cs_pixel(R, cs, x, y), s = cs % R.spp;
+        const float4 h = W.hit0[i];
+        float fx, fy;
+        sample_pos(R, pixel, s, fx, fy);
+        const V3 ray0 = camera_ray(R.cam, (float)x + fx, (float)y + fy);
+        const V3 f = R.cam.pos + ray0 * kMinRayDist;
+        const Surf sp = make_surface(S, R, __float_as_int(h.y), __float_as_uint(h.z), h.x, f, ray0);
+        const V3 eye = R.cam.pos - sp.P;
+        const V3 N0 = face_forward(sp.Ng, sp.N, eye);
+        const float r0 = cp_rot(R.seed, pixel, 0), r1 = cp_rot(R.seed, pixel, 1);
+        for (uint32_t pi = 0; pi < W.npath; pi++) {
+            const uint32_t n = path_index(R, W, s, pi);
+            const float z1 = cp_add(halton(kPrimes[0], n), r0), z2 = cp_add(halton(kPrimes[1], n), r1);
+            const V3 ray = cos_hemi_dir(N0, sp.NU, sp.NV, z1, z2);
+            const uint32_t p = i * W.npath + pi;
+            W.p_where[p] = make_float4(sp.P.x, sp.P.y, sp.P.z, dot(ray, N0));
+            W.p_ray[p] = make_float4(ray.x, ray.y, ray.z, 1.f);
+            W.p_col[p] = make_float4(1.f, 1.f, 1.f, 0.f);
+        }
+        paths = true;
+    }
+    for (uint32_t pi = 0; pi < W.npath; pi++) {
+        const uint32_t q = warp_append(&W.counters[1], paths);
+        if (paths) W.bq[q] = i * W.npath + pi;
+    }
+}
+
+#ifdef YR_WAVE_KERNELS
+static __global__ void __launch_bounds__(kBlock) k_path_round(DevRender R, Wave W) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < W.count) st_path_round(R, W, i);
+}
+
+static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_path_restart(DevScene S, DevRender R, Wave W) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W.count && (i & ~31u) >= W.count) return;  // whole warps past the end leave
+    st_path_restart(S, R, W, i);
+}
+#endif
 
 #ifdef YR_WAVE_KERNELS
 static __global__ void __launch_bounds__(kBlock) k_finish(DevRender R, Wave W) {
@@ -1002,7 +1116,7 @@ inline yr_status make_plan(const yr_scene *scene, Plan &P) {
     return YR_OK;
 }
 
-constexpr int kNumBufs = 22;
+constexpr int kNumBufs = 24;
 constexpr size_t kBufAlign = 256;
 
 // Bytes of each scratch buffer for a wave of `wcap` camera samples, in the
@@ -1014,7 +1128,8 @@ __host__ __device__ inline void wave_sizes(const Plan &P, uint32_t wcap, size_t 
     size_t sizes[kNumBufs] = {f4 * w,  f4 * w * P.nl, f4 * w * P.nl, f4 * w,  f4 * pc, f4 * pc,
                               f4 * pc, f4 * pc,       f4 * pc,       f4 * pc, f4 * pc * P.depth, f4 * pc * P.nl,
                               f4 * slots, slots,      f4 * slots,    f4 * slots, 4 * slots, 4 * pc,
-                              4 * pc,  4 * 8,         8 * 4,         8 * 3 * YR_K_COUNT};
+                              4 * pc,  4 * 8,         8 * 4,         8 * 3 * YR_K_COUNT,
+                              f4 * w,  4 * w};
     for (int i = 0; i < kNumBufs; i++) b[i] = sizes[i];
 }
 
@@ -1058,6 +1173,9 @@ __host__ __device__ inline void assign_wave(const Plan &P, uint32_t wcap, char *
     W.counters = (uint32_t *)ptr[k++];
     W.rays = (unsigned long long *)ptr[k++];
     W.kst = (unsigned long long *)ptr[k++];
+    W.ptot = (float4 *)ptr[k++];
+    W.nrep = (uint32_t *)ptr[k++];
+    W.rep = 0;
     W.ns = P.ns;
     W.npath = P.npath;
 }

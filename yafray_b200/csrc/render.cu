@@ -113,6 +113,7 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
             k_clear_contri<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(W, nc);
         });
         const int gp = (int)(((size_t)W.count * npath + kBlock - 1) / kBlock);
+        auto bounces = [&] {
         for (int j = 0; j < R.path_depth; j++) {
             timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 1); });
             cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
@@ -132,6 +133,25 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
             timed(YR_K_GATHER, [&] { k_gather_path<<<gp, kBlock, 0, st>>>(R, W, j, R.background); });
             std::swap(W.bq, W.bq2);
             timed(YR_K_OTHER, [&] { k_swap_queues<<<1, 1, 0, st>>>(W); });
+        }
+        };
+        bounces();
+        if (R.path_threshold > 0.f) {
+            // the adaptive rounds: round 0's sums and extra rounds, then up
+            // to three more rounds of paths for the samples that take them
+            W.rep = 0;
+            timed(YR_K_OTHER, [&] { k_path_round<<<g, kBlock, 0, st>>>(R, W); });
+            for (uint32_t r = 1; r <= 3; r++) {
+                W.rep = r;
+                timed(YR_K_OTHER, [&] {
+                    k_clear_contri<<<grid_for((uint32_t)std::min<size_t>(nc, 1u << 30), kBlock), kBlock, 0, st>>>(W, nc);
+                });
+                cudaMemsetAsync(W.counters + 1, 0, sizeof(uint32_t), st);
+                timed(YR_K_SHADE_CAMERA, [&] { k_path_restart<<<g, kBlock, 0, st>>>(D, R, W); });
+                bounces();
+                timed(YR_K_OTHER, [&] { k_path_round<<<g, kBlock, 0, st>>>(R, W); });
+            }
+            W.rep = 0;
         }
     }
     const int gf = (int)((W.count / R.spp + kBlock - 1) / kBlock);

@@ -837,6 +837,12 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
             R.path_samples = s->lights[i].samples;
             R.path_depth = s->lights[i].depth;
         }
+    R.path_threshold = 0.f;
+    if (R.path_light >= 0) {
+        const float t = s->light_desc[R.path_light].threshold;
+        if (!(t <= 0.f) && !std::isfinite(t)) return fail(YR_ERR_INVALID_ARG);
+        R.path_threshold = t > 0.f ? t : 0.f;
+    }
 
     // ---- adjoint parameter vector (yr_param_count): per shader color[3] and
     // specular weight, plus amplitude and base colour for textured shaders;
@@ -940,6 +946,10 @@ YR_API yr_status yr_scene_set_params(yr_scene *scene, const yr_shader_desc *shad
         }
         scene->light_desc = ld;
         scene->lights = nl;
+        if (scene->rdr.path_light >= 0) {
+            const float t = ld[scene->rdr.path_light].threshold;
+            scene->rdr.path_threshold = (t > 0.f && std::isfinite(t)) ? t : 0.f;
+        }
     }
     yr_status st = upload_params(scene);
     cudaSetDevice(prev);

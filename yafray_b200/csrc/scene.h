@@ -87,6 +87,7 @@ struct DevRender {
     float exposure;             // scene_t::exposure = -"exposure"
     float gamma_r;              // scene_t::gamma_R = 1/"gamma" (0 for gamma 0)
     int has_guess;              // some area light guesses the penumbra first (psamples > 0)
+    float path_threshold;       // path light "threshold" of its adaptive extra rounds (0: one round)
 };
 
 // Device allocation tracked by the scene (freed in yr_scene_destroy).
