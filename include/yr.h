@@ -266,8 +266,13 @@ typedef struct yr_shader_desc {
 /* yr_shader_desc.tex_map.  TEXCO_ORCO reads the hit point as orco does for
  * a mesh without orco coordinates and without a transform
  * (meshObject_t::toObjectOrco, mesh.cc:510-514); TEXCO_NORMAL reads the
- * shading normal. */
-enum { YR_TEXCO_GLOBAL = 0, YR_TEXCO_ORCO = 1, YR_TEXCO_NORMAL = 2 };
+ * shading normal; TEXCO_WINDOW the camera sample's screen position
+ * (x, y in [-1, 1], z 0) at a camera hit and (0, 0, 0) at a path vertex,
+ * whose surface point has no screen position (scene.cc:234, 749);
+ * TEXCO_REFLECT the eye direction reflected about the face-forwarded
+ * normal, the eye being the direction the shading call looks from
+ * (texture.cc:148-165). */
+enum { YR_TEXCO_GLOBAL = 0, YR_TEXCO_ORCO = 1, YR_TEXCO_NORMAL = 2, YR_TEXCO_WINDOW = 3, YR_TEXCO_REFLECT = 4 };
 enum { YR_PROJ_DEFAULT = 0, YR_PROJ_X = 1, YR_PROJ_Y = 2, YR_PROJ_Z = 3, YR_PROJ_NONE = 4 };
 
 enum { YR_LIGHT_POINT = 0, YR_LIGHT_AREA = 1, YR_LIGHT_HEMI = 2, YR_LIGHT_PATH = 3 };

@@ -333,8 +333,8 @@ static shader_t *make_shader(const yr_shader_desc &d, std::vector<texture_t *> &
         modu.reflection(0);
         modu.displace(0);
         modu.string2maptype("flat");
-        static const char *texco[3] = {"global", "orco", "normal"};
-        modu.string2texcotype(texco[(d.tex_map & 0xffu) < 3 ? (d.tex_map & 0xffu) : 0]);
+        static const char *texco[5] = {"global", "orco", "normal", "window", "reflect"};
+        modu.string2texcotype(texco[(d.tex_map & 0xffu) < 5 ? (d.tex_map & 0xffu) : 0]);
         modu.string2cliptype("extend");
         std::string proj[3];
         for (int k = 0; k < 3; k++) {

@@ -1116,6 +1116,7 @@ struct SP {
     V orco;  // toObjectOrco(P): P, or M^-1 P on a reference
     int obj;
     int shader;
+    float sx = 0.f, sy = 0.f;  // screen position (camera hits only; 0 elsewhere)
 };
 
 void createCS(const V &N, V &u, V &v) {  // vector3d.h:240-258
@@ -1187,9 +1188,14 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from_w, cons
 // procedural path): texco "global" / "orco" (an untransformed mesh without
 // orco data: P) or "normal", then projections size*(src[axis] + ofs) /
 // size*ofs
-V tex_point(const yr_shader_desc &d, const SP &sp) {
+V tex_point(const yr_shader_desc &d, const SP &sp, const V &eye) {
     const uint32_t tc = d.tex_map & 0xffu;
-    const V src = tc == YR_TEXCO_NORMAL ? sp.N : (tc == YR_TEXCO_ORCO ? sp.orco : sp.P);
+    V src = tc == YR_TEXCO_NORMAL ? sp.N : (tc == YR_TEXCO_ORCO ? sp.orco : sp.P);
+    if (tc == YR_TEXCO_WINDOW) src = V(sp.sx, sp.sy, 0.f);
+    if (tc == YR_TEXCO_REFLECT) {  // texture.cc:158-165
+        const V neye = normalize(eye);
+        src = reflectv(faceForward(sp.Ng, sp.N, neye), neye);
+    }
     float t[3];
     for (int k = 0; k < 3; k++) {
         const uint32_t pc = (d.tex_map >> (8 * (k + 1))) & 0xffu;
@@ -1214,14 +1220,14 @@ struct Mod {
     C c, s;
     float h;
 };
-Mod modulated(const Scene &S, const SP &sp) {
+Mod modulated(const Scene &S, const SP &sp, const V &eye) {
     const yr_shader_desc &d = S.shaders[sp.shader];
     Mod m;
     m.c = col3(d.color);
     m.s = col3(d.specular);
     m.h = d.hard;
     if (d.tex_type == YR_TEX_NONE || !(d.mod_color > 0 || d.mod_specular > 0 || d.mod_hard > 0)) return m;
-    const TexVal tv = texture_eval(d, tex_point(d, sp));
+    const TexVal tv = texture_eval(d, tex_point(d, sp, eye));
     const C &tex = tv.col;
     const float tf = tv.f, wc = d.mod_color, ws = d.mod_specular, wh = d.mod_hard;
     switch (d.mod_mode) {
@@ -1251,7 +1257,7 @@ Mod modulated(const Scene &S, const SP &sp) {
 
 // the diffuse colour after the modulator (genericShader_t::getDiffuse,
 // basicshaders.cc:191-204)
-C diffuse(const Scene &S, const SP &sp) { return modulated(S, sp).c; }
+C diffuse(const Scene &S, const SP &sp, const V &eye) { return modulated(S, sp, eye).c; }
 
 // genericShader_t::fromLight (basicshaders.cc:46-70)
 C fromLight(const Scene &S, const SP &sp, const V &ldir, const C &lcol, const V &eye) {
@@ -1259,7 +1265,7 @@ C fromLight(const Scene &S, const SP &sp, const V &ldir, const C &lcol, const V 
     V N = faceForward(sp.Ng, sp.N, edir);
     float inte = N * ldir;
     if (inte < 0) return C();
-    const Mod m = modulated(S, sp);
+    const Mod m = modulated(S, sp, eye);
     edir = reflectv(N, edir);
     float refle = edir * ldir;
     if (refle < 0) refle = 0;
@@ -1447,7 +1453,7 @@ int extra_rounds(const Scene &S, const C *sub, int P, float threshold) {
 // pathLight_t::normalSample + takeSample (pathlight.cc:223-403), explicit indices
 C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx) {
     V N = faceForward(sp.Ng, sp.N, eye);
-    C dif = diffuse(S, sp);
+    C dif = diffuse(S, sp, eye);
     if (below_cut(energy(dif))) return C();
     const int P = L.d.samples, depth = L.d.depth;
     C total, sub[4];
@@ -1481,7 +1487,7 @@ C illum_path(Scene &S, const Light &L, const SP &sp, const V &eye, const Ctx &cx
             total = total + contri;
             if (r == 0) sub[i % 4] = sub[i % 4] + contri;
             const V HN = faceForward(t.Ng, t.N, -ray);
-            raycolor = raycolor * diffuse(S, t);
+            raycolor = raycolor * diffuse(S, t, -ray);
             if (j + 1 < depth) {
                 const int lev = j + 1;
                 ray = cosHemi(HN, t.NU, t.NV,
@@ -1597,6 +1603,9 @@ void camera_sample(Scene &S, uint32_t pixel, uint32_t s, float *rgba) {
         return;
     }
     SP sp = surface(S, h.obj, h.tri, h.Z, f, ray);
+    // state.screenpos, given to the camera hit (scene.cc:234, 749-750, 798-799)
+    sp.sx = (float)(2.0 * (double)(((float)x + fx) / (float)S.cam.resx) - 1.0);
+    sp.sy = (float)(1.0 - 2.0 * (double)(((float)y + fy) / (float)S.cam.resy));
     Ctx cx;
     cx.pixel = pixel;
     cx.s = s;

@@ -444,6 +444,39 @@ def specmod_scene():
     return sc
 
 
+def texco_view_scene():
+    """Textures addressed by the screen position ("window") and by the
+    reflected eye direction ("reflect"), on spheres and the plane, with
+    AA samples (so the screen positions move inside the pixel)."""
+    sc = scenes.config_small(80, 60)
+    ts = scenes.texture_shader
+    sc.shaders = [
+        ts((0.6, 0.6, 0.6), "marble", (0.9, 0.9, 0.85), (0.2, 0.2, 0.3), mod_color=0.8, turbulence=2.0, size=2.0,
+           texco="window"),
+        ts((0.5, 0.5, 0.6), "musgrave", (0.2, 0.4, 0.1), (0.9, 0.9, 0.7), size=2.5, intensity=0.6, texco="reflect"),
+        ts((0.7, 0.7, 0.7), "clouds", (0.1, 0.2, 0.3), (0.9, 0.8, 0.6), mode="mul", mod_color=0.9, depth=3,
+           size=1.5, texco="reflect", proj=("z", "x", "y")),
+        ts((0.5, 0.6, 0.4), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mod_color=0.6, color_type="col1",
+           weight1=1.0, size=4.0, texco="window", proj=("y", "x", "n")),
+    ]
+    meshes = []
+    for k in range(3):
+        v, t = scenes.uv_sphere((-1.4 + 1.4 * k, -0.4, 0.0), 0.6, rings=16, segments=32)
+        meshes.append(scenes.Mesh(v, t, k))
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    meshes.append(scenes.Mesh(pv, pt, 3))
+    sc.meshes = meshes
+    sc.lights = [scenes.point_light((2.0, 4.0, 3.0), 14.0)]
+    sc.camera = scenes.camera((0.0, 2.5, 4.5), (0.0, -0.4, 0.0), (0.0, 3.5, 4.5), 80, 60)
+    sc.render.spp = 3
+    return sc
+
+
+def texco_view_render():
+    img, _ = T.harness_render(texco_view_scene())
+    np.savez_compressed(os.path.join(HERE, "render_texco_view_80x60.npz"), image=img)
+
+
 def specmod_render():
     img, _ = T.harness_render(specmod_scene())
     np.savez_compressed(os.path.join(HERE, "render_specmod_96x72.npz"), image=img)
@@ -580,6 +613,7 @@ if __name__ == "__main__":
     textures()
     texture_render()
     specmod_render()
+    texco_view_render()
     tonemap_renders()
     image_outputs()
     instances()

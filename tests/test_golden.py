@@ -273,6 +273,25 @@ def test_oracle_texture_render_matches_reference():
     assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
 
 
+def test_oracle_window_reflect_texco_matches_reference():
+    """Modulators addressed by the camera sample's screen position
+    ("window") and by the reflected eye ("reflect"), with AA samples and
+    swapped projection axes, against the reference's render."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    ref = load("render_texco_view_80x60.npz")["image"]
+    sc = make_golden.texco_view_scene()
+    img, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
+    # the texture coordinates matter: addressed globally instead, the image differs
+    for s in sc.shaders:
+        s.tex_map = s.tex_map & ~0xFF
+    plain, _ = T.OracleScene(sc).render()
+    assert np.abs(plain - ref).max() > 1e-2
+
+
 def test_oracle_specular_hardness_modulation_matches_reference():
     """Modulators that also drive the specular colour and the Phong
     exponent (the modulator's "specular" / "hard" weights, every mode,

@@ -377,7 +377,9 @@ static yr_status adj_plan(const yr_scene *scene, size_t budget, AdjPlan &A) {
     // the specular colour or exponent
     if (R.has_guess || R.path_threshold > 0.f) return YR_ERR_UNSUPPORTED;
     for (const yr_shader_desc &d : scene->shader_desc)
-        if (d.tex_type != YR_TEX_NONE && (d.mod_specular > 0.f || d.mod_hard > 0.f)) return YR_ERR_UNSUPPORTED;
+        if (d.tex_type != YR_TEX_NONE &&
+            (d.mod_specular > 0.f || d.mod_hard > 0.f || (d.tex_map & 0xffu) == YR_TEXCO_REFLECT))
+            return YR_ERR_UNSUPPORTED;  // (a reflected-eye texture differs between a vertex's shading calls)
     const Plan &P = A.P;
     uint64_t lo = 1, hi = P.rpix;
     while (lo < hi) {

@@ -274,6 +274,7 @@ struct Surf {
     int object;
     int shader;
     float Z;
+    float sx, sy;  // screen position of the camera sample (camera hits; 0 at path vertices)
 };
 
 // createCS (vector3d.h:240-258)
@@ -309,6 +310,7 @@ __device__ __forceinline__ V3 reflect(const V3 &n, const V3 &v) {
 __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender &R, int object, uint32_t tri,
                                              float Z, const V3 &from_w, const V3 &ray_w) {
     Surf s;
+    s.sx = s.sy = 0.f;
     // a reference's hit is formed in its original's space (the ray taken
     // there by M's inverse) and brought back below (reference.cc:100-112)
     const int inst = S.objects[object].inst;
@@ -359,11 +361,17 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
 }
 
 // Texture point of the procedural path of modulator_t::doMapping
-// (texture.cc:122-320): the texco source (hit point, or the shading
+// (texture.cc:122-320): the texco source (hit point, orco point, shading
+// normal, screen position, or the eye reflected about the face-forwarded
 // normal), then per axis size*(source[proj] + ofs), or size*ofs when the
-// axis is switched off.
-__device__ __forceinline__ V3 tex_point(const DevShader &sh, const Surf &sp) {
-    const V3 &src = sh.texco == YR_TEXCO_NORMAL ? sp.N : (sh.texco == YR_TEXCO_ORCO ? sp.orco : sp.P);
+// axis is switched off.  `eye`: the direction the shading call looks from.
+__device__ __forceinline__ V3 tex_point(const DevShader &sh, const Surf &sp, const V3 &eye) {
+    V3 src = sh.texco == YR_TEXCO_NORMAL ? sp.N : (sh.texco == YR_TEXCO_ORCO ? sp.orco : sp.P);
+    if (sh.texco == YR_TEXCO_WINDOW) src = v3(sp.sx, sp.sy, 0.f);
+    if (sh.texco == YR_TEXCO_REFLECT) {  // texture.cc:158-165
+        const V3 neye = normalize(eye);
+        src = reflect(face_forward(sp.Ng, sp.N, neye), neye);
+    }
     float t[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -388,13 +396,14 @@ struct TexDeriv {
 // mix(tex, S, ws), H = f*wh + H*(1-wh); mul: mix(tex, 1, w) * C (S alike),
 // H = (f*wh + (1-wh)) * H; add: tex*w + C, f*wh + H; sub: tex*(-w) + C,
 // f*(-wh) + H - with tex the texture's colour and f its value (getFloat).
-__device__ __forceinline__ void modulated_all(const DevShader *shp, const Surf &sp, C3 &C, C3 &S, float &H) {
+__device__ __forceinline__ void modulated_all(const DevShader *shp, const Surf &sp, const V3 &eye, C3 &C, C3 &S,
+                                              float &H) {
     const DevShader &sh = *shp;
     C = sh.color;
     S = sh.specular;
     H = sh.hard;
     if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f || sh.mod_spec > 0.f || sh.mod_hard > 0.f)) return;
-    const TexEval te = texture_eval(shp, tex_point(sh, sp));
+    const TexEval te = texture_eval(shp, tex_point(sh, sp, eye));
     const C3 tex = te.col;
     const float f = te.f, wc = sh.mod_color, ws = sh.mod_spec, wh = sh.mod_hard;
     const C3 one = c3(1.f, 1.f, 1.f);
@@ -429,17 +438,18 @@ __device__ __forceinline__ void modulated_all(const DevShader *shp, const Surf &
 // a*w + (1-w)*b and returns a for w > 1.  `td` (optional) receives what
 // the adjoint needs.
 // `shp` points at the shader record in device memory.
-__device__ __forceinline__ C3 modulated_color(const DevShader *shp, const Surf &sp, TexDeriv *td = nullptr) {
+__device__ __forceinline__ C3 modulated_color(const DevShader *shp, const Surf &sp, const V3 &eye,
+                                              TexDeriv *td = nullptr) {
     const DevShader &sh = *shp;
     const C3 C = sh.color;
     if (sh.tex_type == YR_TEX_NONE || !(sh.mod_color > 0.f)) return C;
     if (sh.mod_spec > 0.f || sh.mod_hard > 0.f) {  // one texture evaluation for all three channels
         C3 c, s;
         float h;
-        modulated_all(shp, sp, c, s, h);
+        modulated_all(shp, sp, eye, c, s, h);
         return c;
     }
-    const TexEval te = texture_eval(shp, tex_point(sh, sp));
+    const TexEval te = texture_eval(shp, tex_point(sh, sp, eye));
     if (td) {
         td->tex = te.col;
         td->dint = te.dint;

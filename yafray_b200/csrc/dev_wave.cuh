@@ -107,6 +107,13 @@ __device__ __forceinline__ uint32_t path_index(const DevRender &R, const Wave &W
 }
 
 // ---------------------------------------------------------------- camera
+// state.screenpos of a camera sample at pixel (x, y), sub-pixel (fx, fy),
+// given to its camera hit (scene.cc:234, 749-750, 798-799)
+__device__ __forceinline__ void screen_pos(const DevRender &R, int x, int y, float fx, float fy, Surf &sp) {
+    sp.sx = (float)(2.0 * (double)(((float)x + fx) / (float)R.cam.resx) - 1.0);
+    sp.sy = (float)(1.0 - 2.0 * (double)(((float)y + fy) / (float)R.cam.resy));
+}
+
 // camera_t::shootRay, CM_PERSPECTIVE (camera.cc:184-188)
 __device__ __forceinline__ V3 camera_ray(const DevCamera &c, float px, float py) {
     return normalize(c.vto + (c.vright * px + c.vup * py));
@@ -234,9 +241,9 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
         if (!ADJ && (sh.mod_spec > 0.f || sh.mod_hard > 0.f)) {
             // the modulator also sets this point's specular colour and
             // Phong exponent (fromLight, basicshaders.cc:55-62)
-            modulated_all(R.shaders + sp.shader, sp, lkc, sh.specular, sh.hard);
+            modulated_all(R.shaders + sp.shader, sp, eye, lkc, sh.specular, sh.hard);
         } else {
-            lkc = modulated_color(R.shaders + sp.shader, sp, ADJ ? td_out : nullptr);
+            lkc = modulated_color(R.shaders + sp.shader, sp, eye, ADJ ? td_out : nullptr);
         }
         if (ADJ) *lkc_out = lkc;
     }
@@ -513,6 +520,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
             const V3 ray = camera_ray(R.cam, (float)x + fx, (float)y + fy);
             const V3 f = R.cam.pos + ray * kMinRayDist;
             sp = make_surface(S, R, obj, __float_as_uint(h.z), h.x, f, ray);
+            screen_pos(R, x, y, fx, fy, sp);
             eye = R.cam.pos - sp.P;  // scene_t::light: eye = from - sp.P()
             active = true;
         }
@@ -535,7 +543,7 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
     bool paths = false;
     if (active) {
         const DevShader sh = R.shaders[sp.shader];
-        const C3 dif = modulated_color(R.shaders + sp.shader, sp);
+        const C3 dif = modulated_color(R.shaders + sp.shader, sp, eye);  // getDiffuse(sp, eye)
         paths = !(energy(dif) < 0.05f);
         const DevLight PL = R.lights[R.path_light];
         W.diff0[i] = make_float4(dif.r, dif.g, dif.b, paths ? PL.power : 0.f);
@@ -718,7 +726,7 @@ __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender
         shade_lights(S, R, W, active, sp, eye, p, j + 1, path_index(R, W, s, pi), pixel, W.p_aux);
     }
     if (active) {
-        if (!ADJ) dif = modulated_color(R.shaders + sp.shader, sp);
+        if (!ADJ) dif = modulated_color(R.shaders + sp.shader, sp, -ray);  // getDiffuse(tempsp, -ray)
         const float4 col = W.p_col[p];
         const C3 nc = c3(col.x, col.y, col.z) * dif;
         W.p_next[p] = make_float4(nc.r, nc.g, nc.b, 0.f);
@@ -758,6 +766,7 @@ __device__ __forceinline__ void st_guess_camera(const DevScene &S, const DevRend
             const V3 ray = camera_ray(R.cam, (float)x + fx, (float)y + fy);
             const V3 f = R.cam.pos + ray * kMinRayDist;
             sp = make_surface(S, R, obj, __float_as_uint(h.z), h.x, f, ray);
+            screen_pos(R, x, y, fx, fy, sp);
             eye = R.cam.pos - sp.P;
             active = true;
         }

@@ -165,7 +165,7 @@ void make_shader(const yr_shader_desc &d, DevShader &o) {
 // modulator mode, shape / type / metric fields of the texture used).
 bool valid_shader(const yr_shader_desc &d) {
     if (d.tex_type > YR_TEX_GRADIENT || d.mod_mode > YR_MOD_SUB) return false;
-    if ((d.tex_map & 0xffu) > YR_TEXCO_NORMAL) return false;
+    if ((d.tex_map & 0xffu) > YR_TEXCO_REFLECT) return false;
     for (int k = 1; k < 4; k++)
         if (((d.tex_map >> (8 * k)) & 0xffu) > YR_PROJ_NONE) return false;
     if (d.tex_type == YR_TEX_NONE) return true;

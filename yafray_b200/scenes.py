@@ -165,8 +165,10 @@ def shader(color, specular=(0.0, 0.0, 0.0), hard=1.0) -> abi.YrShaderDesc:
 
 def tex_map(texco="global", proj=("x", "y", "z")) -> int:
     """yr_shader_desc.tex_map from the modulator's "texco" and "proj_x/y/z"
-    parameters ("global" / "orco" / "normal"; axes "x" "y" "z" or "n")."""
-    tc = {"global": abi.YR_TEXCO_GLOBAL, "orco": abi.YR_TEXCO_ORCO, "normal": abi.YR_TEXCO_NORMAL}[texco]
+    parameters ("global" / "orco" / "normal" / "window" / "reflect"; axes
+    "x" "y" "z" or "n")."""
+    tc = {"global": abi.YR_TEXCO_GLOBAL, "orco": abi.YR_TEXCO_ORCO, "normal": abi.YR_TEXCO_NORMAL,
+          "window": abi.YR_TEXCO_WINDOW, "reflect": abi.YR_TEXCO_REFLECT}[texco]
     pc = {"x": abi.YR_PROJ_X, "y": abi.YR_PROJ_Y, "z": abi.YR_PROJ_Z, "n": abi.YR_PROJ_NONE}
     return tc | (pc[proj[0]] << 8) | (pc[proj[1]] << 16) | (pc[proj[2]] << 24)
 
