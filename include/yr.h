@@ -271,8 +271,10 @@ typedef struct yr_shader_desc {
  * whose surface point has no screen position (scene.cc:234, 749);
  * TEXCO_REFLECT the eye direction reflected about the face-forwarded
  * normal, the eye being the direction the shading call looks from
- * (texture.cc:148-165). */
-enum { YR_TEXCO_GLOBAL = 0, YR_TEXCO_ORCO = 1, YR_TEXCO_NORMAL = 2, YR_TEXCO_WINDOW = 3, YR_TEXCO_REFLECT = 4 };
+ * (texture.cc:148-165); TEXCO_UV the hit's texture coordinates as
+ * (2u - 1, 1 - 2v, 0) (texture.cc:127-133, yr_object_desc.uvs). */
+enum { YR_TEXCO_GLOBAL = 0, YR_TEXCO_ORCO = 1, YR_TEXCO_NORMAL = 2, YR_TEXCO_WINDOW = 3, YR_TEXCO_REFLECT = 4,
+       YR_TEXCO_UV = 5 };
 enum { YR_PROJ_DEFAULT = 0, YR_PROJ_X = 1, YR_PROJ_Y = 2, YR_PROJ_Z = 3, YR_PROJ_NONE = 4 };
 
 enum { YR_LIGHT_POINT = 0, YR_LIGHT_AREA = 1, YR_LIGHT_HEMI = 2, YR_LIGHT_PATH = 3 };
@@ -399,6 +401,13 @@ typedef struct yr_object_desc {
                                 referenceObject_t::back here.                */
     uint32_t instance_of;
     uint32_t reserved2;
+    const float *uvs;        /* optional texture coordinates per triangle: u, v
+                                at corners a, b, c (6 floats per triangle, the
+                                mesh's facesuv); NULL = none.  The hit's (u, v)
+                                is their barycentric blend (triangle_t::
+                                getSurface, triangle.cc:156-160); without
+                                them it is (-1, -1) on a flat mesh and (0, 0)
+                                on a smoothed one, as the reference's          */
 } yr_object_desc;
 
 #define YR_PER_TRIANGLE 0xffffffffu

@@ -178,6 +178,7 @@ struct SceneFile {
         std::vector<float> v;
         std::vector<uint32_t> t;
         std::vector<uint32_t> tri_shader;  // when shader == YR_PER_TRIANGLE
+        std::vector<float> uv;             // 6 per triangle (record version 6), or none
     };
     std::vector<Obj> objs;
 };
@@ -226,6 +227,10 @@ static void load_scene(const char *path, SceneFile &s) {
             o.nv = o.nt = 0;
             o.shader = oh[2];
             o.cast = oh[3];
+            if (hdr[3] >= 6) {  // record version 6: texture coordinates flag (none on a reference)
+                int32_t has_uv = 0;
+                rd(f, &has_uv, 4);
+            }
             continue;
         }
         o.nv = oh[0];
@@ -239,6 +244,14 @@ static void load_scene(const char *path, SceneFile &s) {
         if (o.shader == YR_PER_TRIANGLE) {
             o.tri_shader.resize(o.nt);
             rd(f, &o.tri_shader[0], 4 * o.nt);
+        }
+        if (hdr[3] >= 6) {  // record version 6: texture coordinates, 6 per triangle
+            int32_t has_uv = 0;
+            rd(f, &has_uv, 4);
+            if (has_uv) {
+                o.uv.resize(6 * (size_t)o.nt);
+                rd(f, &o.uv[0], 4 * o.uv.size());
+            }
         }
     }
     fclose(f);
@@ -333,8 +346,8 @@ static shader_t *make_shader(const yr_shader_desc &d, std::vector<texture_t *> &
         modu.reflection(0);
         modu.displace(0);
         modu.string2maptype("flat");
-        static const char *texco[5] = {"global", "orco", "normal", "window", "reflect"};
-        modu.string2texcotype(texco[(d.tex_map & 0xffu) < 5 ? (d.tex_map & 0xffu) : 0]);
+        static const char *texco[6] = {"global", "orco", "normal", "window", "reflect", "uv"};
+        modu.string2texcotype(texco[(d.tex_map & 0xffu) < 6 ? (d.tex_map & 0xffu) : 0]);
         modu.string2cliptype("extend");
         std::string proj[3];
         for (int k = 0; k < 3; k++) {
@@ -396,12 +409,15 @@ static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true, 
         if (o.shader == YR_PER_TRIANGLE)  // triangle_t::setShader, used by getSurface
             for (uint32_t k = 0; k < o.nt; k++) ts[k].setShader(r.shaders.at(o.tri_shader[k]));
         std::vector<vector3d_t> nor;
-        std::vector<GFLOAT> fuv;
+        std::vector<GFLOAT> fuv(o.uv.begin(), o.uv.end());
         std::vector<CFLOAT> fvcol;
+        if (!fuv.empty())  // each triangle's six coordinates, as the loader sets them
+            for (uint32_t k = 0; k < o.nt; k++) ts[k].setUV(fuv.begin() + 6 * (size_t)k);
         meshObject_t *m = meshObject_t::factory(ver, nor, ts, fuv, fvcol);
         m->setShader(r.shaders.at(o.shader == YR_PER_TRIANGLE ? o.tri_shader[0] : o.shader));
         m->castShadows(o.cast != 0);
         if (o.smooth >= 1.f) m->autoSmooth(o.smooth);  // as the loader does (render.cc:764)
+        m->tangentsFromUV();                           // render.cc:765 (nothing without uv or orco)
         r.meshes.push_back(m);
         r.objs.push_back(m);
         r.objindex[m] = (int)i;

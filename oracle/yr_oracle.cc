@@ -158,6 +158,7 @@ struct Obj {
     std::vector<V> tri_na, tri_nb, tri_nc;  // corner normals when smoothed
     bool smooth = false;
     std::vector<uint32_t> tri_shader;
+    std::vector<float> tri_uv;  // 6 per triangle (u, v at a, b, c), or none
     std::vector<yr_kd_node> nodes;
     std::vector<uint32_t> prims;
     Box tb, ob;
@@ -1117,6 +1118,7 @@ struct SP {
     int obj;
     int shader;
     float sx = 0.f, sy = 0.f;  // screen position (camera hits only; 0 elsewhere)
+    float u = -1.f, v = -1.f;  // texture coordinates (triangle_t::getSurface)
 };
 
 void createCS(const V &N, V &u, V &v) {  // vector3d.h:240-258
@@ -1147,7 +1149,12 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from_w, cons
     s.P = from + Z * ray;
     const Obj &o = ref ? S.objs[ow.inst] : ow;
     s.N = s.Ng = o.tri_n[tri];
-    if (o.smooth) {
+    const bool has_uv = !o.tri_uv.empty();
+    // without uv, corner normals or orco, getSurface returns u = v = -1 at
+    // once; otherwise u, v are the barycentric blend of the triangle's
+    // coordinates, or 0 without any (triangle.cc:138-160)
+    if (o.smooth || has_uv) s.u = s.v = 0.f;
+    if (o.smooth || has_uv) {
         // triangle_t::getSurface + getInterpolation (triangle.cc:74-155), in
         // the shipped build's evaluation order (fast-math): the reciprocal
         // of the denominator, fa from the sum of the numerators, and
@@ -1164,9 +1171,16 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from_w, cons
         }
         const float an = uu0 * vv2 - vv0 * uu2, bn = uu1 * vv0 - vv1 * uu0, den = uu1 * vv2 - vv1 * uu2;
         const float rc = 1.f / den, fb = an * rc, fc = bn * rc, fa = 1.f - (an + bn) * rc;
-        const V &na = o.tri_na[tri], &nb = o.tri_nb[tri], &nc = o.tri_nc[tri];
-        s.N = normalize(V(na.x * fa + (nb.x * fb + nc.x * fc), na.y * fa + (nb.y * fb + nc.y * fc),
-                          na.z * fa + (nb.z * fb + nc.z * fc)));
+        if (o.smooth) {
+            const V &na = o.tri_na[tri], &nb = o.tri_nb[tri], &nc = o.tri_nc[tri];
+            s.N = normalize(V(na.x * fa + (nb.x * fb + nc.x * fc), na.y * fa + (nb.y * fb + nc.y * fc),
+                              na.z * fa + (nb.z * fb + nc.z * fc)));
+        }
+        if (has_uv) {
+            const float *uv = &o.tri_uv[6 * (size_t)tri];
+            s.u = uv[0] * fa + (uv[2] * fb + uv[4] * fc);
+            s.v = uv[1] * fa + (uv[3] * fb + uv[5] * fc);
+        }
     }
     createCS(s.N, s.NU, s.NV);
     s.orco = s.P;
@@ -1192,6 +1206,7 @@ V tex_point(const yr_shader_desc &d, const SP &sp, const V &eye) {
     const uint32_t tc = d.tex_map & 0xffu;
     V src = tc == YR_TEXCO_NORMAL ? sp.N : (tc == YR_TEXCO_ORCO ? sp.orco : sp.P);
     if (tc == YR_TEXCO_WINDOW) src = V(sp.sx, sp.sy, 0.f);
+    if (tc == YR_TEXCO_UV) src = V((float)((double)sp.u * 2.0 - 1.0), (float)(1.0 - (double)sp.v * 2.0), 0.f);
     if (tc == YR_TEXCO_REFLECT) {  // texture.cc:158-165
         const V neye = normalize(eye);
         src = reflectv(faceForward(sp.Ng, sp.N, neye), neye);
@@ -1721,6 +1736,8 @@ orc_scene *orc_load(const char *path) {
                 for (int a = 0; a < 3; a++)
                     for (int b = 0; b < 4; b++) S.objs[i].back[4 * a + b] = inv[4 * a + b];
             S.objs[i].inst = inst;
+            int32_t has_uv = 0;  // record version 6: texture coordinates flag (none on a reference)
+            if (ok && hdr[3] >= 6) ok = rdv(f, &has_uv, 1);
             continue;
         }
         std::vector<float> v(3 * (size_t)oh[0]);
@@ -1731,6 +1748,14 @@ orc_scene *orc_load(const char *path) {
             ok = rdv(f, ts.data(), ts.size());
         }
         Obj &ob = S.objs[i];
+        if (ok && hdr[3] >= 6) {  // record version 6: texture coordinates, 6 per triangle
+            int32_t has_uv = 0;
+            ok = rdv(f, &has_uv, 1);
+            if (ok && has_uv) {
+                ob.tri_uv.resize(6 * (size_t)oh[1]);
+                ok = rdv(f, ob.tri_uv.data(), ob.tri_uv.size());
+            }
+        }
         ob.cast = oh[3] != 0;
         for (uint32_t k = 0; ok && k < oh[1]; k++) {
             V a = vtx(v, t[3 * k]), b = vtx(v, t[3 * k + 1]), c = vtx(v, t[3 * k + 2]);

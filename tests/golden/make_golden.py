@@ -472,6 +472,57 @@ def texco_view_scene():
     return sc
 
 
+def sphere_uvs(verts, tris, center):
+    """Per-corner (u, v) of a sphere's triangles from each corner's
+    longitude and latitude about `center` (seams are not fixed up)."""
+    d = verts[tris.reshape(-1)].astype(np.float64) - np.asarray(center, np.float64)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    u = (np.arctan2(d[:, 2], d[:, 0]) / (2 * np.pi)) % 1.0
+    v = np.arccos(np.clip(d[:, 1], -1, 1)) / np.pi
+    return np.stack([u, v], -1).reshape(-1, 6).astype(np.float32)
+
+
+def texco_uv_scene():
+    """Textures addressed by the triangles' texture coordinates ("uv"): a
+    sphere and the plane with coordinates, a smoothed sphere and a flat
+    sphere without them (u, v = 0 and -1), each with its own texture."""
+    sc = scenes.config_small(80, 60)
+    ts = scenes.texture_shader
+    sc.shaders = [
+        ts((0.6, 0.6, 0.6), "marble", (0.9, 0.9, 0.85), (0.2, 0.2, 0.3), mod_color=0.8, turbulence=1.0, size=3.0,
+           texco="uv"),
+        ts((0.5, 0.5, 0.6), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mod_color=0.7, color_type="col1",
+           weight1=1.0, size=3.0, texco="uv"),
+        ts((0.7, 0.6, 0.5), "clouds", (0.1, 0.2, 0.3), (0.9, 0.8, 0.6), mode="mul", mod_color=0.9, depth=3,
+           size=1.5, texco="uv", proj=("y", "x", "n")),
+        ts((0.5, 0.6, 0.4), "musgrave", (0.2, 0.4, 0.1), (0.9, 0.9, 0.7), size=2.0, intensity=0.6, texco="uv"),
+    ]
+    meshes = []
+    for k in range(3):
+        c = (-1.4 + 1.4 * k, -0.4, 0.0)
+        v, t = scenes.uv_sphere(c, 0.6, rings=16, segments=32)
+        m = scenes.Mesh(v, t, k)
+        if k == 0:
+            m.uvs = sphere_uvs(v, t, c)
+        if k == 1:
+            m.smooth_angle = 180.0
+        meshes.append(m)
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    plane = scenes.Mesh(pv, pt, 3)
+    plane.uvs = ((pv[pt.reshape(-1)][:, [0, 2]] + 20.0) / 40.0).astype(np.float32).reshape(-1, 6)
+    meshes.append(plane)
+    sc.meshes = meshes
+    sc.lights = [scenes.point_light((2.0, 4.0, 3.0), 14.0)]
+    sc.camera = scenes.camera((0.0, 2.5, 4.5), (0.0, -0.4, 0.0), (0.0, 3.5, 4.5), 80, 60)
+    sc.render.spp = 2
+    return sc
+
+
+def texco_uv_render():
+    img, _ = T.harness_render(texco_uv_scene())
+    np.savez_compressed(os.path.join(HERE, "render_texco_uv_80x60.npz"), image=img)
+
+
 def texco_view_render():
     img, _ = T.harness_render(texco_view_scene())
     np.savez_compressed(os.path.join(HERE, "render_texco_view_80x60.npz"), image=img)
@@ -614,6 +665,7 @@ if __name__ == "__main__":
     texture_render()
     specmod_render()
     texco_view_render()
+    texco_uv_render()
     tonemap_renders()
     image_outputs()
     instances()

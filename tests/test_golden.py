@@ -292,6 +292,24 @@ def test_oracle_window_reflect_texco_matches_reference():
     assert np.abs(plain - ref).max() > 1e-2
 
 
+def test_oracle_uv_texco_matches_reference():
+    """Modulators addressed by texture coordinates ("uv"): a sphere and the
+    plane with per-triangle coordinates, a smoothed sphere (u = v = 0) and a
+    flat one (u = v = -1) without them, against the reference's render."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    ref = load("render_texco_uv_80x60.npz")["image"]
+    sc = make_golden.texco_uv_scene()
+    img, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
+    for m in sc.meshes:  # the coordinates matter
+        m.uvs = None
+    plain, _ = T.OracleScene(sc).render()
+    assert np.abs(plain - ref).max() > 1e-2
+
+
 def test_oracle_specular_hardness_modulation_matches_reference():
     """Modulators that also drive the specular colour and the Phong
     exponent (the modulator's "specular" / "hard" weights, every mode,

@@ -36,7 +36,7 @@ GRADIENT_TYPES = {"linear": 0, "quadratic": 1, "cubic": 2, "diagonal": 3, "spher
 MOD_MODES = {"mix": 0, "mul": 1, "add": 2, "sub": 3}
 YR_LIGHT_POINT, YR_LIGHT_AREA, YR_LIGHT_HEMI, YR_LIGHT_PATH = 0, 1, 2, 3
 YR_BATCH_AUTO, YR_BATCH_TILES, YR_BATCH_WAVES = 0, 1, 2
-YR_TEXCO_GLOBAL, YR_TEXCO_ORCO, YR_TEXCO_NORMAL, YR_TEXCO_WINDOW, YR_TEXCO_REFLECT = 0, 1, 2, 3, 4
+YR_TEXCO_GLOBAL, YR_TEXCO_ORCO, YR_TEXCO_NORMAL, YR_TEXCO_WINDOW, YR_TEXCO_REFLECT, YR_TEXCO_UV = 0, 1, 2, 3, 4, 5
 YR_PROJ_DEFAULT, YR_PROJ_X, YR_PROJ_Y, YR_PROJ_Z, YR_PROJ_NONE = 0, 1, 2, 3, 4
 YR_RENDER_SHADOW_TREE, YR_RENDER_EXACT_ORDER, YR_RENDER_TONEMAP = 1, 2, 4
 YR_RENDER_CLAMP_RGB, YR_RENDER_ALPHA_PREMULTIPLY = 8, 16
@@ -121,7 +121,8 @@ class YrObjectDesc(C.Structure):
                 ("tri_shaders", C.POINTER(C.c_uint32)), ("tree", C.POINTER(YrKdTree)),
                 ("smooth_angle", C.c_float), ("reserved", C.c_uint32),
                 ("instance_matrix", C.POINTER(C.c_float)), ("instance_inverse", C.POINTER(C.c_float)),
-                ("instance_of", C.c_uint32), ("reserved2", C.c_uint32)]
+                ("instance_of", C.c_uint32), ("reserved2", C.c_uint32),
+                ("uvs", C.POINTER(C.c_float))]
 
 
 class YrSceneDesc(C.Structure):

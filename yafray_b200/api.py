@@ -55,6 +55,11 @@ class DeviceScene:
                 ts = np.ascontiguousarray(m.tri_shaders, np.uint32)
                 self._keep.append(ts)
                 objs[i].tri_shaders = ts.ctypes.data_as(C.POINTER(C.c_uint32))
+            if m.uvs is not None:
+                uv = np.ascontiguousarray(m.uvs, np.float32).reshape(-1, 6)
+                assert uv.shape[0] == t.shape[0]
+                self._keep.append(uv)
+                objs[i].uvs = uv.ctypes.data_as(C.POINTER(C.c_float))
         shaders = (abi.YrShaderDesc * len(sc.shaders))(*sc.shaders)
         lights = (abi.YrLightDesc * max(1, len(sc.lights)))(*sc.lights)
         desc = abi.YrSceneDesc()

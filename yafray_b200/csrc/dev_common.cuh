@@ -90,7 +90,8 @@ struct DevObject {
     uint32_t root;      // global index of the root kd node
     uint32_t tri_base;  // first global triangle index
     uint32_t ntris;
-    uint32_t flags;     // bit0: casts shadows, bit1: smoothed (corner normals in DevScene::tri_nrm)
+    uint32_t flags;     // bit0: casts shadows, bit1: smoothed (corner normals in DevScene::tri_nrm),
+                        // bit2: texture coordinates (DevScene::tri_uv)
     float ob[6];        // object bound (meshObject_t::getBound), the object tree's leaf box
     int inst;           // instance record (DevScene::insts) or -1; the tree
                         // and triangle fields above are then the original's
@@ -131,6 +132,7 @@ struct DevScene {
     const DevObject *objects;
     const DevInst *insts;       // instance matrices (referenceObject_t)
     const float *tri_nrm;       // corner normals, 9 per triangle, of smoothed objects
+    const float *tri_uv;        // texture coordinates, 6 per triangle, of objects that have them
     // object tree (geomeTree_t): per interior node 4 x float4 = left box
     // (min xyz, max xyz), right box, then the children's codes (>= 0:
     // interior node, < 0: ~object index) as int bits

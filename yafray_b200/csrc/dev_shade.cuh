@@ -275,6 +275,7 @@ struct Surf {
     int shader;
     float Z;
     float sx, sy;  // screen position of the camera sample (camera hits; 0 at path vertices)
+    float u, v;    // texture coordinates (triangle_t::getSurface)
 };
 
 // createCS (vector3d.h:240-258)
@@ -322,7 +323,12 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
                  r = __ldg(S.tris + 3 * (size_t)tri + 2);
     s.Ng = v3(p.w, q.w, r.w);
     s.N = s.Ng;
-    if (S.objects[object].flags & 2u) {
+    // without texture coordinates or corner normals getSurface returns
+    // u = v = -1 at once; otherwise the coordinates' barycentric blend, or 0
+    // without any (triangle.cc:138-160)
+    const uint32_t oflags = S.objects[object].flags;
+    s.u = s.v = (oflags & 6u) ? 0.f : -1.f;
+    if (oflags & 6u) {
         const V3 a = v3(p.x, p.y, p.z), b = v3(q.x, q.y, q.z), c = v3(r.x, r.y, r.z), &h = s.P;
         const float nx = fabsf(s.Ng.x), ny = fabsf(s.Ng.y), nz = fabsf(s.Ng.z);
         float uu0, vv0, uu1, vv1, uu2, vv2;
@@ -338,11 +344,18 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
         const float denum = uu1 * vv2 - vv1 * uu2;
         const float rd = 1.f / denum;
         const float fb = alpha * rd, fc = beta * rd, fa = 1.f - (alpha + beta) * rd;
-        const float *cn = S.tri_nrm + 9 * (size_t)tri;
-        const V3 nn = v3(__ldg(cn + 0) * fa + (__ldg(cn + 3) * fb + __ldg(cn + 6) * fc),
-                         __ldg(cn + 1) * fa + (__ldg(cn + 4) * fb + __ldg(cn + 7) * fc),
-                         __ldg(cn + 2) * fa + (__ldg(cn + 5) * fb + __ldg(cn + 8) * fc));
-        s.N = normalize(nn);
+        if (oflags & 2u) {
+            const float *cn = S.tri_nrm + 9 * (size_t)tri;
+            const V3 nn = v3(__ldg(cn + 0) * fa + (__ldg(cn + 3) * fb + __ldg(cn + 6) * fc),
+                             __ldg(cn + 1) * fa + (__ldg(cn + 4) * fb + __ldg(cn + 7) * fc),
+                             __ldg(cn + 2) * fa + (__ldg(cn + 5) * fb + __ldg(cn + 8) * fc));
+            s.N = normalize(nn);
+        }
+        if (oflags & 4u) {
+            const float *uv = S.tri_uv + 6 * (size_t)tri;
+            s.u = __ldg(uv + 0) * fa + (__ldg(uv + 2) * fb + __ldg(uv + 4) * fc);
+            s.v = __ldg(uv + 1) * fa + (__ldg(uv + 3) * fb + __ldg(uv + 5) * fc);
+        }
     }
     create_cs(s.N, s.NU, s.NV);
     s.orco = s.P;
@@ -368,6 +381,7 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
 __device__ __forceinline__ V3 tex_point(const DevShader &sh, const Surf &sp, const V3 &eye) {
     V3 src = sh.texco == YR_TEXCO_NORMAL ? sp.N : (sh.texco == YR_TEXCO_ORCO ? sp.orco : sp.P);
     if (sh.texco == YR_TEXCO_WINDOW) src = v3(sp.sx, sp.sy, 0.f);
+    if (sh.texco == YR_TEXCO_UV) src = v3((float)((double)sp.u * 2.0 - 1.0), (float)(1.0 - (double)sp.v * 2.0), 0.f);
     if (sh.texco == YR_TEXCO_REFLECT) {  // texture.cc:158-165
         const V3 neye = normalize(eye);
         src = reflect(face_forward(sp.Ng, sp.N, neye), neye);

@@ -165,7 +165,7 @@ void make_shader(const yr_shader_desc &d, DevShader &o) {
 // modulator mode, shape / type / metric fields of the texture used).
 bool valid_shader(const yr_shader_desc &d) {
     if (d.tex_type > YR_TEX_GRADIENT || d.mod_mode > YR_MOD_SUB) return false;
-    if ((d.tex_map & 0xffu) > YR_TEXCO_REFLECT) return false;
+    if ((d.tex_map & 0xffu) > YR_TEXCO_UV) return false;
     for (int k = 1; k < 4; k++)
         if (((d.tex_map >> (8 * k)) & 0xffu) > YR_PROJ_NONE) return false;
     if (d.tex_type == YR_TEX_NONE) return true;
@@ -389,6 +389,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     std::vector<uint2> nodes;
     std::vector<uint32_t> prims, tri_shader;
     std::vector<float> tri_nrm;  // 9 per triangle (corner normals) up to the last smoothed object
+    std::vector<float> tri_uv;   // 6 per triangle (texture coordinates) up to the last object with them
     std::vector<DevObject> objects;
     std::vector<Box> obounds;
     size_t total_tris = 0;
@@ -513,6 +514,13 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
             if (tri_nrm.size() < 9 * (size_t)tri_base) tri_nrm.resize(9 * (size_t)tri_base, 0.f);
             tri_nrm.insert(tri_nrm.end(), cn.begin(), cn.end());
         }
+        // texture coordinates (the mesh's facesuv), 6 per triangle
+        if (od.uvs) {
+            for (size_t k = 0; k < 6 * (size_t)od.ntris; k++)
+                if (!std::isfinite(od.uvs[k])) return fail(YR_ERR_INVALID_ARG);
+            if (tri_uv.size() < 6 * (size_t)tri_base) tri_uv.resize(6 * (size_t)tri_base, 0.f);
+            tri_uv.insert(tri_uv.end(), od.uvs, od.uvs + 6 * (size_t)od.ntris);
+        }
         for (const yr_kd_node &nd : tree.nodes) {
             uint2 g;
             g.y = nd.flags;
@@ -543,7 +551,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         dob.root = node_base;
         dob.tri_base = tri_base;
         dob.ntris = od.ntris;
-        dob.flags = (od.cast_shadows ? 1u : 0u) | (smooth ? 2u : 0u);
+        dob.flags = (od.cast_shadows ? 1u : 0u) | (smooth ? 2u : 0u) | (od.uvs ? 4u : 0u);
         const Box obb = mesh_bound(od.verts, od.tris, od.ntris);
         std::memcpy(dob.ob, obb.a, 12);
         std::memcpy(dob.ob + 3, obb.g, 12);
@@ -710,8 +718,9 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     if (prims.empty()) d_prims = nullptr;
     if ((st = dev_upload(s, tri_shader.data(), tri_shader.size(), (uint32_t **)&d_tri_shader)) != YR_OK)
         return fail(st);
-    const float *d_tri_nrm = nullptr;
+    const float *d_tri_nrm = nullptr, *d_tri_uv = nullptr;
     if ((st = dev_upload(s, tri_nrm.data(), tri_nrm.size(), (float **)&d_tri_nrm)) != YR_OK) return fail(st);
+    if ((st = dev_upload(s, tri_uv.data(), tri_uv.size(), (float **)&d_tri_uv)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
     const DevInst *d_insts = nullptr;
     if (!insts.empty() && (st = dev_upload(s, insts.data(), insts.size(), (DevInst **)&d_insts)) != YR_OK)
@@ -736,6 +745,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.objects = d_objects;
     D.insts = d_insts;
     D.tri_nrm = d_tri_nrm;
+    D.tri_uv = d_tri_uv;
     D.onodes = d_onodes;
     D.oroot = oroot;
     D.sonodes = d_sonodes;

@@ -102,6 +102,7 @@ class Mesh:
     instance_of: int = -1       # >= 0: a referenceObject_t of that mesh, placed by `matrix`
     matrix: Optional[np.ndarray] = None   # 4x4 row-major (instances only)
     inverse: Optional[np.ndarray] = None  # optional M^-1 (else computed by the library)
+    uvs: Optional[np.ndarray] = None      # optional (ntris, 6) texture coordinates (u, v at a, b, c)
 
     @property
     def is_instance(self) -> bool:
@@ -165,10 +166,10 @@ def shader(color, specular=(0.0, 0.0, 0.0), hard=1.0) -> abi.YrShaderDesc:
 
 def tex_map(texco="global", proj=("x", "y", "z")) -> int:
     """yr_shader_desc.tex_map from the modulator's "texco" and "proj_x/y/z"
-    parameters ("global" / "orco" / "normal" / "window" / "reflect"; axes
+    parameters ("global" / "orco" / "normal" / "window" / "reflect" / "uv"; axes
     "x" "y" "z" or "n")."""
     tc = {"global": abi.YR_TEXCO_GLOBAL, "orco": abi.YR_TEXCO_ORCO, "normal": abi.YR_TEXCO_NORMAL,
-          "window": abi.YR_TEXCO_WINDOW, "reflect": abi.YR_TEXCO_REFLECT}[texco]
+          "window": abi.YR_TEXCO_WINDOW, "reflect": abi.YR_TEXCO_REFLECT, "uv": abi.YR_TEXCO_UV}[texco]
     pc = {"x": abi.YR_PROJ_X, "y": abi.YR_PROJ_Y, "z": abi.YR_PROJ_Z, "n": abi.YR_PROJ_NONE}
     return tc | (pc[proj[0]] << 8) | (pc[proj[1]] << 16) | (pc[proj[2]] << 24)
 
@@ -513,8 +514,9 @@ def write_yrs(sc: Scene, path: str) -> None:
         # fields; 3 = render parameters carry exposure and gamma; 4 = object
         # records carry the instance index (-1: a mesh) and, for instances,
         # the 4x4 matrix; 5 = shader records carry the specular / hardness
-        # modulation weights
-        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 5))
+        # modulation weights; 6 = object records end with a flag and, when
+        # set, 6 texture coordinates per triangle
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 6))
         f.write(bytes(sc.camera))
         f.write(bytes(sc.render))
         for s in sc.shaders:
@@ -535,6 +537,9 @@ def write_yrs(sc: Scene, path: str) -> None:
             f.write(t.tobytes())
             if m.shader == abi.YR_PER_TRIANGLE:
                 f.write(np.ascontiguousarray(m.tri_shaders, dtype=np.uint32).tobytes())
+            f.write(struct.pack("<i", 0 if m.uvs is None else 1))
+            if m.uvs is not None:
+                f.write(np.ascontiguousarray(m.uvs, np.float32).reshape(-1, 6).tobytes())
 
 
 def read_yrs(path: str) -> Scene:
@@ -591,7 +596,14 @@ def read_yrs(path: str) -> Scene:
         if shid == abi.YR_PER_TRIANGLE:
             ts = np.frombuffer(data, np.uint32, nt, off).copy()
             off += 4 * nt
-        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast), float(smooth), inst, mat, inv))
+        uvs = None
+        if version >= 6:
+            (has_uv,) = struct.unpack_from("<i", data, off)
+            off += 4
+            if has_uv:
+                uvs = np.frombuffer(data, np.float32, 6 * nt, off).reshape(nt, 6).copy()
+                off += 24 * nt
+        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast), float(smooth), inst, mat, inv, uvs))
     return sc
 
 
