@@ -1,5 +1,6 @@
 """Failure paths end in a status code, never in a device fault: a corrupt
-prebuilt tree is rejected when the scene is created, rays with NaN
+prebuilt tree (a link out of range or back up the tree, a bad leaf) is
+rejected on the host when the scene is created, rays with NaN
 components miss (infinite ones are answered without an error), an empty
 scene is refused, and the library keeps working after each error."""
 import ctypes as C
@@ -22,7 +23,7 @@ def _tree(mesh):
     return p
 
 
-@pytest.mark.parametrize("what", ["child", "leaf_triangle", "prim_range"])
+@pytest.mark.parametrize("what", ["child", "cycle", "leaf_triangle", "prim_range"])
 def test_corrupt_prebuilt_tree_is_rejected(cuda, what):
     sc = scenes.config_small(32, 24)
     lib = abi.load()
@@ -34,6 +35,8 @@ def test_corrupt_prebuilt_tree_is_rejected(cuda, what):
     multi = next((i for i in range(n) if nodes[i].flags & 3 == 3 and nodes[i].flags >> 2 > 1), None)
     if what == "child":
         nodes[interior].flags = (nodes[interior].flags & 3) | ((n + 7) << 2)
+    elif what == "cycle":  # right child pointing back at the node: a walk that would never end
+        nodes[interior].flags = (nodes[interior].flags & 3) | (interior << 2)
     elif what == "leaf_triangle":
         nodes[single].word = sc.meshes[0].tris.shape[0] + 3
     else:

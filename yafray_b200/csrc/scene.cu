@@ -50,7 +50,9 @@ bool valid_tree(const std::vector<uint2> &nodes, const std::vector<uint32_t> &pr
     for (size_t i = 0; i < n; i++) {
         const uint32_t f = nodes[i].y, w = nodes[i].x;
         if ((f & 3u) != 3u) {
-            if (i + 1 >= n || (f >> 2) >= n) return false;
+            // the right child follows the left subtree, so every descent
+            // moves to a higher index and ends
+            if (i + 1 >= n || (f >> 2) >= n || (f >> 2) < i + 2) return false;
         } else {
             const uint32_t np = f >> 2;
             if (np == 1 && w >= ntris) return false;
