@@ -408,6 +408,21 @@ typedef struct yr_object_desc {
                                 getSurface, triangle.cc:156-160); without
                                 them it is (-1, -1) on a flat mesh and (0, 0)
                                 on a smoothed one, as the reference's          */
+    const float *orco_matrix; /* optional 4x4 row-major matrix (16 floats, row
+                                3 unused) giving the "orco" texture point of
+                                this mesh as orco_matrix * P: a mesh that went
+                                through meshObject_t::transform (every mesh
+                                the loader or yafrayInterface_t makes, even
+                                with an identity transform) has
+                                toObjectOrco(P) = backOrco * P (mesh.cc:
+                                422-515), backOrco mapping the mesh's bound
+                                onto [-1, 1]^3.  The reference inverts it with
+                                the shipped build's approximate division, so
+                                the caller passes meshObject_t::backOrco
+                                itself.  NULL = the point itself (a mesh made
+                                without a transform, mesh.cc:510-514); a
+                                reference applies its original's matrix to
+                                M^-1 P (reference.cc:102-106)                 */
 } yr_object_desc;
 
 #define YR_PER_TRIANGLE 0xffffffffu

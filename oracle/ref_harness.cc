@@ -9,6 +9,7 @@
 //   yr_ref_harness rays    SCENE RAYS OUT      kd / scene ray queries
 //   yr_ref_harness camera  SCENE OUT           primary ray directions
 //   yr_ref_harness instmat SCENE OUT           each reference's M^-1 (back)
+//   yr_ref_harness orcomat SCENE OUT           each transformed mesh's orco matrix
 //   yr_ref_cudascene cudarender SCENE OUT [x0 x1 y0 y1 [STOP_AFTER]]
 //                                              the scene through cudascene_t (the
 //                                              library), a build of this file
@@ -179,6 +180,8 @@ struct SceneFile {
         std::vector<uint32_t> t;
         std::vector<uint32_t> tri_shader;  // when shader == YR_PER_TRIANGLE
         std::vector<float> uv;             // 6 per triangle (record version 6), or none
+        bool transformed;                  // record version 7: made as the loader makes meshes
+                                           // (through meshObject_t::transform), for its orco
     };
     std::vector<Obj> objs;
 };
@@ -231,6 +234,12 @@ static void load_scene(const char *path, SceneFile &s) {
                 int32_t has_uv = 0;
                 rd(f, &has_uv, 4);
             }
+            o.transformed = false;
+            if (hdr[3] >= 7) {  // record version 7: orco matrix flag (none on a reference)
+                int32_t has_orco = 0;
+                rd(f, &has_orco, 4);
+                if (has_orco) die("orco matrix on a reference");
+            }
             continue;
         }
         o.nv = oh[0];
@@ -251,6 +260,19 @@ static void load_scene(const char *path, SceneFile &s) {
             if (has_uv) {
                 o.uv.resize(6 * (size_t)o.nt);
                 rd(f, &o.uv[0], 4 * o.uv.size());
+            }
+        }
+        // record version 7: a flag and the orco matrix, the library's input;
+        // the reference makes that mesh through meshObject_t::transform and
+        // computes its own
+        o.transformed = false;
+        if (hdr[3] >= 7) {
+            int32_t has_orco = 0;
+            rd(f, &has_orco, 4);
+            if (has_orco) {
+                float om[16];
+                rd(f, om, 64);
+                o.transformed = true;
             }
         }
     }
@@ -413,7 +435,11 @@ static void build_ref(const SceneFile &s, RefScene &r, bool with_lights = true, 
         std::vector<CFLOAT> fvcol;
         if (!fuv.empty())  // each triangle's six coordinates, as the loader sets them
             for (uint32_t k = 0; k < o.nt; k++) ts[k].setUV(fuv.begin() + 6 * (size_t)k);
-        meshObject_t *m = meshObject_t::factory(ver, nor, ts, fuv, fvcol);
+        // a "transformed" mesh is made as the loader and yafrayInterface_t
+        // make every mesh: with the current transform, here the identity
+        // (interface_impl.cc:242, render.cc:757), which sets its orco matrix
+        meshObject_t *m = o.transformed ? meshObject_t::factory(false, matrix4x4_t(1), ver, nor, ts, fuv, fvcol)
+                                        : meshObject_t::factory(ver, nor, ts, fuv, fvcol);
         m->setShader(r.shaders.at(o.shader == YR_PER_TRIANGLE ? o.tri_shader[0] : o.shader));
         m->castShadows(o.cast != 0);
         if (o.smooth >= 1.f) m->autoSmooth(o.smooth);  // as the loader does (render.cc:764)
@@ -631,6 +657,31 @@ static void cmd_instmat(const SceneFile &s, const char *out) {
         for (int a = 0; a < 4; a++)
             for (int b = 0; b < 4; b++) {
                 const float v = ro->back[a][b];
+                wr(f, &v, 4);
+            }
+    }
+    fclose(f);
+}
+
+// Each transformed mesh's orco matrix as meshObject_t::transform computes
+// it (backOrco, mesh.cc:452-481): u32 count, then per mesh u32 object index
+// and 16 floats.
+static void cmd_orcomat(const SceneFile &s, const char *out) {
+    RefScene r;
+    build_ref(s, r, false);
+    std::vector<uint32_t> idx;
+    for (size_t i = 0; i < s.objs.size(); i++)
+        if (s.objs[i].inst < 0 && s.objs[i].transformed) idx.push_back((uint32_t)i);
+    FILE *f = fopen(out, "wb");
+    if (!f) die("cannot open output");
+    uint32_t n = (uint32_t)idx.size();
+    wr(f, &n, 4);
+    for (size_t k = 0; k < idx.size(); k++) {
+        const meshObject_t *m = r.meshes[idx[k]];
+        wr(f, &idx[k], 4);
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) {
+                const float v = m->backOrco[a][b];
                 wr(f, &v, 4);
             }
     }
@@ -1143,6 +1194,8 @@ int main(int argc, char **argv) {
         cmd_rays(s, argv[3], argv[4]);
     } else if (cmd == "instmat") {
         cmd_instmat(s, argv[3]);
+    } else if (cmd == "orcomat") {
+        cmd_orcomat(s, argv[3]);
     } else if (cmd == "texeval") {
         if (argc < 5) die("texeval SCENE POINTS OUT");
         cmd_texeval(s, argv[3], argv[4]);

@@ -167,6 +167,10 @@ struct Obj {
     // rows of M and of its inverse, and M's rows normalised (reference.cc:9-46)
     int inst = -1;
     float m[12], back[12], rot[9];
+    // a mesh made through meshObject_t::transform: toObjectOrco(P) =
+    // backOrco * P (mesh.cc:422-515), rows 0-2 of backOrco as given
+    bool has_orco = false;
+    float orco[12];
 };
 
 // matrix4x4_t * point3d_t as the shipped build groups it
@@ -1192,6 +1196,7 @@ SP surface(const Scene &S, int obj, uint32_t tri, float Z, const V &from_w, cons
         s.NV = rot_vec(ow.rot, s.NV);
         s.orco = xf_point(ow.back, s.P);  // referenceObject_t::toObjectOrco
     }
+    if (o.has_orco) s.orco = xf_point(o.orco, s.orco);  // meshObject_t::toObjectOrco of a transformed mesh
     s.obj = obj;
     s.shader = (int)o.tri_shader[tri];
     return s;
@@ -1736,8 +1741,9 @@ orc_scene *orc_load(const char *path) {
                 for (int a = 0; a < 3; a++)
                     for (int b = 0; b < 4; b++) S.objs[i].back[4 * a + b] = inv[4 * a + b];
             S.objs[i].inst = inst;
-            int32_t has_uv = 0;  // record version 6: texture coordinates flag (none on a reference)
+            int32_t has_uv = 0, has_orco = 0;  // record versions 6, 7: uv and orco flags (none on a reference)
             if (ok && hdr[3] >= 6) ok = rdv(f, &has_uv, 1);
+            if (ok && hdr[3] >= 7) ok = rdv(f, &has_orco, 1) && has_orco == 0;
             continue;
         }
         std::vector<float> v(3 * (size_t)oh[0]);
@@ -1754,6 +1760,15 @@ orc_scene *orc_load(const char *path) {
             if (ok && has_uv) {
                 ob.tri_uv.resize(6 * (size_t)oh[1]);
                 ok = rdv(f, ob.tri_uv.data(), ob.tri_uv.size());
+            }
+        }
+        if (ok && hdr[3] >= 7) {  // record version 7: the orco matrix (4x4, rows 0-2 used)
+            int32_t has_orco = 0;
+            float om[16];
+            ok = rdv(f, &has_orco, 1) && (!has_orco || rdv(f, om, 16));
+            if (ok && has_orco) {
+                ob.has_orco = true;
+                for (int k = 0; k < 12; k++) ob.orco[k] = om[k];
             }
         }
         ob.cast = oh[3] != 0;

@@ -518,6 +518,56 @@ def texco_uv_scene():
     return sc
 
 
+def texco_orco_scene(mats=None):
+    """Textures addressed by "orco" on meshes made as the loader makes them
+    (through meshObject_t::transform, so orco = backOrco * P: the mesh's
+    bound mapped onto [-1, 1]^3), one of them smoothed, beside a mesh made
+    without a transform (orco = P).  `mats`: {mesh index: backOrco} from
+    the reference; None = placeholders (the reference computes its own)."""
+    sc = scenes.config_small(80, 60)
+    ts = scenes.texture_shader
+    sc.shaders = [
+        ts((0.6, 0.6, 0.6), "marble", (0.9, 0.9, 0.85), (0.2, 0.2, 0.3), mod_color=0.8, turbulence=1.0, size=2.0,
+           texco="orco"),
+        ts((0.5, 0.5, 0.6), "voronoi", (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), mod_color=0.7, color_type="col1",
+           weight1=1.0, size=1.5, texco="orco"),
+        ts((0.7, 0.6, 0.5), "clouds", (0.1, 0.2, 0.3), (0.9, 0.8, 0.6), mode="mul", mod_color=0.9, depth=3,
+           size=1.0, texco="orco", proj=("y", "x", "n")),
+        ts((0.5, 0.6, 0.4), "musgrave", (0.2, 0.4, 0.1), (0.9, 0.9, 0.7), size=1.0, intensity=0.6, texco="orco"),
+    ]
+    meshes = []
+    for k in range(3):
+        c = (-1.4 + 1.4 * k, -0.4 + 0.1 * k, 0.2 * k)
+        v, t = scenes.uv_sphere(c, 0.6 - 0.1 * k, rings=16, segments=32)
+        m = scenes.Mesh(v, t, k)
+        if k == 1:
+            m.smooth_angle = 180.0
+        if k != 2:  # the third sphere is made without a transform
+            m.orco = np.eye(4, dtype=np.float32)
+        meshes.append(m)
+    pv, pt = scenes.ground_plane(20.0, -1.0)
+    plane = scenes.Mesh(pv, pt, 3)
+    plane.orco = np.eye(4, dtype=np.float32)
+    meshes.append(plane)
+    sc.meshes = meshes
+    sc.lights = [scenes.point_light((2.0, 4.0, 3.0), 14.0)]
+    sc.camera = scenes.camera((0.0, 2.5, 4.5), (0.0, -0.4, 0.0), (0.0, 3.5, 4.5), 80, 60)
+    sc.render.spp = 2
+    if mats is not None:
+        for i, m in mats.items():
+            sc.meshes[int(i)].orco = np.asarray(m, np.float32)
+    return sc
+
+
+def texco_orco_render():
+    sc = texco_orco_scene()
+    mats = T.harness_orco_matrices(sc)
+    img, _ = T.harness_render(sc)
+    idx = np.array(sorted(mats))
+    np.savez_compressed(os.path.join(HERE, "render_texco_orco_80x60.npz"), image=img, orco_idx=idx,
+                        orco=np.stack([mats[i] for i in idx]))
+
+
 def texco_uv_render():
     img, _ = T.harness_render(texco_uv_scene())
     np.savez_compressed(os.path.join(HERE, "render_texco_uv_80x60.npz"), image=img)
@@ -666,6 +716,7 @@ if __name__ == "__main__":
     specmod_render()
     texco_view_render()
     texco_uv_render()
+    texco_orco_render()
     tonemap_renders()
     image_outputs()
     instances()

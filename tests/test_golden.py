@@ -310,6 +310,26 @@ def test_oracle_uv_texco_matches_reference():
     assert np.abs(plain - ref).max() > 1e-2
 
 
+def test_oracle_orco_of_transformed_meshes_matches_reference():
+    """"orco" texture coordinates of meshes made as the loader makes them
+    (through meshObject_t::transform: orco = backOrco * P, the reference's
+    own matrix given), one smoothed, beside a mesh made without a
+    transform, against the reference's render."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    g = load("render_texco_orco_80x60.npz")
+    ref = g["image"]
+    sc = make_golden.texco_orco_scene(dict(zip(g["orco_idx"], g["orco"])))
+    img, _ = T.OracleScene(sc).render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    rel = np.abs(img - ref)[..., :3] / np.maximum(np.abs(ref[..., :3]), 1e-30)
+    assert rel[ref[..., :3] > 1e-6].max() <= 1e-6
+    for m in sc.meshes:  # the matrices matter
+        m.orco = None
+    plain, _ = T.OracleScene(sc).render()
+    assert np.abs(plain - ref).max() > 1e-2
+
+
 def test_oracle_specular_hardness_modulation_matches_reference():
     """Modulators that also drive the specular colour and the Phong
     exponent (the modulator's "specular" / "hard" weights, every mode,

@@ -236,6 +236,25 @@ def test_render_uv_texco(cuda):
         _cmp(img, ref, O)
 
 
+def test_render_orco_of_transformed_meshes(cuda):
+    """"orco" coordinates through each mesh's orco matrix (the reference's
+    backOrco), on a smoothed mesh too; with a 2-bounce path light as well."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "render_texco_orco_80x60.npz"))
+    for gi in (False, True):
+        sc = make_golden.texco_orco_scene(dict(zip(g["orco_idx"], g["orco"])))
+        if gi:
+            sc.lights = [scenes.quad_light_down(0.0, 4.0, 1.0, 2.0, 2.0, 30.0, 4),
+                         scenes.path_light(samples=1, depth=2, power=1.0)]
+        img = api.DeviceScene(sc).render()
+        O = T.OracleScene(sc)
+        ref, _ = O.render()
+        assert np.array_equal(img[..., 3], ref[..., 3])
+        _cmp(img, ref, O)
+
+
 def test_render_specular_hardness_modulation(cuda):
     """The modulator's "specular" and "hard" weights: the texture also
     drives the specular colour and the Phong exponent, every mode."""

@@ -365,6 +365,24 @@ def harness_instance_inverses(sc: scenes.Scene) -> dict:
     return out
 
 
+def harness_orco_matrices(sc: scenes.Scene) -> dict:
+    """{object index: 4x4 backOrco} of every mesh whose orco matrix is set
+    (any value: the reference makes those meshes through
+    meshObject_t::transform and computes its own)."""
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "o.bin")
+        scenes.write_yrs(sc, sp)
+        run_harness("orcomat", sp, op)
+        data = open(op, "rb").read()
+    n, = struct.unpack_from("<I", data, 0)
+    out, off = {}, 4
+    for _ in range(n):
+        i, = struct.unpack_from("<I", data, off)
+        out[i] = np.frombuffer(data, np.float32, 16, off + 4).reshape(4, 4).copy()
+        off += 68
+    return out
+
+
 def harness_camera(sc: scenes.Scene) -> np.ndarray:
     with tempfile.TemporaryDirectory() as d:
         sp, op = os.path.join(d, "s.yrs"), os.path.join(d, "o.bin")

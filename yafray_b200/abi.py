@@ -122,7 +122,7 @@ class YrObjectDesc(C.Structure):
                 ("smooth_angle", C.c_float), ("reserved", C.c_uint32),
                 ("instance_matrix", C.POINTER(C.c_float)), ("instance_inverse", C.POINTER(C.c_float)),
                 ("instance_of", C.c_uint32), ("reserved2", C.c_uint32),
-                ("uvs", C.POINTER(C.c_float))]
+                ("uvs", C.POINTER(C.c_float)), ("orco_matrix", C.POINTER(C.c_float))]
 
 
 class YrSceneDesc(C.Structure):

@@ -60,6 +60,10 @@ class DeviceScene:
                 assert uv.shape[0] == t.shape[0]
                 self._keep.append(uv)
                 objs[i].uvs = uv.ctypes.data_as(C.POINTER(C.c_float))
+            if m.orco is not None:
+                om = np.ascontiguousarray(m.orco, np.float32).reshape(16)
+                self._keep.append(om)
+                objs[i].orco_matrix = om.ctypes.data_as(C.POINTER(C.c_float))
         shaders = (abi.YrShaderDesc * len(sc.shaders))(*sc.shaders)
         lights = (abi.YrLightDesc * max(1, len(sc.lights)))(*sc.lights)
         desc = abi.YrSceneDesc()

@@ -95,7 +95,8 @@ struct DevObject {
     float ob[6];        // object bound (meshObject_t::getBound), the object tree's leaf box
     int inst;           // instance record (DevScene::insts) or -1; the tree
                         // and triangle fields above are then the original's
-    int pad[3];
+    int orco;           // orco matrix (DevScene::orco_m, 3 rows) of the mesh, or -1
+    int pad[2];
 };
 
 // referenceObject_t's matrices: rows 0-2 of M and of its inverse, and the
@@ -133,6 +134,7 @@ struct DevScene {
     const DevInst *insts;       // instance matrices (referenceObject_t)
     const float *tri_nrm;       // corner normals, 9 per triangle, of smoothed objects
     const float *tri_uv;        // texture coordinates, 6 per triangle, of objects that have them
+    const float4 *orco_m;       // orco matrices (rows 0-2 of meshObject_t::backOrco), 3 per mesh with one
     // object tree (geomeTree_t): per interior node 4 x float4 = left box
     // (min xyz, max xyz), right box, then the children's codes (>= 0:
     // interior node, < 0: ~object index) as int bits

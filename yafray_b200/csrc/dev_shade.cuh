@@ -367,6 +367,12 @@ __device__ __forceinline__ Surf make_surface(const DevScene &S, const DevRender 
         s.NV = rot_vec(I->rot, s.NV);
         s.orco = xf_point(I->back, s.P);
     }
+    const int om = S.objects[object].orco;
+    if (om >= 0) {  // a transformed mesh: toObjectOrco = backOrco * point (mesh.cc:510-515)
+        const float4 r0 = __ldg(S.orco_m + 3 * om), r1 = __ldg(S.orco_m + 3 * om + 1), r2 = __ldg(S.orco_m + 3 * om + 2);
+        const float m[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+        s.orco = xf_point(m, s.orco);
+    }
     s.object = object;
     s.shader = (int)__ldg(R.tri_shader + tri);
     s.Z = Z;

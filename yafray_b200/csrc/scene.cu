@@ -392,6 +392,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     std::vector<uint32_t> prims, tri_shader;
     std::vector<float> tri_nrm;  // 9 per triangle (corner normals) up to the last smoothed object
     std::vector<float> tri_uv;   // 6 per triangle (texture coordinates) up to the last object with them
+    std::vector<float4> orco_m;  // 3 rows per mesh with an orco matrix
     std::vector<DevObject> objects;
     std::vector<Box> obounds;
     size_t total_tris = 0;
@@ -558,6 +559,15 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
         std::memcpy(dob.ob, obb.a, 12);
         std::memcpy(dob.ob + 3, obb.g, 12);
         dob.inst = -1;
+        dob.orco = -1;
+        if (od.orco_matrix) {  // toObjectOrco of a transformed mesh: rows 0-2 of backOrco
+            for (int k = 0; k < 12; k++)
+                if (!std::isfinite(od.orco_matrix[k])) return fail(YR_ERR_INVALID_ARG);
+            dob.orco = (int)(orco_m.size() / 3);
+            for (int r = 0; r < 3; r++)
+                orco_m.push_back(make_float4(od.orco_matrix[4 * r], od.orco_matrix[4 * r + 1], od.orco_matrix[4 * r + 2],
+                                             od.orco_matrix[4 * r + 3]));
+        }
         objects.push_back(dob);
         obounds.push_back(obb);
     }
@@ -723,6 +733,8 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     const float *d_tri_nrm = nullptr, *d_tri_uv = nullptr;
     if ((st = dev_upload(s, tri_nrm.data(), tri_nrm.size(), (float **)&d_tri_nrm)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, tri_uv.data(), tri_uv.size(), (float **)&d_tri_uv)) != YR_OK) return fail(st);
+    const float4 *d_orco_m = nullptr;
+    if ((st = dev_upload(s, orco_m.data(), orco_m.size(), (float4 **)&d_orco_m)) != YR_OK) return fail(st);
     if ((st = dev_upload(s, objects.data(), objects.size(), (DevObject **)&d_objects)) != YR_OK) return fail(st);
     const DevInst *d_insts = nullptr;
     if (!insts.empty() && (st = dev_upload(s, insts.data(), insts.size(), (DevInst **)&d_insts)) != YR_OK)
@@ -748,6 +760,7 @@ YR_API yr_status yr_scene_create(const yr_scene_desc *desc, int device, yr_scene
     D.insts = d_insts;
     D.tri_nrm = d_tri_nrm;
     D.tri_uv = d_tri_uv;
+    D.orco_m = d_orco_m;
     D.onodes = d_onodes;
     D.oroot = oroot;
     D.sonodes = d_sonodes;

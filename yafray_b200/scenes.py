@@ -103,6 +103,7 @@ class Mesh:
     matrix: Optional[np.ndarray] = None   # 4x4 row-major (instances only)
     inverse: Optional[np.ndarray] = None  # optional M^-1 (else computed by the library)
     uvs: Optional[np.ndarray] = None      # optional (ntris, 6) texture coordinates (u, v at a, b, c)
+    orco: Optional[np.ndarray] = None     # optional 4x4 "orco" matrix (meshObject_t::backOrco)
 
     @property
     def is_instance(self) -> bool:
@@ -515,8 +516,9 @@ def write_yrs(sc: Scene, path: str) -> None:
         # records carry the instance index (-1: a mesh) and, for instances,
         # the 4x4 matrix; 5 = shader records carry the specular / hardness
         # modulation weights; 6 = object records end with a flag and, when
-        # set, 6 texture coordinates per triangle
-        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 6))
+        # set, 6 texture coordinates per triangle; 7 = then a flag and, when
+        # set, the 4x4 orco matrix (meshes only)
+        f.write(struct.pack("<4I", len(sc.meshes), len(sc.shaders), len(sc.lights), 7))
         f.write(bytes(sc.camera))
         f.write(bytes(sc.render))
         for s in sc.shaders:
@@ -540,6 +542,9 @@ def write_yrs(sc: Scene, path: str) -> None:
             f.write(struct.pack("<i", 0 if m.uvs is None else 1))
             if m.uvs is not None:
                 f.write(np.ascontiguousarray(m.uvs, np.float32).reshape(-1, 6).tobytes())
+            f.write(struct.pack("<i", 0 if m.orco is None else 1))
+            if m.orco is not None:
+                f.write(np.ascontiguousarray(m.orco, np.float32).reshape(16).tobytes())
 
 
 def read_yrs(path: str) -> Scene:
@@ -603,7 +608,14 @@ def read_yrs(path: str) -> Scene:
             if has_uv:
                 uvs = np.frombuffer(data, np.float32, 6 * nt, off).reshape(nt, 6).copy()
                 off += 24 * nt
-        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast), float(smooth), inst, mat, inv, uvs))
+        orco = None
+        if version >= 7:
+            (has_orco,) = struct.unpack_from("<i", data, off)
+            off += 4
+            if has_orco:
+                orco = np.frombuffer(data, np.float32, 16, off).reshape(4, 4).copy()
+                off += 64
+        sc.meshes.append(Mesh(v, t, shid, ts, bool(cast), float(smooth), inst, mat, inv, uvs, orco))
     return sc
 
 
