@@ -3,12 +3,16 @@
 // yr_scene_create (the library builds the same kd-trees and object tree);
 // every render is then one yr_render call.
 //
-// What it takes: meshObject_t objects (flat shading, one shader per object
-// or per triangle), genericShader_t shaders without modulators, point
-// lights, the pinhole camera, and the render settings the library models
-// (ray depth, bias, one AA pass resampling every pixel, tone map, alpha
-// premultiply, region).  Anything else is refused with YR_ERR_UNSUPPORTED
-// before any device work; lastStatus() says so.
+// What it takes: meshObject_t objects (flat, or smoothed with the angle
+// given in the hints; one shader per object or per triangle; texture
+// coordinates; the orco matrix of a transformed mesh), referenceObject_t
+// placements of them, genericShader_t shaders without modulators (or with
+// the record given in the hints), point lights (other lights through the
+// hints), the pinhole camera, a constant background (through the hints),
+// and the render settings the library models (ray depth, bias, one AA pass
+// resampling every pixel, tone map, alpha premultiply, region).  Anything
+// else is refused with YR_ERR_UNSUPPORTED before any device work;
+// lastStatus() says so.
 #include "cudascene.h"
 
 #include <cmath>
@@ -20,6 +24,7 @@
 #include "camera.h"
 #include "mesh.h"
 #include "pointlight.h"
+#include "reference.h"
 
 __BEGIN_YAFRAY
 
@@ -32,6 +37,15 @@ struct meshFields : meshObject_t {
     static std::vector<point3d_t> meshObject_t::*m_vertices() { return &meshFields::vertices; }
     static std::vector<triangle_t> meshObject_t::*m_triangles() { return &meshFields::triangles; }
     static std::vector<vector3d_t> meshObject_t::*m_normals() { return &meshFields::normals; }
+    static std::vector<GFLOAT> meshObject_t::*m_facesuv() { return &meshFields::facesuv; }
+    static bool meshObject_t::*m_unt() { return &meshFields::unt; }
+    static bool meshObject_t::*m_hasorco() { return &meshFields::hasorco; }
+    static matrix4x4_t meshObject_t::*m_backOrco() { return &meshFields::backOrco; }
+};
+struct refFields : referenceObject_t {
+    static object3d_t *referenceObject_t::*m_original() { return &refFields::original; }
+    static matrix4x4_t referenceObject_t::*m_M() { return &refFields::M; }
+    static matrix4x4_t referenceObject_t::*m_back() { return &refFields::back; }
 };
 struct shaderFields : genericShader_t {
     static color_t genericShader_t::*m_scolor() { return &shaderFields::scolor; }
@@ -43,6 +57,7 @@ struct pointFields : pointLight_t {
     static point3d_t pointLight_t::*m_from() { return &pointFields::from; }
     static color_t pointLight_t::*m_color() { return &pointFields::color; }
     static bool pointLight_t::*m_cast() { return &pointFields::cast_shadows; }
+    static CFLOAT pointLight_t::*m_glow() { return &pointFields::glow_int; }
 };
 struct cameraFields : camera_t {
     static vector3d_t camera_t::*m_vto() { return &cameraFields::vto; }
@@ -55,6 +70,10 @@ struct cameraFields : camera_t {
 static void put3(float *d, const point3d_t &p) { d[0] = p.x; d[1] = p.y; d[2] = p.z; }
 static void put3(float *d, const vector3d_t &v) { d[0] = v.x; d[1] = v.y; d[2] = v.z; }
 static void put3(float *d, const color_t &c) { d[0] = c.getR(); d[1] = c.getG(); d[2] = c.getB(); }
+static void put16(float *d, const matrix4x4_t &m) {
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) d[4 * a + b] = m[a][b];
+}
 
 cudascene_t::~cudascene_t() {
     if (handle) yr_scene_destroy(handle);
@@ -65,20 +84,26 @@ yr_status cudascene_t::capture() {
     std::map<const shader_t *, uint32_t> shader_index;
     std::vector<yr_shader_desc> shaders;
     struct add_shader {
-        static yr_status run(const shader_t *s, std::map<const shader_t *, uint32_t> &idx,
+        static yr_status run(const shader_t *s, const cudaHints_t *h, std::map<const shader_t *, uint32_t> &idx,
                              std::vector<yr_shader_desc> &out, uint32_t &k) {
             std::map<const shader_t *, uint32_t>::iterator it = idx.find(s);
             if (it != idx.end()) {
                 k = it->second;
                 return YR_OK;
             }
-            const genericShader_t *g = dynamic_cast<const genericShader_t *>(s);
-            if (!g || !(g->*shaderFields::m_mods()).empty()) return YR_ERR_UNSUPPORTED;
             yr_shader_desc d;
             memset(&d, 0, sizeof(d));
-            put3(d.color, g->*shaderFields::m_scolor());
-            put3(d.specular, g->*shaderFields::m_ks());
-            d.hard = g->*shaderFields::m_hard();
+            std::map<const shader_t *, yr_shader_desc>::const_iterator hs;
+            if (h && h->refused.count(s)) return YR_ERR_UNSUPPORTED;
+            if (h && (hs = h->shaders.find(s)) != h->shaders.end()) {
+                d = hs->second;
+            } else {
+                const genericShader_t *g = dynamic_cast<const genericShader_t *>(s);
+                if (!g || !(g->*shaderFields::m_mods()).empty()) return YR_ERR_UNSUPPORTED;
+                put3(d.color, g->*shaderFields::m_scolor());
+                put3(d.specular, g->*shaderFields::m_ks());
+                d.hard = g->*shaderFields::m_hard();
+            }
             k = (uint32_t)out.size();
             idx[s] = k;
             out.push_back(d);
@@ -88,20 +113,52 @@ yr_status cudascene_t::capture() {
 
     // objects, in obj_list order (the order buildObjectTree sees them)
     std::vector<yr_object_desc> objs;
-    std::vector<std::vector<float> > verts;
+    std::vector<std::vector<float> > verts, mats;
     std::vector<std::vector<uint32_t> > tris, tri_shaders;
+    std::map<const object3d_t *, uint32_t> obj_index;
+    for (std::list<object3d_t *>::const_iterator o = obj_list.begin(); o != obj_list.end(); ++o)
+        obj_index[*o] = (uint32_t)obj_index.size();
     for (std::list<object3d_t *>::const_iterator o = obj_list.begin(); o != obj_list.end(); ++o) {
+        if (hints && hints->refused.count(*o)) return YR_ERR_UNSUPPORTED;
+        if ((*o)->caustics()) return YR_ERR_UNSUPPORTED;  // pathlight.cc:198: caustic paths are not modelled
+        verts.push_back(std::vector<float>());
+        tris.push_back(std::vector<uint32_t>());
+        tri_shaders.push_back(std::vector<uint32_t>());
+        mats.push_back(std::vector<float>());
+        const referenceObject_t *ro = dynamic_cast<const referenceObject_t *>(*o);
+        if (ro) {  // a placement of a mesh of this scene: its M and M^-1 as the reference holds them
+            std::map<const object3d_t *, uint32_t>::const_iterator org = obj_index.find(ro->*refFields::m_original());
+            if (org == obj_index.end() || !dynamic_cast<const meshObject_t *>(org->first)) return YR_ERR_UNSUPPORTED;
+            mats.back().resize(32);
+            put16(&mats.back()[0], ro->*refFields::m_M());
+            put16(&mats.back()[16], ro->*refFields::m_back());
+            yr_object_desc d;
+            memset(&d, 0, sizeof(d));
+            d.instance_of = org->second;
+            objs.push_back(d);
+            continue;
+        }
         const meshObject_t *m = dynamic_cast<const meshObject_t *>(*o);
-        if (!m) return YR_ERR_UNSUPPORTED;  // references, spheres: not taken here
+        if (!m) return YR_ERR_UNSUPPORTED;  // spheres: not taken here
+        if (m->*meshFields::m_hasorco()) return YR_ERR_UNSUPPORTED;  // explicit orco points
         const std::vector<point3d_t> &V = m->*meshFields::m_vertices();
         const std::vector<triangle_t> &T = m->*meshFields::m_triangles();
-        if (!(m->*meshFields::m_normals()).empty()) return YR_ERR_UNSUPPORTED;  // smoothed: give the angle instead
-        verts.push_back(std::vector<float>(3 * V.size()));
+        float smooth = 0.f;
+        if (!(m->*meshFields::m_normals()).empty()) {  // smoothed: the library recomputes the normals from the angle
+            std::map<const object3d_t *, float>::const_iterator sa;
+            if (!hints || (sa = hints->smooth_angle.find(m)) == hints->smooth_angle.end()) return YR_ERR_UNSUPPORTED;
+            smooth = sa->second;
+        }
+        if (!(m->*meshFields::m_unt())) {  // made through transform(): its orco matrix
+            mats.back().resize(16);
+            put16(&mats.back()[0], m->*meshFields::m_backOrco());
+        }
+        verts.back().resize(3 * V.size());
         for (size_t i = 0; i < V.size(); i++) put3(&verts.back()[3 * i], V[i]);
-        tris.push_back(std::vector<uint32_t>(3 * T.size()));
-        tri_shaders.push_back(std::vector<uint32_t>(T.size()));
+        tris.back().resize(3 * T.size());
+        tri_shaders.back().resize(T.size());
         uint32_t obj_shader = 0;
-        yr_status st = add_shader::run(m->getShader(), shader_index, shaders, obj_shader);
+        yr_status st = add_shader::run(m->getShader(), hints, shader_index, shaders, obj_shader);
         if (st != YR_OK) return st;
         bool per_triangle = false;
         for (size_t i = 0; i < T.size(); i++) {
@@ -111,7 +168,7 @@ yr_status cudascene_t::capture() {
             const shader_t *ts = T[i].getShader();
             uint32_t k = obj_shader;
             if (ts && ts != m->getShader()) {
-                if ((st = add_shader::run(ts, shader_index, shaders, k)) != YR_OK) return st;
+                if ((st = add_shader::run(ts, hints, shader_index, shaders, k)) != YR_OK) return st;
                 per_triangle = true;
             }
             tri_shaders.back()[i] = k;
@@ -125,19 +182,37 @@ yr_status cudascene_t::capture() {
         d.shader = per_triangle ? YR_PER_TRIANGLE : obj_shader;
         d.tri_shaders = per_triangle ? &tri_shaders.back()[0] : NULL;
         d.cast_shadows = m->castShadows() ? 1 : 0;
+        d.smooth_angle = smooth;
+        // texture coordinates: triangle i holds facesuv[6i .. 6i+5] (setUV)
+        const std::vector<GFLOAT> &uv = m->*meshFields::m_facesuv();
+        if (!uv.empty() && uv.size() >= 6 * T.size()) d.uvs = &uv[0];
         objs.push_back(d);
     }
     // vectors may have moved while growing: point the records again
     for (size_t i = 0; i < objs.size(); i++) {
-        objs[i].verts = &verts[i][0];
-        objs[i].tris = &tris[i][0];
+        if (mats[i].size() == 32) {  // a reference
+            objs[i].instance_matrix = &mats[i][0];
+            objs[i].instance_inverse = &mats[i][16];
+            continue;
+        }
+        objs[i].verts = verts[i].empty() ? NULL : &verts[i][0];
+        objs[i].tris = tris[i].empty() ? NULL : &tris[i][0];
         if (objs[i].shader == YR_PER_TRIANGLE) objs[i].tri_shaders = &tri_shaders[i][0];
+        if (mats[i].size() == 16) objs[i].orco_matrix = &mats[i][0];
     }
 
     std::vector<yr_light_desc> lights;
     for (std::list<light_t *>::const_iterator l = light_list.begin(); l != light_list.end(); ++l) {
+        // every light lights both the camera hits and the path vertices
+        if (!(*l)->useInRender() || !(*l)->useInIndirect()) return YR_ERR_UNSUPPORTED;
+        if (hints && hints->refused.count(*l)) return YR_ERR_UNSUPPORTED;
+        std::map<const light_t *, yr_light_desc>::const_iterator hl;
+        if (hints && (hl = hints->lights.find(*l)) != hints->lights.end()) {
+            lights.push_back(hl->second);
+            continue;
+        }
         const pointLight_t *p = dynamic_cast<const pointLight_t *>(*l);
-        if (!p) return YR_ERR_UNSUPPORTED;
+        if (!p || p->*pointFields::m_glow() != 0) return YR_ERR_UNSUPPORTED;
         yr_light_desc d;
         memset(&d, 0, sizeof(d));
         d.type = YR_LIGHT_POINT;
@@ -151,7 +226,8 @@ yr_status cudascene_t::capture() {
     const camera_t &cam = *render_camera;
     if (cam.*cameraFields::m_type() != camera_t::CM_PERSPECTIVE || cam.*cameraFields::m_aperture() != 0)
         return YR_ERR_UNSUPPORTED;
-    if (background || fog_density != 0) return YR_ERR_UNSUPPORTED;
+    if (fog_density != 0 || alpha_maskbackground) return YR_ERR_UNSUPPORTED;
+    if (background && !(hints && hints->has_background)) return YR_ERR_UNSUPPORTED;
 
     yr_scene_desc d;
     memset(&d, 0, sizeof(d));
@@ -171,7 +247,9 @@ yr_status cudascene_t::capture() {
     d.camera.aspect = 1.0f;
     d.camera.focal = 1.0f;
 
-    yr_render_params &r = d.render;
+    yr_render_params &r = d.render;  // (seed 0: the reference has no rotation seed)
+    if (background)
+        for (int k = 0; k < 3; k++) r.background[k] = hints->background[k];
     r.self_bias = self_bias;
     r.raydepth = maxraylevel;
     // the library resamples every pixel in one AA pass (AA_threshold 0)

@@ -10,6 +10,10 @@
 //   yr_ref_harness camera  SCENE OUT           primary ray directions
 //   yr_ref_harness instmat SCENE OUT           each reference's M^-1 (back)
 //   yr_ref_harness orcomat SCENE OUT           each transformed mesh's orco matrix
+//   yr_ref_cudascene iface SCENE OUT ARM [pathcache]
+//                                              the scene through a yafrayInterface_t,
+//                                              call by call: ARM ref = interfaceImpl_t,
+//                                              cuda = cudaInterface_t (the library)
 //   yr_ref_cudascene cudarender SCENE OUT [x0 x1 y0 y1 [STOP_AFTER]]
 //                                              the scene through cudascene_t (the
 //                                              library), a build of this file
@@ -56,6 +60,8 @@
 #include "HDR_io.h"
 #ifdef YR_HARNESS_CUDASCENE
 #include "cudascene.h"
+#include "cudainterface.h"
+#include "sunsky.h"
 #endif
 #undef private
 #undef protected
@@ -915,6 +921,306 @@ static void cmd_cudarender(const SceneFile &s, const char *out, const int *crop,
 }
 #endif
 
+#ifdef YR_HARNESS_CUDASCENE
+// ------------------------------------------------------------------ iface
+// The host API: the scene handed to a yafrayInterface_t call by call, as a
+// front end does (shaders with their texture and modulator parameter maps,
+// meshes through addObject_trimesh with the identity transform,
+// references through transformPush + addObject_reference, lights and the
+// camera as parameter maps, a "constant" background), then
+// render(params, sink).  ARM "ref" is the reference's interfaceImpl_t
+// (threadedscene_t, the CPU); "cuda" is cudaInterface_t (the library).
+// The plugins are registered by hand, as their registerPlugin functions
+// and bbreg.cc do.  One JSON line: the status (cuda arm) and the time.
+extern "C" {
+void registerPlugin_pointlight(renderEnvironment_t &);
+void registerPlugin_arealight(renderEnvironment_t &);
+void registerPlugin_hemilight(renderEnvironment_t &);
+void registerPlugin_pathlight(renderEnvironment_t &);
+void registerPlugin_basicshaders(renderEnvironment_t &);
+void registerPlugin_sunsky(renderEnvironment_t &);
+}
+
+static void iface_register(yafrayInterface_t &y) {
+    registerPlugin_pointlight(y);
+    registerPlugin_arealight(y);
+    registerPlugin_hemilight(y);
+    registerPlugin_pathlight(y);
+    registerPlugin_basicshaders(y);
+    registerPlugin_sunsky(y);
+    y.registerFactory("clouds", textureClouds_t::factory);
+    y.registerFactory("marble", textureMarble_t::factory);
+    y.registerFactory("wood", textureWood_t::factory);
+    y.registerFactory("voronoi", textureVoronoi_t::factory);
+    y.registerFactory("musgrave", textureMusgrave_t::factory);
+    y.registerFactory("distorted_noise", textureDistortedNoise_t::factory);
+    y.registerFactory("gradient", textureGradient_t::factory);
+}
+
+static parameter_t P_col(const float *c) { return parameter_t(c[0], c[1], c[2]); }
+static parameter_t P_pt(const float *c) { return parameter_t(point3d_t(c[0], c[1], c[2])); }
+static parameter_t P_on(bool b) { return parameter_t(std::string(b ? "on" : "off")); }
+static parameter_t P_str(const char *v) { return parameter_t(std::string(v)); }
+
+// yr_shader_desc -> the generic shader's, its texture's and its
+// modulator's parameter maps (the names of basicshaders.cc / basictex.cc)
+static void iface_shader(yafrayInterface_t &y, const yr_shader_desc &d, int k) {
+    char name[32], tname[32];
+    snprintf(name, sizeof(name), "sh%04d", k);
+    snprintf(tname, sizeof(tname), "tex%04d", k);
+    std::list<paramMap_t> mods;
+    if (d.tex_type != YR_TEX_NONE) {
+        paramMap_t t;
+        t["name"] = P_str(tname);
+        t["color1"] = P_col(d.tex_color1);
+        t["color2"] = P_col(d.tex_color2);
+        static const char *noise[10] = {"newperlin",  "stdperlin",  "blender",      "voronoi_f1",      "voronoi_f2",
+                                        "voronoi_f3", "voronoi_f4", "voronoi_f2f1", "voronoi_crackle", "cellnoise"};
+        static const char *shapes[3] = {"sin", "saw", "tri"};
+        const char *nt = noise[d.tex_noise < 10 ? d.tex_noise : 0];
+        switch (d.tex_type) {
+        case YR_TEX_MUSGRAVE_FBM:
+        case YR_TEX_MUSGRAVE_MULTIFRACTAL:
+        case YR_TEX_MUSGRAVE_HETEROTERRAIN:
+        case YR_TEX_MUSGRAVE_HYBRIDMF:
+        case YR_TEX_MUSGRAVE_RIDGEDMF:
+            // the musgrave factory reads its kind from "type", which through
+            // addTexture is the texture type itself ("musgrave"): every
+            // musgrave texture made this way is fBm (basictex.cc:694,
+            // interface_impl.cc:133)
+            t["type"] = P_str("musgrave");
+            t["noise_type"] = P_str(nt);
+            t["H"] = parameter_t(d.tex_H);
+            t["lacunarity"] = parameter_t(d.tex_lacunarity);
+            t["octaves"] = parameter_t(d.tex_octaves);
+            t["offset"] = parameter_t(d.tex_offset);
+            t["gain"] = parameter_t(d.tex_gain);
+            t["size"] = parameter_t(d.tex_size);
+            t["intensity"] = parameter_t(d.tex_intensity);
+            break;
+        case YR_TEX_CLOUDS:
+            t["type"] = P_str("clouds");
+            t["noise_type"] = P_str(nt);
+            t["depth"] = parameter_t((float)d.tex_depth);
+            t["size"] = parameter_t(d.tex_size);
+            t["hard"] = P_on(d.tex_hard != 0);
+            t["bias"] = P_str(d.tex_variant == 1 ? "positive" : (d.tex_variant == 2 ? "negative" : ""));
+            break;
+        case YR_TEX_MARBLE:
+        case YR_TEX_WOOD:
+            t["type"] = P_str(d.tex_type == YR_TEX_MARBLE ? "marble" : "wood");
+            t["noise_type"] = P_str(nt);
+            t["depth"] = parameter_t((float)d.tex_depth);
+            t["turbulence"] = parameter_t(d.tex_turbulence);
+            t["size"] = parameter_t(d.tex_size);
+            t["hard"] = P_on(d.tex_hard != 0);
+            t["shape"] = P_str(shapes[d.tex_shape < 3 ? d.tex_shape : 0]);
+            if (d.tex_type == YR_TEX_MARBLE) t["sharpness"] = parameter_t(d.tex_sharpness);
+            else t["wood_type"] = P_str(d.tex_variant ? "rings" : "bands");
+            break;
+        case YR_TEX_VORONOI: {
+            static const char *ct[4] = {"int", "col1", "col2", "col3"};
+            static const char *dm[7] = {"real",           "squared",        "manhattan", "chebychev",
+                                        "minkovsky_half", "minkovsky_four", "minkovsky"};
+            t["type"] = P_str("voronoi");
+            t["color_type"] = P_str(ct[d.tex_shape < 4 ? d.tex_shape : 0]);
+            t["weight1"] = parameter_t(d.tex_weights[0]);
+            t["weight2"] = parameter_t(d.tex_weights[1]);
+            t["weight3"] = parameter_t(d.tex_weights[2]);
+            t["weight4"] = parameter_t(d.tex_weights[3]);
+            t["mk_exponent"] = parameter_t(d.tex_mk_exponent);
+            t["intensity"] = parameter_t(d.tex_intensity);
+            t["size"] = parameter_t(d.tex_size);
+            t["distance_metric"] = P_str(dm[d.tex_metric < 7 ? d.tex_metric : 0]);
+            break;
+        }
+        case YR_TEX_DISTORTED_NOISE:
+            t["type"] = P_str("distorted_noise");
+            t["noise_type1"] = P_str(nt);
+            t["noise_type2"] = P_str(noise[d.tex_noise2 < 10 ? d.tex_noise2 : 0]);
+            t["distort"] = parameter_t(d.tex_distort);
+            t["size"] = parameter_t(d.tex_size);
+            break;
+        case YR_TEX_GRADIENT: {
+            static const char *gt[6] = {"linear", "quadratic", "cubic", "diagonal", "sphere", "halo"};
+            t["type"] = P_str("gradient");
+            t["gradient_type"] = P_str(gt[d.tex_shape < 6 ? d.tex_shape : 0]);
+            t["flip_xy"] = P_on(d.tex_variant != 0);
+            break;
+        }
+        default:
+            die("iface: texture type without a parameter map here");
+        }
+        y.addTexture(t);
+        paramMap_t m;
+        static const char *modes[4] = {"mix", "mul", "add", "sub"};
+        static const char *texco[6] = {"global", "orco", "normal", "window", "reflect", "uv"};
+        m["texname"] = P_str(tname);
+        m["mode"] = P_str(modes[d.mod_mode < 4 ? d.mod_mode : 0]);
+        m["color"] = parameter_t(d.mod_color);
+        m["specular"] = parameter_t(d.mod_specular);
+        m["hard"] = parameter_t(d.mod_hard);
+        m["sizex"] = parameter_t(d.mod_size[0]);
+        m["sizey"] = parameter_t(d.mod_size[1]);
+        m["sizez"] = parameter_t(d.mod_size[2]);
+        m["ofsx"] = parameter_t(d.mod_ofs[0]);
+        m["ofsy"] = parameter_t(d.mod_ofs[1]);
+        m["ofsz"] = parameter_t(d.mod_ofs[2]);
+        m["texco"] = P_str(texco[(d.tex_map & 0xffu) < 6 ? (d.tex_map & 0xffu) : 0]);
+        const char *pnames[3] = {"proj_x", "proj_y", "proj_z"};
+        for (int a = 0; a < 3; a++) {
+            const uint32_t pc = (d.tex_map >> (8 * (a + 1))) & 0xffu;
+            static const char *ax[5] = {"", "x", "y", "z", "n"};
+            m[pnames[a]] = P_str(pc == YR_PROJ_DEFAULT ? (a == 0 ? "x" : (a == 1 ? "y" : "z")) : ax[pc < 5 ? pc : 4]);
+        }
+        mods.push_back(m);
+    }
+    paramMap_t p;
+    p["name"] = P_str(name);
+    p["type"] = P_str("generic");
+    p["color"] = P_col(d.color);
+    p["specular"] = P_col(d.specular);
+    p["hard"] = parameter_t(d.hard);
+    y.addShader(p, mods);
+}
+
+static void iface_light(yafrayInterface_t &y, const yr_light_desc &d, int k, bool path_cache) {
+    char name[32];
+    snprintf(name, sizeof(name), "light%04d", k);
+    paramMap_t p;
+    p["name"] = P_str(name);
+    p["power"] = parameter_t(d.power);
+    switch (d.type) {
+    case YR_LIGHT_POINT:
+        p["type"] = P_str("pointlight");
+        p["from"] = P_pt(d.p[0]);
+        p["color"] = P_col(d.color);
+        p["cast_shadows"] = P_on(d.cast_shadows != 0);
+        break;
+    case YR_LIGHT_AREA:
+        p["type"] = P_str("arealight");
+        p["a"] = P_pt(d.p[0]);
+        p["b"] = P_pt(d.p[1]);
+        p["c"] = P_pt(d.p[2]);
+        p["d"] = P_pt(d.p[3]);
+        p["color"] = P_col(d.color);
+        p["samples"] = parameter_t((float)d.samples);
+        p["psamples"] = parameter_t((float)d.psamples);
+        break;
+    case YR_LIGHT_HEMI:
+        p["type"] = P_str("hemilight");
+        p["color"] = P_col(d.color);
+        p["samples"] = parameter_t((float)d.samples);
+        p["maxdistance"] = parameter_t(d.maxdist);
+        p["use_QMC"] = P_on(true);
+        break;
+    case YR_LIGHT_PATH:
+        p["type"] = P_str("pathlight");
+        p["samples"] = parameter_t((float)d.samples);
+        p["depth"] = parameter_t((float)d.depth);
+        p["use_QMC"] = P_on(true);
+        p["threshold"] = parameter_t(d.threshold > 0 ? d.threshold : 1e9f);
+        if (path_cache) p["cache"] = P_on(true);  // the irradiance cache (not modelled by the library)
+        break;
+    }
+    y.addLight(p);
+}
+
+static void cmd_iface(const std::string &arm, const SceneFile &s, const char *out, const std::string &extra) {
+    yafrayInterface_t *y = arm == "cuda" ? (yafrayInterface_t *)new cudaInterface_t(0, "")
+                                         : (yafrayInterface_t *)new interfaceImpl_t(1, "");
+    iface_register(*y);
+    for (size_t k = 0; k < s.shaders.size(); k++) iface_shader(*y, s.shaders[k], (int)k);
+    std::vector<std::string> shader_names;
+    for (size_t k = 0; k < s.shaders.size(); k++) {
+        char name[32];
+        snprintf(name, sizeof(name), "sh%04d", (int)k);
+        shader_names.push_back(name);
+    }
+    // object names keep the file's order (the interface's tables are
+    // ordered by name, and so are the scene's object and light lists)
+    for (size_t i = 0; i < s.objs.size(); i++) {
+        const SceneFile::Obj &o = s.objs[i];
+        char name[32];
+        snprintf(name, sizeof(name), "obj%04d", (int)i);
+        if (o.inst >= 0) continue;
+        std::vector<point3d_t> verts(o.nv);
+        for (uint32_t k = 0; k < o.nv; k++) verts[k] = P3(&o.v[3 * k]);
+        std::vector<int> faces(o.t.begin(), o.t.end());
+        std::vector<GFLOAT> uv(o.uv.begin(), o.uv.end());
+        std::vector<CFLOAT> vcol;
+        std::vector<std::string> shaders;
+        std::vector<int> faceshader;
+        if (o.shader == YR_PER_TRIANGLE) {
+            shaders = shader_names;
+            std::swap(shaders[0], shaders[o.tri_shader[0]]);  // the object's own shader first
+            std::vector<int> slot(shader_names.size());
+            for (size_t k = 0; k < shaders.size(); k++) slot[atoi(shaders[k].c_str() + 2)] = (int)k;
+            for (uint32_t k = 0; k < o.nt; k++) faceshader.push_back(slot[o.tri_shader[k]]);
+        } else {
+            shaders.push_back(shader_names.at(o.shader));
+        }
+        y->addObject_trimesh(name, verts, faces, uv, vcol, shaders, faceshader, o.smooth >= 1.f ? o.smooth : 0.f,
+                             o.cast != 0, true, true, false, false, color_t(0.0), color_t(0.0), 1.0);
+    }
+    for (size_t i = 0; i < s.objs.size(); i++) {
+        const SceneFile::Obj &o = s.objs[i];
+        if (o.inst < 0) continue;
+        char name[32], orig[32];
+        snprintf(name, sizeof(name), "obj%04d", (int)i);
+        snprintf(orig, sizeof(orig), "obj%04d", o.inst);
+        float M[16];
+        memcpy(M, o.M, sizeof(M));
+        y->transformPush(M);
+        y->addObject_reference(name, orig);
+        y->transformPop();
+    }
+    for (size_t k = 0; k < s.lights.size(); k++) iface_light(*y, s.lights[k], (int)k, extra == "pathcache");
+    paramMap_t cam;
+    cam["name"] = P_str("cam");
+    cam["from"] = P_pt(s.cam.pos);
+    cam["to"] = P_pt(s.cam.look);
+    cam["up"] = P_pt(s.cam.up);
+    cam["resx"] = parameter_t((float)s.cam.resx);
+    cam["resy"] = parameter_t((float)s.cam.resy);
+    cam["focal"] = parameter_t(s.cam.focal);
+    cam["aspect_ratio"] = parameter_t(s.cam.aspect);
+    y->addCamera(cam);
+    paramMap_t rp;
+    rp["camera_name"] = P_str("cam");
+    rp["raydepth"] = parameter_t((float)s.rp.raydepth);
+    rp["bias"] = parameter_t(s.rp.self_bias);
+    const uint32_t spp = s.rp.spp ? s.rp.spp : 1;
+    rp["AA_passes"] = parameter_t(spp > 1 ? 1.f : 0.f);
+    rp["AA_minsamples"] = parameter_t(spp > 1 ? (float)(spp - 1) : 1.f);
+    rp["AA_pixelwidth"] = parameter_t(s.rp.aa_pixelwidth);
+    rp["AA_threshold"] = parameter_t(0.f);
+    rp["exposure"] = parameter_t(s.rp.exposure);
+    rp["gamma"] = parameter_t(s.rp.gamma);
+    rp["clamp_rgb"] = P_on((s.rp.flags & YR_RENDER_CLAMP_RGB) != 0);
+    rp["alpha_premultiply"] = P_str((s.rp.flags & YR_RENDER_ALPHA_PREMULTIPLY) ? "on" : "off");
+    if (s.rp.background[0] != 0.f || s.rp.background[1] != 0.f || s.rp.background[2] != 0.f) {
+        paramMap_t bg;
+        bg["name"] = P_str("bg");
+        bg["type"] = P_str("constant");
+        bg["color"] = P_col(s.rp.background);
+        y->addBackground(bg);
+        rp["background_name"] = P_str("bg");
+    }
+    floatSink_t sink(s.cam.resx, s.cam.resy);
+    double t0 = now_s();
+    y->render(rp, sink);
+    double t1 = now_s();
+    const int status = arm == "cuda" ? (int)((cudaInterface_t *)y)->lastStatus() : 0;
+    printf("{\"status\": %d, \"render_s\": %.6f}\n", status, t1 - t0);
+    fflush(stdout);
+    FILE *f = fopen(out, "wb");
+    wr(f, &sink.img[0], 4 * sink.img.size());
+    fclose(f);
+    delete y;
+}
+#endif
+
 // ------------------------------------------------------------- illuminate
 // One light's illuminate() at the first hit of a ray, with the light's
 // sample stream set from outside, so that the oracle can be given the same
@@ -1220,6 +1526,9 @@ int main(int argc, char **argv) {
         if (has_crop)
             for (int k = 0; k < 4; k++) crop[k] = atoi(argv[4 + k]);
         cmd_cudarender(s, argv[3], has_crop ? crop : NULL, argc >= 9 ? atol(argv[8]) : -1L);
+    } else if (cmd == "iface") {
+        if (argc < 5) die("iface SCENE OUT ARM [pathcache]");
+        cmd_iface(argv[4], s, argv[3], argc >= 6 ? argv[5] : "");
 #endif
     } else if (cmd == "render_blocks") {
         if (argc < 6) die("render_blocks SCENE OUT THREADS BLOCKS [REPEATS]");
