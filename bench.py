@@ -438,17 +438,28 @@ def run_batch(args, api, torch, local, barrier, steps=None, warmup=None, count=N
     # what the batch would take if every scene ran at the rate that the
     # fastest scene reaches alone (its own device time, CUDA events inside
     # yr_render), summed over the batch
-    rates, srays = [], []
+    rates, srays, sms = [], [], []
     for d, o in zip(dss, plain):
         st1 = d.render_into(o.data_ptr())
         r1 = st1.rays_primary + st1.rays_shadow + st1.rays_bounce
         srays.append(r1)
+        sms.append(st1.ms)
         rates.append(r1 / max(st1.ms, 1e-6) / 1e3)  # Mrays/s
     best = max(rates)
     ideal_ms = sum(srays) / best / 1e3 * steps
+    # where the per-scene path's time goes: the scenes' own device time
+    # (each render alone, CUDA events inside yr_render) and what the calls
+    # add around it; and how much of the device time the largest quarter
+    # of the scenes (by rays) takes
+    dev_ms = float(sum(sms))
+    order = sorted(range(len(srays)), key=lambda i: -srays[i])
+    top = order[:max(1, len(order) // 4)]
     ceiling = {"best_single_scene_value": best, "ideal_ms_per_step": ideal_ms / steps,
                "max_ratio_vs_plain": ms_p / ideal_ms,
-               "note": "the batch's time if every scene ran at the rate that the fastest scene reaches alone"}
+               "note": "the batch's time if every scene ran at the rate that the fastest scene reaches alone",
+               "scenes_device_ms": dev_ms, "plain_call_overhead_ms": ms_p / steps - dev_ms,
+               "largest_quarter_device_share": float(sum(sms[i] for i in top)) / max(dev_ms, 1e-9),
+               "largest_quarter_rays_share": float(sum(srays[i] for i in top)) / max(1.0, float(sum(srays)))}
     value = rays_b / (ms_b / 1000.0) / 1e6
     plain_value = rays_p / (ms_p / 1000.0) / 1e6
     # end to end: parameters host -> device and every image back to pinned host memory
@@ -754,7 +765,10 @@ def main():
                          "plain_gpu_value": b["plain_gpu"]["value"], "ratio": b["speedup_vs_plain"],
                          "identical_images": b["identical_images"], "ms_per_step": b["ms_per_step"],
                          "plain_ms_per_step": b["plain_gpu"]["ms_per_step"], "steps": b["steps"],
-                         "ceiling_ratio_vs_plain": b["ceiling"]["max_ratio_vs_plain"]}
+                         "ceiling_ratio_vs_plain": b["ceiling"]["max_ratio_vs_plain"],
+                         "ceiling": {k: b["ceiling"][k] for k in ("scenes_device_ms", "plain_call_overhead_ms",
+                                                                  "largest_quarter_device_share",
+                                                                  "largest_quarter_rays_share", "note")}}
         d = run_diff(args, api, torch, local, steps=3, warmup=2)
         line["adjoint"] = {"workload": d["config"]["workload"], "forward_ms": d["forward_ms"],
                            "adjoint_ms": d["adjoint_ms"], "ratio": d["adjoint_over_forward"],
