@@ -436,7 +436,7 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
         W.base = (uint32_t)b;
         W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
         const int g = (int)((W.count + kBlock - 1) / kBlock);
-        cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
+        cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 16, st);
         k_prim<<<g, kBlock, 0, st>>>(D, R, W);
         k_adj_shade_camera<<<g, kBlock, 0, st>>>(D, R, W, A);
         cudaMemsetAsync(W.counters + 6, 0, sizeof(uint32_t), st);

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
     __shared__ DevScene S;
     __shared__ DevRender R;
     __shared__ Wave W;
-    __shared__ uint32_t cnt[8];
+    __shared__ uint32_t cnt[16];
     __shared__ uint32_t item;
     uint2 stk_nt[STACK];
     float stk_split[STACK];
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
             W.ns = A.ns[bi.scene];
             W.npath = A.npath[bi.scene];
             W.out = A.outs[bi.scene];
-            for (int k = 0; k < 8; k++) cnt[k] = 0;
+            for (int k = 0; k < 16; k++) cnt[k] = 0;
         }
         __syncthreads();
         const uint32_t count = W.count;
@@ -92,10 +92,8 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
         __syncthreads();
         {
             const uint32_t n = cnt[0];
-            for (uint32_t q = tid; q < n; q += nthr) {
-                st_trace_shadow<INST>(S, W, q, R.self_bias, stk, nodes, tests);
-                n_sh++;
-            }
+            for (uint32_t q = tid; q < n; q += nthr)
+                if (st_trace_shadow<INST>(S, W, q, R.self_bias, stk, nodes, tests)) n_sh++;
         }
         __syncthreads();
         for (uint32_t i = tid; i < count; i += nthr) st_gather_camera(R, W, i);
@@ -117,10 +115,8 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs A) {
                 __syncthreads();
                 {
                     const uint32_t n = cnt[0];
-                    for (uint32_t q = tid; q < n; q += nthr) {
-                        st_trace_shadow<INST>(S, W, q, R.self_bias, stk, nodes, tests);
-                        n_sh++;
-                    }
+                    for (uint32_t q = tid; q < n; q += nthr)
+                        if (st_trace_shadow<INST>(S, W, q, R.self_bias, stk, nodes, tests)) n_sh++;
                 }
                 __syncthreads();
                 for (uint32_t b0 = tid - lane; b0 < nb; b0 += nthr)

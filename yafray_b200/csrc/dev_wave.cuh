@@ -57,8 +57,9 @@ struct Wave {
     float4 *ptot;        // [count] path light: the rounds' sum of path contributions (adaptive rounds)
     uint32_t *nrep;      // [count] path light: extra rounds of the camera sample
     uint32_t rep;        // the round of paths being traced (0 = the first)
-    uint32_t *counters;  // [0] shadow queue, [1] bounce queue, [2] next bounce queue,
-                         // [3..5] ray totals (primary, shadow, bounce) as 2x u32 lo/hi pairs
+    uint32_t *counters;  // [16]: [0] shadow queue, [1] bounce queue, [2] next bounce queue,
+                         // [3..5] ray totals (primary, shadow, bounce) as 2x u32 lo/hi pairs,
+                         // [6] / [7] traversal fetch counters, [8] empty shadow-queue places
     unsigned long long *rays;  // [3] primary, shadow, bounce
     unsigned long long *kst;   // [YR_K_COUNT][3]: rays, nodes, tests per kernel class
     float *out;          // RGBA image (device)
@@ -150,14 +151,21 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred) {
     return base + (uint32_t)__popc(ball & ((1u << lane) - 1u));
 }
 
+// A shadow-queue entry without a ray (a reserved place that its lane did
+// not fill): the traversal skips it and the ray count leaves it out.
+constexpr uint32_t kNoSlot = 0xffffffffu;
+
+__device__ __forceinline__ void put_shadow(const Wave &W, uint32_t q, const V3 &p, int own, const V3 &dir,
+                                           float dist, uint32_t slot) {
+    W.shq0[q] = make_float4(p.x, p.y, p.z, __int_as_float(own));
+    W.shq1[q] = make_float4(dir.x, dir.y, dir.z, dist);
+    W.shq_slot[q] = slot;
+}
+
 __device__ __forceinline__ void emit_shadow(const Wave &W, bool pred, const V3 &p, int own, const V3 &dir,
                                             float dist, uint32_t slot) {
     const uint32_t q = warp_append(&W.counters[0], pred);
-    if (pred) {
-        W.shq0[q] = make_float4(p.x, p.y, p.z, __int_as_float(own));
-        W.shq1[q] = make_float4(dir.x, dir.y, dir.z, dist);
-        W.shq_slot[q] = slot;
-    }
+    if (pred) put_shadow(W, q, p, own, dir, dist, slot);
 }
 
 // --------------------------------------------------------------- kernels
@@ -352,6 +360,21 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                 }
                 status = decided >= 0 ? decided : ((luz && sombra) ? kGuessPenumbra : (luz ? kGuessLight : kGuessShadow));
             }
+            // one queue reservation per warp for the light's sample rays:
+            // every lane that samples this light takes L.samples places,
+            // sample-major (sample jj of the r-th such lane at jj*nw + r),
+            // so a traversal chunk still holds one sample of neighbouring
+            // points; a sample behind the point's tangent plane leaves its
+            // place empty (kNoSlot)
+            const bool sampling = active && lit_side && status == kGuessPenumbra;
+            const unsigned wmask = __activemask();
+            const unsigned wball = __ballot_sync(wmask, sampling);
+            const int wlane = threadIdx.x & 31, wleader = __ffs(wmask) - 1;
+            const uint32_t nw = (uint32_t)__popc(wball), rank = (uint32_t)__popc(wball & ((1u << wlane) - 1u));
+            uint32_t qbase = 0;
+            if (wlane == wleader && nw) qbase = atomicAdd(&W.counters[0], nw * (uint32_t)L.samples);
+            qbase = __shfl_sync(wmask, qbase, wleader);
+            uint32_t holes = 0;
             for (int jj = 0; jj < L.samples; jj++) {
                 const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
                 bool emit = false;
@@ -402,8 +425,18 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                         }
                     }
                 }
-                emit_shadow(W, emit, sp.P, sp.object, rdir, dist, slot);
+                if (sampling) {
+                    const uint32_t q = qbase + (uint32_t)jj * nw + rank;
+                    if (emit) {
+                        put_shadow(W, q, sp.P, sp.object, rdir, dist, slot);
+                    } else {
+                        W.shq_slot[q] = kNoSlot;
+                        holes++;
+                    }
+                }
             }
+            holes = __reduce_add_sync(wmask, holes);
+            if (wlane == wleader && holes) atomicAdd(&W.counters[8], holes);
             off += (uint32_t)L.samples;
         } else if (L.type == YR_LIGHT_HEMI) {
             // hemiLight_t::illuminate (hemilight.cc:58-100), QMC
@@ -578,13 +611,17 @@ static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_shade_camera(D
 }
 #endif
 
+// one queued shadow ray; false for a place without a ray (kNoSlot)
 template <bool INST>
-__device__ __forceinline__ void st_trace_shadow(const DevScene &S, const Wave &W, uint32_t q, float self_bias,
+__device__ __forceinline__ bool st_trace_shadow(const DevScene &S, const Wave &W, uint32_t q, float self_bias,
                                                 const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
+    const uint32_t slot = W.shq_slot[q];
+    if (slot == kNoSlot) return false;
     const float4 a = W.shq0[q], b = W.shq1[q];
     const bool occ = scene_occluded_t<INST>(S, v3(a.x, a.y, a.z), __float_as_int(a.w), v3(b.x, b.y, b.z), b.w, self_bias,
                                     stk, nodes, tests);
-    W.slot_f[W.shq_slot[q]] = occ ? kSlotShadowed : kSlotLit;
+    W.slot_f[slot] = occ ? kSlotShadowed : kSlotLit;
+    return true;
 }
 
 #ifdef YR_WAVE_KERNELS
@@ -604,16 +641,11 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
         const uint32_t q = base + (threadIdx.x & 31u);
-        if (q < n) {
-            st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests);
-            rays++;
-        }
+        if (q < n && st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests)) rays++;
     }
 #else
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests);
-        rays++;
-    }
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        if (st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests)) rays++;
 #endif
     count_work(W, YR_K_SHADOW, rays, nodes, tests);
 }
@@ -1088,7 +1120,10 @@ static __global__ void k_swap_queues(Wave W) {
 #ifdef YR_WAVE_KERNELS
 static __global__ void k_count(Wave W, int which) {
     // accumulate queue lengths into the 64-bit ray totals
-    if (which == 0) W.rays[1] += W.counters[0];
+    if (which == 0) {  // the queue's rays: its places less the empty ones
+        W.rays[1] += W.counters[0] - W.counters[8];
+        W.counters[8] = 0;
+    }
     if (which == 1) W.rays[2] += W.counters[1];
 }
 #endif
@@ -1137,7 +1172,7 @@ __host__ __device__ inline void wave_sizes(const Plan &P, uint32_t wcap, size_t 
     size_t sizes[kNumBufs] = {f4 * w,  f4 * w * P.nl, f4 * w * P.nl, f4 * w,  f4 * pc, f4 * pc,
                               f4 * pc, f4 * pc,       f4 * pc,       f4 * pc, f4 * pc * P.depth, f4 * pc * P.nl,
                               f4 * slots, slots,      f4 * slots,    f4 * slots, 4 * slots, 4 * pc,
-                              4 * pc,  4 * 8,         8 * 4,         8 * 3 * YR_K_COUNT,
+                              4 * pc,  4 * 16,        8 * 4,         8 * 3 * YR_K_COUNT,
                               f4 * w,  4 * w};
     for (int i = 0; i < kNumBufs; i++) b[i] = sizes[i];
 }

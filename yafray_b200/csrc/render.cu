@@ -91,7 +91,7 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
     W.base = (uint32_t)b;
     W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
     const int g = (int)((W.count + kBlock - 1) / kBlock);
-    cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 8, st);
+    cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * 16, st);
     timed(YR_K_PRIMARY, [&] { k_prim<<<g, kBlock, 0, st>>>(D, R, W); });
     timed(YR_K_SHADE_CAMERA, [&] { k_shade_camera<<<g, kBlock, 0, st>>>(D, R, W); });
     timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 0); });
