@@ -168,6 +168,46 @@ __device__ __forceinline__ void emit_shadow(const Wave &W, bool pred, const V3 &
     if (pred) put_shadow(W, q, p, own, dir, dist, slot);
 }
 
+// One shadow-queue reservation per warp for one light's `n` sample rays:
+// every lane that samples the light takes n places, sample-major (sample j
+// of the r-th such lane at j*nw + r), so a traversal chunk holds one sample
+// of neighbouring points, and the warp pays one atomic instead of n.  A
+// sample that turns out to need no ray leaves its place empty (kNoSlot);
+// the empty places are counted for the ray totals.  Whole warp.
+struct WarpPlaces {
+    unsigned mask;
+    uint32_t base, nw, rank, holes;
+    int lane, leader;
+    bool sampling;
+    __device__ __forceinline__ WarpPlaces(const Wave &W, bool s, uint32_t n) : holes(0), sampling(s) {
+        mask = __activemask();
+        const unsigned ball = __ballot_sync(mask, s);
+        lane = threadIdx.x & 31;
+        leader = __ffs(mask) - 1;
+        nw = (uint32_t)__popc(ball);
+        rank = (uint32_t)__popc(ball & ((1u << lane) - 1u));
+        base = 0;
+        if (lane == leader && nw) base = atomicAdd(&W.counters[0], nw * n);
+        base = __shfl_sync(mask, base, leader);
+    }
+    // sample j's ray (emit) or its empty place
+    __device__ __forceinline__ void put(const Wave &W, uint32_t j, bool emit, const V3 &p, int own, const V3 &dir,
+                                        float dist, uint32_t slot) {
+        if (!sampling) return;
+        const uint32_t q = base + j * nw + rank;
+        if (emit) {
+            put_shadow(W, q, p, own, dir, dist, slot);
+        } else {
+            W.shq_slot[q] = kNoSlot;
+            holes++;
+        }
+    }
+    __device__ __forceinline__ void finish(const Wave &W) {
+        const uint32_t h = __reduce_add_sync(mask, holes);
+        if (lane == leader && h) atomicAdd(&W.counters[8], h);
+    }
+};
+
 // --------------------------------------------------------------- kernels
 // Stage bodies.  Each wavefront kernel runs one stage over the whole wave;
 // the batched persistent kernel runs the same stages over one tile inside
@@ -317,7 +357,8 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             const float r0 = cp_rot(R.seed, pixel, d), r1 = cp_rot(R.seed, pixel, d + 1);
             if (guess && stage == 0) {
                 // the guess's probes: unjittered grid points; a point behind
-                // the surface counts as shadow without a ray
+                // the surface counts as shadow without a ray (an empty place)
+                WarpPlaces wp(W, active && lit_side, (uint32_t)L.psamples);
                 for (int j = 0; j < L.psamples; j++) {
                     const uint32_t slot = vtx * W.ns + (uint32_t)L.probe_off + (uint32_t)j;
                     bool emit = false;
@@ -339,8 +380,9 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                             }
                         }
                     }
-                    emit_shadow(W, emit, sp.P, sp.object, rdir, dist, slot);
+                    wp.put(W, (uint32_t)j, emit, sp.P, sp.object, rdir, dist, slot);
                 }
+                wp.finish(W);
                 if (active)
                     for (int jj = 0; jj < L.samples; jj++) W.slot_f[vtx * W.ns + off + (uint32_t)jj] = kSlotNone;
                 off += (uint32_t)L.samples;
@@ -360,21 +402,9 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                 }
                 status = decided >= 0 ? decided : ((luz && sombra) ? kGuessPenumbra : (luz ? kGuessLight : kGuessShadow));
             }
-            // one queue reservation per warp for the light's sample rays:
-            // every lane that samples this light takes L.samples places,
-            // sample-major (sample jj of the r-th such lane at jj*nw + r),
-            // so a traversal chunk still holds one sample of neighbouring
-            // points; a sample behind the point's tangent plane leaves its
-            // place empty (kNoSlot)
-            const bool sampling = active && lit_side && status == kGuessPenumbra;
-            const unsigned wmask = __activemask();
-            const unsigned wball = __ballot_sync(wmask, sampling);
-            const int wlane = threadIdx.x & 31, wleader = __ffs(wmask) - 1;
-            const uint32_t nw = (uint32_t)__popc(wball), rank = (uint32_t)__popc(wball & ((1u << wlane) - 1u));
-            uint32_t qbase = 0;
-            if (wlane == wleader && nw) qbase = atomicAdd(&W.counters[0], nw * (uint32_t)L.samples);
-            qbase = __shfl_sync(wmask, qbase, wleader);
-            uint32_t holes = 0;
+            // the light's sample rays in one reservation per warp; a sample
+            // behind the point's tangent plane leaves its place empty
+            WarpPlaces wp(W, active && lit_side && status == kGuessPenumbra, (uint32_t)L.samples);
             for (int jj = 0; jj < L.samples; jj++) {
                 const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
                 bool emit = false;
@@ -425,18 +455,9 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                         }
                     }
                 }
-                if (sampling) {
-                    const uint32_t q = qbase + (uint32_t)jj * nw + rank;
-                    if (emit) {
-                        put_shadow(W, q, sp.P, sp.object, rdir, dist, slot);
-                    } else {
-                        W.shq_slot[q] = kNoSlot;
-                        holes++;
-                    }
-                }
+                wp.put(W, (uint32_t)jj, emit, sp.P, sp.object, rdir, dist, slot);
             }
-            holes = __reduce_add_sync(wmask, holes);
-            if (wlane == wleader && holes) atomicAdd(&W.counters[8], holes);
+            wp.finish(W);
             off += (uint32_t)L.samples;
         } else if (L.type == YR_LIGHT_HEMI) {
             // hemiLight_t::illuminate (hemilight.cc:58-100), QMC
@@ -458,6 +479,9 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             }
             const uint32_t d = light_dim(k, v);
             const float r0 = cp_rot(R.seed, pixel, d), r1 = cp_rot(R.seed, pixel, d + 1);
+            // one reservation per warp; a direction below the horizon leaves
+            // its place empty
+            WarpPlaces wp(W, active && go, (uint32_t)L.samples);
             for (int jj = 0; jj < L.samples; jj++) {
                 const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
                 bool emit = false;
@@ -486,8 +510,9 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                         }
                     }
                 }
-                emit_shadow(W, emit, sp.P, sp.object, rdir, dist, slot);
+                wp.put(W, (uint32_t)jj, emit, sp.P, sp.object, rdir, dist, slot);
             }
+            wp.finish(W);
             off += (uint32_t)L.samples;
         }
     }
