@@ -208,125 +208,6 @@ __device__ __forceinline__ float sel3(int a, float v0, float v1, float v2) {
     return a == 0 ? v0 : (a == 1 ? v1 : v2);
 }
 
-#ifndef YR_KD_ONE_LOOP
-#define YR_KD_ONE_LOOP 0
-#endif
-#if YR_KD_ONE_LOOP
-// The same walk as one loop whose every pass is either one descent step or
-// one leaf (its triangles, then the pop to the next far node), so that the
-// lanes of a warp in different phases advance in the same pass instead of
-// waiting for each other's inner loops.  Nodes, order and answers are the
-// nested walk's.
-template <bool ANY>
-__device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V3 &from, const RayR &R, float dist,
-                                float &Z, KdResult &res, const KdStack &stk) {
-    float a, b;
-    if (!box_enter_leave(obj.tb, obj.tb + 3, from, R, dist, a, b)) return false;
-    const V3 &ray = R.d;
-    const float f0 = from.x, f1 = from.y, f2 = from.z, r0 = ray.x, r1 = ray.y, r2 = ray.z;
-    bool hit = false;
-    uint32_t curr = obj.root;
-    float en_t = a, en0, en1, en2;
-    if (a >= 0.f) {
-        en0 = f0 + a * r0;
-        en1 = f1 + a * r1;
-        en2 = f2 + a * r2;
-    } else {
-        en0 = f0;
-        en1 = f1;
-        en2 = f2;
-    }
-    float ex_t = b, ex0 = f0 + b * r0, ex1 = f1 + b * r1, ex2 = f2 + b * r2;
-    stk.nt[0] = make_uint2(kNodeMask | (3u << 30), __float_as_uint(b));
-    int sp = 1;
-    if (dist < en_t) return false;
-    uint32_t leaves = 1;
-    uint2 nd = __ldg(S.nodes + curr);
-    for (;;) {
-        if ((nd.y & 3u) != 3u) {
-            res.nodes++;
-            const int axis = (int)(nd.y & 3u);
-            const float split = __uint_as_float(nd.x);
-            const uint32_t right = nd.y >> 2;
-            const uint2 nl = __ldg(S.nodes + curr + 1), nr = __ldg(S.nodes + right);
-            uint32_t far_child;
-            if (sel3(axis, en0, en1, en2) <= split) {
-                if (sel3(axis, ex0, ex1, ex2) <= split) {
-                    curr = curr + 1;
-                    nd = nl;
-                    continue;
-                }
-                far_child = right;
-                curr = curr + 1;
-            } else {
-                if (split < sel3(axis, ex0, ex1, ex2)) {
-                    curr = right;
-                    nd = nr;
-                    continue;
-                }
-                far_child = curr + 1;
-                curr = right;
-            }
-            const float t = (split - sel3(axis, f0, f1, f2)) * sel3(axis, R.inv.x, R.inv.y, R.inv.z);
-            if (sp >= stk.cap) {
-                dev_fail(S.status, kDevStackOverflow);
-                return false;
-            }
-            stk.nt[sp] = make_uint2(far_child | ((uint32_t)axis << 30), __float_as_uint(t));
-            stk.split[sp] = split;
-            sp++;
-            ex_t = t;
-            ex0 = axis == 0 ? split : f0 + t * r0;
-            ex1 = axis == 1 ? split : f1 + t * r1;
-            ex2 = axis == 2 ? split : f2 + t * r2;
-            nd = curr == right ? nr : nl;
-            continue;
-        }
-        res.nodes++;
-        const uint32_t np = nd.y >> 2;
-        for (uint32_t k = 0; k < np; k++) {
-            const uint32_t ti = (np == 1) ? nd.x : __ldg(S.prims + nd.x + k);
-            res.tests++;
-            const Tri tr = load_tri(S.tris, ti);
-            float rt;
-            if (tri_hit(tr, from, ray, rt)) {
-                if (ANY) {
-                    if (rt < dist && rt > 0.f) {
-                        res.tri = ti;
-                        return true;
-                    }
-                } else if (rt < Z && rt >= 0.f) {
-                    Z = rt;
-                    res.tri = ti;
-                    hit = true;
-                }
-            }
-        }
-        if (!ANY && hit && Z <= ex_t) return true;
-        en_t = ex_t;
-        en0 = ex0;
-        en1 = ex1;
-        en2 = ex2;
-        sp--;
-        curr = stk.nt[sp].x & kNodeMask;
-        if (curr == kNodeMask) break;
-        const uint2 nx = stk.nt[sp - 1];
-        ex_t = __uint_as_float(nx.y);
-        const uint32_t ax = nx.x >> 30;
-        const float sp_split = stk.split[sp - 1];
-        ex0 = ax == 0u ? sp_split : f0 + ex_t * r0;
-        ex1 = ax == 1u ? sp_split : f1 + ex_t * r1;
-        ex2 = ax == 2u ? sp_split : f2 + ex_t * r2;
-        if (dist < en_t) break;
-        if (++leaves > kMaxLeafVisits) {
-            dev_fail(S.status, kDevIterationCap);
-            return false;
-        }
-        nd = __ldg(S.nodes + curr);
-    }
-    return hit;
-}
-#else
 template <bool ANY>
 __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V3 &from, const RayR &R, float dist,
                                 float &Z, KdResult &res, const KdStack &stk) {
@@ -441,7 +322,6 @@ __device__ inline bool kd_trace(const DevScene &S, const DevObject &obj, const V
     }
     return hit;
 }
-#endif
 
 // geomeIterator_t (geometree.h:36-157) in its front-to-back mode: yields
 // objects whose bound the ray crosses before `maximun`, nearest entry first.

@@ -518,31 +518,6 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
     }
 }
 
-// The sum of the lit slots s0 .. s0+n-1 in slot order.  Four slots' flags
-// and colours are loaded before any is used, so that the loads overlap (a
-// colour whose slot is not lit is loaded and left unused).
-__device__ __forceinline__ C3 sum_lit(const Wave &W, uint32_t s0, int n) {
-    C3 t = c3(0.f, 0.f, 0.f);
-    int j = 0;
-    for (; j + 4 <= n; j += 4) {
-        const uint32_t s = s0 + (uint32_t)j;
-        const uint8_t f0 = W.slot_f[s], f1 = W.slot_f[s + 1], f2 = W.slot_f[s + 2], f3 = W.slot_f[s + 3];
-        const float4 c0 = W.slot_c[s], c1 = W.slot_c[s + 1], c2 = W.slot_c[s + 2], c3v = W.slot_c[s + 3];
-        if (f0 == kSlotLit) t = t + c3(c0.x, c0.y, c0.z);
-        if (f1 == kSlotLit) t = t + c3(c1.x, c1.y, c1.z);
-        if (f2 == kSlotLit) t = t + c3(c2.x, c2.y, c2.z);
-        if (f3 == kSlotLit) t = t + c3(c3v.x, c3v.y, c3v.z);
-    }
-    for (; j < n; j++) {
-        const uint32_t s = s0 + (uint32_t)j;
-        if (W.slot_f[s] == kSlotLit) {
-            const float4 c = W.slot_c[s];
-            t = t + c3(c.x, c.y, c.z);
-        }
-    }
-    return t;
-}
-
 // light terms of one vertex from its slots, in light order (scene.cc:267-272)
 __device__ __forceinline__ C3 gather_term(const DevRender &R, const Wave &W, const DevLight &L, int k, uint32_t vtx,
                                           uint32_t off, const float4 *aux) {
@@ -557,12 +532,28 @@ __device__ __forceinline__ C3 gather_term(const DevRender &R, const Wave &W, con
     if (L.type == YR_LIGHT_AREA) {
         const float4 a = aux[vtx * R.nlights + k];
         if (a.y == 0.f) return c3(0.f, 0.f, 0.f);
-        return (a.x * sum_lit(W, vtx * W.ns + off, L.samples)) / (float)L.samples;
+        C3 resul = c3(0.f, 0.f, 0.f);
+        for (int jj = 0; jj < L.samples; jj++) {
+            const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+            if (W.slot_f[slot] == kSlotLit) {
+                const float4 c = W.slot_c[slot];
+                resul = resul + c3(c.x, c.y, c.z);
+            }
+        }
+        return (a.x * resul) / (float)L.samples;
     }
     if (L.type == YR_LIGHT_HEMI) {
         const float4 a = aux[vtx * R.nlights + k];
         if (a.w == 0.f) return c3(0.f, 0.f, 0.f);
-        return (L.sampdiv * sum_lit(W, vtx * W.ns + off, L.samples)) * c3(a.x, a.y, a.z);
+        C3 total = c3(0.f, 0.f, 0.f);
+        for (int jj = 0; jj < L.samples; jj++) {
+            const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+            if (W.slot_f[slot] == kSlotLit) {
+                const float4 c = W.slot_c[slot];
+                total = total + c3(c.x, c.y, c.z);
+            }
+        }
+        return (L.sampdiv * total) * c3(a.x, a.y, a.z);
     }
     return c3(0.f, 0.f, 0.f);
 }
