@@ -114,7 +114,7 @@ __device__ __forceinline__ C3 adj_vertex_direct(const DevRender &R, const Wave &
         const DevLight L = R.lights[k];
         C3 Dk = c3(0.f, 0.f, 0.f), Sk = c3(0.f, 0.f, 0.f);
         if (L.type == YR_LIGHT_POINT) {
-            const uint32_t slot = vtx * W.ns + off;
+            const uint32_t slot = slot_of(W, vtx, off);
             if (W.slot_f[slot] == kSlotLit) {
                 const float4 d = W.slot_c[slot], e = A.slot_s[slot];
                 Dk = c3(d.x, d.y, d.z);
@@ -124,7 +124,7 @@ __device__ __forceinline__ C3 adj_vertex_direct(const DevRender &R, const Wave &
             const float4 a = aux[vtx * R.nlights + k];
             if (a.y != 0.f) {
                 for (int jj = 0; jj < L.samples; jj++) {
-                    const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+                    const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
                     if (W.slot_f[slot] == kSlotLit) {
                         const float4 d = W.slot_c[slot], e = A.slot_s[slot];
                         Dk = Dk + c3(d.x, d.y, d.z);
@@ -140,7 +140,7 @@ __device__ __forceinline__ C3 adj_vertex_direct(const DevRender &R, const Wave &
             if (a.w != 0.f) {
                 C3 total = c3(0.f, 0.f, 0.f);
                 for (int jj = 0; jj < L.samples; jj++) {
-                    const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+                    const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
                     if (W.slot_f[slot] == kSlotLit) {
                         const float4 d = W.slot_c[slot];
                         total = total + c3(d.x, d.y, d.z);

@@ -31,6 +31,7 @@ struct Wave {
     uint32_t base;       // first camera sample (pixel*spp + s) of the wave
     uint32_t count;      // camera samples in the wave
     uint32_t ns;         // shadow slots per vertex
+    uint32_t nv;         // vertices the slot arrays hold (slot s of vertex v at s*nv + v)
     uint32_t npath;      // path samples per camera sample (0: no path light)
     // per camera sample
     float4 *hit0;        // t, object, triangle, (ray count)
@@ -64,6 +65,11 @@ struct Wave {
     unsigned long long *kst;   // [YR_K_COUNT][3]: rays, nodes, tests per kernel class
     float *out;          // RGBA image (device)
 };
+
+// Slot s of vertex v.  Slots are stored sample-major, so that the lanes of
+// a warp (consecutive vertices) write and read one slot of neighbouring
+// vertices at neighbouring addresses.
+__host__ __device__ __forceinline__ uint32_t slot_of(const Wave &W, uint32_t v, uint32_t s) { return s * W.nv + v; }
 
 // Extra per-wave state of the adjoint recompute (yr_backward).
 struct AdjWave {
@@ -310,7 +316,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             continue;
         }
         if (L.type == YR_LIGHT_POINT) {
-            const uint32_t slot = vtx * W.ns + off;
+            const uint32_t slot = slot_of(W, vtx, off);
             bool emit = false;
             V3 rdir;
             float dist = 0.f;
@@ -360,7 +366,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                 // the surface counts as shadow without a ray (an empty place)
                 WarpPlaces wp(W, active && lit_side, (uint32_t)L.psamples);
                 for (int j = 0; j < L.psamples; j++) {
-                    const uint32_t slot = vtx * W.ns + (uint32_t)L.probe_off + (uint32_t)j;
+                    const uint32_t slot = slot_of(W, vtx, (uint32_t)L.probe_off + (uint32_t)j);
                     bool emit = false;
                     V3 rdir;
                     float dist = 0.f;
@@ -384,7 +390,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                 }
                 wp.finish(W);
                 if (active)
-                    for (int jj = 0; jj < L.samples; jj++) W.slot_f[vtx * W.ns + off + (uint32_t)jj] = kSlotNone;
+                    for (int jj = 0; jj < L.samples; jj++) W.slot_f[slot_of(W, vtx, off + (uint32_t)jj)] = kSlotNone;
                 off += (uint32_t)L.samples;
                 continue;
             }
@@ -397,7 +403,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
                         decided = kGuessPenumbra;
                         break;
                     }
-                    if (W.slot_f[vtx * W.ns + (uint32_t)L.probe_off + (uint32_t)j] == kSlotLit) luz = true;
+                    if (W.slot_f[slot_of(W, vtx, (uint32_t)L.probe_off + (uint32_t)j)] == kSlotLit) luz = true;
                     else sombra = true;
                 }
                 status = decided >= 0 ? decided : ((luz && sombra) ? kGuessPenumbra : (luz ? kGuessLight : kGuessShadow));
@@ -406,7 +412,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             // behind the point's tangent plane leaves its place empty
             WarpPlaces wp(W, active && lit_side && status == kGuessPenumbra, (uint32_t)L.samples);
             for (int jj = 0; jj < L.samples; jj++) {
-                const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+                const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
                 bool emit = false;
                 V3 rdir;
                 float dist = 0.f;
@@ -483,7 +489,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             // its place empty
             WarpPlaces wp(W, active && go, (uint32_t)L.samples);
             for (int jj = 0; jj < L.samples; jj++) {
-                const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+                const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
                 bool emit = false;
                 V3 rdir;
                 float dist = 0.f;
@@ -522,7 +528,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
 __device__ __forceinline__ C3 gather_term(const DevRender &R, const Wave &W, const DevLight &L, int k, uint32_t vtx,
                                           uint32_t off, const float4 *aux) {
     if (L.type == YR_LIGHT_POINT) {
-        const uint32_t slot = vtx * W.ns + off;
+        const uint32_t slot = slot_of(W, vtx, off);
         if (W.slot_f[slot] == kSlotLit) {
             const float4 c = W.slot_c[slot];
             return c3(c.x, c.y, c.z);
@@ -534,7 +540,7 @@ __device__ __forceinline__ C3 gather_term(const DevRender &R, const Wave &W, con
         if (a.y == 0.f) return c3(0.f, 0.f, 0.f);
         C3 resul = c3(0.f, 0.f, 0.f);
         for (int jj = 0; jj < L.samples; jj++) {
-            const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+            const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
             if (W.slot_f[slot] == kSlotLit) {
                 const float4 c = W.slot_c[slot];
                 resul = resul + c3(c.x, c.y, c.z);
@@ -547,7 +553,7 @@ __device__ __forceinline__ C3 gather_term(const DevRender &R, const Wave &W, con
         if (a.w == 0.f) return c3(0.f, 0.f, 0.f);
         C3 total = c3(0.f, 0.f, 0.f);
         for (int jj = 0; jj < L.samples; jj++) {
-            const uint32_t slot = vtx * W.ns + off + (uint32_t)jj;
+            const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
             if (W.slot_f[slot] == kSlotLit) {
                 const float4 c = W.slot_c[slot];
                 total = total + c3(c.x, c.y, c.z);
@@ -1247,6 +1253,7 @@ __host__ __device__ inline void assign_wave(const Plan &P, uint32_t wcap, char *
     W.rep = 0;
     W.ns = P.ns;
     W.npath = P.npath;
+    W.nv = P.npath > 1u ? wcap * P.npath : wcap;  // as wave_sizes' vc
 }
 
 // Blocks of kBlock threads that fill every SM once for `kernel` (queried
