@@ -55,12 +55,15 @@ struct Wave {
     uint32_t *shq_slot;
     uint32_t *bq;        // bounce queue (path indices)
     uint32_t *bq2;
+    uint32_t *sq;        // [count * npath] the bounce queue in shading order: hits first, then misses
+    uint32_t part;       // 1: the bounce walk writes sq and the path shading takes its order
     float4 *ptot;        // [count] path light: the rounds' sum of path contributions (adaptive rounds)
     uint32_t *nrep;      // [count] path light: extra rounds of the camera sample
     uint32_t rep;        // the round of paths being traced (0 = the first)
     uint32_t *counters;  // [16]: [0] shadow queue, [1] bounce queue, [2] next bounce queue,
                          // [3..5] ray totals (primary, shadow, bounce) as 2x u32 lo/hi pairs,
-                         // [6] / [7] traversal fetch counters, [8] empty shadow-queue places
+                         // [6] / [7] traversal fetch counters, [8] empty shadow-queue places,
+                         // [9] / [10] hits / misses placed in sq
     unsigned long long *rays;  // [3] primary, shadow, bounce
     unsigned long long *kst;   // [YR_K_COUNT][3]: rays, nodes, tests per kernel class
     float *out;          // RGBA image (device)
@@ -175,17 +178,24 @@ __device__ __forceinline__ void emit_shadow(const Wave &W, bool pred, const V3 &
 }
 
 // One shadow-queue reservation per warp for one light's `n` sample rays:
-// every lane that samples the light takes n places, sample-major (sample j
-// of the r-th such lane at j*nw + r), so a traversal chunk holds one sample
-// of neighbouring points, and the warp pays one atomic instead of n.  A
-// sample that turns out to need no ray leaves its place empty (kNoSlot);
+// every lane that samples the light takes n places, and the warp pays one
+// atomic instead of n.  The places are arranged for the walk, whose warps
+// take the queue 32 places at a time:
+//   at camera hits, sample-major (sample j of the r-th such lane at
+//   j*nw + r): the warp's lanes are neighbouring camera samples, so 32
+//   places are rays from nearly one point into one cell of the light's
+//   sample grid;
+//   at path vertices, lane-major (at r*n + j): the lanes are unrelated
+//   paths, so 32 places are the rays of one or two points.
+// A sample that turns out to need no ray leaves its place empty (kNoSlot);
 // the empty places are counted for the ray totals.  Whole warp.
 struct WarpPlaces {
     unsigned mask;
-    uint32_t base, nw, rank, holes;
+    uint32_t base, nw, rank, holes, n;
     int lane, leader;
-    bool sampling;
-    __device__ __forceinline__ WarpPlaces(const Wave &W, bool s, uint32_t n) : holes(0), sampling(s) {
+    bool sampling, lane_major;
+    __device__ __forceinline__ WarpPlaces(const Wave &W, bool s, uint32_t n_, bool path_vertex)
+        : holes(0), n(n_), sampling(s), lane_major(path_vertex) {
         mask = __activemask();
         const unsigned ball = __ballot_sync(mask, s);
         lane = threadIdx.x & 31;
@@ -200,7 +210,7 @@ struct WarpPlaces {
     __device__ __forceinline__ void put(const Wave &W, uint32_t j, bool emit, const V3 &p, int own, const V3 &dir,
                                         float dist, uint32_t slot) {
         if (!sampling) return;
-        const uint32_t q = base + j * nw + rank;
+        const uint32_t q = lane_major ? base + rank * n + j : base + j * nw + rank;
         if (emit) {
             put_shadow(W, q, p, own, dir, dist, slot);
         } else {
@@ -364,7 +374,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             if (guess && stage == 0) {
                 // the guess's probes: unjittered grid points; a point behind
                 // the surface counts as shadow without a ray (an empty place)
-                WarpPlaces wp(W, active && lit_side, (uint32_t)L.psamples);
+                WarpPlaces wp(W, active && lit_side, (uint32_t)L.psamples, v > 0);
                 for (int j = 0; j < L.psamples; j++) {
                     const uint32_t slot = slot_of(W, vtx, (uint32_t)L.probe_off + (uint32_t)j);
                     bool emit = false;
@@ -410,7 +420,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             }
             // the light's sample rays in one reservation per warp; a sample
             // behind the point's tangent plane leaves its place empty
-            WarpPlaces wp(W, active && lit_side && status == kGuessPenumbra, (uint32_t)L.samples);
+            WarpPlaces wp(W, active && lit_side && status == kGuessPenumbra, (uint32_t)L.samples, v > 0);
             for (int jj = 0; jj < L.samples; jj++) {
                 const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
                 bool emit = false;
@@ -487,7 +497,7 @@ __device__ __forceinline__ void shade_lights(const DevScene &S, const DevRender 
             const float r0 = cp_rot(R.seed, pixel, d), r1 = cp_rot(R.seed, pixel, d + 1);
             // one reservation per warp; a direction below the horizon leaves
             // its place empty
-            WarpPlaces wp(W, active && go, (uint32_t)L.samples);
+            WarpPlaces wp(W, active && go, (uint32_t)L.samples, v > 0);
             for (int jj = 0; jj < L.samples; jj++) {
                 const uint32_t slot = slot_of(W, vtx, off + (uint32_t)jj);
                 bool emit = false;
@@ -730,9 +740,19 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_bounce(D
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
         const uint32_t q = base + (threadIdx.x & 31u);
+        bool hit = false;
         if (q < n) {
             st_trace_bounce<INST>(S, W, q, stk, nodes, tests);
+            hit = __float_as_int(W.p_hit[W.bq[q]].y) >= 0;
             rays++;
+        }
+        if (W.part) {
+            // the shading order: hits from the front, misses from the
+            // back, so that a shading warp takes paths of one kind and its
+            // light reservations hold full warps of points (whole warp)
+            const uint32_t ph = warp_append(&W.counters[9], q < n && hit);
+            const uint32_t pm = warp_append(&W.counters[10], q < n && !hit);
+            if (q < n) W.sq[hit ? ph : n - 1u - pm] = W.bq[q];
         }
     }
 #else
@@ -752,7 +772,7 @@ template <bool ADJ = false>
 __device__ __forceinline__ void st_shade_path(const DevScene &S, const DevRender &R, const Wave &W, int j,
                                               uint32_t q, uint32_t n, const AdjWave *A = nullptr) {
     const bool inq = q < n;
-    const uint32_t p = inq ? W.bq[q] : 0;
+    const uint32_t p = inq ? (W.part ? W.sq[q] : W.bq[q]) : 0;
     const uint32_t i = p / W.npath, pi = p % W.npath;
     const uint32_t cs = W.base + i;
     int px_x, px_y;
@@ -1191,7 +1211,7 @@ inline yr_status make_plan(const yr_scene *scene, Plan &P) {
     return YR_OK;
 }
 
-constexpr int kNumBufs = 24;
+constexpr int kNumBufs = 25;
 constexpr size_t kBufAlign = 256;
 
 // Bytes of each scratch buffer for a wave of `wcap` camera samples, in the
@@ -1204,7 +1224,7 @@ __host__ __device__ inline void wave_sizes(const Plan &P, uint32_t wcap, size_t 
                               f4 * pc, f4 * pc,       f4 * pc,       f4 * pc, f4 * pc * P.depth, f4 * pc * P.nl,
                               f4 * slots, slots,      f4 * slots,    f4 * slots, 4 * slots, 4 * pc,
                               4 * pc,  4 * 16,        8 * 4,         8 * 3 * YR_K_COUNT,
-                              f4 * w,  4 * w};
+                              f4 * w,  4 * w,         4 * pc};
     for (int i = 0; i < kNumBufs; i++) b[i] = sizes[i];
 }
 
@@ -1250,6 +1270,8 @@ __host__ __device__ inline void assign_wave(const Plan &P, uint32_t wcap, char *
     W.kst = (unsigned long long *)ptr[k++];
     W.ptot = (float4 *)ptr[k++];
     W.nrep = (uint32_t *)ptr[k++];
+    W.sq = (uint32_t *)ptr[k++];
+    W.part = 0;
     W.rep = 0;
     W.ns = P.ns;
     W.npath = P.npath;

@@ -52,6 +52,7 @@ struct WaveGrids {
 static WaveGrids waves_begin(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, float *out, cudaStream_t st) {
     DevRender &R = scene->rdr;
     W.out = out;
+    W.part = 1;  // the path shading takes the bounce walk's hits-first order
     cudaMemsetAsync(W.rays, 0, sizeof(unsigned long long) * 4, st);
     cudaMemsetAsync(W.kst, 0, sizeof(unsigned long long) * 3 * YR_K_COUNT, st);
     // pixels outside the region are written as 0 (scene.cc:773)
@@ -117,6 +118,7 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
         for (int j = 0; j < R.path_depth; j++) {
             timed(YR_K_OTHER, [&] { k_count<<<1, 1, 0, st>>>(W, 1); });
             cudaMemsetAsync(W.counters + 7, 0, sizeof(uint32_t), st);
+            cudaMemsetAsync(W.counters + 9, 0, 2 * sizeof(uint32_t), st);
             timed(YR_K_BOUNCE, [&] { k_bounce<<<gb, kBlock, 0, st>>>(D, W); });
             cudaMemsetAsync(W.counters, 0, sizeof(uint32_t), st);
             timed(YR_K_SHADE_PATH, [&] { k_shade_path<<<gp, kBlock, 0, st>>>(D, R, W, j); });
