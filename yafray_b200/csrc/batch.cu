@@ -483,8 +483,8 @@ static yr_status run_config(BatchCtx &C, const BatchConfig &cfg, const std::vect
 }
 
 // Tiles: time every (stack, tile, block) candidate on every 8th item and keep
-// the fastest, then time it on all items.  Waves: time 4, 16 and 32
-// streams on the whole batch.  Keep the fastest schedule.
+// the fastest, then time it on all items.  Waves: time 4 and 16 streams on
+// the whole batch.  Keep the fastest schedule.
 static yr_status autotune(BatchCtx &C, cudaStream_t st, int want_mode, BatchConfig &best) {
     yr_status r;
     float best_ms = 3.4e38f;
@@ -518,8 +518,8 @@ static yr_status autotune(BatchCtx &C, cudaStream_t st, int want_mode, BatchConf
         best = bt;
     }
     if (want_mode != YR_BATCH_TILES) {
-        const int nmax = (int)std::min<size_t>(C.scenes.size(), 32);
-        for (int n : {std::min(4, nmax), std::min(16, nmax), nmax}) {
+        const int nmax = (int)std::min<size_t>(C.scenes.size(), 16);
+        for (int n : {std::min(4, nmax), nmax}) {
             BatchConfig cfg;
             cfg.mode = YR_BATCH_WAVES;
             cfg.streams = n;
