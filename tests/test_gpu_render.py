@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import yrtest as T
-from yafray_b200 import api, scenes
+from yafray_b200 import abi, api, scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -39,6 +39,29 @@ def _cmp(img, ref, O=None):
     assert not unexplained, (f"{len(unexplained)} of {len(bad)} pixels beyond {RTOL} without a cut-off flip: "
                              f"{unexplained[:6]}")
     return rel
+
+
+@pytest.mark.parametrize("idx", [0, 5, 11, 17, 23, 29])
+def test_render_uneven_batch_scenes(cuda, idx):
+    """Scenes of the uneven batch (spheres and tori, 1-4 point and area
+    lights, GI of 1-3 bounces) at a reduced frame, some with a hemi light
+    or a penumbra guess added, against the oracle: the shading warps' queue
+    reservations, the path vertices' lane-major places and the hits-first
+    path-shading order on many scene shapes."""
+    sc = scenes.config_batch(count=30)[idx]
+    sc.camera.resx, sc.camera.resy = 40, 30
+    sc.render.spp = 2
+    if idx % 2:
+        sc.lights.append(scenes.hemi_light(samples=4, power=0.4, maxdist=2.5))
+    if idx % 4 == 1:
+        for l in sc.lights:
+            if l.type == abi.YR_LIGHT_AREA and l.samples > 1:
+                l.psamples = 3
+    img = api.DeviceScene(sc).render()
+    O = T.OracleScene(sc)
+    ref, _ = O.render()
+    assert np.array_equal(img[..., 3], ref[..., 3])
+    _cmp(img, ref, O)
 
 
 def test_render_small_point_light(cuda):
