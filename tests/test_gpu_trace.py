@@ -104,6 +104,58 @@ def test_shadow_many_objects(cuda, flags):
     assert 0 < ref.sum() < len(ref)
 
 
+def _flat_dirs(d, seed):
+    """Directions with one or two components zero (rays parallel to a
+    coordinate plane or along an axis) or subnormal (1/d overflows)."""
+    rng = np.random.default_rng(seed)
+    d = d.astype(np.float64).copy()
+    n = len(d)
+    kind = rng.integers(0, 4, n)   # 0: as given, 1: one zero, 2: two zeros, 3: one subnormal
+    ax = rng.integers(0, 3, n)
+    rows = np.arange(n)
+    one = (kind == 1) | (kind == 3)
+    d[rows[one], ax[one]] = 0.0
+    two = kind == 2
+    keep = ax[two]
+    sign = np.sign(d[rows[two], keep])
+    sign[sign == 0] = 1.0
+    d[two] = 0.0
+    d[rows[two], keep] = sign
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = d.astype(np.float32)
+    sub = kind == 3
+    d[rows[sub], ax[sub]] = np.float32(1e-40) * np.sign(rng.standard_normal(sub.sum())).astype(np.float32)
+    return d, kind
+
+
+@pytest.mark.parametrize("flags", [0, SHADOW_TREE, EXACT])
+def test_axis_parallel_rays(cuda, flags):
+    """Rays with zero or subnormal direction components, whose reciprocals
+    are infinite (bound_t::cross skips a zero axis): closest hits and shadow
+    answers bit for bit, on the many-object scene."""
+    sc = scenes.config_large(seed=3, resx=64, resy=48, spp=1, grid=4)
+    sc.render.flags = flags
+    ds = api.DeviceScene(sc)
+    O = T.OracleScene(sc)
+    rays = T.random_rays(sc, 30000, 21)
+    rays[:, 4:7], kind = _flat_dirs(rays[:, 4:7], 22)
+    got, ref = _run_closest(cuda, ds, rays), O.trace_closest(rays)
+    assert np.array_equal(got[:, :3], ref[:, :3])
+    for k in range(4):
+        assert (ref[kind == k, 1] != 0xFFFFFFFF).sum() > 200
+    s = np.zeros((len(rays), 8), np.float32)
+    s[:, :3] = rays[:, :3]
+    s[:, 3] = np.random.default_rng(23).integers(0, len(sc.meshes), len(rays)).astype(np.uint32).view(np.float32)
+    # half directional (l = the direction), half towards a point along it
+    dirmode = np.arange(len(rays)) % 2 == 0
+    dist = np.random.default_rng(24).uniform(0.5, 8, (len(rays), 1)).astype(np.float32)
+    s[:, 4:7] = np.where(dirmode[:, None], rays[:, 4:7], rays[:, :3] + rays[:, 4:7] * dist)
+    s[:, 7] = dirmode.astype(np.uint32).view(np.float32)
+    occ, oref = _run_shadow(cuda, ds, s), O.trace_shadow(s)
+    assert np.array_equal(occ, oref)
+    assert 0 < oref.sum() < len(oref)
+
+
 def test_empty_query(cuda):
     sc = scenes.config_small(32, 24)
     ds = api.DeviceScene(sc)

@@ -72,19 +72,21 @@ __device__ __forceinline__ bool box_where(const float *bmin, const float *bmax, 
 }
 
 // A ray prepared for the object-tree walk.  Unless the scene asks for the
-// exact order, the walk uses a conservative slab test: t = b*y + (-f*y)
-// with one FMA per plane, widened by a bound on its rounding error so that
-// the interval contains the one bound_t::cross computes.  Crossing tests
-// then never reject a box that the exact test accepts, and entry distances
-// are lower bounds, so pruning by the closest hit so far stays safe; only
-// the visiting order of boxes whose entry distances agree to within that
-// error can differ (which changes the reported object only when two
-// objects are hit at exactly the same distance).
+// exact order, the walk uses a conservative slab test: per axis the near
+// plane's distance is RN(b*y + (nf - e)) and the far plane's RN(b*y + (nf +
+// e)), one FMA each, with y = 1/d, nf = RN(-f*y) and e a bound on the
+// rounding errors, so that the interval contains the one bound_t::cross
+// computes.  Crossing tests then never reject a box that the exact test
+// accepts, and entry distances are lower bounds, so pruning by the closest
+// hit so far stays safe; only the visiting order of boxes whose entry
+// distances agree to within that error can differ (which changes the
+// reported object only when two objects are hit at exactly the same
+// distance).
 struct ObjRay {
     V3 from;
     RayR R;
-    float nf[3];   // RN(-from*y) with y = 1/d
-    float err[3];  // per-axis error bound of t; +inf where d = 0
+    float nlo[3];  // RN(RN(-f*y) - e); NaN where y is infinite
+    float nhi[3];  // RN(RN(-f*y) + e); NaN where y is infinite
     bool exact;
 };
 
@@ -94,16 +96,22 @@ __device__ __forceinline__ ObjRay make_objray(const V3 &from, const RayR &R, flo
     q.R = R;
     q.exact = exact;
     const float f[3] = {from.x, from.y, from.z}, y[3] = {R.inv.x, R.inv.y, R.inv.z};
-    const float d[3] = {R.d.x, R.d.y, R.d.z};
+    const float inf = __int_as_float(0x7f800000), nan = __int_as_float(0x7fffffff);
     for (int k = 0; k < 3; k++) {
-        q.nf[k] = -f[k] * y[k];
-        // |t~ - t| <= 2u|t| + u|f y| (+ rounding) with |t| <= (M + |f|)|y|:
-        // 2^-21 = 8u on (M + 2|f|)|y| leaves a factor of ~2 of headroom.
-        // d = 0 (y infinite): bound_t::cross skips the axis; with an infinite
-        // bound every t of that axis widens to (-inf, inf) or to NaN, which
-        // fminf / fmaxf ignore, so the axis adds no constraint.
-        q.err[k] = d[k] == 0.f ? __int_as_float(0x7f800000)
-                               : (coord_max + 2.f * fabsf(f[k])) * fabsf(y[k]) * 0x1p-21f;
+        // With b and f bounded by M + |f| in magnitude, bound_t::cross's
+        // RN(RN(b - f) / d) is within 2u (M + |f|)|y| of the exact t, and
+        // RN(b*y + RN(nf -+ e)) within 2u (M + 2|f|)|y| of t -+ e; e = 2^-20
+        // (M + 2|f|)|y| = 16u (M + 2|f|)|y| covers both with a factor of 4
+        // to spare.
+        const float nf = -f[k] * y[k];
+        const float e = (coord_max + 2.f * fabsf(f[k])) * fabsf(y[k]) * 0x1p-20f;
+        // An infinite y (d = 0, which bound_t::cross skips, or a subnormal
+        // d) gives the axis NaN plane distances, which the fmaxf / fminf
+        // below ignore: the axis constrains nothing.  The largest component
+        // of a unit direction always has a finite y.
+        const bool skip = fabsf(y[k]) == inf;
+        q.nlo[k] = skip ? nan : nf - e;
+        q.nhi[k] = skip ? nan : nf + e;
     }
     return q;
 }
@@ -116,14 +124,16 @@ __device__ __forceinline__ ObjRay make_objray(const V3 &from, const RayR &R, flo
 __device__ __forceinline__ bool box_where_obj(const float *bmin, const float *bmax, const ObjRay &q, float dist,
                                               float &where) {
     if (q.exact) return box_where(bmin, bmax, q.from, q.R, dist, where);
-    float lo = -__int_as_float(0x7f800000), hi = __int_as_float(0x7f800000);
+    // the near plane is the box's min where y > 0, its max where y < 0
+    float n[3], f[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const float y = k == 0 ? q.R.inv.x : (k == 1 ? q.R.inv.y : q.R.inv.z);
-        const float t1 = __fmaf_rn(bmin[k], y, q.nf[k]), t2 = __fmaf_rn(bmax[k], y, q.nf[k]);
-        lo = fmaxf(lo, fminf(t1, t2) - q.err[k]);
-        hi = fminf(hi, fmaxf(t1, t2) + q.err[k]);
+        const bool ng = y < 0.f;
+        n[k] = __fmaf_rn(ng ? bmax[k] : bmin[k], y, q.nlo[k]);
+        f[k] = __fmaf_rn(ng ? bmin[k] : bmax[k], y, q.nhi[k]);
     }
+    const float lo = fmaxf(fmaxf(n[0], n[1]), n[2]), hi = fminf(fminf(f[0], f[1]), f[2]);
     const bool ok = (lo <= hi) && (hi >= 0.f) && (lo <= dist);
     where = ok ? fmaxf(lo, 0.f) : where;  // untouched on a miss, as box_where
     return ok;
