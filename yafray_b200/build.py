@@ -32,10 +32,8 @@ def _compile(src: str) -> str:
             + [os.path.getmtime(os.path.join(HERE, "..", "include", "yr.h"))]):
         return obj
     cmd = [NVCC] + ARCH + COMMON + EXTRA + ["-c", src, "-o", obj]
-    if src.endswith(".cu"):
-        cmd[1:1] = ["-Xptxas", "-v"] if os.environ.get("YR_PTXAS_V") else []
-    else:
-        cmd += ["-x", "cu"] if False else []
+    if src.endswith(".cu") and os.environ.get("YR_PTXAS_V"):
+        cmd[1:1] = ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -616,7 +616,6 @@ __device__ __forceinline__ void st_shade_camera(const DevScene &S, const DevRend
     // directions of takeSample (pathlight.cc:305-312)
     bool paths = false;
     if (active) {
-        const DevShader sh = R.shaders[sp.shader];
         const C3 dif = modulated_color(R.shaders + sp.shader, sp, eye);  // getDiffuse(sp, eye)
         paths = !(energy(dif) < 0.05f);
         const DevLight PL = R.lights[R.path_light];
