@@ -416,6 +416,71 @@ struct ObjIter {
     }
 };
 
+// The casters' BVH walk of a shadow ray: ObjIter's nearest-first descent
+// without its pruning by distance, which never applies to a shadow ray
+// (the segment's end `dist` stays fixed, and every pushed child was
+// crossed before it), so the stack holds node codes only.
+struct CasterIter {
+    int st[kMaxObjStack];
+    int sp;
+    int current;             // object index or -1
+#ifdef YR_COUNT_OBJ
+    uint32_t steps = 0;
+#endif
+
+    __device__ __forceinline__ void down(const DevScene &S, int code, const ObjRay &ray, float dist) {
+        for (;;) {
+            if (code < 0) {
+                current = ~code;
+                return;
+            }
+            const float4 *rec = S.sonodes + 4 * (size_t)code;
+#ifdef YR_COUNT_OBJ
+            steps++;
+#endif
+            const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
+            const float lmin[3] = {q0.x, q0.y, q0.z}, lmax[3] = {q0.w, q1.x, q1.y};
+            const float rmin[3] = {q1.z, q1.w, q2.x}, rmax[3] = {q2.y, q2.z, q2.w};
+            float hl = __int_as_float(0x7f800000), hr = __int_as_float(0x7f800000);
+            const bool hitl = box_where_obj(lmin, lmax, ray, dist, hl);
+            const bool hitr = box_where_obj(rmin, rmax, ray, dist, hr);
+            if (!hitl && !hitr) {
+                if (sp == 0) {
+                    current = -1;
+                    return;
+                }
+                code = st[--sp];
+                continue;
+            }
+            const int lc = __float_as_int(q3.x), rc = __float_as_int(q3.y);
+            if (hitl && hitr) {
+                if (sp >= kMaxObjStack) {
+                    dev_fail(S.status, kDevStackOverflow);
+                    current = -1;
+                    return;
+                }
+                st[sp++] = hl < hr ? rc : lc;
+                code = hl < hr ? lc : rc;
+            } else {
+                code = hitl ? lc : rc;
+            }
+        }
+    }
+
+    __device__ __forceinline__ void start(const DevScene &S, const ObjRay &ray, float dist) {
+        sp = 0;
+        current = -1;
+        if (S.nsotree == 0) return;
+        float w = 0.f;
+        if (box_where_obj(S.sotb, S.sotb + 3, ray, dist, w)) down(S, S.soroot, ray, dist);
+    }
+
+    __device__ __forceinline__ void next(const DevScene &S, const ObjRay &ray, float dist) {
+        current = -1;
+        if (sp > 0) down(S, st[--sp], ray, dist);
+    }
+};
+
 // scene_t::isShadowed answered with the shadow-ray tree.  The reference
 // shoots each shadow-casting object whose bound the ray crosses, from
 // p + dir*self_bias for the point's own object and from p + dir*MIN_RAYDIST
@@ -710,8 +775,8 @@ __device__ inline bool scene_occluded_bvh(const DevScene &S, const V3 &p, int ow
     const V3 p2 = p + dir * kMinRayDist;
     const RayR ray = make_rayr(dir);
     const ObjRay oray = make_objray(p2, ray, S.coord_max, false);
-    ObjIter it;
-    it.start_tree(S, S.sonodes, S.sotb, S.soroot, S.nsotree, oray, dist);
+    CasterIter it;
+    it.start(S, oray, dist);
     while (it.current >= 0) {
         const int o = it.current;
         const DevObject &obj = S.objects[o];
@@ -733,7 +798,7 @@ __device__ inline bool scene_occluded_bvh(const DevScene &S, const V3 &p, int ow
                 return true;
             }
         }
-        it.next(S, oray);
+        it.next(S, oray, dist);
     }
 #ifdef YR_COUNT_OBJ
     nodes += it.steps;
