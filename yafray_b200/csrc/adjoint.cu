@@ -423,14 +423,18 @@ static yr_status enqueue_backward(yr_scene *scene, const AdjPlan &AP, char *blk,
     const DevScene &D = scene->dev;
     const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
 #if YR_TRACE_GRID_PERSIST
-    const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false>));
+    const int gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false, true>));
     const int gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce<false>));
 #else
     const int gq = grid_for(vcap * std::max(P.ns, 1u), kBlock), gb = gq;
 #endif
     const bool inst = D.insts != nullptr;
     auto k_prim = inst ? k_primary<true> : k_primary<false>;
-    auto k_shadow = inst ? k_trace_shadow_q<true> : k_trace_shadow_q<false>;
+    // the shadow queue kernel with the casters' BVH walk alone when the
+    // scene uses it (no shadow-ray tree, no exact order)
+    const bool bvh = !D.use_sh_tree && !D.exact_order;
+    auto k_shadow = inst ? (bvh ? k_trace_shadow_q<true, true> : k_trace_shadow_q<true, false>)
+                         : (bvh ? k_trace_shadow_q<false, true> : k_trace_shadow_q<false, false>);
     auto k_bounce = inst ? k_trace_bounce<true> : k_trace_bounce<false>;
     for (uint64_t b = 0; b < P.total; b += wcap) {
         W.base = (uint32_t)b;

@@ -651,21 +651,25 @@ static __global__ void __launch_bounds__(kBlock, YR_SHADE_MINB) k_shade_camera(D
 }
 #endif
 
-// one queued shadow ray; false for a place without a ray (kNoSlot)
-template <bool INST>
+// one queued shadow ray; false for a place without a ray (kNoSlot).  BVH:
+// the scene uses the casters' BVH (neither the shadow-ray tree nor the
+// exact order), so the kernel holds that walk alone
+template <bool INST, bool BVH = false>
 __device__ __forceinline__ bool st_trace_shadow(const DevScene &S, const Wave &W, uint32_t q, float self_bias,
                                                 const KdStack &stk, uint32_t &nodes, uint32_t &tests) {
     const uint32_t slot = W.shq_slot[q];
     if (slot == kNoSlot) return false;
     const float4 a = W.shq0[q], b = W.shq1[q];
-    const bool occ = scene_occluded_t<INST>(S, v3(a.x, a.y, a.z), __float_as_int(a.w), v3(b.x, b.y, b.z), b.w, self_bias,
-                                    stk, nodes, tests);
+    const V3 p = v3(a.x, a.y, a.z), l = v3(b.x, b.y, b.z);
+    const int own = __float_as_int(a.w);
+    const bool occ = BVH ? scene_occluded_bvh<INST>(S, p, own, l, b.w, self_bias, stk, nodes, tests)
+                         : scene_occluded_t<INST>(S, p, own, l, b.w, self_bias, stk, nodes, tests);
     W.slot_f[slot] = occ ? kSlotShadowed : kSlotLit;
     return true;
 }
 
 #ifdef YR_WAVE_KERNELS
-template <bool INST>
+template <bool INST, bool BVH>
 static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q(DevScene S, Wave W, float self_bias) {
     uint2 stk_nt[kKdStackCap];
     float stk_split[kKdStackCap];
@@ -681,11 +685,11 @@ static __global__ void __launch_bounds__(kBlock, YR_TRACE_MINB) k_trace_shadow_q
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
         const uint32_t q = base + (threadIdx.x & 31u);
-        if (q < n && st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests)) rays++;
+        if (q < n && st_trace_shadow<INST, BVH>(S, W, q, self_bias, stk, nodes, tests)) rays++;
     }
 #else
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-        if (st_trace_shadow<INST>(S, W, q, self_bias, stk, nodes, tests)) rays++;
+        if (st_trace_shadow<INST, BVH>(S, W, q, self_bias, stk, nodes, tests)) rays++;
 #endif
     count_work(W, YR_K_SHADOW, rays, nodes, tests);
 }

@@ -67,7 +67,7 @@ static WaveGrids waves_begin(yr_scene *scene, const Plan &P, uint32_t wcap, Wave
     }
     const uint32_t vcap = std::max(wcap, wcap * std::max(1u, P.npath));
 #if YR_TRACE_GRID_PERSIST
-    G.gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false>));
+    G.gq = std::min(grid_for(vcap * std::max(P.ns, 1u), kBlock), resident_grid(k_trace_shadow_q<false, true>));
     G.gb = std::min(grid_for(vcap, kBlock), resident_grid(k_trace_bounce<false>));
 #else
     G.gq = grid_for(vcap * std::max(P.ns, 1u), kBlock);
@@ -87,7 +87,11 @@ static void wave_launch(yr_scene *scene, const Plan &P, uint32_t wcap, Wave &W, 
     // for scenes that have references
     const bool inst = D.insts != nullptr;
     auto k_prim = inst ? k_primary<true> : k_primary<false>;
-    auto k_shadow = inst ? k_trace_shadow_q<true> : k_trace_shadow_q<false>;
+    // the shadow queue kernel with the casters' BVH walk alone when the
+    // scene uses it (no shadow-ray tree, no exact order)
+    const bool bvh = !D.use_sh_tree && !D.exact_order;
+    auto k_shadow = inst ? (bvh ? k_trace_shadow_q<true, true> : k_trace_shadow_q<true, false>)
+                         : (bvh ? k_trace_shadow_q<false, true> : k_trace_shadow_q<false, false>);
     auto k_bounce = inst ? k_trace_bounce<true> : k_trace_bounce<false>;
     W.base = (uint32_t)b;
     W.count = (uint32_t)std::min<uint64_t>(wcap, P.total - b);
